@@ -1,0 +1,164 @@
+/* nec2c CUDA backend for NVIDIA B200 (sm_100a): public C ABI.
+ *
+ * A "cuda" choice behind nec2c's --fft-backend and --backend selection.  Each
+ * entry point names the reference interface it replaces (file:line in the
+ * N5HXR/nec2c tree).  Conventions follow the reference: int results are 1 for
+ * success and 0 for failure unless stated; vectors are complex double arrays
+ * in host memory owned by the caller; plans own their device storage.  The
+ * library never falls back to a CPU path: without a usable CUDA device every
+ * compute entry point fails and nec2c_cuda_last_error() says why.
+ */
+#ifndef NEC2C_CUDA_H
+#define NEC2C_CUDA_H
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+typedef struct { double re, im; } nec2c_cuda_complex;
+#else
+#include <complex.h>
+typedef double complex nec2c_cuda_complex;
+#endif
+
+/* ------------------------------------------------------------ runtime */
+/* 1 when a CUDA device of compute capability 10.x is usable. */
+int nec2c_cuda_available(void);
+/* Text of the last failure on this thread ("" when none). */
+const char *nec2c_cuda_last_error(void);
+/* Enqueue this thread's work on the given cudaStream_t (NULL: legacy default). */
+void nec2c_cuda_set_stream(void *cuda_stream);
+/* Number of kernels this library has launched since it was loaded. */
+unsigned long long nec2c_cuda_launch_count(void);
+
+/* ------------------------------------------------- volume FFT operator */
+/* Replaces vie_fft_backend_set (vie_fft.h:8) for the names "cuda" (plain FP64
+   form) and "cuda-mixed" (FP32 transforms, FP64 vectors and epilogue).
+   Returns 0 for any other name. */
+int nec2c_cuda_vie_fft_backend_set(const char *name);
+const char *nec2c_cuda_vie_fft_backend_name(void);
+
+typedef struct nec2c_cuda_vie_plan nec2c_cuda_vie_plan;
+
+/* Certified near-pair Green tensor (the reference passes vie_cuboid_n with the
+   options of vie_fft.c:344): the 3x3 volume-averaged N tensor, row-major, of a
+   source cube of edge pitch at the origin seen from the testing cube centred at
+   pitch*offset.  Called for the displacements the far-pair quadrature does not
+   certify (vie_fft.c:319-335).  Returns 1 on success. */
+typedef int (*nec2c_cuda_near_tensor_fn)(void *context, const size_t offset[3], double pitch,
+                                         double k0, nec2c_cuda_complex out[9]);
+
+/* Replaces vie_fft_create (vie_fft.h:21-23, vie_fft.c:378-441): same
+   validation, padding, byte accounting against byte_limit and failure
+   behaviour (*out = NULL, nothing left allocated).  epsilon_r is passed as
+   (re, im).  The far-pair quadrature, spectrum fill and transforms run on the
+   device; near is called on the host for the remaining displacements. */
+int nec2c_cuda_vie_fft_create(nec2c_cuda_vie_plan **out, const size_t shape[3], size_t cells,
+                              const size_t *xyz, double pitch, double k0, double epsilon_re,
+                              double epsilon_im, size_t byte_limit,
+                              nec2c_cuda_near_tensor_fn near, void *near_context);
+/* Replaces vie_fft_set_permittivity (vie_fft.h:26, vie_fft.c:445-455). */
+int nec2c_cuda_vie_fft_set_permittivity(nec2c_cuda_vie_plan *plan, size_t cell, double epsilon_re,
+                                        double epsilon_im);
+/* Replaces vie_fft_destroy (vie_fft.h:27). */
+void nec2c_cuda_vie_fft_destroy(nec2c_cuda_vie_plan *plan);
+/* Replaces vie_fft_bytes (vie_fft.h:28): the reference's accounted bytes. */
+size_t nec2c_cuda_vie_fft_bytes(const nec2c_cuda_vie_plan *plan);
+/* Device memory the plan holds. */
+size_t nec2c_cuda_vie_fft_device_bytes(const nec2c_cuda_vie_plan *plan);
+/* Number of unknowns (3 x cells). */
+size_t nec2c_cuda_vie_fft_order(const nec2c_cuda_vie_plan *plan);
+/* The operator callbacks of vie_fft_operator (vie_fft.h:32): apply is
+   vie_fft.c:239-263, precondition vie_fft.c:265-273.  Host vectors of
+   3 x cells entries; not reentrant per plan (vie_fft.h:6). */
+int nec2c_cuda_vie_fft_apply(void *plan, const nec2c_cuda_complex *x, nec2c_cuda_complex *y);
+int nec2c_cuda_vie_fft_precondition(void *plan, const nec2c_cuda_complex *x,
+                                    nec2c_cuda_complex *y);
+/* Same product on device-resident vectors (no host copies). */
+int nec2c_cuda_vie_fft_apply_device(nec2c_cuda_vie_plan *plan, const void *x_dev, void *y_dev);
+/* Copies the transformed Green spectrum, 6 x padded-grid complex values in the
+   order xx yy zz xy xz yz, each scaled by 1/grid (validation hook). */
+int nec2c_cuda_vie_fft_spectrum(nec2c_cuda_vie_plan *plan, nec2c_cuda_complex *out);
+
+/* --------------------------------------- hybrid conductor + volume system */
+typedef struct nec2c_cuda_hybrid nec2c_cuda_hybrid;
+/* Device half of dielectric_fft_prepare / dielectric_fft_prepare_pec
+   (dielectric_fft.h:10-18): the [C B; D V] operator over an existing volume
+   plan (NULL when there are no cells).  With pec != 0 the plan holds the
+   physical cells followed by their images (dielectric_fft.c:137-154) and
+   volume_unknowns counts the physical ones only. */
+int nec2c_cuda_hybrid_create(nec2c_cuda_hybrid **out, nec2c_cuda_vie_plan *volume,
+                             size_t conductors, size_t volume_unknowns, int pec);
+void nec2c_cuda_hybrid_destroy(nec2c_cuda_hybrid *system);
+/* Uploads the blocks the caller assembled through dielectric_fft_entry
+   (dielectric_fft.c:34-40 layout: c rows of c+v, then v rows of c). */
+int nec2c_cuda_hybrid_set_blocks(nec2c_cuda_hybrid *system, const nec2c_cuda_complex *blocks);
+size_t nec2c_cuda_hybrid_order(const nec2c_cuda_hybrid *system);
+/* Operator callbacks of dielectric_fft_get_operator (dielectric_fft.c:41-83). */
+int nec2c_cuda_hybrid_apply(void *system, const nec2c_cuda_complex *x, nec2c_cuda_complex *y);
+int nec2c_cuda_hybrid_precondition(void *system, const nec2c_cuda_complex *x,
+                                   nec2c_cuda_complex *y);
+
+/* --------------------------------------------------------------- GMRES */
+/* Same layouts as vie_gmres_options / vie_gmres_report (vie_iterative.h:20-47);
+   status uses vie_iterative_status values. */
+typedef struct {
+  size_t restart;
+  size_t maximum_iterations;
+  double relative_tolerance;
+  double absolute_tolerance;
+} nec2c_cuda_gmres_options;
+typedef struct {
+  int status;
+  size_t iterations;
+  size_t operator_applications;
+  size_t restarts;
+  double residual_norm;
+  double relative_residual;
+} nec2c_cuda_gmres_report;
+/* Replaces vie_gmres (vie_iterative.h:55-57) when the operator is a CUDA plan
+   or hybrid system: right-preconditioned restarted GMRES, two MGS passes,
+   complex Givens, true residual at every restart, run device-resident.  NULL
+   options mean the reference defaults {30, 300, 1e-12, 0}.  x is the initial
+   guess and is updated even on failure. */
+int nec2c_cuda_gmres_plan(nec2c_cuda_vie_plan *plan, const nec2c_cuda_complex *b,
+                          nec2c_cuda_complex *x, const nec2c_cuda_gmres_options *options,
+                          nec2c_cuda_gmres_report *report);
+int nec2c_cuda_gmres_hybrid(nec2c_cuda_hybrid *system, const nec2c_cuda_complex *b,
+                            nec2c_cuda_complex *x, const nec2c_cuda_gmres_options *options,
+                            nec2c_cuda_gmres_report *report);
+
+/* ------------------------------------------------------------ dense LU */
+/* Replaces dense_backend_set (dense_backend.h:14) for "cuda" (FP64 LU) and
+   "cuda-mixed" (split-precision tensor-core update plus FP64 refinement in the
+   solve).  Returns 0 for any other name. */
+int nec2c_cuda_dense_backend_set(const char *name);
+const char *nec2c_cuda_dense_backend_name(void);
+/* Replaces dense_backend_factor_classic (dense_backend.h:22-23), called by
+   factr (matrix.c:1318): factors NEC's transposed storage in place.  The
+   factors are the column-major LU of the algebraic matrix with 1-based pivots
+   (the builtin factr's pivot rule); L follows the getrf row convention.  Only
+   this backend's solves consume them.  Returns 1, or 0 when singular/failed. */
+int nec2c_cuda_dense_factor_classic(size_t order, nec2c_cuda_complex *matrix,
+                                    size_t leading_dimension, int *pivots);
+/* Replaces dense_backend_solve_classic(_many) (dense_backend.h:24-32), called by
+   solve (matrix.c:1561) and solves (matrix.c:1683). */
+int nec2c_cuda_dense_solve_classic(size_t order, const nec2c_cuda_complex *matrix,
+                                   size_t leading_dimension, const int *pivots,
+                                   nec2c_cuda_complex *rhs);
+int nec2c_cuda_dense_solve_classic_many(size_t order, const nec2c_cuda_complex *matrix,
+                                        size_t leading_dimension, const int *pivots,
+                                        nec2c_cuda_complex *rhs, size_t rhs_stride,
+                                        size_t rhs_count);
+/* Replaces dense_backend_solve_row_major (dense_backend.h:36-37): row-major
+   system, pivot rule of dense_backend.c:152-190 (largest |.|, first row on
+   ties, pivot must exceed 64 eps), solution returned in rhs.  The matrix is
+   left unchanged. */
+int nec2c_cuda_dense_solve_row_major(nec2c_cuda_complex *matrix, nec2c_cuda_complex *rhs,
+                                     size_t order);
+/* Drops the device copies kept between a factor and its solves. */
+void nec2c_cuda_dense_release(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,258 @@
+"""ctypes view of libnec2c_cuda.so for the test harness and the benchmark.
+
+The product is the C ABI in include/nec2c_cuda.h; this module only loads the
+in-tree library and wraps its entry points with numpy arrays.  It has no CPU
+fallback: importing it without the built library, or calling a compute entry
+point without a CUDA device, raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libnec2c_cuda.so")
+
+NEAR_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_size_t), C.c_double, C.c_double,
+                      C.POINTER(C.c_double))
+
+STATUS = ["converged", "iteration limit", "Krylov breakdown", "operator/preconditioner failure",
+          "invalid input", "workspace allocation/size failure", "nonfinite arithmetic"]
+
+
+class GmresOptions(C.Structure):
+    _fields_ = [("restart", C.c_size_t), ("maximum_iterations", C.c_size_t),
+                ("relative_tolerance", C.c_double), ("absolute_tolerance", C.c_double)]
+
+
+class GmresReport(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_size_t),
+                ("operator_applications", C.c_size_t), ("restarts", C.c_size_t),
+                ("residual_norm", C.c_double), ("relative_residual", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+_lib = None
+
+
+def load():
+    """Loads the in-tree library (raises when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libnec2c_cuda.so is not built (run __graft_entry__.build())")
+    lib = C.CDLL(LIB_PATH)
+    vp, sz, dbl, i = C.c_void_p, C.c_size_t, C.c_double, C.c_int
+    sigs = {
+        "nec2c_cuda_available": (i, []),
+        "nec2c_cuda_last_error": (C.c_char_p, []),
+        "nec2c_cuda_set_stream": (None, [vp]),
+        "nec2c_cuda_launch_count": (C.c_ulonglong, []),
+        "nec2c_cuda_vie_fft_backend_set": (i, [C.c_char_p]),
+        "nec2c_cuda_vie_fft_backend_name": (C.c_char_p, []),
+        "nec2c_cuda_vie_fft_create": (i, [C.POINTER(vp), C.POINTER(sz), sz, C.POINTER(sz), dbl, dbl,
+                                          dbl, dbl, sz, NEAR_FN, vp]),
+        "nec2c_cuda_vie_fft_set_permittivity": (i, [vp, sz, dbl, dbl]),
+        "nec2c_cuda_vie_fft_destroy": (None, [vp]),
+        "nec2c_cuda_vie_fft_bytes": (sz, [vp]),
+        "nec2c_cuda_vie_fft_device_bytes": (sz, [vp]),
+        "nec2c_cuda_vie_fft_order": (sz, [vp]),
+        "nec2c_cuda_vie_fft_apply": (i, [vp, vp, vp]),
+        "nec2c_cuda_vie_fft_precondition": (i, [vp, vp, vp]),
+        "nec2c_cuda_vie_fft_apply_device": (i, [vp, vp, vp]),
+        "nec2c_cuda_vie_fft_spectrum": (i, [vp, vp]),
+        "nec2c_cuda_hybrid_create": (i, [C.POINTER(vp), vp, sz, sz, i]),
+        "nec2c_cuda_hybrid_destroy": (None, [vp]),
+        "nec2c_cuda_hybrid_set_blocks": (i, [vp, vp]),
+        "nec2c_cuda_hybrid_order": (sz, [vp]),
+        "nec2c_cuda_hybrid_apply": (i, [vp, vp, vp]),
+        "nec2c_cuda_hybrid_precondition": (i, [vp, vp, vp]),
+        "nec2c_cuda_gmres_plan": (i, [vp, vp, vp, vp, vp]),
+        "nec2c_cuda_gmres_hybrid": (i, [vp, vp, vp, vp, vp]),
+        "nec2c_cuda_dense_backend_set": (i, [C.c_char_p]),
+        "nec2c_cuda_dense_backend_name": (C.c_char_p, []),
+        "nec2c_cuda_dense_factor_classic": (i, [sz, vp, sz, vp]),
+        "nec2c_cuda_dense_solve_classic": (i, [sz, vp, sz, vp, vp]),
+        "nec2c_cuda_dense_solve_classic_many": (i, [sz, vp, sz, vp, vp, sz, sz]),
+        "nec2c_cuda_dense_solve_row_major": (i, [vp, vp, sz]),
+        "nec2c_cuda_dense_release": (None, []),
+    }
+    for name, (res, args) in sigs.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error():
+    return load().nec2c_cuda_last_error().decode()
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _cvec(x):
+    return np.ascontiguousarray(x, dtype=np.complex128)
+
+
+def table_near(table):
+    """Near-tensor callback backed by a {(a, b, c): 9 complex} mapping."""
+    def cb(ctx, off, h, k, out):
+        key = (off[0], off[1], off[2])
+        t = table.get(key)
+        if t is None:
+            return 0
+        arr = np.asarray(t, dtype=np.complex128).reshape(9)
+        for e in range(9):
+            out[2 * e] = arr[e].real
+            out[2 * e + 1] = arr[e].imag
+        return 1
+    return NEAR_FN(cb)
+
+
+class VolumePlan:
+    """A CUDA volume FFT plan (vie_fft_create with backend "cuda"/"cuda-mixed")."""
+
+    def __init__(self, shape, xyz, pitch, k0, eps, near, byte_limit=1 << 62, mixed=False):
+        lib = load()
+        if not lib.nec2c_cuda_vie_fft_backend_set(b"cuda-mixed" if mixed else b"cuda"):
+            raise RuntimeError("backend selection failed")
+        self._near = near if isinstance(near, NEAR_FN) else table_near(near)
+        xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.uintp).reshape(-1))
+        self.cells = xyz.size // 3
+        sh = (C.c_size_t * 3)(*shape)
+        self.h = C.c_void_p()
+        ok = lib.nec2c_cuda_vie_fft_create(C.byref(self.h), sh, self.cells,
+                                           xyz.ctypes.data_as(C.POINTER(C.c_size_t)), pitch, k0,
+                                           complex(eps).real, complex(eps).imag, byte_limit,
+                                           self._near, None)
+        if not ok:
+            self.h = None
+            raise RuntimeError("nec2c_cuda_vie_fft_create failed: " + last_error())
+        self.n = 3 * self.cells
+
+    def close(self):
+        if self.h:
+            load().nec2c_cuda_vie_fft_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_permittivity(self, cell, eps):
+        return bool(load().nec2c_cuda_vie_fft_set_permittivity(self.h, cell, complex(eps).real,
+                                                                complex(eps).imag))
+
+    def apply(self, x):
+        x = _cvec(x)
+        y = np.empty_like(x)
+        if not load().nec2c_cuda_vie_fft_apply(self.h, _ptr(x), _ptr(y)):
+            raise RuntimeError("apply failed: " + last_error())
+        return y
+
+    def precondition(self, x):
+        x = _cvec(x)
+        y = np.empty_like(x)
+        if not load().nec2c_cuda_vie_fft_precondition(self.h, _ptr(x), _ptr(y)):
+            raise RuntimeError("precondition failed: " + last_error())
+        return y
+
+    def spectrum(self, grid):
+        out = np.empty(6 * grid, dtype=np.complex128)
+        if not load().nec2c_cuda_vie_fft_spectrum(self.h, _ptr(out)):
+            raise RuntimeError("spectrum failed: " + last_error())
+        return out
+
+    def bytes(self):
+        return load().nec2c_cuda_vie_fft_bytes(self.h)
+
+    def device_bytes(self):
+        return load().nec2c_cuda_vie_fft_device_bytes(self.h)
+
+    def gmres(self, b, x0=None, restart=30, maxit=300, rtol=1e-12, atol=0.0):
+        return _gmres(load().nec2c_cuda_gmres_plan, self.h, b, x0, restart, maxit, rtol, atol)
+
+
+def _gmres(fn, handle, b, x0, restart, maxit, rtol, atol):
+    b = _cvec(b)
+    x = np.zeros_like(b) if x0 is None else _cvec(x0).copy()
+    opts = GmresOptions(restart, maxit, rtol, atol)
+    rep = GmresReport()
+    ok = fn(handle, _ptr(b), _ptr(x), C.byref(opts), C.byref(rep))
+    return bool(ok), x, rep.as_dict()
+
+
+class HybridSystem:
+    """The [C B; D V] operator of dielectric_fft.c on the device."""
+
+    def __init__(self, plan, conductors, volume_unknowns, pec=False):
+        lib = load()
+        self.plan = plan
+        self.h = C.c_void_p()
+        if not lib.nec2c_cuda_hybrid_create(C.byref(self.h), plan.h if plan else None, conductors,
+                                            volume_unknowns, 1 if pec else 0):
+            self.h = None
+            raise RuntimeError("hybrid create failed: " + last_error())
+        self.n = conductors + volume_unknowns
+
+    def close(self):
+        if self.h:
+            load().nec2c_cuda_hybrid_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_blocks(self, blocks):
+        self._blocks = _cvec(blocks)
+        if not load().nec2c_cuda_hybrid_set_blocks(self.h, _ptr(self._blocks)):
+            raise RuntimeError("set_blocks failed: " + last_error())
+
+    def apply(self, x):
+        x = _cvec(x)
+        y = np.empty_like(x)
+        if not load().nec2c_cuda_hybrid_apply(self.h, _ptr(x), _ptr(y)):
+            raise RuntimeError("apply failed: " + last_error())
+        return y
+
+    def precondition(self, x):
+        x = _cvec(x)
+        y = np.empty_like(x)
+        ok = load().nec2c_cuda_hybrid_precondition(self.h, _ptr(x), _ptr(y))
+        return bool(ok), y
+
+    def gmres(self, b, x0=None, restart=30, maxit=300, rtol=1e-12, atol=0.0):
+        return _gmres(load().nec2c_cuda_gmres_hybrid, self.h, b, x0, restart, maxit, rtol, atol)
+
+
+def dense_backend_set(name):
+    return bool(load().nec2c_cuda_dense_backend_set(name.encode()))
+
+
+def factor_classic(storage, ld=None):
+    """Factors NEC's transposed storage (a Fortran-ordered ld x n complex array) in place."""
+    n = storage.shape[1]
+    ld = storage.shape[0] if ld is None else ld
+    assert storage.dtype == np.complex128 and storage.flags.f_contiguous
+    piv = np.zeros(n, dtype=np.int32)
+    ok = load().nec2c_cuda_dense_factor_classic(n, _ptr(storage), ld, _ptr(piv))
+    return bool(ok), piv
+
+
+def solve_classic_many(storage, piv, rhs, ld=None):
+    n = storage.shape[1]
+    ld = storage.shape[0] if ld is None else ld
+    assert rhs.dtype == np.complex128 and rhs.flags.f_contiguous
+    ok = load().nec2c_cuda_dense_solve_classic_many(n, _ptr(storage), ld, _ptr(piv), _ptr(rhs),
+                                                   rhs.shape[0], rhs.shape[1])
+    return bool(ok)
+
+
+def solve_row_major(a, b):
+    a = _cvec(a)
+    b = _cvec(b).copy()
+    ok = load().nec2c_cuda_dense_solve_row_major(_ptr(a), _ptr(b), b.size)
+    return bool(ok), b

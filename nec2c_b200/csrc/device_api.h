@@ -1,0 +1,129 @@
+/* Device layer of the nec2c CUDA backend: C-linkage entry points implemented
+ * in CUDA C++ (csrc/*.cu) and called by the C host layer (host/*.c).  Not part
+ * of the public ABI (that is include/nec2c_cuda.h).  All pointers named *_dev
+ * are device pointers; everything else is host memory. */
+#ifndef NEC2C_DEVICE_API_H
+#define NEC2C_DEVICE_API_H
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error text of the last failed call on this thread. */
+const char *n2d_last_error(void);
+void n2c_set_error(const char *fmt, ...);
+/* Stream all work of this thread is enqueued on (NULL = legacy default). */
+void n2d_set_stream(void *stream);
+void *n2d_get_stream(void);
+int n2d_sync(void);
+/* Device flag checked by operator kernels (0 = skip the launch's work). */
+void n2d_set_gate(const int *gate_dev);
+/* Device buffers and copies on the current stream. */
+void *n2d_alloc(size_t bytes);
+void n2d_free(void *p);
+int n2d_upload(void *dst_dev, const void *src, size_t bytes);
+int n2d_download(void *dst, const void *src_dev, size_t bytes);
+int n2d_memset(void *dst_dev, int value, size_t bytes);
+int n2d_copy_d2d(void *dst_dev, const void *src_dev, size_t bytes);
+/* Pitched copies (cudaMemcpy2D semantics: width bytes per row, rows rows). */
+int n2d_upload2d(void *dst_dev, size_t dpitch, const void *src, size_t spitch, size_t width,
+                 size_t rows);
+int n2d_download2d(void *dst, size_t dpitch, const void *src_dev, size_t spitch, size_t width,
+                   size_t rows);
+/* 1 when a compute capability 10.x device is present. */
+int n2d_device_ok(void);
+/* Kernels this library has launched since load (for the launch-count check). */
+unsigned long long n2d_launch_count(void);
+
+/* ---- volume FFT operator (vie_fft.c's plan) ---- */
+typedef struct n2d_vie n2d_vie;
+/* shape = lattice extent, padded = FFT grid (each a power of two <= 1024,
+   >= 2*shape-1); cell_box[c] = (x*shape1 + y)*shape2 + z. */
+int n2d_vie_create(n2d_vie **out, const long long shape[3], const long long padded[3],
+                   long long cells, const int *cell_box, const double *const twiddles[3],
+                   int fp32);
+/* Gauss-Legendre nodes / weights on [0,1], orders 4, 6, 8, 12 (4 x 12 each). */
+int n2d_vie_set_gauss(const double *nodes, const double *weights);
+void n2d_vie_destroy(n2d_vie *p);
+size_t n2d_vie_device_bytes(const n2d_vie *p);
+int n2d_vie_fp32(const n2d_vie *p);
+long long n2d_vie_cells(const n2d_vie *p);
+/* Green spectrum.  offsets: sorted displacements a>=b>=c in enumeration order
+   (a outer, then b, then c); sorted_shape: shape sorted descending.  The far
+   kernel fills what it can and flags (0) the entries that need the caller's
+   certified near-pair tensor; put_tensors supplies those (6 complex each, xx yy
+   zz xy xz yz, already symmetrised and with the reference's zeroing applied). */
+int n2d_vie_far_tensors(n2d_vie *p, long long count, const int *offsets,
+                        const long long sorted_shape[3], double pitch, double k0,
+                        int *far_ok);
+int n2d_vie_put_tensors(n2d_vie *p, long long count, const long long *index,
+                        const double *tensors);
+int n2d_vie_finish_spectrum(n2d_vie *p);
+/* Downloads the transformed spectrum (6 x G, FP64, scaled by 1/G). */
+int n2d_vie_read_spectrum(n2d_vie *p, double *out);
+/* Per-cell permittivity (2 doubles each) and self terms (3 complex). */
+int n2d_vie_set_eps(n2d_vie *p, const double *eps, const double *self);
+/* y_dev = A z where z = x_dev (or x_dev ./ diag when precondition_input).
+   When norm_dev is non-NULL, the sum of |y|^2 is written there (and a
+   non-finite y sets *flag_dev to 1 when flag_dev is non-NULL). */
+int n2d_vie_apply(n2d_vie *p, const double *x_dev, double *y_dev, int precondition_input,
+                  double *norm_dev, int *flag_dev);
+/* y_dev = x_dev ./ (eps - (eps-1) self). */
+int n2d_vie_precondition(n2d_vie *p, const double *x_dev, double *y_dev);
+const double *n2d_vie_diag(const n2d_vie *p);
+/* PEC image embedding: the plan's cells are physical_cells physical cells
+   followed by their images; apply/precondition then act on the physical half. */
+void n2d_vie_set_mirror(n2d_vie *p, long long physical_cells);
+
+/* ---- hybrid [C B; D V] operator (dielectric_fft.c) ---- */
+typedef struct n2d_hybrid n2d_hybrid;
+int n2d_hybrid_create(n2d_hybrid **out, n2d_vie *volume, long long conductors,
+                      long long volume_unknowns, int pec);
+void n2d_hybrid_destroy(n2d_hybrid *h);
+/* Uploads the dense blocks (c*(c+v) + v*c complex, dielectric_fft.c:34-40). */
+int n2d_hybrid_upload_blocks(n2d_hybrid *h, const double *blocks);
+int n2d_hybrid_apply(n2d_hybrid *h, const double *x_dev, double *y_dev, int precondition_input,
+                     double *norm_dev, int *flag_dev);
+int n2d_hybrid_precondition(n2d_hybrid *h, const double *x_dev, double *y_dev);
+long long n2d_hybrid_order(const n2d_hybrid *h);
+/* 0 when a conductor diagonal is zero or non-finite (dielectric_fft.c:77-81). */
+int n2d_hybrid_precondition_ok(const n2d_hybrid *h);
+
+/* ---- device-resident GMRES (vie_iterative.c) ---- */
+typedef struct {
+  int status;
+  size_t iterations, operator_applications, restarts;
+  double residual_norm, relative_residual;
+} n2d_gmres_report;
+/* kind 0: volume plan, kind 1: hybrid system.  b, x are host vectors. */
+int n2d_gmres(int kind, void *op, long long n, const double *b, double *x,
+              size_t restart, size_t maximum_iterations, double rtol, double atol,
+              n2d_gmres_report *report);
+/* Same with device-resident b and x. */
+int n2d_gmres_dev(int kind, void *op, long long n, const double *b_dev, double *x_dev,
+                  size_t restart, size_t maximum_iterations, double rtol, double atol,
+                  n2d_gmres_report *report);
+
+/* ---- dense LU (matrix.c factr/solve, dense_backend.c) ---- */
+/* Factor order x order in place on the device (column-major, leading dim ld),
+   partial pivoting.  rule 0: largest |.|^2, later row wins ties (factr);
+   rule 1: largest |.|, first row wins, pivot must exceed 64 eps (row-major
+   builtin).  pivots_dev receives 1-based pivot rows.  precision 0 = FP64,
+   1 = split-FP32 tensor-core update (the caller refines). */
+int n2d_lu_factor(double *a_dev, long long order, long long ld, int *pivots_dev, int rule,
+                  int precision, int *info_host);
+/* Solve with factors from n2d_lu_factor: interchanges + unit-lower forward +
+   upper back substitution, for nrhs columns of b_dev (leading dim ldb). */
+int n2d_lu_solve(const double *a_dev, long long order, long long ld, const int *pivots_dev,
+                 double *b_dev, long long ldb, long long nrhs);
+/* In-place device transpose of an order x order block (leading dims lda/ldb). */
+int n2d_transpose(const double *src_dev, long long lds, double *dst_dev, long long ldd,
+                  long long rows, long long cols);
+/* r = b - A x for a column-major complex matrix (FP64), r may alias b. */
+int n2d_residual(const double *a_dev, long long order, long long ld, const double *x_dev,
+                 const double *b_dev, double *r_dev, long long nrhs, long long ldb);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

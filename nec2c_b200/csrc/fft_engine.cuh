@@ -1,0 +1,260 @@
+// Line-FFT engine for the padded Green-convolution grid.
+//
+// A length-L line (L = R1*R2, powers of two up to 1024) is transformed in two
+// register steps with one shared-memory exchange (the "four-step" split):
+//   forward : step 1 (per j2)  R1-point DFT over x[j2 + R2*j1], twiddle W^{j2 k1}
+//             step 2 (per k1)  R2-point DFT  -> X[k1 + R1*k2]
+//   inverse : step A (per k1)  R2-point DFT over X[k1 + R1*k2], twiddle W^{-n1 k1}
+//             step B (per n1)  R1-point DFT  -> x[n1 + R2*n2]
+// The shared slot of intermediate (j2|n1, k1) is (j2|n1) + R2*k1 in both
+// directions, so a forward step 2 can feed an inverse step A in registers with
+// no extra exchange (used by the spectrum-product pass).
+//
+// Tiles hold NL lines (NL a power of two <= 32).  Work items are mapped
+// line-fastest so a warp touches 32 consecutive lines: in the strided passes
+// (y and x axes) consecutive lines are consecutive addresses, so every global
+// access is coalesced.  Shared layout is [slot][line].
+#pragma once
+#include "common.cuh"
+
+namespace n2c {
+
+template <int R> __host__ __device__ constexpr int bitrev_c(int i) {
+  int r = 0;
+  for (int b = 1, rb = R >> 1; b < R; b <<= 1, rb >>= 1)
+    if (i & b) r |= rb;
+  return r;
+}
+
+// In-register radix-2 DIT DFT of R points (natural-order output).
+// tw[m] = exp(-2 pi i m / L); the R-point root W_R^m is tw[m * STRIDE].
+template <int R, bool INV, int STRIDE, typename C>
+__device__ __forceinline__ void dft_reg(C (&a)[R], const C *__restrict__ tw) {
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int r = bitrev_c<R>(i);
+    if (i < r) { C t = a[i]; a[i] = a[r]; a[r] = t; }
+  }
+#pragma unroll
+  for (int span = 2; span <= R; span <<= 1) {
+    const int half = span >> 1;
+#pragma unroll
+    for (int base = 0; base < R; base += span) {
+#pragma unroll
+      for (int k = 0; k < half; ++k) {
+        C u = a[base + k], v = a[base + k + half];
+        if (k != 0) {
+          C w = __ldg(&tw[k * (R / span) * STRIDE]);
+          if (INV) w.y = -w.y;
+          v = cmul(v, w);
+        }
+        a[base + k] = cadd(u, v);
+        a[base + k + half] = csub(u, v);
+      }
+    }
+  }
+}
+
+template <typename C> struct PassArgs {
+  const C *in;
+  C *out;
+  const C *tw;        // exp(-2 pi i m / L), m < L
+  const C *spec;      // product pass: 6 spectrum slots (xx yy zz xy xz yz)
+  long long lines;    // number of lines (B * I)
+  long long I;        // distance between consecutive axis elements (1 = contiguous lines)
+  long long A_in, A_out;        // axis extent stored in the input / output array
+  int n_in, n_out;    // nonzero inputs (rest is zero padding) / outputs kept
+  int NL;             // lines per tile
+  const int *gate;    // skip all work when *gate == 0 (NULL: always run)
+  long long comp_in, comp_out;  // product pass: distance between the 3 components
+  long long spec_comp;          // product pass: distance between spectrum slots
+};
+
+template <typename C>
+__device__ __forceinline__ void line_base(const PassArgs<C> &a, long long l, long long &bin, long long &bout) {
+  const long long b = l / a.I, i = l - b * a.I;
+  bin = b * a.A_in * a.I + i;
+  bout = b * a.A_out * a.I + i;
+}
+
+// Forward transform of one component per tile.
+template <typename C, int R1, int R2>
+__global__ void __launch_bounds__(256) fft_forward_pass(PassArgs<C> a) {
+  if (a.gate && *(volatile const int *)a.gate == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *S = reinterpret_cast<C *>(smem_raw);
+  const int NL = a.NL;
+  const long long l0 = (long long)blockIdx.x * NL;
+  for (int item = threadIdx.x; item < NL * R2; item += blockDim.x) {
+    const int t = item & (NL - 1), j2 = item / NL;
+    const long long l = l0 + t;
+    if (l >= a.lines) continue;
+    long long bin, bout;
+    line_base(a, l, bin, bout);
+    C v[R1];
+#pragma unroll
+    for (int j1 = 0; j1 < R1; ++j1) {
+      const int e = j2 + R2 * j1;
+      v[j1] = e < a.n_in ? a.in[bin + (long long)e * a.I] : czero<C>();
+    }
+    dft_reg<R1, false, R2>(v, a.tw);
+#pragma unroll
+    for (int k1 = 1; k1 < R1; ++k1)
+      if (j2) v[k1] = cmul(v[k1], __ldg(&a.tw[j2 * k1]));
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) S[(j2 + R2 * k1) * NL + t] = v[k1];
+  }
+  __syncthreads();
+  for (int item = threadIdx.x; item < NL * R1; item += blockDim.x) {
+    const int t = item & (NL - 1), k1 = item / NL;
+    const long long l = l0 + t;
+    if (l >= a.lines) continue;
+    long long bin, bout;
+    line_base(a, l, bin, bout);
+    C w[R2];
+#pragma unroll
+    for (int j2 = 0; j2 < R2; ++j2) w[j2] = S[(j2 + R2 * k1) * NL + t];
+    dft_reg<R2, false, R1>(w, a.tw);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) {
+      const int e = k1 + R1 * k2;
+      if (e < a.n_out) a.out[bout + (long long)e * a.I] = w[k2];
+    }
+  }
+}
+
+// Inverse transform (unnormalised) of one component per tile.
+template <typename C, int R1, int R2>
+__global__ void __launch_bounds__(256) fft_inverse_pass(PassArgs<C> a) {
+  if (a.gate && *(volatile const int *)a.gate == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *S = reinterpret_cast<C *>(smem_raw);
+  const int NL = a.NL;
+  const long long l0 = (long long)blockIdx.x * NL;
+  for (int item = threadIdx.x; item < NL * R1; item += blockDim.x) {
+    const int t = item & (NL - 1), k1 = item / NL;
+    const long long l = l0 + t;
+    if (l >= a.lines) continue;
+    long long bin, bout;
+    line_base(a, l, bin, bout);
+    C w[R2];
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) {
+      const int e = k1 + R1 * k2;
+      w[k2] = e < a.n_in ? a.in[bin + (long long)e * a.I] : czero<C>();
+    }
+    dft_reg<R2, true, R1>(w, a.tw);
+#pragma unroll
+    for (int n1 = 1; n1 < R2; ++n1)
+      if (k1) w[n1] = cmulc(w[n1], __ldg(&a.tw[n1 * k1]));
+#pragma unroll
+    for (int n1 = 0; n1 < R2; ++n1) S[(n1 + R2 * k1) * NL + t] = w[n1];
+  }
+  __syncthreads();
+  for (int item = threadIdx.x; item < NL * R2; item += blockDim.x) {
+    const int t = item & (NL - 1), n1 = item / NL;
+    const long long l = l0 + t;
+    if (l >= a.lines) continue;
+    long long bin, bout;
+    line_base(a, l, bin, bout);
+    C v[R1];
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) v[k1] = S[(n1 + R2 * k1) * NL + t];
+    dft_reg<R1, true, R2>(v, a.tw);
+#pragma unroll
+    for (int n2 = 0; n2 < R1; ++n2) {
+      const int e = n1 + R2 * n2;
+      if (e < a.n_out) a.out[bout + (long long)e * a.I] = v[n2];
+    }
+  }
+}
+
+// x-axis pass fused with the Green-tensor product: forward x-FFT of the three
+// source components, 3x3 symmetric spectrum product per frequency point, and
+// the inverse x-FFT, all on one tile of lines.  Lines are the (ky,kz) points
+// (I = Py*Pz, one line per inner index, B = 1 per component).
+template <typename C, int R1, int R2>
+__global__ void __launch_bounds__(256) fft_product_pass(PassArgs<C> a) {
+  if (a.gate && *(volatile const int *)a.gate == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *S = reinterpret_cast<C *>(smem_raw);
+  const int NL = a.NL, L = R1 * R2;
+  const long long l0 = (long long)blockIdx.x * NL;
+  for (int item = threadIdx.x; item < 3 * NL * R2; item += blockDim.x) {
+    const int c = item / (NL * R2), rem = item - c * NL * R2;
+    const int t = rem & (NL - 1), j2 = rem / NL;
+    const long long l = l0 + t;
+    if (l >= a.lines) continue;
+    const C *in = a.in + c * a.comp_in + l;
+    C v[R1];
+#pragma unroll
+    for (int j1 = 0; j1 < R1; ++j1) {
+      const int e = j2 + R2 * j1;
+      v[j1] = e < a.n_in ? in[(long long)e * a.I] : czero<C>();
+    }
+    dft_reg<R1, false, R2>(v, a.tw);
+#pragma unroll
+    for (int k1 = 1; k1 < R1; ++k1)
+      if (j2) v[k1] = cmul(v[k1], __ldg(&a.tw[j2 * k1]));
+    C *Sc = S + c * L * NL;
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) Sc[(j2 + R2 * k1) * NL + t] = v[k1];
+  }
+  __syncthreads();
+  for (int item = threadIdx.x; item < NL * R1; item += blockDim.x) {
+    const int t = item & (NL - 1), k1 = item / NL;
+    const long long l = l0 + t;
+    if (l >= a.lines) continue;
+    C s0[R2], s1[R2], s2[R2];
+#pragma unroll
+    for (int j2 = 0; j2 < R2; ++j2) {
+      const int slot = (j2 + R2 * k1) * NL + t;
+      s0[j2] = S[slot]; s1[j2] = S[L * NL + slot]; s2[j2] = S[2 * L * NL + slot];
+    }
+    dft_reg<R2, false, R1>(s0, a.tw);
+    dft_reg<R2, false, R1>(s1, a.tw);
+    dft_reg<R2, false, R1>(s2, a.tw);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) {
+      const long long g = (long long)(k1 + R1 * k2) * a.I + l;
+      const C gxx = a.spec[g], gyy = a.spec[a.spec_comp + g], gzz = a.spec[2 * a.spec_comp + g];
+      const C gxy = a.spec[3 * a.spec_comp + g], gxz = a.spec[4 * a.spec_comp + g], gyz = a.spec[5 * a.spec_comp + g];
+      const C x0 = s0[k2], x1 = s1[k2], x2 = s2[k2];
+      s0[k2] = cadd(cadd(cmul(gxx, x0), cmul(gxy, x1)), cmul(gxz, x2));
+      s1[k2] = cadd(cadd(cmul(gxy, x0), cmul(gyy, x1)), cmul(gyz, x2));
+      s2[k2] = cadd(cadd(cmul(gxz, x0), cmul(gyz, x1)), cmul(gzz, x2));
+    }
+    dft_reg<R2, true, R1>(s0, a.tw);
+    dft_reg<R2, true, R1>(s1, a.tw);
+    dft_reg<R2, true, R1>(s2, a.tw);
+#pragma unroll
+    for (int n1 = 0; n1 < R2; ++n1) {
+      if (k1 && n1) {
+        const C w = __ldg(&a.tw[n1 * k1]);
+        s0[n1] = cmulc(s0[n1], w); s1[n1] = cmulc(s1[n1], w); s2[n1] = cmulc(s2[n1], w);
+      }
+      const int slot = (n1 + R2 * k1) * NL + t;
+      S[slot] = s0[n1]; S[L * NL + slot] = s1[n1]; S[2 * L * NL + slot] = s2[n1];
+    }
+  }
+  __syncthreads();
+  for (int item = threadIdx.x; item < 3 * NL * R2; item += blockDim.x) {
+    const int c = item / (NL * R2), rem = item - c * NL * R2;
+    const int t = rem & (NL - 1), n1 = rem / NL;
+    const long long l = l0 + t;
+    if (l >= a.lines) continue;
+    const C *Sc = S + c * L * NL;
+    C v[R1];
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) v[k1] = Sc[(n1 + R2 * k1) * NL + t];
+    dft_reg<R1, true, R2>(v, a.tw);
+    C *out = a.out + c * a.comp_out + l;
+#pragma unroll
+    for (int n2 = 0; n2 < R1; ++n2) {
+      const int e = n1 + R2 * n2;
+      if (e < a.n_out) out[(long long)e * a.I] = v[n2];
+    }
+  }
+}
+
+}  // namespace n2c

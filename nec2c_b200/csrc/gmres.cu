@@ -1,0 +1,452 @@
+// Device-resident restarted GMRES(m) for the volume plan and the hybrid
+// system: vie_iterative.c:80-199 (vie_gmres) with the operator, the two-pass
+// modified Gram-Schmidt, the Givens least squares and the true residual all on
+// the device.  The host reads a small state block once per restart cycle.
+//
+// Per inner iteration j the host enqueues: the preconditioned matvec
+// w = A D^-1 v_j (with ||w||), then one cooperative kernel that runs both MGS
+// passes over v_0..v_j with w held in registers, the norm, the Givens update
+// and v_{j+1} = w/||w||.  Every kernel first checks the device "active" flag,
+// so iterations after convergence cost only a launch.  x += D^-1 (V y) and
+// the true residual close the cycle.  Reductions are deterministic (fixed-order
+// block partials), so results are bitwise reproducible run to run.
+#include <float.h>
+#include <math.h>
+#include <string.h>
+#include "common.cuh"
+#include "device_api.h"
+#include "runtime.cuh"
+#include "vie_internal.cuh"
+
+using namespace n2c;
+
+struct n2d_hybrid;
+int n2c_hybrid_precondition_ok(const n2d_hybrid *h);
+const double2 *n2c_hybrid_pdiag(const n2d_hybrid *h);
+int n2c_norm2(const double *y, long long n, double *partials, unsigned int *ticket, double *out,
+              int *flag);
+
+enum { ST_CONVERGED, ST_LIMIT, ST_BREAKDOWN, ST_CALLBACK, ST_INVALID, ST_ALLOC, ST_NONFINITE };
+enum { ST_RUNNING = -1 };
+
+struct GmState {
+  int active;          // inner loop of the current cycle still running
+  int status;          // ST_RUNNING or a final status
+  int breakdown;
+  int used;            // inner iterations done in the current cycle
+  int flag;            // non-finite raised by a kernel
+  int barrier_error;   // grid barrier gave up (never expected under cooperative launch)
+  long long iterations, max_iterations;
+  double target, before_sq, residual_sq;
+  unsigned int bar_count, bar_gen;
+};
+
+struct GmBuffers {
+  GmState *st;
+  double2 *H, *g, *sn, *y;   // (m+1) x m Hessenberg (row-major), rotations, solution
+  double *cs;
+  double2 *V, *w, *r, *tmp;  // basis (m+1) x n, work vectors
+  double *partials;          // 2 x grid partials
+  unsigned int *ticket;
+};
+
+// ---------------------------------------------------------- grid barrier
+// Sense-by-generation barrier for a cooperative launch.  The spin is bounded
+// (clock budget); on time-out the barrier records an error and every block
+// leaves at its next barrier, so the kernel always ends.
+__device__ __forceinline__ bool grid_barrier(GmState *st) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    volatile unsigned int *gen = &st->bar_gen;
+    volatile int *err = &st->barrier_error;
+    if (*err) ok = 0;
+    else {
+      const unsigned int g = *gen;
+      __threadfence();
+      if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
+        st->bar_count = 0;
+        __threadfence();
+        atomicAdd(&st->bar_gen, 1u);
+      } else {
+        const long long t0 = clock64();
+        while (*gen == g) {
+          if (*err || clock64() - t0 > (1LL << 32)) { atomicExch(&st->barrier_error, 1); ok = 0; break; }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// Fixed-order sum of the grid's block partials (same value in every block).
+__device__ __forceinline__ double2 sum_partials(const double2 *partials) {
+  double2 t = make_double2(0, 0);
+  for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) t = cadd(t, partials[i]);
+  return block_sum(t);
+}
+
+__device__ __forceinline__ double cabs_(double2 a) { return hypot(a.x, a.y); }
+
+// Complex unitary Givens [c s; -conj(s) c], vie_iterative.c:66-78.
+__device__ void givens(double2 a, double2 b, double *c, double2 *s) {
+  const double aa = cabs_(a), bb = cabs_(b);
+  if (bb == 0.0) { *c = 1.0; *s = make_double2(0, 0); }
+  else if (aa == 0.0) { *c = 0.0; *s = make_double2(b.x / bb, -b.y / bb); }
+  else {
+    const double len = hypot(aa, bb);
+    *c = aa / len;
+    const double2 ua = make_double2(a.x / aa, a.y / aa), ub = make_double2(b.x / len, -b.y / len);
+    *s = cmul(ua, ub);
+  }
+}
+
+// Both MGS passes, the norm, the Givens update and v_{j+1} for iteration j.
+// E = complex elements of w held per thread.
+template <int E>
+__global__ void __launch_bounds__(512) arnoldi_kernel(GmBuffers b, long long n, int m, int j) {
+  GmState *st = b.st;
+  if (!st->active) return;
+  if (st->flag) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) { st->status = ST_NONFINITE; st->active = 0; }
+    return;
+  }
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long base = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double2 w[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const long long i = base + e * stride;
+    w[e] = i < n ? b.w[i] : make_double2(0, 0);
+  }
+  double2 *part[2] = {(double2 *)(b.partials + 4096), (double2 *)(b.partials + 4096) + gridDim.x};
+  int buf = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int k = 0; k <= j; ++k) {
+      const double2 *vk = b.V + (long long)k * n;
+      double2 acc = make_double2(0, 0);
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const long long i = base + e * stride;
+        if (i < n) acc = cadd(acc, cconjmul(vk[i], w[e]));
+      }
+      acc = block_sum(acc);
+      if (threadIdx.x == 0) part[buf][blockIdx.x] = acc;
+      if (!grid_barrier(st)) return;
+      const double2 proj = sum_partials(part[buf]);
+      buf ^= 1;
+      if (blockIdx.x == 0 && threadIdx.x == 0) b.H[(long long)k * m + j] = cadd(b.H[(long long)k * m + j], proj);
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const long long i = base + e * stride;
+        if (i < n) w[e] = csub(w[e], cmul(proj, vk[i]));
+      }
+    }
+  }
+  double sq = 0;
+#pragma unroll
+  for (int e = 0; e < E; ++e) sq += w[e].x * w[e].x + w[e].y * w[e].y;
+  double2 t = block_sum(make_double2(sq, 0));
+  if (threadIdx.x == 0) part[buf][blockIdx.x] = t;
+  if (!grid_barrier(st)) return;
+  const double after = sqrt(sum_partials(part[buf]).x);
+  const double before = sqrt(st->before_sq);
+  const bool broke = after <= 32 * DBL_EPSILON * before;
+  if (isfinite(after) && !broke) {
+    double2 *vn = b.V + (long long)(j + 1) * n;
+    const double inv = after;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const long long i = base + e * stride;
+      if (i < n) vn[i] = make_double2(w[e].x / inv, w[e].y / inv);
+    }
+  }
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  if (!isfinite(after)) { st->status = ST_NONFINITE; st->active = 0; return; }
+  double2 *H = b.H;
+  H[(long long)(j + 1) * m + j] = make_double2(after, 0);
+  for (int k = 0; k < j; ++k) {
+    const double2 h0 = H[(long long)k * m + j], h1 = H[(long long)(k + 1) * m + j];
+    const double2 s = b.sn[k];
+    H[(long long)k * m + j] = cadd(cscale(h0, b.cs[k]), cmul(s, h1));
+    H[(long long)(k + 1) * m + j] = csub(cscale(h1, b.cs[k]), cconjmul(s, h0));
+  }
+  double c;
+  double2 s;
+  givens(H[(long long)j * m + j], H[(long long)(j + 1) * m + j], &c, &s);
+  b.cs[j] = c; b.sn[j] = s;
+  H[(long long)j * m + j] = cadd(cscale(H[(long long)j * m + j], c), cmul(s, H[(long long)(j + 1) * m + j]));
+  H[(long long)(j + 1) * m + j] = make_double2(0, 0);
+  const double2 gj = b.g[j];
+  b.g[j + 1] = make_double2(-(s.x * gj.x + s.y * gj.y), -(s.x * gj.y - s.y * gj.x));  // -conj(s) g_j
+  b.g[j] = cscale(gj, c);
+  st->iterations += 1;
+  st->used = j + 1;
+  st->breakdown = broke;
+  if (broke || cabs_(b.g[j + 1]) <= st->target || j + 1 >= m || st->iterations >= st->max_iterations)
+    st->active = 0;
+}
+
+// v_0 = r / beta and the Hessenberg / rotation reset for a new cycle.
+__global__ void cycle_start_kernel(GmBuffers b, long long n, int m, double beta) {
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = tid; i < n; i += stride) b.V[i] = make_double2(b.r[i].x / beta, b.r[i].y / beta);
+  for (long long i = tid; i < (long long)(m + 1) * m; i += stride) b.H[i] = make_double2(0, 0);
+  for (long long i = tid; i <= m; i += stride) b.g[i] = make_double2(i == 0 ? beta : 0, 0);
+}
+
+// y = H^{-1} g (back substitution, vie_iterative.c:179-186).
+__global__ void backsolve_kernel(GmBuffers b, int m) {
+  GmState *st = b.st;
+  if (st->status != ST_RUNNING) return;
+  const int used = st->used;
+  for (int i = used - 1; i >= 0; --i) {
+    double2 val = b.g[i];
+    for (int k = i + 1; k < used; ++k) val = csub(val, cmul(b.H[(long long)i * m + k], b.y[k]));
+    const double2 d = b.H[(long long)i * m + i];
+    if (cabs_(d) == 0.0) { st->status = ST_BREAKDOWN; return; }
+    b.y[i] = cdiv(val, d);
+  }
+}
+
+// x += D^-1 (sum_j v_j y_j).
+__global__ void update_kernel(GmBuffers b, const double2 *__restrict__ pdiag, double2 *__restrict__ x,
+                              long long n) {
+  if (b.st->status != ST_RUNNING) return;
+  const int used = b.st->used;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double2 acc = make_double2(0, 0);
+    for (int j = 0; j < used; ++j) {
+      double2 z = b.V[(long long)j * n + i];
+      if (pdiag) z = cdiv(z, pdiag[i]);
+      acc = cadd(acc, cmul(z, b.y[j]));
+    }
+    x[i] = cadd(x[i], acc);
+  }
+}
+
+// r = b - A x (A x already in r) with ||r||^2 into residual_sq.
+__global__ void residual_kernel(const double2 *__restrict__ rhs, double2 *__restrict__ r, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    r[i] = csub(rhs[i], r[i]);
+}
+
+// ------------------------------------------------------------------ host side
+struct OpView {
+  int kind;
+  void *op;
+  long long n;
+  const double2 *pdiag;
+};
+
+static int op_apply(const OpView &o, const double *x, double *y, int precond, double *norm, int *flag) {
+  if (o.kind == 0) return n2d_vie_apply((n2d_vie *)o.op, x, y, precond, norm, flag);
+  return n2d_hybrid_apply((n2d_hybrid *)o.op, x, y, precond, norm, flag);
+}
+
+template <int E>
+static int launch_arnoldi(GmBuffers &b, long long n, int m, int j, int blocks, int threads) {
+  void *args[] = {&b, &n, &m, &j};
+  cudaError_t e = cudaLaunchCooperativeKernel((void *)arnoldi_kernel<E>, blocks, threads, args, 0,
+                                              n2c_stream());
+  if (e != cudaSuccess) { n2c_set_error("arnoldi launch: %s", cudaGetErrorString(e)); return 0; }
+  n2c_count_launch(1);
+  return 1;
+}
+
+typedef int (*ArnoldiLauncher)(GmBuffers &, long long, int, int, int, int);
+
+static int arnoldi_shape(long long n, int *blocks, int *threads, ArnoldiLauncher *fn) {
+  static const int Es[] = {1, 2, 4, 8, 16};
+  static const ArnoldiLauncher fns[] = {launch_arnoldi<1>, launch_arnoldi<2>, launch_arnoldi<4>,
+                                        launch_arnoldi<8>, launch_arnoldi<16>};
+  static const void *kern[] = {(void *)arnoldi_kernel<1>, (void *)arnoldi_kernel<2>,
+                               (void *)arnoldi_kernel<4>, (void *)arnoldi_kernel<8>,
+                               (void *)arnoldi_kernel<16>};
+  const int sms = n2c_sm_count();
+  for (int q = 0; q < 5; ++q) {
+    int occ = 0;
+    const int th = 512;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern[q], th, 0) != cudaSuccess || occ < 1)
+      continue;
+    if (occ > 2) occ = 2;
+    long long cap = (long long)sms * occ * th * Es[q];
+    // Small systems: fewer blocks keep the barrier cheap.
+    if (n <= cap || q == 4) {
+      if (n > cap) { n2c_set_error("GMRES order %lld exceeds the device-resident limit %lld", n, cap); return 0; }
+      long long need = (n + (long long)th * Es[q] - 1) / ((long long)th * Es[q]);
+      int bl = (int)(need < (long long)sms * occ ? need : (long long)sms * occ);
+      if (bl < 1) bl = 1;
+      *blocks = bl; *threads = th; *fn = fns[q];
+      return 1;
+    }
+  }
+  n2c_set_error("no cooperative configuration for the Arnoldi kernel");
+  return 0;
+}
+
+static unsigned grid1(long long n) {
+  long long b = (n + 255) / 256;
+  long long cap = (long long)n2c_sm_count() * 8;
+  return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, size_t restart, size_t maxit,
+                      double rtol, double atol, n2d_gmres_report *rep) {
+  const long long n = o.n;
+  long long m = (long long)restart;
+  if (m > n) m = n;
+  if (m > (long long)maxit) m = (long long)maxit;
+  GmBuffers b;
+  memset(&b, 0, sizeof(b));
+  int blocks = 0, threads = 0;
+  ArnoldiLauncher arnoldi = nullptr;
+  if (!arnoldi_shape(n, &blocks, &threads, &arnoldi)) { rep->status = ST_ALLOC; return 0; }
+  b.st = (GmState *)n2d_alloc(sizeof(GmState));
+  b.H = (double2 *)n2d_alloc((m + 1) * m * sizeof(double2));
+  b.g = (double2 *)n2d_alloc((m + 1) * sizeof(double2));
+  b.sn = (double2 *)n2d_alloc(m * sizeof(double2));
+  b.y = (double2 *)n2d_alloc(m * sizeof(double2));
+  b.cs = (double *)n2d_alloc(m * sizeof(double));
+  b.V = (double2 *)n2d_alloc((m + 1) * n * sizeof(double2));
+  b.w = (double2 *)n2d_alloc(n * sizeof(double2));
+  b.r = (double2 *)n2d_alloc(n * sizeof(double2));
+  b.partials = (double *)n2d_alloc(4 * 4096 * sizeof(double));
+  b.ticket = (unsigned int *)n2d_alloc(64);
+  int ok = 0;
+  GmState hs;
+  double bnorm = 0, target = 0;
+  auto free_all = [&]() {
+    void *bufs[] = {b.st, b.H, b.g, b.sn, b.y, b.cs, b.V, b.w, b.r, b.partials, b.ticket};
+    for (void *q : bufs) n2d_free(q);
+  };
+  if (!b.st || !b.H || !b.g || !b.sn || !b.y || !b.cs || !b.V || !b.w || !b.r || !b.partials || !b.ticket) {
+    rep->status = ST_ALLOC;
+    free_all();
+    return 0;
+  }
+  memset(&hs, 0, sizeof(hs));
+  hs.status = ST_RUNNING;
+  hs.max_iterations = (long long)maxit;
+  double *dnorm = (double *)b.partials + 3 * 4096;  // two scalars past the partial slots
+  int *dflag = (int *)((double *)b.partials + 3 * 4096 + 8);
+  auto read_state = [&]() { return n2d_download(&hs, b.st, sizeof(hs)); };
+  // ||b|| and ||x|| (finite check) before anything else (vie_iterative.c:116-119).
+  double norms[2];
+  if (!n2d_memset(dflag, 0, sizeof(int)) || !n2d_memset(b.ticket, 0, 64) ||
+      !n2c_norm2((const double *)b_dev, n, b.partials, b.ticket, dnorm, dflag) ||
+      !n2c_norm2((const double *)x_dev, n, b.partials, b.ticket, dnorm + 1, dflag) ||
+      !n2d_download(norms, dnorm, sizeof(norms))) { rep->status = ST_ALLOC; free_all(); return 0; }
+  int hflag = 0;
+  if (!n2d_download(&hflag, dflag, sizeof(int))) { free_all(); return 0; }
+  bnorm = sqrt(norms[0]);
+  target = fmax(atol, rtol * bnorm);
+  if (hflag || !isfinite(bnorm) || !isfinite(sqrt(norms[1])) || !isfinite(target)) {
+    rep->status = ST_NONFINITE; free_all(); return 0;
+  }
+  hs.target = target;
+  if (!n2d_upload(b.st, &hs, sizeof(hs))) { free_all(); return 0; }
+  // True residual r = b - A x.
+  auto true_residual = [&]() -> int {
+    ++rep->operator_applications;
+    if (!n2d_memset(dflag, 0, sizeof(int))) return 0;
+    if (!op_apply(o, (const double *)x_dev, (double *)b.r, 0, nullptr, dflag)) { rep->status = ST_CALLBACK; return 0; }
+    residual_kernel<<<grid1(n), 256, 0, n2c_stream()>>>(b_dev, b.r, n);
+    if (!n2c_check_launch("residual")) return 0;
+    double sq = 0;
+    if (!n2c_norm2((const double *)b.r, n, b.partials, b.ticket, dnorm, dflag) ||
+        !n2d_download(&sq, dnorm, sizeof(double)) || !n2d_download(&hflag, dflag, sizeof(int)))
+      return 0;
+    rep->residual_norm = hflag ? NAN : sqrt(sq);
+    if (!isfinite(rep->residual_norm)) { rep->status = ST_NONFINITE; return 0; }
+    return 1;
+  };
+  if (!true_residual()) { free_all(); return 0; }
+  for (;;) {
+    const double beta = rep->residual_norm;
+    rep->relative_residual = bnorm > 0 ? beta / bnorm : beta;
+    if (beta <= target) { rep->status = ST_CONVERGED; ok = 1; break; }
+    if ((long long)rep->iterations >= (long long)maxit) { rep->status = ST_LIMIT; break; }
+    if (o.kind == 1 && !n2c_hybrid_precondition_ok((const n2d_hybrid *)o.op)) { rep->status = ST_CALLBACK; break; }
+    cycle_start_kernel<<<grid1(n), 256, 0, n2c_stream()>>>(b, n, (int)m, beta);
+    if (!n2c_check_launch("cycle_start")) break;
+    // The state block carries the running iteration count across cycles.
+    hs.iterations = (long long)rep->iterations;
+    hs.active = 1; hs.used = 0; hs.breakdown = 0; hs.flag = 0; hs.barrier_error = 0;
+    hs.bar_count = 0; hs.bar_gen = 0;
+    if (!n2d_upload(b.st, &hs, sizeof(hs))) break;
+    bool launch_fail = false;
+    // Matvec kernels launched under the gate return at once when the cycle
+    // has ended; a one-int readback every 8 iterations stops issuing them.
+    n2d_set_gate(&b.st->active);
+    for (int j = 0; j < m; ++j) {
+      if (j > 0 && (j % 8) == 0) {
+        int act = 0;
+        if (!n2d_download(&act, &b.st->active, sizeof(int))) { launch_fail = true; break; }
+        if (!act) break;
+      }
+      if (!op_apply(o, (const double *)(b.V + (long long)j * n), (double *)b.w, o.pdiag != nullptr,
+                    &b.st->before_sq, &b.st->flag)) { launch_fail = true; break; }
+      if (!arnoldi(b, n, (int)m, j, blocks, threads)) { launch_fail = true; break; }
+    }
+    n2d_set_gate(nullptr);
+    if (launch_fail) { rep->status = ST_CALLBACK; break; }
+    backsolve_kernel<<<1, 1, 0, n2c_stream()>>>(b, (int)m);
+    if (!n2c_check_launch("backsolve")) break;
+    update_kernel<<<grid1(n), 256, 0, n2c_stream()>>>(b, o.pdiag, x_dev, n);
+    if (!n2c_check_launch("update")) break;
+    if (!read_state()) break;
+    rep->iterations = (size_t)hs.iterations;
+    rep->operator_applications += (size_t)hs.used;
+    if (hs.barrier_error) { n2c_set_error("grid barrier time-out in GMRES"); rep->status = ST_CALLBACK; break; }
+    if (hs.status != ST_RUNNING) { rep->status = hs.status; break; }
+    if (!true_residual()) break;
+    rep->relative_residual = bnorm > 0 ? rep->residual_norm / bnorm : rep->residual_norm;
+    if (hs.breakdown && rep->residual_norm > target) { rep->status = ST_BREAKDOWN; break; }
+    if (rep->residual_norm > target && (long long)rep->iterations < (long long)maxit) ++rep->restarts;
+  }
+  free_all();
+  return ok;
+}
+
+static int gmres_setup(int kind, void *op, long long n, OpView *o) {
+  o->kind = kind; o->op = op; o->n = n;
+  o->pdiag = kind == 0 ? (const double2 *)n2d_vie_diag((n2d_vie *)op)
+                       : n2c_hybrid_pdiag((const n2d_hybrid *)op);
+  return 1;
+}
+
+extern "C" int n2d_gmres_dev(int kind, void *op, long long n, const double *b_dev, double *x_dev,
+                             size_t restart, size_t maxit, double rtol, double atol,
+                             n2d_gmres_report *rep) {
+  OpView o;
+  memset(rep, 0, sizeof(*rep));
+  rep->status = ST_INVALID;
+  rep->residual_norm = rep->relative_residual = INFINITY;
+  gmres_setup(kind, op, n, &o);
+  return gmres_core(o, (const double2 *)b_dev, (double2 *)x_dev, restart, maxit, rtol, atol, rep);
+}
+
+extern "C" int n2d_gmres(int kind, void *op, long long n, const double *b, double *x, size_t restart,
+                         size_t maxit, double rtol, double atol, n2d_gmres_report *rep) {
+  memset(rep, 0, sizeof(*rep));
+  rep->status = ST_ALLOC;
+  rep->residual_norm = rep->relative_residual = INFINITY;
+  double *bd = (double *)n2d_alloc(n * sizeof(double2)), *xd = (double *)n2d_alloc(n * sizeof(double2));
+  int ok = 0;
+  if (bd && xd && n2d_upload(bd, b, n * sizeof(double2)) && n2d_upload(xd, x, n * sizeof(double2))) {
+    ok = n2d_gmres_dev(kind, op, n, bd, xd, restart, maxit, rtol, atol, rep);
+    // x is updated even on failure (vie_iterative.h:51-53).
+    if (!n2d_download(x, xd, n * sizeof(double2))) ok = 0;
+  }
+  n2d_free(bd);
+  n2d_free(xd);
+  return ok;
+}

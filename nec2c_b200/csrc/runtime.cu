@@ -1,0 +1,111 @@
+// Runtime plumbing of the nec2c CUDA backend: per-thread error text, the
+// stream work is enqueued on, device buffers and a launch counter.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+#include <atomic>
+#include "common.cuh"
+#include "device_api.h"
+#include "runtime.cuh"
+
+static thread_local char g_error[512];
+static thread_local cudaStream_t g_stream = nullptr;
+static thread_local const int *g_gate = nullptr;
+static std::atomic<unsigned long long> g_launches{0};
+
+extern "C" void n2c_set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_error, sizeof(g_error), fmt, ap);
+  va_end(ap);
+}
+extern "C" const char *n2d_last_error(void) { return g_error; }
+extern "C" void n2d_set_stream(void *s) { g_stream = (cudaStream_t)s; }
+extern "C" void *n2d_get_stream(void) { return (void *)g_stream; }
+cudaStream_t n2c_stream() { return g_stream; }
+extern "C" void n2d_set_gate(const int *gate_dev) { g_gate = gate_dev; }
+const int *n2c_gate() { return g_gate; }
+void n2c_count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+extern "C" unsigned long long n2d_launch_count(void) { return g_launches.load(); }
+
+int n2c_check_launch(const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    n2c_set_error("%s launch failed: %s", what, cudaGetErrorString(e));
+    return 0;
+  }
+  n2c_count_launch(1);
+  return 1;
+}
+
+extern "C" int n2d_sync(void) {
+  cudaError_t e = cudaStreamSynchronize(g_stream);
+  if (e != cudaSuccess) { n2c_set_error("stream synchronize: %s", cudaGetErrorString(e)); return 0; }
+  return 1;
+}
+extern "C" void *n2d_alloc(size_t bytes) {
+  void *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) { n2c_set_error("cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e)); return nullptr; }
+  return p;
+}
+extern "C" void n2d_free(void *p) { if (p) cudaFree(p); }
+extern "C" int n2d_upload(void *dst, const void *src, size_t bytes) {
+  if (!bytes) return 1;
+  N2C_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, g_stream));
+  return 1;
+}
+extern "C" int n2d_download(void *dst, const void *src, size_t bytes) {
+  if (!bytes) return 1;
+  N2C_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, g_stream));
+  N2C_CHECK(cudaStreamSynchronize(g_stream));
+  return 1;
+}
+extern "C" int n2d_memset(void *dst, int v, size_t bytes) {
+  if (!bytes) return 1;
+  N2C_CHECK(cudaMemsetAsync(dst, v, bytes, g_stream));
+  return 1;
+}
+extern "C" int n2d_copy_d2d(void *dst, const void *src, size_t bytes) {
+  if (!bytes) return 1;
+  N2C_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, g_stream));
+  return 1;
+}
+
+extern "C" int n2d_upload2d(void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
+                            size_t rows) {
+  if (!width || !rows) return 1;
+  N2C_CHECK(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, cudaMemcpyHostToDevice, g_stream));
+  return 1;
+}
+extern "C" int n2d_download2d(void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
+                              size_t rows) {
+  if (!width || !rows) return 1;
+  N2C_CHECK(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, cudaMemcpyDeviceToHost, g_stream));
+  N2C_CHECK(cudaStreamSynchronize(g_stream));
+  return 1;
+}
+extern "C" int n2d_device_ok(void) {
+  int count = 0, dev = 0, major = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1) {
+    cudaGetLastError();
+    n2c_set_error("no CUDA device available");
+    return 0;
+  }
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (major != 10) { n2c_set_error("device compute capability %d.x is not sm_100", major); return 0; }
+  return 1;
+}
+
+int n2c_sm_count() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}

@@ -1,0 +1,579 @@
+// Volume FFT operator of the nec2c dielectric path on sm_100a.
+//
+// Replaces the builtin/FFTW plan of vie_fft.c: the Green spectrum build
+// (vie_fft.c:338-377, far pairs quadratured on the GPU), the matvec
+// y = eps x - (eps-1) gather(IFFT(Ghat FFT(scatter x)))   (vie_fft.c:239-263)
+// and the Jacobi preconditioner (vie_fft.c:265-273).
+//
+// HBM layout (one plan):
+//   box  [3][nx][ny][nz]      planar source / field on the lattice box
+//   T1   [3][nx][ny][Pz]      after the z transform (x<nx, y<ny only)
+//   T2   [3][nx][Py][Pz]      after the y transform (x<nx only)
+//   spec [6][Px][Py][Pz]      Ghat / G (xx yy zz xy xz yz), 1/G folded in
+// The zero half of the padded source is never stored and the discarded half of
+// the inverse transform is never computed past the pass that drops it.
+#include <math.h>
+#include <string.h>
+#include <vector>
+#include "common.cuh"
+#include "device_api.h"
+#include "fft_engine.cuh"
+#include "runtime.cuh"
+#include "vie_internal.cuh"
+
+using namespace n2c;
+
+// ------------------------------------------------------------ pass dispatch
+template <typename C, int R1, int R2>
+static int launch_pass_rr(int mode, const PassArgs<C> &a, size_t smem, long long tiles) {
+  static bool configured[3] = {false, false, false};
+  void (*k)(PassArgs<C>) = mode == 0 ? fft_forward_pass<C, R1, R2>
+                          : mode == 1 ? fft_inverse_pass<C, R1, R2>
+                                      : fft_product_pass<C, R1, R2>;
+  if (!configured[mode]) {
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess) {
+      n2c_set_error("cannot raise shared memory for FFT pass");
+      return 0;
+    }
+    configured[mode] = true;
+  }
+  k<<<(unsigned)tiles, 256, smem, n2c_stream()>>>(a);
+  return n2c_check_launch("fft pass");
+}
+
+template <typename C>
+static int launch_pass(int mode, int L, const PassArgs<C> &a, size_t smem, long long tiles) {
+  switch (L) {
+    case 1: return launch_pass_rr<C, 1, 1>(mode, a, smem, tiles);
+    case 2: return launch_pass_rr<C, 2, 1>(mode, a, smem, tiles);
+    case 4: return launch_pass_rr<C, 4, 1>(mode, a, smem, tiles);
+    case 8: return launch_pass_rr<C, 8, 1>(mode, a, smem, tiles);
+    case 16: return launch_pass_rr<C, 16, 1>(mode, a, smem, tiles);
+    case 32: return launch_pass_rr<C, 8, 4>(mode, a, smem, tiles);
+    case 64: return launch_pass_rr<C, 8, 8>(mode, a, smem, tiles);
+    case 128: return launch_pass_rr<C, 16, 8>(mode, a, smem, tiles);
+    case 256: return launch_pass_rr<C, 16, 16>(mode, a, smem, tiles);
+    case 512: return launch_pass_rr<C, 32, 16>(mode, a, smem, tiles);
+    case 1024: return launch_pass_rr<C, 32, 32>(mode, a, smem, tiles);
+  }
+  n2c_set_error("unsupported FFT length %d", L);
+  return 0;
+}
+
+// Lines per tile: as many as fit a ~96 KB tile (two CTAs per SM), <= 32.
+static int lines_per_tile(int L, int ncomp, size_t elem) {
+  size_t per_line = (size_t)L * ncomp * elem;
+  int nl = 32;
+  while (nl > 1 && (size_t)nl * per_line > 96 * 1024) nl >>= 1;
+  return nl;
+}
+
+// One axis transform over a batch of lines.  Element e of line (b, i) lives at
+// (b*A + e)*I + i; lines = B*I.
+template <typename C>
+static int axis_pass(int mode, int L, const C *in, C *out, const C *tw, long long B, long long I,
+                     long long A_in, long long A_out, int n_in, int n_out) {
+  PassArgs<C> a;
+  memset(&a, 0, sizeof(a));
+  a.in = in; a.out = out; a.tw = tw;
+  a.lines = B * I; a.I = I; a.A_in = A_in; a.A_out = A_out; a.n_in = n_in; a.n_out = n_out;
+  a.NL = lines_per_tile(L, 1, sizeof(C));
+  a.gate = n2c_gate();
+  const long long tiles = (a.lines + a.NL - 1) / a.NL;
+  return launch_pass<C>(mode, L, a, (size_t)L * a.NL * sizeof(C), tiles);
+}
+
+template <typename C>
+static int product_pass(int L, const C *in, C *out, const C *tw, const C *spec, long long I,
+                        int nx) {
+  PassArgs<C> a;
+  memset(&a, 0, sizeof(a));
+  a.in = in; a.out = out; a.tw = tw; a.spec = spec;
+  a.lines = I; a.I = I; a.A_in = nx; a.A_out = nx; a.n_in = nx; a.n_out = nx;
+  a.comp_in = (long long)nx * I; a.comp_out = (long long)nx * I; a.spec_comp = (long long)L * I;
+  a.NL = lines_per_tile(L, 3, sizeof(C));
+  a.gate = n2c_gate();
+  const long long tiles = (a.lines + a.NL - 1) / a.NL;
+  return launch_pass<C>(2, L, a, (size_t)3 * L * a.NL * sizeof(C), tiles);
+}
+
+// --------------------------------------------------------- scatter / gather
+// box[c][b] = z(cell(b))_c, z = x or x ./ diag.  Non-finite z raises *flag.
+// With PEC images (mirror > 0) cell m+c is the image of cell c and carries
+// diag(-1,-1,+1) times its source (dielectric_fft.c:44-50).
+template <typename C>
+__global__ void scatter_kernel(const double2 *__restrict__ x, const double2 *__restrict__ diag,
+                               const int *__restrict__ box_cell, C *__restrict__ box,
+                               long long nbox, long long mirror, int *flag, const int *gate) {
+  if (gated_off(gate)) return;
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nbox;
+       b += (long long)gridDim.x * blockDim.x) {
+    long long cell = box_cell[b];
+    double sgn[3] = {1, 1, 1};
+    if (mirror && cell >= mirror) { cell -= mirror; sgn[0] = -1; sgn[1] = -1; }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double2 v = make_double2(0, 0);
+      if (cell >= 0) {
+        v = x[3LL * cell + c];
+        if (diag) v = cdiv(v, diag[3LL * cell + c]);
+        if (flag && !finite2(v)) *flag = 1;
+        v.x *= sgn[c]; v.y *= sgn[c];
+      }
+      box[c * nbox + b] = from_d<C>(v);
+    }
+  }
+}
+
+// y = eps z - (eps-1) field, per cell; optional sum |y|^2 (deterministic).
+template <typename C>
+__global__ void gather_kernel(const double2 *__restrict__ x, const double2 *__restrict__ diag,
+                              const double2 *__restrict__ eps, const int *__restrict__ cell_box,
+                              const C *__restrict__ box, long long nbox, long long cells,
+                              double2 *__restrict__ y, double *partials, unsigned int *ticket,
+                              double *norm_out, int *flag, const int *gate) {
+  if (gated_off(gate)) return;
+  double acc = 0;
+  bool bad = false;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < cells;
+       c += (long long)gridDim.x * blockDim.x) {
+    const double2 e = eps[c], em1 = make_double2(e.x - 1.0, e.y);
+    const long long b = cell_box[c];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      double2 z = x[3 * c + i];
+      if (diag) z = cdiv(z, diag[3 * c + i]);
+      const double2 f = to_d(box[i * nbox + b]);
+      const double2 v = csub(cmul(e, z), cmul(em1, f));
+      y[3 * c + i] = v;
+      acc += v.x * v.x + v.y * v.y;
+      bad |= !finite2(v);
+    }
+  }
+  if (!norm_out) return;
+  if (bad && flag) *flag = 1;
+  double2 s = block_sum(make_double2(acc, 0));
+  if (threadIdx.x == 0) partials[blockIdx.x] = s.x;
+  if (last_block_done(ticket)) {
+    double t = 0;
+    for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) t += partials[i];
+    double2 tot = block_sum(make_double2(t, 0));
+    if (threadIdx.x == 0) { *norm_out = tot.x; *ticket = 0; }
+  }
+}
+
+__global__ void precondition_kernel(const double2 *__restrict__ x, const double2 *__restrict__ diag,
+                                    double2 *__restrict__ y, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] = cdiv(x[i], diag[i]);
+}
+
+__global__ void eps_kernel(const double2 *__restrict__ eps, double2 s0, double2 s1, double2 s2,
+                           double2 *__restrict__ diag, long long cells) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < cells;
+       c += (long long)gridDim.x * blockDim.x) {
+    const double2 e = eps[c], em1 = make_double2(e.x - 1.0, e.y);
+    diag[3 * c + 0] = csub(e, cmul(em1, s0));
+    diag[3 * c + 1] = csub(e, cmul(em1, s1));
+    diag[3 * c + 2] = csub(e, cmul(em1, s2));
+  }
+}
+
+// ------------------------------------------------------ far-pair quadrature
+// Gauss-Legendre nodes/weights on [0,1] for orders 4, 6, 8, 12 (host-computed).
+__constant__ double c_gauss_node[4][12];
+__constant__ double c_gauss_weight[4][12];
+
+// One order of the difference-coordinate rule (vie_fft.c:299-318) for offset v;
+// returns the six independent entries (xx yy zz xy xz yz), block-reduced.
+__device__ void far_rule_block(const int v[3], double h, double k, int s, int order,
+                               double2 out[6]) {
+  double2 acc[6];
+#pragma unroll
+  for (int e = 0; e < 6; ++e) acc[e] = make_double2(0, 0);
+  const int total = order * order * order * 8;
+  const double inv4pi = 1.0 / (4.0 * 3.141592653589793238462643383279502884);
+  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const int mask = idx & 7, q = idx >> 3;
+    const int ia = q / (order * order), ib = (q / order) % order, ic = q % order;
+    const double t[3] = {c_gauss_node[s][ia], c_gauss_node[s][ib], c_gauss_node[s][ic]};
+    const double wt = h * h * h * c_gauss_weight[s][ia] * c_gauss_weight[s][ib] *
+                      c_gauss_weight[s][ic] * (1 - t[0]) * (1 - t[1]) * (1 - t[2]);
+    double r[3], r2 = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      r[i] = h * ((double)v[i] + ((mask & (1 << i)) ? -t[i] : t[i]));
+      r2 += r[i] * r[i];
+    }
+    const double rr = sqrt(r2);
+    double sn, cs;
+    sincos(k * rr, &sn, &cs);
+    const double gm = wt * inv4pi / rr;
+    const double2 g = make_double2(gm * cs, -gm * sn);   // wt e^{-ikr} / (4 pi r)
+    const double2 dterm = make_double2(k * k - 1.0 / r2, -k / rr);
+    const double2 rterm = make_double2((-k * k + 3.0 / r2) / r2, (3.0 * k / rr) / r2);
+    const double2 diag = cmul(g, dterm), radial = cmul(g, rterm);
+    acc[0] = cadd(acc[0], cadd(diag, cscale(radial, r[0] * r[0])));
+    acc[1] = cadd(acc[1], cadd(diag, cscale(radial, r[1] * r[1])));
+    acc[2] = cadd(acc[2], cadd(diag, cscale(radial, r[2] * r[2])));
+    acc[3] = cadd(acc[3], cscale(radial, r[0] * r[1]));
+    acc[4] = cadd(acc[4], cscale(radial, r[0] * r[2]));
+    acc[5] = cadd(acc[5], cscale(radial, r[1] * r[2]));
+  }
+#pragma unroll
+  for (int e = 0; e < 6; ++e) out[e] = block_sum(acc[e]);
+}
+
+static __device__ double cabs_d(double2 a) { return hypot(a.x, a.y); }
+
+// Order ladder 4,6,8,12 with 2e-12 abs + 2e-9 rel acceptance, gap^2 > 4 only
+// (vie_fft.c:319-335).  One block per offset.
+__global__ void __launch_bounds__(256) far_kernel(const int *__restrict__ offsets, long long count,
+                                                  double h, double k, double2 *__restrict__ table,
+                                                  int *__restrict__ ok) {
+  const long long o = blockIdx.x;
+  if (o >= count) return;
+  const int v[3] = {offsets[3 * o], offsets[3 * o + 1], offsets[3 * o + 2]};
+  double gap2 = 0;
+  for (int i = 0; i < 3; ++i) { double g = v[i] > 1 ? (double)v[i] - 1 : 0; gap2 += g * g; }
+  if (gap2 <= 4) { if (threadIdx.x == 0) ok[o] = 0; return; }
+  const int ladder[4] = {4, 6, 8, 12};
+  double2 prev[6], cur[6];
+  far_rule_block(v, h, k, 0, ladder[0], prev);
+  for (int s = 1; s < 4; ++s) {
+    far_rule_block(v, h, k, s, ladder[s], cur);
+    bool conv = true;
+    for (int e = 0; e < 6; ++e) {
+      const double2 d = csub(cur[e], prev[e]);
+      if (!finite2(cur[e]) || cabs_d(d) > 2e-12 + 2e-9 * cabs_d(cur[e])) conv = false;
+    }
+    if (conv) {
+      if (threadIdx.x == 0) {
+        // Off-diagonal entries vanish where an offset component is zero
+        // (vie_fft.c:356-359); symmetric averaging leaves far entries as is.
+        cur[3] = (v[0] && v[1]) ? cur[3] : make_double2(0, 0);
+        cur[4] = (v[0] && v[2]) ? cur[4] : make_double2(0, 0);
+        cur[5] = (v[1] && v[2]) ? cur[5] : make_double2(0, 0);
+        for (int e = 0; e < 6; ++e) table[6 * o + e] = cur[e];
+        ok[o] = 1;
+      }
+      return;
+    }
+    for (int e = 0; e < 6; ++e) prev[e] = cur[e];
+  }
+  if (threadIdx.x == 0) ok[o] = 0;
+}
+
+// ------------------------------------------------------------ spectrum fill
+struct FillArgs {
+  long long P[3], S[3];         // padded grid, lattice shape
+  long long Ss[3];              // shape sorted descending
+  const long long *slab_start;  // per a: first table index of slab a
+  const long long *row_start;   // per b: first index of row b within a slab
+  const double2 *table;         // 6 entries per sorted offset
+  double2 *spec;                // 6 x G
+  long long G;
+};
+
+__device__ __forceinline__ int sym_slot(int i, int j) {
+  const int lo = i < j ? i : j, hi = i < j ? j : i;
+  if (lo == hi) return lo;
+  if (lo == 0) return hi == 1 ? 3 : 4;
+  return 5;
+}
+
+// Each padded-grid site takes the value the reference's permutation x sign
+// loop (vie_fft.c:360-373) writes last: the last matching permutation and,
+// for zero components, the negative-sign mask.
+__global__ void fill_kernel(FillArgs f) {
+  const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < f.G;
+       g += (long long)gridDim.x * blockDim.x) {
+    long long pos[3];
+    pos[2] = g % f.P[2];
+    pos[1] = (g / f.P[2]) % f.P[1];
+    pos[0] = g / (f.P[2] * f.P[1]);
+    long long d[3];
+    int sg[3];
+    bool inside = true;
+    for (int i = 0; i < 3; ++i) {
+      if (pos[i] < f.S[i]) { d[i] = pos[i]; sg[i] = pos[i] == 0 ? -1 : 1; }
+      else if (pos[i] > f.P[i] - f.S[i]) { d[i] = f.P[i] - pos[i]; sg[i] = -1; }
+      else inside = false;
+    }
+    double2 val[6];
+    for (int e = 0; e < 6; ++e) val[e] = make_double2(0, 0);
+    if (inside) {
+      long long v[3] = {d[0], d[1], d[2]};
+      // sort descending
+      if (v[0] < v[1]) { long long t = v[0]; v[0] = v[1]; v[1] = t; }
+      if (v[1] < v[2]) { long long t = v[1]; v[1] = v[2]; v[2] = t; }
+      if (v[0] < v[1]) { long long t = v[0]; v[0] = v[1]; v[1] = t; }
+      int q = 0;
+      for (int p = 5; p >= 0; --p)
+        if (v[perms[p][0]] == d[0] && v[perms[p][1]] == d[1] && v[perms[p][2]] == d[2]) { q = p; break; }
+      const long long idx = f.slab_start[v[0]] + f.row_start[v[1]] + v[2];
+      const double2 *n = f.table + 6 * idx;
+      for (int i = 0; i < 3; ++i)
+        for (int j = i; j < 3; ++j) {
+          const double2 src = n[sym_slot(perms[q][i], perms[q][j])];
+          const double s = (double)(sg[i] * sg[j]);
+          val[sym_slot(i, j)] = make_double2(s * src.x, s * src.y);
+        }
+    }
+    for (int e = 0; e < 6; ++e) f.spec[e * f.G + g] = val[e];
+  }
+}
+
+template <typename C>
+__global__ void scale_convert_kernel(const double2 *__restrict__ in, C *__restrict__ out, long long n,
+                                     double s) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double2 v = in[i];
+    out[i] = from_d<C>(make_double2(v.x * s, v.y * s));
+  }
+}
+
+// ------------------------------------------------------------------- plan
+static unsigned grid_for(long long n, int threads = 256) {
+  long long b = (n + threads - 1) / threads;
+  long long cap = (long long)n2c_sm_count() * 8;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+static void free_plan(n2d_vie *p) {
+  if (!p) return;
+  void *bufs[] = {p->cell_box, p->box_cell, p->eps, p->diag, p->spec, p->box, p->t1, p->t2,
+                  p->tw64[0], p->tw64[1], p->tw64[2], p->tw32[0], p->tw32[1], p->tw32[2],
+                  p->table, p->table_ok, p->offsets, p->slab_start, p->row_start, p->partials,
+                  p->ticket};
+  for (void *b : bufs) n2d_free(b);
+  delete p;
+}
+
+extern "C" void n2d_vie_destroy(n2d_vie *p) { free_plan(p); }
+extern "C" size_t n2d_vie_device_bytes(const n2d_vie *p) { return p ? p->device_bytes : 0; }
+extern "C" int n2d_vie_fp32(const n2d_vie *p) { return p ? p->fp32 : 0; }
+extern "C" long long n2d_vie_cells(const n2d_vie *p) { return p ? p->cells : 0; }
+extern "C" const double *n2d_vie_diag(const n2d_vie *p) { return (const double *)p->diag; }
+
+static void *track(n2d_vie *p, size_t bytes) {
+  void *q = n2d_alloc(bytes);
+  if (q) p->device_bytes += bytes;
+  return q;
+}
+
+extern "C" int n2d_vie_create(n2d_vie **out, const long long shape[3], const long long padded[3],
+                              long long cells, const int *cell_box, const double *const twiddles[3],
+                              int fp32) {
+  *out = nullptr;
+  n2d_vie *p = new n2d_vie();
+  memset(p, 0, sizeof(*p));
+  p->fp32 = fp32;
+  p->G = 1;
+  p->nbox = 1;
+  for (int d = 0; d < 3; ++d) {
+    p->S[d] = shape[d];
+    p->P[d] = padded[d];
+    p->G *= padded[d];
+    p->nbox *= shape[d];
+    if (padded[d] > 1024 || (padded[d] & (padded[d] - 1))) {
+      n2c_set_error("padded axis %lld unsupported (power of two <= 1024 required)", padded[d]);
+      delete p;
+      return 0;
+    }
+  }
+  p->cells = cells;
+  const size_t ce = fp32 ? sizeof(float2) : sizeof(double2);
+  p->cell_box = (int *)track(p, cells * sizeof(int));
+  p->box_cell = (int *)track(p, p->nbox * sizeof(int));
+  p->eps = (double2 *)track(p, cells * sizeof(double2));
+  p->diag = (double2 *)track(p, 3 * cells * sizeof(double2));
+  p->spec = track(p, 6 * p->G * ce);
+  p->box = track(p, 3 * p->nbox * ce);
+  p->t1 = track(p, 3 * p->S[0] * p->S[1] * p->P[2] * ce);
+  p->t2 = track(p, 3 * p->S[0] * p->P[1] * p->P[2] * ce);
+  p->partials = (double *)track(p, 4096 * sizeof(double));
+  p->ticket = (unsigned int *)track(p, 64);
+  for (int d = 0; d < 3; ++d) {
+    p->tw64[d] = (double2 *)track(p, padded[d] * sizeof(double2));
+    p->tw32[d] = (float2 *)track(p, padded[d] * sizeof(float2));
+  }
+  if (!p->cell_box || !p->box_cell || !p->eps || !p->diag || !p->spec || !p->box || !p->t1 ||
+      !p->t2 || !p->partials || !p->ticket || !p->tw64[0] || !p->tw64[1] || !p->tw64[2] ||
+      !p->tw32[0] || !p->tw32[1] || !p->tw32[2]) {
+    free_plan(p);
+    return 0;
+  }
+  std::vector<int> inv(p->nbox, -1);
+  for (long long c = 0; c < cells; ++c) inv[cell_box[c]] = (int)c;
+  for (int d = 0; d < 3; ++d) {
+    std::vector<float2> t32(padded[d]);
+    for (long long j = 0; j < padded[d]; ++j)
+      t32[j] = make_float2((float)twiddles[d][2 * j], (float)twiddles[d][2 * j + 1]);
+    if (!n2d_upload(p->tw64[d], twiddles[d], padded[d] * sizeof(double2)) ||
+        !n2d_upload(p->tw32[d], t32.data(), padded[d] * sizeof(float2))) { free_plan(p); return 0; }
+    if (!n2d_sync()) { free_plan(p); return 0; }
+  }
+  if (!n2d_upload(p->cell_box, cell_box, cells * sizeof(int)) ||
+      !n2d_upload(p->box_cell, inv.data(), p->nbox * sizeof(int)) ||
+      !n2d_memset(p->ticket, 0, 64) || !n2d_sync()) {
+    free_plan(p);
+    return 0;
+  }
+  *out = p;
+  return 1;
+}
+
+extern "C" int n2d_vie_set_gauss(const double *nodes, const double *weights) {
+  N2C_CHECK(cudaMemcpyToSymbol(c_gauss_node, nodes, sizeof(double) * 48));
+  N2C_CHECK(cudaMemcpyToSymbol(c_gauss_weight, weights, sizeof(double) * 48));
+  return 1;
+}
+
+extern "C" int n2d_vie_far_tensors(n2d_vie *p, long long count, const int *offsets,
+                                   const long long sorted_shape[3], double pitch, double k0,
+                                   int *far_ok) {
+  // Index tables: slab a starts at slab_start[a]; within a slab, row b starts
+  // at row_start[b] = sum_{b'<b} (min(b', S2-1) + 1).
+  const long long S0 = sorted_shape[0], S1 = sorted_shape[1], S2 = sorted_shape[2];
+  std::vector<long long> row(S1 + 1), slab(S0 + 1);
+  row[0] = 0;
+  for (long long b = 0; b < S1; ++b) row[b + 1] = row[b] + (b < S2 - 1 ? b : S2 - 1) + 1;
+  slab[0] = 0;
+  for (long long a = 0; a < S0; ++a) slab[a + 1] = slab[a] + row[(a < S1 - 1 ? a : S1 - 1) + 1];
+  if (slab[S0] != count) {
+    n2c_set_error("offset enumeration mismatch (%lld vs %lld)", slab[S0], count);
+    return 0;
+  }
+  p->count = count;
+  p->table = (double2 *)track(p, 6 * count * sizeof(double2));
+  p->table_ok = (int *)track(p, count * sizeof(int));
+  p->offsets = (int *)track(p, 3 * count * sizeof(int));
+  p->slab_start = (long long *)track(p, (S0 + 1) * sizeof(long long));
+  p->row_start = (long long *)track(p, (S1 + 1) * sizeof(long long));
+  if (!p->table || !p->table_ok || !p->offsets || !p->slab_start || !p->row_start) return 0;
+  if (!n2d_upload(p->offsets, offsets, 3 * count * sizeof(int)) ||
+      !n2d_upload(p->slab_start, slab.data(), (S0 + 1) * sizeof(long long)) ||
+      !n2d_upload(p->row_start, row.data(), (S1 + 1) * sizeof(long long)))
+    return 0;
+  for (int d = 0; d < 3; ++d) p->Ss[d] = sorted_shape[d];
+  for (long long first = 0; first < count; first += 65535) {
+    const long long n = count - first < 65535 ? count - first : 65535;
+    far_kernel<<<(unsigned)n, 256, 0, n2c_stream()>>>(p->offsets + 3 * first, n, pitch, k0,
+                                                        p->table + 6 * first, p->table_ok + first);
+    if (!n2c_check_launch("far_kernel")) return 0;
+  }
+  return n2d_download(far_ok, p->table_ok, count * sizeof(int));
+}
+
+extern "C" int n2d_vie_put_tensors(n2d_vie *p, long long count, const long long *index,
+                                   const double *tensors) {
+  for (long long i = 0; i < count; ++i)
+    if (!n2d_upload(p->table + 6 * index[i], tensors + 12 * i, 6 * sizeof(double2))) return 0;
+  return n2d_sync();
+}
+
+template <typename C>
+static int transform_spectrum(n2d_vie *p, C *spec, const C *const tw[3]) {
+  const long long Px = p->P[0], Py = p->P[1], Pz = p->P[2];
+  return axis_pass<C>(0, (int)Pz, spec, spec, tw[2], 6 * Px * Py, 1, Pz, Pz, (int)Pz, (int)Pz) &&
+         axis_pass<C>(0, (int)Py, spec, spec, tw[1], 6 * Px, Pz, Py, Py, (int)Py, (int)Py) &&
+         axis_pass<C>(0, (int)Px, spec, spec, tw[0], 6, Py * Pz, Px, Px, (int)Px, (int)Px);
+}
+
+extern "C" int n2d_vie_finish_spectrum(n2d_vie *p) {
+  FillArgs f;
+  for (int d = 0; d < 3; ++d) { f.P[d] = p->P[d]; f.S[d] = p->S[d]; f.Ss[d] = p->Ss[d]; }
+  f.slab_start = p->slab_start; f.row_start = p->row_start; f.table = p->table; f.G = p->G;
+  // The FP64 spectrum is built in place when the plan is FP64, otherwise in a
+  // temporary FP64 grid that is then rounded into the plan's FP32 storage.
+  double2 *work = p->fp32 ? (double2 *)n2d_alloc(6 * p->G * sizeof(double2)) : (double2 *)p->spec;
+  if (!work) return 0;
+  f.spec = work;
+  fill_kernel<<<grid_for(p->G), 256, 0, n2c_stream()>>>(f);
+  int ok = n2c_check_launch("fill_kernel");
+  const double2 *tw[3] = {p->tw64[0], p->tw64[1], p->tw64[2]};
+  ok = ok && transform_spectrum<double2>(p, work, tw);
+  const double scale = 1.0 / (double)p->G;
+  if (ok && p->fp32) {
+    scale_convert_kernel<float2><<<grid_for(6 * p->G), 256, 0, n2c_stream()>>>(
+        work, (float2 *)p->spec, 6 * p->G, scale);
+    ok = n2c_check_launch("scale_convert");
+  } else if (ok) {
+    scale_convert_kernel<double2><<<grid_for(6 * p->G), 256, 0, n2c_stream()>>>(
+        work, (double2 *)p->spec, 6 * p->G, scale);
+    ok = n2c_check_launch("scale_convert");
+  }
+  ok = ok && n2d_sync();
+  if (p->fp32) n2d_free(work);
+  // The offset table is only needed while building.
+  n2d_free(p->table); n2d_free(p->table_ok); n2d_free(p->offsets);
+  n2d_free(p->slab_start); n2d_free(p->row_start);
+  p->device_bytes -= 6 * p->count * sizeof(double2) + p->count * sizeof(int) * 4 +
+                     (p->Ss[0] + 1 + p->Ss[1] + 1) * sizeof(long long);
+  p->table = nullptr; p->table_ok = nullptr; p->offsets = nullptr;
+  p->slab_start = nullptr; p->row_start = nullptr;
+  return ok;
+}
+
+extern "C" int n2d_vie_read_spectrum(n2d_vie *p, double *out) {
+  if (!p->fp32) return n2d_download(out, p->spec, 6 * p->G * sizeof(double2));
+  std::vector<float2> tmp(6 * p->G);
+  if (!n2d_download(tmp.data(), p->spec, 6 * p->G * sizeof(float2))) return 0;
+  for (long long i = 0; i < 6 * p->G; ++i) { out[2 * i] = tmp[i].x; out[2 * i + 1] = tmp[i].y; }
+  return 1;
+}
+
+extern "C" int n2d_vie_set_eps(n2d_vie *p, const double *eps, const double *self) {
+  if (!n2d_upload(p->eps, eps, p->cells * sizeof(double2))) return 0;
+  for (int i = 0; i < 3; ++i) p->self[i] = make_double2(self[2 * i], self[2 * i + 1]);
+  eps_kernel<<<grid_for(p->cells), 256, 0, n2c_stream()>>>(p->eps, p->self[0], p->self[1], p->self[2],
+                                                           p->diag, p->cells);
+  return n2c_check_launch("eps_kernel") && n2d_sync();
+}
+
+template <typename C>
+static int apply_t(n2d_vie *p, const double2 *x, double2 *y, const double2 *diag, double *norm,
+                   int *flag) {
+  const long long nx = p->S[0], ny = p->S[1], nz = p->S[2];
+  const long long Px = p->P[0], Py = p->P[1], Pz = p->P[2];
+  C *box = (C *)p->box, *t1 = (C *)p->t1, *t2 = (C *)p->t2;
+  const C *tw[3];
+  for (int d = 0; d < 3; ++d) tw[d] = p->fp32 ? (const C *)p->tw32[d] : (const C *)p->tw64[d];
+  scatter_kernel<C><<<grid_for(p->nbox), 256, 0, n2c_stream()>>>(x, diag, p->box_cell, box, p->nbox,
+                                                                 p->mirror, flag, n2c_gate());
+  if (!n2c_check_launch("scatter")) return 0;
+  if (!axis_pass<C>(0, (int)Pz, box, t1, tw[2], 3 * nx * ny, 1, nz, Pz, (int)nz, (int)Pz)) return 0;
+  if (!axis_pass<C>(0, (int)Py, t1, t2, tw[1], 3 * nx, Pz, ny, Py, (int)ny, (int)Py)) return 0;
+  if (!product_pass<C>((int)Px, t2, t2, tw[0], (const C *)p->spec, Py * Pz, (int)nx)) return 0;
+  if (!axis_pass<C>(1, (int)Py, t2, t1, tw[1], 3 * nx, Pz, Py, ny, (int)Py, (int)ny)) return 0;
+  if (!axis_pass<C>(1, (int)Pz, t1, box, tw[2], 3 * nx * ny, 1, Pz, nz, (int)Pz, (int)nz)) return 0;
+  const long long out_cells = p->mirror ? p->mirror : p->cells;
+  const unsigned gblocks = norm ? (grid_for(out_cells) < 1024 ? grid_for(out_cells) : 1024)
+                                : grid_for(out_cells);
+  gather_kernel<C><<<gblocks, 256, 0, n2c_stream()>>>(x, diag, p->eps, p->cell_box, box, p->nbox,
+                                                      out_cells, y, p->partials, p->ticket, norm,
+                                                      flag, n2c_gate());
+  return n2c_check_launch("gather");
+}
+
+extern "C" int n2d_vie_apply(n2d_vie *p, const double *x, double *y, int precondition_input,
+                             double *norm, int *flag) {
+  const double2 *diag = precondition_input ? p->diag : nullptr;
+  if (p->fp32) return apply_t<float2>(p, (const double2 *)x, (double2 *)y, diag, norm, flag);
+  return apply_t<double2>(p, (const double2 *)x, (double2 *)y, diag, norm, flag);
+}
+
+extern "C" void n2d_vie_set_mirror(n2d_vie *p, long long physical_cells) { p->mirror = physical_cells; }
+
+extern "C" int n2d_vie_precondition(n2d_vie *p, const double *x, double *y) {
+  const long long n = 3 * (p->mirror ? p->mirror : p->cells);
+  precondition_kernel<<<grid_for(n), 256, 0, n2c_stream()>>>((const double2 *)x, p->diag,
+                                                              (double2 *)y, n);
+  return n2c_check_launch("precondition");
+}

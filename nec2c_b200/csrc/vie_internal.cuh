@@ -1,0 +1,27 @@
+// Device-side state of one volume FFT plan (shared by vie.cu, hybrid.cu, gmres.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+struct n2d_vie {
+  int fp32;                 // 1: FP32 grids/spectrum (FP64 vectors and epilogue)
+  long long S[3], P[3];     // lattice shape, padded FFT grid
+  long long Ss[3];          // shape sorted descending (spectrum build)
+  long long G, nbox, cells, count;
+  long long mirror;         // >0: PEC image embedding, cells = 2*mirror (images last)
+  int *cell_box;            // [cells] box index of each cell
+  int *box_cell;            // [nbox] cell index or -1
+  double2 *eps;             // [cells]
+  double2 *diag;            // [3 cells] eps - (eps-1) self[i]
+  double2 self[3];
+  void *spec;               // [6][G]
+  void *box, *t1, *t2;      // work grids
+  double2 *tw64[3];
+  float2 *tw32[3];
+  double2 *table;           // build only: 6 entries per sorted offset
+  int *table_ok, *offsets;
+  long long *slab_start, *row_start;
+  double *partials;         // reduction scratch
+  unsigned int *ticket;
+  size_t device_bytes;
+};

@@ -1,0 +1,406 @@
+/* Host side of the CUDA volume operator, hybrid system and GMRES (C, like the
+ * reference).  Validation, lattice mapping, byte accounting and the near-pair
+ * callback follow vie_fft.c / dielectric_fft.c / vie_iterative.c; the device
+ * work is done through the device layer (csrc/device_api.h). */
+#include <complex.h>
+#include <float.h>
+#include <limits.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../../include/nec2c_cuda.h"
+#include "../csrc/device_api.h"
+
+static const double kPi = 3.141592653589793238462643383279502884;
+
+enum { ST_CONVERGED, ST_LIMIT, ST_BREAKDOWN, ST_CALLBACK, ST_INVALID, ST_ALLOC, ST_NONFINITE };
+
+static int g_fft_fp32 = 0;
+
+int nec2c_cuda_available(void) { return n2d_device_ok(); }
+const char *nec2c_cuda_last_error(void) { return n2d_last_error(); }
+void nec2c_cuda_set_stream(void *s) { n2d_set_stream(s); }
+unsigned long long nec2c_cuda_launch_count(void) { return n2d_launch_count(); }
+
+int nec2c_cuda_vie_fft_backend_set(const char *name)
+{
+  if(!name) return 0;
+  if(!strcmp(name, "cuda")) g_fft_fp32 = 0;
+  else if(!strcmp(name, "cuda-mixed")) g_fft_fp32 = 1;
+  else return 0;
+  return 1;
+}
+const char *nec2c_cuda_vie_fft_backend_name(void) { return g_fft_fp32 ? "cuda-mixed" : "cuda"; }
+
+struct nec2c_cuda_vie_plan {
+  n2d_vie *dev;
+  size_t cells, shape[3], padded[3], grids, bytes;
+  double complex *eps;      /* host shadow of the per-cell permittivity */
+  double complex self[3];
+  int eps_dirty;
+  double *x_dev, *y_dev;    /* staging for host-vector products */
+};
+
+static int mul_ok(size_t a, size_t b, size_t *out) { if(b && a > SIZE_MAX / b) return 0; *out = a * b; return 1; }
+static int add_ok(size_t a, size_t b, size_t *out) { if(a > SIZE_MAX - b) return 0; *out = a + b; return 1; }
+
+/* Gauss-Legendre nodes/weights on [0,1] by Newton iteration (the rule of
+   vie_fft.c:284-298), orders 4, 6, 8, 12. */
+static void gauss_tables(double nodes[4][12], double weights[4][12])
+{
+  static const int orders[4] = {4, 6, 8, 12};
+  memset(nodes, 0, 48 * sizeof(double)); memset(weights, 0, 48 * sizeof(double));
+  for(int s = 0; s < 4; ++s) {
+    const int n = orders[s];
+    for(int i = 0; i < (n + 1) / 2; ++i) {
+      double z = cos(kPi * (i + .75) / (n + .5)), prev, slope = 0;
+      do {
+        double p0 = 1, p1 = 0;
+        prev = z;
+        for(int j = 1; j <= n; ++j) { double p2 = p1; p1 = p0; p0 = ((2*j - 1) * z * p1 - (j - 1) * p2) / j; }
+        slope = n * (z * p0 - p1) / (z * z - 1);
+        z = prev - p0 / slope;
+      } while(fabs(z - prev) > 2e-15);
+      nodes[s][i] = (1 - z) / 2; nodes[s][n - 1 - i] = (1 + z) / 2;
+      weights[s][i] = weights[s][n - 1 - i] = 1 / ((1 - z * z) * slope * slope);
+    }
+  }
+}
+
+static int diag_ok(const double complex self[3], double complex er)
+{
+  for(int i = 0; i < 3; ++i) {
+    double complex d = er - (er - 1) * self[i];
+    if(!isfinite(cabs(d)) || cabs(d) < 1e-30) return 0;
+  }
+  return 1;
+}
+
+static int upload_eps(struct nec2c_cuda_vie_plan *p)
+{
+  double self[6];
+  for(int i = 0; i < 3; ++i) { self[2*i] = creal(p->self[i]); self[2*i + 1] = cimag(p->self[i]); }
+  if(!n2d_vie_set_eps(p->dev, (const double *)p->eps, self)) return 0;
+  p->eps_dirty = 0;
+  return 1;
+}
+
+void nec2c_cuda_vie_fft_destroy(nec2c_cuda_vie_plan *p)
+{
+  if(!p) return;
+  n2d_vie_destroy(p->dev);
+  n2d_free(p->x_dev); n2d_free(p->y_dev);
+  free(p->eps);
+  free(p);
+}
+
+int nec2c_cuda_vie_fft_create(nec2c_cuda_vie_plan **out, const size_t shape[3], size_t cells,
+                              const size_t *xyz, double h, double k, double er_re, double er_im,
+                              size_t limit, nec2c_cuda_near_tensor_fn near, void *near_ctx)
+{
+  struct nec2c_cuda_vie_plan *p = NULL;
+  double complex er = er_re + I * er_im;
+  size_t padded[3], g = 1, bytes = 256, tmp, root_bytes = 0;
+  int *cell_box = NULL, *offsets = NULL, *far_ok = NULL;
+  unsigned char *seen = NULL;
+  double *tw[3] = {NULL, NULL, NULL}, *near_t = NULL;
+  long long *near_i = NULL;
+  if(!out) return 0;
+  *out = NULL;
+  /* vie_fft.c:383-384 */
+  if(!shape || !xyz || !cells || cells > SIZE_MAX / 3 || !isfinite(h) || h <= 0 || !isfinite(k) ||
+     k < 0 || !isfinite(er_re) || !isfinite(er_im) || er_re < 1 || er_im > 0 || !isfinite(k * h) ||
+     k * h > 1) { n2c_set_error("invalid plan arguments"); return 0; }
+  for(int d = 0; d < 3; ++d) {
+    if(!shape[d] || shape[d] > SIZE_MAX / 2) { n2c_set_error("invalid lattice shape"); return 0; }
+    padded[d] = 1;
+    while(padded[d] < 2 * shape[d] - 1) {
+      if(padded[d] > SIZE_MAX / 2) return 0;
+      padded[d] *= 2;
+    }
+    if(!mul_ok(g, padded[d], &g) || !mul_ok(padded[d], sizeof(double complex), &tmp) ||
+       !add_ok(root_bytes, tmp, &root_bytes)) { n2c_set_error("lattice size overflow"); return 0; }
+  }
+  /* The reference's accounted bytes (vie_fft.c:394-396). */
+  if(!mul_ok(g, 12 * sizeof(double complex), &tmp) || !add_ok(bytes, tmp, &bytes) ||
+     !mul_ok(cells, sizeof(size_t) + sizeof(double complex), &tmp) || !add_ok(bytes, tmp, &bytes) ||
+     !add_ok(bytes, root_bytes, &bytes) || bytes > limit) {
+    n2c_set_error("plan exceeds its byte limit");
+    return 0;
+  }
+  if(!n2d_device_ok()) return 0;
+  for(int d = 0; d < 3; ++d)
+    if(padded[d] > 1024) { n2c_set_error("padded axis %zu exceeds 1024", padded[d]); return 0; }
+  p = calloc(1, sizeof(*p));
+  if(!p) return 0;
+  p->cells = cells; p->grids = g; p->bytes = bytes;
+  memcpy(p->shape, shape, sizeof(p->shape)); memcpy(p->padded, padded, sizeof(p->padded));
+  p->eps = malloc(cells * sizeof(double complex));
+  cell_box = malloc(cells * sizeof(int));
+  size_t nbox = shape[0] * shape[1] * shape[2];
+  seen = calloc(nbox, 1);
+  if(!p->eps || !cell_box || !seen) goto fail;
+  /* Lattice map with duplicate rejection (vie_fft.c:416-423). */
+  for(size_t c = 0; c < cells; ++c) {
+    size_t pos[3];
+    for(int d = 0; d < 3; ++d) { pos[d] = xyz[3*c + d]; if(pos[d] >= shape[d]) { n2c_set_error("cell outside lattice"); goto fail; } }
+    size_t b = (pos[0] * shape[1] + pos[1]) * shape[2] + pos[2];
+    if(seen[b]) { n2c_set_error("duplicate lattice site"); goto fail; }
+    seen[b] = 1;
+    cell_box[c] = (int)b;
+  }
+  for(int d = 0; d < 3; ++d) {
+    tw[d] = malloc(2 * padded[d] * sizeof(double));
+    if(!tw[d]) goto fail;
+    for(size_t j = 0; j < padded[d]; ++j) {
+      double complex w = cexp(-2 * kPi * I * (double)j / (double)padded[d]);
+      tw[d][2*j] = creal(w); tw[d][2*j + 1] = cimag(w);
+    }
+  }
+  {
+    long long ls[3] = {(long long)shape[0], (long long)shape[1], (long long)shape[2]};
+    long long lp[3] = {(long long)padded[0], (long long)padded[1], (long long)padded[2]};
+    const double *twc[3] = {tw[0], tw[1], tw[2]};
+    double nodes[4][12], weights[4][12];
+    gauss_tables(nodes, weights);
+    if(!n2d_vie_set_gauss(&nodes[0][0], &weights[0][0])) goto fail;
+    if(!n2d_vie_create(&p->dev, ls, lp, (long long)cells, cell_box, twc, g_fft_fp32)) goto fail;
+  }
+  /* Sorted displacements a>=b>=c that fit the lattice in some orientation, in
+     the reference's enumeration order (vie_fft.c:345-351). */
+  {
+    long long S[3] = {(long long)shape[0], (long long)shape[1], (long long)shape[2]};
+    for(int i = 0; i < 2; ++i) for(int j = 0; j < 2 - i; ++j)
+      if(S[j] < S[j + 1]) { long long t = S[j]; S[j] = S[j + 1]; S[j + 1] = t; }
+    long long count = 0;
+    for(long long a = 0; a < S[0]; ++a)
+      for(long long b = 0; b <= a && b < S[1]; ++b)
+        count += (b < S[2] ? b : S[2] - 1) + 1;
+    offsets = malloc(3 * count * sizeof(int));
+    far_ok = malloc(count * sizeof(int));
+    if(!offsets || !far_ok) goto fail;
+    long long q = 0;
+    for(long long a = 0; a < S[0]; ++a)
+      for(long long b = 0; b <= a && b < S[1]; ++b)
+        for(long long c = 0; c <= b && c < S[2]; ++c) {
+          offsets[3*q] = (int)a; offsets[3*q + 1] = (int)b; offsets[3*q + 2] = (int)c; ++q;
+        }
+    if(!n2d_vie_far_tensors(p->dev, count, offsets, S, h, k, far_ok)) goto fail;
+    long long nn = 0;
+    for(long long i = 0; i < count; ++i) nn += !far_ok[i];
+    near_t = malloc((nn ? nn : 1) * 12 * sizeof(double));
+    near_i = malloc((nn ? nn : 1) * sizeof(long long));
+    if(!near_t || !near_i) goto fail;
+    long long m = 0;
+    for(long long i = 0; i < count; ++i) {
+      if(far_ok[i]) continue;
+      size_t v[3] = {(size_t)offsets[3*i], (size_t)offsets[3*i + 1], (size_t)offsets[3*i + 2]};
+      nec2c_cuda_complex n9[9];
+      double complex n[9];
+      if(!near || !near(near_ctx, v, h, k, n9)) { n2c_set_error("near-pair tensor unavailable"); goto fail; }
+      memcpy(n, n9, sizeof(n));
+      /* Symmetric off-diagonals, zero where the offset component vanishes
+         (vie_fft.c:353-356). */
+      double complex xy = (v[0] && v[1]) ? (n[1] + n[3]) * 0.5 : 0;
+      double complex xz = (v[0] && v[2]) ? (n[2] + n[6]) * 0.5 : 0;
+      double complex yz = (v[1] && v[2]) ? (n[5] + n[7]) * 0.5 : 0;
+      double complex six[6] = {n[0], n[4], n[8], xy, xz, yz};
+      for(int e = 0; e < 6; ++e) { near_t[12*m + 2*e] = creal(six[e]); near_t[12*m + 2*e + 1] = cimag(six[e]); }
+      near_i[m++] = i;
+      if(v[0] == 0) for(int d = 0; d < 3; ++d) p->self[d] = n[4*d];   /* offset (0,0,0) */
+    }
+    if(!n2d_vie_put_tensors(p->dev, m, near_i, near_t)) goto fail;
+    if(!n2d_vie_finish_spectrum(p->dev)) goto fail;
+  }
+  /* Uniform permittivity, validated like vie_fft.c:437. */
+  if(!diag_ok(p->self, er)) { n2c_set_error("singular local diagonal"); goto fail; }
+  for(size_t c = 0; c < cells; ++c) p->eps[c] = er;
+  if(!upload_eps(p)) goto fail;
+  p->x_dev = n2d_alloc(3 * cells * 2 * sizeof(double));
+  p->y_dev = n2d_alloc(3 * cells * 2 * sizeof(double));
+  if(!p->x_dev || !p->y_dev) goto fail;
+  for(int d = 0; d < 3; ++d) free(tw[d]);
+  free(cell_box); free(seen); free(offsets); free(far_ok); free(near_t); free(near_i);
+  *out = p;
+  return 1;
+fail:
+  for(int d = 0; d < 3; ++d) free(tw[d]);
+  free(cell_box); free(seen); free(offsets); free(far_ok); free(near_t); free(near_i);
+  nec2c_cuda_vie_fft_destroy(p);
+  return 0;
+}
+
+int nec2c_cuda_vie_fft_set_permittivity(nec2c_cuda_vie_plan *p, size_t cell, double re, double im)
+{
+  double complex er = re + I * im;
+  if(!p || cell >= p->cells || !isfinite(re) || !isfinite(im) || re < 1 || im > 0) return 0;
+  if(!diag_ok(p->self, er)) return 0;
+  p->eps[cell] = er;
+  p->eps_dirty = 1;
+  return 1;
+}
+
+size_t nec2c_cuda_vie_fft_bytes(const nec2c_cuda_vie_plan *p) { return p ? p->bytes : 0; }
+size_t nec2c_cuda_vie_fft_device_bytes(const nec2c_cuda_vie_plan *p) { return p ? n2d_vie_device_bytes(p->dev) : 0; }
+size_t nec2c_cuda_vie_fft_order(const nec2c_cuda_vie_plan *p) { return p ? 3 * p->cells : 0; }
+
+/* Exposed to the hybrid and GMRES code in this layer. */
+n2d_vie *nec2c_cuda_plan_device(nec2c_cuda_vie_plan *p)
+{
+  if(p->eps_dirty && !upload_eps(p)) return NULL;
+  return p->dev;
+}
+
+int nec2c_cuda_vie_fft_apply(void *ctx, const nec2c_cuda_complex *x, nec2c_cuda_complex *y)
+{
+  struct nec2c_cuda_vie_plan *p = ctx;
+  size_t bytes = 3 * p->cells * sizeof(double complex);
+  if(!nec2c_cuda_plan_device(p)) return 0;
+  return n2d_upload(p->x_dev, x, bytes) && n2d_vie_apply(p->dev, p->x_dev, p->y_dev, 0, NULL, NULL) &&
+         n2d_download(y, p->y_dev, bytes);
+}
+
+int nec2c_cuda_vie_fft_precondition(void *ctx, const nec2c_cuda_complex *x, nec2c_cuda_complex *y)
+{
+  struct nec2c_cuda_vie_plan *p = ctx;
+  size_t bytes = 3 * p->cells * sizeof(double complex);
+  if(!nec2c_cuda_plan_device(p)) return 0;
+  return n2d_upload(p->x_dev, x, bytes) && n2d_vie_precondition(p->dev, p->x_dev, p->y_dev) &&
+         n2d_download(y, p->y_dev, bytes);
+}
+
+int nec2c_cuda_vie_fft_apply_device(nec2c_cuda_vie_plan *p, const void *x_dev, void *y_dev)
+{
+  if(!nec2c_cuda_plan_device(p)) return 0;
+  return n2d_vie_apply(p->dev, x_dev, y_dev, 0, NULL, NULL);
+}
+
+int nec2c_cuda_vie_fft_spectrum(nec2c_cuda_vie_plan *p, nec2c_cuda_complex *out)
+{
+  return p && out && n2d_vie_read_spectrum(p->dev, (double *)out);
+}
+
+/* ------------------------------------------------------------------ hybrid */
+struct nec2c_cuda_hybrid {
+  n2d_hybrid *dev;
+  nec2c_cuda_vie_plan *volume;
+  size_t c, v;
+  int blocks_set;
+  double *x_dev, *y_dev;
+};
+
+int nec2c_cuda_hybrid_create(nec2c_cuda_hybrid **out, nec2c_cuda_vie_plan *volume, size_t c, size_t v,
+                             int pec)
+{
+  struct nec2c_cuda_hybrid *h;
+  if(!out) return 0;
+  *out = NULL;
+  if((v && !volume) || (volume && v != 3 * volume->cells / (pec ? 2 : 1)) || c > SIZE_MAX - v) {
+    n2c_set_error("hybrid system does not match its volume plan");
+    return 0;
+  }
+  if(!n2d_device_ok()) return 0;
+  h = calloc(1, sizeof(*h));
+  if(!h) return 0;
+  h->volume = volume; h->c = c; h->v = v;
+  if(!n2d_hybrid_create(&h->dev, volume ? volume->dev : NULL, (long long)c, (long long)v, pec)) { free(h); return 0; }
+  h->x_dev = n2d_alloc((c + v) * 2 * sizeof(double));
+  h->y_dev = n2d_alloc((c + v) * 2 * sizeof(double));
+  if(!h->x_dev || !h->y_dev) { nec2c_cuda_hybrid_destroy(h); return 0; }
+  *out = h;
+  return 1;
+}
+
+void nec2c_cuda_hybrid_destroy(nec2c_cuda_hybrid *h)
+{
+  if(!h) return;
+  n2d_hybrid_destroy(h->dev);
+  n2d_free(h->x_dev); n2d_free(h->y_dev);
+  free(h);
+}
+
+int nec2c_cuda_hybrid_set_blocks(nec2c_cuda_hybrid *h, const nec2c_cuda_complex *blocks)
+{
+  if(!h || !blocks) return 0;
+  if(h->volume && !nec2c_cuda_plan_device(h->volume)) return 0;
+  if(!n2d_hybrid_upload_blocks(h->dev, (const double *)blocks)) return 0;
+  h->blocks_set = 1;
+  return 1;
+}
+
+size_t nec2c_cuda_hybrid_order(const nec2c_cuda_hybrid *h) { return h ? h->c + h->v : 0; }
+
+static int hybrid_ready(struct nec2c_cuda_hybrid *h)
+{
+  if(!h->blocks_set) { n2c_set_error("hybrid blocks were never uploaded"); return 0; }
+  return !h->volume || nec2c_cuda_plan_device(h->volume) != NULL;
+}
+
+int nec2c_cuda_hybrid_apply(void *ctx, const nec2c_cuda_complex *x, nec2c_cuda_complex *y)
+{
+  struct nec2c_cuda_hybrid *h = ctx;
+  size_t bytes = (h->c + h->v) * sizeof(double complex);
+  return hybrid_ready(h) && n2d_upload(h->x_dev, x, bytes) &&
+         n2d_hybrid_apply(h->dev, h->x_dev, h->y_dev, 0, NULL, NULL) && n2d_download(y, h->y_dev, bytes);
+}
+
+int nec2c_cuda_hybrid_precondition(void *ctx, const nec2c_cuda_complex *x, nec2c_cuda_complex *y)
+{
+  struct nec2c_cuda_hybrid *h = ctx;
+  size_t bytes = (h->c + h->v) * sizeof(double complex);
+  /* dielectric_fft.c:77-81: a zero or non-finite conductor diagonal fails. */
+  if(h->blocks_set && !n2d_hybrid_precondition_ok(h->dev)) return 0;
+  return hybrid_ready(h) && n2d_upload(h->x_dev, x, bytes) &&
+         n2d_hybrid_precondition(h->dev, h->x_dev, h->y_dev) && n2d_download(y, h->y_dev, bytes);
+}
+
+/* ------------------------------------------------------------------- GMRES */
+static int gmres_common(int kind, void *op, size_t n, const nec2c_cuda_complex *b, nec2c_cuda_complex *x,
+                        const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *report)
+{
+  nec2c_cuda_gmres_report local;
+  nec2c_cuda_gmres_options defaults = {30, 300, 1e-12, 0.0};
+  n2d_gmres_report r;
+  if(!report) report = &local;
+  memset(report, 0, sizeof(*report));
+  report->status = ST_INVALID;
+  report->residual_norm = report->relative_residual = INFINITY;
+  if(!options) options = &defaults;
+  /* vie_iterative.c:97-103 */
+  if(!op || n == 0 || !b || !x || (const void *)b == (const void *)x || options->restart == 0 ||
+     options->maximum_iterations == 0 || !isfinite(options->relative_tolerance) ||
+     options->relative_tolerance < 0 || !isfinite(options->absolute_tolerance) ||
+     options->absolute_tolerance < 0 ||
+     (options->relative_tolerance == 0 && options->absolute_tolerance == 0))
+    return 0;
+  if(options->restart == SIZE_MAX || n > (size_t)LLONG_MAX / 64) { report->status = ST_ALLOC; return 0; }
+  int ok = n2d_gmres(kind, op, (long long)n, (const double *)b, (double *)x, options->restart,
+                     options->maximum_iterations, options->relative_tolerance,
+                     options->absolute_tolerance, &r);
+  report->status = r.status;
+  report->iterations = r.iterations;
+  report->operator_applications = r.operator_applications;
+  report->restarts = r.restarts;
+  report->residual_norm = r.residual_norm;
+  report->relative_residual = r.relative_residual;
+  return ok;
+}
+
+int nec2c_cuda_gmres_plan(nec2c_cuda_vie_plan *p, const nec2c_cuda_complex *b, nec2c_cuda_complex *x,
+                          const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *report)
+{
+  n2d_vie *dev = p ? nec2c_cuda_plan_device(p) : NULL;
+  return gmres_common(0, dev, p ? 3 * p->cells : 0, b, x, options, report);
+}
+
+int nec2c_cuda_gmres_hybrid(nec2c_cuda_hybrid *h, const nec2c_cuda_complex *b, nec2c_cuda_complex *x,
+                            const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *report)
+{
+  if(h && !hybrid_ready(h)) {
+    if(report) { memset(report, 0, sizeof(*report)); report->status = ST_CALLBACK; }
+    return 0;
+  }
+  return gmres_common(1, h ? h->dev : NULL, h ? h->c + h->v : 0, b, x, options, report);
+}

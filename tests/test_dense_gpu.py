@@ -1,0 +1,94 @@
+"""CUDA dense LU (factr/solve and the row-major builtin solve) against the
+oracle: same pivots, same U, solutions within 1e-10 relative."""
+import numpy as np
+import pytest
+
+import nec2c_b200 as nb
+from oracle_lib import oracle, ptr
+
+pytestmark = pytest.mark.gpu
+
+
+def nec_storage(a, ld):
+    """NEC's transposed column-major storage of the algebraic matrix a."""
+    n = a.shape[0]
+    st = np.zeros((ld, n), dtype=np.complex128, order="F")
+    st[:n, :n] = a.T
+    return st
+
+
+def mom_like(n, seed):
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    return a + np.diag(np.full(n, 0.5 * np.sqrt(n)))
+
+
+def test_kat():
+    """tests/dense_backend_test.c:16-33, classic storage with ld 5 and two RHS."""
+    a = np.array([[4 + 1j, 1 - 2j, 0.5], [2, 5 + 0.5j, -1j], [-1 + 1j, 0.25, 3 - 1j]])
+    x1 = np.array([1 + 2j, -0.5 + 1j, 2 - 0.25j])
+    x2 = np.array([-1j, 2 + 0.5j, -1.0])
+    assert nb.dense_backend_set("cuda")
+    st = nec_storage(a, 5)
+    ok, piv = nb.factor_classic(st)
+    assert ok
+    rhs = np.zeros((5, 2), dtype=np.complex128, order="F")
+    rhs[:3, 0] = a @ x1
+    rhs[:3, 1] = a @ x2
+    assert nb.solve_classic_many(st, piv, rhs)
+    assert np.max(np.abs(rhs[:3, 0] - x1)) < 1e-12 and np.max(np.abs(rhs[:3, 1] - x2)) < 1e-12
+    ok, b = nb.solve_row_major(a, a @ x1)
+    assert ok and np.max(np.abs(b - x1)) < 1e-12
+
+
+@pytest.mark.parametrize("n", [1, 2, 31, 32, 33, 100, 257, 700])
+def test_factor_matches_oracle(n):
+    a = mom_like(n, n)
+    ld = n + 5
+    st = nec_storage(a, ld)
+    st_o = st.copy(order="F")
+    assert nb.dense_backend_set("cuda")
+    ok, piv = nb.factor_classic(st)
+    assert ok
+    piv_o = np.zeros(n, dtype=np.int32)
+    assert oracle().oracle_factr(n, ptr(st_o), ptr(piv_o), ld)
+    assert np.array_equal(piv, piv_o)
+    U = np.triu(st[:n, :n])
+    U_o = np.triu(st_o[:n, :n])
+    assert np.max(np.abs(U - U_o)) / np.max(np.abs(U_o)) < 1e-12
+    rng = np.random.default_rng(1000 + n)
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    b = a @ x
+    rhs = np.zeros((ld, 1), dtype=np.complex128, order="F")
+    rhs[:n, 0] = b
+    assert nb.solve_classic_many(st, piv, rhs)
+    bo = np.ascontiguousarray(b.copy())
+    oracle().oracle_solve(n, ptr(st_o), ptr(piv_o), ptr(bo), ld)
+    assert np.linalg.norm(rhs[:n, 0] - bo) / np.linalg.norm(bo) < 1e-10
+    # solve from re-uploaded factors (no device cache)
+    nb.load().nec2c_cuda_dense_release()
+    rhs2 = np.zeros((ld, 1), dtype=np.complex128, order="F")
+    rhs2[:n, 0] = b
+    assert nb.solve_classic_many(st, piv, rhs2)
+    assert np.array_equal(rhs2, rhs)
+
+
+@pytest.mark.parametrize("n", [1, 5, 40, 300])
+def test_row_major_matches_oracle(n):
+    a = mom_like(n, 50 + n)
+    rng = np.random.default_rng(n)
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    ok, x = nb.solve_row_major(a, b)
+    ao, bo = np.ascontiguousarray(a.copy()), np.ascontiguousarray(b.copy())
+    assert ok and oracle().oracle_row_major_solve(ptr(ao), ptr(bo), n)
+    assert np.linalg.norm(x - bo) / np.linalg.norm(bo) < 1e-10
+
+
+def test_singular_rejected():
+    a = np.zeros((4, 4), dtype=np.complex128)
+    a[0, 0] = 1
+    st = nec_storage(a, 4)
+    ok, _ = nb.factor_classic(st)
+    assert not ok
+    ok, _ = nb.solve_row_major(a, np.ones(4))
+    assert not ok
