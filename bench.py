@@ -1,0 +1,464 @@
+#!/usr/bin/env python
+"""Benchmark of the nec2c CUDA backend on one B200 (replicas on N GPUs).
+
+Workload: a 64x64x64-voxel block of side 1 lambda at
+300 MHz (786,432 complex unknowns, 128^3 padded FFT grid), per-voxel
+eps_r ~ U[2,10] and loss tangent ~ U[0.01,0.1] (seeded), x-polarised plane
+wave excitation, GMRES(30) to rtol 1e-6 (iteration limit 10000, the CLI's
+maximum: the reference default of 300 does not reach 1e-6 here).  A step is one solve on a
+device-resident plan in the mixed form (FP32 transforms, FP64 Arnoldi, Givens
+and true residual); its current error against the plain FP64 GPU form is
+reported beside the throughput.  Synthetic, seeded inputs stand in for the
+reference's decks (it publishes no dataset).
+
+Roofline: the FFT matvec (scatter, five fused transform passes, gather) timed
+with CUDA events on the launching stream, L2 flushed between launches, against
+the algorithmic bytes s*(6C + 18G) per product (s = 8 B per complex FP32).
+
+Reference arm (--impl reference): the reference nec2c's own builtin FFT plan
+and vie_gmres (oracle/_ref, compiled from its sources) on the host cores.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+C0 = 299792458.0
+SEED = 2
+MAXIT = 10000
+# dram__bytes_read.sum + dram__bytes_write.sum per FP32 matvec on this
+# workload, summed over its kernels, from the ncu capture summarised in
+# profiles/matvec_c2_fp32.md (None until a capture exists).
+MATVEC_TRAFFIC_BYTES = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload():
+    lam = C0 / 300e6
+    n = 64
+    h, k = lam / n, 2 * math.pi / lam
+    g = np.arange(n)
+    xyz = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3).astype(np.uintp)
+    cells = xyz.shape[0]
+    rng = np.random.default_rng(SEED)
+    er = rng.uniform(2.0, 10.0, cells)
+    tand = rng.uniform(0.01, 0.1, cells)
+    eps = er * (1 - 1j * tand)
+    rhs = np.zeros(3 * cells, dtype=np.complex128)
+    z = xyz[:, 2].astype(np.float64)
+    rhs[0::3] = 2 * np.exp(-1j * k * h * (z + 0.5)) * math.sin(k * h / 2) / (k * h / 2)
+    return dict(shape=(n, n, n), xyz=xyz.reshape(-1), h=h, k=k, eps=eps, rhs=rhs, cells=cells,
+                padded=128, grid=128 ** 3)
+
+
+def near_table():
+    with open(os.path.join(ROOT, "tests", "golden", "near_tensors.json")) as f:
+        raw = json.load(f)["c2"]
+    table = {}
+    for row in raw["tensors"]:
+        v = np.array(row[3:])
+        table[tuple(int(t) for t in row[:3])] = v[0::2] + 1j * v[1::2]
+    return table
+
+
+class Clocks:
+    """nvidia-smi sampler over the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            out, _ = self.proc.communicate(timeout=10)
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [t.strip() for t in l.split(",")]
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except (ValueError, IndexError):
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------ reference arm
+def reference_lib():
+    so = os.path.join(ROOT, "oracle", "_ref", "libnec2c_ref.so")
+    if not os.path.exists(so):
+        return None
+    r = C.CDLL(so)
+    vp, sz, dbl, i = C.c_void_p, C.c_size_t, C.c_double, C.c_int
+    r.ref_fft_backend_set.argtypes = [C.c_char_p]
+    r.ref_fft_create.argtypes = [C.POINTER(sz), sz, C.POINTER(sz), dbl, dbl, dbl, dbl, sz]
+    r.ref_fft_create.restype = vp
+    r.ref_fft_set_permittivity.argtypes = [vp, sz, dbl, dbl]
+    r.ref_fft_destroy.argtypes = [vp]
+
+    class Rep(C.Structure):
+        _fields_ = [("status", C.c_int), ("iterations", C.c_size_t),
+                    ("operator_applications", C.c_size_t), ("restarts", C.c_size_t),
+                    ("residual_norm", C.c_double), ("relative_residual", C.c_double)]
+    r.Rep = Rep
+    r.ref_fft_gmres.argtypes = [vp, vp, vp, sz, sz, dbl, dbl, C.POINTER(Rep)]
+    r.ref_fft_gmres.restype = i
+    return r
+
+
+def reference_plan(r, w):
+    r.ref_fft_backend_set(b"builtin")
+    xyz = np.ascontiguousarray(w["xyz"])
+    p = r.ref_fft_create((C.c_size_t * 3)(*w["shape"]), w["cells"],
+                         xyz.ctypes.data_as(C.POINTER(C.c_size_t)), w["h"], w["k"],
+                         w["eps"][0].real, w["eps"][0].imag, 1 << 40)
+    if not p:
+        raise RuntimeError("reference plan build failed")
+    for c, e in enumerate(w["eps"]):
+        r.ref_fft_set_permittivity(p, c, e.real, e.imag)
+    return p
+
+
+def reference_solve(r, p, w, maxit=MAXIT):
+    b = np.ascontiguousarray(w["rhs"])
+    x = np.zeros_like(b)
+    rep = r.Rep()
+    t0 = time.perf_counter()
+    r.ref_fft_gmres(p, b.ctypes.data_as(C.c_void_p), x.ctypes.data_as(C.c_void_p), 30, maxit, 1e-6,
+                    0.0, C.byref(rep))
+    return time.perf_counter() - t0, rep
+
+
+def cpu_threads():
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+SAMPLE_ITERATIONS = 30
+
+
+def cpu_baseline(w, full_iterations):
+    """The reference on a bounded sample: one 30-iteration restart cycle of its
+    vie_gmres on this workload (plan build untimed, all host threads), scaled
+    to a full solve of full_iterations iterations."""
+    r = reference_lib()
+    if r is None:
+        return None
+    p = reference_plan(r, w)
+    t, rep = reference_solve(r, p, w, maxit=SAMPLE_ITERATIONS)
+    r.ref_fft_destroy(p)
+    per_iter = t / max(rep.iterations, 1)
+    return {"value": 1.0 / (per_iter * full_iterations), "unit": "solves/s", "cores": cpu_threads(),
+            "kind": "reference",
+            "sample": "reference vie_gmres (builtin FFT, OpenMP) for %d iterations (%.2f s incl. the "
+                      "initial true residual), scaled to the %d iterations of a full solve"
+                      % (rep.iterations, t, full_iterations)}
+
+
+# Iterations a full FP64 solve of this workload takes with the reference's
+# GMRES(30) (two-pass MGS, true residual at restart): measured with the plain
+# FP64 GPU form, which runs the same algorithm and matches the reference's
+# iteration counts on its own test models.  Used only to scale the reference
+# arm's bounded per-iteration sample to a full solve.
+C2_FULL_ITERATIONS = 492
+
+
+def run_reference(args, rank, world):
+    """The reference's own CPU code: each step is a bounded sample of one
+    30-iteration restart cycle (the whole solve takes about C2_FULL_ITERATIONS
+    iterations, several minutes on the host), scaled to solves/s."""
+    if rank != 0:
+        return 0
+    w = workload()
+    r = reference_lib()
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+        return 0
+    p = reference_plan(r, w)
+    for _ in range(args.warmup):
+        reference_solve(r, p, w, maxit=1)          # warm-up: one iteration each
+    per_iter = []
+    for _ in range(args.steps):
+        t, rep = reference_solve(r, p, w, maxit=SAMPLE_ITERATIONS)
+        per_iter.append(t / max(rep.iterations, 1))
+    r.ref_fft_destroy(p)
+    solve_s = [t * C2_FULL_ITERATIONS for t in per_iter]
+    v = len(solve_s) / sum(solve_s)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(solve_s) / len(solve_s),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic", "config": CONFIG,
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cpu_threads(), "kind": "reference",
+                         "sample": "per step: reference vie_gmres (builtin FFT, OpenMP) for %d "
+                                   "iterations, scaled to the %d iterations of a full solve; "
+                                   "warm-up steps are 1-iteration solves"
+                                   % (SAMPLE_ITERATIONS, C2_FULL_ITERATIONS)},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "latency_ms": {"p50": 1e3 * statistics.median(solve_s), "p99": 1e3 * max(solve_s)}}))
+    return 0
+
+
+METRIC = ("VIE solves/s at rel.err<=1e-5 vs the FP64 GPU form (64^3 inhomogeneous VIE, "
+          "GMRES(30) rtol 1e-6); FFT matvec HBM GB/s")
+CONFIG = {"workload": "c2: 64^3-voxel inhomogeneous dielectric block, side 1 lambda at 300 MHz, "
+                      "786432 unknowns, 128^3 padded grid, eps_r~U[2,10], tand~U[0.01,0.1], "
+                      "x-polarised plane wave, GMRES(30) rtol 1e-6",
+          "seed": SEED, "precision": "mixed: FP32 transforms; FP64 vectors, Arnoldi, Givens, "
+                                      "true residual",
+          "l2": "solve working set > L2 (Krylov basis 390 MB); matvec timings flush L2 (256 MB write)"}
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import nec2c_b200 as nb
+
+    torch.cuda.set_device(local_rank)
+    lib = nb.load()
+    if not lib.nec2c_cuda_set_device(local_rank) or not lib.nec2c_cuda_available():
+        raise RuntimeError("CUDA backend unavailable: " + nb.last_error())
+    stream = torch.cuda.current_stream()
+    lib.nec2c_cuda_set_stream(C.c_void_p(stream.cuda_stream))
+    w = workload()
+    table = near_table()
+
+    def make_plan(mixed):
+        t0 = time.perf_counter()
+        p = nb.VolumePlan(w["shape"], w["xyz"], w["h"], w["k"], w["eps"][0], table, mixed=mixed)
+        for c, e in enumerate(w["eps"]):
+            if not p.set_permittivity(c, e):
+                raise RuntimeError("permittivity rejected")
+        torch.cuda.synchronize()
+        return p, time.perf_counter() - t0
+
+    plan_m, build_s = make_plan(True)
+    plan_d, _ = make_plan(False)
+    n = plan_m.n
+    b_dev = torch.from_numpy(w["rhs"]).to("cuda")
+    x_dev = torch.zeros(n, dtype=torch.complex128, device="cuda")
+    opts = nb.GmresOptions(30, MAXIT, 1e-6, 0.0)
+
+    def solve_dev(plan, x):
+        x.zero_()
+        rep = nb.GmresReport()
+        ok = lib.nec2c_cuda_gmres_plan_device(plan.h, C.c_void_p(b_dev.data_ptr()),
+                                              C.c_void_p(x.data_ptr()), C.byref(opts), C.byref(rep))
+        if not ok:
+            raise RuntimeError("solve failed: %s %s" % (rep.as_dict(), nb.last_error()))
+        return rep
+
+    for _ in range(args.warmup):
+        solve_dev(plan_m, x_dev)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches0 = lib.nec2c_cuda_launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with Clocks(local_rank) as clk:
+        torch.cuda.synchronize()
+        for e0, e1 in ev:
+            e0.record(stream)
+            rep = solve_dev(plan_m, x_dev)
+            e1.record(stream)
+        torch.cuda.synchronize()
+    launches = lib.nec2c_cuda_launch_count() - launches0
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    iterations = rep.iterations
+    x_mixed = x_dev.clone()
+
+    # Plain FP64 form on the same solve, and the current error against it.
+    solve_dev(plan_d, x_dev)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    rep64 = solve_dev(plan_d, x_dev)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fp64_ms = e0.elapsed_time(e1)
+    rel_err = float(torch.linalg.norm(x_mixed - x_dev) / torch.linalg.norm(x_dev))
+
+    # e2e through the public C ABI with pinned host buffers (H2D + D2H inside).
+    b_host = torch.from_numpy(w["rhs"]).pin_memory()
+    x_host = torch.zeros(n, dtype=torch.complex128).pin_memory()
+    e2e_ms = []
+    for _ in range(max(1, args.steps)):
+        x_host.zero_()
+        rep_h = nb.GmresReport()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ok = lib.nec2c_cuda_gmres_plan(plan_m.h, C.c_void_p(b_host.data_ptr()),
+                                       C.c_void_p(x_host.data_ptr()), C.byref(opts), C.byref(rep_h))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if not ok:
+            raise RuntimeError("host-vector solve failed")
+        e2e_ms.append(e0.elapsed_time(e1))
+
+    # Matvec roofline: device products, L2 flushed between launches.
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    xv = torch.randn(n, dtype=torch.complex128, device="cuda")
+    yv = torch.empty_like(xv)
+
+    def time_matvec(plan, reps=20):
+        out = []
+        for i in range(reps + 3):
+            flush.zero_()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            lib.nec2c_cuda_vie_fft_apply_device(plan.h, C.c_void_p(xv.data_ptr()),
+                                                C.c_void_p(yv.data_ptr()))
+            a1.record(stream)
+            torch.cuda.synchronize()
+            if i >= 3:
+                out.append(a0.elapsed_time(a1))
+        return statistics.median(out)
+
+    mv32_ms = time_matvec(plan_m)
+    mv64_ms = time_matvec(plan_d)
+    C_, G_ = w["cells"], w["grid"]
+    bytes32 = 8 * (6 * C_ + 18 * G_)
+    bytes64 = 16 * (6 * C_ + 18 * G_)
+    peak, peak_kind = peaks()
+    achieved = bytes32 / (mv32_ms * 1e-3) / 1e9
+
+    # Config-1 shaped dense LU (1984 unknowns), FP64, through the classic ABI.
+    dense = dense_bench(nb, torch, stream)
+
+    if rank != 0:
+        return 0
+    cpu = None if (args.no_cpu_baseline or world > 1) else cpu_baseline(w, rep64.iterations)
+    value = world * args.steps / (total_ms * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64 transforms / c128 Krylov",
+        "data": "synthetic", "config": dict(CONFIG, parallelism="replicas" if world > 1 else "1 GPU"),
+        "iterations": iterations, "rel_err_vs_fp64_gpu": rel_err,
+        "latency_ms": {"p50": statistics.median(step_ms), "p99": max(step_ms)},
+        "fp64_form": {"solves_per_s": 1e3 / fp64_ms, "iterations": rep64.iterations,
+                      "ms": fp64_ms},
+        "plan_build_s": build_s,
+        "e2e": {"value": world * 1e3 / statistics.median(e2e_ms), "unit": "solves/s",
+                "h2d_bytes_per_step": 2 * 16 * n, "d2h_bytes_per_step": 16 * n},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": MATVEC_TRAFFIC_BYTES,
+                     "kernel": "FFT matvec (scatter + 5 transform passes + gather), FP32",
+                     "algorithmic_bytes": bytes32, "ms": mv32_ms},
+        "matvec_fp64": {"ms": mv64_ms, "achieved_gbs": bytes64 / (mv64_ms * 1e-3) / 1e9},
+        "dense_lu_c1": dense,
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def dense_bench(nb, torch, stream):
+    n = 1984
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    a += np.diag(np.full(n, 0.5 * math.sqrt(n)))
+    xe = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    b = a @ xe
+    nb.dense_backend_set("cuda")
+    times, err = [], None
+    for it in range(3):
+        st = np.asfortranarray(a.T.copy())
+        rhs = np.asfortranarray(b.reshape(n, 1).copy())
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ok, piv = nb.factor_classic(st)
+        ok = ok and nb.solve_classic_many(st, piv, rhs)
+        t = time.perf_counter() - t0
+        if not ok:
+            raise RuntimeError("dense solve failed")
+        times.append(t)
+        err = float(np.linalg.norm(rhs[:, 0] - xe) / np.linalg.norm(xe))
+    t = min(times)
+    flops = 8 * n ** 3 / 3
+    return {"order": n, "ms": 1e3 * t, "solves_per_s": 1 / t, "gflops": flops / t / 1e9,
+            "rel_err": err, "note": "FP64 factor + solve through the classic C ABI (host buffers)"}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            return run_reference(args, rank, world)
+        return run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -27,6 +27,8 @@ int nec2c_cuda_available(void);
 const char *nec2c_cuda_last_error(void);
 /* Enqueue this thread's work on the given cudaStream_t (NULL: legacy default). */
 void nec2c_cuda_set_stream(void *cuda_stream);
+/* Selects the CUDA device for this thread's subsequent calls (cudaSetDevice). */
+int nec2c_cuda_set_device(int device);
 /* Number of kernels this library has launched since it was loaded. */
 unsigned long long nec2c_cuda_launch_count(void);
 
@@ -126,6 +128,13 @@ int nec2c_cuda_gmres_plan(nec2c_cuda_vie_plan *plan, const nec2c_cuda_complex *b
 int nec2c_cuda_gmres_hybrid(nec2c_cuda_hybrid *system, const nec2c_cuda_complex *b,
                             nec2c_cuda_complex *x, const nec2c_cuda_gmres_options *options,
                             nec2c_cuda_gmres_report *report);
+/* The same solves on device-resident b and x (complex double, order entries). */
+int nec2c_cuda_gmres_plan_device(nec2c_cuda_vie_plan *plan, const void *b_dev, void *x_dev,
+                                 const nec2c_cuda_gmres_options *options,
+                                 nec2c_cuda_gmres_report *report);
+int nec2c_cuda_gmres_hybrid_device(nec2c_cuda_hybrid *system, const void *b_dev, void *x_dev,
+                                   const nec2c_cuda_gmres_options *options,
+                                   nec2c_cuda_gmres_report *report);
 
 /* ------------------------------------------------------------ dense LU */
 /* Replaces dense_backend_set (dense_backend.h:14) for "cuda" (FP64 LU) and

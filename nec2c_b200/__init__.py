@@ -50,6 +50,7 @@ def load():
         "nec2c_cuda_available": (i, []),
         "nec2c_cuda_last_error": (C.c_char_p, []),
         "nec2c_cuda_set_stream": (None, [vp]),
+        "nec2c_cuda_set_device": (i, [i]),
         "nec2c_cuda_launch_count": (C.c_ulonglong, []),
         "nec2c_cuda_vie_fft_backend_set": (i, [C.c_char_p]),
         "nec2c_cuda_vie_fft_backend_name": (C.c_char_p, []),
@@ -72,6 +73,8 @@ def load():
         "nec2c_cuda_hybrid_precondition": (i, [vp, vp, vp]),
         "nec2c_cuda_gmres_plan": (i, [vp, vp, vp, vp, vp]),
         "nec2c_cuda_gmres_hybrid": (i, [vp, vp, vp, vp, vp]),
+        "nec2c_cuda_gmres_plan_device": (i, [vp, vp, vp, vp, vp]),
+        "nec2c_cuda_gmres_hybrid_device": (i, [vp, vp, vp, vp, vp]),
         "nec2c_cuda_dense_backend_set": (i, [C.c_char_p]),
         "nec2c_cuda_dense_backend_name": (C.c_char_p, []),
         "nec2c_cuda_dense_factor_classic": (i, [sz, vp, sz, vp]),

@@ -32,6 +32,7 @@ int n2d_download2d(void *dst, size_t dpitch, const void *src_dev, size_t spitch,
                    size_t rows);
 /* 1 when a compute capability 10.x device is present. */
 int n2d_device_ok(void);
+int n2d_set_device(int device);
 /* Kernels this library has launched since load (for the launch-count check). */
 unsigned long long n2d_launch_count(void);
 
@@ -65,9 +66,10 @@ int n2d_vie_read_spectrum(n2d_vie *p, double *out);
 int n2d_vie_set_eps(n2d_vie *p, const double *eps, const double *self);
 /* y_dev = A z where z = x_dev (or x_dev ./ diag when precondition_input).
    When norm_dev is non-NULL, the sum of |y|^2 is written there (and a
-   non-finite y sets *flag_dev to 1 when flag_dev is non-NULL). */
+   non-finite y sets *flag_dev to 1 when flag_dev is non-NULL).  Mixed plans
+   transform in FP32 unless full_precision is set (FP64 spectrum and grids). */
 int n2d_vie_apply(n2d_vie *p, const double *x_dev, double *y_dev, int precondition_input,
-                  double *norm_dev, int *flag_dev);
+                  double *norm_dev, int *flag_dev, int full_precision);
 /* y_dev = x_dev ./ (eps - (eps-1) self). */
 int n2d_vie_precondition(n2d_vie *p, const double *x_dev, double *y_dev);
 const double *n2d_vie_diag(const n2d_vie *p);
@@ -83,7 +85,7 @@ void n2d_hybrid_destroy(n2d_hybrid *h);
 /* Uploads the dense blocks (c*(c+v) + v*c complex, dielectric_fft.c:34-40). */
 int n2d_hybrid_upload_blocks(n2d_hybrid *h, const double *blocks);
 int n2d_hybrid_apply(n2d_hybrid *h, const double *x_dev, double *y_dev, int precondition_input,
-                     double *norm_dev, int *flag_dev);
+                     double *norm_dev, int *flag_dev, int full_precision);
 int n2d_hybrid_precondition(n2d_hybrid *h, const double *x_dev, double *y_dev);
 long long n2d_hybrid_order(const n2d_hybrid *h);
 /* 0 when a conductor diagonal is zero or non-finite (dielectric_fft.c:77-81). */

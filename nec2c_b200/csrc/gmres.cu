@@ -246,9 +246,12 @@ struct OpView {
   const double2 *pdiag;
 };
 
-static int op_apply(const OpView &o, const double *x, double *y, int precond, double *norm, int *flag) {
-  if (o.kind == 0) return n2d_vie_apply((n2d_vie *)o.op, x, y, precond, norm, flag);
-  return n2d_hybrid_apply((n2d_hybrid *)o.op, x, y, precond, norm, flag);
+// Arnoldi products use the operator's transform precision; the true residual
+// at every restart is always FP64 (full_precision).
+static int op_apply(const OpView &o, const double *x, double *y, int precond, double *norm, int *flag,
+                    int full_precision) {
+  if (o.kind == 0) return n2d_vie_apply((n2d_vie *)o.op, x, y, precond, norm, flag, full_precision);
+  return n2d_hybrid_apply((n2d_hybrid *)o.op, x, y, precond, norm, flag, full_precision);
 }
 
 template <int E>
@@ -357,7 +360,7 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
   auto true_residual = [&]() -> int {
     ++rep->operator_applications;
     if (!n2d_memset(dflag, 0, sizeof(int))) return 0;
-    if (!op_apply(o, (const double *)x_dev, (double *)b.r, 0, nullptr, dflag)) { rep->status = ST_CALLBACK; return 0; }
+    if (!op_apply(o, (const double *)x_dev, (double *)b.r, 0, nullptr, dflag, 1)) { rep->status = ST_CALLBACK; return 0; }
     residual_kernel<<<grid1(n), 256, 0, n2c_stream()>>>(b_dev, b.r, n);
     if (!n2c_check_launch("residual")) return 0;
     double sq = 0;
@@ -393,7 +396,7 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
         if (!act) break;
       }
       if (!op_apply(o, (const double *)(b.V + (long long)j * n), (double *)b.w, o.pdiag != nullptr,
-                    &b.st->before_sq, &b.st->flag)) { launch_fail = true; break; }
+                    &b.st->before_sq, &b.st->flag, 0)) { launch_fail = true; break; }
       if (!arnoldi(b, n, (int)m, j, blocks, threads)) { launch_fail = true; break; }
     }
     n2d_set_gate(nullptr);

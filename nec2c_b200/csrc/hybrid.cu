@@ -156,10 +156,12 @@ extern "C" int n2d_hybrid_precondition_ok(const n2d_hybrid *h) { return h->preco
 const double2 *n2c_hybrid_pdiag(const n2d_hybrid *h) { return h->pdiag; }
 
 extern "C" int n2d_hybrid_apply(n2d_hybrid *h, const double *x, double *y, int precondition_input,
-                                double *norm, int *flag) {
+                                double *norm, int *flag, int full_precision) {
   const long long c = h->c, v = h->v, n = h->n;
   const double2 *pd = precondition_input ? h->pdiag : nullptr;
-  if (v && !n2d_vie_apply(h->vol, x + 2 * c, y + 2 * c, precondition_input, nullptr, flag)) return 0;
+  if (v && !n2d_vie_apply(h->vol, x + 2 * c, y + 2 * c, precondition_input, nullptr, flag,
+                          full_precision))
+    return 0;
   if (c) {
     conductor_rows_kernel<<<(unsigned)c, 256, 0, n2c_stream()>>>(h->blocks, (const double2 *)x, pd, c,
                                                                  n, (double2 *)y, n2c_gate());

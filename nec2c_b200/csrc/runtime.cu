@@ -86,6 +86,11 @@ extern "C" int n2d_download2d(void *dst, size_t dpitch, const void *src, size_t 
   N2C_CHECK(cudaStreamSynchronize(g_stream));
   return 1;
 }
+extern "C" int n2d_set_device(int device) {
+  N2C_CHECK(cudaSetDevice(device));
+  return 1;
+}
+
 extern "C" int n2d_device_ok(void) {
   int count = 0, dev = 0, major = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1) {

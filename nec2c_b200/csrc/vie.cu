@@ -347,7 +347,8 @@ static unsigned grid_for(long long n, int threads = 256) {
 
 static void free_plan(n2d_vie *p) {
   if (!p) return;
-  void *bufs[] = {p->cell_box, p->box_cell, p->eps, p->diag, p->spec, p->box, p->t1, p->t2,
+  void *bufs[] = {p->cell_box, p->box_cell, p->eps, p->diag, p->spec64,
+                  p->fp32 ? p->spec : nullptr, p->box, p->t1, p->t2,
                   p->tw64[0], p->tw64[1], p->tw64[2], p->tw32[0], p->tw32[1], p->tw32[2],
                   p->table, p->table_ok, p->offsets, p->slab_start, p->row_start, p->partials,
                   p->ticket};
@@ -393,17 +394,19 @@ extern "C" int n2d_vie_create(n2d_vie **out, const long long shape[3], const lon
   p->box_cell = (int *)track(p, p->nbox * sizeof(int));
   p->eps = (double2 *)track(p, cells * sizeof(double2));
   p->diag = (double2 *)track(p, 3 * cells * sizeof(double2));
-  p->spec = track(p, 6 * p->G * ce);
-  p->box = track(p, 3 * p->nbox * ce);
-  p->t1 = track(p, 3 * p->S[0] * p->S[1] * p->P[2] * ce);
-  p->t2 = track(p, 3 * p->S[0] * p->P[1] * p->P[2] * ce);
+  p->spec64 = (double2 *)track(p, 6 * p->G * sizeof(double2));
+  p->spec = fp32 ? track(p, 6 * p->G * ce) : (void *)p->spec64;
+  const size_t we = sizeof(double2);
+  p->box = track(p, 3 * p->nbox * we);
+  p->t1 = track(p, 3 * p->S[0] * p->S[1] * p->P[2] * we);
+  p->t2 = track(p, 3 * p->S[0] * p->P[1] * p->P[2] * we);
   p->partials = (double *)track(p, 4096 * sizeof(double));
   p->ticket = (unsigned int *)track(p, 64);
   for (int d = 0; d < 3; ++d) {
     p->tw64[d] = (double2 *)track(p, padded[d] * sizeof(double2));
     p->tw32[d] = (float2 *)track(p, padded[d] * sizeof(float2));
   }
-  if (!p->cell_box || !p->box_cell || !p->eps || !p->diag || !p->spec || !p->box || !p->t1 ||
+  if (!p->cell_box || !p->box_cell || !p->eps || !p->diag || !p->spec || !p->spec64 || !p->box || !p->t1 ||
       !p->t2 || !p->partials || !p->ticket || !p->tw64[0] || !p->tw64[1] || !p->tw64[2] ||
       !p->tw32[0] || !p->tw32[1] || !p->tw32[2]) {
     free_plan(p);
@@ -490,27 +493,26 @@ extern "C" int n2d_vie_finish_spectrum(n2d_vie *p) {
   FillArgs f;
   for (int d = 0; d < 3; ++d) { f.P[d] = p->P[d]; f.S[d] = p->S[d]; f.Ss[d] = p->Ss[d]; }
   f.slab_start = p->slab_start; f.row_start = p->row_start; f.table = p->table; f.G = p->G;
-  // The FP64 spectrum is built in place when the plan is FP64, otherwise in a
-  // temporary FP64 grid that is then rounded into the plan's FP32 storage.
-  double2 *work = p->fp32 ? (double2 *)n2d_alloc(6 * p->G * sizeof(double2)) : (double2 *)p->spec;
-  if (!work) return 0;
+  // The spectrum is built and transformed in FP64, scaled by 1/G in place,
+  // and for mixed plans also rounded into the FP32 copy.
+  double2 *work = p->spec64;
   f.spec = work;
   fill_kernel<<<grid_for(p->G), 256, 0, n2c_stream()>>>(f);
   int ok = n2c_check_launch("fill_kernel");
   const double2 *tw[3] = {p->tw64[0], p->tw64[1], p->tw64[2]};
   ok = ok && transform_spectrum<double2>(p, work, tw);
   const double scale = 1.0 / (double)p->G;
+  if (ok) {
+    scale_convert_kernel<double2><<<grid_for(6 * p->G), 256, 0, n2c_stream()>>>(
+        work, work, 6 * p->G, scale);
+    ok = n2c_check_launch("scale_convert");
+  }
   if (ok && p->fp32) {
     scale_convert_kernel<float2><<<grid_for(6 * p->G), 256, 0, n2c_stream()>>>(
-        work, (float2 *)p->spec, 6 * p->G, scale);
-    ok = n2c_check_launch("scale_convert");
-  } else if (ok) {
-    scale_convert_kernel<double2><<<grid_for(6 * p->G), 256, 0, n2c_stream()>>>(
-        work, (double2 *)p->spec, 6 * p->G, scale);
+        work, (float2 *)p->spec, 6 * p->G, 1.0);
     ok = n2c_check_launch("scale_convert");
   }
   ok = ok && n2d_sync();
-  if (p->fp32) n2d_free(work);
   // The offset table is only needed while building.
   n2d_free(p->table); n2d_free(p->table_ok); n2d_free(p->offsets);
   n2d_free(p->slab_start); n2d_free(p->row_start);
@@ -522,11 +524,7 @@ extern "C" int n2d_vie_finish_spectrum(n2d_vie *p) {
 }
 
 extern "C" int n2d_vie_read_spectrum(n2d_vie *p, double *out) {
-  if (!p->fp32) return n2d_download(out, p->spec, 6 * p->G * sizeof(double2));
-  std::vector<float2> tmp(6 * p->G);
-  if (!n2d_download(tmp.data(), p->spec, 6 * p->G * sizeof(float2))) return 0;
-  for (long long i = 0; i < 6 * p->G; ++i) { out[2 * i] = tmp[i].x; out[2 * i + 1] = tmp[i].y; }
-  return 1;
+  return n2d_download(out, p->spec64, 6 * p->G * sizeof(double2));
 }
 
 extern "C" int n2d_vie_set_eps(n2d_vie *p, const double *eps, const double *self) {
@@ -542,15 +540,17 @@ static int apply_t(n2d_vie *p, const double2 *x, double2 *y, const double2 *diag
                    int *flag) {
   const long long nx = p->S[0], ny = p->S[1], nz = p->S[2];
   const long long Px = p->P[0], Py = p->P[1], Pz = p->P[2];
+  constexpr bool single = sizeof(C) == sizeof(float2);
   C *box = (C *)p->box, *t1 = (C *)p->t1, *t2 = (C *)p->t2;
   const C *tw[3];
-  for (int d = 0; d < 3; ++d) tw[d] = p->fp32 ? (const C *)p->tw32[d] : (const C *)p->tw64[d];
+  for (int d = 0; d < 3; ++d) tw[d] = single ? (const C *)p->tw32[d] : (const C *)p->tw64[d];
+  const C *spec = single ? (const C *)p->spec : (const C *)p->spec64;
   scatter_kernel<C><<<grid_for(p->nbox), 256, 0, n2c_stream()>>>(x, diag, p->box_cell, box, p->nbox,
                                                                  p->mirror, flag, n2c_gate());
   if (!n2c_check_launch("scatter")) return 0;
   if (!axis_pass<C>(0, (int)Pz, box, t1, tw[2], 3 * nx * ny, 1, nz, Pz, (int)nz, (int)Pz)) return 0;
   if (!axis_pass<C>(0, (int)Py, t1, t2, tw[1], 3 * nx, Pz, ny, Py, (int)ny, (int)Py)) return 0;
-  if (!product_pass<C>((int)Px, t2, t2, tw[0], (const C *)p->spec, Py * Pz, (int)nx)) return 0;
+  if (!product_pass<C>((int)Px, t2, t2, tw[0], spec, Py * Pz, (int)nx)) return 0;
   if (!axis_pass<C>(1, (int)Py, t2, t1, tw[1], 3 * nx, Pz, Py, ny, (int)Py, (int)ny)) return 0;
   if (!axis_pass<C>(1, (int)Pz, t1, box, tw[2], 3 * nx * ny, 1, Pz, nz, (int)Pz, (int)nz)) return 0;
   const long long out_cells = p->mirror ? p->mirror : p->cells;
@@ -563,9 +563,9 @@ static int apply_t(n2d_vie *p, const double2 *x, double2 *y, const double2 *diag
 }
 
 extern "C" int n2d_vie_apply(n2d_vie *p, const double *x, double *y, int precondition_input,
-                             double *norm, int *flag) {
+                             double *norm, int *flag, int full_precision) {
   const double2 *diag = precondition_input ? p->diag : nullptr;
-  if (p->fp32) return apply_t<float2>(p, (const double2 *)x, (double2 *)y, diag, norm, flag);
+  if (p->fp32 && !full_precision) return apply_t<float2>(p, (const double2 *)x, (double2 *)y, diag, norm, flag);
   return apply_t<double2>(p, (const double2 *)x, (double2 *)y, diag, norm, flag);
 }
 

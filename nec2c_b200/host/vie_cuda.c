@@ -22,6 +22,7 @@ static int g_fft_fp32 = 0;
 int nec2c_cuda_available(void) { return n2d_device_ok(); }
 const char *nec2c_cuda_last_error(void) { return n2d_last_error(); }
 void nec2c_cuda_set_stream(void *s) { n2d_set_stream(s); }
+int nec2c_cuda_set_device(int device) { return n2d_set_device(device); }
 unsigned long long nec2c_cuda_launch_count(void) { return n2d_launch_count(); }
 
 int nec2c_cuda_vie_fft_backend_set(const char *name)
@@ -247,7 +248,7 @@ size_t nec2c_cuda_vie_fft_device_bytes(const nec2c_cuda_vie_plan *p) { return p 
 size_t nec2c_cuda_vie_fft_order(const nec2c_cuda_vie_plan *p) { return p ? 3 * p->cells : 0; }
 
 /* Exposed to the hybrid and GMRES code in this layer. */
-n2d_vie *nec2c_cuda_plan_device(nec2c_cuda_vie_plan *p)
+__attribute__((visibility("hidden"))) n2d_vie *nec2c_cuda_plan_device(nec2c_cuda_vie_plan *p)
 {
   if(p->eps_dirty && !upload_eps(p)) return NULL;
   return p->dev;
@@ -258,7 +259,7 @@ int nec2c_cuda_vie_fft_apply(void *ctx, const nec2c_cuda_complex *x, nec2c_cuda_
   struct nec2c_cuda_vie_plan *p = ctx;
   size_t bytes = 3 * p->cells * sizeof(double complex);
   if(!nec2c_cuda_plan_device(p)) return 0;
-  return n2d_upload(p->x_dev, x, bytes) && n2d_vie_apply(p->dev, p->x_dev, p->y_dev, 0, NULL, NULL) &&
+  return n2d_upload(p->x_dev, x, bytes) && n2d_vie_apply(p->dev, p->x_dev, p->y_dev, 0, NULL, NULL, 0) &&
          n2d_download(y, p->y_dev, bytes);
 }
 
@@ -274,7 +275,7 @@ int nec2c_cuda_vie_fft_precondition(void *ctx, const nec2c_cuda_complex *x, nec2
 int nec2c_cuda_vie_fft_apply_device(nec2c_cuda_vie_plan *p, const void *x_dev, void *y_dev)
 {
   if(!nec2c_cuda_plan_device(p)) return 0;
-  return n2d_vie_apply(p->dev, x_dev, y_dev, 0, NULL, NULL);
+  return n2d_vie_apply(p->dev, x_dev, y_dev, 0, NULL, NULL, 0);
 }
 
 int nec2c_cuda_vie_fft_spectrum(nec2c_cuda_vie_plan *p, nec2c_cuda_complex *out)
@@ -343,7 +344,7 @@ int nec2c_cuda_hybrid_apply(void *ctx, const nec2c_cuda_complex *x, nec2c_cuda_c
   struct nec2c_cuda_hybrid *h = ctx;
   size_t bytes = (h->c + h->v) * sizeof(double complex);
   return hybrid_ready(h) && n2d_upload(h->x_dev, x, bytes) &&
-         n2d_hybrid_apply(h->dev, h->x_dev, h->y_dev, 0, NULL, NULL) && n2d_download(y, h->y_dev, bytes);
+         n2d_hybrid_apply(h->dev, h->x_dev, h->y_dev, 0, NULL, NULL, 0) && n2d_download(y, h->y_dev, bytes);
 }
 
 int nec2c_cuda_hybrid_precondition(void *ctx, const nec2c_cuda_complex *x, nec2c_cuda_complex *y)
@@ -357,7 +358,7 @@ int nec2c_cuda_hybrid_precondition(void *ctx, const nec2c_cuda_complex *x, nec2c
 }
 
 /* ------------------------------------------------------------------- GMRES */
-static int gmres_common(int kind, void *op, size_t n, const nec2c_cuda_complex *b, nec2c_cuda_complex *x,
+static int gmres_common(int kind, void *op, size_t n, const void *b, void *x, int device,
                         const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *report)
 {
   nec2c_cuda_gmres_report local;
@@ -376,9 +377,10 @@ static int gmres_common(int kind, void *op, size_t n, const nec2c_cuda_complex *
      (options->relative_tolerance == 0 && options->absolute_tolerance == 0))
     return 0;
   if(options->restart == SIZE_MAX || n > (size_t)LLONG_MAX / 64) { report->status = ST_ALLOC; return 0; }
-  int ok = n2d_gmres(kind, op, (long long)n, (const double *)b, (double *)x, options->restart,
-                     options->maximum_iterations, options->relative_tolerance,
-                     options->absolute_tolerance, &r);
+  int ok = (device ? n2d_gmres_dev : n2d_gmres)(kind, op, (long long)n, (const double *)b, (double *)x,
+                                                 options->restart, options->maximum_iterations,
+                                                 options->relative_tolerance,
+                                                 options->absolute_tolerance, &r);
   report->status = r.status;
   report->iterations = r.iterations;
   report->operator_applications = r.operator_applications;
@@ -392,7 +394,14 @@ int nec2c_cuda_gmres_plan(nec2c_cuda_vie_plan *p, const nec2c_cuda_complex *b, n
                           const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *report)
 {
   n2d_vie *dev = p ? nec2c_cuda_plan_device(p) : NULL;
-  return gmres_common(0, dev, p ? 3 * p->cells : 0, b, x, options, report);
+  return gmres_common(0, dev, p ? 3 * p->cells : 0, b, x, 0, options, report);
+}
+
+int nec2c_cuda_gmres_plan_device(nec2c_cuda_vie_plan *p, const void *b, void *x,
+                                 const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *report)
+{
+  n2d_vie *dev = p ? nec2c_cuda_plan_device(p) : NULL;
+  return gmres_common(0, dev, p ? 3 * p->cells : 0, b, x, 1, options, report);
 }
 
 int nec2c_cuda_gmres_hybrid(nec2c_cuda_hybrid *h, const nec2c_cuda_complex *b, nec2c_cuda_complex *x,
@@ -402,5 +411,15 @@ int nec2c_cuda_gmres_hybrid(nec2c_cuda_hybrid *h, const nec2c_cuda_complex *b, n
     if(report) { memset(report, 0, sizeof(*report)); report->status = ST_CALLBACK; }
     return 0;
   }
-  return gmres_common(1, h ? h->dev : NULL, h ? h->c + h->v : 0, b, x, options, report);
+  return gmres_common(1, h ? h->dev : NULL, h ? h->c + h->v : 0, b, x, 0, options, report);
+}
+
+int nec2c_cuda_gmres_hybrid_device(nec2c_cuda_hybrid *h, const void *b, void *x,
+                                   const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *report)
+{
+  if(h && !hybrid_ready(h)) {
+    if(report) { memset(report, 0, sizeof(*report)); report->status = ST_CALLBACK; }
+    return 0;
+  }
+  return gmres_common(1, h ? h->dev : NULL, h ? h->c + h->v : 0, b, x, 1, options, report);
 }
