@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", choices=["matvec", "solve"],
+                    help="profiling driver: build the plans, run --steps FP32 and FP64 products "
+                         "(matvec) or --steps mixed solves (solve), print timings and exit")
     return ap.parse_args()
 
 
@@ -285,6 +288,8 @@ def run_ours(args, rank, world, local_rank):
     plan_m, build_s = make_plan(True)
     plan_d, _ = make_plan(False)
     n = plan_m.n
+    if args.only:
+        return profile_driver(args, lib, nb, torch, stream, plan_m, plan_d, w)
     b_dev = torch.from_numpy(w["rhs"]).to("cuda")
     x_dev = torch.zeros(n, dtype=torch.complex128, device="cuda")
     opts = nb.GmresOptions(30, MAXIT, 1e-6, 0.0)
@@ -410,6 +415,32 @@ def run_ours(args, rank, world, local_rank):
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))
+    return 0
+
+
+def profile_driver(args, lib, nb, torch, stream, plan_m, plan_d, w):
+    n = plan_m.n
+    x = torch.randn(n, dtype=torch.complex128, device="cuda")
+    y = torch.empty_like(x)
+    t0 = time.perf_counter()
+    if args.only == "matvec":
+        for plan in (plan_m, plan_d):
+            for _ in range(args.steps):
+                if not lib.nec2c_cuda_vie_fft_apply_device(plan.h, C.c_void_p(x.data_ptr()),
+                                                           C.c_void_p(y.data_ptr())):
+                    raise RuntimeError(nb.last_error())
+    else:
+        b = torch.from_numpy(w["rhs"]).to("cuda")
+        opts = nb.GmresOptions(30, MAXIT, 1e-6, 0.0)
+        for _ in range(args.steps):
+            y.zero_()
+            rep = nb.GmresReport()
+            if not lib.nec2c_cuda_gmres_plan_device(plan_m.h, C.c_void_p(b.data_ptr()),
+                                                    C.c_void_p(y.data_ptr()), C.byref(opts),
+                                                    C.byref(rep)):
+                raise RuntimeError(nb.last_error())
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": args.only, "steps": args.steps, "s": time.perf_counter() - t0}))
     return 0
 
 
