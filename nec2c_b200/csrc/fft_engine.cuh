@@ -26,33 +26,45 @@ template <int R> __host__ __device__ constexpr int bitrev_c(int i) {
   return r;
 }
 
-// In-register radix-2 DIT DFT of R points (natural-order output).
-// tw[m] = exp(-2 pi i m / L); the R-point root W_R^m is tw[m * STRIDE].
-template <int R, bool INV, int STRIDE, typename C>
-__device__ __forceinline__ void dft_reg(C (&a)[R], const C *__restrict__ tw) {
-#pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const int r = bitrev_c<R>(i);
-    if (i < r) { C t = a[i]; a[i] = a[r]; a[r] = t; }
+// Bit-reversal permutation of a register array, unrolled at compile time.
+template <int R, int I, typename C>
+__device__ __forceinline__ void bitrev_perm(C (&a)[R]) {
+  if constexpr (I < R) {
+    constexpr int J = bitrev_c<R>(I);
+    if constexpr (I < J) { C t = a[I]; a[I] = a[J]; a[J] = t; }
+    bitrev_perm<R, I + 1>(a);
   }
+}
+
+// Butterflies of one radix-2 stage (span SPAN) and, recursively, the rest.
+template <int R, bool INV, int STRIDE, int SPAN, typename C>
+__device__ __forceinline__ void dit_stages(C (&a)[R], const C *__restrict__ tw) {
+  if constexpr (SPAN <= R) {
+    constexpr int HALF = SPAN / 2;
 #pragma unroll
-  for (int span = 2; span <= R; span <<= 1) {
-    const int half = span >> 1;
+    for (int base = 0; base < R; base += SPAN) {
 #pragma unroll
-    for (int base = 0; base < R; base += span) {
-#pragma unroll
-      for (int k = 0; k < half; ++k) {
-        C u = a[base + k], v = a[base + k + half];
+      for (int k = 0; k < HALF; ++k) {
+        C u = a[base + k], v = a[base + k + HALF];
         if (k != 0) {
-          C w = __ldg(&tw[k * (R / span) * STRIDE]);
+          C w = __ldg(&tw[k * (R / SPAN) * STRIDE]);
           if (INV) w.y = -w.y;
           v = cmul(v, w);
         }
         a[base + k] = cadd(u, v);
-        a[base + k + half] = csub(u, v);
+        a[base + k + HALF] = csub(u, v);
       }
     }
+    dit_stages<R, INV, STRIDE, SPAN * 2>(a, tw);
   }
+}
+
+// In-register radix-2 DIT DFT of R points (natural-order output).
+// tw[m] = exp(-2 pi i m / L); the R-point root W_R^m is tw[m * STRIDE].
+template <int R, bool INV, int STRIDE, typename C>
+__device__ __forceinline__ void dft_reg(C (&a)[R], const C *__restrict__ tw) {
+  bitrev_perm<R, 0>(a);
+  dit_stages<R, INV, STRIDE, 2>(a, tw);
 }
 
 template <typename C> struct PassArgs {
@@ -68,7 +80,21 @@ template <typename C> struct PassArgs {
   const int *gate;    // skip all work when *gate == 0 (NULL: always run)
   long long comp_in, comp_out;  // product pass: distance between the 3 components
   long long spec_comp;          // product pass: distance between spectrum slots
+  int Py, Pz, Hy, Hz;           // product pass: padded y/z extents, octant extents
 };
+
+// The transformed Green tensor is even (xx yy zz) or odd (xy: x,y; xz: x,z;
+// yz: y,z) in every axis, so only the octant k <= P/2 per axis is stored:
+// Ghat(k) = sign * Ghat(fold(k)), fold(k) = min(k, P-k).
+struct Fold {
+  int idx;     // folded index
+  float sgn;   // -1 when k > P/2
+};
+__device__ __forceinline__ Fold fold(int k, int P) {
+  Fold f;
+  if (2 * k > P) { f.idx = P - k; f.sgn = -1.f; } else { f.idx = k; f.sgn = 1.f; }
+  return f;
+}
 
 template <typename C>
 __device__ __forceinline__ void line_base(const PassArgs<C> &a, long long l, long long &bin, long long &bout) {
@@ -214,11 +240,17 @@ __global__ void __launch_bounds__(256) fft_product_pass(PassArgs<C> a) {
     dft_reg<R2, false, R1>(s0, a.tw);
     dft_reg<R2, false, R1>(s1, a.tw);
     dft_reg<R2, false, R1>(s2, a.tw);
+    const int ky = (int)(l / a.Pz), kz = (int)(l - (long long)ky * a.Pz);
+    const Fold fy = fold(ky, a.Py), fz = fold(kz, a.Pz);
+    const long long yz = (long long)fy.idx * a.Hz + fz.idx;
 #pragma unroll
     for (int k2 = 0; k2 < R2; ++k2) {
-      const long long g = (long long)(k1 + R1 * k2) * a.I + l;
+      const Fold fx = fold(k1 + R1 * k2, L);
+      const long long g = (long long)fx.idx * a.Hy * a.Hz + yz;
       const C gxx = a.spec[g], gyy = a.spec[a.spec_comp + g], gzz = a.spec[2 * a.spec_comp + g];
-      const C gxy = a.spec[3 * a.spec_comp + g], gxz = a.spec[4 * a.spec_comp + g], gyz = a.spec[5 * a.spec_comp + g];
+      const C gxy = cscale(a.spec[3 * a.spec_comp + g], fx.sgn * fy.sgn);
+      const C gxz = cscale(a.spec[4 * a.spec_comp + g], fx.sgn * fz.sgn);
+      const C gyz = cscale(a.spec[5 * a.spec_comp + g], fy.sgn * fz.sgn);
       const C x0 = s0[k2], x1 = s1[k2], x2 = s2[k2];
       s0[k2] = cadd(cadd(cmul(gxx, x0), cmul(gxy, x1)), cmul(gxz, x2));
       s1[k2] = cadd(cadd(cmul(gxy, x0), cmul(gyy, x1)), cmul(gyz, x2));

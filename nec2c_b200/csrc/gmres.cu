@@ -37,15 +37,24 @@ struct GmState {
   int flag;            // non-finite raised by a kernel
   int barrier_error;   // grid barrier gave up (never expected under cooperative launch)
   long long iterations, max_iterations;
-  double target, before_sq, residual_sq;
+  double target, before_sq, residual_sq, after;
+  int normalize;       // CGS2 step produced v_{j+1}
   unsigned int bar_count, bar_gen;
 };
+
+// Scratch layout of GmBuffers::partials (doubles): [0, 4096) norm partials,
+// [4096, 4096 + 2*1024*32) per-block partials of the Arnoldi kernels, then a
+// few device scalars.
+constexpr long long PART_BLOCKS = 4096;
+constexpr long long PART_SCALARS = 4096 + 2 * 1024 * 32;
+constexpr long long PART_TOTAL = PART_SCALARS + 64;
 
 struct GmBuffers {
   GmState *st;
   double2 *H, *g, *sn, *y;   // (m+1) x m Hessenberg (row-major), rotations, solution
   double *cs;
   double2 *V, *w, *r, *tmp;  // basis (m+1) x n, work vectors
+  double2 *cgs_h;            // 2 x MAXM: CGS2 pass coefficients
   double *partials;          // 2 x grid partials
   unsigned int *ticket;
 };
@@ -123,27 +132,48 @@ __global__ void __launch_bounds__(512) arnoldi_kernel(GmBuffers b, long long n, 
     const long long i = base + e * stride;
     w[e] = i < n ? b.w[i] : make_double2(0, 0);
   }
-  double2 *part[2] = {(double2 *)(b.partials + 4096), (double2 *)(b.partials + 4096) + gridDim.x};
+  double2 *part[2] = {(double2 *)(b.partials + PART_BLOCKS), (double2 *)(b.partials + PART_BLOCKS) + gridDim.x};
   int buf = 0;
-  for (int pass = 0; pass < 2; ++pass) {
-    for (int k = 0; k <= j; ++k) {
-      const double2 *vk = b.V + (long long)k * n;
-      double2 acc = make_double2(0, 0);
+  // vk holds the basis vector of the current step; vn prefetches the next one
+  // while the block waits at the grid barrier.
+  double2 vk[E], vn[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const long long i = base + e * stride;
+    vk[e] = i < n ? b.V[i] : make_double2(0, 0);
+  }
+  const int steps = 2 * (j + 1);
+  for (int s = 0; s < steps; ++s) {
+    const int k = s % (j + 1);
+    double2 acc = make_double2(0, 0);
+#pragma unroll
+    for (int e = 0; e < E; ++e) acc = cadd(acc, cconjmul(vk[e], w[e]));
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) part[buf][blockIdx.x] = acc;
+    const int kn = (s + 1) % (j + 1);
+    if (E <= 8 && s + 1 < steps) {
+      const double2 *vnext = b.V + (long long)kn * n;
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const long long i = base + e * stride;
-        if (i < n) acc = cadd(acc, cconjmul(vk[i], w[e]));
+        vn[e] = i < n ? vnext[i] : make_double2(0, 0);
       }
-      acc = block_sum(acc);
-      if (threadIdx.x == 0) part[buf][blockIdx.x] = acc;
-      if (!grid_barrier(st)) return;
-      const double2 proj = sum_partials(part[buf]);
-      buf ^= 1;
-      if (blockIdx.x == 0 && threadIdx.x == 0) b.H[(long long)k * m + j] = cadd(b.H[(long long)k * m + j], proj);
+    }
+    if (!grid_barrier(st)) return;
+    const double2 proj = sum_partials(part[buf]);
+    buf ^= 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) b.H[(long long)k * m + j] = cadd(b.H[(long long)k * m + j], proj);
+#pragma unroll
+    for (int e = 0; e < E; ++e) w[e] = csub(w[e], cmul(proj, vk[e]));
+    if (E <= 8) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) vk[e] = vn[e];
+    } else if (s + 1 < steps) {
+      const double2 *vnext = b.V + (long long)kn * n;
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const long long i = base + e * stride;
-        if (i < n) w[e] = csub(w[e], cmul(proj, vk[i]));
+        vk[e] = i < n ? vnext[i] : make_double2(0, 0);
       }
     }
   }
@@ -189,6 +219,168 @@ __global__ void __launch_bounds__(512) arnoldi_kernel(GmBuffers b, long long n, 
   st->breakdown = broke;
   if (broke || cabs_(b.g[j + 1]) <= st->target || j + 1 >= m || st->iterations >= st->max_iterations)
     st->active = 0;
+}
+
+// ---------------------------------------------------------------- CGS2
+// Classical Gram-Schmidt applied twice, in three sweeps over the basis with
+// kernel boundaries as the only grid synchronisation (mixed form):
+//   sweep 1: h1 = V^H w
+//   sweep 2: w -= V h1,  h2 = V^H w       (H column += h1 + h2)
+//   sweep 3: w -= V h2,  ||w||^2, then the Givens update of column j
+// Layout: warp q of a 1024-thread block streams basis vector k = q % kk over
+// element group q / kk (coalesced 512 B rows, 4 elements per lane); the block's
+// w chunk lives in shared memory; the update sums the per-k contributions in
+// k order, so every sweep reads V once and results are deterministic.
+constexpr int MAXM = 30;   // restarts up to MAXM use the CGS2 path
+constexpr int CGS_E = 4;   // elements per lane
+constexpr int CGS_GROUP = 32 * CGS_E;   // elements per warp group
+
+template <int MODE>
+__global__ void __launch_bounds__(1024) cgs_sweep_kernel(GmBuffers b, long long n, int m, int j) {
+  GmState *st = b.st;
+  if (!st->active) return;
+  if (MODE == 1 && st->flag) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) { st->status = ST_NONFINITE; st->active = 0; }
+    return;
+  }
+  const int kk = j + 1;
+  const int groups = 32 / kk;                    // element groups per block (>= 1)
+  const int chunk = groups * CGS_GROUP;          // elements per block iteration
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int k = warp % kk, grp = warp / kk;
+  const bool active = grp < groups;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2 *sw = reinterpret_cast<double2 *>(smem_raw);          // [chunk]
+  double2 *contrib = sw + 32 * CGS_GROUP;                        // [kk][chunk]
+  __shared__ double2 hs[MAXM];
+  if (MODE >= 2 && threadIdx.x < kk) hs[threadIdx.x] = b.cgs_h[(MODE == 3 ? MAXM : 0) + threadIdx.x];
+  double2 acc = make_double2(0, 0);
+  double sq = 0;
+  for (long long base = (long long)blockIdx.x * chunk; base < n; base += (long long)gridDim.x * chunk) {
+    for (int t = threadIdx.x; t < chunk; t += blockDim.x)
+      sw[t] = base + t < n ? b.w[base + t] : make_double2(0, 0);
+    double2 v[CGS_E];
+    if (active) {
+      const double2 *vk = b.V + (long long)k * n;
+#pragma unroll
+      for (int e = 0; e < CGS_E; ++e) {
+        const long long i = base + grp * CGS_GROUP + lane + 32 * e;
+        v[e] = i < n ? vk[i] : make_double2(0, 0);
+      }
+    }
+    __syncthreads();
+    if (MODE >= 2) {
+      if (active) {
+        const double2 h = hs[k];
+#pragma unroll
+        for (int e = 0; e < CGS_E; ++e) contrib[k * chunk + grp * CGS_GROUP + lane + 32 * e] = cmul(h, v[e]);
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < chunk; t += blockDim.x) {
+        double2 wi = sw[t];
+        for (int q = 0; q < kk; ++q) wi = csub(wi, contrib[q * chunk + t]);
+        sw[t] = wi;
+        if (base + t < n) {
+          b.w[base + t] = wi;
+          if (MODE == 3) sq += wi.x * wi.x + wi.y * wi.y;
+        }
+      }
+      __syncthreads();
+    }
+    if (MODE <= 2 && active) {
+#pragma unroll
+      for (int e = 0; e < CGS_E; ++e) acc = cadd(acc, cconjmul(v[e], sw[grp * CGS_GROUP + lane + 32 * e]));
+    }
+    __syncthreads();
+  }
+  // Per-block partials: [block][MAXM] (index k; the norm uses slot 0).
+  double2 *parts = (double2 *)(b.partials + PART_BLOCKS);
+  __shared__ double2 red[32];
+  if (MODE <= 2) {
+    for (int o = 16; o > 0; o >>= 1) {
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+    }
+    if (lane == 0) red[warp] = active ? acc : make_double2(0, 0);
+    __syncthreads();
+    if (threadIdx.x < kk) {
+      double2 t = make_double2(0, 0);
+      for (int g = 0; g < groups; ++g) t = cadd(t, red[g * kk + threadIdx.x]);
+      parts[(long long)blockIdx.x * MAXM + threadIdx.x] = t;
+    }
+  } else {
+    const double2 t = block_sum(make_double2(sq, 0));
+    if (threadIdx.x == 0) parts[(long long)blockIdx.x * MAXM] = t;
+  }
+  if (!last_block_done(b.ticket)) return;
+  // Last block: warp q sums slot q over the blocks in a fixed order.
+  __shared__ double2 tot[32];
+  const int nv = MODE == 3 ? 1 : kk;
+  if (warp < nv) {
+    double2 t = make_double2(0, 0);
+    for (unsigned bl = lane; bl < gridDim.x; bl += 32) t = cadd(t, parts[(long long)bl * MAXM + warp]);
+    for (int o = 16; o > 0; o >>= 1) {
+      t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
+      t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
+    }
+    if (lane == 0) tot[warp] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  *b.ticket = 0;
+  double2 *H = b.H;
+  if (MODE <= 2) {
+    // MODE 1 stores h1 (applied by sweep 2); MODE 2 stores h2 (applied by
+    // sweep 3).  The Hessenberg column accumulates both passes.
+    for (int q = 0; q < kk; ++q) {
+      b.cgs_h[(MODE == 1 ? 0 : MAXM) + q] = tot[q];
+      H[(long long)q * m + j] = cadd(H[(long long)q * m + j], tot[q]);
+    }
+    return;
+  }
+  const double after = sqrt(tot[0].x);
+  const double before = sqrt(st->before_sq);
+  const bool broke = after <= 32 * DBL_EPSILON * before;
+  st->after = after;
+  if (!isfinite(after)) { st->status = ST_NONFINITE; st->active = 0; return; }
+  H[(long long)(j + 1) * m + j] = make_double2(after, 0);
+  for (int q = 0; q < j; ++q) {
+    const double2 h0 = H[(long long)q * m + j], h1 = H[(long long)(q + 1) * m + j];
+    const double2 s = b.sn[q];
+    H[(long long)q * m + j] = cadd(cscale(h0, b.cs[q]), cmul(s, h1));
+    H[(long long)(q + 1) * m + j] = csub(cscale(h1, b.cs[q]), cconjmul(s, h0));
+  }
+  double c;
+  double2 s;
+  givens(H[(long long)j * m + j], H[(long long)(j + 1) * m + j], &c, &s);
+  b.cs[j] = c; b.sn[j] = s;
+  H[(long long)j * m + j] = cadd(cscale(H[(long long)j * m + j], c), cmul(s, H[(long long)(j + 1) * m + j]));
+  H[(long long)(j + 1) * m + j] = make_double2(0, 0);
+  const double2 gj = b.g[j];
+  b.g[j + 1] = make_double2(-(s.x * gj.x + s.y * gj.y), -(s.x * gj.y - s.y * gj.x));
+  b.g[j] = cscale(gj, c);
+  st->iterations += 1;
+  st->used = j + 1;
+  st->breakdown = broke;
+  st->normalize = !broke;
+  if (broke || cabs_(b.g[j + 1]) <= st->target || j + 1 >= m || st->iterations >= st->max_iterations)
+    st->active = 0;
+}
+
+// Dynamic shared memory of a CGS2 sweep: the w chunk plus the kk x chunk
+// contributions (kk * chunk <= 32 groups of CGS_GROUP elements).
+constexpr size_t CGS_SMEM = (size_t)(2 * 32 * CGS_GROUP) * sizeof(double2);
+
+// v_{j+1} = w / ||w|| after a CGS2 step (skipped on breakdown and once the
+// cycle has ended: only v_0..v_{used-1} enter the update).
+__global__ void normalize_kernel(GmBuffers b, long long n, int j) {
+  GmState *st = b.st;
+  if (!st->active || !st->normalize) return;
+  const double inv = st->after;
+  double2 *vn = b.V + (long long)(j + 1) * n;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    vn[i] = make_double2(b.w[i].x / inv, b.w[i].y / inv);
 }
 
 // v_0 = r / beta and the Hessenberg / rotation reset for a new cycle.
@@ -244,7 +436,9 @@ struct OpView {
   void *op;
   long long n;
   const double2 *pdiag;
+  int mixed;          // FP32 transforms: Arnoldi by CGS2 sweeps
 };
+n2d_vie *n2c_hybrid_volume(const n2d_hybrid *h);
 
 // Arnoldi products use the operator's transform precision; the true residual
 // at every restart is always FP64 (full_precision).
@@ -266,6 +460,8 @@ static int launch_arnoldi(GmBuffers &b, long long n, int m, int j, int blocks, i
 
 typedef int (*ArnoldiLauncher)(GmBuffers &, long long, int, int, int, int);
 
+// Among the co-resident shapes (E elements of w per thread, 256 or 512
+// threads) pick the one that spreads w over the most SMs, then the smaller E.
 static int arnoldi_shape(long long n, int *blocks, int *threads, ArnoldiLauncher *fn) {
   static const int Es[] = {1, 2, 4, 8, 16};
   static const ArnoldiLauncher fns[] = {launch_arnoldi<1>, launch_arnoldi<2>, launch_arnoldi<4>,
@@ -274,25 +470,28 @@ static int arnoldi_shape(long long n, int *blocks, int *threads, ArnoldiLauncher
                                (void *)arnoldi_kernel<4>, (void *)arnoldi_kernel<8>,
                                (void *)arnoldi_kernel<16>};
   const int sms = n2c_sm_count();
-  for (int q = 0; q < 5; ++q) {
-    int occ = 0;
-    const int th = 512;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern[q], th, 0) != cudaSuccess || occ < 1)
-      continue;
-    if (occ > 2) occ = 2;
-    long long cap = (long long)sms * occ * th * Es[q];
-    // Small systems: fewer blocks keep the barrier cheap.
-    if (n <= cap || q == 4) {
-      if (n > cap) { n2c_set_error("GMRES order %lld exceeds the device-resident limit %lld", n, cap); return 0; }
-      long long need = (n + (long long)th * Es[q] - 1) / ((long long)th * Es[q]);
-      int bl = (int)(need < (long long)sms * occ ? need : (long long)sms * occ);
+  long long best_cover = -1;
+  for (int q = 0; q < 5; ++q)
+    for (int th = 256; th <= 512; th *= 2) {
+      int occ = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern[q], th, 0) != cudaSuccess || occ < 1)
+        continue;
+      if (occ > 2) occ = 2;
+      const long long per_block = (long long)th * Es[q];
+      long long bl = (n + per_block - 1) / per_block;
       if (bl < 1) bl = 1;
-      *blocks = bl; *threads = th; *fn = fns[q];
-      return 1;
+      if (bl > (long long)sms * occ) continue;
+      const long long cover = bl < sms ? bl : sms;
+      if (cover > best_cover) {
+        best_cover = cover;
+        *blocks = (int)bl; *threads = th; *fn = fns[q];
+      }
     }
+  if (best_cover < 0) {
+    n2c_set_error("GMRES order %lld exceeds the device-resident Arnoldi limit", n);
+    return 0;
   }
-  n2c_set_error("no cooperative configuration for the Arnoldi kernel");
-  return 0;
+  return 1;
 }
 
 static unsigned grid1(long long n) {
@@ -311,7 +510,17 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
   memset(&b, 0, sizeof(b));
   int blocks = 0, threads = 0;
   ArnoldiLauncher arnoldi = nullptr;
-  if (!arnoldi_shape(n, &blocks, &threads, &arnoldi)) { rep->status = ST_ALLOC; return 0; }
+  const bool use_cgs = o.mixed && m <= MAXM;
+  if (use_cgs) {
+    static bool configured = false;
+    if (!configured) {
+      cudaFuncSetAttribute(cgs_sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
+      cudaFuncSetAttribute(cgs_sweep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
+      cudaFuncSetAttribute(cgs_sweep_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
+      configured = true;
+    }
+  }
+  if (!use_cgs && !arnoldi_shape(n, &blocks, &threads, &arnoldi)) { rep->status = ST_ALLOC; return 0; }
   b.st = (GmState *)n2d_alloc(sizeof(GmState));
   b.H = (double2 *)n2d_alloc((m + 1) * m * sizeof(double2));
   b.g = (double2 *)n2d_alloc((m + 1) * sizeof(double2));
@@ -321,16 +530,18 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
   b.V = (double2 *)n2d_alloc((m + 1) * n * sizeof(double2));
   b.w = (double2 *)n2d_alloc(n * sizeof(double2));
   b.r = (double2 *)n2d_alloc(n * sizeof(double2));
-  b.partials = (double *)n2d_alloc(4 * 4096 * sizeof(double));
+  b.partials = (double *)n2d_alloc(PART_TOTAL * sizeof(double));
+  b.cgs_h = (double2 *)n2d_alloc(2 * MAXM * sizeof(double2));
   b.ticket = (unsigned int *)n2d_alloc(64);
   int ok = 0;
   GmState hs;
   double bnorm = 0, target = 0;
   auto free_all = [&]() {
-    void *bufs[] = {b.st, b.H, b.g, b.sn, b.y, b.cs, b.V, b.w, b.r, b.partials, b.ticket};
+    void *bufs[] = {b.st, b.H, b.g, b.sn, b.y, b.cs, b.V, b.w, b.r, b.partials, b.ticket, b.cgs_h};
     for (void *q : bufs) n2d_free(q);
   };
-  if (!b.st || !b.H || !b.g || !b.sn || !b.y || !b.cs || !b.V || !b.w || !b.r || !b.partials || !b.ticket) {
+  if (!b.st || !b.H || !b.g || !b.sn || !b.y || !b.cs || !b.V || !b.w || !b.r || !b.partials || !b.ticket ||
+      !b.cgs_h) {
     rep->status = ST_ALLOC;
     free_all();
     return 0;
@@ -338,8 +549,8 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
   memset(&hs, 0, sizeof(hs));
   hs.status = ST_RUNNING;
   hs.max_iterations = (long long)maxit;
-  double *dnorm = (double *)b.partials + 3 * 4096;  // two scalars past the partial slots
-  int *dflag = (int *)((double *)b.partials + 3 * 4096 + 8);
+  double *dnorm = b.partials + PART_SCALARS;
+  int *dflag = (int *)(b.partials + PART_SCALARS + 8);
   auto read_state = [&]() { return n2d_download(&hs, b.st, sizeof(hs)); };
   // ||b|| and ||x|| (finite check) before anything else (vie_iterative.c:116-119).
   double norms[2];
@@ -397,7 +608,15 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
       }
       if (!op_apply(o, (const double *)(b.V + (long long)j * n), (double *)b.w, o.pdiag != nullptr,
                     &b.st->before_sq, &b.st->flag, 0)) { launch_fail = true; break; }
-      if (!arnoldi(b, n, (int)m, j, blocks, threads)) { launch_fail = true; break; }
+      if (use_cgs) {
+        const unsigned gb = (unsigned)n2c_sm_count();
+        cgs_sweep_kernel<1><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
+        cgs_sweep_kernel<2><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
+        cgs_sweep_kernel<3><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
+        normalize_kernel<<<grid1(n), 256, 0, n2c_stream()>>>(b, n, j);
+        if (!n2c_check_launch("cgs sweeps")) { launch_fail = true; break; }
+        n2c_count_launch(3);
+      } else if (!arnoldi(b, n, (int)m, j, blocks, threads)) { launch_fail = true; break; }
     }
     n2d_set_gate(nullptr);
     if (launch_fail) { rep->status = ST_CALLBACK; break; }
@@ -423,6 +642,8 @@ static int gmres_setup(int kind, void *op, long long n, OpView *o) {
   o->kind = kind; o->op = op; o->n = n;
   o->pdiag = kind == 0 ? (const double2 *)n2d_vie_diag((n2d_vie *)op)
                        : n2c_hybrid_pdiag((const n2d_hybrid *)op);
+  n2d_vie *vol = kind == 0 ? (n2d_vie *)op : n2c_hybrid_volume((const n2d_hybrid *)op);
+  o->mixed = vol && n2d_vie_fp32(vol);
   return 1;
 }
 

@@ -154,6 +154,7 @@ extern "C" int n2d_hybrid_upload_blocks(n2d_hybrid *h, const double *blocks) {
 int n2c_hybrid_precondition_ok(const n2d_hybrid *h) { return h->precondition_ok; }
 extern "C" int n2d_hybrid_precondition_ok(const n2d_hybrid *h) { return h->precondition_ok; }
 const double2 *n2c_hybrid_pdiag(const n2d_hybrid *h) { return h->pdiag; }
+n2d_vie *n2c_hybrid_volume(const n2d_hybrid *h) { return h->vol; }
 
 extern "C" int n2d_hybrid_apply(n2d_hybrid *h, const double *x, double *y, int precondition_input,
                                 double *norm, int *flag, int full_precision) {

@@ -84,13 +84,15 @@ static int axis_pass(int mode, int L, const C *in, C *out, const C *tw, long lon
 }
 
 template <typename C>
-static int product_pass(int L, const C *in, C *out, const C *tw, const C *spec, long long I,
-                        int nx) {
+static int product_pass(const n2d_vie *p, const C *in, C *out, const C *tw, const C *spec) {
+  const int L = (int)p->P[0], nx = (int)p->S[0];
+  const long long I = p->P[1] * p->P[2];
   PassArgs<C> a;
   memset(&a, 0, sizeof(a));
   a.in = in; a.out = out; a.tw = tw; a.spec = spec;
   a.lines = I; a.I = I; a.A_in = nx; a.A_out = nx; a.n_in = nx; a.n_out = nx;
-  a.comp_in = (long long)nx * I; a.comp_out = (long long)nx * I; a.spec_comp = (long long)L * I;
+  a.comp_in = (long long)nx * I; a.comp_out = (long long)nx * I; a.spec_comp = p->GH;
+  a.Py = (int)p->P[1]; a.Pz = (int)p->P[2]; a.Hy = (int)p->H[1]; a.Hz = (int)p->H[2];
   a.NL = lines_per_tile(L, 3, sizeof(C));
   a.gate = n2c_gate();
   const long long tiles = (a.lines + a.NL - 1) / a.NL;
@@ -326,6 +328,40 @@ __global__ void fill_kernel(FillArgs f) {
   }
 }
 
+// Octant of the full transformed spectrum, scaled: out[s][kx][ky][kz] for
+// k <= P/2 per axis.
+__global__ void compress_kernel(const double2 *__restrict__ full, double2 *__restrict__ oct,
+                                long long Px, long long Py, long long Pz, long long Hx,
+                                long long Hy, long long Hz, double scale) {
+  const long long GH = Hx * Hy * Hz, G = Px * Py * Pz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 6 * GH;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long s = i / GH, r = i - s * GH;
+    const long long kz = r % Hz, ky = (r / Hz) % Hy, kx = r / (Hz * Hy);
+    const double2 v = full[s * G + (kx * Py + ky) * Pz + kz];
+    oct[i] = make_double2(v.x * scale, v.y * scale);
+  }
+}
+
+// Full 6 x G spectrum from the octant (validation read-back).
+__global__ void expand_kernel(const double2 *__restrict__ oct, double2 *__restrict__ full,
+                              long long Px, long long Py, long long Pz, long long Hy, long long Hz,
+                              long long GH) {
+  const long long G = Px * Py * Pz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 6 * G;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long s = i / G, r = i - s * G;
+    const int kz = (int)(r % Pz), ky = (int)((r / Pz) % Py), kx = (int)(r / (Pz * Py));
+    const Fold fx = fold(kx, (int)Px), fy = fold(ky, (int)Py), fz = fold(kz, (int)Pz);
+    double sg = 1;
+    if (s == 3) sg = fx.sgn * fy.sgn;
+    if (s == 4) sg = fx.sgn * fz.sgn;
+    if (s == 5) sg = fy.sgn * fz.sgn;
+    const double2 v = oct[s * GH + ((long long)fx.idx * Hy + fy.idx) * Hz + fz.idx];
+    full[i] = make_double2(sg * v.x, sg * v.y);
+  }
+}
+
 template <typename C>
 __global__ void scale_convert_kernel(const double2 *__restrict__ in, C *__restrict__ out, long long n,
                                      double s) {
@@ -394,8 +430,10 @@ extern "C" int n2d_vie_create(n2d_vie **out, const long long shape[3], const lon
   p->box_cell = (int *)track(p, p->nbox * sizeof(int));
   p->eps = (double2 *)track(p, cells * sizeof(double2));
   p->diag = (double2 *)track(p, 3 * cells * sizeof(double2));
-  p->spec64 = (double2 *)track(p, 6 * p->G * sizeof(double2));
-  p->spec = fp32 ? track(p, 6 * p->G * ce) : (void *)p->spec64;
+  for (int d = 0; d < 3; ++d) p->H[d] = padded[d] / 2 + 1;
+  p->GH = p->H[0] * p->H[1] * p->H[2];
+  p->spec64 = (double2 *)track(p, 6 * p->GH * sizeof(double2));
+  p->spec = fp32 ? track(p, 6 * p->GH * ce) : (void *)p->spec64;
   const size_t we = sizeof(double2);
   p->box = track(p, 3 * p->nbox * we);
   p->t1 = track(p, 3 * p->S[0] * p->S[1] * p->P[2] * we);
@@ -493,26 +531,28 @@ extern "C" int n2d_vie_finish_spectrum(n2d_vie *p) {
   FillArgs f;
   for (int d = 0; d < 3; ++d) { f.P[d] = p->P[d]; f.S[d] = p->S[d]; f.Ss[d] = p->Ss[d]; }
   f.slab_start = p->slab_start; f.row_start = p->row_start; f.table = p->table; f.G = p->G;
-  // The spectrum is built and transformed in FP64, scaled by 1/G in place,
-  // and for mixed plans also rounded into the FP32 copy.
-  double2 *work = p->spec64;
+  // The spectrum is built and transformed in FP64 on a temporary full grid,
+  // then its octant is kept, scaled by 1/G, and for mixed plans also rounded
+  // into the FP32 copy.
+  double2 *work = (double2 *)n2d_alloc(6 * p->G * sizeof(double2));
+  if (!work) return 0;
   f.spec = work;
   fill_kernel<<<grid_for(p->G), 256, 0, n2c_stream()>>>(f);
   int ok = n2c_check_launch("fill_kernel");
   const double2 *tw[3] = {p->tw64[0], p->tw64[1], p->tw64[2]};
   ok = ok && transform_spectrum<double2>(p, work, tw);
-  const double scale = 1.0 / (double)p->G;
   if (ok) {
-    scale_convert_kernel<double2><<<grid_for(6 * p->G), 256, 0, n2c_stream()>>>(
-        work, work, 6 * p->G, scale);
-    ok = n2c_check_launch("scale_convert");
+    compress_kernel<<<grid_for(6 * p->GH), 256, 0, n2c_stream()>>>(
+        work, p->spec64, p->P[0], p->P[1], p->P[2], p->H[0], p->H[1], p->H[2], 1.0 / (double)p->G);
+    ok = n2c_check_launch("compress");
   }
   if (ok && p->fp32) {
-    scale_convert_kernel<float2><<<grid_for(6 * p->G), 256, 0, n2c_stream()>>>(
-        work, (float2 *)p->spec, 6 * p->G, 1.0);
+    scale_convert_kernel<float2><<<grid_for(6 * p->GH), 256, 0, n2c_stream()>>>(
+        p->spec64, (float2 *)p->spec, 6 * p->GH, 1.0);
     ok = n2c_check_launch("scale_convert");
   }
   ok = ok && n2d_sync();
+  n2d_free(work);
   // The offset table is only needed while building.
   n2d_free(p->table); n2d_free(p->table_ok); n2d_free(p->offsets);
   n2d_free(p->slab_start); n2d_free(p->row_start);
@@ -524,7 +564,13 @@ extern "C" int n2d_vie_finish_spectrum(n2d_vie *p) {
 }
 
 extern "C" int n2d_vie_read_spectrum(n2d_vie *p, double *out) {
-  return n2d_download(out, p->spec64, 6 * p->G * sizeof(double2));
+  double2 *full = (double2 *)n2d_alloc(6 * p->G * sizeof(double2));
+  if (!full) return 0;
+  expand_kernel<<<grid_for(6 * p->G), 256, 0, n2c_stream()>>>(p->spec64, full, p->P[0], p->P[1],
+                                                              p->P[2], p->H[1], p->H[2], p->GH);
+  int ok = n2c_check_launch("expand") && n2d_download(out, full, 6 * p->G * sizeof(double2));
+  n2d_free(full);
+  return ok;
 }
 
 extern "C" int n2d_vie_set_eps(n2d_vie *p, const double *eps, const double *self) {
@@ -550,7 +596,7 @@ static int apply_t(n2d_vie *p, const double2 *x, double2 *y, const double2 *diag
   if (!n2c_check_launch("scatter")) return 0;
   if (!axis_pass<C>(0, (int)Pz, box, t1, tw[2], 3 * nx * ny, 1, nz, Pz, (int)nz, (int)Pz)) return 0;
   if (!axis_pass<C>(0, (int)Py, t1, t2, tw[1], 3 * nx, Pz, ny, Py, (int)ny, (int)Py)) return 0;
-  if (!product_pass<C>((int)Px, t2, t2, tw[0], spec, Py * Pz, (int)nx)) return 0;
+  if (!product_pass<C>(p, t2, t2, tw[0], spec)) return 0;
   if (!axis_pass<C>(1, (int)Py, t2, t1, tw[1], 3 * nx, Pz, Py, ny, (int)Py, (int)ny)) return 0;
   if (!axis_pass<C>(1, (int)Pz, t1, box, tw[2], 3 * nx * ny, 1, Pz, nz, (int)Pz, (int)nz)) return 0;
   const long long out_cells = p->mirror ? p->mirror : p->cells;

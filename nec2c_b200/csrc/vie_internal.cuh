@@ -14,8 +14,9 @@ struct n2d_vie {
   double2 *eps;             // [cells]
   double2 *diag;            // [3 cells] eps - (eps-1) self[i]
   double2 self[3];
-  void *spec;               // [6][G] in the plan's transform precision
-  double2 *spec64;          // [6][G] FP64 (== spec for FP64 plans; mixed plans keep
+  long long H[3], GH;       // octant extents P/2+1 and their product
+  void *spec;               // [6][Hx][Hy][Hz] octant of Ghat/G, transform precision
+  double2 *spec64;          // same in FP64 (== spec for FP64 plans; mixed plans keep
                             // both: FP32 for Arnoldi products, FP64 for residuals)
   void *box, *t1, *t2;      // work grids, sized for FP64
   double2 *tw64[3];
