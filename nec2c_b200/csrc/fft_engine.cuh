@@ -81,7 +81,55 @@ template <typename C> struct PassArgs {
   long long comp_in, comp_out;  // product pass: distance between the 3 components
   long long spec_comp;          // product pass: distance between spectrum slots
   int Py, Pz, Hy, Hz;           // product pass: padded y/z extents, octant extents
+  // Cell I/O of the z passes (scatter on the forward load, permittivity
+  // epilogue on the inverse store).  Lines are (component, x, y) of the box.
+  const double2 *cx;            // cell vector x (3 per cell)
+  double2 *cy;                  // cell vector y (3 per cell)
+  const double2 *eps;           // per-cell permittivity
+  const int *box_cell;          // box index -> cell (-1: empty)
+  double2 self0, self1, self2;  // self terms of the Jacobi divisor
+  long long nxy, mirror;        // lines per component; PEC physical cells (0: none)
+  int precondition;             // input is v, the operator acts on v ./ diag
+  int *flag;                    // non-finite input / output
+  double *partials, *norm;      // |y|^2 reduction (norm NULL: none)
+  unsigned int *ticket;
 };
+
+template <typename C> __device__ __forceinline__ double2 jacobi_divisor(const PassArgs<C> &a, double2 e, int c) {
+  const double2 s = c == 0 ? a.self0 : (c == 1 ? a.self1 : a.self2);
+  const double2 em1 = make_double2(e.x - 1.0, e.y);
+  return csub(e, cmul(em1, s));
+}
+
+// Source value of box element e of line l (scatter with the Jacobi divisor
+// and the PEC image sign diag(-1,-1,+1)).
+template <typename C>
+__device__ __forceinline__ C cell_load(const PassArgs<C> &a, long long l, int e) {
+  const long long comp = l / a.nxy, xy = l - comp * a.nxy;
+  long long cell = a.box_cell[xy * a.A_in + e];
+  if (cell < 0) return czero<C>();
+  double sgn = 1;
+  if (a.mirror && cell >= a.mirror) { cell -= a.mirror; if (comp < 2) sgn = -1; }
+  double2 v = a.cx[3 * cell + comp];
+  if (a.precondition) v = cdiv(v, jacobi_divisor(a, a.eps[cell], (int)comp));
+  if (a.flag && !finite2(v)) *a.flag = 1;
+  return from_d<C>(make_double2(sgn * v.x, sgn * v.y));
+}
+
+// Epilogue y = eps z - (eps-1) field of box element e of line l; returns |y|^2.
+template <typename C>
+__device__ __forceinline__ double cell_store(const PassArgs<C> &a, long long l, int e, C field) {
+  const long long comp = l / a.nxy, xy = l - comp * a.nxy;
+  const long long cell = a.box_cell[xy * a.A_out + e];
+  if (cell < 0 || (a.mirror && cell >= a.mirror)) return 0;
+  const double2 ep = a.eps[cell], em1 = make_double2(ep.x - 1.0, ep.y);
+  double2 z = a.cx[3 * cell + comp];
+  if (a.precondition) z = cdiv(z, jacobi_divisor(a, ep, (int)comp));
+  const double2 v = csub(cmul(ep, z), cmul(em1, to_d(field)));
+  a.cy[3 * cell + comp] = v;
+  if (a.flag && !finite2(v)) *a.flag = 1;
+  return v.x * v.x + v.y * v.y;
+}
 
 // The transformed Green tensor is even (xx yy zz) or odd (xy: x,y; xz: x,z;
 // yz: y,z) in every axis, so only the octant k <= P/2 per axis is stored:
@@ -103,8 +151,9 @@ __device__ __forceinline__ void line_base(const PassArgs<C> &a, long long l, lon
   bout = b * a.A_out * a.I + i;
 }
 
-// Forward transform of one component per tile.
-template <typename C, int R1, int R2>
+// Forward transform of one component per tile (CELLS: loads scatter the cell
+// vector, see cell_load).
+template <typename C, int R1, int R2, bool CELLS = false>
 __global__ void __launch_bounds__(256) fft_forward_pass(PassArgs<C> a) {
   if (a.gate && *(volatile const int *)a.gate == 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -121,7 +170,8 @@ __global__ void __launch_bounds__(256) fft_forward_pass(PassArgs<C> a) {
 #pragma unroll
     for (int j1 = 0; j1 < R1; ++j1) {
       const int e = j2 + R2 * j1;
-      v[j1] = e < a.n_in ? a.in[bin + (long long)e * a.I] : czero<C>();
+      if (CELLS) v[j1] = e < a.n_in ? cell_load(a, l, e) : czero<C>();
+      else v[j1] = e < a.n_in ? a.in[bin + (long long)e * a.I] : czero<C>();
     }
     dft_reg<R1, false, R2>(v, a.tw);
 #pragma unroll
@@ -149,14 +199,16 @@ __global__ void __launch_bounds__(256) fft_forward_pass(PassArgs<C> a) {
   }
 }
 
-// Inverse transform (unnormalised) of one component per tile.
-template <typename C, int R1, int R2>
+// Inverse transform (unnormalised) of one component per tile (CELLS: stores
+// run the permittivity epilogue into the cell vector and reduce |y|^2).
+template <typename C, int R1, int R2, bool CELLS = false>
 __global__ void __launch_bounds__(256) fft_inverse_pass(PassArgs<C> a) {
   if (a.gate && *(volatile const int *)a.gate == 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *S = reinterpret_cast<C *>(smem_raw);
   const int NL = a.NL;
   const long long l0 = (long long)blockIdx.x * NL;
+  double sq = 0;
   for (int item = threadIdx.x; item < NL * R1; item += blockDim.x) {
     const int t = item & (NL - 1), k1 = item / NL;
     const long long l = l0 + t;
@@ -190,7 +242,26 @@ __global__ void __launch_bounds__(256) fft_inverse_pass(PassArgs<C> a) {
 #pragma unroll
     for (int n2 = 0; n2 < R1; ++n2) {
       const int e = n1 + R2 * n2;
-      if (e < a.n_out) a.out[bout + (long long)e * a.I] = v[n2];
+      if (e < a.n_out) {
+        if (CELLS) sq += cell_store(a, l, e, v[n2]);
+        else a.out[bout + (long long)e * a.I] = v[n2];
+      }
+    }
+  }
+  if (CELLS && a.norm) {
+    // Deterministic |y|^2: block partials summed by the last block.
+    const double2 bs = block_sum(make_double2(sq, 0));
+    if (threadIdx.x == 0) a.partials[blockIdx.x] = bs.x;
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (last) {
+      double t2 = 0;
+      for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) t2 += a.partials[i];
+      const double2 tot = block_sum(make_double2(t2, 0));
+      if (threadIdx.x == 0) { *a.norm = tot.x; *a.ticket = 0; }
     }
   }
 }

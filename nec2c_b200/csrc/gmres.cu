@@ -256,18 +256,35 @@ __global__ void __launch_bounds__(1024) cgs_sweep_kernel(GmBuffers b, long long 
   if (MODE >= 2 && threadIdx.x < kk) hs[threadIdx.x] = b.cgs_h[(MODE == 3 ? MAXM : 0) + threadIdx.x];
   double2 acc = make_double2(0, 0);
   double sq = 0;
-  for (long long base = (long long)blockIdx.x * chunk; base < n; base += (long long)gridDim.x * chunk) {
-    for (int t = threadIdx.x; t < chunk; t += blockDim.x)
-      sw[t] = base + t < n ? b.w[base + t] : make_double2(0, 0);
-    double2 v[CGS_E];
+  // Software pipeline: the basis rows and w of the next chunk are loaded into
+  // registers while the current chunk is reduced.
+  const long long stride = (long long)gridDim.x * chunk;
+  const int wper = (chunk + blockDim.x - 1) / blockDim.x;    // <= 4
+  double2 v[CGS_E], vn[CGS_E], wv[4], wn[4];
+  auto load = [&](long long base, double2 (&vv)[CGS_E], double2 (&ww)[4]) {
     if (active) {
       const double2 *vk = b.V + (long long)k * n;
 #pragma unroll
       for (int e = 0; e < CGS_E; ++e) {
         const long long i = base + grp * CGS_GROUP + lane + 32 * e;
-        v[e] = i < n ? vk[i] : make_double2(0, 0);
+        vv[e] = i < n ? vk[i] : make_double2(0, 0);
       }
     }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int t = threadIdx.x + q * blockDim.x;
+      ww[q] = (q < wper && t < chunk && base + t < n) ? b.w[base + t] : make_double2(0, 0);
+    }
+  };
+  long long base = (long long)blockIdx.x * chunk;
+  if (base < n) load(base, v, wv);
+  for (; base < n; base += stride) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int t = threadIdx.x + q * blockDim.x;
+      if (q < wper && t < chunk) sw[t] = wv[q];
+    }
+    if (base + stride < n) load(base + stride, vn, wn);
     __syncthreads();
     if (MODE >= 2) {
       if (active) {
@@ -292,6 +309,10 @@ __global__ void __launch_bounds__(1024) cgs_sweep_kernel(GmBuffers b, long long 
       for (int e = 0; e < CGS_E; ++e) acc = cadd(acc, cconjmul(v[e], sw[grp * CGS_GROUP + lane + 32 * e]));
     }
     __syncthreads();
+#pragma unroll
+    for (int e = 0; e < CGS_E; ++e) v[e] = vn[e];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) wv[q] = wn[q];
   }
   // Per-block partials: [block][MAXM] (index k; the norm uses slot 0).
   double2 *parts = (double2 *)(b.partials + PART_BLOCKS);
@@ -500,27 +521,45 @@ static unsigned grid1(long long n) {
   return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
-static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, size_t restart, size_t maxit,
-                      double rtol, double atol, n2d_gmres_report *rep) {
-  const long long n = o.n;
-  long long m = (long long)restart;
-  if (m > n) m = n;
-  if (m > (long long)maxit) m = (long long)maxit;
+// Persistent GMRES workspace of one operator: buffers for (n, m) and the
+// captured CUDA graph of a restart cycle's inner iterations.
+struct GmWork {
+  long long n, m;
+  int mixed;
   GmBuffers b;
-  memset(&b, 0, sizeof(b));
-  int blocks = 0, threads = 0;
-  ArnoldiLauncher arnoldi = nullptr;
+  int blocks, threads;
+  ArnoldiLauncher arnoldi;
+  cudaGraphExec_t inner;      // null: launch the inner loop directly
+  unsigned inner_launches;    // kernels per replay (launch accounting)
+  bool tried_graph;
+};
+
+static void work_free(GmWork *w) {
+  if (!w) return;
+  if (w->inner) cudaGraphExecDestroy(w->inner);
+  GmBuffers &b = w->b;
+  void *bufs[] = {b.st, b.H, b.g, b.sn, b.y, b.cs, b.V, b.w, b.r, b.partials, b.ticket, b.cgs_h};
+  for (void *q : bufs) n2d_free(q);
+  delete w;
+}
+
+void n2c_gmres_work_free(void *w) { work_free((GmWork *)w); }
+void **n2c_vie_gm_slot(n2d_vie *p);
+void **n2c_hybrid_gm_slot(n2d_hybrid *h);
+
+static GmWork *work_get(const OpView &o, long long m) {
+  void **slot = o.kind == 0 ? n2c_vie_gm_slot((n2d_vie *)o.op) : n2c_hybrid_gm_slot((n2d_hybrid *)o.op);
+  GmWork *w = (GmWork *)*slot;
+  if (w && w->n == o.n && w->m == m && w->mixed == o.mixed) return w;
+  work_free(w);
+  *slot = nullptr;
+  const long long n = o.n;
+  w = new GmWork();
+  memset(w, 0, sizeof(*w));
+  w->n = n; w->m = m; w->mixed = o.mixed;
   const bool use_cgs = o.mixed && m <= MAXM;
-  if (use_cgs) {
-    static bool configured = false;
-    if (!configured) {
-      cudaFuncSetAttribute(cgs_sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
-      cudaFuncSetAttribute(cgs_sweep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
-      cudaFuncSetAttribute(cgs_sweep_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
-      configured = true;
-    }
-  }
-  if (!use_cgs && !arnoldi_shape(n, &blocks, &threads, &arnoldi)) { rep->status = ST_ALLOC; return 0; }
+  if (!use_cgs && !arnoldi_shape(n, &w->blocks, &w->threads, &w->arnoldi)) { delete w; return nullptr; }
+  GmBuffers &b = w->b;
   b.st = (GmState *)n2d_alloc(sizeof(GmState));
   b.H = (double2 *)n2d_alloc((m + 1) * m * sizeof(double2));
   b.g = (double2 *)n2d_alloc((m + 1) * sizeof(double2));
@@ -533,19 +572,86 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
   b.partials = (double *)n2d_alloc(PART_TOTAL * sizeof(double));
   b.cgs_h = (double2 *)n2d_alloc(2 * MAXM * sizeof(double2));
   b.ticket = (unsigned int *)n2d_alloc(64);
+  if (!b.st || !b.H || !b.g || !b.sn || !b.y || !b.cs || !b.V || !b.w || !b.r || !b.partials || !b.ticket ||
+      !b.cgs_h || !n2d_memset(b.ticket, 0, 64)) {
+    work_free(w);
+    return nullptr;
+  }
+  *slot = w;
+  return w;
+}
+
+// Enqueues the m gated inner iterations of a cycle on the current stream.
+static int enqueue_inner(const OpView &o, GmWork *w) {
+  GmBuffers &b = w->b;
+  const long long n = w->n, m = w->m;
+  const bool use_cgs = o.mixed && m <= MAXM;
+  n2d_set_gate(&b.st->active);
+  int ok = 1;
+  for (int j = 0; j < m && ok; ++j) {
+    ok = op_apply(o, (const double *)(b.V + (long long)j * n), (double *)b.w, o.pdiag != nullptr,
+                  &b.st->before_sq, &b.st->flag, 0);
+    if (!ok) break;
+    if (use_cgs) {
+      const unsigned gb = (unsigned)n2c_sm_count();
+      cgs_sweep_kernel<1><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
+      cgs_sweep_kernel<2><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
+      cgs_sweep_kernel<3><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
+      normalize_kernel<<<grid1(n), 256, 0, n2c_stream()>>>(b, n, j);
+      ok = n2c_check_launch("cgs sweeps");
+      n2c_count_launch(3);
+    } else {
+      ok = w->arnoldi(b, n, (int)m, j, w->blocks, w->threads);
+    }
+  }
+  n2d_set_gate(nullptr);
+  return ok;
+}
+
+// Captures the inner loop once into a graph (launched on the caller's stream
+// every cycle); falls back to direct launches when capture is unavailable.
+static void try_capture(const OpView &o, GmWork *w) {
+  w->tried_graph = true;
+  static thread_local cudaStream_t cap = nullptr;
+  if (!cap && cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) { cap = nullptr; return; }
+  void *user = n2d_get_stream();
+  const unsigned long long before = n2d_launch_count();
+  n2d_set_stream(cap);
+  cudaGraph_t graph = nullptr;
+  int ok = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) ok = enqueue_inner(o, w);
+  cudaError_t e = cudaStreamEndCapture(cap, &graph);
+  n2d_set_stream(user);
+  if (ok && e == cudaSuccess && graph && cudaGraphInstantiate(&w->inner, graph, 0) == cudaSuccess) {
+    w->inner_launches = (unsigned)(n2d_launch_count() - before);
+  } else {
+    w->inner = nullptr;
+  }
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();
+}
+
+static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, size_t restart, size_t maxit,
+                      double rtol, double atol, n2d_gmres_report *rep) {
+  const long long n = o.n;
+  long long m = (long long)restart;
+  if (m > n) m = n;
+  if (m > (long long)maxit) m = (long long)maxit;
+  if (o.mixed && m <= MAXM) {
+    static bool configured = false;
+    if (!configured) {
+      cudaFuncSetAttribute(cgs_sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
+      cudaFuncSetAttribute(cgs_sweep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
+      cudaFuncSetAttribute(cgs_sweep_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
+      configured = true;
+    }
+  }
+  GmWork *w = work_get(o, m);
+  if (!w) { rep->status = ST_ALLOC; return 0; }
+  GmBuffers &b = w->b;
   int ok = 0;
   GmState hs;
   double bnorm = 0, target = 0;
-  auto free_all = [&]() {
-    void *bufs[] = {b.st, b.H, b.g, b.sn, b.y, b.cs, b.V, b.w, b.r, b.partials, b.ticket, b.cgs_h};
-    for (void *q : bufs) n2d_free(q);
-  };
-  if (!b.st || !b.H || !b.g || !b.sn || !b.y || !b.cs || !b.V || !b.w || !b.r || !b.partials || !b.ticket ||
-      !b.cgs_h) {
-    rep->status = ST_ALLOC;
-    free_all();
-    return 0;
-  }
   memset(&hs, 0, sizeof(hs));
   hs.status = ST_RUNNING;
   hs.max_iterations = (long long)maxit;
@@ -554,20 +660,20 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
   auto read_state = [&]() { return n2d_download(&hs, b.st, sizeof(hs)); };
   // ||b|| and ||x|| (finite check) before anything else (vie_iterative.c:116-119).
   double norms[2];
-  if (!n2d_memset(dflag, 0, sizeof(int)) || !n2d_memset(b.ticket, 0, 64) ||
+  if (!n2d_memset(dflag, 0, sizeof(int)) ||
       !n2c_norm2((const double *)b_dev, n, b.partials, b.ticket, dnorm, dflag) ||
       !n2c_norm2((const double *)x_dev, n, b.partials, b.ticket, dnorm + 1, dflag) ||
-      !n2d_download(norms, dnorm, sizeof(norms))) { rep->status = ST_ALLOC; free_all(); return 0; }
+      !n2d_download(norms, dnorm, sizeof(norms))) { rep->status = ST_ALLOC; return 0; }
   int hflag = 0;
-  if (!n2d_download(&hflag, dflag, sizeof(int))) { free_all(); return 0; }
+  if (!n2d_download(&hflag, dflag, sizeof(int))) return 0;
   bnorm = sqrt(norms[0]);
   target = fmax(atol, rtol * bnorm);
   if (hflag || !isfinite(bnorm) || !isfinite(sqrt(norms[1])) || !isfinite(target)) {
-    rep->status = ST_NONFINITE; free_all(); return 0;
+    rep->status = ST_NONFINITE;
+    return 0;
   }
   hs.target = target;
-  if (!n2d_upload(b.st, &hs, sizeof(hs))) { free_all(); return 0; }
-  // True residual r = b - A x.
+  // True residual r = b - A x (always FP64).
   auto true_residual = [&]() -> int {
     ++rep->operator_applications;
     if (!n2d_memset(dflag, 0, sizeof(int))) return 0;
@@ -582,7 +688,7 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
     if (!isfinite(rep->residual_norm)) { rep->status = ST_NONFINITE; return 0; }
     return 1;
   };
-  if (!true_residual()) { free_all(); return 0; }
+  if (!true_residual()) return 0;
   for (;;) {
     const double beta = rep->residual_norm;
     rep->relative_residual = bnorm > 0 ? beta / bnorm : beta;
@@ -594,31 +700,16 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
     // The state block carries the running iteration count across cycles.
     hs.iterations = (long long)rep->iterations;
     hs.active = 1; hs.used = 0; hs.breakdown = 0; hs.flag = 0; hs.barrier_error = 0;
-    hs.bar_count = 0; hs.bar_gen = 0;
+    hs.bar_count = 0; hs.bar_gen = 0; hs.normalize = 0;
     if (!n2d_upload(b.st, &hs, sizeof(hs))) break;
-    bool launch_fail = false;
-    // Matvec kernels launched under the gate return at once when the cycle
-    // has ended; a one-int readback every 8 iterations stops issuing them.
-    n2d_set_gate(&b.st->active);
-    for (int j = 0; j < m; ++j) {
-      if (j > 0 && (j % 8) == 0) {
-        int act = 0;
-        if (!n2d_download(&act, &b.st->active, sizeof(int))) { launch_fail = true; break; }
-        if (!act) break;
-      }
-      if (!op_apply(o, (const double *)(b.V + (long long)j * n), (double *)b.w, o.pdiag != nullptr,
-                    &b.st->before_sq, &b.st->flag, 0)) { launch_fail = true; break; }
-      if (use_cgs) {
-        const unsigned gb = (unsigned)n2c_sm_count();
-        cgs_sweep_kernel<1><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
-        cgs_sweep_kernel<2><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
-        cgs_sweep_kernel<3><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
-        normalize_kernel<<<grid1(n), 256, 0, n2c_stream()>>>(b, n, j);
-        if (!n2c_check_launch("cgs sweeps")) { launch_fail = true; break; }
-        n2c_count_launch(3);
-      } else if (!arnoldi(b, n, (int)m, j, blocks, threads)) { launch_fail = true; break; }
+    if (!w->tried_graph) try_capture(o, w);
+    bool launch_fail;
+    if (w->inner) {
+      launch_fail = cudaGraphLaunch(w->inner, (cudaStream_t)n2d_get_stream()) != cudaSuccess;
+      n2c_count_launch(w->inner_launches);
+    } else {
+      launch_fail = !enqueue_inner(o, w);
     }
-    n2d_set_gate(nullptr);
     if (launch_fail) { rep->status = ST_CALLBACK; break; }
     backsolve_kernel<<<1, 1, 0, n2c_stream()>>>(b, (int)m);
     if (!n2c_check_launch("backsolve")) break;
@@ -634,7 +725,6 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
     if (hs.breakdown && rep->residual_norm > target) { rep->status = ST_BREAKDOWN; break; }
     if (rep->residual_norm > target && (long long)rep->iterations < (long long)maxit) ++rep->restarts;
   }
-  free_all();
   return ok;
 }
 

@@ -22,7 +22,10 @@ struct n2d_hybrid {
   int precondition_ok;
   double *partials;
   unsigned int *ticket;
+  void *gm_work;     // persistent GMRES workspace (gmres.cu)
 };
+void n2c_gmres_work_free(void *w);
+void **n2c_hybrid_gm_slot(n2d_hybrid *h) { return &h->gm_work; }
 
 // One block per conductor row: y_i = sum_j [C|B]_ij z_j, z = x (or x ./ pdiag).
 __global__ void __launch_bounds__(256) conductor_rows_kernel(const double2 *__restrict__ blocks,
@@ -127,6 +130,7 @@ extern "C" int n2d_hybrid_create(n2d_hybrid **out, n2d_vie *vol, long long c, lo
 
 extern "C" void n2d_hybrid_destroy(n2d_hybrid *h) {
   if (!h) return;
+  n2c_gmres_work_free(h->gm_work);
   n2d_free(h->blocks); n2d_free(h->pdiag); n2d_free(h->partials); n2d_free(h->ticket);
   delete h;
 }

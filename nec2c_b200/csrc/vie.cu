@@ -24,12 +24,16 @@
 using namespace n2c;
 
 // ------------------------------------------------------------ pass dispatch
+// mode 0: forward, 1: inverse, 2: forward x + spectrum product + inverse x,
+// 3: forward with the cell scatter, 4: inverse with the permittivity epilogue.
 template <typename C, int R1, int R2>
 static int launch_pass_rr(int mode, const PassArgs<C> &a, size_t smem, long long tiles) {
-  static bool configured[3] = {false, false, false};
+  static bool configured[5] = {false, false, false, false, false};
   void (*k)(PassArgs<C>) = mode == 0 ? fft_forward_pass<C, R1, R2>
                           : mode == 1 ? fft_inverse_pass<C, R1, R2>
-                                      : fft_product_pass<C, R1, R2>;
+                          : mode == 2 ? fft_product_pass<C, R1, R2>
+                          : mode == 3 ? fft_forward_pass<C, R1, R2, true>
+                                      : fft_inverse_pass<C, R1, R2, true>;
   if (!configured[mode]) {
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess) {
       n2c_set_error("cannot raise shared memory for FFT pass");
@@ -37,6 +41,7 @@ static int launch_pass_rr(int mode, const PassArgs<C> &a, size_t smem, long long
     }
     configured[mode] = true;
   }
+  if (tiles > 0x7fffffffLL) { n2c_set_error("FFT pass grid too large"); return 0; }
   k<<<(unsigned)tiles, 256, smem, n2c_stream()>>>(a);
   return n2c_check_launch("fft pass");
 }
@@ -381,8 +386,12 @@ static unsigned grid_for(long long n, int threads = 256) {
   return (unsigned)b;
 }
 
+void n2c_gmres_work_free(void *w);
+void **n2c_vie_gm_slot(n2d_vie *p) { return &p->gm_work; }
+
 static void free_plan(n2d_vie *p) {
   if (!p) return;
+  n2c_gmres_work_free(p->gm_work);
   void *bufs[] = {p->cell_box, p->box_cell, p->eps, p->diag, p->spec64,
                   p->fp32 ? p->spec : nullptr, p->box, p->t1, p->t2,
                   p->tw64[0], p->tw64[1], p->tw64[2], p->tw32[0], p->tw32[1], p->tw32[2],
@@ -438,7 +447,7 @@ extern "C" int n2d_vie_create(n2d_vie **out, const long long shape[3], const lon
   p->box = track(p, 3 * p->nbox * we);
   p->t1 = track(p, 3 * p->S[0] * p->S[1] * p->P[2] * we);
   p->t2 = track(p, 3 * p->S[0] * p->P[1] * p->P[2] * we);
-  p->partials = (double *)track(p, 4096 * sizeof(double));
+  p->partials = (double *)track(p, 65536 * sizeof(double));
   p->ticket = (unsigned int *)track(p, 64);
   for (int d = 0; d < 3; ++d) {
     p->tw64[d] = (double2 *)track(p, padded[d] * sizeof(double2));
@@ -581,41 +590,61 @@ extern "C" int n2d_vie_set_eps(n2d_vie *p, const double *eps, const double *self
   return n2c_check_launch("eps_kernel") && n2d_sync();
 }
 
+// z passes with the cell vector as input / output: the forward z pass
+// scatters (and preconditions) the cells, the inverse z pass applies
+// y = eps z - (eps-1) field and reduces |y|^2.
 template <typename C>
-static int apply_t(n2d_vie *p, const double2 *x, double2 *y, const double2 *diag, double *norm,
+static int z_cell_pass(int mode, n2d_vie *p, const C *in, C *out, const C *tw, const double2 *x,
+                       double2 *y, int precondition, double *norm, int *flag) {
+  const long long nx = p->S[0], ny = p->S[1], nz = p->S[2], Pz = p->P[2];
+  PassArgs<C> a;
+  memset(&a, 0, sizeof(a));
+  a.in = in; a.out = out; a.tw = tw;
+  a.lines = 3 * nx * ny; a.I = 1;
+  if (mode == 3) { a.A_in = nz; a.A_out = Pz; a.n_in = (int)nz; a.n_out = (int)Pz; }
+  else { a.A_in = Pz; a.A_out = nz; a.n_in = (int)Pz; a.n_out = (int)nz; }
+  a.NL = lines_per_tile((int)Pz, 1, sizeof(C));
+  a.gate = n2c_gate();
+  a.cx = x; a.cy = y; a.eps = p->eps; a.box_cell = p->box_cell;
+  a.self0 = p->self[0]; a.self1 = p->self[1]; a.self2 = p->self[2];
+  a.nxy = nx * ny; a.mirror = p->mirror; a.precondition = precondition;
+  a.flag = flag; a.partials = p->partials; a.ticket = p->ticket; a.norm = norm;
+  const long long tiles = (a.lines + a.NL - 1) / a.NL;
+  if (norm && tiles > 65536) { n2c_set_error("norm reduction grid too large"); return 0; }
+  return launch_pass<C>(mode, (int)Pz, a, (size_t)Pz * a.NL * sizeof(C), tiles);
+}
+
+template <typename C>
+static int apply_t(n2d_vie *p, const double2 *x, double2 *y, int precondition, double *norm,
                    int *flag) {
-  const long long nx = p->S[0], ny = p->S[1], nz = p->S[2];
-  const long long Px = p->P[0], Py = p->P[1], Pz = p->P[2];
+  const long long nx = p->S[0], ny = p->S[1];
+  const long long Py = p->P[1], Pz = p->P[2];
   constexpr bool single = sizeof(C) == sizeof(float2);
-  C *box = (C *)p->box, *t1 = (C *)p->t1, *t2 = (C *)p->t2;
+  C *t1 = (C *)p->t1, *t2 = (C *)p->t2;
   const C *tw[3];
   for (int d = 0; d < 3; ++d) tw[d] = single ? (const C *)p->tw32[d] : (const C *)p->tw64[d];
   const C *spec = single ? (const C *)p->spec : (const C *)p->spec64;
-  scatter_kernel<C><<<grid_for(p->nbox), 256, 0, n2c_stream()>>>(x, diag, p->box_cell, box, p->nbox,
-                                                                 p->mirror, flag, n2c_gate());
-  if (!n2c_check_launch("scatter")) return 0;
-  if (!axis_pass<C>(0, (int)Pz, box, t1, tw[2], 3 * nx * ny, 1, nz, Pz, (int)nz, (int)Pz)) return 0;
-  if (!axis_pass<C>(0, (int)Py, t1, t2, tw[1], 3 * nx, Pz, ny, Py, (int)ny, (int)Py)) return 0;
-  if (!product_pass<C>(p, t2, t2, tw[0], spec)) return 0;
-  if (!axis_pass<C>(1, (int)Py, t2, t1, tw[1], 3 * nx, Pz, Py, ny, (int)Py, (int)ny)) return 0;
-  if (!axis_pass<C>(1, (int)Pz, t1, box, tw[2], 3 * nx * ny, 1, Pz, nz, (int)Pz, (int)nz)) return 0;
-  const long long out_cells = p->mirror ? p->mirror : p->cells;
-  const unsigned gblocks = norm ? (grid_for(out_cells) < 1024 ? grid_for(out_cells) : 1024)
-                                : grid_for(out_cells);
-  gather_kernel<C><<<gblocks, 256, 0, n2c_stream()>>>(x, diag, p->eps, p->cell_box, box, p->nbox,
-                                                      out_cells, y, p->partials, p->ticket, norm,
-                                                      flag, n2c_gate());
-  return n2c_check_launch("gather");
+  return z_cell_pass<C>(3, p, nullptr, t1, tw[2], x, y, precondition, nullptr, flag) &&
+         axis_pass<C>(0, (int)Py, t1, t2, tw[1], 3 * nx, Pz, ny, Py, (int)ny, (int)Py) &&
+         product_pass<C>(p, t2, t2, tw[0], spec) &&
+         axis_pass<C>(1, (int)Py, t2, t1, tw[1], 3 * nx, Pz, Py, ny, (int)Py, (int)ny) &&
+         z_cell_pass<C>(4, p, t1, nullptr, tw[2], x, y, precondition, norm, flag);
 }
 
 extern "C" int n2d_vie_apply(n2d_vie *p, const double *x, double *y, int precondition_input,
                              double *norm, int *flag, int full_precision) {
-  const double2 *diag = precondition_input ? p->diag : nullptr;
-  if (p->fp32 && !full_precision) return apply_t<float2>(p, (const double2 *)x, (double2 *)y, diag, norm, flag);
-  return apply_t<double2>(p, (const double2 *)x, (double2 *)y, diag, norm, flag);
+  if (p->fp32 && !full_precision)
+    return apply_t<float2>(p, (const double2 *)x, (double2 *)y, precondition_input, norm, flag);
+  return apply_t<double2>(p, (const double2 *)x, (double2 *)y, precondition_input, norm, flag);
 }
 
-extern "C" void n2d_vie_set_mirror(n2d_vie *p, long long physical_cells) { p->mirror = physical_cells; }
+extern "C" void n2d_vie_set_mirror(n2d_vie *p, long long physical_cells) {
+  if (p->mirror == physical_cells) return;
+  p->mirror = physical_cells;
+  // A captured GMRES cycle bakes the cell layout into its launches.
+  n2c_gmres_work_free(p->gm_work);
+  p->gm_work = nullptr;
+}
 
 extern "C" int n2d_vie_precondition(n2d_vie *p, const double *x, double *y) {
   const long long n = 3 * (p->mirror ? p->mirror : p->cells);

@@ -27,4 +27,5 @@ struct n2d_vie {
   double *partials;         // reduction scratch
   unsigned int *ticket;
   size_t device_bytes;
+  void *gm_work;            // persistent GMRES workspace (gmres.cu)
 };

@@ -359,6 +359,7 @@ int nec2c_cuda_hybrid_precondition(void *ctx, const nec2c_cuda_complex *x, nec2c
 
 /* ------------------------------------------------------------------- GMRES */
 static int gmres_common(int kind, void *op, size_t n, const void *b, void *x, int device,
+                        double *stage_b, double *stage_x,
                         const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *report)
 {
   nec2c_cuda_gmres_report local;
@@ -377,10 +378,26 @@ static int gmres_common(int kind, void *op, size_t n, const void *b, void *x, in
      (options->relative_tolerance == 0 && options->absolute_tolerance == 0))
     return 0;
   if(options->restart == SIZE_MAX || n > (size_t)LLONG_MAX / 64) { report->status = ST_ALLOC; return 0; }
-  int ok = (device ? n2d_gmres_dev : n2d_gmres)(kind, op, (long long)n, (const double *)b, (double *)x,
-                                                 options->restart, options->maximum_iterations,
-                                                 options->relative_tolerance,
-                                                 options->absolute_tolerance, &r);
+  int ok;
+  if(device || !stage_b) {
+    ok = (device ? n2d_gmres_dev : n2d_gmres)(kind, op, (long long)n, (const double *)b, (double *)x,
+                                              options->restart, options->maximum_iterations,
+                                              options->relative_tolerance,
+                                              options->absolute_tolerance, &r);
+  } else {
+    /* Host vectors through the operator's persistent staging buffers; x is
+       copied back even when the solve fails (vie_iterative.h:51-53). */
+    size_t bytes = n * sizeof(double complex);
+    memset(&r, 0, sizeof(r));
+    r.status = ST_ALLOC;
+    ok = n2d_upload(stage_b, b, bytes) && n2d_upload(stage_x, x, bytes);
+    if(ok) {
+      ok = n2d_gmres_dev(kind, op, (long long)n, stage_b, stage_x, options->restart,
+                         options->maximum_iterations, options->relative_tolerance,
+                         options->absolute_tolerance, &r);
+      if(!n2d_download(x, stage_x, bytes)) ok = 0;
+    }
+  }
   report->status = r.status;
   report->iterations = r.iterations;
   report->operator_applications = r.operator_applications;
@@ -394,14 +411,15 @@ int nec2c_cuda_gmres_plan(nec2c_cuda_vie_plan *p, const nec2c_cuda_complex *b, n
                           const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *report)
 {
   n2d_vie *dev = p ? nec2c_cuda_plan_device(p) : NULL;
-  return gmres_common(0, dev, p ? 3 * p->cells : 0, b, x, 0, options, report);
+  return gmres_common(0, dev, p ? 3 * p->cells : 0, b, x, 0, p ? p->x_dev : NULL, p ? p->y_dev : NULL,
+                      options, report);
 }
 
 int nec2c_cuda_gmres_plan_device(nec2c_cuda_vie_plan *p, const void *b, void *x,
                                  const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *report)
 {
   n2d_vie *dev = p ? nec2c_cuda_plan_device(p) : NULL;
-  return gmres_common(0, dev, p ? 3 * p->cells : 0, b, x, 1, options, report);
+  return gmres_common(0, dev, p ? 3 * p->cells : 0, b, x, 1, NULL, NULL, options, report);
 }
 
 int nec2c_cuda_gmres_hybrid(nec2c_cuda_hybrid *h, const nec2c_cuda_complex *b, nec2c_cuda_complex *x,
@@ -411,7 +429,8 @@ int nec2c_cuda_gmres_hybrid(nec2c_cuda_hybrid *h, const nec2c_cuda_complex *b, n
     if(report) { memset(report, 0, sizeof(*report)); report->status = ST_CALLBACK; }
     return 0;
   }
-  return gmres_common(1, h ? h->dev : NULL, h ? h->c + h->v : 0, b, x, 0, options, report);
+  return gmres_common(1, h ? h->dev : NULL, h ? h->c + h->v : 0, b, x, 0, h ? h->x_dev : NULL,
+                      h ? h->y_dev : NULL, options, report);
 }
 
 int nec2c_cuda_gmres_hybrid_device(nec2c_cuda_hybrid *h, const void *b, void *x,
@@ -421,5 +440,5 @@ int nec2c_cuda_gmres_hybrid_device(nec2c_cuda_hybrid *h, const void *b, void *x,
     if(report) { memset(report, 0, sizeof(*report)); report->status = ST_CALLBACK; }
     return 0;
   }
-  return gmres_common(1, h ? h->dev : NULL, h ? h->c + h->v : 0, b, x, 1, options, report);
+  return gmres_common(1, h ? h->dev : NULL, h ? h->c + h->v : 0, b, x, 1, NULL, NULL, options, report);
 }
