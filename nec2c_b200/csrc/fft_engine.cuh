@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(256) fft_inverse_pass(PassArgs<C> a) {
 // the inverse x-FFT, all on one tile of lines.  Lines are the (ky,kz) points
 // (I = Py*Pz, one line per inner index, B = 1 per component).
 template <typename C, int R1, int R2>
-__global__ void __launch_bounds__(256) fft_product_pass(PassArgs<C> a) {
+__global__ void __launch_bounds__(256, 3) fft_product_pass(PassArgs<C> a) {
   if (a.gate && *(volatile const int *)a.gate == 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *S = reinterpret_cast<C *>(smem_raw);
@@ -356,6 +356,176 @@ __global__ void __launch_bounds__(256) fft_product_pass(PassArgs<C> a) {
     for (int n2 = 0; n2 < R1; ++n2) {
       const int e = n1 + R2 * n2;
       if (e < a.n_out) out[(long long)e * a.I] = v[n2];
+    }
+  }
+}
+
+}  // namespace n2c
+
+namespace n2c {
+
+// ---------------------------------------------------------------- z lines
+// Passes along the contiguous axis.  The tile (NL lines of length L) is
+// staged through shared memory with coalesced cooperative loads and stores,
+// transformed in place with the four-step split using a second buffer, and
+// written back.  Shared layout [slot][line] with a padded row (NL + 1).
+//
+// CELLS: the tile is NP lattice columns (x, y) x 3 components, line
+// t = c * NP + p; loads scatter the cell vector (Jacobi divisor, PEC image
+// sign), stores run the permittivity epilogue and reduce |y|^2.  Cell data are
+// touched three components at a time, so those accesses are contiguous too.
+
+// Forward four-step on shared memory: input natural order in S, output
+// natural order in T.
+template <typename C, int R1, int R2>
+__device__ __forceinline__ void smem_forward(C *S, C *T, int NL, int NLP, const C *__restrict__ tw) {
+  for (int item = threadIdx.x; item < NL * R2; item += blockDim.x) {
+    const int t = item % NL, j2 = item / NL;
+    C v[R1];
+#pragma unroll
+    for (int j1 = 0; j1 < R1; ++j1) v[j1] = S[(j2 + R2 * j1) * NLP + t];
+    dft_reg<R1, false, R2>(v, tw);
+#pragma unroll
+    for (int k1 = 1; k1 < R1; ++k1)
+      if (j2) v[k1] = cmul(v[k1], __ldg(&tw[j2 * k1]));
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) S[(j2 + R2 * k1) * NLP + t] = v[k1];
+  }
+  __syncthreads();
+  for (int item = threadIdx.x; item < NL * R1; item += blockDim.x) {
+    const int t = item % NL, k1 = item / NL;
+    C w[R2];
+#pragma unroll
+    for (int j2 = 0; j2 < R2; ++j2) w[j2] = S[(j2 + R2 * k1) * NLP + t];
+    dft_reg<R2, false, R1>(w, tw);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) T[(k1 + R1 * k2) * NLP + t] = w[k2];
+  }
+  __syncthreads();
+}
+
+// Inverse four-step (unnormalised): input natural order in S, output natural
+// order in S (T is scratch).
+template <typename C, int R1, int R2>
+__device__ __forceinline__ void smem_inverse(C *S, C *T, int NL, int NLP, const C *__restrict__ tw) {
+  for (int item = threadIdx.x; item < NL * R1; item += blockDim.x) {
+    const int t = item % NL, k1 = item / NL;
+    C w[R2];
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) w[k2] = S[(k1 + R1 * k2) * NLP + t];
+    dft_reg<R2, true, R1>(w, tw);
+#pragma unroll
+    for (int n1 = 1; n1 < R2; ++n1)
+      if (k1) w[n1] = cmulc(w[n1], __ldg(&tw[n1 * k1]));
+#pragma unroll
+    for (int n1 = 0; n1 < R2; ++n1) T[(n1 + R2 * k1) * NLP + t] = w[n1];
+  }
+  __syncthreads();
+  for (int item = threadIdx.x; item < NL * R2; item += blockDim.x) {
+    const int t = item % NL, n1 = item / NL;
+    C v[R1];
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) v[k1] = T[(n1 + R2 * k1) * NLP + t];
+    dft_reg<R1, true, R2>(v, tw);
+#pragma unroll
+    for (int n2 = 0; n2 < R1; ++n2) S[(n1 + R2 * n2) * NLP + t] = v[n2];
+  }
+  __syncthreads();
+}
+
+// Global line of tile line t: plain tiles hold lines l0 .. l0+NL-1; cell
+// tiles hold NP lattice columns of all 3 component planes ([3][nxy][L]).
+template <typename C>
+__device__ __forceinline__ long long zline_global(const PassArgs<C> &a, bool cells, int NP, int t) {
+  if (!cells) {
+    const long long l = (long long)blockIdx.x * a.NL + t;
+    return l < a.lines ? l : -1;
+  }
+  const int c = t / NP, p = t - c * NP;
+  const long long pos = (long long)blockIdx.x * NP + p;
+  return pos < a.nxy ? c * a.nxy + pos : -1;
+}
+
+// CELLS: the forward pass loads from the cell vector and stores T1 rows; the
+// inverse pass loads T1 rows and stores through the permittivity epilogue.
+template <typename C, int R1, int R2, bool INV, bool CELLS>
+__global__ void __launch_bounds__(256, 3) fft_zline_pass(PassArgs<C> a) {
+  if (a.gate && *(volatile const int *)a.gate == 0) return;
+  constexpr int L = R1 * R2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int NL = a.NL, NLP = NL + 1;
+  C *S = reinterpret_cast<C *>(smem_raw);
+  C *T = S + (size_t)L * NLP;
+  const int NP = NL / 3;
+  // ---- load
+  if (CELLS && !INV) {
+    const long long p0 = (long long)blockIdx.x * NP;
+    for (int idx = threadIdx.x; idx < NP * L * 3; idx += blockDim.x) {
+      const int c = idx % 3, rest = idx / 3, e = rest % L, p = rest / L;
+      C val = czero<C>();
+      const long long pos = p0 + p;
+      if (e < a.n_in && pos < a.nxy) {
+        long long cell = a.box_cell[pos * a.A_in + e];
+        if (cell >= 0) {
+          double sgn = 1;
+          if (a.mirror && cell >= a.mirror) { cell -= a.mirror; if (c < 2) sgn = -1; }
+          double2 v = a.cx[3 * cell + c];
+          if (a.precondition) v = cdiv(v, jacobi_divisor(a, a.eps[cell], c));
+          if (a.flag && !finite2(v)) *a.flag = 1;
+          val = from_d<C>(make_double2(sgn * v.x, sgn * v.y));
+        }
+      }
+      S[e * NLP + c * NP + p] = val;
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < NL * L; idx += blockDim.x) {
+      const int t = idx / L, e = idx - t * L;
+      const long long l = zline_global(a, CELLS, NP, t);
+      S[e * NLP + t] = (e < a.n_in && l >= 0) ? a.in[l * a.A_in + e] : czero<C>();
+    }
+  }
+  __syncthreads();
+  C *R = S;
+  if (INV) smem_inverse<C, R1, R2>(S, T, NL, NLP, a.tw);
+  else { smem_forward<C, R1, R2>(S, T, NL, NLP, a.tw); R = T; }
+  // ---- store
+  if (CELLS && INV) {
+    double sq = 0;
+    const long long p0 = (long long)blockIdx.x * NP;
+    for (int idx = threadIdx.x; idx < NP * a.n_out * 3; idx += blockDim.x) {
+      const int c = idx % 3, rest = idx / 3, e = rest % a.n_out, p = rest / a.n_out;
+      const long long pos = p0 + p;
+      if (pos >= a.nxy) continue;
+      const long long cell = a.box_cell[pos * a.A_out + e];
+      if (cell < 0 || (a.mirror && cell >= a.mirror)) continue;
+      const double2 ep = a.eps[cell], em1 = make_double2(ep.x - 1.0, ep.y);
+      double2 z = a.cx[3 * cell + c];
+      if (a.precondition) z = cdiv(z, jacobi_divisor(a, ep, c));
+      const double2 v = csub(cmul(ep, z), cmul(em1, to_d(R[e * NLP + c * NP + p])));
+      a.cy[3 * cell + c] = v;
+      if (a.flag && !finite2(v)) *a.flag = 1;
+      sq += v.x * v.x + v.y * v.y;
+    }
+    if (a.norm) {
+      const double2 bs = block_sum(make_double2(sq, 0));
+      if (threadIdx.x == 0) a.partials[blockIdx.x] = bs.x;
+      __shared__ bool last;
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+      __syncthreads();
+      if (last) {
+        double t2 = 0;
+        for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) t2 += a.partials[i];
+        const double2 tot = block_sum(make_double2(t2, 0));
+        if (threadIdx.x == 0) { *a.norm = tot.x; *a.ticket = 0; }
+      }
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < NL * a.n_out; idx += blockDim.x) {
+      const int t = idx / a.n_out, e = idx - t * a.n_out;
+      const long long l = zline_global(a, CELLS, NP, t);
+      if (l >= 0) a.out[l * a.A_out + e] = R[e * NLP + t];
     }
   }
 }

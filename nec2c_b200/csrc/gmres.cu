@@ -38,7 +38,9 @@ struct GmState {
   int barrier_error;   // grid barrier gave up (never expected under cooperative launch)
   long long iterations, max_iterations;
   double target, before_sq, residual_sq, after;
-  int normalize;       // CGS2 step produced v_{j+1}
+  int normalize;       // CGS step produced v_{j+1}
+  int reorth;          // CGS: second pass requested for the current column
+  long long reorth_count;
   unsigned int bar_count, bar_gen;
 };
 
@@ -221,45 +223,76 @@ __global__ void __launch_bounds__(512) arnoldi_kernel(GmBuffers b, long long n, 
     st->active = 0;
 }
 
-// ---------------------------------------------------------------- CGS2
-// Classical Gram-Schmidt applied twice, in three sweeps over the basis with
-// kernel boundaries as the only grid synchronisation (mixed form):
-//   sweep 1: h1 = V^H w
-//   sweep 2: w -= V h1,  h2 = V^H w       (H column += h1 + h2)
-//   sweep 3: w -= V h2,  ||w||^2, then the Givens update of column j
-// Layout: warp q of a 1024-thread block streams basis vector k = q % kk over
-// element group q / kk (coalesced 512 B rows, 4 elements per lane); the block's
-// w chunk lives in shared memory; the update sums the per-k contributions in
-// k order, so every sweep reads V once and results are deterministic.
-constexpr int MAXM = 30;   // restarts up to MAXM use the CGS2 path
-constexpr int CGS_E = 4;   // elements per lane
+// ---------------------------------------------------------------- CGS
+// Classical Gram-Schmidt with selective reorthogonalisation (mixed form):
+//   dots   h = V^H w                          (warp per basis vector)
+//   update w -= V h, ||w||^2                   (thread per element)
+// and a second dots/update pass only when ||w_new|| < ||w|| / sqrt(2) (the
+// Daniel-Gragg-Kaufman-Stewart criterion; "twice is enough").  Both passes
+// add into the Hessenberg column, as the two MGS passes of vie_iterative.c
+// do.  Kernel boundaries are the only grid synchronisation; reductions are
+// fixed-order block partials finished by the last block (deterministic).
+constexpr int MAXM = 30;   // restarts up to MAXM use this path
+constexpr int CGS_E = 4;   // elements per lane in the dots kernel
 constexpr int CGS_GROUP = 32 * CGS_E;   // elements per warp group
+constexpr size_t CGS_SMEM = (size_t)(32 * CGS_GROUP) * sizeof(double2);
 
-template <int MODE>
-__global__ void __launch_bounds__(1024) cgs_sweep_kernel(GmBuffers b, long long n, int m, int j) {
+// Hessenberg column j finished with h_{j+1,j} = after: previous rotations,
+// the new rotation, the residual estimate and the cycle's stop conditions
+// (vie_iterative.c:160-177).
+__device__ void finish_step(GmBuffers &b, GmState *st, int m, int j, double after) {
+  const double before = sqrt(st->before_sq);
+  const bool broke = after <= 32 * DBL_EPSILON * before;
+  st->after = after;
+  st->reorth = 0;
+  if (!isfinite(after)) { st->status = ST_NONFINITE; st->active = 0; return; }
+  double2 *H = b.H;
+  H[(long long)(j + 1) * m + j] = make_double2(after, 0);
+  for (int q = 0; q < j; ++q) {
+    const double2 h0 = H[(long long)q * m + j], h1 = H[(long long)(q + 1) * m + j];
+    const double2 s = b.sn[q];
+    H[(long long)q * m + j] = cadd(cscale(h0, b.cs[q]), cmul(s, h1));
+    H[(long long)(q + 1) * m + j] = csub(cscale(h1, b.cs[q]), cconjmul(s, h0));
+  }
+  double c;
+  double2 s;
+  givens(H[(long long)j * m + j], H[(long long)(j + 1) * m + j], &c, &s);
+  b.cs[j] = c; b.sn[j] = s;
+  H[(long long)j * m + j] = cadd(cscale(H[(long long)j * m + j], c), cmul(s, H[(long long)(j + 1) * m + j]));
+  H[(long long)(j + 1) * m + j] = make_double2(0, 0);
+  const double2 gj = b.g[j];
+  b.g[j + 1] = make_double2(-(s.x * gj.x + s.y * gj.y), -(s.x * gj.y - s.y * gj.x));
+  b.g[j] = cscale(gj, c);
+  st->iterations += 1;
+  st->used = j + 1;
+  st->breakdown = broke;
+  st->normalize = !broke;
+  if (broke || cabs_(b.g[j + 1]) <= st->target || j + 1 >= m || st->iterations >= st->max_iterations)
+    st->active = 0;
+}
+
+// h = V^H w for pass P (0: first, 1: reorthogonalisation, run only when
+// requested).  Warp q of a 1024-thread block handles basis vector q % kk over
+// element group q / kk; the w chunk sits in shared memory.
+template <int P>
+__global__ void __launch_bounds__(1024) cgs_dots_kernel(GmBuffers b, long long n, int m, int j) {
   GmState *st = b.st;
-  if (!st->active) return;
-  if (MODE == 1 && st->flag) {
+  if (!st->active || (P == 1 && !st->reorth)) return;
+  if (P == 0 && st->flag) {
     if (blockIdx.x == 0 && threadIdx.x == 0) { st->status = ST_NONFINITE; st->active = 0; }
     return;
   }
   const int kk = j + 1;
-  const int groups = 32 / kk;                    // element groups per block (>= 1)
-  const int chunk = groups * CGS_GROUP;          // elements per block iteration
+  const int groups = 32 / kk;
+  const int chunk = groups * CGS_GROUP;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int k = warp % kk, grp = warp / kk;
   const bool active = grp < groups;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2 *sw = reinterpret_cast<double2 *>(smem_raw);          // [chunk]
-  double2 *contrib = sw + 32 * CGS_GROUP;                        // [kk][chunk]
-  __shared__ double2 hs[MAXM];
-  if (MODE >= 2 && threadIdx.x < kk) hs[threadIdx.x] = b.cgs_h[(MODE == 3 ? MAXM : 0) + threadIdx.x];
+  double2 *sw = reinterpret_cast<double2 *>(smem_raw);   // [chunk]
   double2 acc = make_double2(0, 0);
-  double sq = 0;
-  // Software pipeline: the basis rows and w of the next chunk are loaded into
-  // registers while the current chunk is reduced.
   const long long stride = (long long)gridDim.x * chunk;
-  const int wper = (chunk + blockDim.x - 1) / blockDim.x;    // <= 4
+  const int wper = (chunk + blockDim.x - 1) / blockDim.x;
   double2 v[CGS_E], vn[CGS_E], wv[4], wn[4];
   auto load = [&](long long base, double2 (&vv)[CGS_E], double2 (&ww)[4]) {
     if (active) {
@@ -286,25 +319,7 @@ __global__ void __launch_bounds__(1024) cgs_sweep_kernel(GmBuffers b, long long 
     }
     if (base + stride < n) load(base + stride, vn, wn);
     __syncthreads();
-    if (MODE >= 2) {
-      if (active) {
-        const double2 h = hs[k];
-#pragma unroll
-        for (int e = 0; e < CGS_E; ++e) contrib[k * chunk + grp * CGS_GROUP + lane + 32 * e] = cmul(h, v[e]);
-      }
-      __syncthreads();
-      for (int t = threadIdx.x; t < chunk; t += blockDim.x) {
-        double2 wi = sw[t];
-        for (int q = 0; q < kk; ++q) wi = csub(wi, contrib[q * chunk + t]);
-        sw[t] = wi;
-        if (base + t < n) {
-          b.w[base + t] = wi;
-          if (MODE == 3) sq += wi.x * wi.x + wi.y * wi.y;
-        }
-      }
-      __syncthreads();
-    }
-    if (MODE <= 2 && active) {
+    if (active) {
 #pragma unroll
       for (int e = 0; e < CGS_E; ++e) acc = cadd(acc, cconjmul(v[e], sw[grp * CGS_GROUP + lane + 32 * e]));
     }
@@ -314,83 +329,71 @@ __global__ void __launch_bounds__(1024) cgs_sweep_kernel(GmBuffers b, long long 
 #pragma unroll
     for (int q = 0; q < 4; ++q) wv[q] = wn[q];
   }
-  // Per-block partials: [block][MAXM] (index k; the norm uses slot 0).
   double2 *parts = (double2 *)(b.partials + PART_BLOCKS);
   __shared__ double2 red[32];
-  if (MODE <= 2) {
-    for (int o = 16; o > 0; o >>= 1) {
-      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
-      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
-    }
-    if (lane == 0) red[warp] = active ? acc : make_double2(0, 0);
-    __syncthreads();
-    if (threadIdx.x < kk) {
-      double2 t = make_double2(0, 0);
-      for (int g = 0; g < groups; ++g) t = cadd(t, red[g * kk + threadIdx.x]);
-      parts[(long long)blockIdx.x * MAXM + threadIdx.x] = t;
-    }
-  } else {
-    const double2 t = block_sum(make_double2(sq, 0));
-    if (threadIdx.x == 0) parts[(long long)blockIdx.x * MAXM] = t;
+  for (int o = 16; o > 0; o >>= 1) {
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+  }
+  if (lane == 0) red[warp] = active ? acc : make_double2(0, 0);
+  __syncthreads();
+  if (threadIdx.x < kk) {
+    double2 t = make_double2(0, 0);
+    for (int g = 0; g < groups; ++g) t = cadd(t, red[g * kk + threadIdx.x]);
+    parts[(long long)blockIdx.x * MAXM + threadIdx.x] = t;
   }
   if (!last_block_done(b.ticket)) return;
   // Last block: warp q sums slot q over the blocks in a fixed order.
-  __shared__ double2 tot[32];
-  const int nv = MODE == 3 ? 1 : kk;
-  if (warp < nv) {
+  if (warp < kk) {
     double2 t = make_double2(0, 0);
     for (unsigned bl = lane; bl < gridDim.x; bl += 32) t = cadd(t, parts[(long long)bl * MAXM + warp]);
     for (int o = 16; o > 0; o >>= 1) {
       t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
       t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
     }
-    if (lane == 0) tot[warp] = t;
-  }
-  __syncthreads();
-  if (threadIdx.x != 0) return;
-  *b.ticket = 0;
-  double2 *H = b.H;
-  if (MODE <= 2) {
-    // MODE 1 stores h1 (applied by sweep 2); MODE 2 stores h2 (applied by
-    // sweep 3).  The Hessenberg column accumulates both passes.
-    for (int q = 0; q < kk; ++q) {
-      b.cgs_h[(MODE == 1 ? 0 : MAXM) + q] = tot[q];
-      H[(long long)q * m + j] = cadd(H[(long long)q * m + j], tot[q]);
+    if (lane == 0) {
+      b.cgs_h[P * MAXM + warp] = t;
+      b.H[(long long)warp * m + j] = cadd(b.H[(long long)warp * m + j], t);
     }
-    return;
   }
-  const double after = sqrt(tot[0].x);
-  const double before = sqrt(st->before_sq);
-  const bool broke = after <= 32 * DBL_EPSILON * before;
-  st->after = after;
-  if (!isfinite(after)) { st->status = ST_NONFINITE; st->active = 0; return; }
-  H[(long long)(j + 1) * m + j] = make_double2(after, 0);
-  for (int q = 0; q < j; ++q) {
-    const double2 h0 = H[(long long)q * m + j], h1 = H[(long long)(q + 1) * m + j];
-    const double2 s = b.sn[q];
-    H[(long long)q * m + j] = cadd(cscale(h0, b.cs[q]), cmul(s, h1));
-    H[(long long)(q + 1) * m + j] = csub(cscale(h1, b.cs[q]), cconjmul(s, h0));
-  }
-  double c;
-  double2 s;
-  givens(H[(long long)j * m + j], H[(long long)(j + 1) * m + j], &c, &s);
-  b.cs[j] = c; b.sn[j] = s;
-  H[(long long)j * m + j] = cadd(cscale(H[(long long)j * m + j], c), cmul(s, H[(long long)(j + 1) * m + j]));
-  H[(long long)(j + 1) * m + j] = make_double2(0, 0);
-  const double2 gj = b.g[j];
-  b.g[j + 1] = make_double2(-(s.x * gj.x + s.y * gj.y), -(s.x * gj.y - s.y * gj.x));
-  b.g[j] = cscale(gj, c);
-  st->iterations += 1;
-  st->used = j + 1;
-  st->breakdown = broke;
-  st->normalize = !broke;
-  if (broke || cabs_(b.g[j + 1]) <= st->target || j + 1 >= m || st->iterations >= st->max_iterations)
-    st->active = 0;
+  if (threadIdx.x == 0) *b.ticket = 0;
 }
 
-// Dynamic shared memory of a CGS2 sweep: the w chunk plus the kk x chunk
-// contributions (kk * chunk <= 32 groups of CGS_GROUP elements).
-constexpr size_t CGS_SMEM = (size_t)(2 * 32 * CGS_GROUP) * sizeof(double2);
+// w -= V h for pass P and ||w||^2 (thread per element); the last block
+// either requests the reorthogonalisation pass or finishes the column.
+template <int P>
+__global__ void __launch_bounds__(256) cgs_update_kernel(GmBuffers b, long long n, int m, int j) {
+  GmState *st = b.st;
+  if (!st->active || (P == 1 && !st->reorth)) return;
+  const int kk = j + 1;
+  __shared__ double2 hs[MAXM];
+  if (threadIdx.x < kk) hs[threadIdx.x] = b.cgs_h[P * MAXM + threadIdx.x];
+  __syncthreads();
+  double sq = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double2 wi = b.w[i];
+#pragma unroll 6
+    for (int k = 0; k < kk; ++k) wi = csub(wi, cmul(hs[k], b.V[(long long)k * n + i]));
+    b.w[i] = wi;
+    sq += wi.x * wi.x + wi.y * wi.y;
+  }
+  const double2 t = block_sum(make_double2(sq, 0));
+  if (threadIdx.x == 0) b.partials[blockIdx.x] = t.x;
+  if (!last_block_done(b.ticket)) return;
+  double tot = 0;
+  for (unsigned bl = threadIdx.x; bl < gridDim.x; bl += blockDim.x) tot += b.partials[bl];
+  const double2 all = block_sum(make_double2(tot, 0));
+  if (threadIdx.x != 0) return;
+  *b.ticket = 0;
+  const double after = sqrt(all.x);
+  if (P == 0 && isfinite(after) && after < sqrt(0.5 * st->before_sq)) {
+    st->reorth = 1;
+    st->reorth_count += 1;
+    return;
+  }
+  finish_step(b, st, m, j, after);
+}
 
 // v_{j+1} = w / ||w|| after a CGS2 step (skipped on breakdown and once the
 // cycle has ended: only v_0..v_{used-1} enter the update).
@@ -594,12 +597,14 @@ static int enqueue_inner(const OpView &o, GmWork *w) {
     if (!ok) break;
     if (use_cgs) {
       const unsigned gb = (unsigned)n2c_sm_count();
-      cgs_sweep_kernel<1><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
-      cgs_sweep_kernel<2><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
-      cgs_sweep_kernel<3><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
+      const unsigned ub = grid1(n) < 4096 ? grid1(n) : 4096;
+      cgs_dots_kernel<0><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
+      cgs_update_kernel<0><<<ub, 256, 0, n2c_stream()>>>(b, n, (int)m, j);
+      cgs_dots_kernel<1><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
+      cgs_update_kernel<1><<<ub, 256, 0, n2c_stream()>>>(b, n, (int)m, j);
       normalize_kernel<<<grid1(n), 256, 0, n2c_stream()>>>(b, n, j);
       ok = n2c_check_launch("cgs sweeps");
-      n2c_count_launch(3);
+      n2c_count_launch(4);
     } else {
       ok = w->arnoldi(b, n, (int)m, j, w->blocks, w->threads);
     }
@@ -640,9 +645,8 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
   if (o.mixed && m <= MAXM) {
     static bool configured = false;
     if (!configured) {
-      cudaFuncSetAttribute(cgs_sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
-      cudaFuncSetAttribute(cgs_sweep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
-      cudaFuncSetAttribute(cgs_sweep_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
+      cudaFuncSetAttribute(cgs_dots_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
+      cudaFuncSetAttribute(cgs_dots_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
       configured = true;
     }
   }
@@ -700,7 +704,7 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
     // The state block carries the running iteration count across cycles.
     hs.iterations = (long long)rep->iterations;
     hs.active = 1; hs.used = 0; hs.breakdown = 0; hs.flag = 0; hs.barrier_error = 0;
-    hs.bar_count = 0; hs.bar_gen = 0; hs.normalize = 0;
+    hs.bar_count = 0; hs.bar_gen = 0; hs.normalize = 0; hs.reorth = 0;
     if (!n2d_upload(b.st, &hs, sizeof(hs))) break;
     if (!w->tried_graph) try_capture(o, w);
     bool launch_fail;

@@ -24,18 +24,23 @@
 using namespace n2c;
 
 // ------------------------------------------------------------ pass dispatch
-// mode 0: forward, 1: inverse, 2: forward x + spectrum product + inverse x,
-// 3: forward with the cell scatter, 4: inverse with the permittivity epilogue.
+// Strided axes (y, x): mode 0 forward, 1 inverse, 2 forward x + spectrum
+// product + inverse x.  Contiguous axis (z), staged through shared memory:
+// mode 5 forward, 6 inverse, 7 forward with the cell scatter, 8 inverse with
+// the permittivity epilogue.
 template <typename C, int R1, int R2>
 static int launch_pass_rr(int mode, const PassArgs<C> &a, size_t smem, long long tiles) {
-  static bool configured[5] = {false, false, false, false, false};
+  static bool configured[9] = {false, false, false, false, false, false, false, false, false};
   void (*k)(PassArgs<C>) = mode == 0 ? fft_forward_pass<C, R1, R2>
                           : mode == 1 ? fft_inverse_pass<C, R1, R2>
                           : mode == 2 ? fft_product_pass<C, R1, R2>
-                          : mode == 3 ? fft_forward_pass<C, R1, R2, true>
-                                      : fft_inverse_pass<C, R1, R2, true>;
+                          : mode == 5 ? fft_zline_pass<C, R1, R2, false, false>
+                          : mode == 6 ? fft_zline_pass<C, R1, R2, true, false>
+                          : mode == 7 ? fft_zline_pass<C, R1, R2, false, true>
+                                      : fft_zline_pass<C, R1, R2, true, true>;
   if (!configured[mode]) {
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess) {
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
+        cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess) {
       n2c_set_error("cannot raise shared memory for FFT pass");
       return 0;
     }
@@ -65,16 +70,25 @@ static int launch_pass(int mode, int L, const PassArgs<C> &a, size_t smem, long 
   return 0;
 }
 
-// Lines per tile: as many as fit a ~96 KB tile (two CTAs per SM), <= 32.
+// Lines per tile: as many as fit a ~48 KB tile (four CTAs per SM), <= 32.
 static int lines_per_tile(int L, int ncomp, size_t elem) {
   size_t per_line = (size_t)L * ncomp * elem;
   int nl = 32;
-  while (nl > 1 && (size_t)nl * per_line > 96 * 1024) nl >>= 1;
+  while (nl > 1 && (size_t)nl * per_line > 48 * 1024) nl >>= 1;
   return nl;
 }
 
 // One axis transform over a batch of lines.  Element e of line (b, i) lives at
 // (b*A + e)*I + i; lines = B*I.
+// Lines per tile of a staged z pass: two padded [L][NL+1] buffers within
+// ~56 KB (three to four blocks per SM); `unit` keeps NL a multiple of 3 for
+// cell tiles.
+static int zlines_per_tile(int L, size_t elem, int unit) {
+  int nl = 32 * unit;
+  while (nl > unit && (size_t)2 * (nl + 1) * L * elem > 56 * 1024) nl -= unit;
+  return nl;
+}
+
 template <typename C>
 static int axis_pass(int mode, int L, const C *in, C *out, const C *tw, long long B, long long I,
                      long long A_in, long long A_out, int n_in, int n_out) {
@@ -82,8 +96,13 @@ static int axis_pass(int mode, int L, const C *in, C *out, const C *tw, long lon
   memset(&a, 0, sizeof(a));
   a.in = in; a.out = out; a.tw = tw;
   a.lines = B * I; a.I = I; a.A_in = A_in; a.A_out = A_out; a.n_in = n_in; a.n_out = n_out;
-  a.NL = lines_per_tile(L, 1, sizeof(C));
   a.gate = n2c_gate();
+  if (I == 1) {
+    a.NL = zlines_per_tile(L, sizeof(C), 1);
+    const long long tiles = (a.lines + a.NL - 1) / a.NL;
+    return launch_pass<C>(mode + 5, L, a, (size_t)2 * (a.NL + 1) * L * sizeof(C), tiles);
+  }
+  a.NL = lines_per_tile(L, 1, sizeof(C));
   const long long tiles = (a.lines + a.NL - 1) / a.NL;
   return launch_pass<C>(mode, L, a, (size_t)L * a.NL * sizeof(C), tiles);
 }
@@ -603,15 +622,18 @@ static int z_cell_pass(int mode, n2d_vie *p, const C *in, C *out, const C *tw, c
   a.lines = 3 * nx * ny; a.I = 1;
   if (mode == 3) { a.A_in = nz; a.A_out = Pz; a.n_in = (int)nz; a.n_out = (int)Pz; }
   else { a.A_in = Pz; a.A_out = nz; a.n_in = (int)Pz; a.n_out = (int)nz; }
-  a.NL = lines_per_tile((int)Pz, 1, sizeof(C));
+  a.NL = zlines_per_tile((int)Pz, sizeof(C), 3);
   a.gate = n2c_gate();
   a.cx = x; a.cy = y; a.eps = p->eps; a.box_cell = p->box_cell;
   a.self0 = p->self[0]; a.self1 = p->self[1]; a.self2 = p->self[2];
   a.nxy = nx * ny; a.mirror = p->mirror; a.precondition = precondition;
   a.flag = flag; a.partials = p->partials; a.ticket = p->ticket; a.norm = norm;
-  const long long tiles = (a.lines + a.NL - 1) / a.NL;
+  const int NP = a.NL / 3;
+  const long long tiles = (a.nxy + NP - 1) / NP;
   if (norm && tiles > 65536) { n2c_set_error("norm reduction grid too large"); return 0; }
-  return launch_pass<C>(mode, (int)Pz, a, (size_t)Pz * a.NL * sizeof(C), tiles);
+  // Cell tiles take T1 rows of 3 components: T1 is [3][nx*ny][Pz], so the
+  // component planes are addressed through lines = comp * nxy + pos.
+  return launch_pass<C>(mode == 3 ? 7 : 8, (int)Pz, a, (size_t)2 * (a.NL + 1) * Pz * sizeof(C), tiles);
 }
 
 template <typename C>
