@@ -143,10 +143,11 @@ int nec2c_cuda_gmres_hybrid_device(nec2c_cuda_hybrid *system, const void *b_dev,
 int nec2c_cuda_dense_backend_set(const char *name);
 const char *nec2c_cuda_dense_backend_name(void);
 /* Replaces dense_backend_factor_classic (dense_backend.h:22-23), called by
-   factr (matrix.c:1318): factors NEC's transposed storage in place.  The
-   factors are the column-major LU of the algebraic matrix with 1-based pivots
-   (the builtin factr's pivot rule); L follows the getrf row convention.  Only
-   this backend's solves consume them.  Returns 1, or 0 when singular/failed. */
+   factr (matrix.c:1318): factors NEC's transposed storage in place.  That
+   storage is the algebraic matrix row-major; the factors are its LU in the
+   same layout with 1-based pivots chosen by the builtin factr's rule (largest
+   |.|^2, later row on ties), L in the getrf row convention.  Only this
+   backend's solves consume them.  Returns 1, or 0 when singular/failed. */
 int nec2c_cuda_dense_factor_classic(size_t order, nec2c_cuda_complex *matrix,
                                     size_t leading_dimension, int *pivots);
 /* Replaces dense_backend_solve_classic(_many) (dense_backend.h:24-32), called by

@@ -51,13 +51,96 @@ extern "C" void *n2d_alloc(size_t bytes) {
   return p;
 }
 extern "C" void n2d_free(void *p) { if (p) cudaFree(p); }
+// ------------------------------------------------------------- host copies
+// Pageable host memory above STAGE_MIN bytes moves through two pinned staging
+// buffers so that the host memcpy of one chunk overlaps the DMA of the other.
+// Pinned (page-locked or registered) host memory is copied directly.
+static const size_t STAGE_CHUNK = 8u << 20, STAGE_MIN = 1u << 20;
+struct Stage {
+  void *buf[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  bool ok = false;
+};
+static thread_local Stage g_stage;
+
+static bool stage_ready() {
+  Stage &s = g_stage;
+  if (s.ok) return true;
+  for (int i = 0; i < 2; ++i) {
+    if (cudaHostAlloc(&s.buf[i], STAGE_CHUNK, cudaHostAllocDefault) != cudaSuccess) { cudaGetLastError(); return false; }
+    if (cudaEventCreateWithFlags(&s.ev[i], cudaEventDisableTiming) != cudaSuccess) { cudaGetLastError(); return false; }
+  }
+  s.ok = true;
+  return true;
+}
+
+static bool is_pinned(const void *p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) { cudaGetLastError(); return false; }
+  return at.type == cudaMemoryTypeHost;
+}
+
+// Rows of `width` bytes: host rows at pitch hp, device rows at pitch dp.
+static int staged_h2d(void *dst, size_t dp, const void *src, size_t hp, size_t width, size_t rows) {
+  Stage &s = g_stage;
+  const size_t per = STAGE_CHUNK / width;         // rows per chunk (>= 1: width <= chunk)
+  int k = 0;
+  for (size_t r0 = 0; r0 < rows; r0 += per, k ^= 1) {
+    const size_t nr = rows - r0 < per ? rows - r0 : per;
+    N2C_CHECK(cudaEventSynchronize(s.ev[k]));
+    char *b = (char *)s.buf[k];
+    for (size_t r = 0; r < nr; ++r) memcpy(b + r * width, (const char *)src + (r0 + r) * hp, width);
+    N2C_CHECK(cudaMemcpy2DAsync((char *)dst + r0 * dp, dp, b, width, width, nr, cudaMemcpyHostToDevice, g_stream));
+    N2C_CHECK(cudaEventRecord(s.ev[k], g_stream));
+  }
+  return 1;
+}
+
+static int staged_d2h(void *dst, size_t hp, const void *src, size_t dp, size_t width, size_t rows) {
+  Stage &s = g_stage;
+  const size_t per = STAGE_CHUNK / width;
+  const size_t chunks = (rows + per - 1) / per;
+  auto issue = [&](size_t c) -> int {
+    const size_t r0 = c * per, nr = rows - r0 < per ? rows - r0 : per;
+    N2C_CHECK(cudaMemcpy2DAsync(s.buf[c & 1], width, (const char *)src + r0 * dp, dp, width, nr,
+                                cudaMemcpyDeviceToHost, g_stream));
+    N2C_CHECK(cudaEventRecord(s.ev[c & 1], g_stream));
+    return 1;
+  };
+  if (!issue(0)) return 0;
+  for (size_t c = 0; c < chunks; ++c) {
+    if (c + 1 < chunks && !issue(c + 1)) return 0;
+    N2C_CHECK(cudaEventSynchronize(s.ev[c & 1]));
+    const size_t r0 = c * per, nr = rows - r0 < per ? rows - r0 : per;
+    const char *b = (const char *)s.buf[c & 1];
+    for (size_t r = 0; r < nr; ++r) memcpy((char *)dst + (r0 + r) * hp, b + r * width, width);
+  }
+  return 1;
+}
+
 extern "C" int n2d_upload(void *dst, const void *src, size_t bytes) {
   if (!bytes) return 1;
+  if (bytes >= STAGE_MIN && !is_pinned(src) && stage_ready()) {
+    const size_t w = 64 * 1024, rows = bytes / w, tail = bytes - rows * w;
+    if (rows && !staged_h2d(dst, w, src, w, w, rows)) return 0;
+    if (tail) N2C_CHECK(cudaMemcpyAsync((char *)dst + rows * w, (const char *)src + rows * w, tail,
+                                        cudaMemcpyHostToDevice, g_stream));
+    N2C_CHECK(cudaStreamSynchronize(g_stream));   // the caller may reuse src
+    return 1;
+  }
   N2C_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, g_stream));
   return 1;
 }
 extern "C" int n2d_download(void *dst, const void *src, size_t bytes) {
   if (!bytes) return 1;
+  if (bytes >= STAGE_MIN && !is_pinned(dst) && stage_ready()) {
+    const size_t w = 64 * 1024, rows = bytes / w, tail = bytes - rows * w;
+    if (rows && !staged_d2h(dst, w, src, w, w, rows)) return 0;
+    if (tail) N2C_CHECK(cudaMemcpyAsync((char *)dst + rows * w, (const char *)src + rows * w, tail,
+                                        cudaMemcpyDeviceToHost, g_stream));
+    N2C_CHECK(cudaStreamSynchronize(g_stream));
+    return 1;
+  }
   N2C_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, g_stream));
   N2C_CHECK(cudaStreamSynchronize(g_stream));
   return 1;
@@ -76,12 +159,22 @@ extern "C" int n2d_copy_d2d(void *dst, const void *src, size_t bytes) {
 extern "C" int n2d_upload2d(void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
                             size_t rows) {
   if (!width || !rows) return 1;
+  if (width * rows >= STAGE_MIN && width <= STAGE_CHUNK && !is_pinned(src) && stage_ready()) {
+    if (!staged_h2d(dst, dpitch, src, spitch, width, rows)) return 0;
+    N2C_CHECK(cudaStreamSynchronize(g_stream));
+    return 1;
+  }
   N2C_CHECK(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, cudaMemcpyHostToDevice, g_stream));
   return 1;
 }
 extern "C" int n2d_download2d(void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
                               size_t rows) {
   if (!width || !rows) return 1;
+  if (width * rows >= STAGE_MIN && width <= STAGE_CHUNK && !is_pinned(dst) && stage_ready()) {
+    if (!staged_d2h(dst, dpitch, src, spitch, width, rows)) return 0;
+    N2C_CHECK(cudaStreamSynchronize(g_stream));
+    return 1;
+  }
   N2C_CHECK(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, cudaMemcpyDeviceToHost, g_stream));
   N2C_CHECK(cudaStreamSynchronize(g_stream));
   return 1;

@@ -43,18 +43,14 @@ void nec2c_cuda_dense_release(void)
 
 static const size_t CPX = 2 * sizeof(double);
 
-/* Uploads NEC's transposed storage (column-major A^T, leading dim ld) and
-   returns the column-major algebraic matrix A (leading dim order). */
-static double *upload_algebraic(const void *matrix, size_t n, size_t ld)
+/* Uploads NEC's transposed storage (column-major A^T, leading dim ld), which
+   is the algebraic matrix A row-major: the device factors it in that layout
+   (leading dim order). */
+static double *upload_matrix(const void *matrix, size_t n, size_t ld)
 {
-  double *raw = n2d_alloc(n * n * CPX), *a = n2d_alloc(n * n * CPX);
-  if(!raw || !a || !n2d_upload2d(raw, n * CPX, matrix, ld * CPX, n * CPX, n) ||
-     !n2d_transpose(raw, (long long)n, a, (long long)n, (long long)n, (long long)n)) {
-    n2d_free(raw); n2d_free(a);
-    return NULL;
-  }
-  if(!n2d_sync()) { n2d_free(raw); n2d_free(a); return NULL; }
-  n2d_free(raw);
+  double *a = n2d_alloc(n * n * CPX);
+  if(!a) return NULL;
+  if(!n2d_upload2d(a, n * CPX, matrix, ld * CPX, n * CPX, n) || !n2d_sync()) { n2d_free(a); return NULL; }
   return a;
 }
 
@@ -66,7 +62,7 @@ int nec2c_cuda_dense_factor_classic(size_t n, nec2c_cuda_complex *matrix, size_t
   if(!matrix || !pivots || n == 0 || n > INT_MAX || ld < n || ld > INT_MAX) return 0;
   if(!n2d_device_ok()) return 0;
   nec2c_cuda_dense_release();
-  a = upload_algebraic(matrix, n, ld);
+  a = upload_matrix(matrix, n, ld);
   piv = n2d_alloc(n * sizeof(int));
   if(!a || !piv) { n2d_free(a); n2d_free(piv); return 0; }
   if(g_dense_mixed) {
@@ -123,8 +119,8 @@ int nec2c_cuda_dense_solve_row_major(nec2c_cuda_complex *matrix, nec2c_cuda_comp
   int *piv = NULL, info = 0, ok;
   if(!matrix || !rhs || n == 0 || n > INT_MAX) return 0;
   if(!n2d_device_ok()) return 0;
-  /* Row-major A is column-major A^T: the same upload as the classic storage. */
-  a = upload_algebraic(matrix, n, n);
+  /* The row-major system is the classic storage with leading dimension n. */
+  a = upload_matrix(matrix, n, n);
   if(!a) return 0;
   piv = n2d_alloc(n * sizeof(int));
   b = n2d_alloc(n * CPX);

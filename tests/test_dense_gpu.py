@@ -41,7 +41,7 @@ def test_kat():
     assert ok and np.max(np.abs(b - x1)) < 1e-12
 
 
-@pytest.mark.parametrize("n", [1, 2, 31, 32, 33, 100, 257, 700])
+@pytest.mark.parametrize("n", [1, 2, 31, 32, 33, 100, 257, 700, 2500, 4100])
 def test_factor_matches_oracle(n):
     a = mom_like(n, n)
     ld = n + 5
@@ -53,9 +53,13 @@ def test_factor_matches_oracle(n):
     piv_o = np.zeros(n, dtype=np.int32)
     assert oracle().oracle_factr(n, ptr(st_o), ptr(piv_o), ld)
     assert np.array_equal(piv, piv_o)
-    U = np.triu(st[:n, :n])
+    # Ours: the LU row-major in NEC's storage (the Fortran view is its
+    # transpose); the oracle's factr output is the column-major LU.
+    U = np.triu(st[:n, :n].T)
     U_o = np.triu(st_o[:n, :n])
-    assert np.max(np.abs(U - U_o)) / np.max(np.abs(U_o)) < 1e-12
+    # Blocked and column-by-column elimination sum in different orders; the
+    # rounding difference grows with the order.
+    assert np.max(np.abs(U - U_o)) / np.max(np.abs(U_o)) < max(1e-12, 2e-15 * n)
     rng = np.random.default_rng(1000 + n)
     x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
     b = a @ x
