@@ -167,6 +167,22 @@ int nec2c_cuda_dense_solve_row_major(nec2c_cuda_complex *matrix, nec2c_cuda_comp
                                      size_t order);
 /* Drops the device copies kept between a factor and its solves. */
 void nec2c_cuda_dense_release(void);
+/* No counterpart in the reference.  The classic factor above, for callers that
+   must not allocate device memory during the call (a process whose GPU memory
+   belongs to its own pool allocator, or a loop that cannot absorb cudaMalloc's
+   device synchronisation).  matrix_dev and pivots_dev are device pointers the
+   caller owns: NEC's storage (the algebraic matrix row-major, leading
+   dimension >= order) factored in place with the same pivots and factors as
+   nec2c_cuda_dense_factor_classic, and 1-based pivots written to pivots_dev.
+   The work runs on this thread's stream and the call returns when it is done.
+   Scratch is one 4 MiB array inside the library that each GPU using it holds
+   until exit; calls that overlap on the GPU share it and race.  The first
+   call on a device looks up that array's address, so make it before any
+   stream capture.  Orders above NEC2C_CUDA_STATIC_LU_MAX_ORDER are rejected.
+   Returns 1, or 0 when singular, too large or failed. */
+#define NEC2C_CUDA_STATIC_LU_MAX_ORDER 4096
+int nec2c_cuda_dense_factor_device_static(size_t order, nec2c_cuda_complex *matrix_dev,
+                                          size_t leading_dimension, int *pivots_dev);
 
 #ifdef __cplusplus
 }

@@ -636,3 +636,124 @@ extern "C" int n2d_lu_solve(const double *a_dev, long long n, long long ld, cons
                                                              (double2 *)b_dev, ldb);
   return n2c_check_launch("lu_solve");
 }
+
+// ------------------------------------------------------ allocation-free factor
+// A variant of the classic factor for callers that cannot allocate device
+// memory when they call in: a host application that hands the GPU's memory to
+// its own pool allocator at start-up and forbids allocation afterwards, a
+// plug-in living inside such a process, or a loop with a latency budget that
+// cudaMalloc's implicit device synchronisation would break.  The caller passes
+// the matrix and the pivot array already resident on the device; the panel
+// status, the interchange pairs and the row buffer of the interchanges live in
+// one array defined in this file instead of being allocated per call.
+//
+// That array is a module global: every GPU on which the library is loaded
+// holds it (4 MiB + 1 KiB) until the process exits, and every call on that
+// GPU shares it.  Calls whose work overlaps on the GPU (two streams, two host
+// threads) therefore race on it; callers serialise them.  The array keeps the
+// previous call's contents; only the panel status needs to start at zero and
+// is cleared at the start of every call.
+//
+// Set-up: the first call on a device, with that device current, looks up the
+// array's device address (cudaGetSymbolAddress; the array's name in host code
+// is only a stand-in) and keeps it.  Make that first call before any stream
+// capture on the device.
+#include <climits>
+#include <mutex>
+#include "../../include/nec2c_cuda.h"
+
+namespace {
+constexpr size_t STATIC_STATUS_OFF = 0;
+constexpr size_t STATIC_PAIRS_OFF = 256;
+constexpr size_t STATIC_ROWS_OFF = 1024;
+constexpr size_t STATIC_SCRATCH_BYTES =
+    STATIC_ROWS_OFF + (size_t)2 * KB * NEC2C_CUDA_STATIC_LU_MAX_ORDER * sizeof(double2);
+static_assert(sizeof(LuStatus) <= STATIC_PAIRS_OFF - STATIC_STATUS_OFF, "status slot");
+static_assert(4 * KB * sizeof(int) <= STATIC_ROWS_OFF - STATIC_PAIRS_OFF, "pairs slot");
+constexpr int STATIC_MAX_DEVICES = 64;
+std::mutex g_static_lock;
+unsigned char *g_static_addr[STATIC_MAX_DEVICES];
+}  // namespace
+
+static __device__ __align__(256) unsigned char lu_static_scratch[STATIC_SCRATCH_BYTES];
+
+// Device address of the scratch array on the current device (looked up once
+// per device).
+static unsigned char *static_scratch() {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) { n2c_set_error("cudaGetDevice: %s", cudaGetErrorString(e)); return nullptr; }
+  if (dev < 0 || dev >= STATIC_MAX_DEVICES) { n2c_set_error("device %d out of range", dev); return nullptr; }
+  std::lock_guard<std::mutex> hold(g_static_lock);
+  if (!g_static_addr[dev]) {
+    void *ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, lu_static_scratch);
+    if (e != cudaSuccess || !ptr) {
+      n2c_set_error("scratch address on device %d: %s", dev, cudaGetErrorString(e));
+      return nullptr;
+    }
+    g_static_addr[dev] = (unsigned char *)ptr;
+  }
+  return g_static_addr[dev];
+}
+
+extern "C" int nec2c_cuda_dense_factor_device_static(size_t order, nec2c_cuda_complex *matrix_dev,
+                                                     size_t leading_dimension, int *pivots_dev) {
+  if (!matrix_dev || !pivots_dev || order == 0 || leading_dimension < order ||
+      leading_dimension > (size_t)INT_MAX) {
+    n2c_set_error("invalid arguments");
+    return 0;
+  }
+  if (order > NEC2C_CUDA_STATIC_LU_MAX_ORDER) {
+    n2c_set_error("order %zu exceeds the allocation-free factor's maximum of %d", order,
+                  NEC2C_CUDA_STATIC_LU_MAX_ORDER);
+    return 0;
+  }
+  if (!n2d_device_ok()) return 0;
+  unsigned char *base = static_scratch();
+  if (!base) return 0;
+  LuStatus *st = (LuStatus *)(base + STATIC_STATUS_OFF);
+  int *pairs = (int *)(base + STATIC_PAIRS_OFF);
+  double2 *tmp = (double2 *)(base + STATIC_ROWS_OFF);
+  double2 *a = (double2 *)matrix_dev;
+  const long long n = (long long)order, ld = (long long)leading_dimension;
+  cudaStream_t s = n2c_stream();
+  cudaError_t e = cudaMemsetAsync(st, 0, sizeof(LuStatus), s);
+  if (e != cudaSuccess) { n2c_set_error("clearing the panel status: %s", cudaGetErrorString(e)); return 0; }
+  int ok = 1;
+  for (long long k0 = 0; ok && k0 < n; k0 += KB) {
+    const int kb = (int)(n - k0 < KB ? n - k0 : KB);
+    PanelArgs p;
+    memset(&p, 0, sizeof(p));
+    p.a = a; p.n = n; p.ld = ld; p.k0 = k0; p.kb = kb; p.rule = 0; p.ipiv = pivots_dev;
+    p.pairs = pairs; p.st = st;
+    if (n <= (long long)CS * 256) panel_cluster_kernel<256><<<CS, 256, 0, s>>>(p);
+    else panel_cluster_kernel<512><<<CS, 512, 0, s>>>(p);
+    if (!n2c_check_launch("panel")) { ok = 0; break; }
+    if (n > kb) {
+      const unsigned gb = blocks_for(2LL * KB * (n - kb));
+      rows_gather_kernel<<<gb, 256, 0, s>>>(a, n, ld, k0, kb, pairs, st, tmp);
+      rows_scatter_kernel<<<gb, 256, 0, s>>>(a, n, ld, k0, kb, pairs, st, tmp);
+      if (!n2c_check_launch("interchanges")) { ok = 0; break; }
+      n2c_count_launch(1);
+    }
+    const long long right = n - k0 - kb;
+    if (right > 0) {
+      trsm_kernel<<<(unsigned)((right + 127) / 128), 128, 0, s>>>(a, n, ld, k0, kb);
+      if (!n2c_check_launch("trsm")) { ok = 0; break; }
+      dim3 grid((unsigned)((right + GT - 1) / GT), (unsigned)((right + GT - 1) / GT));
+      gemm_update_kernel<<<grid, 256, 0, s>>>(a + (k0 + kb) * ld + (k0 + kb), a + (k0 + kb) * ld + k0,
+                                              a + k0 * ld + (k0 + kb), right, right, kb, ld);
+      if (!n2c_check_launch("gemm_update")) { ok = 0; break; }
+    }
+  }
+  if (!ok) return 0;
+  LuStatus hs;
+  memset(&hs, 0, sizeof(hs));
+  e = cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) { n2c_set_error("reading the panel status: %s", cudaGetErrorString(e)); return 0; }
+  if (hs.error) { n2c_set_error("LU panel barrier time-out"); return 0; }
+  if (hs.info) { n2c_set_error("matrix is singular (pivot %d)", hs.info); return 0; }
+  return 1;
+}

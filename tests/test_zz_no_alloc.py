@@ -1,0 +1,75 @@
+"""Allocation-free dense factor (nec2c_cuda_dense_factor_device_static)
+against the classic factor entry point.
+
+Callers that own all of a GPU's memory through their own pool, or that cannot
+afford cudaMalloc's device synchronisation mid-run, use the allocation-free
+variant; it must give the same pivots and factors as the classic factor
+(within the dense tests' tolerance) on two calls in a row that share the
+library's scratch array.  Named to run last, after every other test has used
+the library; it also passes alone in a fresh process."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import nec2c_b200 as nb
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(n, seed):
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    return a + np.diag(np.full(n, 0.5 * np.sqrt(n)))
+
+
+def _nec_storage(a, ld):
+    n = a.shape[0]
+    st = np.zeros((ld, n), dtype=np.complex128, order="F")
+    st[:n, :n] = a.T
+    return st
+
+
+def _factor_static(st):
+    """Factors a copy of NEC storage st (ld x n, Fortran order) held in device
+    memory the test allocates; returns (ok, factors, pivots)."""
+    import torch
+    ld, n = st.shape
+    # Column j of the Fortran array is row j of the algebraic matrix: the
+    # C-ordered transpose has the same bytes.
+    dev = torch.from_numpy(np.ascontiguousarray(st.T)).cuda()
+    piv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    ok = nb.load().nec2c_cuda_dense_factor_device_static(n, dev.data_ptr(), ld, piv.data_ptr())
+    torch.cuda.synchronize()
+    return bool(ok), dev.cpu().numpy().T, piv.cpu().numpy()
+
+
+def test_static_factor_matches_classic():
+    lib = nb.load()
+    assert nb.dense_backend_set("cuda")
+    lib.nec2c_cuda_set_stream(None)
+    for n, ld, seed in [(700, 703, 7), (2500, 2500, 25)]:
+        a = _system(n, seed)
+        st = _nec_storage(a, ld)
+        ok_s, lu_s, piv_s = _factor_static(st)
+        assert ok_s, lib.nec2c_cuda_last_error()
+        st_c = st.copy(order="F")
+        ok_c, piv_c = nb.factor_classic(st_c)
+        assert ok_c
+        assert np.array_equal(piv_s, piv_c)
+        U_s, U_c = np.triu(lu_s[:n, :n].T), np.triu(st_c[:n, :n].T)
+        L_s, L_c = np.tril(lu_s[:n, :n].T, -1), np.tril(st_c[:n, :n].T, -1)
+        tol = max(1e-12, 2e-15 * n)
+        assert np.max(np.abs(U_s - U_c)) / np.max(np.abs(U_c)) < tol
+        assert np.max(np.abs(L_s - L_c)) < tol
+        # The padding rows of the storage are left as they were.
+        assert np.array_equal(lu_s[n:, :], st[n:, :])
+
+
+def test_static_factor_rejects_large_order():
+    lib = nb.load()
+    n = 4097
+    # Rejected on the size alone, before any device pointer is used.
+    assert not lib.nec2c_cuda_dense_factor_device_static(n, C.c_void_p(16), n, C.c_void_p(16))
+    assert b"maximum" in lib.nec2c_cuda_last_error()
