@@ -22,6 +22,7 @@
 //   gemm        A22 -= L21 U12, 64x64 complex tiles, K chunks of 16
 #include <cooperative_groups.h>
 #include <float.h>
+#include <limits.h>
 #include <math.h>
 #include <string.h>
 #include "common.cuh"
@@ -35,7 +36,6 @@ namespace {
 
 constexpr int KB = 32;        // panel width
 constexpr int PT = 256;       // panel threads per CTA
-constexpr int CS = 8;         // panel cluster size (portable maximum)
 
 struct LuStatus {
   unsigned int count, gen;
@@ -75,7 +75,9 @@ struct PanelArgs {
 // row r receives the old content of row src(r) for at most 2 KB rows.  The
 // panel's own rows k0..k0+kb-1 are slots 0..kb-1; pivot rows below the panel
 // get slots kb.. (matched with a warp ballot).
-__device__ void panel_pairs_warp(const PanelArgs &p) {
+// piv_rel: the panel's pivot rows relative to k0 (shared memory), or null to
+// read them from ipiv.
+__device__ void panel_pairs_warp(const PanelArgs &p, const int *piv_rel = nullptr) {
   __shared__ int rows[2 * KB], src[2 * KB], cnt;
   const int lane = threadIdx.x & 31;
   const int k0 = (int)p.k0, kb = p.kb;
@@ -83,7 +85,7 @@ __device__ void panel_pairs_warp(const PanelArgs &p) {
   if (lane == 0) cnt = kb;
   __syncwarp();
   for (int i = 0; i < kb; ++i) {
-    const int q = p.ipiv[k0 + i] - 1;
+    const int q = piv_rel ? k0 + piv_rel[i] : p.ipiv[k0 + i] - 1;
     int iq;
     if (q < k0 + kb) {
       iq = q - k0;
@@ -159,93 +161,286 @@ __device__ __forceinline__ void block_best(double mv, int mi, int rule, double *
   *i = bi;
 }
 
-// Cluster panel: CTA r, thread t owns panel row g = r*TPB + t (TPB threads
-// per CTA, one row each in registers, up to CS*TPB rows).  Per column every
-// CTA pushes its best candidate (value, row index, row) and, from the owner,
-// the current row j into the shared memory of all CTAs of the cluster, then
-// one cluster barrier makes them visible: the winner and the pivot row are
-// then read locally (double-buffered by column parity).
-struct ClusterSlot {
-  double val[2][CS];
-  int idx[2][CS];
-  double2 row[2][CS][KB];   // candidate rows, one per CTA
-  double2 rowj[2][KB];      // row j
+// Cluster panel.  A cluster of CSZ CTAs (256 threads each) keeps the panel in
+// registers: CTA r holds panel rows r*256 .. r*256+255; warp w of a CTA holds
+// columns 4w..4w+3 and lane L the rows L, L+32, ..., L+224 of them.  Rows are
+// never moved while the panel is factored: each row carries its logical
+// position (pos), interchanges only exchange positions, and the rows are
+// written to their final positions at the end.  Per column j (owned by warp
+// wj = j/4):
+//   1  warp wj: best candidate of the CTA (rows with pos >= j), published to
+//      the CTA through a local mbarrier, and its header pushed to every CTA
+//   2  every warp pushes its four elements of that candidate row to every CTA
+//      (st.async, counted in transaction bytes on the receiver's mbarrier)
+//   3  every warp waits for all CTAs' candidates, picks the winner in rank
+//      order and exchanges positions (pivot row -> j, row at j -> old place)
+//   4  warp wj forms the multipliers, publishes them through shared memory and
+//      a local mbarrier, and updates its own later columns
+//   5  warps w > wj apply the rank-1 update to their four columns
+// There is no CTA-wide barrier per column; every wait is bounded.  Buffers and
+// mbarriers alternate by column parity; reuse is safe because a warp reaches
+// column j+2's publication only after every warp of every CTA has pushed
+// column j+1, which each did after finishing its reads of column j.
+constexpr int CROWS = 256;            // panel rows per CTA
+constexpr int CPT = 256;              // threads per CTA (8 warps x 4 columns)
+constexpr int CRL = CROWS / 32;       // rows per lane
+constexpr int CCW = KB / (CPT / 32);  // columns per warp
+constexpr int CMAX = 16;              // largest cluster (non-portable size, opt-in)
+
+struct CandEntry {
+  double val;
+  int idx, pad;
+  double2 row[KB];
 };
 
-template <int TPB>
-__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(TPB, 1) panel_cluster_kernel(PanelArgs p) {
+template <int CSZ>
+struct PanelShared {
+  CandEntry cand[2][CSZ];             // candidates pushed by every CTA
+  double2 mult[2][CROWS];             // multipliers of column j (by physical row)
+  double best_val[2];
+  int best_idx[2], best_phys[2];      // CTA best: logical index, physical row
+  unsigned long long xbar[2], lbar[2], mbar[2];
+  int piv[KB];                        // panel-relative pivot rows
+  int info;                           // first zero pivot (column + 1), 0 = none
+  int fail;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t local, int rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+  return r;
+}
+// 16-byte store into a CTA's shared memory (any CTA of the cluster),
+// completing 16 transaction bytes on that CTA's mbarrier.
+__device__ __forceinline__ void push16(uint32_t dst, uint4 v, uint32_t bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];"
+               :: "r"(dst), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "r"(bar) : "memory");
+}
+__device__ __forceinline__ uint4 as_u4(double2 v) {
+  return make_uint4((unsigned)__double2loint(v.x), (unsigned)__double2hiint(v.x), (unsigned)__double2loint(v.y),
+                    (unsigned)__double2hiint(v.y));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint32_t bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint32_t bar, unsigned parity) {
+  uint32_t ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+               " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+  return ok != 0;
+}
+// Bounded wait (about a second at boost clock) that also gives up as soon as
+// another warp of the CTA has recorded a failure; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, unsigned parity, const int *fail) {
+  if (mbar_test(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_test(bar, parity))
+    if (*(volatile const int *)fail || clock64() - t0 > (1LL << 31)) return false;
+  return true;
+}
+
+// Column j = 4*wj + CC (CC compile-time) for this thread: a[k][c] is row
+// L+32k, column 4*warp+c; pos[k] its logical position (panel-relative).
+template <int CSZ, int CC, int RULE>
+__device__ __forceinline__ bool panel_column(const PanelArgs &p, PanelShared<CSZ> &sh, double2 (&a)[CRL][CCW],
+                                             int (&pos)[CRL], int rank, int wj) {
+  constexpr unsigned XBYTES = CSZ * sizeof(CandEntry);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int j = CCW * wj + CC, buf = j & 1;
+  const unsigned par = (unsigned)(j >> 1) & 1u;
+  const uint32_t xbar = smem_addr(&sh.xbar[buf]);
+  if (threadIdx.x == 0) mbar_expect(xbar, XBYTES);
+  // 1: the CTA's best candidate of column j.
+  if (warp == wj) {
+    double bv = -1.0;
+    int bi = -1, bk = 0;
+#pragma unroll
+    for (int k = 0; k < CRL; ++k) {
+      if (pos[k] >= j && pos[k] < p.n - p.k0) {
+        const double m = magnitude(a[k][CC], RULE);
+        if (bi < 0 || better(m, pos[k], bv, bi, RULE)) { bv = m; bi = pos[k]; bk = k; }
+      }
+    }
+    int bp = bi >= 0 ? lane + 32 * bk : -1;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+      if (oi >= 0 && (bi < 0 || better(ov, oi, bv, bi, RULE))) { bv = ov; bi = oi; bp = op; }
+    }
+    if (lane < CSZ) {
+      const uint4 hdr = make_uint4((unsigned)__double2loint(bv), (unsigned)__double2hiint(bv), (unsigned)bi, 0u);
+      push16(cluster_addr(smem_addr(&sh.cand[buf][rank]), lane), hdr, cluster_addr(xbar, lane));
+    }
+    if (lane == 0) {
+      sh.best_val[buf] = bv;
+      sh.best_idx[buf] = bi;
+      sh.best_phys[buf] = bp;
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(smem_addr(&sh.lbar[buf]));
+  }
+  // 2: every warp pushes its elements of the candidate row.
+  if (!mbar_wait(smem_addr(&sh.lbar[buf]), par, &sh.fail)) return false;
+  {
+    const int bp = sh.best_phys[buf];
+    const int hl = bp >= 0 ? (bp & 31) : 0, hk = bp >= 0 ? (bp >> 5) : 0;
+    double2 v[CCW];
+#pragma unroll
+    for (int c = 0; c < CCW; ++c) v[c] = make_double2(0, 0);
+    if (lane == hl) {
+      switch (hk) {
+#define N2C_TAKE(K) case K: _Pragma("unroll") for (int c = 0; c < CCW; ++c) v[c] = a[K][c]; break;
+        N2C_TAKE(0) N2C_TAKE(1) N2C_TAKE(2) N2C_TAKE(3) N2C_TAKE(4) N2C_TAKE(5) N2C_TAKE(6) N2C_TAKE(7)
+#undef N2C_TAKE
+        default: break;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CCW; ++c) {
+      v[c].x = __shfl_sync(0xffffffffu, v[c].x, hl);
+      v[c].y = __shfl_sync(0xffffffffu, v[c].y, hl);
+    }
+    if (lane < CSZ) {
+      const uint32_t rb = cluster_addr(xbar, lane);
+#pragma unroll
+      for (int c = 0; c < CCW; ++c)
+        push16(cluster_addr(smem_addr(&sh.cand[buf][rank].row[CCW * warp + c]), lane), as_u4(v[c]), rb);
+    }
+  }
+  // 3: the winner (fixed rank order) and the position exchange.
+  if (!mbar_wait(xbar, par, &sh.fail)) return false;
+  double v = -2.0;
+  int pi = -1;
+  if (lane < CSZ) { v = sh.cand[buf][lane].val; pi = sh.cand[buf][lane].idx; }
+  int pr = lane;
+  for (int o = CSZ >> 1; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, pi, o);
+    const int orr = __shfl_xor_sync(0xffffffffu, pr, o);
+    if (oi >= 0 && (pi < 0 || better(ov, oi, v, pi, RULE))) { v = ov; pi = oi; pr = orr; }
+  }
+  v = __shfl_sync(0xffffffffu, v, 0);
+  pi = __shfl_sync(0xffffffffu, pi, 0);
+  pr = __shfl_sync(0xffffffffu, pr, 0);
+  const bool zero = RULE == 0 ? !(v > 0.0) : !(v > 64.0 * DBL_EPSILON);
+#pragma unroll
+  for (int k = 0; k < CRL; ++k) {
+    if (pos[k] == pi) pos[k] = j;
+    else if (pos[k] == j) pos[k] = pi;
+  }
+  if (threadIdx.x == 0) {
+    sh.piv[j] = pi;
+    if (zero && sh.info == 0) sh.info = j + 1;
+  }
+  const double2 *prow = sh.cand[buf][pr].row;
+  // 4: multipliers (by the reciprocal, as factr does, matrix.c:1393-1398).
+  if (warp == wj) {
+    double2 l[CRL];
+    const double2 pv = prow[j];
+    const double r = 1.0 / (pv.x * pv.x + pv.y * pv.y);
+    const double2 inv = make_double2(pv.x * r, -pv.y * r);
+#pragma unroll
+    for (int k = 0; k < CRL; ++k) {
+      l[k] = make_double2(0, 0);
+      if (!zero && pos[k] > j && pos[k] < p.n - p.k0) { l[k] = cmul(a[k][CC], inv); a[k][CC] = l[k]; }
+      sh.mult[buf][lane + 32 * k] = l[k];
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(smem_addr(&sh.mbar[buf]));
+    if (!zero) {
+#pragma unroll
+      for (int c = CC + 1; c < CCW; ++c) {
+        const double2 u = prow[CCW * warp + c];
+#pragma unroll
+        for (int k = 0; k < CRL; ++k)
+          if (pos[k] > j && pos[k] < p.n - p.k0) a[k][c] = csub(a[k][c], cmul(l[k], u));
+      }
+    }
+  } else if (warp > wj) {
+    // 5: rank-1 update of this warp's columns.
+    if (!mbar_wait(smem_addr(&sh.mbar[buf]), par, &sh.fail)) return false;
+    if (!zero) {
+      double2 u[CCW];
+#pragma unroll
+      for (int c = 0; c < CCW; ++c) u[c] = prow[CCW * warp + c];
+#pragma unroll
+      for (int k = 0; k < CRL; ++k) {
+        if (!(pos[k] > j && pos[k] < p.n - p.k0)) continue;
+        const double2 lk = sh.mult[buf][lane + 32 * k];
+#pragma unroll
+        for (int c = 0; c < CCW; ++c) a[k][c] = csub(a[k][c], cmul(lk, u[c]));
+      }
+    }
+  }
+  return true;
+}
+
+template <int CSZ, int RULE>
+__global__ void __launch_bounds__(CPT, 1) panel_cluster_kernel(PanelArgs p) {
+  static_assert(sizeof(CandEntry) % 16 == 0 && CSZ <= 32 && CCW == 4 && KB == 32, "panel layout");
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
-  __shared__ ClusterSlot slot;
-  __shared__ double2 mine[KB], minej[KB];
-  __shared__ double m_val;
-  __shared__ int m_idx;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ __align__(16) PanelShared<CSZ> sh;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_addr(&sh.xbar[b]), 1);
+      mbar_init(smem_addr(&sh.lbar[b]), 1);
+      mbar_init(smem_addr(&sh.mbar[b]), 1);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    sh.fail = 0;
+    sh.info = 0;
+  }
+  cluster.sync();
   const long long rows = p.n - p.k0;
-  double2 a[1][KB];
-  const int g[1] = {rank * TPB + (int)threadIdx.x};
-  const bool have[1] = {g[0] < rows};
-  {
-    const double2 *row = p.a + (p.k0 + g[0]) * p.ld + p.k0;
+  double2 a[CRL][CCW];
+  int pos[CRL];
 #pragma unroll
-    for (int c = 0; c < KB; ++c) a[0][c] = (have[0] && c < p.kb) ? row[c] : make_double2(0, 0);
+  for (int k = 0; k < CRL; ++k) {
+    const int g = rank * CROWS + lane + 32 * k;
+    pos[k] = g < rows ? g : INT_MAX;
+    const double2 *row = p.a + (p.k0 + g) * p.ld + p.k0 + CCW * warp;
+#pragma unroll
+    for (int c = 0; c < CCW; ++c)
+      a[k][c] = (g < rows && CCW * warp + c < p.kb) ? row[c] : make_double2(0, 0);
   }
-  for (int j = 0; j < p.kb; ++j) {
-    const int buf = j & 1;
-    double mv = -1.0;
-    int mi = -1;
-    if (have[0] && g[0] >= j) {
-      double2 z = make_double2(0, 0);
-#pragma unroll
-      for (int c = 0; c < KB; ++c) if (c == j) z = a[0][c];
-      mv = magnitude(z, p.rule);
-      mi = g[0];
-    }
-    double bv;
-    int bi;
-    block_best(mv, mi, p.rule, &bv, &bi);
-    if (have[0] && g[0] == bi) {
-#pragma unroll
-      for (int c = 0; c < KB; ++c) mine[c] = a[0][c];
-    }
-    const bool jown = j / TPB == rank;
-    if (have[0] && g[0] == j) {
-#pragma unroll
-      for (int c = 0; c < KB; ++c) minej[c] = a[0][c];
-    }
-    if (threadIdx.x == 0) { m_val = bv; m_idx = bi; }
-    __syncthreads();
-    // Push to every CTA (including this one): thread t -> (CTA t / 32, entry t % 32).
-    for (int t = threadIdx.x; t < CS * KB; t += TPB) {
-      const int dest = t / KB, e = t % KB;
-      ClusterSlot *rs = cluster.map_shared_rank(&slot, dest);
-      rs->row[buf][rank][e] = mine[e];
-      if (jown) rs->rowj[buf][e] = minej[e];
-      if (e == 0) { rs->val[buf][rank] = m_val; rs->idx[buf][rank] = m_idx; }
-    }
-    cluster.sync();
-    // Global winner in fixed rank order, from local shared memory.
-    double v = -2.0;
-    int pi = -1, pr = 0;
-#pragma unroll
-    for (int r = 0; r < CS; ++r) {
-      const int ri = slot.idx[buf][r];
-      const double rv = slot.val[buf][r];
-      if (ri >= 0 && (pi < 0 || better(rv, ri, v, pi, p.rule))) { v = rv; pi = ri; pr = r; }
-    }
-    const bool zero = p.rule == 0 ? !(v > 0.0) : !(v > 64.0 * DBL_EPSILON);
-    if (rank == 0 && threadIdx.x == 0) {
-      p.ipiv[p.k0 + j] = (int)(p.k0 + pi + 1);
-      if (zero && p.st->info == 0) p.st->info = (int)(p.k0 + j + 1);
-    }
-    apply_column<1>(a, g, have, j, pi, slot.row[buf][pr], slot.rowj[buf], zero, p.kb);
+  bool ok = true;
+  for (int wj = 0; wj < KB / CCW && ok; ++wj) {
+    if (CCW * wj + 0 < p.kb) ok = panel_column<CSZ, 0, RULE>(p, sh, a, pos, rank, wj);
+    if (ok && CCW * wj + 1 < p.kb) ok = panel_column<CSZ, 1, RULE>(p, sh, a, pos, rank, wj);
+    if (ok && CCW * wj + 2 < p.kb) ok = panel_column<CSZ, 2, RULE>(p, sh, a, pos, rank, wj);
+    if (ok && CCW * wj + 3 < p.kb) ok = panel_column<CSZ, 3, RULE>(p, sh, a, pos, rank, wj);
   }
+  if (!ok) sh.fail = 1;
   cluster.sync();   // no CTA exits while others may still push into it
-  if (have[0]) {
-    double2 *row = p.a + (p.k0 + g[0]) * p.ld + p.k0;
-#pragma unroll
-    for (int c = 0; c < KB; ++c) if (c < p.kb) row[c] = a[0][c];
+  if (sh.fail) {
+    if (threadIdx.x == 0) atomicExch(&p.st->error, 1);
+    return;
   }
-  if (rank == 0 && threadIdx.x < 32) panel_pairs_warp(p);
+#pragma unroll
+  for (int k = 0; k < CRL; ++k) {
+    if (pos[k] == INT_MAX) continue;
+    double2 *row = p.a + (p.k0 + pos[k]) * p.ld + p.k0 + CCW * warp;
+#pragma unroll
+    for (int c = 0; c < CCW; ++c) if (CCW * warp + c < p.kb) row[c] = a[k][c];
+  }
+  if (rank == 0 && warp == 0) {
+    for (int j = lane; j < p.kb; j += 32) p.ipiv[p.k0 + j] = (int)(p.k0 + sh.piv[j] + 1);
+    if (lane == 0 && sh.info && p.st->info == 0) p.st->info = (int)(p.k0 + sh.info);
+    panel_pairs_warp(p, sh.piv);
+  }
 }
 
 // Cooperative-grid panel for orders beyond the cluster's capacity: one row per
@@ -559,73 +754,156 @@ static unsigned blocks_for(long long work) {
   return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
-extern "C" int n2d_lu_factor(double *a_dev, long long n, long long ld, int *ipiv, int rule, int precision,
-                             int *info_host) {
-  (void)precision;
-  *info_host = 0;
-  if (n <= 0) return 1;
-  double2 *a = (double2 *)a_dev;
-  const long long grid_blocks = (n + PT - 1) / PT;
-  // Cluster panel with 256 or 512 threads per CTA (one row each); beyond
-  // 8 x 512 rows the cooperative-grid panel.
-  const int rows_per_thread = n <= (long long)CS * 256 ? 1 : (n <= (long long)CS * 512 ? 2 : 0);
-  LuStatus *st = (LuStatus *)n2d_alloc(sizeof(LuStatus));
-  int *pairs = (int *)n2d_alloc(4 * KB * sizeof(int));
-  double2 *tmp = (double2 *)n2d_alloc((size_t)2 * KB * n * sizeof(double2));
-  double *gval = nullptr;
-  int *gidx = nullptr;
-  double2 *grow = nullptr, *growj = nullptr;
-  if (!rows_per_thread) {
-    gval = (double *)n2d_alloc(2 * grid_blocks * sizeof(double));
-    gidx = (int *)n2d_alloc(2 * grid_blocks * sizeof(int));
-    grow = (double2 *)n2d_alloc(2 * grid_blocks * KB * sizeof(double2));
-    growj = (double2 *)n2d_alloc(2 * KB * sizeof(double2));
+// Panel launch: the smallest cluster of 256-thread CTAs that holds the
+// panel's rows (16-CTA clusters where the device allows that non-portable
+// size), else the cooperative grid panel.
+template <int CSZ>
+static cudaError_t launch_cluster_panel(const PanelArgs &p, cudaStream_t s) {
+  void (*kernel)(PanelArgs) = p.rule == 0 ? panel_cluster_kernel<CSZ, 0> : panel_cluster_kernel<CSZ, 1>;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(CSZ);
+  cfg.blockDim = dim3(CPT);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CSZ;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, p);
+}
+
+// 1 when 16-CTA clusters of the panel kernel can be resident (checked once).
+static int cluster16_ok() {
+  static int state = -1;
+  if (state >= 0) return state;
+  state = 0;
+  if (cudaFuncSetAttribute(panel_cluster_kernel<CMAX, 0>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(panel_cluster_kernel<CMAX, 1>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return state;
   }
-  int ok = st && pairs && tmp && n2d_memset(st, 0, sizeof(LuStatus)) &&
-           (rows_per_thread || (gval && gidx && grow && growj));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(CMAX);
+  cfg.blockDim = dim3(CPT);
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CMAX;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, panel_cluster_kernel<CMAX, 0>, &cfg) == cudaSuccess && clusters > 0)
+    state = 1;
+  cudaGetLastError();
+  return state;
+}
+
+// Largest panel row count the cluster kernel takes on this device.
+static long long cluster_rows() { return (long long)CROWS * (cluster16_ok() ? CMAX : 8); }
+
+static int launch_panel(const PanelArgs &p, long long rows, cudaStream_t s) {
+  cudaError_t e;
+  if (rows <= cluster_rows()) {
+    if (rows <= CROWS) e = launch_cluster_panel<1>(p, s);
+    else if (rows <= 2 * CROWS) e = launch_cluster_panel<2>(p, s);
+    else if (rows <= 4 * CROWS) e = launch_cluster_panel<4>(p, s);
+    else if (rows <= 8 * CROWS) e = launch_cluster_panel<8>(p, s);
+    else e = launch_cluster_panel<CMAX>(p, s);
+  } else {
+    const int blocks = (int)((rows + PT - 1) / PT);
+    void *args[] = {const_cast<PanelArgs *>(&p)};
+    e = cudaLaunchCooperativeKernel((void *)panel_grid_kernel, blocks, PT, args, 0, s);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    n2c_set_error("panel launch: %s", cudaGetErrorString(e));
+    return 0;
+  }
+  n2c_count_launch(1);
+  return 1;
+}
+
+// Scratch of one factorisation: status, interchange pairs, the row buffer of
+// the interchanges (2 KB x n) and, for the grid panel, its candidate arrays.
+struct FactorScratch {
+  LuStatus *st;
+  int *pairs;
+  double2 *tmp;
+  double *gval;
+  int *gidx;
+  double2 *grow, *growj;
+};
+
+static int grid_blocks_for(long long n) { return (int)((n + PT - 1) / PT); }
+
+// The blocked factorisation; the status must be zero on entry.  Reads the
+// status back (synchronising the stream) and sets *info_host.
+static int factor_panels(double2 *a, long long n, long long ld, int *ipiv, int rule, const FactorScratch &w,
+                         int *info_host) {
+  cudaStream_t s = n2c_stream();
+  int ok = 1;
   for (long long k0 = 0; ok && k0 < n; k0 += KB) {
     const int kb = (int)(n - k0 < KB ? n - k0 : KB);
     PanelArgs p;
     memset(&p, 0, sizeof(p));
     p.a = a; p.n = n; p.ld = ld; p.k0 = k0; p.kb = kb; p.rule = rule; p.ipiv = ipiv;
-    p.pairs = pairs; p.st = st; p.gval = gval; p.gidx = gidx; p.grow = grow; p.growj = growj;
-    if (rows_per_thread == 1) {
-      panel_cluster_kernel<256><<<CS, 256, 0, n2c_stream()>>>(p);
-      if (!n2c_check_launch("panel")) { ok = 0; break; }
-    } else if (rows_per_thread == 2) {
-      panel_cluster_kernel<512><<<CS, 512, 0, n2c_stream()>>>(p);
-      if (!n2c_check_launch("panel")) { ok = 0; break; }
-    } else {
-      const int blocks = (int)((n - k0 + PT - 1) / PT);
-      void *args[] = {&p};
-      cudaError_t e = cudaLaunchCooperativeKernel((void *)panel_grid_kernel, blocks, PT, args, 0, n2c_stream());
-      if (e != cudaSuccess) { n2c_set_error("panel launch: %s", cudaGetErrorString(e)); ok = 0; break; }
-      n2c_count_launch(1);
-    }
+    p.pairs = w.pairs; p.st = w.st; p.gval = w.gval; p.gidx = w.gidx; p.grow = w.grow; p.growj = w.growj;
+    if (!launch_panel(p, n - k0, s)) { ok = 0; break; }
     if (n > kb) {
       const unsigned gb = blocks_for(2LL * KB * (n - kb));
-      rows_gather_kernel<<<gb, 256, 0, n2c_stream()>>>(a, n, ld, k0, kb, pairs, st, tmp);
-      rows_scatter_kernel<<<gb, 256, 0, n2c_stream()>>>(a, n, ld, k0, kb, pairs, st, tmp);
+      rows_gather_kernel<<<gb, 256, 0, s>>>(a, n, ld, k0, kb, w.pairs, w.st, w.tmp);
+      rows_scatter_kernel<<<gb, 256, 0, s>>>(a, n, ld, k0, kb, w.pairs, w.st, w.tmp);
       if (!n2c_check_launch("interchanges")) { ok = 0; break; }
       n2c_count_launch(1);
     }
     const long long right = n - k0 - kb;
     if (right > 0) {
-      trsm_kernel<<<(unsigned)((right + 127) / 128), 128, 0, n2c_stream()>>>(a, n, ld, k0, kb);
+      trsm_kernel<<<(unsigned)((right + 127) / 128), 128, 0, s>>>(a, n, ld, k0, kb);
       if (!n2c_check_launch("trsm")) { ok = 0; break; }
       dim3 grid((unsigned)((right + GT - 1) / GT), (unsigned)((right + GT - 1) / GT));
-      gemm_update_kernel<<<grid, 256, 0, n2c_stream()>>>(a + (k0 + kb) * ld + (k0 + kb), a + (k0 + kb) * ld + k0,
-                                                         a + k0 * ld + (k0 + kb), right, right, kb, ld);
+      gemm_update_kernel<<<grid, 256, 0, s>>>(a + (k0 + kb) * ld + (k0 + kb), a + (k0 + kb) * ld + k0,
+                                              a + k0 * ld + (k0 + kb), right, right, kb, ld);
       if (!n2c_check_launch("gemm_update")) { ok = 0; break; }
     }
   }
   LuStatus hs;
   memset(&hs, 0, sizeof(hs));
-  if (ok && !n2d_download(&hs, st, sizeof(hs))) ok = 0;
-  if (ok && hs.error) { n2c_set_error("LU panel barrier time-out"); ok = 0; }
+  cudaError_t e = cudaMemcpyAsync(&hs, w.st, sizeof(hs), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (ok && e != cudaSuccess) { n2c_set_error("reading the panel status: %s", cudaGetErrorString(e)); ok = 0; }
+  if (ok && hs.error) { n2c_set_error("LU panel exchange time-out"); ok = 0; }
   *info_host = hs.info;
-  n2d_free(st); n2d_free(pairs); n2d_free(tmp);
-  n2d_free(gval); n2d_free(gidx); n2d_free(grow); n2d_free(growj);
+  return ok;
+}
+
+extern "C" int n2d_lu_factor(double *a_dev, long long n, long long ld, int *ipiv, int rule, int precision,
+                             int *info_host) {
+  (void)precision;
+  *info_host = 0;
+  if (n <= 0) return 1;
+  FactorScratch w;
+  memset(&w, 0, sizeof(w));
+  w.st = (LuStatus *)n2d_alloc(sizeof(LuStatus));
+  w.pairs = (int *)n2d_alloc(4 * KB * sizeof(int));
+  w.tmp = (double2 *)n2d_alloc((size_t)2 * KB * n * sizeof(double2));
+  const bool grid = n > cluster_rows();
+  const int gb = grid_blocks_for(n);
+  if (grid) {
+    w.gval = (double *)n2d_alloc(2 * gb * sizeof(double));
+    w.gidx = (int *)n2d_alloc(2 * gb * sizeof(int));
+    w.grow = (double2 *)n2d_alloc((size_t)2 * gb * KB * sizeof(double2));
+    w.growj = (double2 *)n2d_alloc(2 * KB * sizeof(double2));
+  }
+  int ok = w.st && w.pairs && w.tmp && n2d_memset(w.st, 0, sizeof(LuStatus)) &&
+           (!grid || (w.gval && w.gidx && w.grow && w.growj));
+  ok = ok && factor_panels((double2 *)a_dev, n, ld, ipiv, rule, w, info_host);
+  n2d_free(w.st); n2d_free(w.pairs); n2d_free(w.tmp);
+  n2d_free(w.gval); n2d_free(w.gidx); n2d_free(w.grow); n2d_free(w.growj);
   return ok;
 }
 
@@ -644,11 +922,11 @@ extern "C" int n2d_lu_solve(const double *a_dev, long long n, long long ld, cons
 // plug-in living inside such a process, or a loop with a latency budget that
 // cudaMalloc's implicit device synchronisation would break.  The caller passes
 // the matrix and the pivot array already resident on the device; the panel
-// status, the interchange pairs and the row buffer of the interchanges live in
-// one array defined in this file instead of being allocated per call.
+// status, the interchange pairs, the row buffer of the interchanges and the
+// grid panel's candidate arrays live in one array defined in this file instead of being allocated per call.
 //
 // That array is a module global: every GPU on which the library is loaded
-// holds it (4 MiB + 1 KiB) until the process exits, and every call on that
+// holds it (4 MiB + 20 KiB) until the process exits, and every call on that
 // GPU shares it.  Calls whose work overlaps on the GPU (two streams, two host
 // threads) therefore race on it; callers serialise them.  The array keeps the
 // previous call's contents; only the panel status needs to start at zero and
@@ -663,13 +941,20 @@ extern "C" int n2d_lu_solve(const double *a_dev, long long n, long long ld, cons
 #include "../../include/nec2c_cuda.h"
 
 namespace {
+constexpr int STATIC_GRID = (NEC2C_CUDA_STATIC_LU_MAX_ORDER + PT - 1) / PT;   // grid-panel blocks
 constexpr size_t STATIC_STATUS_OFF = 0;
 constexpr size_t STATIC_PAIRS_OFF = 256;
-constexpr size_t STATIC_ROWS_OFF = 1024;
+constexpr size_t STATIC_GVAL_OFF = 1024;
+constexpr size_t STATIC_GIDX_OFF = STATIC_GVAL_OFF + 2 * STATIC_GRID * sizeof(double);
+constexpr size_t STATIC_GROWJ_OFF = 2048;
+constexpr size_t STATIC_GROW_OFF = STATIC_GROWJ_OFF + 2 * KB * sizeof(double2);
+constexpr size_t STATIC_ROWS_OFF = STATIC_GROW_OFF + (size_t)2 * STATIC_GRID * KB * sizeof(double2);
 constexpr size_t STATIC_SCRATCH_BYTES =
     STATIC_ROWS_OFF + (size_t)2 * KB * NEC2C_CUDA_STATIC_LU_MAX_ORDER * sizeof(double2);
 static_assert(sizeof(LuStatus) <= STATIC_PAIRS_OFF - STATIC_STATUS_OFF, "status slot");
-static_assert(4 * KB * sizeof(int) <= STATIC_ROWS_OFF - STATIC_PAIRS_OFF, "pairs slot");
+static_assert(4 * KB * sizeof(int) <= STATIC_GVAL_OFF - STATIC_PAIRS_OFF, "pairs slot");
+static_assert(STATIC_GIDX_OFF + 2 * STATIC_GRID * sizeof(int) <= STATIC_GROWJ_OFF, "grid candidates slot");
+static_assert(STATIC_ROWS_OFF % 256 == 0, "row buffer alignment");
 constexpr int STATIC_MAX_DEVICES = 64;
 std::mutex g_static_lock;
 unsigned char *g_static_addr[STATIC_MAX_DEVICES];
@@ -712,48 +997,19 @@ extern "C" int nec2c_cuda_dense_factor_device_static(size_t order, nec2c_cuda_co
   if (!n2d_device_ok()) return 0;
   unsigned char *base = static_scratch();
   if (!base) return 0;
-  LuStatus *st = (LuStatus *)(base + STATIC_STATUS_OFF);
-  int *pairs = (int *)(base + STATIC_PAIRS_OFF);
-  double2 *tmp = (double2 *)(base + STATIC_ROWS_OFF);
-  double2 *a = (double2 *)matrix_dev;
-  const long long n = (long long)order, ld = (long long)leading_dimension;
-  cudaStream_t s = n2c_stream();
-  cudaError_t e = cudaMemsetAsync(st, 0, sizeof(LuStatus), s);
+  FactorScratch w;
+  w.st = (LuStatus *)(base + STATIC_STATUS_OFF);
+  w.pairs = (int *)(base + STATIC_PAIRS_OFF);
+  w.gval = (double *)(base + STATIC_GVAL_OFF);
+  w.gidx = (int *)(base + STATIC_GIDX_OFF);
+  w.growj = (double2 *)(base + STATIC_GROWJ_OFF);
+  w.grow = (double2 *)(base + STATIC_GROW_OFF);
+  w.tmp = (double2 *)(base + STATIC_ROWS_OFF);
+  cudaError_t e = cudaMemsetAsync(w.st, 0, sizeof(LuStatus), n2c_stream());
   if (e != cudaSuccess) { n2c_set_error("clearing the panel status: %s", cudaGetErrorString(e)); return 0; }
-  int ok = 1;
-  for (long long k0 = 0; ok && k0 < n; k0 += KB) {
-    const int kb = (int)(n - k0 < KB ? n - k0 : KB);
-    PanelArgs p;
-    memset(&p, 0, sizeof(p));
-    p.a = a; p.n = n; p.ld = ld; p.k0 = k0; p.kb = kb; p.rule = 0; p.ipiv = pivots_dev;
-    p.pairs = pairs; p.st = st;
-    if (n <= (long long)CS * 256) panel_cluster_kernel<256><<<CS, 256, 0, s>>>(p);
-    else panel_cluster_kernel<512><<<CS, 512, 0, s>>>(p);
-    if (!n2c_check_launch("panel")) { ok = 0; break; }
-    if (n > kb) {
-      const unsigned gb = blocks_for(2LL * KB * (n - kb));
-      rows_gather_kernel<<<gb, 256, 0, s>>>(a, n, ld, k0, kb, pairs, st, tmp);
-      rows_scatter_kernel<<<gb, 256, 0, s>>>(a, n, ld, k0, kb, pairs, st, tmp);
-      if (!n2c_check_launch("interchanges")) { ok = 0; break; }
-      n2c_count_launch(1);
-    }
-    const long long right = n - k0 - kb;
-    if (right > 0) {
-      trsm_kernel<<<(unsigned)((right + 127) / 128), 128, 0, s>>>(a, n, ld, k0, kb);
-      if (!n2c_check_launch("trsm")) { ok = 0; break; }
-      dim3 grid((unsigned)((right + GT - 1) / GT), (unsigned)((right + GT - 1) / GT));
-      gemm_update_kernel<<<grid, 256, 0, s>>>(a + (k0 + kb) * ld + (k0 + kb), a + (k0 + kb) * ld + k0,
-                                              a + k0 * ld + (k0 + kb), right, right, kb, ld);
-      if (!n2c_check_launch("gemm_update")) { ok = 0; break; }
-    }
-  }
-  if (!ok) return 0;
-  LuStatus hs;
-  memset(&hs, 0, sizeof(hs));
-  e = cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) { n2c_set_error("reading the panel status: %s", cudaGetErrorString(e)); return 0; }
-  if (hs.error) { n2c_set_error("LU panel barrier time-out"); return 0; }
-  if (hs.info) { n2c_set_error("matrix is singular (pivot %d)", hs.info); return 0; }
+  int info = 0;
+  if (!factor_panels((double2 *)matrix_dev, (long long)order, (long long)leading_dimension, pivots_dev, 0, w, &info))
+    return 0;
+  if (info) { n2c_set_error("matrix is singular (pivot %d)", info); return 0; }
   return 1;
 }
