@@ -175,7 +175,7 @@ void nec2c_cuda_dense_release(void);
    dimension >= order) factored in place with the same pivots and factors as
    nec2c_cuda_dense_factor_classic, and 1-based pivots written to pivots_dev.
    The work runs on this thread's stream and the call returns when it is done.
-   Scratch is one 4 MiB array inside the library that each GPU using it holds
+   Scratch is one 20 KiB array inside the library that each GPU using it holds
    until exit; calls that overlap on the GPU share it and race.  The first
    call on a device looks up that array's address, so make it before any
    stream capture.  Orders above NEC2C_CUDA_STATIC_LU_MAX_ORDER are rejected.

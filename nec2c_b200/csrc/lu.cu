@@ -538,59 +538,51 @@ __global__ void __launch_bounds__(PT) panel_grid_kernel(PanelArgs p) {
   if (blockIdx.x == 0 && threadIdx.x < 32) panel_pairs_warp(p);
 }
 
-// Row interchanges outside the panel columns [k0, k0+kb): gather the source
-// rows of the affected pairs into scratch, then scatter them to their
-// destinations.  Thread (pair, column), columns consecutive across threads.
-__global__ void rows_gather_kernel(const double2 *a, long long n, long long ld, long long k0, int kb,
-                                   const int *pairs, const LuStatus *st, double2 *tmp) {
-  const int np = st->npairs;
-  const long long cols = n - kb;
-  const long long total = (long long)np * cols;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long q = t / cols, c0 = t - q * cols;
-    const long long c = c0 < k0 ? c0 : c0 + kb;
-    tmp[t] = a[(long long)pairs[2 * KB + q] * ld + c];
-  }
-}
-
-__global__ void rows_scatter_kernel(double2 *a, long long n, long long ld, long long k0, int kb,
-                                    const int *pairs, const LuStatus *st, const double2 *tmp) {
-  const int np = st->npairs;
-  const long long cols = n - kb;
-  const long long total = (long long)np * cols;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long q = t / cols, c0 = t - q * cols;
-    const long long c = c0 < k0 ? c0 : c0 + kb;
-    a[(long long)pairs[q] * ld + c] = tmp[t];
-  }
-}
-
-// U12 = L11^-1 A12 (unit lower), one thread per column right of the panel.
-__global__ void __launch_bounds__(128) trsm_kernel(double2 *a, long long n, long long ld, long long k0, int kb) {
+// Row interchanges outside the panel columns [k0, k0+kb) and, right of the
+// panel, U12 = L11^-1 A12 (unit lower).  One warp per column: its lanes gather
+// the source rows of the interchange pairs into registers, then scatter them
+// (so overlapping pairs need no scratch), then lane i holds row k0+i of the
+// column and the forward substitution runs column-oriented, broadcasting x_k
+// by shuffle; each x_i subtracts L[i][k] x_k in increasing k, the order of the
+// row-oriented sum.
+constexpr int SWT = 256;   // threads per block (8 columns)
+__global__ void __launch_bounds__(SWT) swap_trsm_kernel(double2 *a, long long n, long long ld, long long k0, int kb,
+                                                        const int *pairs, const LuStatus *st) {
+  __shared__ int dst[2 * KB], src[2 * KB];
   __shared__ double2 L[KB][KB + 1];
-  for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-    const int i = t / kb, j = t % kb;
-    L[i][j] = a[(k0 + i) * ld + k0 + j];
-  }
-  __syncthreads();
-  const long long c = k0 + kb + blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (c >= n) return;
-  double2 x[KB];
-#pragma unroll
-  for (int i = 0; i < KB; ++i) x[i] = i < kb ? a[(k0 + i) * ld + c] : make_double2(0, 0);
-#pragma unroll
-  for (int i = 1; i < KB; ++i) {
-    if (i < kb) {
-      double2 s = x[i];
-#pragma unroll
-      for (int j = 0; j < KB; ++j) if (j < i) s = csub(s, cmul(L[i][j], x[j]));
-      x[i] = s;
+  const int np = st->npairs;
+  for (int t = threadIdx.x; t < np; t += blockDim.x) { dst[t] = pairs[t]; src[t] = pairs[2 * KB + t]; }
+  const long long first = (long long)blockIdx.x * (SWT / 32);
+  const long long cols = n - kb;
+  const bool any_right = first + SWT / 32 - 1 >= k0;   // some column of this block is right of the panel
+  if (any_right) {
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+      const int i = t / kb, j = t % kb;
+      L[i][j] = a[(k0 + i) * ld + k0 + j];
     }
   }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const long long c0 = first + (threadIdx.x >> 5);
+  if (c0 >= cols) return;
+  const long long c = c0 < k0 ? c0 : c0 + kb;
+  double2 v0 = make_double2(0, 0), v1 = make_double2(0, 0);
+  if (lane < np) v0 = a[(long long)src[lane] * ld + c];
+  if (lane + 32 < np) v1 = a[(long long)src[lane + 32] * ld + c];
+  __syncwarp();
+  if (lane < np) a[(long long)dst[lane] * ld + c] = v0;
+  if (lane + 32 < np) a[(long long)dst[lane + 32] * ld + c] = v1;
+  if (c < k0) return;
+  __syncwarp();
+  double2 x = lane < kb ? a[(k0 + lane) * ld + c] : make_double2(0, 0);
 #pragma unroll
-  for (int i = 1; i < KB; ++i) if (i < kb) a[(k0 + i) * ld + c] = x[i];
+  for (int k = 0; k < KB - 1; ++k) {
+    double2 xk;
+    xk.x = __shfl_sync(0xffffffffu, x.x, k);
+    xk.y = __shfl_sync(0xffffffffu, x.y, k);
+    if (lane > k && lane < kb) x = csub(x, cmul(L[lane][k], xk));
+  }
+  if (lane >= 1 && lane < kb) a[(k0 + lane) * ld + c] = x;
 }
 
 // C[M x N] -= A[M x K] B[K x N], row-major complex FP64 blocks (leading dim ld).
@@ -748,12 +740,6 @@ extern "C" int n2d_transpose(const double *src, long long lds, double *dst, long
   return n2c_check_launch("transpose");
 }
 
-static unsigned blocks_for(long long work) {
-  long long b = (work + 255) / 256;
-  const long long cap = (long long)n2c_sm_count() * 8;
-  return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
-}
-
 // Panel launch: the smallest cluster of 256-thread CTAs that holds the
 // panel's rows (16-CTA clusters where the device allows that non-portable
 // size), else the cooperative grid panel.
@@ -828,12 +814,11 @@ static int launch_panel(const PanelArgs &p, long long rows, cudaStream_t s) {
   return 1;
 }
 
-// Scratch of one factorisation: status, interchange pairs, the row buffer of
-// the interchanges (2 KB x n) and, for the grid panel, its candidate arrays.
+// Scratch of one factorisation: status, interchange pairs and, for the grid
+// panel, its candidate arrays.
 struct FactorScratch {
   LuStatus *st;
   int *pairs;
-  double2 *tmp;
   double *gval;
   int *gidx;
   double2 *grow, *growj;
@@ -855,16 +840,12 @@ static int factor_panels(double2 *a, long long n, long long ld, int *ipiv, int r
     p.pairs = w.pairs; p.st = w.st; p.gval = w.gval; p.gidx = w.gidx; p.grow = w.grow; p.growj = w.growj;
     if (!launch_panel(p, n - k0, s)) { ok = 0; break; }
     if (n > kb) {
-      const unsigned gb = blocks_for(2LL * KB * (n - kb));
-      rows_gather_kernel<<<gb, 256, 0, s>>>(a, n, ld, k0, kb, w.pairs, w.st, w.tmp);
-      rows_scatter_kernel<<<gb, 256, 0, s>>>(a, n, ld, k0, kb, w.pairs, w.st, w.tmp);
-      if (!n2c_check_launch("interchanges")) { ok = 0; break; }
-      n2c_count_launch(1);
+      const unsigned gb = (unsigned)((n - kb + SWT / 32 - 1) / (SWT / 32));
+      swap_trsm_kernel<<<gb, SWT, 0, s>>>(a, n, ld, k0, kb, w.pairs, w.st);
+      if (!n2c_check_launch("interchanges and triangular solve")) { ok = 0; break; }
     }
     const long long right = n - k0 - kb;
     if (right > 0) {
-      trsm_kernel<<<(unsigned)((right + 127) / 128), 128, 0, s>>>(a, n, ld, k0, kb);
-      if (!n2c_check_launch("trsm")) { ok = 0; break; }
       dim3 grid((unsigned)((right + GT - 1) / GT), (unsigned)((right + GT - 1) / GT));
       gemm_update_kernel<<<grid, 256, 0, s>>>(a + (k0 + kb) * ld + (k0 + kb), a + (k0 + kb) * ld + k0,
                                               a + k0 * ld + (k0 + kb), right, right, kb, ld);
@@ -890,7 +871,6 @@ extern "C" int n2d_lu_factor(double *a_dev, long long n, long long ld, int *ipiv
   memset(&w, 0, sizeof(w));
   w.st = (LuStatus *)n2d_alloc(sizeof(LuStatus));
   w.pairs = (int *)n2d_alloc(4 * KB * sizeof(int));
-  w.tmp = (double2 *)n2d_alloc((size_t)2 * KB * n * sizeof(double2));
   const bool grid = n > cluster_rows();
   const int gb = grid_blocks_for(n);
   if (grid) {
@@ -899,10 +879,10 @@ extern "C" int n2d_lu_factor(double *a_dev, long long n, long long ld, int *ipiv
     w.grow = (double2 *)n2d_alloc((size_t)2 * gb * KB * sizeof(double2));
     w.growj = (double2 *)n2d_alloc(2 * KB * sizeof(double2));
   }
-  int ok = w.st && w.pairs && w.tmp && n2d_memset(w.st, 0, sizeof(LuStatus)) &&
+  int ok = w.st && w.pairs && n2d_memset(w.st, 0, sizeof(LuStatus)) &&
            (!grid || (w.gval && w.gidx && w.grow && w.growj));
   ok = ok && factor_panels((double2 *)a_dev, n, ld, ipiv, rule, w, info_host);
-  n2d_free(w.st); n2d_free(w.pairs); n2d_free(w.tmp);
+  n2d_free(w.st); n2d_free(w.pairs);
   n2d_free(w.gval); n2d_free(w.gidx); n2d_free(w.grow); n2d_free(w.growj);
   return ok;
 }
@@ -922,11 +902,11 @@ extern "C" int n2d_lu_solve(const double *a_dev, long long n, long long ld, cons
 // plug-in living inside such a process, or a loop with a latency budget that
 // cudaMalloc's implicit device synchronisation would break.  The caller passes
 // the matrix and the pivot array already resident on the device; the panel
-// status, the interchange pairs, the row buffer of the interchanges and the
-// grid panel's candidate arrays live in one array defined in this file instead of being allocated per call.
+// status, the interchange pairs and the grid panel's candidate arrays live in
+// one array defined in this file instead of being allocated per call.
 //
 // That array is a module global: every GPU on which the library is loaded
-// holds it (4 MiB + 20 KiB) until the process exits, and every call on that
+// holds it (about 20 KiB) until the process exits, and every call on that
 // GPU shares it.  Calls whose work overlaps on the GPU (two streams, two host
 // threads) therefore race on it; callers serialise them.  The array keeps the
 // previous call's contents; only the panel status needs to start at zero and
@@ -948,13 +928,10 @@ constexpr size_t STATIC_GVAL_OFF = 1024;
 constexpr size_t STATIC_GIDX_OFF = STATIC_GVAL_OFF + 2 * STATIC_GRID * sizeof(double);
 constexpr size_t STATIC_GROWJ_OFF = 2048;
 constexpr size_t STATIC_GROW_OFF = STATIC_GROWJ_OFF + 2 * KB * sizeof(double2);
-constexpr size_t STATIC_ROWS_OFF = STATIC_GROW_OFF + (size_t)2 * STATIC_GRID * KB * sizeof(double2);
-constexpr size_t STATIC_SCRATCH_BYTES =
-    STATIC_ROWS_OFF + (size_t)2 * KB * NEC2C_CUDA_STATIC_LU_MAX_ORDER * sizeof(double2);
+constexpr size_t STATIC_SCRATCH_BYTES = STATIC_GROW_OFF + (size_t)2 * STATIC_GRID * KB * sizeof(double2);
 static_assert(sizeof(LuStatus) <= STATIC_PAIRS_OFF - STATIC_STATUS_OFF, "status slot");
 static_assert(4 * KB * sizeof(int) <= STATIC_GVAL_OFF - STATIC_PAIRS_OFF, "pairs slot");
 static_assert(STATIC_GIDX_OFF + 2 * STATIC_GRID * sizeof(int) <= STATIC_GROWJ_OFF, "grid candidates slot");
-static_assert(STATIC_ROWS_OFF % 256 == 0, "row buffer alignment");
 constexpr int STATIC_MAX_DEVICES = 64;
 std::mutex g_static_lock;
 unsigned char *g_static_addr[STATIC_MAX_DEVICES];
@@ -1004,7 +981,6 @@ extern "C" int nec2c_cuda_dense_factor_device_static(size_t order, nec2c_cuda_co
   w.gidx = (int *)(base + STATIC_GIDX_OFF);
   w.growj = (double2 *)(base + STATIC_GROWJ_OFF);
   w.grow = (double2 *)(base + STATIC_GROW_OFF);
-  w.tmp = (double2 *)(base + STATIC_ROWS_OFF);
   cudaError_t e = cudaMemsetAsync(w.st, 0, sizeof(LuStatus), n2c_stream());
   if (e != cudaSuccess) { n2c_set_error("clearing the panel status: %s", cudaGetErrorString(e)); return 0; }
   int info = 0;
