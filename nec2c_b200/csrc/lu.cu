@@ -826,32 +826,96 @@ struct FactorScratch {
 
 static int grid_blocks_for(long long n) { return (int)((n + PT - 1) / PT); }
 
+// Side stream of this thread (per device) for the look-ahead panel, created
+// with the highest priority so its CTAs are dispatched ahead of the trailing
+// update's as SMs free up.
+struct LookAhead {
+  int dev = -1;
+  cudaStream_t aux = nullptr;
+  cudaEvent_t next = nullptr, panel = nullptr;
+};
+static thread_local LookAhead g_look;
+
+static LookAhead *look_ahead() {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+  LookAhead &l = g_look;
+  if (l.dev == dev && l.aux) return &l;
+  if (l.aux) {
+    cudaStreamDestroy(l.aux);
+    cudaEventDestroy(l.next);
+    cudaEventDestroy(l.panel);
+    l = LookAhead();
+  }
+  int lo = 0, hi = 0;
+  cudaDeviceGetStreamPriorityRange(&lo, &hi);
+  if (cudaStreamCreateWithPriority(&l.aux, cudaStreamNonBlocking, hi) != cudaSuccess ||
+      cudaEventCreateWithFlags(&l.next, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&l.panel, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    n2c_set_error("look-ahead stream set-up failed");
+    return nullptr;
+  }
+  l.dev = dev;
+  return &l;
+}
+
+static int launch_gemm(double2 *a, long long ld, long long k0, int kb, long long c_first, long long cols,
+                       long long rows, cudaStream_t s) {
+  if (cols <= 0 || rows <= 0) return 1;
+  dim3 grid((unsigned)((cols + GT - 1) / GT), (unsigned)((rows + GT - 1) / GT));
+  gemm_update_kernel<<<grid, 256, 0, s>>>(a + (k0 + kb) * ld + c_first, a + (k0 + kb) * ld + k0,
+                                          a + k0 * ld + c_first, rows, cols, kb, ld);
+  return n2c_check_launch("gemm_update");
+}
+
 // The blocked factorisation; the status must be zero on entry.  Reads the
-// status back (synchronising the stream) and sets *info_host.
+// status back (synchronising the stream) and sets *info_host.  With look-ahead
+// the trailing update of each panel is split: the next panel's columns are
+// updated first, then that panel is factored on the side stream while the
+// rest of the update runs on the caller's stream (the two touch disjoint
+// columns); the next interchange waits for both.
 static int factor_panels(double2 *a, long long n, long long ld, int *ipiv, int rule, const FactorScratch &w,
-                         int *info_host) {
+                         bool lookahead, int *info_host) {
   cudaStream_t s = n2c_stream();
-  int ok = 1;
-  for (long long k0 = 0; ok && k0 < n; k0 += KB) {
-    const int kb = (int)(n - k0 < KB ? n - k0 : KB);
+  LookAhead *la = lookahead && n > KB ? look_ahead() : nullptr;
+  if (lookahead && n > KB && !la) return 0;
+  auto panel_args = [&](long long k0) {
     PanelArgs p;
     memset(&p, 0, sizeof(p));
-    p.a = a; p.n = n; p.ld = ld; p.k0 = k0; p.kb = kb; p.rule = rule; p.ipiv = ipiv;
+    p.a = a; p.n = n; p.ld = ld; p.k0 = k0; p.kb = (int)(n - k0 < KB ? n - k0 : KB); p.rule = rule; p.ipiv = ipiv;
     p.pairs = w.pairs; p.st = w.st; p.gval = w.gval; p.gidx = w.gidx; p.grow = w.grow; p.growj = w.growj;
-    if (!launch_panel(p, n - k0, s)) { ok = 0; break; }
+    return p;
+  };
+  int ok = launch_panel(panel_args(0), n, s);
+  for (long long k0 = 0; ok && k0 < n; k0 += KB) {
+    const int kb = (int)(n - k0 < KB ? n - k0 : KB);
     if (n > kb) {
       const unsigned gb = (unsigned)((n - kb + SWT / 32 - 1) / (SWT / 32));
       swap_trsm_kernel<<<gb, SWT, 0, s>>>(a, n, ld, k0, kb, w.pairs, w.st);
       if (!n2c_check_launch("interchanges and triangular solve")) { ok = 0; break; }
     }
     const long long right = n - k0 - kb;
-    if (right > 0) {
-      dim3 grid((unsigned)((right + GT - 1) / GT), (unsigned)((right + GT - 1) / GT));
-      gemm_update_kernel<<<grid, 256, 0, s>>>(a + (k0 + kb) * ld + (k0 + kb), a + (k0 + kb) * ld + k0,
-                                              a + k0 * ld + (k0 + kb), right, right, kb, ld);
-      if (!n2c_check_launch("gemm_update")) { ok = 0; break; }
+    if (right <= 0) break;
+    const long long c1 = k0 + kb;
+    // Cooperative grid panels (orders beyond the cluster's rows) need the
+    // whole device co-resident: those run in order on the caller's stream.
+    if (!la || right > cluster_rows()) {
+      if (!launch_gemm(a, ld, k0, kb, c1, right, right, s) || !launch_panel(panel_args(c1), right, s)) ok = 0;
+      continue;
     }
+    const long long nb = right < KB ? right : KB;
+    ok = launch_gemm(a, ld, k0, kb, c1, nb, right, s);
+    if (ok && (cudaEventRecord(la->next, s) != cudaSuccess || cudaStreamWaitEvent(la->aux, la->next, 0) != cudaSuccess)) {
+      n2c_set_error("look-ahead event");
+      ok = 0;
+    }
+    ok = ok && launch_panel(panel_args(c1), right, la->aux);
+    if (ok && cudaEventRecord(la->panel, la->aux) != cudaSuccess) { n2c_set_error("look-ahead event"); ok = 0; }
+    ok = ok && launch_gemm(a, ld, k0, kb, c1 + nb, right - nb, right, s);
+    if (ok && cudaStreamWaitEvent(s, la->panel, 0) != cudaSuccess) { n2c_set_error("look-ahead event"); ok = 0; }
   }
+  if (la && !ok) cudaStreamSynchronize(la->aux);
   LuStatus hs;
   memset(&hs, 0, sizeof(hs));
   cudaError_t e = cudaMemcpyAsync(&hs, w.st, sizeof(hs), cudaMemcpyDeviceToHost, s);
@@ -881,7 +945,7 @@ extern "C" int n2d_lu_factor(double *a_dev, long long n, long long ld, int *ipiv
   }
   int ok = w.st && w.pairs && n2d_memset(w.st, 0, sizeof(LuStatus)) &&
            (!grid || (w.gval && w.gidx && w.grow && w.growj));
-  ok = ok && factor_panels((double2 *)a_dev, n, ld, ipiv, rule, w, info_host);
+  ok = ok && factor_panels((double2 *)a_dev, n, ld, ipiv, rule, w, true, info_host);
   n2d_free(w.st); n2d_free(w.pairs);
   n2d_free(w.gval); n2d_free(w.gidx); n2d_free(w.grow); n2d_free(w.growj);
   return ok;
@@ -984,7 +1048,8 @@ extern "C" int nec2c_cuda_dense_factor_device_static(size_t order, nec2c_cuda_co
   cudaError_t e = cudaMemsetAsync(w.st, 0, sizeof(LuStatus), n2c_stream());
   if (e != cudaSuccess) { n2c_set_error("clearing the panel status: %s", cudaGetErrorString(e)); return 0; }
   int info = 0;
-  if (!factor_panels((double2 *)matrix_dev, (long long)order, (long long)leading_dimension, pivots_dev, 0, w, &info))
+  if (!factor_panels((double2 *)matrix_dev, (long long)order, (long long)leading_dimension, pivots_dev, 0, w, false,
+                     &info))
     return 0;
   if (info) { n2c_set_error("matrix is singular (pivot %d)", info); return 0; }
   return 1;
