@@ -167,6 +167,10 @@ int nec2c_cuda_dense_solve_row_major(nec2c_cuda_complex *matrix, nec2c_cuda_comp
                                      size_t order);
 /* Drops the device copies kept between a factor and its solves. */
 void nec2c_cuda_dense_release(void);
+/* No counterpart in the reference (diagnostic of the "cuda-mixed" form):
+   refinement steps the last split-precision solve took, -1 when it fell back
+   to an FP64 factorisation, 0 before any. */
+int nec2c_cuda_dense_last_refinement(void);
 /* No counterpart in the reference.  The classic factor above, for callers that
    must not allocate device memory during the call (a process whose GPU memory
    belongs to its own pool allocator, or a loop that cannot absorb cudaMalloc's

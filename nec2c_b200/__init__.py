@@ -79,6 +79,7 @@ def load():
         "nec2c_cuda_dense_backend_name": (C.c_char_p, []),
         "nec2c_cuda_dense_factor_classic": (i, [sz, vp, sz, vp]),
         "nec2c_cuda_dense_factor_device_static": (i, [sz, vp, sz, vp]),
+        "nec2c_cuda_dense_last_refinement": (i, []),
         "nec2c_cuda_dense_solve_classic": (i, [sz, vp, sz, vp, vp]),
         "nec2c_cuda_dense_solve_classic_many": (i, [sz, vp, sz, vp, vp, sz, sz]),
         "nec2c_cuda_dense_solve_row_major": (i, [vp, vp, sz]),

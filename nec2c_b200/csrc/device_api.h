@@ -107,23 +107,43 @@ int n2d_gmres_dev(int kind, void *op, long long n, const double *b_dev, double *
                   n2d_gmres_report *report);
 
 /* ---- dense LU (matrix.c factr/solve, dense_backend.c) ---- */
-/* Factor order x order in place on the device (column-major, leading dim ld),
+/* Factor order x order in place on the device: the algebraic matrix
+   row-major with leading dim ld (NEC's transposed column-major storage),
    partial pivoting.  rule 0: largest |.|^2, later row wins ties (factr);
    rule 1: largest |.|, first row wins, pivot must exceed 64 eps (row-major
-   builtin).  pivots_dev receives 1-based pivot rows.  precision 0 = FP64,
-   1 = split-FP32 tensor-core update (the caller refines). */
+   builtin).  pivots_dev receives 1-based pivot rows; *info_host the first
+   zero/rejected pivot (1-based) or 0.  precision is ignored (FP64). */
 int n2d_lu_factor(double *a_dev, long long order, long long ld, int *pivots_dev, int rule,
                   int precision, int *info_host);
+/* Split-precision form: the same factorisation of a complex FP32 matrix
+   (float pairs, ld even); panels and triangular solves compute in FP64, the
+   trailing update runs on the tensor cores (3xTF32). */
+int n2d_lu_factor32(float *a_dev, long long order, long long ld, int *pivots_dev, int rule, int *info_host);
 /* Solve with factors from n2d_lu_factor: interchanges + unit-lower forward +
    upper back substitution, for nrhs columns of b_dev (leading dim ldb). */
 int n2d_lu_solve(const double *a_dev, long long order, long long ld, const int *pivots_dev,
                  double *b_dev, long long ldb, long long nrhs);
+/* The same with FP32 factors (FP64 arithmetic and right-hand sides). */
+int n2d_lu_solve32(const float *a_dev, long long order, long long ld, const int *pivots_dev,
+                   double *b_dev, long long ldb, long long nrhs);
+/* Complex block copies between FP64 and FP32 (rows x cols, leading dims in
+   complex elements). */
+int n2d_narrow(const double *src_dev, long long lds, float *dst_dev, long long ldd, long long rows, long long cols);
+int n2d_widen(const float *src_dev, long long lds, double *dst_dev, long long ldd, long long rows, long long cols);
+/* Infinity norm of the row-major complex matrix (max row sum of |Re|+|Im|).
+   norm_dev: caller-owned device scratch of 8 bytes per column. */
+int n2d_norm_inf(const double *a_dev, long long order, long long ld, void *norm_dev, double *norm_host);
+/* Refinement step pieces for nrhs columns (leading dim ldb): r = b - A x with
+   A row-major (ld), and x += d; each reports per-column infinity norms
+   (|Re|+|Im|) of r and of the updated x into rnorm_host / xnorm_host. */
+int n2d_residual(const double *a_dev, long long order, long long ld, const double *x_dev,
+                 const double *b_dev, double *r_dev, long long nrhs, long long ldb, void *norm_dev,
+                 double *rnorm_host);
+int n2d_add_correction(double *x_dev, const double *d_dev, long long order, long long nrhs, long long ldb,
+                       void *norm_dev, double *xnorm_host);
 /* In-place device transpose of an order x order block (leading dims lda/ldb). */
 int n2d_transpose(const double *src_dev, long long lds, double *dst_dev, long long ldd,
                   long long rows, long long cols);
-/* r = b - A x for a column-major complex matrix (FP64), r may alias b. */
-int n2d_residual(const double *a_dev, long long order, long long ld, const double *x_dev,
-                 const double *b_dev, double *r_dev, long long nrhs, long long ldb);
 
 #ifdef __cplusplus
 }

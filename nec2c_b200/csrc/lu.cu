@@ -58,7 +58,7 @@ __device__ __forceinline__ double magnitude(double2 z, int rule) {
 }
 
 struct PanelArgs {
-  double2 *a;
+  void *a;                    // the matrix: double2 (FP64 form) or float2 (split-precision form)
   long long n, ld, k0;
   int kb, rule;
   int *ipiv;
@@ -385,7 +385,7 @@ __device__ __forceinline__ bool panel_column(const PanelArgs &p, PanelShared<CSZ
   return true;
 }
 
-template <int CSZ, int RULE>
+template <int CSZ, int RULE, typename S>
 __global__ void __launch_bounds__(CPT, 1) panel_cluster_kernel(PanelArgs p) {
   static_assert(sizeof(CandEntry) % 16 == 0 && CSZ <= 32 && CCW == 4 && KB == 32, "panel layout");
   cg::cluster_group cluster = cg::this_cluster();
@@ -411,10 +411,10 @@ __global__ void __launch_bounds__(CPT, 1) panel_cluster_kernel(PanelArgs p) {
   for (int k = 0; k < CRL; ++k) {
     const int g = rank * CROWS + lane + 32 * k;
     pos[k] = g < rows ? g : INT_MAX;
-    const double2 *row = p.a + (p.k0 + g) * p.ld + p.k0 + CCW * warp;
+    const S *row = (const S *)p.a + (p.k0 + g) * p.ld + p.k0 + CCW * warp;
 #pragma unroll
     for (int c = 0; c < CCW; ++c)
-      a[k][c] = (g < rows && CCW * warp + c < p.kb) ? row[c] : make_double2(0, 0);
+      a[k][c] = (g < rows && CCW * warp + c < p.kb) ? to_d(row[c]) : make_double2(0, 0);
   }
   bool ok = true;
   for (int wj = 0; wj < KB / CCW && ok; ++wj) {
@@ -432,9 +432,9 @@ __global__ void __launch_bounds__(CPT, 1) panel_cluster_kernel(PanelArgs p) {
 #pragma unroll
   for (int k = 0; k < CRL; ++k) {
     if (pos[k] == INT_MAX) continue;
-    double2 *row = p.a + (p.k0 + pos[k]) * p.ld + p.k0 + CCW * warp;
+    S *row = (S *)p.a + (p.k0 + pos[k]) * p.ld + p.k0 + CCW * warp;
 #pragma unroll
-    for (int c = 0; c < CCW; ++c) if (CCW * warp + c < p.kb) row[c] = a[k][c];
+    for (int c = 0; c < CCW; ++c) if (CCW * warp + c < p.kb) row[c] = from_d<S>(a[k][c]);
   }
   if (rank == 0 && warp == 0) {
     for (int j = lane; j < p.kb; j += 32) p.ipiv[p.k0 + j] = (int)(p.k0 + sh.piv[j] + 1);
@@ -474,14 +474,15 @@ __device__ bool lu_barrier(LuStatus *b) {
   return ok != 0;
 }
 
+template <typename S>
 __global__ void __launch_bounds__(PT) panel_grid_kernel(PanelArgs p) {
   const long long rows = p.n - p.k0;
   double2 a[1][KB];
   int g[1] = {(int)(blockIdx.x * PT + threadIdx.x)};
   bool have[1] = {g[0] < rows};
-  const double2 *row0 = p.a + (p.k0 + g[0]) * p.ld + p.k0;
+  const S *row0 = (const S *)p.a + (p.k0 + g[0]) * p.ld + p.k0;
 #pragma unroll
-  for (int c = 0; c < KB; ++c) a[0][c] = (have[0] && c < p.kb) ? row0[c] : make_double2(0, 0);
+  for (int c = 0; c < KB; ++c) a[0][c] = (have[0] && c < p.kb) ? to_d(row0[c]) : make_double2(0, 0);
   __shared__ int s_win;
   for (int j = 0; j < p.kb; ++j) {
     const int buf = j & 1;
@@ -532,9 +533,9 @@ __global__ void __launch_bounds__(PT) panel_grid_kernel(PanelArgs p) {
     __syncthreads();
   }
   if (!lu_barrier(p.st)) return;
-  double2 *row = p.a + (p.k0 + g[0]) * p.ld + p.k0;
+  S *row = (S *)p.a + (p.k0 + g[0]) * p.ld + p.k0;
 #pragma unroll
-  for (int c = 0; c < KB; ++c) if (have[0] && c < p.kb) row[c] = a[0][c];
+  for (int c = 0; c < KB; ++c) if (have[0] && c < p.kb) row[c] = from_d<S>(a[0][c]);
   if (blockIdx.x == 0 && threadIdx.x < 32) panel_pairs_warp(p);
 }
 
@@ -546,8 +547,14 @@ __global__ void __launch_bounds__(PT) panel_grid_kernel(PanelArgs p) {
 // by shuffle; each x_i subtracts L[i][k] x_k in increasing k, the order of the
 // row-oriented sum.
 constexpr int SWT = 256;   // threads per block (8 columns)
-__global__ void __launch_bounds__(SWT) swap_trsm_kernel(double2 *a, long long n, long long ld, long long k0, int kb,
-                                                        const int *pairs, const LuStatus *st) {
+// For the split-precision form (S = float2) the kernel also writes column c of
+// U12, as stored, into the packed real expansion the tensor-core update reads:
+// rows 2c', 2c'+1 (c' = c - k0 - kb) of 64 floats, (Re, -Im) and (Im, Re) per
+// k, each split into a TF32-representable hi part and the FP32 remainder.
+template <typename S>
+__global__ void __launch_bounds__(SWT) swap_trsm_kernel(S *a, long long n, long long ld, long long k0, int kb,
+                                                        const int *pairs, const LuStatus *st, float *bt_hi,
+                                                        float *bt_lo) {
   __shared__ int dst[2 * KB], src[2 * KB];
   __shared__ double2 L[KB][KB + 1];
   const int np = st->npairs;
@@ -558,7 +565,7 @@ __global__ void __launch_bounds__(SWT) swap_trsm_kernel(double2 *a, long long n,
   if (any_right) {
     for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
       const int i = t / kb, j = t % kb;
-      L[i][j] = a[(k0 + i) * ld + k0 + j];
+      L[i][j] = to_d(a[(k0 + i) * ld + k0 + j]);
     }
   }
   __syncthreads();
@@ -566,7 +573,7 @@ __global__ void __launch_bounds__(SWT) swap_trsm_kernel(double2 *a, long long n,
   const long long c0 = first + (threadIdx.x >> 5);
   if (c0 >= cols) return;
   const long long c = c0 < k0 ? c0 : c0 + kb;
-  double2 v0 = make_double2(0, 0), v1 = make_double2(0, 0);
+  S v0 = a[0], v1 = a[0];
   if (lane < np) v0 = a[(long long)src[lane] * ld + c];
   if (lane + 32 < np) v1 = a[(long long)src[lane + 32] * ld + c];
   __syncwarp();
@@ -574,7 +581,7 @@ __global__ void __launch_bounds__(SWT) swap_trsm_kernel(double2 *a, long long n,
   if (lane + 32 < np) a[(long long)dst[lane + 32] * ld + c] = v1;
   if (c < k0) return;
   __syncwarp();
-  double2 x = lane < kb ? a[(k0 + lane) * ld + c] : make_double2(0, 0);
+  double2 x = lane < kb ? to_d(a[(k0 + lane) * ld + c]) : make_double2(0, 0);
 #pragma unroll
   for (int k = 0; k < KB - 1; ++k) {
     double2 xk;
@@ -582,7 +589,21 @@ __global__ void __launch_bounds__(SWT) swap_trsm_kernel(double2 *a, long long n,
     xk.y = __shfl_sync(0xffffffffu, x.y, k);
     if (lane > k && lane < kb) x = csub(x, cmul(L[lane][k], xk));
   }
-  if (lane >= 1 && lane < kb) a[(k0 + lane) * ld + c] = x;
+  const S u = from_d<S>(x);
+  if (lane >= 1 && lane < kb) a[(k0 + lane) * ld + c] = u;
+  if (bt_hi) {
+    const long long r2 = 2 * (c - k0 - kb);
+    const double2 v = lane < kb ? to_d(u) : make_double2(0, 0);
+    const float re = (float)v.x, im = (float)v.y;
+    const float e[4] = {re, -im, im, re};   // row 2c' (k: Re, -Im), row 2c'+1 (k: Im, Re)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float h = __uint_as_float(__float_as_uint(e[q]) & 0xFFFFE000u);
+      const long long at = (r2 + (q >> 1)) * (2 * KB) + 2 * lane + (q & 1);
+      bt_hi[at] = h;
+      bt_lo[at] = e[q] - h;
+    }
+  }
 }
 
 // C[M x N] -= A[M x K] B[K x N], row-major complex FP64 blocks (leading dim ld).
@@ -645,7 +666,8 @@ __global__ void __launch_bounds__(256) gemm_update_kernel(double2 *C, const doub
 // matrix.c:1523-1555 solves).  One block per RHS; each 32-row step is solved
 // by warp 0 and the rows below / above are updated by the whole block with
 // contiguous row segments.
-__global__ void __launch_bounds__(1024) lu_solve_kernel(const double2 *a, long long n, long long ld,
+template <typename S>
+__global__ void __launch_bounds__(1024) lu_solve_kernel(const S *a, long long n, long long ld,
                                                         const int *ipiv, double2 *b, long long ldb) {
   double2 *x = b + blockIdx.x * ldb;
   __shared__ double2 xs[32];
@@ -663,7 +685,7 @@ __global__ void __launch_bounds__(1024) lu_solve_kernel(const double2 *a, long l
       double2 v = lane < w ? x[j0 + lane] : make_double2(0, 0);
       for (int i = 1; i < w; ++i) {
         // Row j0+i of the diagonal block against the solved entries above it.
-        const double2 l = lane < i ? a[(j0 + i) * ld + j0 + lane] : make_double2(0, 0);
+        const double2 l = lane < i ? to_d(a[(j0 + i) * ld + j0 + lane]) : make_double2(0, 0);
         double2 s = cmul(l, make_double2(__shfl_sync(0xffffffffu, v.x, lane), __shfl_sync(0xffffffffu, v.y, lane)));
         s = lane < i ? s : make_double2(0, 0);
         for (int o = 16; o > 0; o >>= 1) {
@@ -676,7 +698,7 @@ __global__ void __launch_bounds__(1024) lu_solve_kernel(const double2 *a, long l
     }
     __syncthreads();
     for (long long r = j0 + w + warp; r < n; r += nw) {
-      double2 s = lane < w ? cmul(a[r * ld + j0 + lane], xs[lane]) : make_double2(0, 0);
+      double2 s = lane < w ? cmul(to_d(a[r * ld + j0 + lane]), xs[lane]) : make_double2(0, 0);
       for (int o = 16; o > 0; o >>= 1) {
         s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
         s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
@@ -692,20 +714,20 @@ __global__ void __launch_bounds__(1024) lu_solve_kernel(const double2 *a, long l
     if (warp == 0) {
       double2 v = lane < w ? x[j0 + lane] : make_double2(0, 0);
       for (int i = w - 1; i >= 0; --i) {
-        const double2 u = (lane > i && lane < w) ? a[(j0 + i) * ld + j0 + lane] : make_double2(0, 0);
+        const double2 u = (lane > i && lane < w) ? to_d(a[(j0 + i) * ld + j0 + lane]) : make_double2(0, 0);
         double2 s = cmul(u, v);
         s = (lane > i && lane < w) ? s : make_double2(0, 0);
         for (int o = 16; o > 0; o >>= 1) {
           s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
           s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
         }
-        if (lane == i) v = cdiv(csub(v, s), a[(j0 + i) * ld + j0 + i]);
+        if (lane == i) v = cdiv(csub(v, s), to_d(a[(j0 + i) * ld + j0 + i]));
       }
       if (lane < w) { x[j0 + lane] = v; xs[lane] = v; }
     }
     __syncthreads();
     for (long long r = warp; r < j0; r += nw) {
-      double2 s = lane < w ? cmul(a[r * ld + j0 + lane], xs[lane]) : make_double2(0, 0);
+      double2 s = lane < w ? cmul(to_d(a[r * ld + j0 + lane]), xs[lane]) : make_double2(0, 0);
       for (int o = 16; o > 0; o >>= 1) {
         s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
         s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
@@ -743,9 +765,9 @@ extern "C" int n2d_transpose(const double *src, long long lds, double *dst, long
 // Panel launch: the smallest cluster of 256-thread CTAs that holds the
 // panel's rows (16-CTA clusters where the device allows that non-portable
 // size), else the cooperative grid panel.
-template <int CSZ>
+template <int CSZ, typename S>
 static cudaError_t launch_cluster_panel(const PanelArgs &p, cudaStream_t s) {
-  void (*kernel)(PanelArgs) = p.rule == 0 ? panel_cluster_kernel<CSZ, 0> : panel_cluster_kernel<CSZ, 1>;
+  void (*kernel)(PanelArgs) = p.rule == 0 ? panel_cluster_kernel<CSZ, 0, S> : panel_cluster_kernel<CSZ, 1, S>;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(CSZ);
   cfg.blockDim = dim3(CPT);
@@ -765,12 +787,13 @@ static int cluster16_ok() {
   static int state = -1;
   if (state >= 0) return state;
   state = 0;
-  if (cudaFuncSetAttribute(panel_cluster_kernel<CMAX, 0>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
-          cudaSuccess ||
-      cudaFuncSetAttribute(panel_cluster_kernel<CMAX, 1>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
-          cudaSuccess) {
-    cudaGetLastError();
-    return state;
+  void (*kernels[4])(PanelArgs) = {panel_cluster_kernel<CMAX, 0, double2>, panel_cluster_kernel<CMAX, 1, double2>,
+                                   panel_cluster_kernel<CMAX, 0, float2>, panel_cluster_kernel<CMAX, 1, float2>};
+  for (auto k : kernels) {
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+      cudaGetLastError();
+      return state;
+    }
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(CMAX);
@@ -783,7 +806,7 @@ static int cluster16_ok() {
   cfg.attrs = at;
   cfg.numAttrs = 1;
   int clusters = 0;
-  if (cudaOccupancyMaxActiveClusters(&clusters, panel_cluster_kernel<CMAX, 0>, &cfg) == cudaSuccess && clusters > 0)
+  if (cudaOccupancyMaxActiveClusters(&clusters, panel_cluster_kernel<CMAX, 0, double2>, &cfg) == cudaSuccess && clusters > 0)
     state = 1;
   cudaGetLastError();
   return state;
@@ -792,18 +815,19 @@ static int cluster16_ok() {
 // Largest panel row count the cluster kernel takes on this device.
 static long long cluster_rows() { return (long long)CROWS * (cluster16_ok() ? CMAX : 8); }
 
+template <typename S>
 static int launch_panel(const PanelArgs &p, long long rows, cudaStream_t s) {
   cudaError_t e;
   if (rows <= cluster_rows()) {
-    if (rows <= CROWS) e = launch_cluster_panel<1>(p, s);
-    else if (rows <= 2 * CROWS) e = launch_cluster_panel<2>(p, s);
-    else if (rows <= 4 * CROWS) e = launch_cluster_panel<4>(p, s);
-    else if (rows <= 8 * CROWS) e = launch_cluster_panel<8>(p, s);
-    else e = launch_cluster_panel<CMAX>(p, s);
+    if (rows <= CROWS) e = launch_cluster_panel<1, S>(p, s);
+    else if (rows <= 2 * CROWS) e = launch_cluster_panel<2, S>(p, s);
+    else if (rows <= 4 * CROWS) e = launch_cluster_panel<4, S>(p, s);
+    else if (rows <= 8 * CROWS) e = launch_cluster_panel<8, S>(p, s);
+    else e = launch_cluster_panel<CMAX, S>(p, s);
   } else {
     const int blocks = (int)((rows + PT - 1) / PT);
     void *args[] = {const_cast<PanelArgs *>(&p)};
-    e = cudaLaunchCooperativeKernel((void *)panel_grid_kernel, blocks, PT, args, 0, s);
+    e = cudaLaunchCooperativeKernel((void *)panel_grid_kernel<S>, blocks, PT, args, 0, s);
   }
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -819,6 +843,7 @@ static int launch_panel(const PanelArgs &p, long long rows, cudaStream_t s) {
 struct FactorScratch {
   LuStatus *st;
   int *pairs;
+  float *bt_hi, *bt_lo;       // split-precision form: packed U12 expansion (2n x 64 floats each)
   double *gval;
   int *gidx;
   double2 *grow, *growj;
@@ -860,13 +885,23 @@ static LookAhead *look_ahead() {
   return &l;
 }
 
+// Trailing update of columns [c_first, c_first + cols) for rows below the
+// panel: FP64 tiles on the FP64 pipe, or the split-precision form on the
+// tensor cores (U12 from the packed expansion).
 static int launch_gemm(double2 *a, long long ld, long long k0, int kb, long long c_first, long long cols,
-                       long long rows, cudaStream_t s) {
+                       long long rows, const FactorScratch &, cudaStream_t s) {
   if (cols <= 0 || rows <= 0) return 1;
   dim3 grid((unsigned)((cols + GT - 1) / GT), (unsigned)((rows + GT - 1) / GT));
   gemm_update_kernel<<<grid, 256, 0, s>>>(a + (k0 + kb) * ld + c_first, a + (k0 + kb) * ld + k0,
                                           a + k0 * ld + c_first, rows, cols, kb, ld);
   return n2c_check_launch("gemm_update");
+}
+static int launch_gemm(float2 *a, long long ld, long long k0, int kb, long long c_first, long long cols,
+                       long long rows, const FactorScratch &w, cudaStream_t s) {
+  if (cols <= 0 || rows <= 0) return 1;
+  const long long r2 = 2 * (c_first - k0 - kb);
+  return n2c_tc_update((float *)(a + (k0 + kb) * ld + c_first), ld, (const float *)(a + (k0 + kb) * ld + k0), ld,
+                       w.bt_hi + r2 * (2 * KB), w.bt_lo + r2 * (2 * KB), rows, cols, &w.st->error, s);
 }
 
 // The blocked factorisation; the status must be zero on entry.  Reads the
@@ -875,8 +910,9 @@ static int launch_gemm(double2 *a, long long ld, long long k0, int kb, long long
 // updated first, then that panel is factored on the side stream while the
 // rest of the update runs on the caller's stream (the two touch disjoint
 // columns); the next interchange waits for both.
-static int factor_panels(double2 *a, long long n, long long ld, int *ipiv, int rule, const FactorScratch &w,
-                         bool lookahead, int *info_host) {
+template <typename S>
+static int factor_panels(S *a, long long n, long long ld, int *ipiv, int rule, const FactorScratch &w, bool lookahead,
+                         int *info_host) {
   cudaStream_t s = n2c_stream();
   LookAhead *la = lookahead && n > KB ? look_ahead() : nullptr;
   if (lookahead && n > KB && !la) return 0;
@@ -887,12 +923,12 @@ static int factor_panels(double2 *a, long long n, long long ld, int *ipiv, int r
     p.pairs = w.pairs; p.st = w.st; p.gval = w.gval; p.gidx = w.gidx; p.grow = w.grow; p.growj = w.growj;
     return p;
   };
-  int ok = launch_panel(panel_args(0), n, s);
+  int ok = launch_panel<S>(panel_args(0), n, s);
   for (long long k0 = 0; ok && k0 < n; k0 += KB) {
     const int kb = (int)(n - k0 < KB ? n - k0 : KB);
     if (n > kb) {
       const unsigned gb = (unsigned)((n - kb + SWT / 32 - 1) / (SWT / 32));
-      swap_trsm_kernel<<<gb, SWT, 0, s>>>(a, n, ld, k0, kb, w.pairs, w.st);
+      swap_trsm_kernel<S><<<gb, SWT, 0, s>>>(a, n, ld, k0, kb, w.pairs, w.st, w.bt_hi, w.bt_lo);
       if (!n2c_check_launch("interchanges and triangular solve")) { ok = 0; break; }
     }
     const long long right = n - k0 - kb;
@@ -901,18 +937,18 @@ static int factor_panels(double2 *a, long long n, long long ld, int *ipiv, int r
     // Cooperative grid panels (orders beyond the cluster's rows) need the
     // whole device co-resident: those run in order on the caller's stream.
     if (!la || right > cluster_rows()) {
-      if (!launch_gemm(a, ld, k0, kb, c1, right, right, s) || !launch_panel(panel_args(c1), right, s)) ok = 0;
+      if (!launch_gemm(a, ld, k0, kb, c1, right, right, w, s) || !launch_panel<S>(panel_args(c1), right, s)) ok = 0;
       continue;
     }
     const long long nb = right < KB ? right : KB;
-    ok = launch_gemm(a, ld, k0, kb, c1, nb, right, s);
+    ok = launch_gemm(a, ld, k0, kb, c1, nb, right, w, s);
     if (ok && (cudaEventRecord(la->next, s) != cudaSuccess || cudaStreamWaitEvent(la->aux, la->next, 0) != cudaSuccess)) {
       n2c_set_error("look-ahead event");
       ok = 0;
     }
-    ok = ok && launch_panel(panel_args(c1), right, la->aux);
+    ok = ok && launch_panel<S>(panel_args(c1), right, la->aux);
     if (ok && cudaEventRecord(la->panel, la->aux) != cudaSuccess) { n2c_set_error("look-ahead event"); ok = 0; }
-    ok = ok && launch_gemm(a, ld, k0, kb, c1 + nb, right - nb, right, s);
+    ok = ok && launch_gemm(a, ld, k0, kb, c1 + nb, right - nb, right, w, s);
     if (ok && cudaStreamWaitEvent(s, la->panel, 0) != cudaSuccess) { n2c_set_error("look-ahead event"); ok = 0; }
   }
   if (la && !ok) cudaStreamSynchronize(la->aux);
@@ -921,16 +957,18 @@ static int factor_panels(double2 *a, long long n, long long ld, int *ipiv, int r
   cudaError_t e = cudaMemcpyAsync(&hs, w.st, sizeof(hs), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (ok && e != cudaSuccess) { n2c_set_error("reading the panel status: %s", cudaGetErrorString(e)); ok = 0; }
-  if (ok && hs.error) { n2c_set_error("LU panel exchange time-out"); ok = 0; }
+  if (ok && hs.error) { n2c_set_error("LU kernel wait time-out"); ok = 0; }
   *info_host = hs.info;
   return ok;
 }
 
-extern "C" int n2d_lu_factor(double *a_dev, long long n, long long ld, int *ipiv, int rule, int precision,
-                             int *info_host) {
-  (void)precision;
+// Scratch allocation around factor_panels; the split-precision form also
+// holds the packed U12 expansion.
+template <typename S>
+static int factor_alloc(S *a, long long n, long long ld, int *ipiv, int rule, int *info_host) {
   *info_host = 0;
   if (n <= 0) return 1;
+  const bool split = sizeof(S) == sizeof(float2);
   FactorScratch w;
   memset(&w, 0, sizeof(w));
   w.st = (LuStatus *)n2d_alloc(sizeof(LuStatus));
@@ -943,19 +981,48 @@ extern "C" int n2d_lu_factor(double *a_dev, long long n, long long ld, int *ipiv
     w.grow = (double2 *)n2d_alloc((size_t)2 * gb * KB * sizeof(double2));
     w.growj = (double2 *)n2d_alloc(2 * KB * sizeof(double2));
   }
+  if (split) {
+    w.bt_hi = (float *)n2d_alloc((size_t)2 * n * 2 * KB * sizeof(float));
+    w.bt_lo = (float *)n2d_alloc((size_t)2 * n * 2 * KB * sizeof(float));
+  }
   int ok = w.st && w.pairs && n2d_memset(w.st, 0, sizeof(LuStatus)) &&
-           (!grid || (w.gval && w.gidx && w.grow && w.growj));
-  ok = ok && factor_panels((double2 *)a_dev, n, ld, ipiv, rule, w, true, info_host);
+           (!grid || (w.gval && w.gidx && w.grow && w.growj)) && (!split || (w.bt_hi && w.bt_lo));
+  ok = ok && factor_panels(a, n, ld, ipiv, rule, w, true, info_host);
   n2d_free(w.st); n2d_free(w.pairs);
   n2d_free(w.gval); n2d_free(w.gidx); n2d_free(w.grow); n2d_free(w.growj);
+  n2d_free(w.bt_hi); n2d_free(w.bt_lo);
   return ok;
+}
+
+extern "C" int n2d_lu_factor(double *a_dev, long long n, long long ld, int *ipiv, int rule, int precision,
+                             int *info_host) {
+  (void)precision;
+  return factor_alloc((double2 *)a_dev, n, ld, ipiv, rule, info_host);
+}
+
+extern "C" int n2d_lu_factor32(float *a_dev, long long n, long long ld, int *ipiv, int rule, int *info_host) {
+  if (ld & 1) {
+    n2c_set_error("split-precision LU needs an even leading dimension");
+    return 0;
+  }
+  return factor_alloc((float2 *)a_dev, n, ld, ipiv, rule, info_host);
 }
 
 extern "C" int n2d_lu_solve(const double *a_dev, long long n, long long ld, const int *ipiv, double *b_dev,
                             long long ldb, long long nrhs) {
   if (n <= 0 || nrhs <= 0) return 1;
-  lu_solve_kernel<<<(unsigned)nrhs, 1024, 0, n2c_stream()>>>((const double2 *)a_dev, n, ld, ipiv,
+  lu_solve_kernel<double2><<<(unsigned)nrhs, 1024, 0, n2c_stream()>>>((const double2 *)a_dev, n, ld, ipiv,
                                                              (double2 *)b_dev, ldb);
+  return n2c_check_launch("lu_solve");
+}
+
+// Solve with FP32 factors (split-precision form); the arithmetic and the
+// right-hand sides are FP64.
+extern "C" int n2d_lu_solve32(const float *a_dev, long long n, long long ld, const int *ipiv, double *b_dev,
+                              long long ldb, long long nrhs) {
+  if (n <= 0 || nrhs <= 0) return 1;
+  lu_solve_kernel<float2><<<(unsigned)nrhs, 1024, 0, n2c_stream()>>>((const float2 *)a_dev, n, ld, ipiv,
+                                                                     (double2 *)b_dev, ldb);
   return n2c_check_launch("lu_solve");
 }
 
@@ -1039,6 +1106,7 @@ extern "C" int nec2c_cuda_dense_factor_device_static(size_t order, nec2c_cuda_co
   unsigned char *base = static_scratch();
   if (!base) return 0;
   FactorScratch w;
+  memset(&w, 0, sizeof(w));
   w.st = (LuStatus *)(base + STATIC_STATUS_OFF);
   w.pairs = (int *)(base + STATIC_PAIRS_OFF);
   w.gval = (double *)(base + STATIC_GVAL_OFF);

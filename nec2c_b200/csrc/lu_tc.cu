@@ -1,0 +1,239 @@
+// Trailing update of the split-precision LU on the 5th-generation tensor
+// cores: C -= A B for complex FP32 blocks, C (M x N) and A (M x KB) row-major
+// in the working matrix, B given as the packed real expansion of U12.
+//
+// A complex product is one real product over interleaved (re, im) values:
+// with A read as an M x 2KB real matrix and B expanded to the 2KB x 2N real
+// matrix [[Br, Bi], [-Bi, Br]] per (k, n) pair, the real result's columns
+// 2n, 2n+1 are Re and Im of the complex C.  The expansion is stored K-major,
+// one 2KB-float row per real column (Bt), split into hi and lo parts.
+//
+// Precision: every operand x is split as x = hi + lo with hi holding the top
+// 11 significant bits (TF32-representable, low 13 mantissa bits cleared) and
+// lo = x - hi exact in FP32; D = Ahi Bhi + Ahi Blo + Alo Bhi accumulates in
+// FP32 in tensor memory (3xTF32), close to an FP32 product.
+//
+// One CTA per 128-row x 128-complex-column tile, 128 threads: the threads
+// stage A (split on the fly) and Bt (pre-split) into 128B-swizzled shared
+// memory, one elected thread issues the 24 tcgen05.mma (8 K-steps x 3
+// products, M=128 N=256 K=8), tcgen05.commit signals an mbarrier, and the
+// four warps read their 32 tensor-memory lanes back (tcgen05.ld) and update C.
+// No cluster, no multicast.
+#include <stdint.h>
+#include <string.h>
+#include "common.cuh"
+#include "device_api.h"
+#include "runtime.cuh"
+
+namespace {
+
+constexpr int TM = 128;             // tile rows
+constexpr int TNC = 128;            // tile complex columns
+constexpr int TN = 2 * TNC;         // tile real columns (MMA N)
+constexpr int KR = 64;              // real K (2 x panel width 32)
+constexpr int ATOM_ROW = 128;       // bytes per swizzle-atom row (32 floats)
+constexpr int KATOMS = KR * 4 / ATOM_ROW;   // 2 atoms along K
+constexpr int A_BYTES = KATOMS * TM * ATOM_ROW;   // 32 KB
+constexpr int B_BYTES = KATOMS * TN * ATOM_ROW;   // 64 KB
+constexpr int SMEM_BYTES = 2 * A_BYTES + 2 * B_BYTES + 1024;   // + alignment slack
+constexpr int THREADS = 128;
+constexpr uint32_t TMEM_COLS = 256;
+
+__device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Byte offset of 16-byte chunk c (0..15 along K) of row r in a K-major
+// operand region of `rows` rows: K atoms of rows x 128 B, 128B swizzle
+// (chunk index XOR row mod 8 within each 1024-byte group of 8 rows).
+__device__ __forceinline__ uint32_t swz(int r, int c, int rows) {
+  const int atom = c >> 3, cc = c & 7;
+  return (uint32_t)(atom * rows * ATOM_ROW + r * ATOM_ROW + ((cc ^ (r & 7)) << 4));
+}
+
+// Shared-memory matrix descriptor: K-major, 128B swizzle, 8-row groups 1024 B
+// apart, descriptor version 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
+  return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// Instruction descriptor, kind::tf32: D F32, A and B TF32, both K-major.
+constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n"
+      :: "r"(tmem), "l"(a), "l"(b), "r"(IDESC), "r"(accumulate));
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+               : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+  return ok != 0;
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+gemm_tf32x3_kernel(float2 *C, long long ldc, const float2 *A, long long lda, const float *bt_hi, const float *bt_lo,
+                   long long M, long long N, int *error) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ uint32_t tmem_base;
+  __shared__ __align__(8) unsigned long long done_bar;
+  unsigned char *sm = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char *a_hi = sm, *a_lo = sm + A_BYTES, *b_hi = sm + 2 * A_BYTES, *b_lo = sm + 2 * A_BYTES + B_BYTES;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long r0 = (long long)blockIdx.y * TM, c0 = (long long)blockIdx.x * TNC;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(&tmem_base)), "r"(TMEM_COLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&done_bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // A: TM rows x 16 chunks of 4 floats, split on the fly.
+  for (int q = tid; q < TM * 16; q += THREADS) {
+    const int r = q >> 4, c = q & 15;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (r0 + r < M) v = *reinterpret_cast<const float4 *>(reinterpret_cast<const float *>(A + (r0 + r) * lda) + 4 * c);
+    const float4 h = make_float4(tf32_hi(v.x), tf32_hi(v.y), tf32_hi(v.z), tf32_hi(v.w));
+    const float4 l = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+    const uint32_t off = swz(r, c, TM);
+    *reinterpret_cast<float4 *>(a_hi + off) = h;
+    *reinterpret_cast<float4 *>(a_lo + off) = l;
+  }
+  // Bt: TN real rows x 16 chunks, hi and lo as stored.
+  for (int q = tid; q < TN * 16; q += THREADS) {
+    const int r = q >> 4, c = q & 15;
+    const long long gr = 2 * c0 + r;
+    float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
+    if (gr < 2 * N) {
+      h = *reinterpret_cast<const float4 *>(bt_hi + gr * KR + 4 * c);
+      l = *reinterpret_cast<const float4 *>(bt_lo + gr * KR + 4 * c);
+    }
+    const uint32_t off = swz(r, c, TN);
+    *reinterpret_cast<float4 *>(b_hi + off) = h;
+    *reinterpret_cast<float4 *>(b_lo + off) = l;
+  }
+  // Generic-proxy shared-memory writes become visible to the tensor cores.
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  if (tid == 0) {
+    const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo), bh = smem_u32(b_hi), bl = smem_u32(b_lo);
+    uint32_t acc = 0;
+    // 8 K-steps of 8 TF32 values (32 bytes): 4 per swizzle atom.
+#pragma unroll
+    for (int k = 0; k < KR / 8; ++k) {
+      const uint32_t ao = (uint32_t)((k >> 2) * TM * ATOM_ROW + (k & 3) * 32);
+      const uint32_t bo = (uint32_t)((k >> 2) * TN * ATOM_ROW + (k & 3) * 32);
+      mma_tf32(tmem, sdesc(al + ao), sdesc(bh + bo), acc);
+      acc = 1;
+      mma_tf32(tmem, sdesc(ah + ao), sdesc(bl + bo), 1);
+    }
+#pragma unroll
+    for (int k = 0; k < KR / 8; ++k) {
+      const uint32_t ao = (uint32_t)((k >> 2) * TM * ATOM_ROW + (k & 3) * 32);
+      const uint32_t bo = (uint32_t)((k >> 2) * TN * ATOM_ROW + (k & 3) * 32);
+      mma_tf32(tmem, sdesc(ah + ao), sdesc(bh + bo), 1);
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(smem_u32(&done_bar)) : "memory");
+  }
+  // Bounded wait for the products (about a second at boost clock).
+  bool ok = true;
+  {
+    const uint32_t bar = smem_u32(&done_bar);
+    const long long t0 = clock64();
+    while (!mbar_try(bar, 0)) {
+      if (clock64() - t0 > (1LL << 31)) { ok = false; break; }
+    }
+  }
+  // Every thread takes the same path (tcgen05.ld is warp-aligned).
+  ok = __syncthreads_and(ok) != 0;
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    const long long row = r0 + warp * 32 + lane;
+    float2 *crow = C + row * ldc + c0;
+#pragma unroll 1
+    for (int j = 0; j < TN / 32; ++j) {
+      uint32_t d[32];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * 32);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14,"
+          " %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+            "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]),
+            "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]), "=r"(d[23]),
+            "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < M) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const long long col = c0 + j * 16 + q;
+          if (col < N) {
+            float2 cv = crow[j * 16 + q];
+            cv.x -= __uint_as_float(d[2 * q]);
+            cv.y -= __uint_as_float(d[2 * q + 1]);
+            crow[j * 16 + q] = cv;
+          }
+        }
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(error, 1);
+    // Give the products in flight another bounded wait before the memory is freed.
+    const uint32_t bar = smem_u32(&done_bar);
+    const long long t0 = clock64();
+    while (!mbar_try(bar, 0) && clock64() - t0 < (1LL << 31)) {
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TMEM_COLS) : "memory");
+  }
+}
+
+}  // namespace
+
+// C (M x N complex FP32, row-major, leading dimension ldc in complex units)
+// -= A (M x 32, lda) times the complex 32 x N block whose packed expansion is
+// bt_hi + bt_lo (2N rows of 64 floats).  A's rows must start 16-byte aligned
+// (lda even, A 16-byte aligned).  error: device int set to 1 on a time-out.
+int n2c_tc_update(float *C, long long ldc, const float *A, long long lda, const float *bt_hi, const float *bt_lo,
+                  long long M, long long N, int *error, cudaStream_t s) {
+  if (M <= 0 || N <= 0) return 1;
+  if ((lda & 1) || ((uintptr_t)A & 15) || ((uintptr_t)bt_hi & 15) || ((uintptr_t)bt_lo & 15)) {
+    n2c_set_error("tensor-core update: operand rows must start 16-byte aligned");
+    return 0;
+  }
+  static int configured = 0;
+  if (!configured) {
+    if (cudaFuncSetAttribute(gemm_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) !=
+        cudaSuccess) {
+      n2c_set_error("tensor-core update: shared memory configuration failed");
+      return 0;
+    }
+    configured = 1;
+  }
+  dim3 grid((unsigned)((N + TNC - 1) / TNC), (unsigned)((M + TM - 1) / TM));
+  gemm_tf32x3_kernel<<<grid, THREADS, SMEM_BYTES, s>>>((float2 *)C, ldc, (const float2 *)A, lda, bt_hi, bt_lo, M, N,
+                                                       error);
+  return n2c_check_launch("tensor-core update");
+}
+
+extern "C" int n2d_gemm_tf32x3(float *C, long long ldc, const float *A, long long lda, const float *bt_hi,
+                               const float *bt_lo, long long M, long long N, int *error) {
+  return n2c_tc_update(C, ldc, A, lda, bt_hi, bt_lo, M, N, error, n2c_stream());
+}

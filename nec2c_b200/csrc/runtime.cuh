@@ -10,6 +10,10 @@ void n2c_count_launch(unsigned n);
 // Checks cudaGetLastError after a launch; counts the launch on success.
 int n2c_check_launch(const char *what);
 int n2c_sm_count();
+// Split-precision (3xTF32) tensor-core trailing update of the FP32 LU on
+// stream s; see lu_tc.cu.
+int n2c_tc_update(float *C, long long ldc, const float *A, long long lda, const float *bt_hi, const float *bt_lo,
+                  long long M, long long N, int *error, cudaStream_t s);
 
 // Deterministic block-partial reduction: each block stores its partial in
 // partials[blockIdx.x]; the block that arrives last (ticket counter) sums the

@@ -29,17 +29,24 @@ const char *nec2c_cuda_dense_backend_name(void) { return g_dense_mixed ? "cuda-m
 static struct {
   const void *host;      /* host matrix the factors were written to */
   size_t order, ld;
-  double *lu_dev;        /* column-major LU, leading dimension order */
+  double *lu_dev;        /* FP64 form: row-major LU, leading dim order */
   int *piv_dev;
-  double *orig_dev;      /* mixed form: the unfactored matrix (for refinement) */
+  float *lu32_dev;       /* split form: FP32 LU, leading dim ld32 (even) */
+  size_t ld32;
+  double *orig_dev;      /* split form: the FP64 matrix (refinement residuals) */
+  double anorm;          /* split form: its infinity norm */
   int mixed;
 } g_cache;
 
+static int g_last_refinement = 0;
+
 void nec2c_cuda_dense_release(void)
 {
-  n2d_free(g_cache.lu_dev); n2d_free(g_cache.piv_dev); n2d_free(g_cache.orig_dev);
+  n2d_free(g_cache.lu_dev); n2d_free(g_cache.piv_dev); n2d_free(g_cache.lu32_dev); n2d_free(g_cache.orig_dev);
   memset(&g_cache, 0, sizeof(g_cache));
 }
+
+int nec2c_cuda_dense_last_refinement(void) { return g_last_refinement; }
 
 static const size_t CPX = 2 * sizeof(double);
 
@@ -54,10 +61,34 @@ static double *upload_matrix(const void *matrix, size_t n, size_t ld)
   return a;
 }
 
+/* Split-precision factorisation of the uploaded matrix a (kept as the
+   refinement original): FP32 copy, tensor-core LU, FP32 factors widened back
+   into the host storage. */
+static int factor_split(double *a, size_t n, size_t ld, int *piv, nec2c_cuda_complex *matrix, int *pivots)
+{
+  const size_t ld32 = n + (n & 1);
+  float *lu32 = n2d_alloc(n * ld32 * 2 * sizeof(float));
+  double *wide = NULL;
+  void *norm = n2d_alloc(sizeof(unsigned long long));
+  double anorm = 0;
+  int info = 0;
+  int ok = lu32 && norm && n2d_narrow(a, (long long)n, lu32, (long long)ld32, (long long)n, (long long)n) &&
+           n2d_norm_inf(a, (long long)n, (long long)n, norm, &anorm) &&
+           n2d_lu_factor32(lu32, (long long)n, (long long)ld32, piv, 0, &info);
+  if(ok && info) { n2c_set_error("matrix is singular (pivot %d)", info); ok = 0; }
+  wide = ok ? n2d_alloc(n * n * CPX) : NULL;
+  ok = ok && wide && n2d_widen(lu32, (long long)ld32, wide, (long long)n, (long long)n, (long long)n) &&
+       n2d_download2d(matrix, ld * CPX, wide, n * CPX, n * CPX, n) && n2d_download(pivots, piv, n * sizeof(int));
+  n2d_free(wide); n2d_free(norm);
+  if(!ok) { n2d_free(lu32); return 0; }
+  g_cache.lu32_dev = lu32; g_cache.ld32 = ld32; g_cache.orig_dev = a; g_cache.anorm = anorm;
+  return 1;
+}
+
 int nec2c_cuda_dense_factor_classic(size_t n, nec2c_cuda_complex *matrix, size_t ld, int *pivots)
 {
   int info = 0, ok;
-  double *a, *orig = NULL;
+  double *a;
   int *piv;
   if(!matrix || !pivots || n == 0 || n > INT_MAX || ld < n || ld > INT_MAX) return 0;
   if(!n2d_device_ok()) return 0;
@@ -66,16 +97,56 @@ int nec2c_cuda_dense_factor_classic(size_t n, nec2c_cuda_complex *matrix, size_t
   piv = n2d_alloc(n * sizeof(int));
   if(!a || !piv) { n2d_free(a); n2d_free(piv); return 0; }
   if(g_dense_mixed) {
-    orig = n2d_alloc(n * n * CPX);
-    if(!orig || !n2d_copy_d2d(orig, a, n * n * CPX)) { n2d_free(a); n2d_free(piv); n2d_free(orig); return 0; }
+    if(!factor_split(a, n, ld, piv, matrix, pivots)) { n2d_free(a); n2d_free(piv); return 0; }
+    g_cache.host = matrix; g_cache.order = n; g_cache.ld = ld; g_cache.piv_dev = piv; g_cache.mixed = 1;
+    return 1;
   }
-  ok = n2d_lu_factor(a, (long long)n, (long long)n, piv, 0, g_dense_mixed, &info);
+  ok = n2d_lu_factor(a, (long long)n, (long long)n, piv, 0, 0, &info);
   ok = ok && n2d_download2d(matrix, ld * CPX, a, n * CPX, n * CPX, n) &&
        n2d_download(pivots, piv, n * sizeof(int));
-  if(!ok || info) { n2d_free(a); n2d_free(piv); n2d_free(orig); if(ok && info) n2c_set_error("matrix is singular (pivot %d)", info); return 0; }
+  if(!ok || info) { n2d_free(a); n2d_free(piv); if(ok && info) n2c_set_error("matrix is singular (pivot %d)", info); return 0; }
   g_cache.host = matrix; g_cache.order = n; g_cache.ld = ld;
-  g_cache.lu_dev = a; g_cache.piv_dev = piv; g_cache.orig_dev = orig; g_cache.mixed = g_dense_mixed;
+  g_cache.lu_dev = a; g_cache.piv_dev = piv; g_cache.mixed = 0;
   return 1;
+}
+
+/* Refined solve with the cached split-precision factors (the iteration of
+   LAPACK's mixed-precision zcgesv): x = 0, r = b; repeat d = LU32 \ r,
+   x += d, r = b - A x until every column has ||r||_inf <= ||x||_inf ||A||_inf
+   eps sqrt(n), at most 30 steps; otherwise an FP64 factorisation solves it. */
+static int solve_refined(size_t n, double *b, size_t count)
+{
+  const long long N = (long long)n, K = (long long)count;
+  const double cte = g_cache.anorm * DBL_EPSILON * sqrt((double)n);
+  double *x = n2d_alloc(n * count * CPX), *r = n2d_alloc(n * count * CPX), *d = n2d_alloc(n * count * CPX);
+  void *norm = n2d_alloc(count * sizeof(unsigned long long));
+  double *rn = malloc(count * sizeof(double)), *xn = malloc(count * sizeof(double));
+  int ok = x && r && d && norm && rn && xn && n2d_memset(x, 0, n * count * CPX) && n2d_copy_d2d(r, b, n * count * CPX);
+  int done = 0, it;
+  for(it = 1; ok && it <= 30 && !done; ++it) {
+    size_t j;
+    ok = n2d_copy_d2d(d, r, n * count * CPX) &&
+         n2d_lu_solve32(g_cache.lu32_dev, N, (long long)g_cache.ld32, g_cache.piv_dev, d, N, K) &&
+         n2d_add_correction(x, d, N, K, N, norm, xn) &&
+         n2d_residual(g_cache.orig_dev, N, N, x, b, r, K, N, norm, rn);
+    done = ok;
+    for(j = 0; ok && j < count; ++j) if(!(rn[j] <= xn[j] * cte)) done = 0;
+    if(done) g_last_refinement = it;
+  }
+  if(ok && !done) {
+    /* Not converged: FP64 factorisation of a copy of the original. */
+    double *a = n2d_alloc(n * n * CPX);
+    int *piv = n2d_alloc(n * sizeof(int)), info = 0;
+    ok = a && piv && n2d_copy_d2d(a, g_cache.orig_dev, n * n * CPX) &&
+         n2d_lu_factor(a, N, N, piv, 0, 0, &info) && !info && n2d_copy_d2d(x, b, n * count * CPX) &&
+         n2d_lu_solve(a, N, N, piv, x, N, K);
+    n2d_free(a); n2d_free(piv);
+    g_last_refinement = -1;
+  }
+  ok = ok && n2d_copy_d2d(b, x, n * count * CPX);
+  n2d_free(x); n2d_free(r); n2d_free(d); n2d_free(norm);
+  free(rn); free(xn);
+  return ok;
 }
 
 int nec2c_cuda_dense_solve_classic_many(size_t n, const nec2c_cuda_complex *matrix, size_t ld,
@@ -88,19 +159,26 @@ int nec2c_cuda_dense_solve_classic_many(size_t n, const nec2c_cuda_complex *matr
   if(!matrix || !pivots || !rhs || n == 0 || n > INT_MAX || ld < n || ld > INT_MAX || stride < n ||
      count > INT_MAX) return 0;
   if(!n2d_device_ok()) return 0;
-  if(g_cache.lu_dev && g_cache.host == (const void *)matrix && g_cache.order == n && g_cache.ld == ld) {
+  const int cached = g_cache.piv_dev && g_cache.host == (const void *)matrix && g_cache.order == n && g_cache.ld == ld;
+  b = n2d_alloc(n * count * CPX);
+  if(!b || !n2d_upload2d(b, n * CPX, rhs, stride * CPX, n * CPX, count)) { n2d_free(b); return 0; }
+  if(cached && g_cache.mixed) {
+    ok = solve_refined(n, b, count) && n2d_download2d(rhs, stride * CPX, b, n * CPX, n * CPX, count);
+    n2d_free(b);
+    return ok;
+  }
+  if(cached) {
     lu = g_cache.lu_dev; piv = g_cache.piv_dev;
   } else {
-    /* Factors produced earlier (or in another process): upload them as stored. */
+    /* Factors produced earlier (or in another process): upload them as
+       stored.  Split-precision factors solved this way carry FP32 accuracy. */
     own = 1;
     lu = n2d_alloc(n * n * CPX);
     piv = n2d_alloc(n * sizeof(int));
     if(!lu || !piv || !n2d_upload2d(lu, n * CPX, matrix, ld * CPX, n * CPX, n) ||
-       !n2d_upload(piv, pivots, n * sizeof(int))) { n2d_free(lu); n2d_free(piv); return 0; }
+       !n2d_upload(piv, pivots, n * sizeof(int))) { n2d_free(lu); n2d_free(piv); n2d_free(b); return 0; }
   }
-  b = n2d_alloc(n * count * CPX);
-  ok = b && n2d_upload2d(b, n * CPX, rhs, stride * CPX, n * CPX, count) &&
-       n2d_lu_solve(lu, (long long)n, (long long)n, piv, b, (long long)n, (long long)count) &&
+  ok = n2d_lu_solve(lu, (long long)n, (long long)n, piv, b, (long long)n, (long long)count) &&
        n2d_download2d(rhs, stride * CPX, b, n * CPX, n * CPX, count);
   n2d_free(b);
   if(own) { n2d_free(lu); n2d_free(piv); }

@@ -96,3 +96,46 @@ def test_singular_rejected():
     assert not ok
     ok, _ = nb.solve_row_major(a, np.ones(4))
     assert not ok
+
+
+@pytest.mark.parametrize("n", [1, 33, 300, 1984, 2500])
+def test_split_precision_refined_solve(n):
+    """"cuda-mixed": FP32 factors with the tensor-core update, FP64 refinement
+    in the solve; the solution matches the oracle's FP64 solve to 1e-10
+    relative, reached by refinement (no FP64 fallback)."""
+    a = mom_like(n, 7 * n)
+    ld = n + 3
+    st = nec_storage(a, ld)
+    assert nb.dense_backend_set("cuda-mixed")
+    try:
+        ok, piv = nb.factor_classic(st)
+        assert ok, nb.load().nec2c_cuda_last_error()
+        rng = np.random.default_rng(n)
+        x = rng.standard_normal((n, 3)) + 1j * rng.standard_normal((n, 3))
+        rhs = np.zeros((ld, 3), dtype=np.complex128, order="F")
+        rhs[:n] = a @ x
+        assert nb.solve_classic_many(st, piv, rhs)
+        steps = nb.load().nec2c_cuda_dense_last_refinement()
+        assert steps >= 1
+        ao = nec_storage(a, ld).copy(order="F")
+        po = np.zeros(n, dtype=np.int32)
+        assert oracle().oracle_factr(n, ptr(ao), ptr(po), ld)
+        for j in range(3):
+            bo = np.ascontiguousarray((a @ x)[:, j].copy())
+            oracle().oracle_solve(n, ptr(ao), ptr(po), ptr(bo), ld)
+            assert np.linalg.norm(rhs[:n, j] - bo) / np.linalg.norm(bo) < 1e-10
+        # The factors written back are the FP32 factors: the product of the
+        # unit-lower and upper parts reproduces the row-interchanged matrix
+        # to FP32 accuracy.
+        lu = st[:n, :n].T
+        L = np.tril(lu, -1) + np.eye(n)
+        U = np.triu(lu)
+        pa = a.copy()
+        for i in range(n):
+            q = piv[i] - 1
+            if q != i:
+                pa[[i, q]] = pa[[q, i]]
+        assert np.max(np.abs(L @ U - pa)) / np.max(np.abs(a)) < 1e-4 * max(1.0, np.sqrt(n) / 10)
+    finally:
+        nb.dense_backend_set("cuda")
+        nb.load().nec2c_cuda_dense_release()

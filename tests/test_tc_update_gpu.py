@@ -1,0 +1,64 @@
+"""Tensor-core trailing update of the split-precision LU (n2d_gemm_tf32x3):
+C -= A B for complex FP32 blocks through tcgen05 3xTF32, against a float64
+numpy product.  The 3xTF32 split keeps the result at FP32 accuracy: the
+tolerance is 2e-6 relative to the largest |A||B| term."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import nec2c_b200 as nb
+
+pytestmark = pytest.mark.gpu
+
+
+def pack_bt(u):
+    """Packed real expansion of the 32 x N complex block u: 2N rows of 64
+    floats (row 2n: Re, -Im per k; row 2n+1: Im, Re), split hi + lo."""
+    k, n = u.shape
+    bt = np.empty((2 * n, 2 * k), dtype=np.float32)
+    ur = u.real.astype(np.float32).T
+    ui = u.imag.astype(np.float32).T
+    bt[0::2, 0::2] = ur
+    bt[0::2, 1::2] = -ui
+    bt[1::2, 0::2] = ui
+    bt[1::2, 1::2] = ur
+    hi = (bt.view(np.uint32) & np.uint32(0xFFFFE000)).view(np.float32)
+    lo = (bt - hi).astype(np.float32)
+    return np.ascontiguousarray(hi), np.ascontiguousarray(lo)
+
+
+@pytest.mark.parametrize("m,n,ld", [(128, 128, 256), (300, 517, 600), (1, 3, 64), (1000, 1000, 1040)])
+def test_tf32x3_update(m, n, ld):
+    import torch
+    rng = np.random.default_rng(m + n)
+    a = (rng.standard_normal((m, 32)) + 1j * rng.standard_normal((m, 32))).astype(np.complex64)
+    u = (rng.standard_normal((32, n)) + 1j * rng.standard_normal((32, n))).astype(np.complex64)
+    c = (rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))).astype(np.complex64)
+    # Working-matrix layout: C and A inside one row-major array with leading
+    # dimension ld (A in columns 0..31, C from column 32).
+    w = np.zeros((m, ld), dtype=np.complex64)
+    w[:, :32] = a
+    w[:, 32:32 + n] = c
+    hi, lo = pack_bt(u)
+    dw = torch.from_numpy(w.view(np.float32)).cuda()
+    dhi, dlo = torch.from_numpy(hi).cuda(), torch.from_numpy(lo).cuda()
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    lib = nb.load()
+    f = lib.n2d_gemm_tf32x3
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_longlong,
+                  C.c_longlong, C.c_void_p]
+    base = dw.data_ptr()
+    ok = f(base + 32 * 8, ld, base, ld, dhi.data_ptr(), dlo.data_ptr(), m, n, err.data_ptr())
+    torch.cuda.synchronize()
+    assert ok, lib.nec2c_cuda_last_error()
+    assert int(err.item()) == 0
+    out = dw.cpu().numpy().view(np.complex64)
+    expect = c.astype(np.complex128) - a.astype(np.complex128) @ u.astype(np.complex128)
+    scale = (np.abs(a).astype(np.float64) @ np.abs(u).astype(np.float64)).max()
+    assert np.max(np.abs(out[:, 32:32 + n] - expect)) / scale < 2e-6
+    # Columns outside C untouched.
+    assert np.array_equal(out[:, :32], a)
+    assert np.array_equal(out[:, 32 + n:], w[:, 32 + n:])
