@@ -13,11 +13,12 @@
 // lo = x - hi exact in FP32; D = Ahi Bhi + Ahi Blo + Alo Bhi accumulates in
 // FP32 in tensor memory (3xTF32), close to an FP32 product.
 //
-// One CTA per 128-row x 128-complex-column tile, 128 threads: the threads
+// One CTA per 128-row x 128-complex-column tile, 256 threads: the threads
 // stage A (split on the fly) and Bt (pre-split) into 128B-swizzled shared
 // memory, one elected thread issues the 24 tcgen05.mma (8 K-steps x 3
 // products, M=128 N=256 K=8), tcgen05.commit signals an mbarrier, and the
-// four warps read their 32 tensor-memory lanes back (tcgen05.ld) and update C.
+// eight warps read the accumulator back (tcgen05.ld: warp w its 32 lanes of
+// quarter w%4, half the columns per warpgroup) and update C.
 // No cluster, no multicast.
 #include <stdint.h>
 #include <string.h>
@@ -36,7 +37,7 @@ constexpr int KATOMS = KR * 4 / ATOM_ROW;   // 2 atoms along K
 constexpr int A_BYTES = KATOMS * TM * ATOM_ROW;   // 32 KB
 constexpr int B_BYTES = KATOMS * TN * ATOM_ROW;   // 64 KB
 constexpr int SMEM_BYTES = 2 * A_BYTES + 2 * B_BYTES + 1024;   // + alignment slack
-constexpr int THREADS = 128;
+constexpr int THREADS = 256;      // two warpgroups: staging and epilogue split between them
 constexpr uint32_t TMEM_COLS = 256;
 
 __device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
@@ -97,29 +98,50 @@ gemm_tf32x3_kernel(float2 *C, long long ldc, const float2 *A, long long lda, con
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&done_bar)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  // A: TM rows x 16 chunks of 4 floats, split on the fly.
-  for (int q = tid; q < TM * 16; q += THREADS) {
-    const int r = q >> 4, c = q & 15;
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (r0 + r < M) v = *reinterpret_cast<const float4 *>(reinterpret_cast<const float *>(A + (r0 + r) * lda) + 4 * c);
-    const float4 h = make_float4(tf32_hi(v.x), tf32_hi(v.y), tf32_hi(v.z), tf32_hi(v.w));
-    const float4 l = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
-    const uint32_t off = swz(r, c, TM);
-    *reinterpret_cast<float4 *>(a_hi + off) = h;
-    *reinterpret_cast<float4 *>(a_lo + off) = l;
+  // A: TM rows x 16 chunks of 4 floats, split on the fly; loads batched
+  // ahead of the shared-memory stores.
+  constexpr int AQ = TM * 16 / THREADS;
+#pragma unroll
+  for (int b = 0; b < AQ; b += 4) {
+    float4 v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = tid + (b + u) * THREADS, r = q >> 4, c = q & 15;
+      v[u] = r0 + r < M ? *reinterpret_cast<const float4 *>(reinterpret_cast<const float *>(A + (r0 + r) * lda) + 4 * c)
+                        : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = tid + (b + u) * THREADS, r = q >> 4, c = q & 15;
+      const float4 h = make_float4(tf32_hi(v[u].x), tf32_hi(v[u].y), tf32_hi(v[u].z), tf32_hi(v[u].w));
+      const float4 l = make_float4(v[u].x - h.x, v[u].y - h.y, v[u].z - h.z, v[u].w - h.w);
+      const uint32_t off = swz(r, c, TM);
+      *reinterpret_cast<float4 *>(a_hi + off) = h;
+      *reinterpret_cast<float4 *>(a_lo + off) = l;
+    }
   }
   // Bt: TN real rows x 16 chunks, hi and lo as stored.
-  for (int q = tid; q < TN * 16; q += THREADS) {
-    const int r = q >> 4, c = q & 15;
-    const long long gr = 2 * c0 + r;
-    float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
-    if (gr < 2 * N) {
-      h = *reinterpret_cast<const float4 *>(bt_hi + gr * KR + 4 * c);
-      l = *reinterpret_cast<const float4 *>(bt_lo + gr * KR + 4 * c);
+  constexpr int BQ = TN * 16 / THREADS;
+#pragma unroll
+  for (int b = 0; b < BQ; b += 4) {
+    float4 h[4], l[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = tid + (b + u) * THREADS, r = q >> 4, c = q & 15;
+      const long long gr = 2 * c0 + r;
+      h[u] = l[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (gr < 2 * N) {
+        h[u] = *reinterpret_cast<const float4 *>(bt_hi + gr * KR + 4 * c);
+        l[u] = *reinterpret_cast<const float4 *>(bt_lo + gr * KR + 4 * c);
+      }
     }
-    const uint32_t off = swz(r, c, TN);
-    *reinterpret_cast<float4 *>(b_hi + off) = h;
-    *reinterpret_cast<float4 *>(b_lo + off) = l;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = tid + (b + u) * THREADS, r = q >> 4, c = q & 15;
+      const uint32_t off = swz(r, c, TN);
+      *reinterpret_cast<float4 *>(b_hi + off) = h[u];
+      *reinterpret_cast<float4 *>(b_lo + off) = l[u];
+    }
   }
   // Generic-proxy shared-memory writes become visible to the tensor cores.
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -161,12 +183,22 @@ gemm_tf32x3_kernel(float2 *C, long long ldc, const float2 *A, long long lda, con
   ok = __syncthreads_and(ok) != 0;
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
-    const long long row = r0 + warp * 32 + lane;
-    float2 *crow = C + row * ldc + c0;
+    // Warp w reads tensor-memory lanes 32*(w%4).. (its rows) and the column
+    // chunks of its warpgroup: chunks 0..3 for warps 0-3, 4..7 for warps 4-7.
+    const int quarter = warp & 3, half = warp >> 2;
+    const long long row = r0 + quarter * 32 + lane;
+    float4 *crow = reinterpret_cast<float4 *>(C + row * ldc + c0);
 #pragma unroll 1
-    for (int j = 0; j < TN / 32; ++j) {
+    for (int jj = 0; jj < TN / 64; ++jj) {
+      const int j = half * (TN / 64) + jj;   // 32-float chunk = 16 complex = 8 float4
+      float4 cv[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const long long col = c0 + j * 16 + 2 * q;
+        cv[q] = (row < M && col < N) ? crow[j * 8 + q] : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
       uint32_t d[32];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * 32);
+      const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(j * 32);
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14,"
           " %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
@@ -178,14 +210,15 @@ gemm_tf32x3_kernel(float2 *C, long long ldc, const float2 *A, long long lda, con
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (row < M) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const long long col = c0 + j * 16 + q;
-          if (col < N) {
-            float2 cv = crow[j * 16 + q];
-            cv.x -= __uint_as_float(d[2 * q]);
-            cv.y -= __uint_as_float(d[2 * q + 1]);
-            crow[j * 16 + q] = cv;
-          }
+        for (int q = 0; q < 8; ++q) {
+          const long long col = c0 + j * 16 + 2 * q;
+          float4 v = cv[q];
+          v.x -= __uint_as_float(d[4 * q]);
+          v.y -= __uint_as_float(d[4 * q + 1]);
+          v.z -= __uint_as_float(d[4 * q + 2]);
+          v.w -= __uint_as_float(d[4 * q + 3]);
+          if (col + 1 < N) crow[j * 8 + q] = v;
+          else if (col < N) reinterpret_cast<float2 *>(crow + j * 8 + q)[0] = make_float2(v.x, v.y);
         }
       }
     }
@@ -209,13 +242,15 @@ gemm_tf32x3_kernel(float2 *C, long long ldc, const float2 *A, long long lda, con
 
 // C (M x N complex FP32, row-major, leading dimension ldc in complex units)
 // -= A (M x 32, lda) times the complex 32 x N block whose packed expansion is
-// bt_hi + bt_lo (2N rows of 64 floats).  A's rows must start 16-byte aligned
-// (lda even, A 16-byte aligned).  error: device int set to 1 on a time-out.
+// bt_hi + bt_lo (2N rows of 64 floats).  The rows of A and C must start
+// 16-byte aligned (lda, ldc even; A, C 16-byte aligned).  error: device int
+// set to 1 on a time-out.
 int n2c_tc_update(float *C, long long ldc, const float *A, long long lda, const float *bt_hi, const float *bt_lo,
                   long long M, long long N, int *error, cudaStream_t s) {
   if (M <= 0 || N <= 0) return 1;
-  if ((lda & 1) || ((uintptr_t)A & 15) || ((uintptr_t)bt_hi & 15) || ((uintptr_t)bt_lo & 15)) {
-    n2c_set_error("tensor-core update: operand rows must start 16-byte aligned");
+  if ((lda & 1) || (ldc & 1) || ((uintptr_t)A & 15) || ((uintptr_t)C & 15) || ((uintptr_t)bt_hi & 15) ||
+      ((uintptr_t)bt_lo & 15)) {
+    n2c_set_error("tensor-core update: operand and result rows must start 16-byte aligned");
     return 0;
   }
   static int configured = 0;
