@@ -188,6 +188,56 @@ int nec2c_cuda_dense_last_refinement(void);
 int nec2c_cuda_dense_factor_device_static(size_t order, nec2c_cuda_complex *matrix_dev,
                                           size_t leading_dimension, int *pivots_dev);
 
+/* ------------------------------------------------------- request server */
+/* No single counterpart in the reference: replaces the fork()ed frequency
+   workers (main.c:586-760) and their memory-capped job count
+   (concurrency.c:118-171) for a stream of solve requests on one GPU.  Worker
+   threads, each with its own CUDA stream, take queued requests as their
+   device footprint fits the budget left by the requests in flight; the work
+   of requests in flight overlaps on the device.  Dense requests factor and
+   solve a private device copy of the matrix (the host matrix is not
+   modified; rhs receives the solutions); volume requests run GMRES on a plan
+   or hybrid system the caller created and keeps resident across requests
+   (never two at once on the same operator). */
+enum { NEC2C_CUDA_REQUEST_DENSE = 1, NEC2C_CUDA_REQUEST_VOLUME = 2 };
+typedef struct {
+  int kind;
+  /* dense: NEC's storage (order x order, leading dimension ld) and
+     rhs_count right-hand sides (stride rhs_stride), overwritten with x */
+  size_t order, ld, rhs_count, rhs_stride;
+  const nec2c_cuda_complex *matrix;
+  nec2c_cuda_complex *rhs;
+  /* volume: exactly one of plan / system; x is the initial guess and the
+     result, as for nec2c_cuda_gmres_plan */
+  nec2c_cuda_vie_plan *plan;
+  nec2c_cuda_hybrid *system;
+  const nec2c_cuda_complex *b;
+  nec2c_cuda_complex *x;
+  nec2c_cuda_gmres_options options;
+  /* filled by the server */
+  int status;                      /* 1 solved, 0 failed (error holds why) */
+  int done;
+  unsigned skipped;
+  nec2c_cuda_gmres_report report;  /* volume: GMRES report; dense: iterations = refinement steps */
+  size_t footprint;                /* device bytes admitted for it */
+  double queued_s, started_s, finished_s;   /* CLOCK_MONOTONIC seconds */
+  char error[128];
+} nec2c_cuda_request;
+typedef struct nec2c_cuda_server nec2c_cuda_server;
+/* slots worker threads on device; device_budget 0 means the free device
+   memory less max(1/5, 1 GiB) (the reserve of concurrency.c:131-136).
+   split != 0 selects the split-precision dense form. */
+int nec2c_cuda_server_create(nec2c_cuda_server **out, int device, int slots, size_t device_budget, int split);
+/* Queues a request (caller-owned until it is done); returns at once. */
+int nec2c_cuda_server_submit(nec2c_cuda_server *server, nec2c_cuda_request *request);
+/* Blocks until the request is done; returns its status. */
+int nec2c_cuda_server_wait(nec2c_cuda_server *server, nec2c_cuda_request *request);
+/* Blocks until every submitted request is done. */
+int nec2c_cuda_server_drain(nec2c_cuda_server *server);
+size_t nec2c_cuda_server_budget(const nec2c_cuda_server *server);
+/* Drains, stops the workers and frees the server. */
+void nec2c_cuda_server_destroy(nec2c_cuda_server *server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,6 +34,18 @@ class GmresReport(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class Request(C.Structure):
+    """nec2c_cuda_request (include/nec2c_cuda.h)."""
+    _fields_ = [("kind", C.c_int), ("order", C.c_size_t), ("ld", C.c_size_t), ("rhs_count", C.c_size_t),
+                ("rhs_stride", C.c_size_t), ("matrix", C.c_void_p), ("rhs", C.c_void_p), ("plan", C.c_void_p),
+                ("system", C.c_void_p), ("b", C.c_void_p), ("x", C.c_void_p), ("options", GmresOptions),
+                ("status", C.c_int), ("done", C.c_int), ("skipped", C.c_uint), ("report", GmresReport),
+                ("footprint", C.c_size_t), ("queued_s", C.c_double), ("started_s", C.c_double),
+                ("finished_s", C.c_double), ("error", C.c_char * 128)]
+
+
+REQUEST_DENSE, REQUEST_VOLUME = 1, 2
+
 _lib = None
 
 
@@ -80,6 +92,12 @@ def load():
         "nec2c_cuda_dense_factor_classic": (i, [sz, vp, sz, vp]),
         "nec2c_cuda_dense_factor_device_static": (i, [sz, vp, sz, vp]),
         "nec2c_cuda_dense_last_refinement": (i, []),
+        "nec2c_cuda_server_create": (i, [C.POINTER(vp), i, i, sz, i]),
+        "nec2c_cuda_server_submit": (i, [vp, C.POINTER(Request)]),
+        "nec2c_cuda_server_wait": (i, [vp, C.POINTER(Request)]),
+        "nec2c_cuda_server_drain": (i, [vp]),
+        "nec2c_cuda_server_budget": (sz, [vp]),
+        "nec2c_cuda_server_destroy": (None, [vp]),
         "nec2c_cuda_dense_solve_classic": (i, [sz, vp, sz, vp, vp]),
         "nec2c_cuda_dense_solve_classic_many": (i, [sz, vp, sz, vp, vp, sz, sz]),
         "nec2c_cuda_dense_solve_row_major": (i, [vp, vp, sz]),
@@ -261,3 +279,68 @@ def solve_row_major(a, b):
     b = _cvec(b).copy()
     ok = load().nec2c_cuda_dense_solve_row_major(_ptr(a), _ptr(b), b.size)
     return bool(ok), b
+
+
+class Server:
+    """Request server (nec2c_cuda_server_*): requests run concurrently on
+    worker threads with their own streams, admitted by device footprint."""
+
+    def __init__(self, slots=4, budget=0, split=False, device=0):
+        self.h = C.c_void_p()
+        if not load().nec2c_cuda_server_create(C.byref(self.h), device, slots, budget, 1 if split else 0):
+            self.h = None
+            raise RuntimeError("server create failed: " + last_error())
+        self._keep = {}
+
+    def budget(self):
+        return load().nec2c_cuda_server_budget(self.h)
+
+    def dense(self, storage, rhs):
+        """Queues a dense solve of NEC storage (Fortran ld x n) for rhs
+        (Fortran ld_rhs x k, overwritten with the solutions)."""
+        assert storage.dtype == np.complex128 and storage.flags.f_contiguous
+        assert rhs.dtype == np.complex128 and rhs.flags.f_contiguous
+        r = Request()
+        r.kind = REQUEST_DENSE
+        r.order, r.ld = storage.shape[1], storage.shape[0]
+        r.rhs_count, r.rhs_stride = rhs.shape[1], rhs.shape[0]
+        r.matrix, r.rhs = _ptr(storage), _ptr(rhs)
+        self._submit(r, (storage, rhs))
+        return r
+
+    def volume(self, op, b, x, restart=30, maxit=300, rtol=1e-12, atol=0.0):
+        """Queues GMRES on a VolumePlan or HybridSystem; x is the initial guess
+        and receives the solution."""
+        r = Request()
+        r.kind = REQUEST_VOLUME
+        if isinstance(op, VolumePlan):
+            r.plan = op.h
+        else:
+            r.system = op.h
+        r.b, r.x = _ptr(b), _ptr(x)
+        r.options = GmresOptions(restart, maxit, rtol, atol)
+        self._submit(r, (op, b, x))
+        return r
+
+    def _submit(self, r, keep):
+        self._keep[C.addressof(r)] = (r, keep)
+        if not load().nec2c_cuda_server_submit(self.h, C.byref(r)):
+            del self._keep[C.addressof(r)]
+            raise RuntimeError("submit rejected: " + last_error())
+
+    def wait(self, r):
+        ok = load().nec2c_cuda_server_wait(self.h, C.byref(r))
+        self._keep.pop(C.addressof(r), None)
+        return bool(ok)
+
+    def drain(self):
+        load().nec2c_cuda_server_drain(self.h)
+        self._keep.clear()
+
+    def close(self):
+        if self.h:
+            load().nec2c_cuda_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    __del__ = close

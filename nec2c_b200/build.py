@@ -57,7 +57,7 @@ def build(verbose=False):
     for f in sorted(os.listdir(HOST)):
         if f.endswith(".c"):
             src, obj = os.path.join(HOST, f), os.path.join(OBJ, "host_" + f[:-2] + ".o")
-            cmd = ["gcc", "-O2", "-std=gnu11", "-fPIC", "-Wall", "-Wno-unused-function",
+            cmd = ["gcc", "-O2", "-std=gnu11", "-fPIC", "-pthread", "-Wall", "-Wno-unused-function",
                    "-I" + os.path.join(ROOT, "include"), "-c", src, "-o", obj]
             jobs.append((src, obj, cmd))
     todo = [j for j in jobs if _stale(j[0], j[1], deps)]
@@ -67,7 +67,7 @@ def build(verbose=False):
                 print(out)
     objs = [j[1] for j in jobs]
     if todo or not os.path.exists(LIB):
-        _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs + ["-lm"])
+        _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs + ["-lm", "-lpthread"])
     return LIB
 
 

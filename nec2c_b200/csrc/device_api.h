@@ -21,6 +21,16 @@ void n2d_set_gate(const int *gate_dev);
 /* Device buffers and copies on the current stream. */
 void *n2d_alloc(size_t bytes);
 void n2d_free(void *p);
+/* Stream-ordered allocation on this thread's stream (pool keeps freed memory;
+   no device-wide synchronisation).  Free with n2d_free_async on the same
+   stream. */
+void *n2d_alloc_async(size_t bytes);
+void n2d_free_async(void *p);
+/* A new non-blocking stream / its release. */
+void *n2d_stream_create(void);
+void n2d_stream_destroy(void *stream);
+/* cudaMemGetInfo of the current device. */
+int n2d_mem_info(size_t *free_bytes, size_t *total_bytes);
 int n2d_upload(void *dst_dev, const void *src, size_t bytes);
 int n2d_download(void *dst, const void *src_dev, size_t bytes);
 int n2d_memset(void *dst_dev, int value, size_t bytes);

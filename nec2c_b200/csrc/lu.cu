@@ -962,8 +962,9 @@ static int factor_panels(S *a, long long n, long long ld, int *ipiv, int rule, c
   return ok;
 }
 
-// Scratch allocation around factor_panels; the split-precision form also
-// holds the packed U12 expansion.
+// Scratch allocation around factor_panels (stream-ordered, so factorisations
+// on several streams do not synchronise each other); the split-precision form
+// also holds the packed U12 expansion.
 template <typename S>
 static int factor_alloc(S *a, long long n, long long ld, int *ipiv, int rule, int *info_host) {
   *info_host = 0;
@@ -971,26 +972,26 @@ static int factor_alloc(S *a, long long n, long long ld, int *ipiv, int rule, in
   const bool split = sizeof(S) == sizeof(float2);
   FactorScratch w;
   memset(&w, 0, sizeof(w));
-  w.st = (LuStatus *)n2d_alloc(sizeof(LuStatus));
-  w.pairs = (int *)n2d_alloc(4 * KB * sizeof(int));
+  w.st = (LuStatus *)n2d_alloc_async(sizeof(LuStatus));
+  w.pairs = (int *)n2d_alloc_async(4 * KB * sizeof(int));
   const bool grid = n > cluster_rows();
   const int gb = grid_blocks_for(n);
   if (grid) {
-    w.gval = (double *)n2d_alloc(2 * gb * sizeof(double));
-    w.gidx = (int *)n2d_alloc(2 * gb * sizeof(int));
-    w.grow = (double2 *)n2d_alloc((size_t)2 * gb * KB * sizeof(double2));
-    w.growj = (double2 *)n2d_alloc(2 * KB * sizeof(double2));
+    w.gval = (double *)n2d_alloc_async(2 * gb * sizeof(double));
+    w.gidx = (int *)n2d_alloc_async(2 * gb * sizeof(int));
+    w.grow = (double2 *)n2d_alloc_async((size_t)2 * gb * KB * sizeof(double2));
+    w.growj = (double2 *)n2d_alloc_async(2 * KB * sizeof(double2));
   }
   if (split) {
-    w.bt_hi = (float *)n2d_alloc((size_t)2 * n * 2 * KB * sizeof(float));
-    w.bt_lo = (float *)n2d_alloc((size_t)2 * n * 2 * KB * sizeof(float));
+    w.bt_hi = (float *)n2d_alloc_async((size_t)2 * n * 2 * KB * sizeof(float));
+    w.bt_lo = (float *)n2d_alloc_async((size_t)2 * n * 2 * KB * sizeof(float));
   }
   int ok = w.st && w.pairs && n2d_memset(w.st, 0, sizeof(LuStatus)) &&
            (!grid || (w.gval && w.gidx && w.grow && w.growj)) && (!split || (w.bt_hi && w.bt_lo));
   ok = ok && factor_panels(a, n, ld, ipiv, rule, w, true, info_host);
-  n2d_free(w.st); n2d_free(w.pairs);
-  n2d_free(w.gval); n2d_free(w.gidx); n2d_free(w.grow); n2d_free(w.growj);
-  n2d_free(w.bt_hi); n2d_free(w.bt_lo);
+  n2d_free_async(w.st); n2d_free_async(w.pairs);
+  n2d_free_async(w.gval); n2d_free_async(w.gidx); n2d_free_async(w.grow); n2d_free_async(w.growj);
+  n2d_free_async(w.bt_hi); n2d_free_async(w.bt_lo);
   return ok;
 }
 

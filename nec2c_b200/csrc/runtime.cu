@@ -51,6 +51,46 @@ extern "C" void *n2d_alloc(size_t bytes) {
   return p;
 }
 extern "C" void n2d_free(void *p) { if (p) cudaFree(p); }
+// Stream-ordered allocation on this thread's stream from the device's default
+// pool, which keeps freed memory for reuse (no device-wide synchronisation,
+// unlike cudaFree): for per-call scratch of work that runs concurrently on
+// several streams.
+extern "C" void *n2d_alloc_async(size_t bytes) {
+  static thread_local int pool_dev = -1;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+  if (pool_dev != dev) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      unsigned long long keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+    pool_dev = dev;
+  }
+  void *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMallocAsync(&p, bytes, g_stream);
+  if (e != cudaSuccess) { n2c_set_error("cudaMallocAsync(%zu): %s", bytes, cudaGetErrorString(e)); return nullptr; }
+  return p;
+}
+extern "C" void n2d_free_async(void *p) { if (p) cudaFreeAsync(p, g_stream); }
+// This thread's own non-blocking stream (created once per thread and device)
+// for hosts that run several solves concurrently.
+extern "C" void *n2d_stream_create(void) {
+  cudaStream_t s = nullptr;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    n2c_set_error("stream creation failed");
+    return nullptr;
+  }
+  return (void *)s;
+}
+extern "C" void n2d_stream_destroy(void *s) { if (s) cudaStreamDestroy((cudaStream_t)s); }
+extern "C" int n2d_mem_info(size_t *free_bytes, size_t *total_bytes) {
+  N2C_CHECK(cudaMemGetInfo(free_bytes, total_bytes));
+  return 1;
+}
 // ------------------------------------------------------------- host copies
 // Pageable host memory above STAGE_MIN bytes moves through two pinned staging
 // buffers so that the host memcpy of one chunk overlaps the DMA of the other.

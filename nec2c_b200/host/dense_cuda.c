@@ -1,7 +1,10 @@
 /* Host side of the CUDA dense backend: dense_backend.c's classic factor/solve
  * and row-major solve entry points (C, like the reference).  The factor keeps
  * its device copy (and, for the mixed form, the original matrix) so the
- * solves that follow in the same process do not re-upload it. */
+ * solves that follow on the same thread do not re-upload it.  The cache is
+ * per thread: the reference keeps one factorisation per process
+ * (dense_backend.c:15), and threads that each own a stream (the request
+ * server) keep one each. */
 #include <complex.h>
 #include <float.h>
 #include <limits.h>
@@ -25,8 +28,8 @@ int nec2c_cuda_dense_backend_set(const char *name)
 }
 const char *nec2c_cuda_dense_backend_name(void) { return g_dense_mixed ? "cuda-mixed" : "cuda"; }
 
-/* The most recent classic factorisation, kept on the device. */
-static struct {
+/* The most recent classic factorisation of this thread, kept on the device. */
+static _Thread_local struct {
   const void *host;      /* host matrix the factors were written to */
   size_t order, ld;
   double *lu_dev;        /* FP64 form: row-major LU, leading dim order */
@@ -38,11 +41,11 @@ static struct {
   int mixed;
 } g_cache;
 
-static int g_last_refinement = 0;
+static _Thread_local int g_last_refinement = 0;
 
 void nec2c_cuda_dense_release(void)
 {
-  n2d_free(g_cache.lu_dev); n2d_free(g_cache.piv_dev); n2d_free(g_cache.lu32_dev); n2d_free(g_cache.orig_dev);
+  n2d_free(g_cache.lu_dev); n2d_free(g_cache.piv_dev); n2d_free_async(g_cache.lu32_dev); n2d_free(g_cache.orig_dev);
   memset(&g_cache, 0, sizeof(g_cache));
 }
 
@@ -61,28 +64,105 @@ static double *upload_matrix(const void *matrix, size_t n, size_t ld)
   return a;
 }
 
-/* Split-precision factorisation of the uploaded matrix a (kept as the
-   refinement original): FP32 copy, tensor-core LU, FP32 factors widened back
-   into the host storage. */
-static int factor_split(double *a, size_t n, size_t ld, int *piv, nec2c_cuda_complex *matrix, int *pivots)
+/* Split-precision factors on the device, with the FP64 original. */
+typedef struct {
+  float *lu32;
+  size_t ld32;
+  int *piv;
+  const double *orig;
+  double anorm;
+} split_factors;
+
+/* Refined solve with split-precision factors (the iteration of LAPACK's
+   mixed-precision zcgesv): x = 0, r = b; repeat d = LU32 \ r, x += d,
+   r = b - A x until every column has ||r||_inf <= ||x||_inf ||A||_inf eps
+   sqrt(n), at most 30 steps; otherwise an FP64 factorisation solves it.  b
+   (order x count on the device) is replaced by the solution.  Buffers are
+   stream-ordered. */
+static int solve_refined(size_t n, const split_factors *f, double *b, size_t count, int *steps)
+{
+  const long long N = (long long)n, K = (long long)count;
+  const double cte = f->anorm * DBL_EPSILON * sqrt((double)n);
+  double *x = n2d_alloc_async(n * count * CPX), *r = n2d_alloc_async(n * count * CPX);
+  double *d = n2d_alloc_async(n * count * CPX);
+  void *norm = n2d_alloc_async(count * sizeof(unsigned long long));
+  double *rn = malloc(count * sizeof(double)), *xn = malloc(count * sizeof(double));
+  int ok = x && r && d && norm && rn && xn && n2d_memset(x, 0, n * count * CPX) && n2d_copy_d2d(r, b, n * count * CPX);
+  int done = 0, it;
+  *steps = 0;
+  for(it = 1; ok && it <= 30 && !done; ++it) {
+    size_t j;
+    ok = n2d_copy_d2d(d, r, n * count * CPX) &&
+         n2d_lu_solve32(f->lu32, N, (long long)f->ld32, f->piv, d, N, K) &&
+         n2d_add_correction(x, d, N, K, N, norm, xn) &&
+         n2d_residual(f->orig, N, N, x, b, r, K, N, norm, rn);
+    done = ok;
+    for(j = 0; ok && j < count; ++j) if(!(rn[j] <= xn[j] * cte)) done = 0;
+    if(done) *steps = it;
+  }
+  if(ok && !done) {
+    /* Not converged: FP64 factorisation of a copy of the original. */
+    double *a = n2d_alloc_async(n * n * CPX);
+    int *piv = n2d_alloc_async(n * sizeof(int)), info = 0;
+    ok = a && piv && n2d_copy_d2d(a, f->orig, n * n * CPX) &&
+         n2d_lu_factor(a, N, N, piv, 0, 0, &info) && !info && n2d_copy_d2d(x, b, n * count * CPX) &&
+         n2d_lu_solve(a, N, N, piv, x, N, K);
+    n2d_free_async(a); n2d_free_async(piv);
+    *steps = -1;
+  }
+  ok = ok && n2d_copy_d2d(b, x, n * count * CPX);
+  n2d_free_async(x); n2d_free_async(r); n2d_free_async(d); n2d_free_async(norm);
+  free(rn); free(xn);
+  return ok;
+}
+
+/* Split-precision factorisation of the device matrix a (order n, leading
+   dim n), which stays as the refinement original. */
+static int split_factor(double *a, size_t n, int *piv, split_factors *f)
 {
   const size_t ld32 = n + (n & 1);
-  float *lu32 = n2d_alloc(n * ld32 * 2 * sizeof(float));
-  double *wide = NULL;
-  void *norm = n2d_alloc(sizeof(unsigned long long));
+  float *lu32 = n2d_alloc_async(n * ld32 * 2 * sizeof(float));
+  void *norm = n2d_alloc_async(sizeof(unsigned long long));
   double anorm = 0;
   int info = 0;
   int ok = lu32 && norm && n2d_narrow(a, (long long)n, lu32, (long long)ld32, (long long)n, (long long)n) &&
            n2d_norm_inf(a, (long long)n, (long long)n, norm, &anorm) &&
            n2d_lu_factor32(lu32, (long long)n, (long long)ld32, piv, 0, &info);
   if(ok && info) { n2c_set_error("matrix is singular (pivot %d)", info); ok = 0; }
-  wide = ok ? n2d_alloc(n * n * CPX) : NULL;
-  ok = ok && wide && n2d_widen(lu32, (long long)ld32, wide, (long long)n, (long long)n, (long long)n) &&
-       n2d_download2d(matrix, ld * CPX, wide, n * CPX, n * CPX, n) && n2d_download(pivots, piv, n * sizeof(int));
-  n2d_free(wide); n2d_free(norm);
-  if(!ok) { n2d_free(lu32); return 0; }
-  g_cache.lu32_dev = lu32; g_cache.ld32 = ld32; g_cache.orig_dev = a; g_cache.anorm = anorm;
+  n2d_free_async(norm);
+  if(!ok) { n2d_free_async(lu32); return 0; }
+  f->lu32 = lu32; f->ld32 = ld32; f->piv = piv; f->orig = a; f->anorm = anorm;
   return 1;
+}
+
+/* Factor and solve on a private device copy (the host matrix is left as it
+   is and no factors are kept): the request server's dense solve.  split
+   selects the split-precision form.  Every device buffer is stream-ordered on
+   this thread's stream. */
+int n2c_dense_solve_private(size_t n, const nec2c_cuda_complex *matrix, size_t ld, nec2c_cuda_complex *rhs,
+                            size_t stride, size_t count, int split, int *steps)
+{
+  double *a, *b;
+  int *piv, ok, info = 0;
+  split_factors f;
+  *steps = 0;
+  if(!matrix || !rhs || n == 0 || n > INT_MAX || ld < n || stride < n || count == 0 || count > INT_MAX) return 0;
+  a = n2d_alloc_async(n * n * CPX);
+  b = n2d_alloc_async(n * count * CPX);
+  piv = n2d_alloc_async(n * sizeof(int));
+  ok = a && b && piv && n2d_upload2d(a, n * CPX, matrix, ld * CPX, n * CPX, n) &&
+       n2d_upload2d(b, n * CPX, rhs, stride * CPX, n * CPX, count);
+  if(ok && split) {
+    ok = split_factor(a, n, piv, &f) && solve_refined(n, &f, b, count, steps);
+    if(f.lu32 && ok) n2d_free_async(f.lu32);
+  } else if(ok) {
+    ok = n2d_lu_factor(a, (long long)n, (long long)n, piv, 0, 0, &info);
+    if(ok && info) { n2c_set_error("matrix is singular (pivot %d)", info); ok = 0; }
+    ok = ok && n2d_lu_solve(a, (long long)n, (long long)n, piv, b, (long long)n, (long long)count);
+  }
+  ok = ok && n2d_download2d(rhs, stride * CPX, b, n * CPX, n * CPX, count);
+  n2d_free_async(a); n2d_free_async(b); n2d_free_async(piv);
+  return ok;
 }
 
 int nec2c_cuda_dense_factor_classic(size_t n, nec2c_cuda_complex *matrix, size_t ld, int *pivots)
@@ -97,8 +177,19 @@ int nec2c_cuda_dense_factor_classic(size_t n, nec2c_cuda_complex *matrix, size_t
   piv = n2d_alloc(n * sizeof(int));
   if(!a || !piv) { n2d_free(a); n2d_free(piv); return 0; }
   if(g_dense_mixed) {
-    if(!factor_split(a, n, ld, piv, matrix, pivots)) { n2d_free(a); n2d_free(piv); return 0; }
+    /* Split form: FP32 factors on the device, widened into the host storage;
+       the FP64 matrix stays for the refinement. */
+    split_factors f;
+    double *wide = NULL;
+    memset(&f, 0, sizeof(f));
+    ok = split_factor(a, n, piv, &f);
+    wide = ok ? n2d_alloc(n * n * CPX) : NULL;
+    ok = ok && wide && n2d_widen(f.lu32, (long long)f.ld32, wide, (long long)n, (long long)n, (long long)n) &&
+         n2d_download2d(matrix, ld * CPX, wide, n * CPX, n * CPX, n) && n2d_download(pivots, piv, n * sizeof(int));
+    n2d_free(wide);
+    if(!ok) { n2d_free_async(f.lu32); n2d_free(a); n2d_free(piv); return 0; }
     g_cache.host = matrix; g_cache.order = n; g_cache.ld = ld; g_cache.piv_dev = piv; g_cache.mixed = 1;
+    g_cache.lu32_dev = f.lu32; g_cache.ld32 = f.ld32; g_cache.orig_dev = a; g_cache.anorm = f.anorm;
     return 1;
   }
   ok = n2d_lu_factor(a, (long long)n, (long long)n, piv, 0, 0, &info);
@@ -108,45 +199,6 @@ int nec2c_cuda_dense_factor_classic(size_t n, nec2c_cuda_complex *matrix, size_t
   g_cache.host = matrix; g_cache.order = n; g_cache.ld = ld;
   g_cache.lu_dev = a; g_cache.piv_dev = piv; g_cache.mixed = 0;
   return 1;
-}
-
-/* Refined solve with the cached split-precision factors (the iteration of
-   LAPACK's mixed-precision zcgesv): x = 0, r = b; repeat d = LU32 \ r,
-   x += d, r = b - A x until every column has ||r||_inf <= ||x||_inf ||A||_inf
-   eps sqrt(n), at most 30 steps; otherwise an FP64 factorisation solves it. */
-static int solve_refined(size_t n, double *b, size_t count)
-{
-  const long long N = (long long)n, K = (long long)count;
-  const double cte = g_cache.anorm * DBL_EPSILON * sqrt((double)n);
-  double *x = n2d_alloc(n * count * CPX), *r = n2d_alloc(n * count * CPX), *d = n2d_alloc(n * count * CPX);
-  void *norm = n2d_alloc(count * sizeof(unsigned long long));
-  double *rn = malloc(count * sizeof(double)), *xn = malloc(count * sizeof(double));
-  int ok = x && r && d && norm && rn && xn && n2d_memset(x, 0, n * count * CPX) && n2d_copy_d2d(r, b, n * count * CPX);
-  int done = 0, it;
-  for(it = 1; ok && it <= 30 && !done; ++it) {
-    size_t j;
-    ok = n2d_copy_d2d(d, r, n * count * CPX) &&
-         n2d_lu_solve32(g_cache.lu32_dev, N, (long long)g_cache.ld32, g_cache.piv_dev, d, N, K) &&
-         n2d_add_correction(x, d, N, K, N, norm, xn) &&
-         n2d_residual(g_cache.orig_dev, N, N, x, b, r, K, N, norm, rn);
-    done = ok;
-    for(j = 0; ok && j < count; ++j) if(!(rn[j] <= xn[j] * cte)) done = 0;
-    if(done) g_last_refinement = it;
-  }
-  if(ok && !done) {
-    /* Not converged: FP64 factorisation of a copy of the original. */
-    double *a = n2d_alloc(n * n * CPX);
-    int *piv = n2d_alloc(n * sizeof(int)), info = 0;
-    ok = a && piv && n2d_copy_d2d(a, g_cache.orig_dev, n * n * CPX) &&
-         n2d_lu_factor(a, N, N, piv, 0, 0, &info) && !info && n2d_copy_d2d(x, b, n * count * CPX) &&
-         n2d_lu_solve(a, N, N, piv, x, N, K);
-    n2d_free(a); n2d_free(piv);
-    g_last_refinement = -1;
-  }
-  ok = ok && n2d_copy_d2d(b, x, n * count * CPX);
-  n2d_free(x); n2d_free(r); n2d_free(d); n2d_free(norm);
-  free(rn); free(xn);
-  return ok;
 }
 
 int nec2c_cuda_dense_solve_classic_many(size_t n, const nec2c_cuda_complex *matrix, size_t ld,
@@ -163,7 +215,9 @@ int nec2c_cuda_dense_solve_classic_many(size_t n, const nec2c_cuda_complex *matr
   b = n2d_alloc(n * count * CPX);
   if(!b || !n2d_upload2d(b, n * CPX, rhs, stride * CPX, n * CPX, count)) { n2d_free(b); return 0; }
   if(cached && g_cache.mixed) {
-    ok = solve_refined(n, b, count) && n2d_download2d(rhs, stride * CPX, b, n * CPX, n * CPX, count);
+    split_factors f = {g_cache.lu32_dev, g_cache.ld32, g_cache.piv_dev, g_cache.orig_dev, g_cache.anorm};
+    ok = solve_refined(n, &f, b, count, &g_last_refinement) &&
+         n2d_download2d(rhs, stride * CPX, b, n * CPX, n * CPX, count);
     n2d_free(b);
     return ok;
   }

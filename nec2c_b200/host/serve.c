@@ -1,0 +1,268 @@
+/* Request server: concurrent dense MoM and volume (VIE) solves on one GPU.
+ *
+ * The reference runs a frequency sweep as fork()ed worker processes
+ * (main.c:586-760), as many as the host's memory allows for the estimated
+ * per-worker bytes (concurrency.c:118-171: usable memory = available minus a
+ * reserve of max(1/5, 1 GiB), jobs = usable / worker bytes).  On the GPU the
+ * workers are host threads, each owning a CUDA stream, and the memory they
+ * share is device memory: a request is admitted when its device footprint
+ * fits the budget left by the requests in flight, so requests that arrive
+ * while others run start as soon as a worker and memory free up and their
+ * work overlaps on the device.
+ *
+ * Dense requests factor and solve a private device copy (the split-precision
+ * form with FP64 refinement when the server was created with split != 0).
+ * Volume requests run GMRES on a plan or hybrid system the caller created and
+ * keeps on the device across requests (a frequency's spectrum is built once);
+ * a plan is not reentrant (vie_fft.h:6), so two requests on the same plan
+ * never run at the same time.  Admission is FIFO, except that a request that
+ * does not fit may be passed by later ones that do, at most `slots` times
+ * each before the queue waits for it. */
+#include <errno.h>
+#include <limits.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include "../../include/nec2c_cuda.h"
+#include "../csrc/device_api.h"
+
+int n2c_dense_solve_private(size_t n, const nec2c_cuda_complex *matrix, size_t ld, nec2c_cuda_complex *rhs,
+                            size_t stride, size_t count, int split, int *steps);
+
+struct nec2c_cuda_server {
+  int device, slots, split;
+  size_t budget, in_use;
+  pthread_mutex_t lock;
+  pthread_cond_t work, done;
+  nec2c_cuda_request **queue;   /* FIFO, [head, head + count) modulo cap */
+  size_t head, count, cap;
+  const void **busy;            /* operators with a request in flight */
+  size_t pending;               /* submitted, not finished */
+  int stop, started;
+  pthread_t *threads;
+};
+
+static double now_s(void)
+{
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
+static const size_t CPX = 2 * sizeof(double);
+
+/* Device bytes a request holds while it runs. */
+static size_t footprint(const nec2c_cuda_server *s, const nec2c_cuda_request *r)
+{
+  if(r->kind == NEC2C_CUDA_REQUEST_DENSE) {
+    const size_t n = r->order, k = r->rhs_count;
+    size_t bytes = n * n * CPX + n * k * CPX + n * sizeof(int) + 4096;
+    if(s->split) bytes += n * (n + 1) * 2 * sizeof(float) + 4 * n * 2 * 32 * sizeof(float) + 3 * n * k * CPX;
+    return bytes;
+  }
+  {
+    const size_t n = r->plan ? nec2c_cuda_vie_fft_order(r->plan) : nec2c_cuda_hybrid_order(r->system);
+    const size_t m = r->options.restart ? r->options.restart : 30;
+    return (m + 4) * n * CPX;
+  }
+}
+
+static const void *request_op(const nec2c_cuda_request *r)
+{
+  return r->kind == NEC2C_CUDA_REQUEST_VOLUME ? (r->plan ? (const void *)r->plan : (const void *)r->system) : NULL;
+}
+
+static int op_busy(const nec2c_cuda_server *s, const void *op)
+{
+  int i;
+  if(!op) return 0;
+  for(i = 0; i < s->slots; ++i) if(s->busy[i] == op) return 1;
+  return 0;
+}
+
+static void run_request(nec2c_cuda_server *s, nec2c_cuda_request *r)
+{
+  int steps = 0;
+  memset(&r->report, 0, sizeof(r->report));
+  if(r->kind == NEC2C_CUDA_REQUEST_DENSE) {
+    r->status = n2c_dense_solve_private(r->order, r->matrix, r->ld, r->rhs, r->rhs_stride, r->rhs_count, s->split,
+                                        &steps);
+    r->report.status = r->status;
+    r->report.iterations = steps < 0 ? 0 : (size_t)steps;
+  } else if(r->plan) {
+    r->status = nec2c_cuda_gmres_plan(r->plan, r->b, r->x, &r->options, &r->report);
+  } else {
+    r->status = nec2c_cuda_gmres_hybrid(r->system, r->b, r->x, &r->options, &r->report);
+  }
+  if(!r->status) {
+    strncpy(r->error, nec2c_cuda_last_error(), sizeof(r->error) - 1);
+    r->error[sizeof(r->error) - 1] = 0;
+  }
+}
+
+static void *worker(void *arg)
+{
+  nec2c_cuda_server *s = arg;
+  void *stream;
+  int slot = -1, i;
+  n2d_set_device(s->device);
+  stream = n2d_stream_create();
+  n2d_set_stream(stream);
+  pthread_mutex_lock(&s->lock);
+  for(;;) {
+    nec2c_cuda_request *r = NULL;
+    size_t pick = 0, q, fp = 0;
+    if(s->stop && s->count == 0) break;
+    for(q = 0; q < s->count; ++q) {
+      nec2c_cuda_request *c = s->queue[(s->head + q) % s->cap];
+      const size_t f = footprint(s, c);
+      const int fits = s->in_use == 0 || (f <= s->budget && s->in_use + f <= s->budget);
+      if(fits && !op_busy(s, request_op(c))) { r = c; pick = q; fp = f; break; }
+      /* A request that does not fit may be passed only `slots` times. */
+      if(!fits && c->skipped >= (unsigned)s->slots) break;
+    }
+    if(!r) { pthread_cond_wait(&s->work, &s->lock); continue; }
+    for(q = 0; q < pick; ++q) {
+      nec2c_cuda_request *c = s->queue[(s->head + q) % s->cap];
+      const size_t f = footprint(s, c);
+      if(!(s->in_use == 0 || (f <= s->budget && s->in_use + f <= s->budget))) c->skipped++;
+    }
+    for(q = pick; q + 1 < s->count; ++q)
+      s->queue[(s->head + q) % s->cap] = s->queue[(s->head + q + 1) % s->cap];
+    s->count--;
+    s->in_use += fp;
+    for(i = 0; i < s->slots; ++i) if(!s->busy[i]) { s->busy[i] = request_op(r) ? request_op(r) : (const void *)r; slot = i; break; }
+    r->footprint = fp;
+    r->started_s = now_s();
+    pthread_mutex_unlock(&s->lock);
+    run_request(s, r);
+    pthread_mutex_lock(&s->lock);
+    r->finished_s = now_s();
+    s->in_use -= fp;
+    if(slot >= 0) s->busy[slot] = NULL;
+    slot = -1;
+    r->done = 1;
+    s->pending--;
+    pthread_cond_broadcast(&s->done);
+    pthread_cond_broadcast(&s->work);
+  }
+  pthread_mutex_unlock(&s->lock);
+  n2d_sync();
+  n2d_set_stream(NULL);
+  n2d_stream_destroy(stream);
+  return NULL;
+}
+
+int nec2c_cuda_server_create(nec2c_cuda_server **out, int device, int slots, size_t device_budget, int split)
+{
+  nec2c_cuda_server *s;
+  int i;
+  if(!out) return 0;
+  *out = NULL;
+  if(slots < 1 || slots > 64) { n2c_set_error("slots must be 1..64"); return 0; }
+  if(!n2d_set_device(device) || !n2d_device_ok()) return 0;
+  if(device_budget == 0) {
+    /* concurrency.c:131-136: keep max(1/5, 1 GiB) of the free memory back. */
+    size_t free_b = 0, total_b = 0, reserve;
+    if(!n2d_mem_info(&free_b, &total_b)) return 0;
+    reserve = free_b / 5 > ((size_t)1 << 30) ? free_b / 5 : ((size_t)1 << 30);
+    device_budget = free_b > reserve ? free_b - reserve : free_b / 2;
+  }
+  s = calloc(1, sizeof(*s));
+  if(!s) return 0;
+  s->device = device; s->slots = slots; s->split = split != 0; s->budget = device_budget;
+  s->cap = 64;
+  s->queue = calloc(s->cap, sizeof(*s->queue));
+  s->busy = calloc((size_t)slots, sizeof(*s->busy));
+  s->threads = calloc((size_t)slots, sizeof(*s->threads));
+  if(!s->queue || !s->busy || !s->threads) { free(s->queue); free(s->busy); free(s->threads); free(s); return 0; }
+  pthread_mutex_init(&s->lock, NULL);
+  pthread_cond_init(&s->work, NULL);
+  pthread_cond_init(&s->done, NULL);
+  for(i = 0; i < slots; ++i) {
+    if(pthread_create(&s->threads[i], NULL, worker, s) != 0) {
+      pthread_mutex_lock(&s->lock);
+      s->stop = 1;
+      pthread_cond_broadcast(&s->work);
+      pthread_mutex_unlock(&s->lock);
+      while(i-- > 0) pthread_join(s->threads[i], NULL);
+      free(s->queue); free(s->busy); free(s->threads); free(s);
+      n2c_set_error("worker thread creation failed");
+      return 0;
+    }
+  }
+  s->started = slots;
+  *out = s;
+  return 1;
+}
+
+int nec2c_cuda_server_submit(nec2c_cuda_server *s, nec2c_cuda_request *r)
+{
+  if(!s || !r) return 0;
+  if(r->kind == NEC2C_CUDA_REQUEST_DENSE) {
+    if(!r->matrix || !r->rhs || r->order == 0 || r->ld < r->order || r->rhs_count == 0 ||
+       r->rhs_stride < r->order) return 0;
+  } else if(r->kind == NEC2C_CUDA_REQUEST_VOLUME) {
+    if((!r->plan) == (!r->system) || !r->b || !r->x) return 0;
+  } else {
+    return 0;
+  }
+  pthread_mutex_lock(&s->lock);
+  if(s->stop) { pthread_mutex_unlock(&s->lock); return 0; }
+  if(s->count == s->cap) {
+    nec2c_cuda_request **q = malloc(2 * s->cap * sizeof(*q));
+    size_t i;
+    if(!q) { pthread_mutex_unlock(&s->lock); return 0; }
+    for(i = 0; i < s->count; ++i) q[i] = s->queue[(s->head + i) % s->cap];
+    free(s->queue);
+    s->queue = q; s->head = 0; s->cap *= 2;
+  }
+  r->done = 0; r->status = 0; r->skipped = 0; r->footprint = 0; r->error[0] = 0;
+  r->queued_s = now_s(); r->started_s = r->finished_s = 0;
+  s->queue[(s->head + s->count) % s->cap] = r;
+  s->count++;
+  s->pending++;
+  pthread_cond_broadcast(&s->work);
+  pthread_mutex_unlock(&s->lock);
+  return 1;
+}
+
+int nec2c_cuda_server_wait(nec2c_cuda_server *s, nec2c_cuda_request *r)
+{
+  if(!s || !r) return 0;
+  pthread_mutex_lock(&s->lock);
+  while(!r->done) pthread_cond_wait(&s->done, &s->lock);
+  pthread_mutex_unlock(&s->lock);
+  return r->status;
+}
+
+int nec2c_cuda_server_drain(nec2c_cuda_server *s)
+{
+  if(!s) return 0;
+  pthread_mutex_lock(&s->lock);
+  while(s->pending) pthread_cond_wait(&s->done, &s->lock);
+  pthread_mutex_unlock(&s->lock);
+  return 1;
+}
+
+size_t nec2c_cuda_server_budget(const nec2c_cuda_server *s) { return s ? s->budget : 0; }
+
+void nec2c_cuda_server_destroy(nec2c_cuda_server *s)
+{
+  int i;
+  if(!s) return;
+  nec2c_cuda_server_drain(s);
+  pthread_mutex_lock(&s->lock);
+  s->stop = 1;
+  pthread_cond_broadcast(&s->work);
+  pthread_mutex_unlock(&s->lock);
+  for(i = 0; i < s->started; ++i) pthread_join(s->threads[i], NULL);
+  pthread_mutex_destroy(&s->lock);
+  pthread_cond_destroy(&s->work);
+  pthread_cond_destroy(&s->done);
+  free(s->queue); free(s->busy); free(s->threads);
+  free(s);
+}

@@ -1,0 +1,175 @@
+"""Request server (nec2c_cuda_server_*): dense and volume solves submitted
+together run concurrently on worker streams, and each result is the same as
+when the request runs alone (bitwise: every kernel on the path reduces in a
+fixed order).  Dense solutions match numpy's FP64 solve to 1e-10 relative;
+the split-precision server's match the FP64 server's to 1e-10 relative.  The
+admission budget holds at every instant."""
+import numpy as np
+import pytest
+
+import cases
+import nec2c_b200 as nb
+
+pytestmark = pytest.mark.gpu
+
+
+def dense_case(n, seed, k=2):
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    a += np.diag(np.full(n, 0.5 * np.sqrt(n)))
+    ld = n + 3
+    st = np.zeros((ld, n), dtype=np.complex128, order="F")
+    st[:n, :n] = a.T
+    x = rng.standard_normal((n, k)) + 1j * rng.standard_normal((n, k))
+    rhs = np.zeros((n + 1, k), dtype=np.complex128, order="F")
+    rhs[:n] = a @ x
+    return a, st, rhs
+
+
+def volume_cases(near_tables):
+    out = []
+    for name, shape, fill, seed in (("rand_k0.3", (12, 9, 17), 0.5, 7), ("c0", (16, 16, 16), 1.0, 3)):
+        h, k, table = near_tables[name]
+        xyz = cases.random_lattice(shape, fill, seed)
+        eps = cases.random_eps(xyz.size // 3, seed + 1, er=(2.0, 4.0))
+        plan = nb.VolumePlan(shape, xyz, h, k, 3.0, table)
+        for c, e in enumerate(eps):
+            plan.set_permittivity(c, e)
+        rng = np.random.default_rng(seed + 2)
+        b = rng.standard_normal(plan.n) + 1j * rng.standard_normal(plan.n)
+        out.append((plan, b))
+    return out
+
+
+def submit_all(server, dense, volume):
+    """Interleaved dense and volume requests (each volume plan twice)."""
+    reqs, outs = [], []
+    vol = [(p, b) for p, b in volume] * 2
+    for i in range(max(len(dense), len(vol))):
+        if i < len(dense):
+            _, st, rhs = dense[i]
+            out = rhs.copy(order="F")
+            reqs.append(server.dense(st, out))
+            outs.append(out)
+        if i < len(vol):
+            plan, b = vol[i]
+            x = np.zeros_like(b)
+            reqs.append(server.volume(plan, b, x, rtol=1e-10, maxit=500))
+            outs.append(x)
+    return reqs, outs
+
+
+def max_concurrent_bytes(reqs):
+    events = sorted([(r.started_s, r.footprint) for r in reqs] + [(r.finished_s, -r.footprint) for r in reqs],
+                    key=lambda e: (e[0], e[1]))
+    cur = peak = 0
+    for _, d in events:
+        cur += d
+        peak = max(peak, cur)
+    return peak
+
+
+def test_same_alone_and_in_the_mix(near_tables):
+    dense = [dense_case(n, 100 + n) for n in (40, 200, 513, 1100, 777)]
+    volume = volume_cases(near_tables)
+    # Alone: one worker, each request waited for before the next is queued.
+    alone = nb.Server(slots=1)
+    ref = []
+    for i in range(len(dense)):
+        _, st, rhs = dense[i]
+        out = rhs.copy(order="F")
+        r = alone.dense(st, out)
+        assert alone.wait(r), r.error
+        ref.append(("dense", out, r))
+    for plan, b in volume:
+        x = np.zeros_like(b)
+        r = alone.volume(plan, b, x, rtol=1e-10, maxit=500)
+        assert alone.wait(r), r.error
+        ref.append(("volume", x, r))
+    alone.close()
+    # In the mix: four workers, everything queued at once.
+    mix = nb.Server(slots=4)
+    reqs, outs = submit_all(mix, dense, volume)
+    mix.drain()
+    for r in reqs:
+        assert r.done and r.status, r.error
+    # Requests overlapped on the device.
+    overlaps = sum(1 for a in reqs for b in reqs
+                   if a is not b and a.started_s < b.finished_s and b.started_s < a.finished_s)
+    assert overlaps > 0
+    assert max_concurrent_bytes(reqs) <= mix.budget()
+    # Same plan never in flight twice.
+    vol_reqs = [r for r in reqs if r.kind == nb.REQUEST_VOLUME]
+    for a in vol_reqs:
+        for b in vol_reqs:
+            if a is not b and a.plan == b.plan:
+                assert a.finished_s <= b.started_s or b.finished_s <= a.started_s
+    mix.close()
+    di = vi = 0
+    for r, out in zip(reqs, outs):
+        if r.kind == nb.REQUEST_DENSE:
+            kind, expect, rr = ref[di]
+            di += 1
+            a = dense[di - 1][0]
+            assert kind == "dense" and np.array_equal(out, expect)
+            sol = np.linalg.solve(a, (dense[di - 1][2])[: a.shape[0]])
+            assert np.linalg.norm(out[: a.shape[0]] - sol) / np.linalg.norm(sol) < 1e-10
+        else:
+            kind, expect, rr = ref[len(dense) + (vi % len(volume))]
+            vi += 1
+            assert kind == "volume" and np.array_equal(out, expect)
+            assert r.report.iterations == rr.report.iterations
+            assert r.report.relative_residual <= 1e-10
+
+
+def test_split_precision_server_matches_fp64():
+    dense = [dense_case(n, 300 + n, k=3) for n in (64, 600, 1500)]
+    outs = {}
+    for split in (False, True):
+        srv = nb.Server(slots=3, split=split)
+        res = []
+        reqs = []
+        for a, st, rhs in dense:
+            out = rhs.copy(order="F")
+            reqs.append(srv.dense(st, out))
+            res.append(out)
+        srv.drain()
+        for r in reqs:
+            assert r.status, r.error
+            if split:
+                assert r.report.iterations >= 1   # refinement steps, no FP64 fallback
+        srv.close()
+        outs[split] = res
+    for (a, _, _), x64, xs in zip(dense, outs[False], outs[True]):
+        n = a.shape[0]
+        assert np.linalg.norm(xs[:n] - x64[:n]) / np.linalg.norm(x64[:n]) < 1e-10
+
+
+def test_budget_limits_concurrency():
+    dense = [dense_case(n, 500 + n, k=1) for n in (900, 1000, 950, 1024)]
+    big = max(n for n in (900, 1000, 950, 1024))
+    budget = 16 * big * big + (1 << 20)      # room for one of these at a time
+    srv = nb.Server(slots=4, budget=budget)
+    assert srv.budget() == budget
+    reqs = []
+    for a, st, rhs in dense:
+        reqs.append(srv.dense(st, rhs.copy(order="F")))
+    srv.drain()
+    for r in reqs:
+        assert r.status, r.error
+        assert r.footprint <= budget
+    assert max_concurrent_bytes(reqs) <= budget
+    srv.close()
+
+
+def test_rejects_malformed_requests():
+    srv = nb.Server(slots=1)
+    import ctypes as C
+    r = nb.Request()
+    r.kind = 7
+    assert not nb.load().nec2c_cuda_server_submit(srv.h, C.byref(r))
+    r.kind = nb.REQUEST_VOLUME          # neither plan nor system
+    assert not nb.load().nec2c_cuda_server_submit(srv.h, C.byref(r))
+    r.kind = nb.REQUEST_DENSE           # no matrix
+    assert not nb.load().nec2c_cuda_server_submit(srv.h, C.byref(r))
+    srv.close()
