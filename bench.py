@@ -83,6 +83,20 @@ def near_table():
     return table
 
 
+def near_tables_all():
+    """{case: (h, k, table)} of every case in tests/golden/near_tensors.json."""
+    with open(os.path.join(ROOT, "tests", "golden", "near_tensors.json")) as f:
+        raw = json.load(f)
+    out = {}
+    for name, c in raw.items():
+        table = {}
+        for row in c["tensors"]:
+            vals = np.array(row[3:], dtype=np.float64)
+            table[tuple(int(t) for t in row[:3])] = vals[0::2] + 1j * vals[1::2]
+        out[name] = (c["h"], c["k"], table)
+    return out
+
+
 class Clocks:
     """nvidia-smi sampler over the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -384,8 +398,11 @@ def run_ours(args, rank, world, local_rank):
     peak, peak_kind = peaks()
     achieved = bytes32 / (mv32_ms * 1e-3) / 1e9
 
-    # Config-1 shaped dense LU (1984 unknowns), FP64, through the classic ABI.
+    # Config-1 shaped dense LU (1984 unknowns), both forms.
     dense = dense_bench(nb, torch, stream)
+    # Config-4 shaped serving stream (bounded), both forms.
+    serving = serving_bench(nb, torch) if world == 1 else None
+    lib.nec2c_cuda_set_stream(C.c_void_p(stream.cuda_stream))
 
     if rank != 0:
         return 0
@@ -411,6 +428,7 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic_bytes": bytes32, "ms": mv32_ms},
         "matvec_fp64": {"ms": mv64_ms, "achieved_gbs": bytes64 / (mv64_ms * 1e-3) / 1e9},
         "dense_lu_c1": dense,
+        "serving_c4": serving,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }
@@ -445,30 +463,192 @@ def profile_driver(args, lib, nb, torch, stream, plan_m, plan_d, w):
 
 
 def dense_bench(nb, torch, stream):
+    """Config-1 shaped dense solve (1984 unknowns, one right-hand side) in the
+    FP64 form and the split-precision form (FP32 tensor-core factors + FP64
+    refinement), through the classic C ABI with host buffers, plus the device
+    factor alone on resident matrices."""
     n = 1984
     rng = np.random.default_rng(1)
     a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
     a += np.diag(np.full(n, 0.5 * math.sqrt(n)))
     xe = rng.standard_normal(n) + 1j * rng.standard_normal(n)
     b = a @ xe
+    lib = nb.load()
+    out = {"order": n, "flops": 8 * n ** 3 / 3,
+           "note": "factor + solve through the classic C ABI (host buffers); device_factor_ms: "
+                   "factorisation of a resident matrix alone"}
+    sols = {}
+    for form in ("cuda", "cuda-mixed"):
+        nb.dense_backend_set(form)
+        times = []
+        for _ in range(3):
+            st = np.asfortranarray(a.T.copy())
+            rhs = np.asfortranarray(b.reshape(n, 1).copy())
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ok, piv = nb.factor_classic(st)
+            ok = ok and nb.solve_classic_many(st, piv, rhs)
+            times.append(time.perf_counter() - t0)
+            if not ok:
+                raise RuntimeError("dense solve failed: " + nb.last_error())
+        sols[form] = rhs[:, 0].copy()
+        t = min(times)
+        out[form] = {"ms": 1e3 * t, "solves_per_s": 1 / t, "gflops": out["flops"] / t / 1e9,
+                     "rel_err_vs_exact": float(np.linalg.norm(rhs[:, 0] - xe) / np.linalg.norm(xe))}
+        if form == "cuda-mixed":
+            out[form]["refinement_steps"] = int(lib.nec2c_cuda_dense_last_refinement())
     nb.dense_backend_set("cuda")
-    times, err = [], None
-    for it in range(3):
-        st = np.asfortranarray(a.T.copy())
-        rhs = np.asfortranarray(b.reshape(n, 1).copy())
-        torch.cuda.synchronize()
+    lib.nec2c_cuda_dense_release()
+    out["cuda-mixed"]["rel_err_vs_fp64_gpu"] = float(
+        np.linalg.norm(sols["cuda-mixed"] - sols["cuda"]) / np.linalg.norm(sols["cuda"]))
+    # Device factor alone (resident matrices, CUDA events).
+    f64 = lib.n2d_lu_factor
+    f64.restype, f64.argtypes = C.c_int, [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_int,
+                                          C.c_int, C.POINTER(C.c_int)]
+    f32 = lib.n2d_lu_factor32
+    f32.restype, f32.argtypes = C.c_int, [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_int,
+                                          C.POINTER(C.c_int)]
+    d64 = torch.from_numpy(a).cuda()
+    ld32 = n + (n & 1)
+    a32 = np.zeros((n, ld32), dtype=np.complex64)
+    a32[:, :n] = a
+    d32 = torch.from_numpy(a32).cuda()
+    piv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    for form, src in (("cuda", d64), ("cuda-mixed", d32)):
+        work = src.clone()
+        ts = []
+        for i in range(4):
+            work.copy_(src)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            info = C.c_int(0)
+            e0.record(stream)
+            ok = (f64(work.data_ptr(), n, n, piv.data_ptr(), 0, 0, C.byref(info)) if form == "cuda" else
+                  f32(work.data_ptr(), n, ld32, piv.data_ptr(), 0, C.byref(info)))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if not ok or info.value:
+                raise RuntimeError("device factor failed: " + nb.last_error())
+            if i:
+                ts.append(e0.elapsed_time(e1))
+        out[form]["device_factor_ms"] = min(ts)
+    return out
+
+
+# Config-4 shaped serving stream (bounded): 60% wire-only dense MoM solves of
+# 200-3000 unknowns (log-uniform), 40% volume solves on resident plans of two
+# lattices (0.2-lambda cubes voxelised 16^3 and 32^3 at 300 MHz, eps_r~U[2,10],
+# tand 0.05) with GMRES(30) to rtol 1e-6, two resident replicas per lattice.
+# One solve per request (one frequency).
+SERVE_REQUESTS = 96
+SERVE_SLOTS = 8
+
+
+def serving_bench(nb, torch):
+    rng = np.random.default_rng(4)
+    table_all = near_tables_all()
+    sizes = sorted(set(int(round(math.exp(v))) for v in rng.uniform(math.log(200), math.log(3000), 10)))
+    pool = []
+    for i, n in enumerate(sizes):
+        r = np.random.default_rng(100 + i)
+        a = r.standard_normal((n, n)) + 1j * r.standard_normal((n, n))
+        a += np.diag(np.full(n, 0.5 * math.sqrt(n)))
+        st = np.asfortranarray(a.T)
+        x = r.standard_normal(n) + 1j * r.standard_normal(n)
+        pool.append((st, np.asfortranarray((a @ x).reshape(n, 1))))
+    lam = C0 / 300e6
+    geoms = []
+    for name, nside in (("c0", 16), ("c3_32", 32)):
+        h, k, table = table_all[name]
+        g = np.arange(nside)
+        xyz = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1).astype(np.uintp)
+        cells = nside ** 3
+        r = np.random.default_rng(200 + nside)
+        eps = r.uniform(2.0, 10.0, cells) * (1 - 0.05j)
+        bvec = np.zeros(3 * cells, dtype=np.complex128)
+        z = xyz[2::3].astype(np.float64)
+        bvec[0::3] = 2 * np.exp(-1j * k * h * (z + 0.5)) * math.sin(k * h / 2) / (k * h / 2)
+        geoms.append(((nside,) * 3, xyz, h, k, eps, table, bvec))
+    kinds = rng.random(SERVE_REQUESTS) < 0.6
+    picks = rng.integers(0, 1 << 30, SERVE_REQUESTS)
+
+    def plans(mixed):
+        out = []
+        for shape, xyz, h, k, eps, table, bvec in geoms:
+            for _ in range(2):   # two resident replicas per lattice
+                p = nb.VolumePlan(shape, xyz, h, k, eps[0], table, mixed=mixed)
+                for c, e in enumerate(eps):
+                    p.set_permittivity(c, e)
+                out.append((p, bvec))
+        return out
+
+    def run(split, gaps, slots=SERVE_SLOTS):
+        ps = plans(split)
+        srv = nb.Server(slots=slots, split=split)
+        # warm-up: one request of each kind per plan / a mid-size matrix
+        warm = [srv.volume(p, b, np.zeros_like(b), rtol=1e-6, maxit=2000) for p, b in ps]
+        st, rhs = pool[len(pool) // 2]
+        warm.append(srv.dense(st, rhs.copy(order="F")))
+        srv.drain()
+        reqs, outs = [], []
         t0 = time.perf_counter()
-        ok, piv = nb.factor_classic(st)
-        ok = ok and nb.solve_classic_many(st, piv, rhs)
-        t = time.perf_counter() - t0
-        if not ok:
-            raise RuntimeError("dense solve failed")
-        times.append(t)
-        err = float(np.linalg.norm(rhs[:, 0] - xe) / np.linalg.norm(xe))
-    t = min(times)
-    flops = 8 * n ** 3 / 3
-    return {"order": n, "ms": 1e3 * t, "solves_per_s": 1 / t, "gflops": flops / t / 1e9,
-            "rel_err": err, "note": "FP64 factor + solve through the classic C ABI (host buffers)"}
+        for i in range(SERVE_REQUESTS):
+            if gaps is not None:
+                target = t0 + gaps[i]
+                while time.perf_counter() < target:
+                    time.sleep(min(1e-3, max(0.0, target - time.perf_counter())))
+            if kinds[i]:
+                st, rhs = pool[picks[i] % len(pool)]
+                o = rhs.copy(order="F")
+                reqs.append(srv.dense(st, o))
+            else:
+                p, b = ps[picks[i] % len(ps)]
+                o = np.zeros_like(b)
+                reqs.append(srv.volume(p, b, o, rtol=1e-6, maxit=2000))
+            outs.append(o)
+        srv.drain()
+        for r in reqs:
+            if not r.status:
+                raise RuntimeError("serving request failed: " + r.error.decode())
+        first = min(r.queued_s for r in reqs)
+        last = max(r.finished_s for r in reqs)
+        lat = sorted(1e3 * (r.finished_s - r.queued_s) for r in reqs)
+        res = {"solves_per_s": len(reqs) / (last - first),
+               "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+               "makespan_s": last - first}
+        srv.close()
+        for p, _ in ps:
+            p.close()
+        return res, outs
+
+    lib = nb.load()
+    l0 = lib.nec2c_cuda_launch_count()
+    out = {"requests": SERVE_REQUESTS, "dense": int(kinds.sum()), "volume": int((~kinds).sum()),
+           "slots": SERVE_SLOTS, "dense_orders": sizes,
+           "lattices": ["16^3 (12288 unknowns)", "32^3 (98304 unknowns)"]}
+    sat = {}
+    for split in (False, True):
+        sat[split], outs = run(split, None)
+        if split:
+            outs_m = outs
+        else:
+            outs_d = outs
+    err = max(float(np.linalg.norm(m - d) / np.linalg.norm(d)) for m, d in zip(outs_m, outs_d))
+    out["saturation"] = {"fp64": sat[False], "mixed": sat[True]}
+    # The plain FP64 GPU form: one request at a time, FP64 plans and LU.
+    plain, _ = run(False, None, slots=1)
+    out["plain_fp64_one_at_a_time"] = plain
+    out["mixed_serving_vs_plain_fp64"] = sat[True]["solves_per_s"] / plain["solves_per_s"]
+    rate = 0.7 * sat[True]["solves_per_s"]
+    gaps = np.cumsum(np.random.default_rng(5).exponential(1.0 / rate, SERVE_REQUESTS))
+    pois = {}
+    for split in (False, True):
+        pois[split], _ = run(split, gaps)
+    out["poisson"] = {"rate_per_s": rate, "fp64": pois[False], "mixed": pois[True]}
+    out["mixed_vs_fp64_solves_per_s"] = sat[True]["solves_per_s"] / sat[False]["solves_per_s"]
+    out["max_rel_err_mixed_vs_fp64"] = err
+    out["gpu_launches"] = int(lib.nec2c_cuda_launch_count() - l0)
+    return out
 
 
 def main():

@@ -95,7 +95,7 @@ unsigned grid_for(long long work, int threads) {
 }
 
 // Per-column maxima: cleared, filled by a kernel, read back (synchronises).
-int read_maxima(unsigned long long *dev, long long count, double *host) {
+int read_maxima(const unsigned long long *dev, long long count, double *host) {
   unsigned long long tmp[64];
   for (long long j0 = 0; j0 < count; j0 += 64) {
     const long long m = count - j0 < 64 ? count - j0 : 64;
@@ -138,7 +138,7 @@ extern "C" int n2d_residual(const double *a, long long n, long long ld, const do
   if (!n2d_memset(m, 0, (size_t)nrhs * sizeof(unsigned long long))) return 0;
   residual_kernel<<<grid_for(n * 32, 256), 256, 0, n2c_stream()>>>((const double2 *)a, n, ld, (const double2 *)x,
                                                                     (const double2 *)b, (double2 *)r, nrhs, ldb, m);
-  return n2c_check_launch("residual") && read_maxima(m, nrhs, rnorm_host);
+  return n2c_check_launch("residual") && (!rnorm_host || read_maxima(m, nrhs, rnorm_host));
 }
 
 extern "C" int n2d_add_correction(double *x, const double *d, long long n, long long nrhs, long long ldb,
@@ -146,5 +146,9 @@ extern "C" int n2d_add_correction(double *x, const double *d, long long n, long 
   unsigned long long *m = (unsigned long long *)norm_dev;
   if (!n2d_memset(m, 0, (size_t)nrhs * sizeof(unsigned long long))) return 0;
   add_kernel<<<grid_for(n * nrhs, 256), 256, 0, n2c_stream()>>>((double2 *)x, (const double2 *)d, n, nrhs, ldb, m);
-  return n2c_check_launch("correction") && read_maxima(m, nrhs, xnorm_host);
+  return n2c_check_launch("correction") && (!xnorm_host || read_maxima(m, nrhs, xnorm_host));
+}
+
+extern "C" int n2d_read_norms(const void *norm_dev, long long count, double *host) {
+  return read_maxima((unsigned long long *)norm_dev, count, host);
 }

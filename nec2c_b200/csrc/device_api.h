@@ -151,6 +151,9 @@ int n2d_residual(const double *a_dev, long long order, long long ld, const doubl
                  double *rnorm_host);
 int n2d_add_correction(double *x_dev, const double *d_dev, long long order, long long nrhs, long long ldb,
                        void *norm_dev, double *xnorm_host);
+/* With a NULL host pointer the two above leave their norms on the device;
+   this reads count of them back (synchronises). */
+int n2d_read_norms(const void *norm_dev, long long count, double *host);
 /* In-place device transpose of an order x order block (leading dims lda/ldb). */
 int n2d_transpose(const double *src_dev, long long lds, double *dst_dev, long long ldd,
                   long long rows, long long cols);

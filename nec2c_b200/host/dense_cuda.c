@@ -85,8 +85,8 @@ static int solve_refined(size_t n, const split_factors *f, double *b, size_t cou
   const double cte = f->anorm * DBL_EPSILON * sqrt((double)n);
   double *x = n2d_alloc_async(n * count * CPX), *r = n2d_alloc_async(n * count * CPX);
   double *d = n2d_alloc_async(n * count * CPX);
-  void *norm = n2d_alloc_async(count * sizeof(unsigned long long));
-  double *rn = malloc(count * sizeof(double)), *xn = malloc(count * sizeof(double));
+  unsigned long long *norm = n2d_alloc_async(2 * count * sizeof(unsigned long long));
+  double *rn = malloc(2 * count * sizeof(double)), *xn = rn ? rn + count : NULL;
   int ok = x && r && d && norm && rn && xn && n2d_memset(x, 0, n * count * CPX) && n2d_copy_d2d(r, b, n * count * CPX);
   int done = 0, it;
   *steps = 0;
@@ -94,8 +94,8 @@ static int solve_refined(size_t n, const split_factors *f, double *b, size_t cou
     size_t j;
     ok = n2d_copy_d2d(d, r, n * count * CPX) &&
          n2d_lu_solve32(f->lu32, N, (long long)f->ld32, f->piv, d, N, K) &&
-         n2d_add_correction(x, d, N, K, N, norm, xn) &&
-         n2d_residual(f->orig, N, N, x, b, r, K, N, norm, rn);
+         n2d_add_correction(x, d, N, K, N, norm + count, NULL) &&
+         n2d_residual(f->orig, N, N, x, b, r, K, N, norm, NULL) && n2d_read_norms(norm, 2 * K, rn);
     done = ok;
     for(j = 0; ok && j < count; ++j) if(!(rn[j] <= xn[j] * cte)) done = 0;
     if(done) *steps = it;
@@ -112,7 +112,7 @@ static int solve_refined(size_t n, const split_factors *f, double *b, size_t cou
   }
   ok = ok && n2d_copy_d2d(b, x, n * count * CPX);
   n2d_free_async(x); n2d_free_async(r); n2d_free_async(d); n2d_free_async(norm);
-  free(rn); free(xn);
+  free(rn);
   return ok;
 }
 
