@@ -49,9 +49,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", choices=["matvec", "solve"],
+    ap.add_argument("--only", choices=["matvec", "solve", "lu"],
                     help="profiling driver: build the plans, run --steps FP32 and FP64 products "
-                         "(matvec) or --steps mixed solves (solve), print timings and exit")
+                         "(matvec) or --steps mixed solves (solve), or factor the config-1 shaped "
+                         "matrix --steps times in each LU form (lu); print timings and exit")
     return ap.parse_args()
 
 
@@ -287,6 +288,8 @@ def run_ours(args, rank, world, local_rank):
         raise RuntimeError("CUDA backend unavailable: " + nb.last_error())
     stream = torch.cuda.current_stream()
     lib.nec2c_cuda_set_stream(C.c_void_p(stream.cuda_stream))
+    if args.only == "lu":
+        return lu_driver(args, nb, torch, stream)
     w = workload()
     table = near_table()
 
@@ -462,16 +465,68 @@ def profile_driver(args, lib, nb, torch, stream, plan_m, plan_d, w):
     return 0
 
 
+def c1_matrix():
+    n = 1984
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    a += np.diag(np.full(n, 0.5 * math.sqrt(n)))
+    return a
+
+
+def device_factor(nb, torch, stream, a, form, reps):
+    """Factors a resident copy of a (reps + 1 times, the first untimed) with
+    the device LU of the given form; returns the fastest time in ms."""
+    lib = nb.load()
+    n = a.shape[0]
+    if form == "cuda":
+        f = lib.n2d_lu_factor
+        f.restype, f.argtypes = C.c_int, [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_int, C.c_int,
+                                          C.POINTER(C.c_int)]
+        src = torch.from_numpy(a).cuda()
+        ld = n
+    else:
+        f = lib.n2d_lu_factor32
+        f.restype, f.argtypes = C.c_int, [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_int,
+                                          C.POINTER(C.c_int)]
+        ld = n + (n & 1)
+        a32 = np.zeros((n, ld), dtype=np.complex64)
+        a32[:, :n] = a
+        src = torch.from_numpy(a32).cuda()
+    work = src.clone()
+    piv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ts = []
+    for i in range(reps + 1):
+        work.copy_(src)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        info = C.c_int(0)
+        e0.record(stream)
+        ok = (f(work.data_ptr(), n, ld, piv.data_ptr(), 0, 0, C.byref(info)) if form == "cuda" else
+              f(work.data_ptr(), n, ld, piv.data_ptr(), 0, C.byref(info)))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if not ok or info.value:
+            raise RuntimeError("device factor failed: " + nb.last_error())
+        if i:
+            ts.append(e0.elapsed_time(e1))
+    return min(ts)
+
+
+def lu_driver(args, nb, torch, stream):
+    a = c1_matrix()
+    out = {form: device_factor(nb, torch, stream, a, form, max(1, args.steps)) for form in ("cuda", "cuda-mixed")}
+    print(json.dumps({"profile": "lu", "order": a.shape[0], "device_factor_ms": out}))
+    return 0
+
+
 def dense_bench(nb, torch, stream):
     """Config-1 shaped dense solve (1984 unknowns, one right-hand side) in the
     FP64 form and the split-precision form (FP32 tensor-core factors + FP64
     refinement), through the classic C ABI with host buffers, plus the device
     factor alone on resident matrices."""
-    n = 1984
-    rng = np.random.default_rng(1)
-    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
-    a += np.diag(np.full(n, 0.5 * math.sqrt(n)))
-    xe = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    a = c1_matrix()
+    n = a.shape[0]
+    xe = np.random.default_rng(11).standard_normal(n) + 1j * np.random.default_rng(12).standard_normal(n)
     b = a @ xe
     lib = nb.load()
     out = {"order": n, "flops": 8 * n ** 3 / 3,
@@ -502,36 +557,8 @@ def dense_bench(nb, torch, stream):
     out["cuda-mixed"]["rel_err_vs_fp64_gpu"] = float(
         np.linalg.norm(sols["cuda-mixed"] - sols["cuda"]) / np.linalg.norm(sols["cuda"]))
     # Device factor alone (resident matrices, CUDA events).
-    f64 = lib.n2d_lu_factor
-    f64.restype, f64.argtypes = C.c_int, [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_int,
-                                          C.c_int, C.POINTER(C.c_int)]
-    f32 = lib.n2d_lu_factor32
-    f32.restype, f32.argtypes = C.c_int, [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_int,
-                                          C.POINTER(C.c_int)]
-    d64 = torch.from_numpy(a).cuda()
-    ld32 = n + (n & 1)
-    a32 = np.zeros((n, ld32), dtype=np.complex64)
-    a32[:, :n] = a
-    d32 = torch.from_numpy(a32).cuda()
-    piv = torch.zeros(n, dtype=torch.int32, device="cuda")
-    for form, src in (("cuda", d64), ("cuda-mixed", d32)):
-        work = src.clone()
-        ts = []
-        for i in range(4):
-            work.copy_(src)
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            info = C.c_int(0)
-            e0.record(stream)
-            ok = (f64(work.data_ptr(), n, n, piv.data_ptr(), 0, 0, C.byref(info)) if form == "cuda" else
-                  f32(work.data_ptr(), n, ld32, piv.data_ptr(), 0, C.byref(info)))
-            e1.record(stream)
-            torch.cuda.synchronize()
-            if not ok or info.value:
-                raise RuntimeError("device factor failed: " + nb.last_error())
-            if i:
-                ts.append(e0.elapsed_time(e1))
-        out[form]["device_factor_ms"] = min(ts)
+    for form in ("cuda", "cuda-mixed"):
+        out[form]["device_factor_ms"] = device_factor(nb, torch, stream, a, form, 3)
     return out
 
 

@@ -227,13 +227,19 @@ __global__ void __launch_bounds__(512) arnoldi_kernel(GmBuffers b, long long n, 
 // Classical Gram-Schmidt with selective reorthogonalisation (mixed form):
 //   dots   h = V^H w                          (warp per basis vector)
 //   update w -= V h, ||w||^2                   (thread per element)
-// and a second dots/update pass only when ||w_new|| < ||w|| / sqrt(2) (the
-// Daniel-Gragg-Kaufman-Stewart criterion; "twice is enough").  Both passes
-// add into the Hessenberg column, as the two MGS passes of vie_iterative.c
-// do.  Kernel boundaries are the only grid synchronisation; reductions are
+// and a second dots/update pass only when the projection cancelled more than
+// a factor REORTH of the norm (||w_new|| < ||w|| / REORTH).  One CGS pass
+// loses orthogonality by about eps (||w|| / ||w_new||)^2, so the basis stays
+// orthogonal to ~100 eps per vector; GMRES here needs far less (the restart
+// test is an FP64 true residual, so lost orthogonality could only cost
+// iterations, not accuracy), and the 1/sqrt(2) threshold of the
+// Daniel-Gragg-Kaufman-Stewart criterion would rerun the pass on nearly every
+// Arnoldi step.  Both passes add into the Hessenberg column, as the two MGS
+// passes of vie_iterative.c do.  Kernel boundaries are the only grid synchronisation; reductions are
 // fixed-order block partials finished by the last block (deterministic).
 constexpr int MAXM = 30;   // restarts up to MAXM use this path
 constexpr int CGS_E = 4;   // elements per lane in the dots kernel
+constexpr double REORTH = 10.0;   // cancellation factor that triggers the second pass
 constexpr int CGS_GROUP = 32 * CGS_E;   // elements per warp group
 constexpr size_t CGS_SMEM = (size_t)(32 * CGS_GROUP) * sizeof(double2);
 
@@ -387,7 +393,7 @@ __global__ void __launch_bounds__(256) cgs_update_kernel(GmBuffers b, long long 
   if (threadIdx.x != 0) return;
   *b.ticket = 0;
   const double after = sqrt(all.x);
-  if (P == 0 && isfinite(after) && after < sqrt(0.5 * st->before_sq)) {
+  if (P == 0 && isfinite(after) && REORTH * after < sqrt(st->before_sq)) {
     st->reorth = 1;
     st->reorth_count += 1;
     return;
