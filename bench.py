@@ -49,10 +49,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", choices=["matvec", "solve", "lu"],
+    ap.add_argument("--only", choices=["matvec", "solve", "lu", "serving"],
                     help="profiling driver: build the plans, run --steps FP32 and FP64 products "
                          "(matvec) or --steps mixed solves (solve), or factor the config-1 shaped "
-                         "matrix --steps times in each LU form (lu); print timings and exit")
+                         "matrix --steps times in each LU form (lu), or run the serving stream "
+                         "(serving); print timings and exit")
     return ap.parse_args()
 
 
@@ -290,6 +291,9 @@ def run_ours(args, rank, world, local_rank):
     lib.nec2c_cuda_set_stream(C.c_void_p(stream.cuda_stream))
     if args.only == "lu":
         return lu_driver(args, nb, torch, stream)
+    if args.only == "serving":
+        print(json.dumps({"profile": "serving", "serving_c4": serving_bench(nb, torch)}))
+        return 0
     w = workload()
     table = near_table()
 
@@ -643,6 +647,9 @@ def serving_bench(nb, torch):
         res = {"solves_per_s": len(reqs) / (last - first),
                "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                "makespan_s": last - first}
+        for kind, name in ((nb.REQUEST_DENSE, "dense"), (nb.REQUEST_VOLUME, "volume")):
+            svc = [1e3 * (r.finished_s - r.started_s) for r in reqs if r.kind == kind]
+            res[name + "_service_ms_mean"] = sum(svc) / max(1, len(svc))
         srv.close()
         for p, _ in ps:
             p.close()

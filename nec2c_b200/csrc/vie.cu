@@ -17,6 +17,7 @@
 #include <vector>
 #include "common.cuh"
 #include "device_api.h"
+#include <mutex>
 #include "fft_engine.cuh"
 #include "runtime.cuh"
 #include "vie_internal.cuh"
@@ -49,6 +50,37 @@ static int launch_pass_rr(int mode, const PassArgs<C> &a, size_t smem, long long
   if (tiles > 0x7fffffffLL) { n2c_set_error("FFT pass grid too large"); return 0; }
   k<<<(unsigned)tiles, 256, smem, n2c_stream()>>>(a);
   return n2c_check_launch("fft pass");
+}
+
+template <typename C, int R1, int R2>
+static int occupancy_rr(int mode, size_t smem) {
+  void (*k)(PassArgs<C>) = mode == 5 ? fft_zline_pass<C, R1, R2, false, false>
+                          : mode == 6 ? fft_zline_pass<C, R1, R2, true, false>
+                          : mode == 7 ? fft_zline_pass<C, R1, R2, false, true>
+                                      : fft_zline_pass<C, R1, R2, true, true>;
+  int blocks = 0;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
+      cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, 256, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return blocks;
+}
+
+// Resident blocks per SM of a staged z pass (modes 5-8) with smem bytes.
+template <typename C>
+static int zline_occupancy(int mode, int L, size_t smem) {
+  switch (L) {
+    case 16: return occupancy_rr<C, 16, 1>(mode, smem);
+    case 32: return occupancy_rr<C, 8, 4>(mode, smem);
+    case 64: return occupancy_rr<C, 8, 8>(mode, smem);
+    case 128: return occupancy_rr<C, 16, 8>(mode, smem);
+    case 256: return occupancy_rr<C, 16, 16>(mode, smem);
+    case 512: return occupancy_rr<C, 32, 16>(mode, smem);
+    case 1024: return occupancy_rr<C, 32, 32>(mode, smem);
+  }
+  return 0;
 }
 
 template <typename C>
@@ -89,6 +121,47 @@ static int zlines_per_tile(int L, size_t elem, int unit) {
   return nl;
 }
 
+// Lines per tile of a staged z pass covering `groups` groups of `unit` lines,
+// chosen to fill whole waves of resident blocks: among heights from half the
+// default up to buffers of 80 KB, the one that leaves the fewest block slots
+// of the last wave idle (a grid just past one wave would take two).  Ties go
+// to more resident blocks per SM, then to the taller tile.  Cached per shape.
+template <typename C>
+static int zline_tile(int mode, int L, int unit, long long groups) {
+  struct Entry { int mode, L, unit, elem; long long groups; int nl; };
+  static Entry cache[32];
+  static int used = 0;
+  static std::mutex lock;
+  {
+    std::lock_guard<std::mutex> hold(lock);
+    for (int i = 0; i < used; ++i)
+      if (cache[i].mode == mode && cache[i].L == L && cache[i].unit == unit && cache[i].elem == (int)sizeof(C) &&
+          cache[i].groups == groups)
+        return cache[i].nl;
+  }
+  const int def = zlines_per_tile(L, sizeof(C), unit);
+  const int sms = n2c_sm_count();
+  int best = def, best_bps = 0;
+  double best_eff = -1.0;
+  for (int nl = (def / 2 / unit > 0 ? def / 2 / unit : 1) * unit; (size_t)2 * (nl + 1) * L * sizeof(C) <= 80 * 1024;
+       nl += unit) {
+    const size_t smem = (size_t)2 * (nl + 1) * L * sizeof(C);
+    const int bps = zline_occupancy<C>(mode, L, smem);
+    if (bps <= 0) continue;
+    const long long per = nl / unit, tiles = (groups + per - 1) / per, slots = (long long)sms * bps;
+    const long long waves = (tiles + slots - 1) / slots;
+    const double eff = (double)tiles / (double)(waves * slots);
+    if (eff > best_eff + 0.02 || (eff > best_eff - 0.02 && (bps > best_bps || (bps == best_bps && nl > best)))) {
+      if (eff > best_eff) best_eff = eff;
+      best = nl;
+      best_bps = bps;
+    }
+  }
+  std::lock_guard<std::mutex> hold(lock);
+  if (used < 32) cache[used++] = Entry{mode, L, unit, (int)sizeof(C), groups, best};
+  return best;
+}
+
 template <typename C>
 static int axis_pass(int mode, int L, const C *in, C *out, const C *tw, long long B, long long I,
                      long long A_in, long long A_out, int n_in, int n_out) {
@@ -98,7 +171,7 @@ static int axis_pass(int mode, int L, const C *in, C *out, const C *tw, long lon
   a.lines = B * I; a.I = I; a.A_in = A_in; a.A_out = A_out; a.n_in = n_in; a.n_out = n_out;
   a.gate = n2c_gate();
   if (I == 1) {
-    a.NL = zlines_per_tile(L, sizeof(C), 1);
+    a.NL = zline_tile<C>(mode + 5, L, 1, a.lines);
     const long long tiles = (a.lines + a.NL - 1) / a.NL;
     return launch_pass<C>(mode + 5, L, a, (size_t)2 * (a.NL + 1) * L * sizeof(C), tiles);
   }
@@ -622,7 +695,7 @@ static int z_cell_pass(int mode, n2d_vie *p, const C *in, C *out, const C *tw, c
   a.lines = 3 * nx * ny; a.I = 1;
   if (mode == 3) { a.A_in = nz; a.A_out = Pz; a.n_in = (int)nz; a.n_out = (int)Pz; }
   else { a.A_in = Pz; a.A_out = nz; a.n_in = (int)Pz; a.n_out = (int)nz; }
-  a.NL = zlines_per_tile((int)Pz, sizeof(C), 3);
+  a.NL = zline_tile<C>(mode == 3 ? 7 : 8, (int)Pz, 3, nx * ny);
   a.gate = n2c_gate();
   a.cx = x; a.cy = y; a.eps = p->eps; a.box_cell = p->box_cell;
   a.self0 = p->self[0]; a.self1 = p->self[1]; a.self2 = p->self[2];
