@@ -666,16 +666,51 @@ __global__ void __launch_bounds__(256) gemm_update_kernel(double2 *C, const doub
 // matrix.c:1523-1555 solves).  One block per RHS; each 32-row step is solved
 // by warp 0 and the rows below / above are updated by the whole block with
 // contiguous row segments.
+// One right-hand side per CTA (1024 threads).  Interchanges: the sequential
+// swaps of ipiv are composed into an index permutation in shared memory by
+// one thread (orders up to SOLVE_PERM_MAX; beyond, the swaps run on x
+// directly), then x is gathered through it in registers.  Forward and back
+// substitution in blocks of 32 rows: warp 0 solves the diagonal block
+// column-oriented (x_k broadcast by shuffle, each later row subtracting its
+// L or U entry times x_k), then all warps update the remaining rows (warp per
+// row, a 32-wide dot product).
+constexpr int SOLVE_THREADS = 1024;
+constexpr int SOLVE_PERM_MAX = 8 * 1024;    // 8 bytes of shared memory per row, 8 values per thread
+constexpr int SOLVE_REG = SOLVE_PERM_MAX / SOLVE_THREADS;
 template <typename S>
-__global__ void __launch_bounds__(1024) lu_solve_kernel(const S *a, long long n, long long ld,
-                                                        const int *ipiv, double2 *b, long long ldb) {
+__global__ void __launch_bounds__(SOLVE_THREADS) lu_solve_kernel(const S *a, long long n, long long ld,
+                                                                 const int *ipiv, double2 *b, long long ldb) {
+  extern __shared__ int perm_smem[];
   double2 *x = b + blockIdx.x * ldb;
   __shared__ double2 xs[32];
-  if (threadIdx.x == 0)
+  if (n <= SOLVE_PERM_MAX) {
+    int *idx = perm_smem, *pv = perm_smem + n;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) { idx[i] = (int)i; pv[i] = ipiv[i] - 1; }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int i = 0; i < (int)n; ++i) {
+        const int q = pv[i];
+        if (q != i) { const int t = idx[q]; idx[q] = idx[i]; idx[i] = t; }
+      }
+    __syncthreads();
+    double2 v[SOLVE_REG];
+#pragma unroll
+    for (int r = 0; r < SOLVE_REG; ++r) {
+      const long long i = threadIdx.x + (long long)r * SOLVE_THREADS;
+      if (i < n) v[r] = x[idx[i]];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < SOLVE_REG; ++r) {
+      const long long i = threadIdx.x + (long long)r * SOLVE_THREADS;
+      if (i < n) x[i] = v[r];
+    }
+  } else if (threadIdx.x == 0) {
     for (long long i = 0; i < n; ++i) {
       const long long pi = ipiv[i] - 1;
       if (pi != i) { const double2 t = x[pi]; x[pi] = x[i]; x[i] = t; }
     }
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   // Forward: L unit lower.
@@ -683,16 +718,10 @@ __global__ void __launch_bounds__(1024) lu_solve_kernel(const S *a, long long n,
     const int w = (int)(n - j0 < 32 ? n - j0 : 32);
     if (warp == 0) {
       double2 v = lane < w ? x[j0 + lane] : make_double2(0, 0);
-      for (int i = 1; i < w; ++i) {
-        // Row j0+i of the diagonal block against the solved entries above it.
-        const double2 l = lane < i ? to_d(a[(j0 + i) * ld + j0 + lane]) : make_double2(0, 0);
-        double2 s = cmul(l, make_double2(__shfl_sync(0xffffffffu, v.x, lane), __shfl_sync(0xffffffffu, v.y, lane)));
-        s = lane < i ? s : make_double2(0, 0);
-        for (int o = 16; o > 0; o >>= 1) {
-          s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
-          s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
-        }
-        if (lane == i) v = csub(v, s);
+      for (int k = 0; k < w - 1; ++k) {
+        const double2 l = (lane > k && lane < w) ? to_d(a[(j0 + lane) * ld + j0 + k]) : make_double2(0, 0);
+        const double2 xk = make_double2(__shfl_sync(0xffffffffu, v.x, k), __shfl_sync(0xffffffffu, v.y, k));
+        if (lane > k && lane < w) v = csub(v, cmul(l, xk));
       }
       if (lane < w) { x[j0 + lane] = v; xs[lane] = v; }
     }
@@ -713,15 +742,11 @@ __global__ void __launch_bounds__(1024) lu_solve_kernel(const S *a, long long n,
     const int w = (int)(j1 - j0);
     if (warp == 0) {
       double2 v = lane < w ? x[j0 + lane] : make_double2(0, 0);
-      for (int i = w - 1; i >= 0; --i) {
-        const double2 u = (lane > i && lane < w) ? to_d(a[(j0 + i) * ld + j0 + lane]) : make_double2(0, 0);
-        double2 s = cmul(u, v);
-        s = (lane > i && lane < w) ? s : make_double2(0, 0);
-        for (int o = 16; o > 0; o >>= 1) {
-          s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
-          s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
-        }
-        if (lane == i) v = cdiv(csub(v, s), to_d(a[(j0 + i) * ld + j0 + i]));
+      for (int k = w - 1; k >= 0; --k) {
+        if (lane == k) v = cdiv(v, to_d(a[(j0 + k) * ld + j0 + k]));
+        const double2 u = lane < k ? to_d(a[(j0 + lane) * ld + j0 + k]) : make_double2(0, 0);
+        const double2 xk = make_double2(__shfl_sync(0xffffffffu, v.x, k), __shfl_sync(0xffffffffu, v.y, k));
+        if (lane < k) v = csub(v, cmul(u, xk));
       }
       if (lane < w) { x[j0 + lane] = v; xs[lane] = v; }
     }
@@ -1009,10 +1034,25 @@ extern "C" int n2d_lu_factor32(float *a_dev, long long n, long long ld, int *ipi
   return factor_alloc((float2 *)a_dev, n, ld, ipiv, rule, info_host);
 }
 
+static size_t solve_smem(long long n) { return n <= SOLVE_PERM_MAX ? (size_t)8 * n : 0; }
+template <typename S>
+static int solve_configure() {
+  static int done = 0;
+  if (done) return 1;
+  if (cudaFuncSetAttribute(lu_solve_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * SOLVE_PERM_MAX) !=
+      cudaSuccess) {
+    n2c_set_error("triangular solve: shared memory configuration failed");
+    return 0;
+  }
+  done = 1;
+  return 1;
+}
+
 extern "C" int n2d_lu_solve(const double *a_dev, long long n, long long ld, const int *ipiv, double *b_dev,
                             long long ldb, long long nrhs) {
   if (n <= 0 || nrhs <= 0) return 1;
-  lu_solve_kernel<double2><<<(unsigned)nrhs, 1024, 0, n2c_stream()>>>((const double2 *)a_dev, n, ld, ipiv,
+  if (!solve_configure<double2>()) return 0;
+  lu_solve_kernel<double2><<<(unsigned)nrhs, SOLVE_THREADS, solve_smem(n), n2c_stream()>>>((const double2 *)a_dev, n, ld, ipiv,
                                                              (double2 *)b_dev, ldb);
   return n2c_check_launch("lu_solve");
 }
@@ -1022,7 +1062,8 @@ extern "C" int n2d_lu_solve(const double *a_dev, long long n, long long ld, cons
 extern "C" int n2d_lu_solve32(const float *a_dev, long long n, long long ld, const int *ipiv, double *b_dev,
                               long long ldb, long long nrhs) {
   if (n <= 0 || nrhs <= 0) return 1;
-  lu_solve_kernel<float2><<<(unsigned)nrhs, 1024, 0, n2c_stream()>>>((const float2 *)a_dev, n, ld, ipiv,
+  if (!solve_configure<float2>()) return 0;
+  lu_solve_kernel<float2><<<(unsigned)nrhs, SOLVE_THREADS, solve_smem(n), n2c_stream()>>>((const float2 *)a_dev, n, ld, ipiv,
                                                                      (double2 *)b_dev, ldb);
   return n2c_check_launch("lu_solve");
 }
