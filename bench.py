@@ -37,9 +37,9 @@ C0 = 299792458.0
 SEED = 2
 MAXIT = 10000
 # dram__bytes_read.sum + dram__bytes_write.sum per FP32 matvec on this
-# workload, summed over its kernels, from the ncu capture summarised in
-# profiles/matvec_c2_fp32.md (None until a capture exists).
-MATVEC_TRAFFIC_BYTES = None
+# workload, summed over its five kernels, from the ncu capture summarised in
+# profiles/fft_matvec_c2_64cube.md (the intermediate grids stay in L2).
+MATVEC_TRAFFIC_BYTES = 120.3e6
 
 
 def parse():
