@@ -165,6 +165,18 @@ int nec2c_cuda_dense_solve_classic_many(size_t order, const nec2c_cuda_complex *
    left unchanged. */
 int nec2c_cuda_dense_solve_row_major(nec2c_cuda_complex *matrix, nec2c_cuda_complex *rhs,
                                      size_t order);
+/* No single counterpart in the reference: factr + solve (matrix.c:1313-1416,
+   1523-1555) of count independent systems (the wire blocks of many
+   frequencies or geometries) at once.  Systems of order <= 64 are factored
+   and solved together in one launch (one CTA per system); larger ones run
+   through the classic factor and solve.  Each matrix is NEC's storage
+   (leading dimension lds[i]) and receives its factors as
+   nec2c_cuda_dense_factor_classic writes them; pivots[i] (optional) the
+   1-based pivots; rhs[i] the solution.  status[i] is 1 when system i was
+   solved, 0 when singular or failed; returns 1 when all were solved. */
+int nec2c_cuda_dense_solve_batched(size_t count, const size_t *orders, nec2c_cuda_complex *const *matrices,
+                                   const size_t *lds, int *const *pivots, nec2c_cuda_complex *const *rhs,
+                                   int *status);
 /* Drops the device copies kept between a factor and its solves. */
 void nec2c_cuda_dense_release(void);
 /* No counterpart in the reference (diagnostic of the "cuda-mixed" form):

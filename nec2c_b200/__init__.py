@@ -92,6 +92,7 @@ def load():
         "nec2c_cuda_dense_factor_classic": (i, [sz, vp, sz, vp]),
         "nec2c_cuda_dense_factor_device_static": (i, [sz, vp, sz, vp]),
         "nec2c_cuda_dense_last_refinement": (i, []),
+        "nec2c_cuda_dense_solve_batched": (i, [sz, vp, vp, vp, vp, vp, vp]),
         "nec2c_cuda_server_create": (i, [C.POINTER(vp), i, i, sz, i]),
         "nec2c_cuda_server_submit": (i, [vp, C.POINTER(Request)]),
         "nec2c_cuda_server_wait": (i, [vp, C.POINTER(Request)]),
@@ -344,3 +345,23 @@ class Server:
             self._keep.clear()
 
     __del__ = close
+
+
+def solve_batched(systems):
+    """Factors and solves a ragged batch [(storage, rhs), ...] in place
+    (storage: Fortran ld x n NEC storage; rhs: n complex); returns
+    (all_ok, status list, pivots list)."""
+    count = len(systems)
+    orders = (C.c_size_t * count)(*[st.shape[1] for st, _ in systems])
+    lds = (C.c_size_t * count)(*[st.shape[0] for st, _ in systems])
+    mats = (C.c_void_p * count)()
+    rhs = (C.c_void_p * count)()
+    pivs = [np.zeros(st.shape[1], dtype=np.int32) for st, _ in systems]
+    pp = (C.c_void_p * count)()
+    for k, (st, b) in enumerate(systems):
+        assert st.dtype == np.complex128 and st.flags.f_contiguous
+        assert b.dtype == np.complex128 and b.flags.c_contiguous
+        mats[k], rhs[k], pp[k] = _ptr(st), _ptr(b), _ptr(pivs[k])
+    status = (C.c_int * count)()
+    ok = load().nec2c_cuda_dense_solve_batched(count, orders, mats, lds, pp, rhs, status)
+    return bool(ok), list(status), pivs

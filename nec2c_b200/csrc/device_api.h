@@ -154,6 +154,14 @@ int n2d_add_correction(double *x_dev, const double *d_dev, long long order, long
 /* With a NULL host pointer the two above leave their norms on the device;
    this reads count of them back (synchronises). */
 int n2d_read_norms(const void *norm_dev, long long count, double *host);
+/* Ragged batch of count small systems (orders[i] <= 64) in one launch:
+   mats_dev holds the row-major matrices back to back, rhs_dev and piv_dev the
+   right-hand sides and pivots (orders[i] entries each), info_dev (count ints,
+   zeroed) the first singular column + 1 of each; systems_dev is scratch of
+   n2d_lu_batched_descriptor_bytes(count) bytes. */
+int n2d_lu_batched(double *mats_dev, double *rhs_dev, int *piv_dev, const int *orders, long long count,
+                   int *info_dev, void *systems_dev);
+size_t n2d_lu_batched_descriptor_bytes(long long count);
 /* In-place device transpose of an order x order block (leading dims lda/ldb). */
 int n2d_transpose(const double *src_dev, long long lds, double *dst_dev, long long ldd,
                   long long rows, long long cols);

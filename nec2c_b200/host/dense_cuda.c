@@ -264,3 +264,86 @@ int nec2c_cuda_dense_solve_row_major(nec2c_cuda_complex *matrix, nec2c_cuda_comp
   n2d_free(a); n2d_free(b); n2d_free(piv);
   return ok;
 }
+
+/* Ragged batch of small systems (orders <= 64) in one launch: factored in
+   place (factr's pivots and factors, as nec2c_cuda_dense_factor_classic
+   writes them) and solved for one right-hand side each.  Larger orders go
+   through the classic factor and solve one after another. */
+int nec2c_cuda_dense_solve_batched(size_t count, const size_t *orders, nec2c_cuda_complex *const *matrices,
+                                   const size_t *lds, int *const *pivots, nec2c_cuda_complex *const *rhs,
+                                   int *status)
+{
+  size_t i, small = 0, a_total = 0, b_total = 0;
+  int all = 1, ok = 1;
+  int *order32 = NULL, *info = NULL, *piv_host = NULL;
+  double complex *a_host = NULL, *b_host = NULL;
+  double *a_dev = NULL, *b_dev = NULL;
+  int *piv_dev = NULL, *info_dev = NULL;
+  void *desc_dev = NULL;
+  if(count == 0) return 1;
+  if(!orders || !matrices || !lds || !rhs || !status) return 0;
+  if(!n2d_device_ok()) return 0;
+  for(i = 0; i < count; ++i) {
+    if(orders[i] == 0 || !matrices[i] || !rhs[i] || lds[i] < orders[i]) { n2c_set_error("invalid system %zu", i); return 0; }
+    status[i] = 0;
+    if(orders[i] <= 64) { small++; a_total += orders[i] * orders[i]; b_total += orders[i]; }
+  }
+  if(small) {
+    size_t k = 0, ao = 0, bo = 0;
+    order32 = malloc(small * sizeof(int));
+    info = calloc(small, sizeof(int));
+    piv_host = malloc(b_total * sizeof(int));
+    a_host = malloc(a_total * sizeof(double complex));
+    b_host = malloc(b_total * sizeof(double complex));
+    ok = order32 && info && piv_host && a_host && b_host;
+    for(i = 0; ok && i < count; ++i) {
+      const size_t n = orders[i];
+      size_t r;
+      if(n > 64) continue;
+      order32[k++] = (int)n;
+      /* NEC storage column r is algebraic row r: copy the first n entries. */
+      for(r = 0; r < n; ++r) memcpy(a_host + ao + r * n, matrices[i] + r * lds[i], n * sizeof(double complex));
+      memcpy(b_host + bo, rhs[i], n * sizeof(double complex));
+      ao += n * n;
+      bo += n;
+    }
+    a_dev = ok ? n2d_alloc_async(a_total * CPX) : NULL;
+    b_dev = ok ? n2d_alloc_async(b_total * CPX) : NULL;
+    piv_dev = ok ? n2d_alloc_async(b_total * sizeof(int)) : NULL;
+    info_dev = ok ? n2d_alloc_async(small * sizeof(int)) : NULL;
+    desc_dev = ok ? n2d_alloc_async(n2d_lu_batched_descriptor_bytes((long long)small)) : NULL;
+    ok = ok && a_dev && b_dev && piv_dev && info_dev && desc_dev &&
+         n2d_upload(a_dev, a_host, a_total * CPX) && n2d_upload(b_dev, b_host, b_total * CPX) &&
+         n2d_memset(info_dev, 0, small * sizeof(int)) &&
+         n2d_lu_batched(a_dev, b_dev, piv_dev, order32, (long long)small, info_dev, desc_dev) &&
+         n2d_download(a_host, a_dev, a_total * CPX) && n2d_download(b_host, b_dev, b_total * CPX) &&
+         n2d_download(piv_host, piv_dev, b_total * sizeof(int)) && n2d_download(info, info_dev, small * sizeof(int));
+    for(i = 0, k = 0, ao = 0, bo = 0; ok && i < count; ++i) {
+      const size_t n = orders[i];
+      size_t r;
+      if(n > 64) continue;
+      for(r = 0; r < n; ++r) memcpy(matrices[i] + r * lds[i], a_host + ao + r * n, n * sizeof(double complex));
+      memcpy(rhs[i], b_host + bo, n * sizeof(double complex));
+      if(pivots && pivots[i]) memcpy(pivots[i], piv_host + bo, n * sizeof(int));
+      status[i] = info[k] == 0;
+      if(!status[i]) all = 0;
+      ao += n * n;
+      bo += n;
+      k++;
+    }
+    n2d_free_async(a_dev); n2d_free_async(b_dev); n2d_free_async(piv_dev); n2d_free_async(info_dev);
+    n2d_free_async(desc_dev);
+    free(order32); free(info); free(piv_host); free(a_host); free(b_host);
+    if(!ok) return 0;
+  }
+  for(i = 0; i < count; ++i) {
+    int *p;
+    if(orders[i] <= 64) continue;
+    p = (pivots && pivots[i]) ? pivots[i] : malloc(orders[i] * sizeof(int));
+    status[i] = p && nec2c_cuda_dense_factor_classic(orders[i], matrices[i], lds[i], p) &&
+                nec2c_cuda_dense_solve_classic(orders[i], matrices[i], lds[i], p, rhs[i]);
+    if(!(pivots && pivots[i])) free(p);
+    if(!status[i]) all = 0;
+  }
+  return all;
+}

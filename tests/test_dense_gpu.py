@@ -139,3 +139,39 @@ def test_split_precision_refined_solve(n):
     finally:
         nb.dense_backend_set("cuda")
         nb.load().nec2c_cuda_dense_release()
+
+
+def test_batched_ragged_matches_oracle():
+    """Ragged batch (wire-block sized systems in one launch, plus two above
+    the one-launch limit): per system the same pivots as factr, U to the dense
+    tests' tolerance, the solution within 1e-12 of the oracle's; a singular
+    system in the batch is reported without disturbing the others."""
+    sizes = [1, 2, 11, 21, 33, 41, 64, 17, 65, 100]
+    systems, ref = [], []
+    for k, n in enumerate(sizes):
+        a = mom_like(n, 900 + k)
+        if k == 7:
+            a[:, 3] = 0.0            # singular
+        ld = n + (k % 3)
+        st = nec_storage(a, ld)
+        rng = np.random.default_rng(k)
+        x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        b = np.ascontiguousarray(a @ x)
+        systems.append((st, b.copy()))
+        ref.append((a, st.copy(order="F"), b, ld))
+    assert nb.dense_backend_set("cuda")
+    ok, status, pivs = nb.solve_batched(systems)
+    assert not ok                      # the singular one
+    for k, (n, (st, xb), piv, (a, st0, b, ld)) in enumerate(zip(sizes, systems, pivs, ref)):
+        if k == 7:
+            assert status[k] == 0
+            continue
+        assert status[k] == 1, k
+        po = np.zeros(n, dtype=np.int32)
+        assert oracle().oracle_factr(n, ptr(st0), ptr(po), ld)
+        assert np.array_equal(piv, po), k
+        U, U_o = np.triu(st[:n, :n].T), np.triu(st0[:n, :n])
+        assert np.max(np.abs(U - U_o)) / np.max(np.abs(U_o)) < 1e-12, k
+        bo = b.copy()
+        oracle().oracle_solve(n, ptr(st0), ptr(po), ptr(bo), ld)
+        assert np.linalg.norm(xb - bo) / np.linalg.norm(bo) < 1e-12, k
