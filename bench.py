@@ -407,6 +407,8 @@ def run_ours(args, rank, world, local_rank):
 
     # Config-1 shaped dense LU (1984 unknowns), both forms.
     dense = dense_bench(nb, torch, stream)
+    # Config-3 shaped wire blocks, ragged batch in one launch.
+    batched = batched_bench(nb, torch)
     # Config-4 shaped serving stream (bounded), both forms.
     serving = serving_bench(nb, torch) if world == 1 else None
     lib.nec2c_cuda_set_stream(C.c_void_p(stream.cuda_stream))
@@ -435,6 +437,7 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic_bytes": bytes32, "ms": mv32_ms},
         "matvec_fp64": {"ms": mv64_ms, "achieved_gbs": bytes64 / (mv64_ms * 1e-3) / 1e9},
         "dense_lu_c1": dense,
+        "batched_wire_blocks_c3": batched,
         "serving_c4": serving,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
@@ -564,6 +567,50 @@ def dense_bench(nb, torch, stream):
     for form in ("cuda", "cuda-mixed"):
         out[form]["device_factor_ms"] = device_factor(nb, torch, stream, a, form, 3)
     return out
+
+
+def batched_bench(nb, torch):
+    """Config-3 shaped wire blocks: 128 frequencies of the 21-segment dipole
+    plus 64 dipoles of 11-41 segments (seeded), each block factored and solved:
+    the ragged batch in one call against one classic factor + solve per block."""
+    rng = np.random.default_rng(6)
+    sizes = [21] * 128 + [int(v) for v in rng.integers(11, 42, 64)]
+    mats = []
+    for k, n in enumerate(sizes):
+        r = np.random.default_rng(1000 + k)
+        a = r.standard_normal((n, n)) + 1j * r.standard_normal((n, n))
+        a += np.diag(np.full(n, 0.5 * math.sqrt(n)))
+        mats.append((np.asfortranarray(a.T), np.ascontiguousarray(a @ (r.standard_normal(n) + 0j))))
+
+    def batch():
+        sy = [(st.copy(order="F"), b.copy()) for st, b in mats]
+        t0 = time.perf_counter()
+        ok, status, _ = nb.solve_batched(sy)
+        t = time.perf_counter() - t0
+        if not ok:
+            raise RuntimeError("batched solve failed")
+        return t, sy
+
+    def one_by_one():
+        sy = [(st.copy(order="F"), b.copy().reshape(-1, 1).copy(order="F")) for st, b in mats]
+        t0 = time.perf_counter()
+        for st, b in sy:
+            ok, piv = nb.factor_classic(st)
+            if not ok or not nb.solve_classic_many(st, piv, b):
+                raise RuntimeError("classic solve failed")
+        return time.perf_counter() - t0, sy
+
+    nb.dense_backend_set("cuda")
+    batch()
+    tb, sb = min((batch() for _ in range(3)), key=lambda r: r[0])
+    one_by_one()
+    ts, ss = min((one_by_one() for _ in range(2)), key=lambda r: r[0])
+    nb.load().nec2c_cuda_dense_release()
+    err = max(float(np.linalg.norm(x1 - x2[:, 0]) / np.linalg.norm(x2[:, 0])) for (_, x1), (_, x2) in zip(sb, ss))
+    return {"systems": len(sizes), "orders": "128 x 21 + 64 in 11..41",
+            "one_launch": {"ms": 1e3 * tb, "solves_per_s": len(sizes) / tb},
+            "one_call_each": {"ms": 1e3 * ts, "solves_per_s": len(sizes) / ts},
+            "max_rel_diff": err, "note": "host buffers through the C ABI, wall clock"}
 
 
 # Config-4 shaped serving stream (bounded): 60% wire-only dense MoM solves of
