@@ -278,6 +278,24 @@ CONFIG = {"workload": "c2: 64^3-voxel inhomogeneous dielectric block, side 1 lam
           "l2": "solve working set > L2 (Krylov basis 390 MB); matvec timings flush L2 (256 MB write)"}
 
 
+# ------------------------------------------------------------ replicas
+def max_over_ranks(ms, world, device):
+    """The slowest rank's device time (replicas: every rank runs the whole
+    workload on its own GPU; the job takes as long as the slowest)."""
+    if world <= 1:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world, steps, total_ms):
+    """Whole-job solves/s: every rank solved `steps` systems in at most
+    total_ms."""
+    return world * steps / (total_ms * 1e-3)
+
+
 # ------------------------------------------------------------------ our arm
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -341,11 +359,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
     launches = lib.nec2c_cuda_launch_count() - launches0
     step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms), world, "cuda")
     iterations = rep.iterations
     x_mixed = x_dev.clone()
 
@@ -416,7 +430,7 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return 0
     cpu = None if (args.no_cpu_baseline or world > 1) else cpu_baseline(w, rep64.iterations)
-    value = world * args.steps / (total_ms * 1e-3)
+    value = replica_rate(world, args.steps, total_ms)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
