@@ -4,6 +4,7 @@
 #include <stdio.h>
 #include <string.h>
 #include <atomic>
+#include <thread>
 #include "common.cuh"
 #include "device_api.h"
 #include "runtime.cuh"
@@ -96,10 +97,47 @@ extern "C" int n2d_mem_info(size_t *free_bytes, size_t *total_bytes) {
 // buffers so that the host memcpy of one chunk overlaps the DMA of the other.
 // Pinned (page-locked or registered) host memory is copied directly.
 static const size_t STAGE_CHUNK = 8u << 20, STAGE_MIN = 1u << 20;
+
+// Host rows copied by several threads (a single thread moves pageable memory
+// at a fraction of the host's bandwidth): half the host cores, at most 8,
+// shared among the copies in progress on all threads (several streams'
+// workers copy at once), rows split evenly; small copies stay on the calling
+// thread.
+static std::atomic<int> g_copies{0};
+static void copy_rows(char *dst, size_t dp, const char *src, size_t sp, size_t width, size_t rows) {
+  const size_t bytes = width * rows;
+  const int active = g_copies.fetch_add(1) + 1;
+  unsigned hw = std::thread::hardware_concurrency() / 2 / (unsigned)active;
+  unsigned nt = hw < 1 ? 1 : (hw > 8 ? 8 : hw);
+  if (bytes < (4u << 20) || rows < 2 * nt) nt = 1;
+  auto part = [=](unsigned i) {
+    const size_t r0 = rows * i / nt, r1 = rows * (i + 1) / nt;
+    if (dp == width && sp == width) memcpy(dst + r0 * width, src + r0 * width, (r1 - r0) * width);
+    else for (size_t r = r0; r < r1; ++r) memcpy(dst + r * dp, src + r * sp, width);
+  };
+  if (nt == 1) {
+    part(0);
+  } else {
+    std::thread th[8];
+    for (unsigned i = 1; i < nt; ++i) th[i] = std::thread(part, i);
+    part(0);
+    for (unsigned i = 1; i < nt; ++i) th[i].join();
+  }
+  g_copies.fetch_sub(1);
+}
 struct Stage {
   void *buf[2] = {nullptr, nullptr};
   cudaEvent_t ev[2] = {nullptr, nullptr};
   bool ok = false;
+  // Released when the owning thread exits (worker threads of a server);
+  // errors after the process has torn CUDA down are ignored.
+  ~Stage() {
+    for (int i = 0; i < 2; ++i) {
+      if (ev[i]) cudaEventDestroy(ev[i]);
+      if (buf[i]) cudaFreeHost(buf[i]);
+    }
+    cudaGetLastError();
+  }
 };
 static thread_local Stage g_stage;
 
@@ -129,7 +167,7 @@ static int staged_h2d(void *dst, size_t dp, const void *src, size_t hp, size_t w
     const size_t nr = rows - r0 < per ? rows - r0 : per;
     N2C_CHECK(cudaEventSynchronize(s.ev[k]));
     char *b = (char *)s.buf[k];
-    for (size_t r = 0; r < nr; ++r) memcpy(b + r * width, (const char *)src + (r0 + r) * hp, width);
+    copy_rows(b, width, (const char *)src + r0 * hp, hp, width, nr);
     N2C_CHECK(cudaMemcpy2DAsync((char *)dst + r0 * dp, dp, b, width, width, nr, cudaMemcpyHostToDevice, g_stream));
     N2C_CHECK(cudaEventRecord(s.ev[k], g_stream));
   }
@@ -152,8 +190,7 @@ static int staged_d2h(void *dst, size_t hp, const void *src, size_t dp, size_t w
     if (c + 1 < chunks && !issue(c + 1)) return 0;
     N2C_CHECK(cudaEventSynchronize(s.ev[c & 1]));
     const size_t r0 = c * per, nr = rows - r0 < per ? rows - r0 : per;
-    const char *b = (const char *)s.buf[c & 1];
-    for (size_t r = 0; r < nr; ++r) memcpy((char *)dst + (r0 + r) * hp, b + r * width, width);
+    copy_rows((char *)dst + r0 * hp, hp, (const char *)s.buf[c & 1], width, width, nr);
   }
   return 1;
 }
