@@ -883,6 +883,13 @@ struct LookAhead {
   int dev = -1;
   cudaStream_t aux = nullptr;
   cudaEvent_t next = nullptr, panel = nullptr;
+  // Released when the owning thread exits.
+  ~LookAhead() {
+    if (aux) cudaStreamDestroy(aux);
+    if (next) cudaEventDestroy(next);
+    if (panel) cudaEventDestroy(panel);
+    cudaGetLastError();
+  }
 };
 static thread_local LookAhead g_look;
 
