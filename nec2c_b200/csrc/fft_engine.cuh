@@ -93,7 +93,26 @@ template <typename C> struct PassArgs {
   int *flag;                    // non-finite input / output
   double *partials, *norm;      // |y|^2 reduction (norm NULL: none)
   unsigned int *ticket;
+  // z passes: reciprocals ceil(2^32 / d) of the tile height NL, the lattice
+  // columns per cell tile NP = NL / 3 and n_out, so that the index arithmetic
+  // divides by a multiply-high (exact for the indices of a tile); 0 when
+  // d == 1.
+  unsigned nl_div, np_div, nout_div;
 };
+
+// n / d for 0 <= n < 2^32 / d through the reciprocal m = ceil(2^32 / d)
+// (m == 0 stands for d == 1).
+__device__ __forceinline__ int fdiv(int n, unsigned m) { return m ? (int)__umulhi((unsigned)n, m) : n; }
+
+// z / d with one real division: conj(d) z / |d|^2 (the split-precision form,
+// whose transforms are FP32 anyway; the FP64 form divides as C99 does).
+__device__ __forceinline__ double2 cdiv_once(double2 z, double2 d) {
+  const double r = 1.0 / (d.x * d.x + d.y * d.y);
+  return make_double2((z.x * d.x + z.y * d.y) * r, (z.y * d.x - z.x * d.y) * r);
+}
+template <typename C> __device__ __forceinline__ double2 jacobi_apply(double2 v, double2 d) {
+  return sizeof(C) == sizeof(float2) ? cdiv_once(v, d) : cdiv(v, d);
+}
 
 template <typename C> __device__ __forceinline__ double2 jacobi_divisor(const PassArgs<C> &a, double2 e, int c) {
   const double2 s = c == 0 ? a.self0 : (c == 1 ? a.self1 : a.self2);
@@ -378,9 +397,9 @@ namespace n2c {
 // Forward four-step on shared memory: input natural order in S, output
 // natural order in T.
 template <typename C, int R1, int R2>
-__device__ __forceinline__ void smem_forward(C *S, C *T, int NL, int NLP, const C *__restrict__ tw) {
+__device__ __forceinline__ void smem_forward(C *S, C *T, int NL, int NLP, unsigned nlm, const C *__restrict__ tw) {
   for (int item = threadIdx.x; item < NL * R2; item += blockDim.x) {
-    const int t = item % NL, j2 = item / NL;
+    const int j2 = fdiv(item, nlm), t = item - j2 * NL;
     C v[R1];
 #pragma unroll
     for (int j1 = 0; j1 < R1; ++j1) v[j1] = S[(j2 + R2 * j1) * NLP + t];
@@ -393,7 +412,7 @@ __device__ __forceinline__ void smem_forward(C *S, C *T, int NL, int NLP, const 
   }
   __syncthreads();
   for (int item = threadIdx.x; item < NL * R1; item += blockDim.x) {
-    const int t = item % NL, k1 = item / NL;
+    const int k1 = fdiv(item, nlm), t = item - k1 * NL;
     C w[R2];
 #pragma unroll
     for (int j2 = 0; j2 < R2; ++j2) w[j2] = S[(j2 + R2 * k1) * NLP + t];
@@ -407,9 +426,9 @@ __device__ __forceinline__ void smem_forward(C *S, C *T, int NL, int NLP, const 
 // Inverse four-step (unnormalised): input natural order in S, output natural
 // order in S (T is scratch).
 template <typename C, int R1, int R2>
-__device__ __forceinline__ void smem_inverse(C *S, C *T, int NL, int NLP, const C *__restrict__ tw) {
+__device__ __forceinline__ void smem_inverse(C *S, C *T, int NL, int NLP, unsigned nlm, const C *__restrict__ tw) {
   for (int item = threadIdx.x; item < NL * R1; item += blockDim.x) {
-    const int t = item % NL, k1 = item / NL;
+    const int k1 = fdiv(item, nlm), t = item - k1 * NL;
     C w[R2];
 #pragma unroll
     for (int k2 = 0; k2 < R2; ++k2) w[k2] = S[(k1 + R1 * k2) * NLP + t];
@@ -422,7 +441,7 @@ __device__ __forceinline__ void smem_inverse(C *S, C *T, int NL, int NLP, const 
   }
   __syncthreads();
   for (int item = threadIdx.x; item < NL * R2; item += blockDim.x) {
-    const int t = item % NL, n1 = item / NL;
+    const int n1 = fdiv(item, nlm), t = item - n1 * NL;
     C v[R1];
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1) v[k1] = T[(n1 + R2 * k1) * NLP + t];
@@ -441,7 +460,7 @@ __device__ __forceinline__ long long zline_global(const PassArgs<C> &a, bool cel
     const long long l = (long long)blockIdx.x * a.NL + t;
     return l < a.lines ? l : -1;
   }
-  const int c = t / NP, p = t - c * NP;
+  const int c = fdiv(t, a.np_div), p = t - c * NP;
   const long long pos = (long long)blockIdx.x * NP + p;
   return pos < a.nxy ? c * a.nxy + pos : -1;
 }
@@ -470,7 +489,7 @@ __global__ void __launch_bounds__(256, 3) fft_zline_pass(PassArgs<C> a) {
           double sgn = 1;
           if (a.mirror && cell >= a.mirror) { cell -= a.mirror; if (c < 2) sgn = -1; }
           double2 v = a.cx[3 * cell + c];
-          if (a.precondition) v = cdiv(v, jacobi_divisor(a, a.eps[cell], c));
+          if (a.precondition) v = jacobi_apply<C>(v, jacobi_divisor(a, a.eps[cell], c));
           if (a.flag && !finite2(v)) *a.flag = 1;
           val = from_d<C>(make_double2(sgn * v.x, sgn * v.y));
         }
@@ -486,21 +505,21 @@ __global__ void __launch_bounds__(256, 3) fft_zline_pass(PassArgs<C> a) {
   }
   __syncthreads();
   C *R = S;
-  if (INV) smem_inverse<C, R1, R2>(S, T, NL, NLP, a.tw);
-  else { smem_forward<C, R1, R2>(S, T, NL, NLP, a.tw); R = T; }
+  if (INV) smem_inverse<C, R1, R2>(S, T, NL, NLP, a.nl_div, a.tw);
+  else { smem_forward<C, R1, R2>(S, T, NL, NLP, a.nl_div, a.tw); R = T; }
   // ---- store
   if (CELLS && INV) {
     double sq = 0;
     const long long p0 = (long long)blockIdx.x * NP;
     for (int idx = threadIdx.x; idx < NP * a.n_out * 3; idx += blockDim.x) {
-      const int c = idx % 3, rest = idx / 3, e = rest % a.n_out, p = rest / a.n_out;
+      const int c = idx % 3, rest = idx / 3, p = fdiv(rest, a.nout_div), e = rest - p * a.n_out;
       const long long pos = p0 + p;
       if (pos >= a.nxy) continue;
       const long long cell = a.box_cell[pos * a.A_out + e];
       if (cell < 0 || (a.mirror && cell >= a.mirror)) continue;
       const double2 ep = a.eps[cell], em1 = make_double2(ep.x - 1.0, ep.y);
       double2 z = a.cx[3 * cell + c];
-      if (a.precondition) z = cdiv(z, jacobi_divisor(a, ep, c));
+      if (a.precondition) z = jacobi_apply<C>(z, jacobi_divisor(a, ep, c));
       const double2 v = csub(cmul(ep, z), cmul(em1, to_d(R[e * NLP + c * NP + p])));
       a.cy[3 * cell + c] = v;
       if (a.flag && !finite2(v)) *a.flag = 1;
@@ -523,7 +542,7 @@ __global__ void __launch_bounds__(256, 3) fft_zline_pass(PassArgs<C> a) {
     }
   } else {
     for (int idx = threadIdx.x; idx < NL * a.n_out; idx += blockDim.x) {
-      const int t = idx / a.n_out, e = idx - t * a.n_out;
+      const int t = fdiv(idx, a.nout_div), e = idx - t * a.n_out;
       const long long l = zline_global(a, CELLS, NP, t);
       if (l >= 0) a.out[l * a.A_out + e] = R[e * NLP + t];
     }

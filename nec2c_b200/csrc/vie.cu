@@ -115,6 +115,11 @@ static int lines_per_tile(int L, int ncomp, size_t elem) {
 // Lines per tile of a staged z pass: two padded [L][NL+1] buffers within
 // ~56 KB (three to four blocks per SM); `unit` keeps NL a multiple of 3 for
 // cell tiles.
+// ceil(2^32 / d) for the device's multiply-high division (0 for d == 1).
+static unsigned div_magic(long long d) {
+  return d <= 1 ? 0u : (unsigned)((0x100000000ULL + (unsigned long long)d - 1) / (unsigned long long)d);
+}
+
 static int zlines_per_tile(int L, size_t elem, int unit) {
   int nl = 32 * unit;
   while (nl > unit && (size_t)2 * (nl + 1) * L * elem > 56 * 1024) nl -= unit;
@@ -172,6 +177,8 @@ static int axis_pass(int mode, int L, const C *in, C *out, const C *tw, long lon
   a.gate = n2c_gate();
   if (I == 1) {
     a.NL = zline_tile<C>(mode + 5, L, 1, a.lines);
+    a.nl_div = div_magic(a.NL);
+    a.nout_div = div_magic(a.n_out);
     const long long tiles = (a.lines + a.NL - 1) / a.NL;
     return launch_pass<C>(mode + 5, L, a, (size_t)2 * (a.NL + 1) * L * sizeof(C), tiles);
   }
@@ -696,6 +703,9 @@ static int z_cell_pass(int mode, n2d_vie *p, const C *in, C *out, const C *tw, c
   if (mode == 3) { a.A_in = nz; a.A_out = Pz; a.n_in = (int)nz; a.n_out = (int)Pz; }
   else { a.A_in = Pz; a.A_out = nz; a.n_in = (int)Pz; a.n_out = (int)nz; }
   a.NL = zline_tile<C>(mode == 3 ? 7 : 8, (int)Pz, 3, nx * ny);
+  a.nl_div = div_magic(a.NL);
+  a.np_div = div_magic(a.NL / 3);
+  a.nout_div = div_magic(a.n_out);
   a.gate = n2c_gate();
   a.cx = x; a.cy = y; a.eps = p->eps; a.box_cell = p->box_cell;
   a.self0 = p->self[0]; a.self1 = p->self[1]; a.self2 = p->self[2];
