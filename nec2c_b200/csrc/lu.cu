@@ -402,6 +402,7 @@ __global__ void __launch_bounds__(CPT, 1) panel_cluster_kernel(PanelArgs p) {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     sh.fail = 0;
     sh.info = 0;
+    if (rank == 0) p.st->npairs = 0;   // the CTAs append their moved rows at the end
   }
   cluster.sync();
   const long long rows = p.n - p.k0;
@@ -439,7 +440,32 @@ __global__ void __launch_bounds__(CPT, 1) panel_cluster_kernel(PanelArgs p) {
   if (rank == 0 && warp == 0) {
     for (int j = lane; j < p.kb; j += 32) p.ipiv[p.k0 + j] = (int)(p.k0 + sh.piv[j] + 1);
     if (lane == 0 && sh.info && p.st->info == 0) p.st->info = (int)(p.k0 + sh.info);
-    panel_pairs_warp(p, sh.piv);
+  }
+  // Net interchange of the panel: a row now at position pos[k] holds the old
+  // row g, so destination k0 + pos[k] takes source k0 + g.  Warp 0 of each
+  // CTA appends its moved rows (at most 2 KB over the cluster).
+  if (warp == 0) {
+    unsigned moved[CRL];
+    int total = 0;
+#pragma unroll
+    for (int k = 0; k < CRL; ++k) {
+      const int g = rank * CROWS + lane + 32 * k;
+      moved[k] = __ballot_sync(0xffffffffu, pos[k] != INT_MAX && pos[k] != g);
+      total += __popc(moved[k]);
+    }
+    int base = 0;
+    if (lane == 0 && total) base = atomicAdd(&p.st->npairs, total);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < CRL; ++k) {
+      if (moved[k] >> lane & 1u) {
+        const int at = base + __popc(moved[k] & below);
+        p.pairs[at] = (int)(p.k0 + pos[k]);
+        p.pairs[2 * KB + at] = (int)(p.k0 + rank * CROWS + lane + 32 * k);
+      }
+      base += __popc(moved[k]);
+    }
   }
 }
 
