@@ -13,10 +13,11 @@
 // lo = x - hi exact in FP32; D = Ahi Bhi + Ahi Blo + Alo Bhi accumulates in
 // FP32 in tensor memory (3xTF32), close to an FP32 product.
 //
-// One CTA per 128-row x 128-complex-column tile, 256 threads: the threads
+// One CTA per 128-row x 32-complex-column tile (97 KB of shared memory, two
+// CTAs per SM beside other work), 256 threads: the threads
 // stage A (split on the fly) and Bt (pre-split) into 128B-swizzled shared
 // memory, one elected thread issues the 24 tcgen05.mma (8 K-steps x 3
-// products, M=128 N=256 K=8), tcgen05.commit signals an mbarrier, and the
+// products, M=128 N=64 K=8), tcgen05.commit signals an mbarrier, and the
 // eight warps read the accumulator back (tcgen05.ld: warp w its 32 lanes of
 // quarter w%4, half the columns per warpgroup) and update C.
 // No cluster, no multicast.
@@ -29,16 +30,16 @@
 namespace {
 
 constexpr int TM = 128;             // tile rows
-constexpr int TNC = 128;            // tile complex columns
+constexpr int TNC = 32;             // tile complex columns
 constexpr int TN = 2 * TNC;         // tile real columns (MMA N)
 constexpr int KR = 64;              // real K (2 x panel width 32)
 constexpr int ATOM_ROW = 128;       // bytes per swizzle-atom row (32 floats)
 constexpr int KATOMS = KR * 4 / ATOM_ROW;   // 2 atoms along K
 constexpr int A_BYTES = KATOMS * TM * ATOM_ROW;   // 32 KB
-constexpr int B_BYTES = KATOMS * TN * ATOM_ROW;   // 64 KB
+constexpr int B_BYTES = KATOMS * TN * ATOM_ROW;   // 16 KB
 constexpr int SMEM_BYTES = 2 * A_BYTES + 2 * B_BYTES + 1024;   // + alignment slack
 constexpr int THREADS = 256;      // two warpgroups: staging and epilogue split between them
-constexpr uint32_t TMEM_COLS = 256;
+constexpr uint32_t TMEM_COLS = TN;   // 64 accumulator columns
 
 __device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
 
@@ -78,7 +79,7 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(THREADS, 2)
 gemm_tf32x3_kernel(float2 *C, long long ldc, const float2 *A, long long lda, const float *bt_hi, const float *bt_lo,
                    long long M, long long N, int *error) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
