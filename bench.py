@@ -764,6 +764,8 @@ def serving_bench(nb, torch):
     plain, _ = run(False, None, slots=1)
     out["plain_fp64_one_at_a_time"] = plain
     out["mixed_serving_vs_plain_fp64"] = sat[True]["solves_per_s"] / plain["solves_per_s"]
+    out["fp32_volume_fp64_lu_serving_vs_plain_fp64"] = (out["saturation"]["fp32_volume_fp64_lu"]["solves_per_s"] /
+                                                         plain["solves_per_s"])
     rate = 0.7 * sat[True]["solves_per_s"]
     gaps = np.cumsum(np.random.default_rng(5).exponential(1.0 / rate, SERVE_REQUESTS))
     pois = {}

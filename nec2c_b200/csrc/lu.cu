@@ -692,7 +692,7 @@ __global__ void __launch_bounds__(256) gemm_update_kernel(double2 *C, const doub
 // matrix.c:1523-1555 solves).  One block per RHS; each 32-row step is solved
 // by warp 0 and the rows below / above are updated by the whole block with
 // contiguous row segments.
-// One right-hand side per CTA (1024 threads).  Interchanges: the sequential
+// One right-hand side per CTA (512 threads).  Interchanges: the sequential
 // swaps of ipiv are composed into an index permutation in shared memory by
 // one thread (orders up to SOLVE_PERM_MAX; beyond, the swaps run on x
 // directly), then x is gathered through it in registers.  Forward and back
@@ -700,11 +700,11 @@ __global__ void __launch_bounds__(256) gemm_update_kernel(double2 *C, const doub
 // column-oriented (x_k broadcast by shuffle, each later row subtracting its
 // L or U entry times x_k), then all warps update the remaining rows (warp per
 // row, a 32-wide dot product).
-constexpr int SOLVE_THREADS = 1024;
-constexpr int SOLVE_PERM_MAX = 8 * 1024;    // 8 bytes of shared memory per row, 8 values per thread
+constexpr int SOLVE_THREADS = 512;    // fits beside other work on a busy SM
+constexpr int SOLVE_PERM_MAX = 4 * 1024;    // 8 bytes of shared memory per row, 8 values per thread
 constexpr int SOLVE_REG = SOLVE_PERM_MAX / SOLVE_THREADS;
 template <typename S>
-__global__ void __launch_bounds__(SOLVE_THREADS) lu_solve_kernel(const S *a, long long n, long long ld,
+__global__ void __launch_bounds__(SOLVE_THREADS, 2) lu_solve_kernel(const S *a, long long n, long long ld,
                                                                  const int *ipiv, double2 *b, long long ldb) {
   extern __shared__ int perm_smem[];
   double2 *x = b + blockIdx.x * ldb;
