@@ -81,6 +81,34 @@ int nec2c_cuda_vie_fft_apply_device(nec2c_cuda_vie_plan *plan, const void *x_dev
    order xx yy zz xy xz yz, each scaled by 1/grid (validation hook). */
 int nec2c_cuda_vie_fft_spectrum(nec2c_cuda_vie_plan *plan, nec2c_cuda_complex *out);
 
+/* FFT pass schedule.  A product runs five line-FFT passes: 0 z forward with
+   the cell scatter, 1 y forward, 2 x forward + Green-tensor product + x
+   inverse, 3 y inverse, 4 z inverse with the permittivity epilogue.  Each has
+   a tile height (lines per CTA) and a radix split L = R1 x R2.  With
+   autotuning on (the default; NEC2C_CUDA_FFT_AUTOTUNE=0 in the environment
+   turns it off) nec2c_cuda_vie_fft_create times the candidates on the new
+   plan and keeps the fastest, cached per grid shape for the process.  The
+   reference plans its FFTW transforms with FFTW_ESTIMATE (vie_fft.c:227-235),
+   i.e. untimed; this is the measured counterpart.  Every schedule computes
+   the same transform; the radix split changes the rounding only. */
+void nec2c_cuda_vie_fft_autotune(int enable);
+int nec2c_cuda_vie_fft_autotune_enabled(void);
+/* Re-plans one plan's schedule: measure = 0 the heuristic, 1 timed (reusing
+   a cached choice for the same shape), 2 timed afresh.  Returns 1 on success. */
+int nec2c_cuda_vie_fft_tune(nec2c_cuda_vie_plan *plan, int measure);
+/* Schedule in use for the FP64 (fp64 != 0) or FP32 transforms: tiles[i]
+   lines per tile and r1[i] the first radix of pass i.  Returns 1 when that
+   precision was timed or pinned, 0 when it runs the heuristic, -1 on a bad
+   argument. */
+int nec2c_cuda_vie_fft_schedule(nec2c_cuda_vie_plan *plan, int fp64, int tiles[5], int r1[5]);
+/* Pins a schedule, e.g. one read back from an earlier run so that results
+   repeat bit for bit across processes.  Heights: whole lattice columns
+   (multiples of 3 lines, at most 96) for passes 0 and 4, powers of two up to
+   64 for passes 1-3, each within 100 KB of shared memory; r1 one of the
+   splits on offer for the pass's length.  Returns 0 (schedule unchanged) on
+   anything else. */
+int nec2c_cuda_vie_fft_set_schedule(nec2c_cuda_vie_plan *plan, int fp64, const int tiles[5], const int r1[5]);
+
 /* --------------------------------------- hybrid conductor + volume system */
 typedef struct nec2c_cuda_hybrid nec2c_cuda_hybrid;
 /* Device half of dielectric_fft_prepare / dielectric_fft_prepare_pec

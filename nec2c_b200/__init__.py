@@ -77,6 +77,11 @@ def load():
         "nec2c_cuda_vie_fft_precondition": (i, [vp, vp, vp]),
         "nec2c_cuda_vie_fft_apply_device": (i, [vp, vp, vp]),
         "nec2c_cuda_vie_fft_spectrum": (i, [vp, vp]),
+        "nec2c_cuda_vie_fft_autotune": (None, [i]),
+        "nec2c_cuda_vie_fft_autotune_enabled": (i, []),
+        "nec2c_cuda_vie_fft_tune": (i, [vp, i]),
+        "nec2c_cuda_vie_fft_schedule": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
+        "nec2c_cuda_vie_fft_set_schedule": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
         "nec2c_cuda_hybrid_create": (i, [C.POINTER(vp), vp, sz, sz, i]),
         "nec2c_cuda_hybrid_destroy": (None, [vp]),
         "nec2c_cuda_hybrid_set_blocks": (i, [vp, vp]),
@@ -110,6 +115,15 @@ def load():
         f.argtypes = args
     _lib = lib
     return lib
+
+
+def set_fft_autotune(enable):
+    """Turns the measured FFT schedule of new plans on or off (process-wide)."""
+    load().nec2c_cuda_vie_fft_autotune(int(bool(enable)))
+
+
+def fft_autotune_enabled():
+    return bool(load().nec2c_cuda_vie_fft_autotune_enabled())
 
 
 def last_error():
@@ -190,6 +204,26 @@ class VolumePlan:
         if not load().nec2c_cuda_vie_fft_spectrum(self.h, _ptr(out)):
             raise RuntimeError("spectrum failed: " + last_error())
         return out
+
+    def tune(self, measure=1):
+        """Re-plans the FFT pass schedule: 0 heuristic, 1 timed (shape cache),
+        2 timed afresh."""
+        if not load().nec2c_cuda_vie_fft_tune(self.h, measure):
+            raise RuntimeError("tune failed: " + last_error())
+
+    def schedule(self, fp64=False):
+        """(measured, [(lines per tile, R1), ...] for the five passes)."""
+        tiles, r1 = (C.c_int * 5)(), (C.c_int * 5)()
+        r = load().nec2c_cuda_vie_fft_schedule(self.h, int(bool(fp64)), tiles, r1)
+        if r < 0:
+            raise RuntimeError("schedule: no such precision on this plan")
+        return bool(r), list(zip(tiles, r1))
+
+    def set_schedule(self, passes, fp64=False):
+        """Pins [(lines per tile, R1)] x 5; returns False when refused."""
+        tiles = (C.c_int * 5)(*[int(t) for t, _ in passes])
+        r1 = (C.c_int * 5)(*[int(r) for _, r in passes])
+        return bool(load().nec2c_cuda_vie_fft_set_schedule(self.h, int(bool(fp64)), tiles, r1))
 
     def bytes(self):
         return load().nec2c_cuda_vie_fft_bytes(self.h)

@@ -86,6 +86,19 @@ const double *n2d_vie_diag(const n2d_vie *p);
 /* PEC image embedding: the plan's cells are physical_cells physical cells
    followed by their images; apply/precondition then act on the physical half. */
 void n2d_vie_set_mirror(n2d_vie *p, long long physical_cells);
+/* Pass schedule (tile height and radix split of the five matvec passes).
+   measure: 0 the heuristic, 1 timed on this plan (a cached choice for the
+   same grid shape and precision is reused), 2 timed afresh.  Plans are tuned
+   with measure = 1 at the end of n2d_vie_finish_spectrum while autotuning is
+   enabled (the default; NEC2C_CUDA_FFT_AUTOTUNE=0 disables it). */
+int n2d_vie_tune(n2d_vie *p, int measure);
+void n2d_vie_autotune(int enable);
+int n2d_vie_autotune_enabled(void);
+/* Lines per tile and R1 (R2 = L / R1) of each pass for precision prec
+   (0 FP32, 1 FP64); returns 1 when the schedule was measured. */
+int n2d_vie_schedule(n2d_vie *p, int prec, int *tiles, int *r1);
+/* Pins a schedule (heights and splits the tuner would try; 0 otherwise). */
+int n2d_vie_set_schedule(n2d_vie *p, int prec, const int *tiles, const int *r1);
 
 /* ---- hybrid [C B; D V] operator (dielectric_fft.c) ---- */
 typedef struct n2d_hybrid n2d_hybrid;

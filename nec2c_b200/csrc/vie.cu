@@ -17,92 +17,23 @@
 #include <vector>
 #include "common.cuh"
 #include "device_api.h"
+#include <atomic>
 #include <mutex>
-#include "fft_engine.cuh"
+#include <stdlib.h>
+#include "fft_passes.cuh"
 #include "runtime.cuh"
 #include "vie_internal.cuh"
 
 using namespace n2c;
 
-// ------------------------------------------------------------ pass dispatch
-// Strided axes (y, x): mode 0 forward, 1 inverse, 2 forward x + spectrum
-// product + inverse x.  Contiguous axis (z), staged through shared memory:
-// mode 5 forward, 6 inverse, 7 forward with the cell scatter, 8 inverse with
-// the permittivity epilogue.
-template <typename C, int R1, int R2>
-static int launch_pass_rr(int mode, const PassArgs<C> &a, size_t smem, long long tiles) {
-  static bool configured[9] = {false, false, false, false, false, false, false, false, false};
-  void (*k)(PassArgs<C>) = mode == 0 ? fft_forward_pass<C, R1, R2>
-                          : mode == 1 ? fft_inverse_pass<C, R1, R2>
-                          : mode == 2 ? fft_product_pass<C, R1, R2>
-                          : mode == 5 ? fft_zline_pass<C, R1, R2, false, false>
-                          : mode == 6 ? fft_zline_pass<C, R1, R2, true, false>
-                          : mode == 7 ? fft_zline_pass<C, R1, R2, false, true>
-                                      : fft_zline_pass<C, R1, R2, true, true>;
-  if (!configured[mode]) {
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
-        cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess) {
-      n2c_set_error("cannot raise shared memory for FFT pass");
-      return 0;
-    }
-    configured[mode] = true;
-  }
-  if (tiles > 0x7fffffffLL) { n2c_set_error("FFT pass grid too large"); return 0; }
-  k<<<(unsigned)tiles, 256, smem, n2c_stream()>>>(a);
-  return n2c_check_launch("fft pass");
-}
+// ------------------------------------------------------------ pass schedule
+// The passes themselves are launched through fft_passes.cuh.  Each of the
+// five matvec passes runs with a tile height and radix split taken from the
+// plan's schedule: the heuristic below, or the measured choice of the tuner
+// (n2d_vie_tune).
 
-template <typename C, int R1, int R2>
-static int occupancy_rr(int mode, size_t smem) {
-  void (*k)(PassArgs<C>) = mode == 5 ? fft_zline_pass<C, R1, R2, false, false>
-                          : mode == 6 ? fft_zline_pass<C, R1, R2, true, false>
-                          : mode == 7 ? fft_zline_pass<C, R1, R2, false, true>
-                                      : fft_zline_pass<C, R1, R2, true, true>;
-  int blocks = 0;
-  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
-      cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, 256, smem) != cudaSuccess) {
-    cudaGetLastError();
-    return 0;
-  }
-  return blocks;
-}
-
-// Resident blocks per SM of a staged z pass (modes 5-8) with smem bytes.
-template <typename C>
-static int zline_occupancy(int mode, int L, size_t smem) {
-  switch (L) {
-    case 16: return occupancy_rr<C, 16, 1>(mode, smem);
-    case 32: return occupancy_rr<C, 8, 4>(mode, smem);
-    case 64: return occupancy_rr<C, 8, 8>(mode, smem);
-    case 128: return occupancy_rr<C, 16, 8>(mode, smem);
-    case 256: return occupancy_rr<C, 16, 16>(mode, smem);
-    case 512: return occupancy_rr<C, 32, 16>(mode, smem);
-    case 1024: return occupancy_rr<C, 32, 32>(mode, smem);
-  }
-  return 0;
-}
-
-template <typename C>
-static int launch_pass(int mode, int L, const PassArgs<C> &a, size_t smem, long long tiles) {
-  switch (L) {
-    case 1: return launch_pass_rr<C, 1, 1>(mode, a, smem, tiles);
-    case 2: return launch_pass_rr<C, 2, 1>(mode, a, smem, tiles);
-    case 4: return launch_pass_rr<C, 4, 1>(mode, a, smem, tiles);
-    case 8: return launch_pass_rr<C, 8, 1>(mode, a, smem, tiles);
-    case 16: return launch_pass_rr<C, 16, 1>(mode, a, smem, tiles);
-    case 32: return launch_pass_rr<C, 8, 4>(mode, a, smem, tiles);
-    case 64: return launch_pass_rr<C, 8, 8>(mode, a, smem, tiles);
-    case 128: return launch_pass_rr<C, 16, 8>(mode, a, smem, tiles);
-    case 256: return launch_pass_rr<C, 16, 16>(mode, a, smem, tiles);
-    case 512: return launch_pass_rr<C, 32, 16>(mode, a, smem, tiles);
-    case 1024: return launch_pass_rr<C, 32, 32>(mode, a, smem, tiles);
-  }
-  n2c_set_error("unsupported FFT length %d", L);
-  return 0;
-}
-
-// Lines per tile: as many as fit a ~48 KB tile (four CTAs per SM), <= 32.
+// Lines per tile of a strided pass: as many as fit a ~48 KB tile (four CTAs
+// per SM), <= 32.
 static int lines_per_tile(int L, int ncomp, size_t elem) {
   size_t per_line = (size_t)L * ncomp * elem;
   int nl = 32;
@@ -110,16 +41,14 @@ static int lines_per_tile(int L, int ncomp, size_t elem) {
   return nl;
 }
 
-// One axis transform over a batch of lines.  Element e of line (b, i) lives at
-// (b*A + e)*I + i; lines = B*I.
-// Lines per tile of a staged z pass: two padded [L][NL+1] buffers within
-// ~56 KB (three to four blocks per SM); `unit` keeps NL a multiple of 3 for
-// cell tiles.
 // ceil(2^32 / d) for the device's multiply-high division (0 for d == 1).
 static unsigned div_magic(long long d) {
   return d <= 1 ? 0u : (unsigned)((0x100000000ULL + (unsigned long long)d - 1) / (unsigned long long)d);
 }
 
+// Lines per tile of a staged z pass: two padded [L][NL+1] buffers within
+// ~56 KB (three to four blocks per SM); `unit` keeps NL a multiple of 3 for
+// cell tiles.
 static int zlines_per_tile(int L, size_t elem, int unit) {
   int nl = 32 * unit;
   while (nl > unit && (size_t)2 * (nl + 1) * L * elem > 56 * 1024) nl -= unit;
@@ -151,7 +80,7 @@ static int zline_tile(int mode, int L, int unit, long long groups) {
   for (int nl = (def / 2 / unit > 0 ? def / 2 / unit : 1) * unit; (size_t)2 * (nl + 1) * L * sizeof(C) <= 80 * 1024;
        nl += unit) {
     const size_t smem = (size_t)2 * (nl + 1) * L * sizeof(C);
-    const int bps = zline_occupancy<C>(mode, L, smem);
+    const int bps = fft_zline_occupancy<C>(mode, L, 0, smem);
     if (bps <= 0) continue;
     const long long per = nl / unit, tiles = (groups + per - 1) / per, slots = (long long)sms * bps;
     const long long waves = (tiles + slots - 1) / slots;
@@ -167,9 +96,13 @@ static int zline_tile(int mode, int L, int unit, long long groups) {
   return best;
 }
 
+// One axis transform over a batch of lines.  Element e of line (b, i) lives at
+// (b*A + e)*I + i; lines = B*I.  Strided lines (I > 1) take the tile height
+// and radix split of `ch` (heuristic height when ch.nl == 0); contiguous lines
+// (the spectrum build) always take the heuristic.
 template <typename C>
 static int axis_pass(int mode, int L, const C *in, C *out, const C *tw, long long B, long long I,
-                     long long A_in, long long A_out, int n_in, int n_out) {
+                     long long A_in, long long A_out, int n_in, int n_out, n2d_pass_choice ch = {0, 0}) {
   PassArgs<C> a;
   memset(&a, 0, sizeof(a));
   a.in = in; a.out = out; a.tw = tw;
@@ -180,15 +113,15 @@ static int axis_pass(int mode, int L, const C *in, C *out, const C *tw, long lon
     a.nl_div = div_magic(a.NL);
     a.nout_div = div_magic(a.n_out);
     const long long tiles = (a.lines + a.NL - 1) / a.NL;
-    return launch_pass<C>(mode + 5, L, a, (size_t)2 * (a.NL + 1) * L * sizeof(C), tiles);
+    return fft_launch_pass<C>(mode + 5, L, 0, a, (size_t)2 * (a.NL + 1) * L * sizeof(C), tiles);
   }
-  a.NL = lines_per_tile(L, 1, sizeof(C));
+  a.NL = ch.nl ? ch.nl : lines_per_tile(L, 1, sizeof(C));
   const long long tiles = (a.lines + a.NL - 1) / a.NL;
-  return launch_pass<C>(mode, L, a, (size_t)L * a.NL * sizeof(C), tiles);
+  return fft_launch_pass<C>(mode, L, ch.radix, a, (size_t)L * a.NL * sizeof(C), tiles);
 }
 
 template <typename C>
-static int product_pass(const n2d_vie *p, const C *in, C *out, const C *tw, const C *spec) {
+static int product_pass(const n2d_vie *p, const C *in, C *out, const C *tw, const C *spec, n2d_pass_choice ch) {
   const int L = (int)p->P[0], nx = (int)p->S[0];
   const long long I = p->P[1] * p->P[2];
   PassArgs<C> a;
@@ -197,10 +130,10 @@ static int product_pass(const n2d_vie *p, const C *in, C *out, const C *tw, cons
   a.lines = I; a.I = I; a.A_in = nx; a.A_out = nx; a.n_in = nx; a.n_out = nx;
   a.comp_in = (long long)nx * I; a.comp_out = (long long)nx * I; a.spec_comp = p->GH;
   a.Py = (int)p->P[1]; a.Pz = (int)p->P[2]; a.Hy = (int)p->H[1]; a.Hz = (int)p->H[2];
-  a.NL = lines_per_tile(L, 3, sizeof(C));
+  a.NL = ch.nl ? ch.nl : lines_per_tile(L, 3, sizeof(C));
   a.gate = n2c_gate();
   const long long tiles = (a.lines + a.NL - 1) / a.NL;
-  return launch_pass<C>(2, L, a, (size_t)3 * L * a.NL * sizeof(C), tiles);
+  return fft_launch_pass<C>(2, L, ch.radix, a, (size_t)3 * L * a.NL * sizeof(C), tiles);
 }
 
 // --------------------------------------------------------- scatter / gather
@@ -668,6 +601,7 @@ extern "C" int n2d_vie_finish_spectrum(n2d_vie *p) {
                      (p->Ss[0] + 1 + p->Ss[1] + 1) * sizeof(long long);
   p->table = nullptr; p->table_ok = nullptr; p->offsets = nullptr;
   p->slab_start = nullptr; p->row_start = nullptr;
+  if (ok && n2d_vie_autotune_enabled()) ok = n2d_vie_tune(p, 1);
   return ok;
 }
 
@@ -694,7 +628,7 @@ extern "C" int n2d_vie_set_eps(n2d_vie *p, const double *eps, const double *self
 // y = eps z - (eps-1) field and reduces |y|^2.
 template <typename C>
 static int z_cell_pass(int mode, n2d_vie *p, const C *in, C *out, const C *tw, const double2 *x,
-                       double2 *y, int precondition, double *norm, int *flag) {
+                       double2 *y, int precondition, double *norm, int *flag, n2d_pass_choice ch) {
   const long long nx = p->S[0], ny = p->S[1], nz = p->S[2], Pz = p->P[2];
   PassArgs<C> a;
   memset(&a, 0, sizeof(a));
@@ -702,7 +636,7 @@ static int z_cell_pass(int mode, n2d_vie *p, const C *in, C *out, const C *tw, c
   a.lines = 3 * nx * ny; a.I = 1;
   if (mode == 3) { a.A_in = nz; a.A_out = Pz; a.n_in = (int)nz; a.n_out = (int)Pz; }
   else { a.A_in = Pz; a.A_out = nz; a.n_in = (int)Pz; a.n_out = (int)nz; }
-  a.NL = zline_tile<C>(mode == 3 ? 7 : 8, (int)Pz, 3, nx * ny);
+  a.NL = ch.nl ? ch.nl : zline_tile<C>(mode == 3 ? 7 : 8, (int)Pz, 3, nx * ny);
   a.nl_div = div_magic(a.NL);
   a.np_div = div_magic(a.NL / 3);
   a.nout_div = div_magic(a.n_out);
@@ -716,12 +650,17 @@ static int z_cell_pass(int mode, n2d_vie *p, const C *in, C *out, const C *tw, c
   if (norm && tiles > 65536) { n2c_set_error("norm reduction grid too large"); return 0; }
   // Cell tiles take T1 rows of 3 components: T1 is [3][nx*ny][Pz], so the
   // component planes are addressed through lines = comp * nxy + pos.
-  return launch_pass<C>(mode == 3 ? 7 : 8, (int)Pz, a, (size_t)2 * (a.NL + 1) * Pz * sizeof(C), tiles);
+  return fft_launch_pass<C>(mode == 3 ? 7 : 8, (int)Pz, ch.radix, a, (size_t)2 * (a.NL + 1) * Pz * sizeof(C),
+                            tiles);
 }
 
+template <typename C> static constexpr int prec_of() { return sizeof(C) == sizeof(float2) ? 0 : 1; }
+
+// Pass `pass` of the matvec y = A x (numbering of n2d_pass_choice) with the
+// tile height and radix split of ch.
 template <typename C>
-static int apply_t(n2d_vie *p, const double2 *x, double2 *y, int precondition, double *norm,
-                   int *flag) {
+static int run_pass(n2d_vie *p, int pass, n2d_pass_choice ch, const double2 *x, double2 *y, int precondition,
+                    double *norm, int *flag) {
   const long long nx = p->S[0], ny = p->S[1];
   const long long Py = p->P[1], Pz = p->P[2];
   constexpr bool single = sizeof(C) == sizeof(float2);
@@ -729,11 +668,24 @@ static int apply_t(n2d_vie *p, const double2 *x, double2 *y, int precondition, d
   const C *tw[3];
   for (int d = 0; d < 3; ++d) tw[d] = single ? (const C *)p->tw32[d] : (const C *)p->tw64[d];
   const C *spec = single ? (const C *)p->spec : (const C *)p->spec64;
-  return z_cell_pass<C>(3, p, nullptr, t1, tw[2], x, y, precondition, nullptr, flag) &&
-         axis_pass<C>(0, (int)Py, t1, t2, tw[1], 3 * nx, Pz, ny, Py, (int)ny, (int)Py) &&
-         product_pass<C>(p, t2, t2, tw[0], spec) &&
-         axis_pass<C>(1, (int)Py, t2, t1, tw[1], 3 * nx, Pz, Py, ny, (int)Py, (int)ny) &&
-         z_cell_pass<C>(4, p, t1, nullptr, tw[2], x, y, precondition, norm, flag);
+  switch (pass) {
+    case 0: return z_cell_pass<C>(3, p, nullptr, t1, tw[2], x, y, precondition, nullptr, flag, ch);
+    case 1: return axis_pass<C>(0, (int)Py, t1, t2, tw[1], 3 * nx, Pz, ny, Py, (int)ny, (int)Py, ch);
+    case 2: return product_pass<C>(p, t2, t2, tw[0], spec, ch);
+    case 3: return axis_pass<C>(1, (int)Py, t2, t1, tw[1], 3 * nx, Pz, Py, ny, (int)Py, (int)ny, ch);
+    case 4: return z_cell_pass<C>(4, p, t1, nullptr, tw[2], x, y, precondition, norm, flag, ch);
+  }
+  n2c_set_error("no FFT pass %d", pass);
+  return 0;
+}
+
+template <typename C>
+static int apply_t(n2d_vie *p, const double2 *x, double2 *y, int precondition, double *norm,
+                   int *flag) {
+  const n2d_pass_choice *s = p->sched[prec_of<C>()];
+  for (int i = 0; i < N2D_VIE_PASSES; ++i)
+    if (!run_pass<C>(p, i, s[i], x, y, precondition, norm, flag)) return 0;
+  return 1;
 }
 
 extern "C" int n2d_vie_apply(n2d_vie *p, const double *x, double *y, int precondition_input,
@@ -741,6 +693,239 @@ extern "C" int n2d_vie_apply(n2d_vie *p, const double *x, double *y, int precond
   if (p->fp32 && !full_precision)
     return apply_t<float2>(p, (const double2 *)x, (double2 *)y, precondition_input, norm, flag);
   return apply_t<double2>(p, (const double2 *)x, (double2 *)y, precondition_input, norm, flag);
+}
+
+// ------------------------------------------------------------------- tuner
+// The tile height and radix split of each matvec pass are chosen by timing
+// candidates on the plan's own grids (CUDA events on the plan's stream; per
+// candidate one warm-up launch, then the best of two runs of three launches):
+// first the radix split at the heuristic height, then the height at the split
+// kept.  A candidate replaces the incumbent only when it is at least 3%
+// faster, so timing noise does not move a pass off the heuristic for nothing.
+// Choices are cached per (lattice, padded grid, precision) for the process,
+// so the plans of a frequency sweep or of many same-sized models are timed
+// once.  Every candidate computes the same transform; the split only changes
+// the order of the butterflies, hence the rounding.
+namespace {
+
+struct TuneEntry {
+  long long S[3], P[3];
+  int prec;
+  n2d_pass_choice c[N2D_VIE_PASSES];
+};
+std::mutex g_tune_lock;
+std::vector<TuneEntry> g_tune_cache;
+std::atomic<int> g_autotune{-1};   // -1: NEC2C_CUDA_FFT_AUTOTUNE not read yet
+
+bool tune_key_is(const TuneEntry &e, const n2d_vie *p, int prec) {
+  for (int d = 0; d < 3; ++d)
+    if (e.S[d] != p->S[d] || e.P[d] != p->P[d]) return false;
+  return e.prec == prec;
+}
+
+int autotune_enabled() {
+  int v = g_autotune.load();
+  if (v < 0) {
+    const char *env = getenv("NEC2C_CUDA_FFT_AUTOTUNE");
+    v = (env && env[0] == '0') ? 0 : 1;
+    int expected = -1;
+    g_autotune.compare_exchange_strong(expected, v);
+    v = g_autotune.load();
+  }
+  return v;
+}
+
+int pass_length(const n2d_vie *p, int pass) {
+  return (int)(pass == 0 || pass == 4 ? p->P[2] : pass == 2 ? p->P[0] : p->P[1]);
+}
+
+// The height the heuristic gives pass `pass`.
+template <typename C>
+int heuristic_height(const n2d_vie *p, int pass) {
+  switch (pass) {
+    case 0: return zline_tile<C>(7, (int)p->P[2], 3, p->S[0] * p->S[1]);
+    case 4: return zline_tile<C>(8, (int)p->P[2], 3, p->S[0] * p->S[1]);
+    case 2: return lines_per_tile((int)p->P[0], 3, sizeof(C));
+  }
+  return lines_per_tile((int)p->P[1], 1, sizeof(C));
+}
+
+// Heights tried: whole lattice columns (multiples of 3 lines) for the z
+// passes, powers of two for the strided passes, each within 100 KB of shared
+// memory (two CTAs per SM at least); the z epilogue also keeps its norm
+// reduction within the 65,536 partials of the plan.
+template <typename C>
+std::vector<int> candidate_heights(const n2d_vie *p, int pass) {
+  std::vector<int> out;
+  const size_t e = sizeof(C), L = (size_t)pass_length(p, pass);
+  if (pass == 0 || pass == 4) {
+    const long long cols = p->S[0] * p->S[1];
+    for (int nl = 3; nl <= 96 && (size_t)2 * (nl + 1) * L * e <= 100 * 1024; nl += 3)
+      if (pass == 0 || (cols + nl / 3 - 1) / (nl / 3) <= 65536) out.push_back(nl);
+  } else {
+    const size_t ncomp = pass == 2 ? 3 : 1;
+    for (int nl = 1; nl <= 64; nl *= 2)
+      if (L * ncomp * nl * e <= 100 * 1024) out.push_back(nl);
+  }
+  return out;
+}
+
+// Milliseconds of three launches of one candidate (best of two runs), or a
+// negative value when the candidate cannot run.
+template <typename C>
+float time_candidate(n2d_vie *p, int pass, n2d_pass_choice ch, const double2 *x, double2 *y, double *norm,
+                     cudaEvent_t e0, cudaEvent_t e1) {
+  if (!run_pass<C>(p, pass, ch, x, y, 0, norm, nullptr)) return -1.0f;
+  float best = -1.0f;
+  for (int trial = 0; trial < 2; ++trial) {
+    if (cudaEventRecord(e0, n2c_stream()) != cudaSuccess) return -1.0f;
+    for (int r = 0; r < 3; ++r)
+      if (!run_pass<C>(p, pass, ch, x, y, 0, norm, nullptr)) return -1.0f;
+    float ms = 0;
+    if (cudaEventRecord(e1, n2c_stream()) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+      return -1.0f;
+    if (best < 0 || ms < best) best = ms;
+  }
+  return best;
+}
+
+template <typename C>
+int tune_precision(n2d_vie *p, const double2 *x, double2 *y, double *norm, bool use_cache) {
+  const int prec = prec_of<C>();
+  if (use_cache) {
+    std::lock_guard<std::mutex> hold(g_tune_lock);
+    for (const TuneEntry &e : g_tune_cache)
+      if (tune_key_is(e, p, prec)) {
+        memcpy(p->sched[prec], e.c, sizeof(e.c));
+        p->tuned[prec] = 1;
+        return 1;
+      }
+  }
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) { n2c_set_error("tuner: event creation failed"); return 0; }
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    n2c_set_error("tuner: event creation failed");
+    return 0;
+  }
+  n2d_pass_choice chosen[N2D_VIE_PASSES];
+  for (int pass = 0; pass < N2D_VIE_PASSES; ++pass) {
+    // A heuristic that cannot run here (a z epilogue whose norm reduction
+    // would need more than 65,536 partials) stays the fallback; any
+    // candidate that runs replaces it.
+    n2d_pass_choice best = {heuristic_height<C>(p, pass), 0};
+    float bt = time_candidate<C>(p, pass, best, x, y, norm, e0, e1);
+    if (bt < 0) {
+      best = n2d_pass_choice{0, 0};
+      bt = 3.0e38f;
+    }
+    const int L = pass_length(p, pass);
+    for (int v = 1; v < fft_radix_variants(L); ++v) {
+      const n2d_pass_choice c = {best.nl, v};
+      const float t = time_candidate<C>(p, pass, c, x, y, norm, e0, e1);
+      if (t >= 0 && t < 0.97f * bt) { best = c; bt = t; }
+    }
+    for (int nl : candidate_heights<C>(p, pass)) {
+      if (nl == best.nl) continue;
+      const n2d_pass_choice c = {nl, best.radix};
+      const float t = time_candidate<C>(p, pass, c, x, y, norm, e0, e1);
+      if (t >= 0 && t < 0.97f * bt) { best = c; bt = t; }
+    }
+    chosen[pass] = best;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // A candidate that could not run may have left a launch error behind.
+  cudaGetLastError();
+  memcpy(p->sched[prec], chosen, sizeof(chosen));
+  p->tuned[prec] = 1;
+  std::lock_guard<std::mutex> hold(g_tune_lock);
+  TuneEntry e;
+  for (int d = 0; d < 3; ++d) { e.S[d] = p->S[d]; e.P[d] = p->P[d]; }
+  e.prec = prec;
+  memcpy(e.c, chosen, sizeof(chosen));
+  for (TuneEntry &old : g_tune_cache)
+    if (tune_key_is(old, p, prec)) { old = e; return 1; }
+  if (g_tune_cache.size() < 4096) g_tune_cache.push_back(e);
+  return 1;
+}
+
+}  // namespace
+
+extern "C" void n2d_vie_autotune(int enable) { g_autotune.store(enable ? 1 : 0); }
+extern "C" int n2d_vie_autotune_enabled(void) { return autotune_enabled(); }
+
+// measure: 0 the heuristic schedule, 1 measured (a cached choice for the same
+// shape is reused), 2 measured afresh (the cache entry is replaced).
+extern "C" int n2d_vie_tune(n2d_vie *p, int measure) {
+  // A captured GMRES cycle bakes the tile heights into its launches.
+  n2c_gmres_work_free(p->gm_work);
+  p->gm_work = nullptr;
+  memset(p->sched, 0, sizeof(p->sched));
+  p->tuned[0] = p->tuned[1] = 0;
+  if (measure == 0 || p->cells == 0) return 1;
+  const size_t vec = 3 * (size_t)p->cells * sizeof(double2);
+  double2 *x = (double2 *)n2d_alloc(vec), *y = (double2 *)n2d_alloc(vec);
+  double *norm = (double *)n2d_alloc(sizeof(double));
+  int ok = x && y && norm && n2d_memset(x, 0, vec);
+  ok = ok && (!p->fp32 || tune_precision<float2>(p, x, y, norm, measure == 1));
+  ok = ok && tune_precision<double2>(p, x, y, norm, measure == 1);
+  ok = ok && n2d_sync();
+  n2d_free(x);
+  n2d_free(y);
+  n2d_free(norm);
+  if (!ok) {
+    memset(p->sched, 0, sizeof(p->sched));
+    p->tuned[0] = p->tuned[1] = 0;
+  }
+  return ok;
+}
+
+// Pins the schedule of precision prec (0 FP32, 1 FP64): pass i runs tiles[i]
+// lines per tile with the split whose first radix is r1[i].  Each height and
+// split must be one the tuner would try; otherwise nothing changes and 0 is
+// returned with the error set.
+extern "C" int n2d_vie_set_schedule(n2d_vie *p, int prec, const int *tiles, const int *r1) {
+  prec = prec ? 1 : 0;
+  n2d_pass_choice c[N2D_VIE_PASSES];
+  for (int i = 0; i < N2D_VIE_PASSES; ++i) {
+    const int L = pass_length(p, i);
+    int v = -1;
+    for (int k = 0; k < fft_radix_variants(L); ++k)
+      if (fft_radix_r1(L, k) == r1[i]) v = k;
+    if (v < 0) {
+      n2c_set_error("FFT pass %d: R1 = %d is not a radix split of %d on offer", i, r1[i], L);
+      return 0;
+    }
+    const std::vector<int> ok = prec ? candidate_heights<double2>(p, i) : candidate_heights<float2>(p, i);
+    bool found = false;
+    for (int nl : ok) found = found || nl == tiles[i];
+    if (!found) {
+      n2c_set_error("FFT pass %d: %d lines per tile is not a height on offer", i, tiles[i]);
+      return 0;
+    }
+    c[i] = n2d_pass_choice{tiles[i], v};
+  }
+  n2c_gmres_work_free(p->gm_work);
+  p->gm_work = nullptr;
+  memcpy(p->sched[prec], c, sizeof(c));
+  p->tuned[prec] = 1;
+  return 1;
+}
+
+// Schedule of precision prec (0 FP32, 1 FP64): lines per tile and R1 of the
+// radix split of each pass.  Returns 1 when timed or pinned, 0 when
+// heuristic.
+extern "C" int n2d_vie_schedule(n2d_vie *p, int prec, int *tiles, int *r1) {
+  prec = prec ? 1 : 0;
+  for (int i = 0; i < N2D_VIE_PASSES; ++i) {
+    const n2d_pass_choice c = p->sched[prec][i];
+    const int nl = c.nl ? c.nl : (prec ? heuristic_height<double2>(p, i) : heuristic_height<float2>(p, i));
+    if (tiles) tiles[i] = nl;
+    if (r1) r1[i] = fft_radix_r1(pass_length(p, i), c.radix);
+  }
+  return p->tuned[prec];
 }
 
 extern "C" void n2d_vie_set_mirror(n2d_vie *p, long long physical_cells) {

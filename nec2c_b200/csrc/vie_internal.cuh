@@ -3,6 +3,17 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
+// Tile height (lines per CTA) and radix variant (fft_passes.cuh) of one FFT
+// pass; nl == 0 means the heuristic choice.
+struct n2d_pass_choice {
+  int nl, radix;
+};
+
+// The five passes of one matvec: 0 z forward with the cell scatter, 1 y
+// forward, 2 x forward + spectrum product + x inverse, 3 y inverse, 4 z
+// inverse with the permittivity epilogue.
+enum { N2D_VIE_PASSES = 5 };
+
 struct n2d_vie {
   int fp32;                 // 1: FP32 grids/spectrum (FP64 vectors and epilogue)
   long long S[3], P[3];     // lattice shape, padded FFT grid
@@ -28,4 +39,8 @@ struct n2d_vie {
   unsigned int *ticket;
   size_t device_bytes;
   void *gm_work;            // persistent GMRES workspace (gmres.cu)
+  // Pass schedule per transform precision (0 FP32, 1 FP64); tuned[i] != 0
+  // once the tuner has measured precision i for this plan.
+  n2d_pass_choice sched[2][N2D_VIE_PASSES];
+  int tuned[2];
 };

@@ -283,6 +283,32 @@ int nec2c_cuda_vie_fft_spectrum(nec2c_cuda_vie_plan *p, nec2c_cuda_complex *out)
   return p && out && n2d_vie_read_spectrum(p->dev, (double *)out);
 }
 
+void nec2c_cuda_vie_fft_autotune(int enable) { n2d_vie_autotune(enable); }
+int nec2c_cuda_vie_fft_autotune_enabled(void) { return n2d_vie_autotune_enabled(); }
+
+int nec2c_cuda_vie_fft_tune(nec2c_cuda_vie_plan *p, int measure)
+{
+  if(!p || measure < 0 || measure > 2) { n2c_set_error("tune: bad argument"); return 0; }
+  if(!nec2c_cuda_plan_device(p)) return 0;
+  return n2d_vie_tune(p->dev, measure);
+}
+
+int nec2c_cuda_vie_fft_schedule(nec2c_cuda_vie_plan *p, int fp64, int tiles[5], int r1[5])
+{
+  if(!p || !tiles || !r1) return -1;
+  if(!fp64 && !n2d_vie_fp32(p->dev)) return -1;
+  if(!nec2c_cuda_plan_device(p)) return -1;
+  return n2d_vie_schedule(p->dev, fp64 ? 1 : 0, tiles, r1);
+}
+
+int nec2c_cuda_vie_fft_set_schedule(nec2c_cuda_vie_plan *p, int fp64, const int tiles[5], const int r1[5])
+{
+  if(!p || !tiles || !r1) { n2c_set_error("set_schedule: bad argument"); return 0; }
+  if(!fp64 && !n2d_vie_fp32(p->dev)) { n2c_set_error("set_schedule: the plan has no FP32 transforms"); return 0; }
+  if(!nec2c_cuda_plan_device(p)) return 0;
+  return n2d_vie_set_schedule(p->dev, fp64 ? 1 : 0, tiles, r1);
+}
+
 /* ------------------------------------------------------------------ hybrid */
 struct nec2c_cuda_hybrid {
   n2d_hybrid *dev;
