@@ -164,6 +164,41 @@ int nec2c_cuda_gmres_hybrid_device(nec2c_cuda_hybrid *system, const void *b_dev,
                                    const nec2c_cuda_gmres_options *options,
                                    nec2c_cuda_gmres_report *report);
 
+/* ------------------------------------------------- ragged batch of plans */
+typedef struct nec2c_cuda_vie_batch nec2c_cuda_vie_batch;
+/* Many volume plans (frequencies or geometries with ragged lattices, padded
+   axes up to 128, all with the same transform precision, each at most once)
+   solved together: every FFT pass of a GMRES step is one launch over all the
+   plans, every Gram-Schmidt sweep one launch over all the systems, and the
+   steps of a restart cycle one CUDA graph.  The reference solves such a sweep
+   one vie_gmres at a time in its frequency workers (main.c:586-760); there is
+   no counterpart function.  The plans stay the caller's, must outlive the
+   batch and must not be used elsewhere while a batched call runs;
+   permittivity changes made to them are picked up by the next call. */
+int nec2c_cuda_vie_batch_create(nec2c_cuda_vie_batch **out, nec2c_cuda_vie_plan *const *plans, size_t count);
+void nec2c_cuda_vie_batch_destroy(nec2c_cuda_vie_batch *batch);
+/* Unknowns of the batch (sum of 3 x cells); plan q's entries start at
+   nec2c_cuda_vie_batch_offset(batch, q). */
+size_t nec2c_cuda_vie_batch_order(const nec2c_cuda_vie_batch *batch);
+size_t nec2c_cuda_vie_batch_offset(const nec2c_cuda_vie_batch *batch, size_t plan);
+/* y = A x of every plan (vie_fft.c:239-263 per plan) on device vectors of the
+   batch's order. */
+int nec2c_cuda_vie_batch_apply_device(nec2c_cuda_vie_batch *batch, const void *x_dev, void *y_dev);
+/* vie_gmres (vie_iterative.h:55-57) on every plan at once with the same
+   options (restart at most 30): right-preconditioned restarted GMRES, complex
+   Givens, true residual at every restart, each system stopping on its own
+   test; reports[q] as vie_gmres reports plan q's solve.  The Arnoldi process
+   is classical Gram-Schmidt, with a second pass always (FP64 plans) or on a
+   tenfold cancellation (FP32 transforms).  b_dev, x_dev: device vectors of
+   the batch's order; x is the initial guess and is updated.  Returns 1 when
+   every system converged. */
+int nec2c_cuda_gmres_batch_device(nec2c_cuda_vie_batch *batch, const void *b_dev, void *x_dev,
+                                  const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *reports);
+/* The same with host vectors: b[q] and x[q] hold 3 x cells of plan q. */
+int nec2c_cuda_gmres_batch(nec2c_cuda_vie_batch *batch, const nec2c_cuda_complex *const *b,
+                           nec2c_cuda_complex *const *x, const nec2c_cuda_gmres_options *options,
+                           nec2c_cuda_gmres_report *reports);
+
 /* ------------------------------------------------------------ dense LU */
 /* Replaces dense_backend_set (dense_backend.h:14) for "cuda" (FP64 LU) and
    "cuda-mixed" (split-precision tensor-core update plus FP64 refinement in the

@@ -82,6 +82,13 @@ def load():
         "nec2c_cuda_vie_fft_tune": (i, [vp, i]),
         "nec2c_cuda_vie_fft_schedule": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
         "nec2c_cuda_vie_fft_set_schedule": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
+        "nec2c_cuda_vie_batch_create": (i, [C.POINTER(vp), C.POINTER(vp), sz]),
+        "nec2c_cuda_vie_batch_destroy": (None, [vp]),
+        "nec2c_cuda_vie_batch_order": (sz, [vp]),
+        "nec2c_cuda_vie_batch_offset": (sz, [vp, sz]),
+        "nec2c_cuda_vie_batch_apply_device": (i, [vp, vp, vp]),
+        "nec2c_cuda_gmres_batch_device": (i, [vp, vp, vp, vp, vp]),
+        "nec2c_cuda_gmres_batch": (i, [vp, C.POINTER(vp), C.POINTER(vp), vp, vp]),
         "nec2c_cuda_hybrid_create": (i, [C.POINTER(vp), vp, sz, sz, i]),
         "nec2c_cuda_hybrid_destroy": (None, [vp]),
         "nec2c_cuda_hybrid_set_blocks": (i, [vp, vp]),
@@ -242,6 +249,43 @@ def _gmres(fn, handle, b, x0, restart, maxit, rtol, atol):
     rep = GmresReport()
     ok = fn(handle, _ptr(b), _ptr(x), C.byref(opts), C.byref(rep))
     return bool(ok), x, rep.as_dict()
+
+
+class VolumeBatch:
+    """Ragged batch of VolumePlans solved together (nec2c_cuda_vie_batch_*)."""
+
+    def __init__(self, plans):
+        self.plans = list(plans)      # the plans must outlive the batch
+        lib = load()
+        arr = (C.c_void_p * len(self.plans))(*[p.h.value for p in self.plans])
+        self.h = C.c_void_p()
+        if not lib.nec2c_cuda_vie_batch_create(C.byref(self.h), arr, len(self.plans)):
+            self.h = None
+            raise RuntimeError("nec2c_cuda_vie_batch_create failed: " + last_error())
+        self.order = lib.nec2c_cuda_vie_batch_order(self.h)
+        self.offsets = [lib.nec2c_cuda_vie_batch_offset(self.h, q) for q in range(len(self.plans) + 1)]
+
+    def close(self):
+        if self.h:
+            load().nec2c_cuda_vie_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def split(self, v):
+        return [v[self.offsets[q]:self.offsets[q + 1]] for q in range(len(self.plans))]
+
+    def gmres(self, bs, x0s=None, restart=30, maxit=300, rtol=1e-12, atol=0.0):
+        """(ok, [x_q], [report dict]) of vie_gmres on every plan at once."""
+        K = len(self.plans)
+        bs = [_cvec(b) for b in bs]
+        xs = [np.zeros_like(b) for b in bs] if x0s is None else [_cvec(x).copy() for x in x0s]
+        bp = (C.c_void_p * K)(*[b.ctypes.data for b in bs])
+        xp = (C.c_void_p * K)(*[x.ctypes.data for x in xs])
+        opts = GmresOptions(restart, maxit, rtol, atol)
+        reps = (GmresReport * K)()
+        ok = load().nec2c_cuda_gmres_batch(self.h, bp, xp, C.byref(opts), reps)
+        return bool(ok), xs, [r.as_dict() for r in reps]
 
 
 class HybridSystem:

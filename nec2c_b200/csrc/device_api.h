@@ -129,6 +129,23 @@ int n2d_gmres_dev(int kind, void *op, long long n, const double *b_dev, double *
                   size_t restart, size_t maximum_iterations, double rtol, double atol,
                   n2d_gmres_report *report);
 
+/* ---- ragged batch of volume plans (vie_batch.cu) ---- */
+typedef struct n2d_vie_batch n2d_vie_batch;
+/* Plans with the same transform precision, padded axes <= 128, each at most
+   once; their permittivities must have been uploaded (self terms set). */
+int n2d_vie_batch_create(n2d_vie_batch **out, n2d_vie *const *plans, long long count);
+void n2d_vie_batch_destroy(n2d_vie_batch *b);
+/* Unknowns of the batch and the offset of plan q's vector in it. */
+long long n2d_vie_batch_order(const n2d_vie_batch *b);
+long long n2d_vie_batch_offset(const n2d_vie_batch *b, long long q);
+/* y = A x of every plan (transform precision, no preconditioning), five
+   launches in all. */
+int n2d_vie_batch_apply(n2d_vie_batch *b, const double *x_dev, double *y_dev);
+/* GMRES(restart <= 30) on every plan in lockstep; reports[q] per system.
+   Returns 1 when every system converged. */
+int n2d_gmres_batch_dev(n2d_vie_batch *b, const double *b_dev, double *x_dev, size_t restart,
+                        size_t maximum_iterations, double rtol, double atol, n2d_gmres_report *reports);
+
 /* ---- dense LU (matrix.c factr/solve, dense_backend.c) ---- */
 /* Factor order x order in place on the device: the algebraic matrix
    row-major with leading dim ld (NEC's transposed column-major storage),

@@ -173,12 +173,12 @@ __device__ __forceinline__ void line_base(const PassArgs<C> &a, long long l, lon
 // Forward transform of one component per tile (CELLS: loads scatter the cell
 // vector, see cell_load).
 template <typename C, int R1, int R2, bool CELLS = false>
-__global__ void __launch_bounds__(256) fft_forward_pass(PassArgs<C> a) {
+__device__ __forceinline__ void fft_forward_tile(const PassArgs<C> &a, long long tile) {
   if (a.gate && *(volatile const int *)a.gate == 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *S = reinterpret_cast<C *>(smem_raw);
   const int NL = a.NL;
-  const long long l0 = (long long)blockIdx.x * NL;
+  const long long l0 = tile * NL;
   for (int item = threadIdx.x; item < NL * R2; item += blockDim.x) {
     const int t = item & (NL - 1), j2 = item / NL;
     const long long l = l0 + t;
@@ -217,16 +217,20 @@ __global__ void __launch_bounds__(256) fft_forward_pass(PassArgs<C> a) {
     }
   }
 }
+template <typename C, int R1, int R2, bool CELLS = false>
+__global__ void __launch_bounds__(256) fft_forward_pass(PassArgs<C> a) {
+  fft_forward_tile<C, R1, R2, CELLS>(a, blockIdx.x);
+}
 
 // Inverse transform (unnormalised) of one component per tile (CELLS: stores
 // run the permittivity epilogue into the cell vector and reduce |y|^2).
 template <typename C, int R1, int R2, bool CELLS = false>
-__global__ void __launch_bounds__(256) fft_inverse_pass(PassArgs<C> a) {
+__device__ __forceinline__ void fft_inverse_tile(const PassArgs<C> &a, long long tile, unsigned ntiles) {
   if (a.gate && *(volatile const int *)a.gate == 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *S = reinterpret_cast<C *>(smem_raw);
   const int NL = a.NL;
-  const long long l0 = (long long)blockIdx.x * NL;
+  const long long l0 = tile * NL;
   double sq = 0;
   for (int item = threadIdx.x; item < NL * R1; item += blockDim.x) {
     const int t = item & (NL - 1), k1 = item / NL;
@@ -270,19 +274,23 @@ __global__ void __launch_bounds__(256) fft_inverse_pass(PassArgs<C> a) {
   if (CELLS && a.norm) {
     // Deterministic |y|^2: block partials summed by the last block.
     const double2 bs = block_sum(make_double2(sq, 0));
-    if (threadIdx.x == 0) a.partials[blockIdx.x] = bs.x;
+    if (threadIdx.x == 0) a.partials[tile] = bs.x;
     __shared__ bool last;
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) last = atomicAdd(a.ticket, 1u) == ntiles - 1;
     __syncthreads();
     if (last) {
       double t2 = 0;
-      for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) t2 += a.partials[i];
+      for (unsigned i = threadIdx.x; i < ntiles; i += blockDim.x) t2 += a.partials[i];
       const double2 tot = block_sum(make_double2(t2, 0));
       if (threadIdx.x == 0) { *a.norm = tot.x; *a.ticket = 0; }
     }
   }
+}
+template <typename C, int R1, int R2, bool CELLS = false>
+__global__ void __launch_bounds__(256) fft_inverse_pass(PassArgs<C> a) {
+  fft_inverse_tile<C, R1, R2, CELLS>(a, blockIdx.x, gridDim.x);
 }
 
 // x-axis pass fused with the Green-tensor product: forward x-FFT of the three
@@ -290,12 +298,12 @@ __global__ void __launch_bounds__(256) fft_inverse_pass(PassArgs<C> a) {
 // the inverse x-FFT, all on one tile of lines.  Lines are the (ky,kz) points
 // (I = Py*Pz, one line per inner index, B = 1 per component).
 template <typename C, int R1, int R2>
-__global__ void __launch_bounds__(256, 3) fft_product_pass(PassArgs<C> a) {
+__device__ __forceinline__ void fft_product_tile(const PassArgs<C> &a, long long tile) {
   if (a.gate && *(volatile const int *)a.gate == 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *S = reinterpret_cast<C *>(smem_raw);
   const int NL = a.NL, L = R1 * R2;
-  const long long l0 = (long long)blockIdx.x * NL;
+  const long long l0 = tile * NL;
   for (int item = threadIdx.x; item < 3 * NL * R2; item += blockDim.x) {
     const int c = item / (NL * R2), rem = item - c * NL * R2;
     const int t = rem & (NL - 1), j2 = rem / NL;
@@ -378,6 +386,10 @@ __global__ void __launch_bounds__(256, 3) fft_product_pass(PassArgs<C> a) {
     }
   }
 }
+template <typename C, int R1, int R2>
+__global__ void __launch_bounds__(256, 3) fft_product_pass(PassArgs<C> a) {
+  fft_product_tile<C, R1, R2>(a, blockIdx.x);
+}
 
 }  // namespace n2c
 
@@ -455,20 +467,20 @@ __device__ __forceinline__ void smem_inverse(C *S, C *T, int NL, int NLP, unsign
 // Global line of tile line t: plain tiles hold lines l0 .. l0+NL-1; cell
 // tiles hold NP lattice columns of all 3 component planes ([3][nxy][L]).
 template <typename C>
-__device__ __forceinline__ long long zline_global(const PassArgs<C> &a, bool cells, int NP, int t) {
+__device__ __forceinline__ long long zline_global(const PassArgs<C> &a, bool cells, int NP, int t, long long tile) {
   if (!cells) {
-    const long long l = (long long)blockIdx.x * a.NL + t;
+    const long long l = tile * a.NL + t;
     return l < a.lines ? l : -1;
   }
   const int c = fdiv(t, a.np_div), p = t - c * NP;
-  const long long pos = (long long)blockIdx.x * NP + p;
+  const long long pos = tile * NP + p;
   return pos < a.nxy ? c * a.nxy + pos : -1;
 }
 
 // CELLS: the forward pass loads from the cell vector and stores T1 rows; the
 // inverse pass loads T1 rows and stores through the permittivity epilogue.
 template <typename C, int R1, int R2, bool INV, bool CELLS>
-__global__ void __launch_bounds__(256, 3) fft_zline_pass(PassArgs<C> a) {
+__device__ __forceinline__ void fft_zline_tile(const PassArgs<C> &a, long long tile, unsigned ntiles) {
   if (a.gate && *(volatile const int *)a.gate == 0) return;
   constexpr int L = R1 * R2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -478,7 +490,7 @@ __global__ void __launch_bounds__(256, 3) fft_zline_pass(PassArgs<C> a) {
   const int NP = NL / 3;
   // ---- load
   if (CELLS && !INV) {
-    const long long p0 = (long long)blockIdx.x * NP;
+    const long long p0 = tile * NP;
     for (int idx = threadIdx.x; idx < NP * L * 3; idx += blockDim.x) {
       const int c = idx % 3, rest = idx / 3, e = rest % L, p = rest / L;
       C val = czero<C>();
@@ -499,7 +511,7 @@ __global__ void __launch_bounds__(256, 3) fft_zline_pass(PassArgs<C> a) {
   } else {
     for (int idx = threadIdx.x; idx < NL * L; idx += blockDim.x) {
       const int t = idx / L, e = idx - t * L;
-      const long long l = zline_global(a, CELLS, NP, t);
+      const long long l = zline_global(a, CELLS, NP, t, tile);
       S[e * NLP + t] = (e < a.n_in && l >= 0) ? a.in[l * a.A_in + e] : czero<C>();
     }
   }
@@ -510,7 +522,7 @@ __global__ void __launch_bounds__(256, 3) fft_zline_pass(PassArgs<C> a) {
   // ---- store
   if (CELLS && INV) {
     double sq = 0;
-    const long long p0 = (long long)blockIdx.x * NP;
+    const long long p0 = tile * NP;
     for (int idx = threadIdx.x; idx < NP * a.n_out * 3; idx += blockDim.x) {
       const int c = idx % 3, rest = idx / 3, p = fdiv(rest, a.nout_div), e = rest - p * a.n_out;
       const long long pos = p0 + p;
@@ -527,15 +539,15 @@ __global__ void __launch_bounds__(256, 3) fft_zline_pass(PassArgs<C> a) {
     }
     if (a.norm) {
       const double2 bs = block_sum(make_double2(sq, 0));
-      if (threadIdx.x == 0) a.partials[blockIdx.x] = bs.x;
+      if (threadIdx.x == 0) a.partials[tile] = bs.x;
       __shared__ bool last;
       __threadfence();
       __syncthreads();
-      if (threadIdx.x == 0) last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+      if (threadIdx.x == 0) last = atomicAdd(a.ticket, 1u) == ntiles - 1;
       __syncthreads();
       if (last) {
         double t2 = 0;
-        for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) t2 += a.partials[i];
+        for (unsigned i = threadIdx.x; i < ntiles; i += blockDim.x) t2 += a.partials[i];
         const double2 tot = block_sum(make_double2(t2, 0));
         if (threadIdx.x == 0) { *a.norm = tot.x; *a.ticket = 0; }
       }
@@ -543,10 +555,14 @@ __global__ void __launch_bounds__(256, 3) fft_zline_pass(PassArgs<C> a) {
   } else {
     for (int idx = threadIdx.x; idx < NL * a.n_out; idx += blockDim.x) {
       const int t = fdiv(idx, a.nout_div), e = idx - t * a.n_out;
-      const long long l = zline_global(a, CELLS, NP, t);
+      const long long l = zline_global(a, CELLS, NP, t, tile);
       if (l >= 0) a.out[l * a.A_out + e] = R[e * NLP + t];
     }
   }
+}
+template <typename C, int R1, int R2, bool INV, bool CELLS>
+__global__ void __launch_bounds__(256, 3) fft_zline_pass(PassArgs<C> a) {
+  fft_zline_tile<C, R1, R2, INV, CELLS>(a, blockIdx.x, gridDim.x);
 }
 
 }  // namespace n2c

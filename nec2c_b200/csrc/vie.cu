@@ -23,6 +23,7 @@
 #include "fft_passes.cuh"
 #include "runtime.cuh"
 #include "vie_internal.cuh"
+#include "vie_batch.cuh"
 
 using namespace n2c;
 
@@ -120,11 +121,21 @@ static int axis_pass(int mode, int L, const C *in, C *out, const C *tw, long lon
   return fft_launch_pass<C>(mode, L, ch.radix, a, (size_t)L * a.NL * sizeof(C), tiles);
 }
 
+// Launch description of one pass: its arguments, kernel mode, line length,
+// radix variant, dynamic shared memory and tile count.
+template <typename C> struct PassPlan {
+  PassArgs<C> a;
+  int mode, L, variant;
+  size_t smem;
+  long long tiles;
+};
+
 template <typename C>
-static int product_pass(const n2d_vie *p, const C *in, C *out, const C *tw, const C *spec, n2d_pass_choice ch) {
+static void product_plan(const n2d_vie *p, const C *in, C *out, const C *tw, const C *spec, n2d_pass_choice ch,
+                         PassPlan<C> *pp) {
   const int L = (int)p->P[0], nx = (int)p->S[0];
   const long long I = p->P[1] * p->P[2];
-  PassArgs<C> a;
+  PassArgs<C> &a = pp->a;
   memset(&a, 0, sizeof(a));
   a.in = in; a.out = out; a.tw = tw; a.spec = spec;
   a.lines = I; a.I = I; a.A_in = nx; a.A_out = nx; a.n_in = nx; a.n_out = nx;
@@ -132,8 +143,24 @@ static int product_pass(const n2d_vie *p, const C *in, C *out, const C *tw, cons
   a.Py = (int)p->P[1]; a.Pz = (int)p->P[2]; a.Hy = (int)p->H[1]; a.Hz = (int)p->H[2];
   a.NL = ch.nl ? ch.nl : lines_per_tile(L, 3, sizeof(C));
   a.gate = n2c_gate();
-  const long long tiles = (a.lines + a.NL - 1) / a.NL;
-  return fft_launch_pass<C>(2, L, ch.radix, a, (size_t)3 * L * a.NL * sizeof(C), tiles);
+  pp->mode = 2; pp->L = L; pp->variant = ch.radix;
+  pp->smem = (size_t)3 * L * a.NL * sizeof(C);
+  pp->tiles = (a.lines + a.NL - 1) / a.NL;
+}
+
+// Strided y pass of the matvec (mode 0 forward, 1 inverse).
+template <typename C>
+static void strided_plan(int mode, int L, const C *in, C *out, const C *tw, long long B, long long I,
+                         long long A_in, long long A_out, int n_in, int n_out, n2d_pass_choice ch, PassPlan<C> *pp) {
+  PassArgs<C> &a = pp->a;
+  memset(&a, 0, sizeof(a));
+  a.in = in; a.out = out; a.tw = tw;
+  a.lines = B * I; a.I = I; a.A_in = A_in; a.A_out = A_out; a.n_in = n_in; a.n_out = n_out;
+  a.gate = n2c_gate();
+  a.NL = ch.nl ? ch.nl : lines_per_tile(L, 1, sizeof(C));
+  pp->mode = mode; pp->L = L; pp->variant = ch.radix;
+  pp->smem = (size_t)L * a.NL * sizeof(C);
+  pp->tiles = (a.lines + a.NL - 1) / a.NL;
 }
 
 // --------------------------------------------------------- scatter / gather
@@ -627,10 +654,10 @@ extern "C" int n2d_vie_set_eps(n2d_vie *p, const double *eps, const double *self
 // scatters (and preconditions) the cells, the inverse z pass applies
 // y = eps z - (eps-1) field and reduces |y|^2.
 template <typename C>
-static int z_cell_pass(int mode, n2d_vie *p, const C *in, C *out, const C *tw, const double2 *x,
-                       double2 *y, int precondition, double *norm, int *flag, n2d_pass_choice ch) {
+static int z_cell_plan(int mode, n2d_vie *p, const C *in, C *out, const C *tw, const double2 *x, double2 *y,
+                       int precondition, double *norm, int *flag, n2d_pass_choice ch, PassPlan<C> *pp) {
   const long long nx = p->S[0], ny = p->S[1], nz = p->S[2], Pz = p->P[2];
-  PassArgs<C> a;
+  PassArgs<C> &a = pp->a;
   memset(&a, 0, sizeof(a));
   a.in = in; a.out = out; a.tw = tw;
   a.lines = 3 * nx * ny; a.I = 1;
@@ -646,21 +673,22 @@ static int z_cell_pass(int mode, n2d_vie *p, const C *in, C *out, const C *tw, c
   a.nxy = nx * ny; a.mirror = p->mirror; a.precondition = precondition;
   a.flag = flag; a.partials = p->partials; a.ticket = p->ticket; a.norm = norm;
   const int NP = a.NL / 3;
-  const long long tiles = (a.nxy + NP - 1) / NP;
-  if (norm && tiles > 65536) { n2c_set_error("norm reduction grid too large"); return 0; }
+  pp->tiles = (a.nxy + NP - 1) / NP;
+  if (norm && pp->tiles > 65536) { n2c_set_error("norm reduction grid too large"); return 0; }
   // Cell tiles take T1 rows of 3 components: T1 is [3][nx*ny][Pz], so the
   // component planes are addressed through lines = comp * nxy + pos.
-  return fft_launch_pass<C>(mode == 3 ? 7 : 8, (int)Pz, ch.radix, a, (size_t)2 * (a.NL + 1) * Pz * sizeof(C),
-                            tiles);
+  pp->mode = mode == 3 ? 7 : 8; pp->L = (int)Pz; pp->variant = ch.radix;
+  pp->smem = (size_t)2 * (a.NL + 1) * Pz * sizeof(C);
+  return 1;
 }
 
 template <typename C> static constexpr int prec_of() { return sizeof(C) == sizeof(float2) ? 0 : 1; }
 
-// Pass `pass` of the matvec y = A x (numbering of n2d_pass_choice) with the
-// tile height and radix split of ch.
+// Launch description of pass `pass` of the matvec y = A x (numbering of
+// n2d_pass_choice) with the tile height and radix split of ch.
 template <typename C>
-static int run_pass(n2d_vie *p, int pass, n2d_pass_choice ch, const double2 *x, double2 *y, int precondition,
-                    double *norm, int *flag) {
+static int pass_plan(n2d_vie *p, int pass, n2d_pass_choice ch, const double2 *x, double2 *y, int precondition,
+                     double *norm, int *flag, PassPlan<C> *pp) {
   const long long nx = p->S[0], ny = p->S[1];
   const long long Py = p->P[1], Pz = p->P[2];
   constexpr bool single = sizeof(C) == sizeof(float2);
@@ -669,14 +697,22 @@ static int run_pass(n2d_vie *p, int pass, n2d_pass_choice ch, const double2 *x, 
   for (int d = 0; d < 3; ++d) tw[d] = single ? (const C *)p->tw32[d] : (const C *)p->tw64[d];
   const C *spec = single ? (const C *)p->spec : (const C *)p->spec64;
   switch (pass) {
-    case 0: return z_cell_pass<C>(3, p, nullptr, t1, tw[2], x, y, precondition, nullptr, flag, ch);
-    case 1: return axis_pass<C>(0, (int)Py, t1, t2, tw[1], 3 * nx, Pz, ny, Py, (int)ny, (int)Py, ch);
-    case 2: return product_pass<C>(p, t2, t2, tw[0], spec, ch);
-    case 3: return axis_pass<C>(1, (int)Py, t2, t1, tw[1], 3 * nx, Pz, Py, ny, (int)Py, (int)ny, ch);
-    case 4: return z_cell_pass<C>(4, p, t1, nullptr, tw[2], x, y, precondition, norm, flag, ch);
+    case 0: return z_cell_plan<C>(3, p, nullptr, t1, tw[2], x, y, precondition, nullptr, flag, ch, pp);
+    case 1: strided_plan<C>(0, (int)Py, t1, t2, tw[1], 3 * nx, Pz, ny, Py, (int)ny, (int)Py, ch, pp); return 1;
+    case 2: product_plan<C>(p, t2, t2, tw[0], spec, ch, pp); return 1;
+    case 3: strided_plan<C>(1, (int)Py, t2, t1, tw[1], 3 * nx, Pz, Py, ny, (int)Py, (int)ny, ch, pp); return 1;
+    case 4: return z_cell_plan<C>(4, p, t1, nullptr, tw[2], x, y, precondition, norm, flag, ch, pp);
   }
   n2c_set_error("no FFT pass %d", pass);
   return 0;
+}
+
+template <typename C>
+static int run_pass(n2d_vie *p, int pass, n2d_pass_choice ch, const double2 *x, double2 *y, int precondition,
+                    double *norm, int *flag) {
+  PassPlan<C> pp;
+  if (!pass_plan<C>(p, pass, ch, x, y, precondition, norm, flag, &pp)) return 0;
+  return fft_launch_pass<C>(pp.mode, pp.L, pp.variant, pp.a, pp.smem, pp.tiles);
 }
 
 template <typename C>
@@ -942,3 +978,22 @@ extern "C" int n2d_vie_precondition(n2d_vie *p, const double *x, double *y) {
                                                               (double2 *)y, n);
   return n2c_check_launch("precondition");
 }
+
+template <typename C>
+int n2c_vie_pass_plans(n2d_vie *p, int precondition, double *norm, int *flag, PassArgs<C> args[5], int mode[5],
+                       int L[5], size_t smem[5], long long tiles[5]) {
+  for (int i = 0; i < N2D_VIE_PASSES; ++i) {
+    PassPlan<C> pp;
+    if (!pass_plan<C>(p, i, n2d_pass_choice{0, 0}, nullptr, nullptr, precondition, norm, flag, &pp)) return 0;
+    args[i] = pp.a;
+    mode[i] = pp.mode;
+    L[i] = pp.L;
+    smem[i] = pp.smem;
+    tiles[i] = pp.tiles;
+  }
+  return 1;
+}
+template int n2c_vie_pass_plans<float2>(n2d_vie *, int, double *, int *, PassArgs<float2> *, int *, int *, size_t *,
+                                        long long *);
+template int n2c_vie_pass_plans<double2>(n2d_vie *, int, double *, int *, PassArgs<double2> *, int *, int *,
+                                         size_t *, long long *);

@@ -1,0 +1,825 @@
+// Ragged batch of volume FFT plans solved together on one GPU.
+//
+// Many frequencies or geometries, each a plan with its own lattice, padded
+// grid (axes up to 128) and spectrum, advance through GMRES(m) in lockstep:
+//   - every FFT pass of a product is ONE launch over the tiles of all plans:
+//     a CTA finds its plan by binary search over the plans' first tiles and
+//     runs the tile body of that plan's line length (fft_engine.cuh);
+//   - every Gram-Schmidt sweep, update and norm is one launch over all
+//     systems' unknowns: a CTA covers a fixed range of one system, and the
+//     last CTA of each system finishes its reduction in a fixed order;
+//   - the m Arnoldi steps of a restart cycle are one captured CUDA graph.
+// Each system keeps its own GMRES state (Hessenberg matrix, rotations,
+// status) with vie_gmres's per-system semantics (vie_iterative.c:90-200);
+// a system that has converged or stopped is gated off and costs nothing.
+// The Arnoldi process is classical Gram-Schmidt: the second pass runs on a
+// tenfold cancellation for plans with FP32 transforms and always for FP64
+// plans (CGS2, as stable as the two MGS passes of vie_iterative.c).
+//
+// The batch's vectors are the plans' cell vectors (3 x cells each)
+// concatenated in plan order.
+#include <float.h>
+#include <math.h>
+#include <string.h>
+#include <algorithm>
+#include <vector>
+#include "common.cuh"
+#include "device_api.h"
+#include "runtime.cuh"
+#include "vie_batch.cuh"
+#include "vie_internal.cuh"
+
+using namespace n2c;
+
+namespace {
+
+enum { ST_CONVERGED, ST_LIMIT, ST_BREAKDOWN, ST_CALLBACK, ST_INVALID, ST_ALLOC, ST_NONFINITE };
+enum { ST_RUNNING = -1 };
+
+constexpr int BMAXM = 30;                         // longest restart cycle of a batch
+constexpr int MAX_L = 128;                        // longest padded axis of a batched plan
+constexpr double REORTH = 10.0;                   // cancellation factor of the FP32-transform form
+constexpr int DOT_E = 4;                          // elements per lane per dots load
+constexpr int DOT_GROUP = 32 * DOT_E;             // elements per warp group
+constexpr long long DOT_RANGE = 32 * DOT_GROUP;   // elements per dots CTA
+constexpr size_t DOT_SMEM = (size_t)DOT_RANGE * sizeof(double2);
+constexpr int VEC_THREADS = 256;
+constexpr long long VEC_RANGE = 4 * VEC_THREADS;  // elements per vector-kernel CTA
+
+template <typename C> struct BatchDesc {
+  PassArgs<C> a;
+  long long off;   // first element of the plan's cell vector in the batch vectors
+  int L;           // line length of the pass
+};
+
+// Per-system GMRES state (device).
+struct BSys {
+  int active;      // inner iterations of the current cycle still running
+  int running;     // gate of the true-residual product
+  int status;      // ST_RUNNING or a final status
+  int flag;        // non-finite raised in an Arnoldi product
+  int rflag;       // non-finite raised in a residual product or norm
+  int used, breakdown, normalize, reorth;
+  int m;           // cycle length of this system, min(restart, unknowns)
+  long long iterations, max_iterations;
+  double target, before_sq, after, beta;
+  unsigned ticket;
+  int pad;
+};
+
+struct BView {
+  BSys *sys;
+  const long long *off;                 // K + 1 element offsets
+  const long long *first_d, *first_v;   // K + 1 first CTAs (dots / vector kernels)
+  int K, m;                             // systems; Hessenberg leading dimension
+  long long N;
+  double2 *V, *w, *r, *H, *g, *sn, *y, *hp;
+  double *cs;
+  double2 *parts_d;
+  double *parts_v, *norms;
+  const double2 *const *diag;           // Jacobi divisors of each system
+  int always_reorth;
+};
+
+__device__ __forceinline__ int find_seg(const long long *first, int count, long long x) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (first[mid] <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// True in the one CTA that arrives last among `count` CTAs sharing ticket.
+__device__ __forceinline__ bool last_of(unsigned *ticket, unsigned count) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == count - 1;
+  __syncthreads();
+  return last;
+}
+
+__device__ __forceinline__ double cabs_(double2 a) { return hypot(a.x, a.y); }
+
+// ------------------------------------------------------- batched FFT passes
+template <typename C, int R1, int R2, int MODE>
+__device__ __forceinline__ void tile_body(const PassArgs<C> &a, long long tile, unsigned ntiles) {
+  if constexpr (MODE == 0) fft_forward_tile<C, R1, R2>(a, tile);
+  else if constexpr (MODE == 1) fft_inverse_tile<C, R1, R2>(a, tile, ntiles);
+  else if constexpr (MODE == 2) fft_product_tile<C, R1, R2>(a, tile);
+  else if constexpr (MODE == 7) fft_zline_tile<C, R1, R2, false, true>(a, tile, ntiles);
+  else fft_zline_tile<C, R1, R2, true, true>(a, tile, ntiles);
+}
+
+// One pass over the tiles of every plan; x / y are the batch vectors the z
+// passes scatter from and gather into.
+template <typename C, int MODE>
+__global__ void __launch_bounds__(256, MODE <= 1 ? 1 : 3)
+    batch_pass_kernel(const BatchDesc<C> *desc, const long long *first, int count, const double2 *x, double2 *y) {
+  const int q = find_seg(first, count, blockIdx.x);
+  PassArgs<C> a = desc[q].a;
+  if (MODE >= 7) {
+    a.cx = x + desc[q].off;
+    a.cy = y + desc[q].off;
+  }
+  const long long tile = (long long)blockIdx.x - first[q];
+  const unsigned ntiles = (unsigned)(first[q + 1] - first[q]);
+  switch (desc[q].L) {
+    case 1: tile_body<C, 1, 1, MODE>(a, tile, ntiles); break;
+    case 2: tile_body<C, 2, 1, MODE>(a, tile, ntiles); break;
+    case 4: tile_body<C, 4, 1, MODE>(a, tile, ntiles); break;
+    case 8: tile_body<C, 8, 1, MODE>(a, tile, ntiles); break;
+    case 16: tile_body<C, 16, 1, MODE>(a, tile, ntiles); break;
+    case 32: tile_body<C, 8, 4, MODE>(a, tile, ntiles); break;
+    case 64: tile_body<C, 8, 8, MODE>(a, tile, ntiles); break;
+    case 128: tile_body<C, 16, 8, MODE>(a, tile, ntiles); break;
+  }
+}
+
+template <typename C>
+void (*batch_kernel(int mode))(const BatchDesc<C> *, const long long *, int, const double2 *, double2 *) {
+  switch (mode) {
+    case 0: return batch_pass_kernel<C, 0>;
+    case 1: return batch_pass_kernel<C, 1>;
+    case 2: return batch_pass_kernel<C, 2>;
+    case 7: return batch_pass_kernel<C, 7>;
+  }
+  return batch_pass_kernel<C, 8>;
+}
+
+// ---------------------------------------------------------- vector kernels
+// CTA (q, t) of a vector kernel covers elements [t VEC_RANGE, (t+1) VEC_RANGE)
+// of system q (clipped to the system).
+struct VecCta {
+  int q;
+  long long lo, hi, nctas;
+  bool first;
+};
+__device__ __forceinline__ VecCta vec_cta(const BView &v) {
+  VecCta c;
+  c.q = find_seg(v.first_v, v.K, blockIdx.x);
+  const long long t = (long long)blockIdx.x - v.first_v[c.q];
+  c.lo = v.off[c.q] + t * VEC_RANGE;
+  c.hi = min(c.lo + VEC_RANGE, v.off[c.q + 1]);
+  c.nctas = v.first_v[c.q + 1] - v.first_v[c.q];
+  c.first = t == 0;
+  return c;
+}
+
+// Sum over the vector CTAs of system q of their partials, in CTA order (same
+// value in every thread of the calling CTA).
+__device__ double sum_parts_v(const BView &v, int q) {
+  double t = 0;
+  for (long long c = v.first_v[q] + threadIdx.x; c < v.first_v[q + 1]; c += blockDim.x) t += v.parts_v[c];
+  return block_sum(make_double2(t, 0)).x;
+}
+
+// norms[q] = ||x_q||^2 of every system; a non-finite sum raises rflag.
+__global__ void __launch_bounds__(VEC_THREADS) seg_norm_kernel(BView v, const double2 *x, double *norms) {
+  const VecCta c = vec_cta(v);
+  double sq = 0;
+  for (long long i = c.lo + threadIdx.x; i < c.hi; i += VEC_THREADS) sq += x[i].x * x[i].x + x[i].y * x[i].y;
+  const double2 bs = block_sum(make_double2(sq, 0));
+  if (threadIdx.x == 0) v.parts_v[blockIdx.x] = bs.x;
+  BSys *s = v.sys + c.q;
+  if (!last_of(&s->ticket, (unsigned)c.nctas)) return;
+  const double tot = sum_parts_v(v, c.q);
+  if (threadIdx.x == 0) {
+    norms[c.q] = tot;
+    if (!isfinite(tot)) s->rflag = 1;
+    s->ticket = 0;
+  }
+}
+
+// r = b - r (A x already in r) for the systems whose residual is taken.
+__global__ void __launch_bounds__(VEC_THREADS) seg_residual_kernel(BView v, const double2 *rhs) {
+  const VecCta c = vec_cta(v);
+  if (!v.sys[c.q].running) return;
+  for (long long i = c.lo + threadIdx.x; i < c.hi; i += VEC_THREADS) v.r[i] = csub(rhs[i], v.r[i]);
+}
+
+// v_0 = r / beta, Hessenberg and right-hand side reset for a new cycle.
+__global__ void __launch_bounds__(VEC_THREADS) seg_cycle_start_kernel(BView v) {
+  const VecCta c = vec_cta(v);
+  const BSys *s = v.sys + c.q;
+  if (!s->active) return;
+  const double beta = s->beta;
+  for (long long i = c.lo + threadIdx.x; i < c.hi; i += VEC_THREADS)
+    v.V[i] = make_double2(v.r[i].x / beta, v.r[i].y / beta);
+  if (!c.first) return;
+  double2 *H = v.H + (long long)c.q * (v.m + 1) * v.m, *g = v.g + (long long)c.q * (v.m + 1);
+  for (int i = threadIdx.x; i < (v.m + 1) * v.m; i += VEC_THREADS) H[i] = make_double2(0, 0);
+  for (int i = threadIdx.x; i <= v.m; i += VEC_THREADS) g[i] = make_double2(i == 0 ? beta : 0, 0);
+}
+
+// Complex unitary Givens [c s; -conj(s) c], vie_iterative.c:66-78.
+__device__ void givens(double2 a, double2 b, double *c, double2 *s) {
+  const double aa = cabs_(a), bb = cabs_(b);
+  if (bb == 0.0) { *c = 1.0; *s = make_double2(0, 0); }
+  else if (aa == 0.0) { *c = 0.0; *s = make_double2(b.x / bb, -b.y / bb); }
+  else {
+    const double len = hypot(aa, bb);
+    *c = aa / len;
+    const double2 ua = make_double2(a.x / aa, a.y / aa), ub = make_double2(b.x / len, -b.y / len);
+    *s = cmul(ua, ub);
+  }
+}
+
+// Column j of system q finished with h_{j+1,j} = after: previous rotations,
+// the new rotation, the residual estimate and the cycle's stop conditions
+// (vie_iterative.c:160-177).
+__device__ void finish_column(const BView &v, int q, int j, double after) {
+  BSys *s = v.sys + q;
+  const int m = v.m;
+  const double before = sqrt(s->before_sq);
+  const bool broke = after <= 32 * DBL_EPSILON * before;
+  s->after = after;
+  s->reorth = 0;
+  if (!isfinite(after)) { s->status = ST_NONFINITE; s->active = 0; return; }
+  double2 *H = v.H + (long long)q * (m + 1) * m, *g = v.g + (long long)q * (m + 1), *sn = v.sn + (long long)q * m;
+  double *cs = v.cs + (long long)q * m;
+  H[(long long)(j + 1) * m + j] = make_double2(after, 0);
+  for (int k = 0; k < j; ++k) {
+    const double2 h0 = H[(long long)k * m + j], h1 = H[(long long)(k + 1) * m + j];
+    H[(long long)k * m + j] = cadd(cscale(h0, cs[k]), cmul(sn[k], h1));
+    H[(long long)(k + 1) * m + j] = csub(cscale(h1, cs[k]), cconjmul(sn[k], h0));
+  }
+  double c;
+  double2 sr;
+  givens(H[(long long)j * m + j], H[(long long)(j + 1) * m + j], &c, &sr);
+  cs[j] = c;
+  sn[j] = sr;
+  H[(long long)j * m + j] = cadd(cscale(H[(long long)j * m + j], c), cmul(sr, H[(long long)(j + 1) * m + j]));
+  H[(long long)(j + 1) * m + j] = make_double2(0, 0);
+  const double2 gj = g[j];
+  g[j + 1] = make_double2(-(sr.x * gj.x + sr.y * gj.y), -(sr.x * gj.y - sr.y * gj.x));   // -conj(s) g_j
+  g[j] = cscale(gj, c);
+  s->iterations += 1;
+  s->used = j + 1;
+  s->breakdown = broke;
+  s->normalize = !broke;
+  if (broke || cabs_(g[j + 1]) <= s->target || j + 1 >= s->m || s->iterations >= s->max_iterations) s->active = 0;
+}
+
+// h = V^H w of pass P for every active system.  CTA (q, t) covers DOT_RANGE
+// elements of system q; warp k % kk of each group of kk warps handles basis
+// vector k over its element group, the w chunk sits in shared memory.
+template <int P>
+__global__ void __launch_bounds__(1024) seg_dots_kernel(BView v, int j) {
+  const int q = find_seg(v.first_d, v.K, blockIdx.x);
+  BSys *s = v.sys + q;
+  if (!s->active || (P == 1 && !s->reorth)) return;
+  const long long t0 = (long long)blockIdx.x - v.first_d[q];
+  if (P == 0 && s->flag) {
+    if (t0 == 0 && threadIdx.x == 0) { s->status = ST_NONFINITE; s->active = 0; }
+    return;
+  }
+  const int kk = j + 1, groups = 32 / kk, chunk = groups * DOT_GROUP;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, k = warp % kk, grp = warp / kk;
+  const bool act = grp < groups;
+  const long long lo = v.off[q] + t0 * DOT_RANGE, hi = min(lo + DOT_RANGE, v.off[q + 1]);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2 *sw = reinterpret_cast<double2 *>(smem_raw);   // [chunk]
+  const double2 *Vk = v.V + (long long)k * v.N;
+  const int wper = (chunk + blockDim.x - 1) / blockDim.x;
+  double2 acc = make_double2(0, 0), vv[DOT_E], vn[DOT_E], wv[4], wn[4];
+  auto load = [&](long long base, double2 (&a)[DOT_E], double2 (&b)[4]) {
+    if (act) {
+#pragma unroll
+      for (int e = 0; e < DOT_E; ++e) {
+        const long long i = base + grp * DOT_GROUP + lane + 32 * e;
+        a[e] = i < hi ? Vk[i] : make_double2(0, 0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int tt = threadIdx.x + u * blockDim.x;
+      b[u] = (u < wper && tt < chunk && base + tt < hi) ? v.w[base + tt] : make_double2(0, 0);
+    }
+  };
+  load(lo, vv, wv);
+  for (long long base = lo; base < hi; base += chunk) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int tt = threadIdx.x + u * blockDim.x;
+      if (u < wper && tt < chunk) sw[tt] = wv[u];
+    }
+    if (base + chunk < hi) load(base + chunk, vn, wn);
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int e = 0; e < DOT_E; ++e) acc = cadd(acc, cconjmul(vv[e], sw[grp * DOT_GROUP + lane + 32 * e]));
+    }
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < DOT_E; ++e) vv[e] = vn[e];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) wv[u] = wn[u];
+  }
+  __shared__ double2 red[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+  }
+  if (lane == 0) red[warp] = act ? acc : make_double2(0, 0);
+  __syncthreads();
+  if (threadIdx.x < kk) {
+    double2 tt = make_double2(0, 0);
+    for (int gg = 0; gg < groups; ++gg) tt = cadd(tt, red[gg * kk + threadIdx.x]);
+    v.parts_d[(long long)blockIdx.x * BMAXM + threadIdx.x] = tt;
+  }
+  const long long nctas = v.first_d[q + 1] - v.first_d[q];
+  if (!last_of(&s->ticket, (unsigned)nctas)) return;
+  if (warp < kk) {
+    double2 tt = make_double2(0, 0);
+    for (long long c = v.first_d[q] + lane; c < v.first_d[q + 1]; c += 32)
+      tt = cadd(tt, v.parts_d[c * BMAXM + warp]);
+    for (int o = 16; o > 0; o >>= 1) {
+      tt.x += __shfl_xor_sync(0xffffffffu, tt.x, o);
+      tt.y += __shfl_xor_sync(0xffffffffu, tt.y, o);
+    }
+    if (lane == 0) {
+      const int m = v.m;
+      v.hp[((long long)q * 2 + P) * BMAXM + warp] = tt;
+      double2 *H = v.H + (long long)q * (m + 1) * m;
+      H[(long long)warp * m + j] = cadd(H[(long long)warp * m + j], tt);
+    }
+  }
+  if (threadIdx.x == 0) s->ticket = 0;
+}
+
+// w -= V h of pass P and ||w||^2 for every active system; the last CTA of a
+// system requests its second pass or finishes its column.
+template <int P>
+__global__ void __launch_bounds__(VEC_THREADS) seg_update_kernel(BView v, int j) {
+  const VecCta c = vec_cta(v);
+  BSys *s = v.sys + c.q;
+  if (!s->active || (P == 1 && !s->reorth)) return;
+  const int kk = j + 1;
+  __shared__ double2 hs[BMAXM];
+  if (threadIdx.x < kk) hs[threadIdx.x] = v.hp[((long long)c.q * 2 + P) * BMAXM + threadIdx.x];
+  __syncthreads();
+  double sq = 0;
+  for (long long i = c.lo + threadIdx.x; i < c.hi; i += VEC_THREADS) {
+    double2 wi = v.w[i];
+#pragma unroll 6
+    for (int k = 0; k < kk; ++k) wi = csub(wi, cmul(hs[k], v.V[(long long)k * v.N + i]));
+    v.w[i] = wi;
+    sq += wi.x * wi.x + wi.y * wi.y;
+  }
+  const double2 bs = block_sum(make_double2(sq, 0));
+  if (threadIdx.x == 0) v.parts_v[blockIdx.x] = bs.x;
+  if (!last_of(&s->ticket, (unsigned)c.nctas)) return;
+  const double tot = sum_parts_v(v, c.q);
+  if (threadIdx.x != 0) return;
+  s->ticket = 0;
+  const double after = sqrt(tot);
+  if (P == 0 && isfinite(after) && (v.always_reorth || REORTH * after < sqrt(s->before_sq))) {
+    s->reorth = 1;
+    return;
+  }
+  finish_column(v, c.q, j, after);
+}
+
+// v_{j+1} = w / ||w|| of every system whose column j was finished without
+// breakdown and whose cycle continues.
+__global__ void __launch_bounds__(VEC_THREADS) seg_normalize_kernel(BView v, int j) {
+  const VecCta c = vec_cta(v);
+  const BSys *s = v.sys + c.q;
+  if (!s->active || !s->normalize) return;
+  const double inv = s->after;
+  double2 *vn = v.V + (long long)(j + 1) * v.N;
+  for (long long i = c.lo + threadIdx.x; i < c.hi; i += VEC_THREADS)
+    vn[i] = make_double2(v.w[i].x / inv, v.w[i].y / inv);
+}
+
+// y = H^{-1} g of every running system (vie_iterative.c:179-186), one thread
+// per system.
+__global__ void seg_backsolve_kernel(BView v) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= v.K) return;
+  BSys *s = v.sys + q;
+  if (s->status != ST_RUNNING) return;
+  const int m = v.m, used = s->used;
+  const double2 *H = v.H + (long long)q * (m + 1) * m, *g = v.g + (long long)q * (m + 1);
+  double2 *y = v.y + (long long)q * m;
+  for (int i = used - 1; i >= 0; --i) {
+    double2 val = g[i];
+    for (int k = i + 1; k < used; ++k) val = csub(val, cmul(H[(long long)i * m + k], y[k]));
+    const double2 d = H[(long long)i * m + i];
+    if (cabs_(d) == 0.0) { s->status = ST_BREAKDOWN; return; }
+    y[i] = cdiv(val, d);
+  }
+}
+
+// x += D^-1 (sum_j v_j y_j) of every running system.
+__global__ void __launch_bounds__(VEC_THREADS) seg_xupdate_kernel(BView v, double2 *x) {
+  const VecCta c = vec_cta(v);
+  const BSys *s = v.sys + c.q;
+  if (s->status != ST_RUNNING) return;
+  const int used = s->used;
+  const double2 *y = v.y + (long long)c.q * v.m, *diag = v.diag[c.q];
+  const long long base = v.off[c.q];
+  for (long long i = c.lo + threadIdx.x; i < c.hi; i += VEC_THREADS) {
+    double2 acc = make_double2(0, 0);
+    for (int jj = 0; jj < used; ++jj) {
+      const double2 z = cdiv(v.V[(long long)jj * v.N + i], diag[i - base]);
+      acc = cadd(acc, cmul(z, y[jj]));
+    }
+    x[i] = cadd(x[i], acc);
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host side
+// Pass descriptor sets: 0 Arnoldi products (transform precision, Jacobi
+// preconditioned input, ||w||^2, gated by each system's cycle), 1 true
+// residual products (FP64, gated by the running systems), 2 plain products
+// (transform precision, ungated).
+struct PassSet {
+  void *desc = nullptr;        // BatchDesc<C>[K]
+  long long *first = nullptr;  // K + 1 first tiles
+  long long tiles = 0;
+  size_t smem = 0;
+  int mode = 0;
+  bool fp32 = false;
+};
+
+struct BatchWork {
+  int m = 0;
+  BView v;
+  cudaGraphExec_t inner = nullptr;
+  unsigned inner_launches = 0;
+  bool tried_graph = false;
+};
+
+struct n2d_vie_batch {
+  int K = 0, fp32 = 0;
+  long long N = 0;
+  std::vector<n2d_vie *> plans;
+  std::vector<long long> off, first_d, first_v;
+  long long *off_dev = nullptr, *first_d_dev = nullptr, *first_v_dev = nullptr;
+  BSys *sys = nullptr;
+  const double2 **diag_dev = nullptr;
+  PassSet sets[3][N2D_VIE_PASSES];
+  BatchWork *work = nullptr;
+};
+
+static void work_free(BatchWork *w) {
+  if (!w) return;
+  if (w->inner) cudaGraphExecDestroy(w->inner);
+  BView &v = w->v;
+  void *bufs[] = {v.V, v.w, v.r, v.H, v.g, v.sn, v.y, v.hp, v.cs, v.parts_d, v.parts_v, v.norms};
+  for (void *q : bufs) n2d_free(q);
+  delete w;
+}
+
+extern "C" void n2d_vie_batch_destroy(n2d_vie_batch *b) {
+  if (!b) return;
+  work_free(b->work);
+  for (auto &set : b->sets)
+    for (PassSet &ps : set) {
+      n2d_free(ps.desc);
+      n2d_free(ps.first);
+    }
+  n2d_free(b->off_dev);
+  n2d_free(b->first_d_dev);
+  n2d_free(b->first_v_dev);
+  n2d_free(b->sys);
+  n2d_free((void *)b->diag_dev);
+  delete b;
+}
+
+template <typename C>
+static int build_set(n2d_vie_batch *b, int set) {
+  const int K = b->K;
+  std::vector<BatchDesc<C>> desc[N2D_VIE_PASSES];
+  std::vector<long long> first[N2D_VIE_PASSES];
+  for (int i = 0; i < N2D_VIE_PASSES; ++i) {
+    desc[i].resize(K);
+    first[i].assign(K + 1, 0);
+  }
+  for (int q = 0; q < K; ++q) {
+    BSys *s = b->sys + q;
+    PassArgs<C> args[N2D_VIE_PASSES];
+    int mode[N2D_VIE_PASSES], L[N2D_VIE_PASSES];
+    size_t smem[N2D_VIE_PASSES];
+    long long tiles[N2D_VIE_PASSES];
+    const int precondition = set == 0;
+    double *norm = set == 0 ? &s->before_sq : nullptr;
+    int *flag = set == 0 ? &s->flag : set == 1 ? &s->rflag : nullptr;
+    if (!n2c_vie_pass_plans<C>(b->plans[q], precondition, norm, flag, args, mode, L, smem, tiles)) return 0;
+    for (int i = 0; i < N2D_VIE_PASSES; ++i) {
+      args[i].gate = set == 0 ? &s->active : set == 1 ? &s->running : nullptr;
+      desc[i][q].a = args[i];
+      desc[i][q].off = b->off[q];
+      desc[i][q].L = L[i];
+      first[i][q + 1] = first[i][q] + tiles[i];
+      PassSet &ps = b->sets[set][i];
+      ps.mode = mode[i];
+      ps.smem = std::max(ps.smem, smem[i]);
+    }
+  }
+  for (int i = 0; i < N2D_VIE_PASSES; ++i) {
+    PassSet &ps = b->sets[set][i];
+    ps.fp32 = sizeof(C) == sizeof(float2);
+    ps.tiles = first[i][K];
+    if (ps.tiles > 0x7fffffffLL) { n2c_set_error("batch pass grid too large"); return 0; }
+    ps.desc = n2d_alloc(K * sizeof(BatchDesc<C>));
+    ps.first = (long long *)n2d_alloc((K + 1) * sizeof(long long));
+    if (!ps.desc || !ps.first || !n2d_upload(ps.desc, desc[i].data(), K * sizeof(BatchDesc<C>)) ||
+        !n2d_upload(ps.first, first[i].data(), (K + 1) * sizeof(long long)))
+      return 0;
+  }
+  return 1;
+}
+
+template <typename C>
+static int launch_set_t(const n2d_vie_batch *b, const PassSet &ps, const double2 *x, double2 *y) {
+  auto k = batch_kernel<C>(ps.mode);
+  static bool configured[9] = {false, false, false, false, false, false, false, false, false};
+  if (!configured[ps.mode]) {
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
+        cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess) {
+      n2c_set_error("cannot raise shared memory for the batched FFT pass");
+      return 0;
+    }
+    configured[ps.mode] = true;
+  }
+  k<<<(unsigned)ps.tiles, 256, ps.smem, n2c_stream()>>>((const BatchDesc<C> *)ps.desc, ps.first, b->K, x, y);
+  return n2c_check_launch("batched fft pass");
+}
+
+// y = A x over the whole batch with descriptor set `set`.
+static int batch_apply(const n2d_vie_batch *b, int set, const double2 *x, double2 *y) {
+  for (int i = 0; i < N2D_VIE_PASSES; ++i) {
+    const PassSet &ps = b->sets[set][i];
+    const int ok = ps.fp32 ? launch_set_t<float2>(b, ps, x, y) : launch_set_t<double2>(b, ps, x, y);
+    if (!ok) return 0;
+  }
+  return 1;
+}
+
+extern "C" int n2d_vie_batch_create(n2d_vie_batch **out, n2d_vie *const *plans, long long count) {
+  *out = nullptr;
+  if (count < 1 || count > (1 << 20)) { n2c_set_error("batch of %lld plans", count); return 0; }
+  n2d_vie_batch *b = new n2d_vie_batch();
+  b->K = (int)count;
+  b->fp32 = n2d_vie_fp32(plans[0]);
+  b->off.assign(count + 1, 0);
+  b->first_d.assign(count + 1, 0);
+  b->first_v.assign(count + 1, 0);
+  std::vector<const double2 *> diag(count);
+  for (long long q = 0; q < count; ++q) {
+    n2d_vie *p = plans[q];
+    if (!p || p->cells < 1) { n2c_set_error("batch plan %lld is empty", q); delete b; return 0; }
+    if (n2d_vie_fp32(p) != b->fp32) {
+      n2c_set_error("batch plans mix FP32 and FP64 transforms");
+      delete b;
+      return 0;
+    }
+    for (int d = 0; d < 3; ++d)
+      if (p->P[d] > MAX_L) {
+        n2c_set_error("batch plan %lld: padded axis %lld exceeds %d", q, p->P[d], MAX_L);
+        delete b;
+        return 0;
+      }
+    for (long long r = 0; r < q; ++r)
+      if (plans[r] == p) { n2c_set_error("plan %lld appears twice in the batch", q); delete b; return 0; }
+    const long long n = 3 * (p->mirror ? p->mirror : p->cells);
+    b->plans.push_back(p);
+    b->off[q + 1] = b->off[q] + n;
+    b->first_d[q + 1] = b->first_d[q] + (n + DOT_RANGE - 1) / DOT_RANGE;
+    b->first_v[q + 1] = b->first_v[q] + (n + VEC_RANGE - 1) / VEC_RANGE;
+    diag[q] = (const double2 *)n2d_vie_diag(p);
+  }
+  b->N = b->off[count];
+  if (b->first_v[count] > 0x7fffffffLL) { n2c_set_error("batch too large"); delete b; return 0; }
+  b->off_dev = (long long *)n2d_alloc((count + 1) * sizeof(long long));
+  b->first_d_dev = (long long *)n2d_alloc((count + 1) * sizeof(long long));
+  b->first_v_dev = (long long *)n2d_alloc((count + 1) * sizeof(long long));
+  b->sys = (BSys *)n2d_alloc(count * sizeof(BSys));
+  b->diag_dev = (const double2 **)n2d_alloc(count * sizeof(double2 *));
+  int ok = b->off_dev && b->first_d_dev && b->first_v_dev && b->sys && b->diag_dev &&
+           n2d_upload(b->off_dev, b->off.data(), (count + 1) * sizeof(long long)) &&
+           n2d_upload(b->first_d_dev, b->first_d.data(), (count + 1) * sizeof(long long)) &&
+           n2d_upload(b->first_v_dev, b->first_v.data(), (count + 1) * sizeof(long long)) &&
+           n2d_upload((void *)b->diag_dev, diag.data(), count * sizeof(double2 *)) &&
+           n2d_memset(b->sys, 0, count * sizeof(BSys));
+  if (ok) ok = b->fp32 ? build_set<float2>(b, 0) : build_set<double2>(b, 0);
+  if (ok) ok = build_set<double2>(b, 1);
+  if (ok) ok = b->fp32 ? build_set<float2>(b, 2) : build_set<double2>(b, 2);
+  if (!ok || !n2d_sync()) { n2d_vie_batch_destroy(b); return 0; }
+  *out = b;
+  return 1;
+}
+
+extern "C" long long n2d_vie_batch_order(const n2d_vie_batch *b) { return b ? b->N : 0; }
+extern "C" long long n2d_vie_batch_offset(const n2d_vie_batch *b, long long q) {
+  return b && q >= 0 && q <= b->K ? b->off[q] : -1;
+}
+
+extern "C" int n2d_vie_batch_apply(n2d_vie_batch *b, const double *x_dev, double *y_dev) {
+  return batch_apply(b, 2, (const double2 *)x_dev, (double2 *)y_dev);
+}
+
+static BatchWork *work_get(n2d_vie_batch *b, int m) {
+  if (b->work && b->work->m == m) return b->work;
+  work_free(b->work);
+  b->work = nullptr;
+  BatchWork *w = new BatchWork();
+  w->m = m;
+  BView &v = w->v;
+  memset(&v, 0, sizeof(v));
+  const long long N = b->N, K = b->K;
+  v.sys = b->sys; v.off = b->off_dev; v.first_d = b->first_d_dev; v.first_v = b->first_v_dev;
+  v.K = b->K; v.m = m; v.N = N; v.diag = b->diag_dev; v.always_reorth = !b->fp32;
+  v.V = (double2 *)n2d_alloc((size_t)(m + 1) * N * sizeof(double2));
+  v.w = (double2 *)n2d_alloc(N * sizeof(double2));
+  v.r = (double2 *)n2d_alloc(N * sizeof(double2));
+  v.H = (double2 *)n2d_alloc(K * (m + 1) * m * sizeof(double2));
+  v.g = (double2 *)n2d_alloc(K * (m + 1) * sizeof(double2));
+  v.sn = (double2 *)n2d_alloc(K * m * sizeof(double2));
+  v.y = (double2 *)n2d_alloc(K * m * sizeof(double2));
+  v.hp = (double2 *)n2d_alloc(K * 2 * BMAXM * sizeof(double2));
+  v.cs = (double *)n2d_alloc(K * m * sizeof(double));
+  v.parts_d = (double2 *)n2d_alloc(b->first_d[K] * BMAXM * sizeof(double2));
+  v.parts_v = (double *)n2d_alloc(b->first_v[K] * sizeof(double));
+  v.norms = (double *)n2d_alloc(2 * K * sizeof(double));
+  if (!v.V || !v.w || !v.r || !v.H || !v.g || !v.sn || !v.y || !v.hp || !v.cs || !v.parts_d || !v.parts_v ||
+      !v.norms) {
+    work_free(w);
+    return nullptr;
+  }
+  b->work = w;
+  return w;
+}
+
+// The m gated Arnoldi steps of a cycle on the current stream.
+static int enqueue_inner(n2d_vie_batch *b, BatchWork *w) {
+  BView &v = w->v;
+  const unsigned nd = (unsigned)b->first_d[b->K], nv = (unsigned)b->first_v[b->K];
+  for (int j = 0; j < w->m; ++j) {
+    if (!batch_apply(b, 0, v.V + (long long)j * v.N, v.w)) return 0;
+    seg_dots_kernel<0><<<nd, 1024, DOT_SMEM, n2c_stream()>>>(v, j);
+    seg_update_kernel<0><<<nv, VEC_THREADS, 0, n2c_stream()>>>(v, j);
+    seg_dots_kernel<1><<<nd, 1024, DOT_SMEM, n2c_stream()>>>(v, j);
+    seg_update_kernel<1><<<nv, VEC_THREADS, 0, n2c_stream()>>>(v, j);
+    seg_normalize_kernel<<<nv, VEC_THREADS, 0, n2c_stream()>>>(v, j);
+    if (!n2c_check_launch("batched Gram-Schmidt")) return 0;
+    n2c_count_launch(4);
+  }
+  return 1;
+}
+
+static void try_capture(n2d_vie_batch *b, BatchWork *w) {
+  w->tried_graph = true;
+  static thread_local cudaStream_t cap = nullptr;
+  if (!cap && cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) { cap = nullptr; return; }
+  void *user = n2d_get_stream();
+  const unsigned long long before = n2d_launch_count();
+  n2d_set_stream(cap);
+  cudaGraph_t graph = nullptr;
+  int ok = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) ok = enqueue_inner(b, w);
+  const cudaError_t e = cudaStreamEndCapture(cap, &graph);
+  n2d_set_stream(user);
+  if (ok && e == cudaSuccess && graph && cudaGraphInstantiate(&w->inner, graph, 0) == cudaSuccess)
+    w->inner_launches = (unsigned)(n2d_launch_count() - before);
+  else
+    w->inner = nullptr;
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();
+}
+
+extern "C" int n2d_gmres_batch_dev(n2d_vie_batch *b, const double *b_dev, double *x_dev, size_t restart,
+                                   size_t maxit, double rtol, double atol, n2d_gmres_report *reps) {
+  const int K = b->K;
+  for (int q = 0; q < K; ++q) {
+    memset(&reps[q], 0, sizeof(reps[q]));
+    reps[q].status = ST_INVALID;
+    reps[q].residual_norm = reps[q].relative_residual = INFINITY;
+  }
+  if (restart < 1 || maxit < 1) return 0;
+  const int m = (int)std::min<size_t>(std::min<size_t>(restart, maxit), BMAXM);
+  if (restart > (size_t)BMAXM && maxit > (size_t)BMAXM) {
+    n2c_set_error("batched GMRES restarts after at most %d steps", BMAXM);
+    return 0;
+  }
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(seg_dots_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DOT_SMEM);
+    cudaFuncSetAttribute(seg_dots_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DOT_SMEM);
+    configured = true;
+  }
+  BatchWork *w = work_get(b, m);
+  if (!w) {
+    for (int q = 0; q < K; ++q) reps[q].status = ST_ALLOC;
+    return 0;
+  }
+  BView &v = w->v;
+  const double2 *rhs = (const double2 *)b_dev;
+  double2 *x = (double2 *)x_dev;
+  const unsigned nv = (unsigned)b->first_v[K];
+  std::vector<BSys> hs(K);
+  std::vector<double> bnorm(K), target(K), norms(2 * K);
+  std::vector<char> done(K, 0);
+  auto put = [&]() { return n2d_upload(b->sys, hs.data(), K * sizeof(BSys)); };
+  auto get = [&]() { return n2d_download(hs.data(), b->sys, K * sizeof(BSys)); };
+  auto norms_of = [&](const double2 *vec, double *outh) {
+    seg_norm_kernel<<<nv, VEC_THREADS, 0, n2c_stream()>>>(v, vec, v.norms);
+    return n2c_check_launch("batched norm") && n2d_download(outh, v.norms, K * sizeof(double));
+  };
+  memset(hs.data(), 0, K * sizeof(BSys));
+  for (int q = 0; q < K; ++q) {
+    const long long n = b->off[q + 1] - b->off[q];
+    hs[q].status = ST_RUNNING;
+    hs[q].max_iterations = (long long)maxit;
+    hs[q].m = (int)std::min<long long>(m, n);
+  }
+  // ||b|| and ||x|| (finite check) of every system (vie_iterative.c:116-119).
+  if (!put() || !norms_of(rhs, norms.data()) || !norms_of(x, norms.data() + K) || !get()) return 0;
+  for (int q = 0; q < K; ++q) {
+    bnorm[q] = sqrt(norms[q]);
+    target[q] = fmax(atol, rtol * bnorm[q]);
+    hs[q].target = target[q];
+    if (hs[q].rflag || !isfinite(bnorm[q]) || !isfinite(sqrt(norms[K + q])) || !isfinite(target[q])) {
+      reps[q].status = ST_NONFINITE;
+      hs[q].status = ST_NONFINITE;
+      done[q] = 1;
+    }
+  }
+  // True residual r = b - A x (FP64) of the systems still running.
+  auto true_residual = [&]() -> int {
+    for (int q = 0; q < K; ++q) {
+      hs[q].running = !done[q];
+      hs[q].rflag = 0;
+      hs[q].active = 0;
+      if (!done[q]) ++reps[q].operator_applications;
+    }
+    if (!put() || !batch_apply(b, 1, x, v.r)) return 0;
+    seg_residual_kernel<<<nv, VEC_THREADS, 0, n2c_stream()>>>(v, rhs);
+    if (!n2c_check_launch("batched residual") || !norms_of(v.r, norms.data()) || !get()) return 0;
+    for (int q = 0; q < K; ++q) {
+      if (done[q]) continue;
+      reps[q].residual_norm = hs[q].rflag ? NAN : sqrt(norms[q]);
+      reps[q].relative_residual = bnorm[q] > 0 ? reps[q].residual_norm / bnorm[q] : reps[q].residual_norm;
+      if (!isfinite(reps[q].residual_norm)) { reps[q].status = ST_NONFINITE; done[q] = 1; }
+    }
+    return 1;
+  };
+  if (!true_residual()) return 0;
+  for (;;) {
+    int cycling = 0;
+    for (int q = 0; q < K; ++q) {
+      hs[q].active = 0;
+      if (done[q]) continue;
+      const double beta = reps[q].residual_norm;
+      if (beta <= target[q]) { reps[q].status = ST_CONVERGED; done[q] = 1; continue; }
+      if ((long long)reps[q].iterations >= (long long)maxit) { reps[q].status = ST_LIMIT; done[q] = 1; continue; }
+      hs[q].active = 1; hs[q].beta = beta; hs[q].used = 0; hs[q].breakdown = 0; hs[q].flag = 0;
+      hs[q].normalize = 0; hs[q].reorth = 0; hs[q].status = ST_RUNNING;
+      hs[q].iterations = (long long)reps[q].iterations;
+      ++cycling;
+    }
+    if (!cycling) break;
+    for (int q = 0; q < K; ++q) if (done[q]) hs[q].status = reps[q].status;
+    if (!put()) return 0;
+    seg_cycle_start_kernel<<<nv, VEC_THREADS, 0, n2c_stream()>>>(v);
+    if (!n2c_check_launch("batched cycle start")) return 0;
+    if (!w->tried_graph) try_capture(b, w);
+    if (w->inner) {
+      if (cudaGraphLaunch(w->inner, (cudaStream_t)n2d_get_stream()) != cudaSuccess) {
+        n2c_set_error("batched GMRES graph launch failed");
+        return 0;
+      }
+      n2c_count_launch(w->inner_launches);
+    } else if (!enqueue_inner(b, w)) {
+      return 0;
+    }
+    seg_backsolve_kernel<<<(K + 127) / 128, 128, 0, n2c_stream()>>>(v);
+    seg_xupdate_kernel<<<nv, VEC_THREADS, 0, n2c_stream()>>>(v, x);
+    if (!n2c_check_launch("batched solution update") || !get()) return 0;
+    std::vector<char> cycled(K, 0);
+    for (int q = 0; q < K; ++q) {
+      if (done[q]) continue;
+      cycled[q] = 1;
+      reps[q].iterations = (size_t)hs[q].iterations;
+      reps[q].operator_applications += (size_t)hs[q].used;
+      if (hs[q].status != ST_RUNNING) { reps[q].status = hs[q].status; done[q] = 1; }
+    }
+    if (!true_residual()) return 0;
+    for (int q = 0; q < K; ++q) {
+      if (!cycled[q] || done[q]) continue;
+      const double rn = reps[q].residual_norm;
+      if (hs[q].breakdown && rn > target[q]) { reps[q].status = ST_BREAKDOWN; done[q] = 1; continue; }
+      if (rn > target[q] && (long long)reps[q].iterations < (long long)maxit) ++reps[q].restarts;
+    }
+  }
+  int all = 1;
+  for (int q = 0; q < K; ++q) all = all && reps[q].status == ST_CONVERGED;
+  return all;
+}

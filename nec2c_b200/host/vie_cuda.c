@@ -468,3 +468,140 @@ int nec2c_cuda_gmres_hybrid_device(nec2c_cuda_hybrid *h, const void *b, void *x,
   }
   return gmres_common(1, h ? h->dev : NULL, h ? h->c + h->v : 0, b, x, 1, NULL, NULL, options, report);
 }
+
+/* ------------------------------------------------------- batch of plans */
+struct nec2c_cuda_vie_batch {
+  n2d_vie_batch *dev;
+  size_t count, order;
+  nec2c_cuda_vie_plan **plans;
+  size_t *offsets;
+  void *b_dev, *x_dev;   /* staging of the host-vector solve */
+};
+
+static int batch_ready(nec2c_cuda_vie_batch *b)
+{
+  for(size_t q = 0; q < b->count; ++q)
+    if(!nec2c_cuda_plan_device(b->plans[q])) return 0;
+  return 1;
+}
+
+void nec2c_cuda_vie_batch_destroy(nec2c_cuda_vie_batch *b)
+{
+  if(!b) return;
+  n2d_vie_batch_destroy(b->dev);
+  n2d_free(b->b_dev);
+  n2d_free(b->x_dev);
+  free(b->plans);
+  free(b->offsets);
+  free(b);
+}
+
+int nec2c_cuda_vie_batch_create(nec2c_cuda_vie_batch **out, nec2c_cuda_vie_plan *const *plans, size_t count)
+{
+  nec2c_cuda_vie_batch *b;
+  n2d_vie **devs;
+  if(!out) return 0;
+  *out = NULL;
+  if(!plans || count == 0 || count > ((size_t)1 << 20)) { n2c_set_error("batch: bad plan list"); return 0; }
+  b = calloc(1, sizeof(*b));
+  devs = calloc(count, sizeof(*devs));
+  if(!b || !devs) { free(b); free(devs); return 0; }
+  b->count = count;
+  b->plans = calloc(count, sizeof(*b->plans));
+  b->offsets = calloc(count + 1, sizeof(*b->offsets));
+  if(!b->plans || !b->offsets) { free(devs); nec2c_cuda_vie_batch_destroy(b); return 0; }
+  for(size_t q = 0; q < count; ++q) {
+    if(!plans[q]) { n2c_set_error("batch: plan %zu is NULL", q); free(devs); nec2c_cuda_vie_batch_destroy(b); return 0; }
+    b->plans[q] = plans[q];
+    devs[q] = nec2c_cuda_plan_device(plans[q]);
+    if(!devs[q]) { free(devs); nec2c_cuda_vie_batch_destroy(b); return 0; }
+  }
+  if(!n2d_vie_batch_create(&b->dev, devs, (long long)count)) { free(devs); nec2c_cuda_vie_batch_destroy(b); return 0; }
+  free(devs);
+  for(size_t q = 0; q <= count; ++q) b->offsets[q] = (size_t)n2d_vie_batch_offset(b->dev, (long long)q);
+  b->order = b->offsets[count];
+  *out = b;
+  return 1;
+}
+
+size_t nec2c_cuda_vie_batch_order(const nec2c_cuda_vie_batch *b) { return b ? b->order : 0; }
+size_t nec2c_cuda_vie_batch_offset(const nec2c_cuda_vie_batch *b, size_t q)
+{
+  return b && q <= b->count ? b->offsets[q] : 0;
+}
+
+int nec2c_cuda_vie_batch_apply_device(nec2c_cuda_vie_batch *b, const void *x_dev, void *y_dev)
+{
+  if(!b || !x_dev || !y_dev || x_dev == y_dev) return 0;
+  return batch_ready(b) && n2d_vie_batch_apply(b->dev, x_dev, y_dev);
+}
+
+static int batch_options_ok(const nec2c_cuda_gmres_options *o)
+{
+  /* vie_iterative.c:97-103 */
+  return o->restart > 0 && o->maximum_iterations > 0 && isfinite(o->relative_tolerance) &&
+         o->relative_tolerance >= 0 && isfinite(o->absolute_tolerance) && o->absolute_tolerance >= 0 &&
+         !(o->relative_tolerance == 0 && o->absolute_tolerance == 0);
+}
+
+static int batch_solve(nec2c_cuda_vie_batch *b, const void *b_dev, void *x_dev,
+                       const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *reports)
+{
+  nec2c_cuda_gmres_options defaults = {30, 300, 1e-12, 0.0};
+  n2d_gmres_report *r;
+  int ok;
+  for(size_t q = 0; q < b->count; ++q) {
+    memset(&reports[q], 0, sizeof(reports[q]));
+    reports[q].status = ST_INVALID;
+    reports[q].residual_norm = reports[q].relative_residual = INFINITY;
+  }
+  if(!options) options = &defaults;
+  if(!batch_options_ok(options) || b_dev == x_dev) return 0;
+  r = calloc(b->count, sizeof(*r));
+  if(!r) return 0;
+  ok = batch_ready(b) &&
+       n2d_gmres_batch_dev(b->dev, b_dev, x_dev, options->restart, options->maximum_iterations,
+                           options->relative_tolerance, options->absolute_tolerance, r);
+  for(size_t q = 0; q < b->count; ++q) {
+    reports[q].status = r[q].status;
+    reports[q].iterations = r[q].iterations;
+    reports[q].operator_applications = r[q].operator_applications;
+    reports[q].restarts = r[q].restarts;
+    reports[q].residual_norm = r[q].residual_norm;
+    reports[q].relative_residual = r[q].relative_residual;
+  }
+  free(r);
+  return ok;
+}
+
+int nec2c_cuda_gmres_batch_device(nec2c_cuda_vie_batch *b, const void *b_dev, void *x_dev,
+                                  const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *reports)
+{
+  if(!b || !b_dev || !x_dev || !reports) return 0;
+  return batch_solve(b, b_dev, x_dev, options, reports);
+}
+
+int nec2c_cuda_gmres_batch(nec2c_cuda_vie_batch *b, const nec2c_cuda_complex *const *bv,
+                           nec2c_cuda_complex *const *xv, const nec2c_cuda_gmres_options *options,
+                           nec2c_cuda_gmres_report *reports)
+{
+  const size_t cpx = sizeof(nec2c_cuda_complex);
+  int ok = 1;
+  if(!b || !bv || !xv || !reports) return 0;
+  for(size_t q = 0; q < b->count; ++q) if(!bv[q] || !xv[q]) return 0;
+  if(!b->b_dev) b->b_dev = n2d_alloc(b->order * cpx);
+  if(!b->x_dev) b->x_dev = n2d_alloc(b->order * cpx);
+  if(!b->b_dev || !b->x_dev) return 0;
+  for(size_t q = 0; q < b->count && ok; ++q) {
+    const size_t off = b->offsets[q] * cpx, bytes = (b->offsets[q + 1] - b->offsets[q]) * cpx;
+    ok = n2d_upload((char *)b->b_dev + off, bv[q], bytes) && n2d_upload((char *)b->x_dev + off, xv[q], bytes);
+  }
+  if(!ok) return 0;
+  ok = batch_solve(b, b->b_dev, b->x_dev, options, reports);
+  /* x is copied back even when a solve fails (vie_iterative.h:51-53). */
+  for(size_t q = 0; q < b->count; ++q) {
+    const size_t off = b->offsets[q] * cpx, bytes = (b->offsets[q + 1] - b->offsets[q]) * cpx;
+    if(!n2d_download(xv[q], (char *)b->x_dev + off, bytes)) ok = 0;
+  }
+  return ok;
+}
