@@ -49,11 +49,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", choices=["matvec", "solve", "lu", "serving"],
+    ap.add_argument("--only", choices=["matvec", "solve", "lu", "serving", "volume_batch"],
                     help="profiling driver: build the plans, run --steps FP32 and FP64 products "
                          "(matvec) or --steps mixed solves (solve), or factor the config-1 shaped "
-                         "matrix --steps times in each LU form (lu), or run the serving stream "
-                         "(serving); print timings and exit")
+                         "matrix --steps times in each LU form (lu), run the serving stream "
+                         "(serving) or the config-3 shaped volume batch (volume_batch); print "
+                         "timings and exit")
     return ap.parse_args()
 
 
@@ -312,6 +313,9 @@ def run_ours(args, rank, world, local_rank):
     if args.only == "serving":
         print(json.dumps({"profile": "serving", "serving_c4": serving_bench(nb, torch)}))
         return 0
+    if args.only == "volume_batch":
+        print(json.dumps({"profile": "volume_batch", "batched_volume_c3": volume_batch_bench(nb, torch, stream)}))
+        return 0
     w = workload()
     table = near_table()
 
@@ -438,6 +442,8 @@ def run_ours(args, rank, world, local_rank):
     dense = dense_bench(nb, torch, stream)
     # Config-3 shaped wire blocks, ragged batch in one launch.
     batched = batched_bench(nb, torch)
+    # Config-3 shaped volume sweep, ragged batch of plans.
+    volume_batch = volume_batch_bench(nb, torch, stream)
     # Config-4 shaped serving stream (bounded), both forms.
     serving = serving_bench(nb, torch) if world == 1 else None
     lib.nec2c_cuda_set_stream(C.c_void_p(stream.cuda_stream))
@@ -468,6 +474,7 @@ def run_ours(args, rank, world, local_rank):
         "fft_schedule": schedule,
         "dense_lu_c1": dense,
         "batched_wire_blocks_c3": batched,
+        "batched_volume_c3": volume_batch,
         "serving_c4": serving,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
@@ -649,6 +656,102 @@ def batched_bench(nb, torch):
             "one_launch": {"ms": 1e3 * tb, "solves_per_s": len(sizes) / tb},
             "one_call_each": {"ms": 1e3 * ts, "solves_per_s": len(sizes) / ts},
             "max_rel_diff": err, "note": "host buffers through the C ABI, wall clock"}
+
+
+def volume_batch_bench(nb, torch, stream):
+    """Config-3 shaped volume sweep in one batch: the config-0 cube (16^3 cells,
+    0.2 lambda at 300 MHz, eps_r = 4 - 0.1j) at 128 frequencies uniform in
+    100-400 MHz, and 64 seeded random cubes of 8^3-32^3 cells (0.2 lambda at
+    300 MHz, eps_r ~ U[2,8], tan d = 0.05), x-polarised plane-wave excitation,
+    GMRES(30) to rtol 1e-6.  The far pairs of every plan are quadratured on the
+    GPU at its own frequency; the 13 near-pair tensors (the caller's certified
+    quadrature) come from the golden table of the nearest lattice, reused at
+    every frequency.  Timed: the whole batch in one nec2c_cuda_gmres_batch_device
+    call (FP32 transforms, and the plain FP64 form), against one device GMRES
+    call per plan (both forms), CUDA events on the launching stream."""
+    tabs = near_tables_all()
+    lam = C0 / 300e6
+    rng = np.random.default_rng(7)
+    specs = [(16, 2 * math.pi * f / C0, "c0", 4 - 0.1j) for f in np.linspace(100e6, 400e6, 128)]
+    for n in rng.choice([8, 12, 16, 24, 32], 64):
+        specs.append((int(n), 2 * math.pi / lam, "c0" if n <= 16 else "c3_32", rng.uniform(2, 8) * (1 - 0.05j)))
+    lib = nb.load()
+
+    def build(mixed):
+        plans, rhs = [], []
+        for n, k, tab, eps in specs:
+            h = 0.2 * lam / n
+            g = np.arange(n)
+            xyz = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1).astype(np.uintp)
+            p = nb.VolumePlan((n, n, n), xyz, h, k, eps, tabs[tab][2], mixed=mixed)
+            b = np.zeros(3 * n ** 3, dtype=np.complex128)
+            z = xyz[2::3].astype(np.float64)
+            b[0::3] = 2 * np.exp(-1j * k * h * (z + 0.5)) * math.sin(k * h / 2) / (k * h / 2)
+            plans.append(p)
+            rhs.append(b)
+        return plans, rhs
+
+    t0 = time.perf_counter()
+    plans_m, rhs = build(True)
+    build_s = time.perf_counter() - t0
+    plans_d, _ = build(False)
+    opts = nb.GmresOptions(30, 3000, 1e-6, 0.0)
+    out = {"systems": len(specs), "lattices": "128 x 16^3 (100-400 MHz) + 64 random in {8,12,16,24,32}^3",
+           "unknowns": int(sum(p.n for p in plans_m)), "plan_build_s_fp32": build_s}
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), r
+
+    sols = {}
+    for form, plans in (("fp32_transforms", plans_m), ("fp64", plans_d)):
+        batch = nb.VolumeBatch(plans)
+        b_dev = torch.from_numpy(np.concatenate(rhs)).cuda()
+        x_dev = torch.zeros_like(b_dev)
+        reps = (nb.GmresReport * len(plans))()
+
+        def solve_batch():
+            x_dev.zero_()
+            return lib.nec2c_cuda_gmres_batch_device(batch.h, C.c_void_p(b_dev.data_ptr()),
+                                                     C.c_void_p(x_dev.data_ptr()), C.byref(opts), reps)
+        timed(solve_batch)
+        ms, ok = min((timed(solve_batch) for _ in range(2)), key=lambda t: t[0])
+        if not ok:
+            raise RuntimeError("batched volume solve failed: " + nb.last_error())
+        sols[form] = x_dev.cpu().numpy()
+        its = [r.iterations for r in reps]
+        batch.close()
+
+        def one_by_one():
+            ok = 1
+            for p, b in zip(plans, bs):
+                x.zero_()
+                ok &= lib.nec2c_cuda_gmres_plan_device(p.h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()),
+                                                       C.byref(opts), C.byref(nb.GmresReport()))
+            return ok
+        bs = [torch.from_numpy(b).cuda() for b in rhs]
+        x = torch.zeros(max(b.numel() for b in bs), dtype=torch.complex128, device="cuda")
+        timed(one_by_one)
+        ms1, ok1 = timed(one_by_one)
+        if not ok1:
+            raise RuntimeError("per-plan volume solve failed: " + nb.last_error())
+        out[form] = {"one_batch": {"ms": ms, "solves_per_s": 1e3 * len(plans) / ms},
+                     "one_call_per_plan": {"ms": ms1, "solves_per_s": 1e3 * len(plans) / ms1},
+                     "iterations": {"min": int(min(its)), "max": int(max(its)), "mean": float(np.mean(its))}}
+        for p in plans:
+            p.close()
+    off = np.cumsum([0] + [b.size for b in rhs])
+    out["max_rel_err_fp32_transforms_vs_fp64"] = max(
+        float(np.linalg.norm(sols["fp32_transforms"][a:b] - sols["fp64"][a:b]) / np.linalg.norm(sols["fp64"][a:b]))
+        for a, b in zip(off[:-1], off[1:]))
+    out["batch_fp32_vs_plain_fp64_one_call_per_plan"] = (
+        out["fp32_transforms"]["one_batch"]["solves_per_s"] / out["fp64"]["one_call_per_plan"]["solves_per_s"])
+    return out
 
 
 # Config-4 shaped serving stream (bounded): 60% wire-only dense MoM solves of
