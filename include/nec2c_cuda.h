@@ -170,7 +170,8 @@ typedef struct nec2c_cuda_vie_batch nec2c_cuda_vie_batch;
    axes up to 128, all with the same transform precision, each at most once)
    solved together: every FFT pass of a GMRES step is one launch over all the
    plans, every Gram-Schmidt sweep one launch over all the systems, and the
-   steps of a restart cycle one CUDA graph.  The reference solves such a sweep
+   steps of a restart cycle run as CUDA graphs of five steps, the cycle ending
+   after the graph in which the last system stopped.  The reference solves such a sweep
    one vie_gmres at a time in its frequency workers (main.c:586-760); there is
    no counterpart function.  The plans stay the caller's, must outlive the
    batch and must not be used elsewhere while a batched call runs;

@@ -8,7 +8,9 @@
 //   - every Gram-Schmidt sweep, update and norm is one launch over all
 //     systems' unknowns: a CTA covers a fixed range of one system, and the
 //     last CTA of each system finishes its reduction in a fixed order;
-//   - the m Arnoldi steps of a restart cycle are one captured CUDA graph.
+//   - the Arnoldi steps of a restart cycle are captured CUDA graphs of five
+//     steps each; between graphs the host reads how many systems are still
+//     in the cycle and ends it when none is.
 // Each system keeps its own GMRES state (Hessenberg matrix, rotations,
 // status) with vie_gmres's per-system semantics (vie_iterative.c:90-200);
 // a system that has converged or stopped is gated off and costs nothing.
@@ -119,6 +121,9 @@ template <typename C, int MODE>
 __global__ void __launch_bounds__(256, MODE <= 1 ? 1 : 3)
     batch_pass_kernel(const BatchDesc<C> *desc, const long long *first, int count, const double2 *x, double2 *y) {
   const int q = find_seg(first, count, blockIdx.x);
+  // A stopped system's tiles leave before its arguments are read.
+  const int *gate = desc[q].a.gate;
+  if (gate && *(volatile const int *)gate == 0) return;
   PassArgs<C> a = desc[q].a;
   if (MODE >= 7) {
     a.cx = x + desc[q].off;
@@ -395,6 +400,21 @@ __global__ void __launch_bounds__(VEC_THREADS) seg_normalize_kernel(BView v, int
     vn[i] = make_double2(v.w[i].x / inv, v.w[i].y / inv);
 }
 
+// *out = number of systems still in their cycle.
+__global__ void count_active_kernel(BView v, int *out) {
+  int c = 0;
+  for (int q = threadIdx.x; q < v.K; q += blockDim.x) c += v.sys[q].active != 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  __shared__ int red[8];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    *out = t;
+  }
+}
+
 // y = H^{-1} g of every running system (vie_iterative.c:179-186), one thread
 // per system.
 __global__ void seg_backsolve_kernel(BView v) {
@@ -448,11 +468,18 @@ struct PassSet {
   bool fp32 = false;
 };
 
+// Arnoldi steps per captured graph: after each chunk the host reads how many
+// systems are still in their cycle and ends the cycle when none is, so the
+// steps after the last system's stop test are not launched.
+constexpr int CHUNK = 5;
+constexpr int MAX_CHUNKS = (BMAXM + CHUNK - 1) / CHUNK;
+
 struct BatchWork {
   int m = 0;
   BView v;
-  cudaGraphExec_t inner = nullptr;
-  unsigned inner_launches = 0;
+  int *active_count = nullptr;   // device: systems still in the cycle
+  cudaGraphExec_t chunk[MAX_CHUNKS] = {};
+  unsigned chunk_launches[MAX_CHUNKS] = {};
   bool tried_graph = false;
 };
 
@@ -470,9 +497,10 @@ struct n2d_vie_batch {
 
 static void work_free(BatchWork *w) {
   if (!w) return;
-  if (w->inner) cudaGraphExecDestroy(w->inner);
+  for (cudaGraphExec_t &g : w->chunk)
+    if (g) cudaGraphExecDestroy(g);
   BView &v = w->v;
-  void *bufs[] = {v.V, v.w, v.r, v.H, v.g, v.sn, v.y, v.hp, v.cs, v.parts_d, v.parts_v, v.norms};
+  void *bufs[] = {v.V, v.w, v.r, v.H, v.g, v.sn, v.y, v.hp, v.cs, v.parts_d, v.parts_v, v.norms, w->active_count};
   for (void *q : bufs) n2d_free(q);
   delete w;
 }
@@ -649,8 +677,9 @@ static BatchWork *work_get(n2d_vie_batch *b, int m) {
   v.parts_d = (double2 *)n2d_alloc(b->first_d[K] * BMAXM * sizeof(double2));
   v.parts_v = (double *)n2d_alloc(b->first_v[K] * sizeof(double));
   v.norms = (double *)n2d_alloc(2 * K * sizeof(double));
+  w->active_count = (int *)n2d_alloc(sizeof(int));
   if (!v.V || !v.w || !v.r || !v.H || !v.g || !v.sn || !v.y || !v.hp || !v.cs || !v.parts_d || !v.parts_v ||
-      !v.norms) {
+      !v.norms || !w->active_count) {
     work_free(w);
     return nullptr;
   }
@@ -658,11 +687,12 @@ static BatchWork *work_get(n2d_vie_batch *b, int m) {
   return w;
 }
 
-// The m gated Arnoldi steps of a cycle on the current stream.
-static int enqueue_inner(n2d_vie_batch *b, BatchWork *w) {
+// Steps [j0, j1) of a cycle, gated per system, then the count of systems
+// still in the cycle, on the current stream.
+static int enqueue_steps(n2d_vie_batch *b, BatchWork *w, int j0, int j1) {
   BView &v = w->v;
   const unsigned nd = (unsigned)b->first_d[b->K], nv = (unsigned)b->first_v[b->K];
-  for (int j = 0; j < w->m; ++j) {
+  for (int j = j0; j < j1; ++j) {
     if (!batch_apply(b, 0, v.V + (long long)j * v.N, v.w)) return 0;
     seg_dots_kernel<0><<<nd, 1024, DOT_SMEM, n2c_stream()>>>(v, j);
     seg_update_kernel<0><<<nv, VEC_THREADS, 0, n2c_stream()>>>(v, j);
@@ -672,27 +702,32 @@ static int enqueue_inner(n2d_vie_batch *b, BatchWork *w) {
     if (!n2c_check_launch("batched Gram-Schmidt")) return 0;
     n2c_count_launch(4);
   }
-  return 1;
+  count_active_kernel<<<1, 256, 0, n2c_stream()>>>(v, w->active_count);
+  return n2c_check_launch("active count");
 }
 
+// Captures each chunk of steps once into a graph (launched on the caller's
+// stream); a chunk that cannot be captured is launched directly.
 static void try_capture(n2d_vie_batch *b, BatchWork *w) {
   w->tried_graph = true;
   static thread_local cudaStream_t cap = nullptr;
   if (!cap && cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) { cap = nullptr; return; }
   void *user = n2d_get_stream();
-  const unsigned long long before = n2d_launch_count();
-  n2d_set_stream(cap);
-  cudaGraph_t graph = nullptr;
-  int ok = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-  if (ok) ok = enqueue_inner(b, w);
-  const cudaError_t e = cudaStreamEndCapture(cap, &graph);
-  n2d_set_stream(user);
-  if (ok && e == cudaSuccess && graph && cudaGraphInstantiate(&w->inner, graph, 0) == cudaSuccess)
-    w->inner_launches = (unsigned)(n2d_launch_count() - before);
-  else
-    w->inner = nullptr;
-  if (graph) cudaGraphDestroy(graph);
-  cudaGetLastError();
+  for (int c = 0; c * CHUNK < w->m; ++c) {
+    const unsigned long long before = n2d_launch_count();
+    n2d_set_stream(cap);
+    cudaGraph_t graph = nullptr;
+    int ok = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) ok = enqueue_steps(b, w, c * CHUNK, std::min(w->m, (c + 1) * CHUNK));
+    const cudaError_t e = cudaStreamEndCapture(cap, &graph);
+    n2d_set_stream(user);
+    if (ok && e == cudaSuccess && graph && cudaGraphInstantiate(&w->chunk[c], graph, 0) == cudaSuccess)
+      w->chunk_launches[c] = (unsigned)(n2d_launch_count() - before);
+    else
+      w->chunk[c] = nullptr;
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+  }
 }
 
 extern "C" int n2d_gmres_batch_dev(n2d_vie_batch *b, const double *b_dev, double *x_dev, size_t restart,
@@ -791,14 +826,19 @@ extern "C" int n2d_gmres_batch_dev(n2d_vie_batch *b, const double *b_dev, double
     seg_cycle_start_kernel<<<nv, VEC_THREADS, 0, n2c_stream()>>>(v);
     if (!n2c_check_launch("batched cycle start")) return 0;
     if (!w->tried_graph) try_capture(b, w);
-    if (w->inner) {
-      if (cudaGraphLaunch(w->inner, (cudaStream_t)n2d_get_stream()) != cudaSuccess) {
-        n2c_set_error("batched GMRES graph launch failed");
+    for (int c = 0; c * CHUNK < w->m; ++c) {
+      if (w->chunk[c]) {
+        if (cudaGraphLaunch(w->chunk[c], (cudaStream_t)n2d_get_stream()) != cudaSuccess) {
+          n2c_set_error("batched GMRES graph launch failed");
+          return 0;
+        }
+        n2c_count_launch(w->chunk_launches[c]);
+      } else if (!enqueue_steps(b, w, c * CHUNK, std::min(w->m, (c + 1) * CHUNK))) {
         return 0;
       }
-      n2c_count_launch(w->inner_launches);
-    } else if (!enqueue_inner(b, w)) {
-      return 0;
+      int still = 0;
+      if (!n2d_download(&still, w->active_count, sizeof(int))) return 0;
+      if (!still) break;
     }
     seg_backsolve_kernel<<<(K + 127) / 128, 128, 0, n2c_stream()>>>(v);
     seg_xupdate_kernel<<<nv, VEC_THREADS, 0, n2c_stream()>>>(v, x);
