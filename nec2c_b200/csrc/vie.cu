@@ -979,12 +979,29 @@ extern "C" int n2d_vie_precondition(n2d_vie *p, const double *x, double *y) {
   return n2c_check_launch("precondition");
 }
 
+// Tile height of pass `pass` in a batch.  A batch fills the GPU with the
+// tiles of many plans, so a tile is made as large as a single plan's tile may
+// be at most: about 4096 complex elements per component in the strided y
+// passes and 2048 in the x product pass (within 48 KB of shared memory), and
+// the default z tile of 56 KB (whole lattice columns).  Small plans then
+// give each thread several butterflies instead of leaving threads idle.
+static int batch_height(const n2d_vie *p, int pass, size_t elem) {
+  const int L = pass_length(p, pass);
+  if (pass == 0 || pass == 4) return zlines_per_tile(L, elem, 3);
+  const size_t ncomp = pass == 2 ? 3 : 1;
+  const long long target = pass == 2 ? 2048 : 4096;
+  int nl = 1;
+  while ((long long)nl * 2 * L <= target && (size_t)nl * 2 * L * ncomp * elem <= 48 * 1024) nl *= 2;
+  return nl;
+}
+
 template <typename C>
 int n2c_vie_pass_plans(n2d_vie *p, int precondition, double *norm, int *flag, PassArgs<C> args[5], int mode[5],
                        int L[5], size_t smem[5], long long tiles[5]) {
   for (int i = 0; i < N2D_VIE_PASSES; ++i) {
     PassPlan<C> pp;
-    if (!pass_plan<C>(p, i, n2d_pass_choice{0, 0}, nullptr, nullptr, precondition, norm, flag, &pp)) return 0;
+    const n2d_pass_choice ch = {batch_height(p, i, sizeof(C)), 0};
+    if (!pass_plan<C>(p, i, ch, nullptr, nullptr, precondition, norm, flag, &pp)) return 0;
     args[i] = pp.a;
     mode[i] = pp.mode;
     L[i] = pp.L;

@@ -4,8 +4,9 @@
 #include "fft_engine.cuh"
 #include "vie_internal.cuh"
 
-// The five matvec passes of plan p with the heuristic tile heights and the
-// default radix split: arguments (cell vectors left unset: the batched
+// The five matvec passes of plan p with the batch's tile heights (large
+// tiles: the batch fills the GPU with many plans) and the default radix
+// split: arguments (cell vectors left unset: the batched
 // launch points them into the batch vectors), kernel mode, line length,
 // dynamic shared memory and tiles.  precondition, norm and flag as in
 // n2d_vie_apply.  Returns 0 with the error set when a pass cannot be

@@ -1,9 +1,9 @@
 """Ragged batch of volume plans (nec2c_cuda_vie_batch_*, nec2c_cuda_gmres_batch).
 
-The batched product runs the same tile bodies as a single plan's product,
-inlined into other kernels (the compiler may fuse a multiply-add differently),
-so with the plans on the heuristic schedule each plan's slice of the batched
-product equals its own product to rounding (1e-14 of the largest entry in
+The batched product runs the same tile bodies as a single plan's product, on
+taller tiles and inlined into other kernels (the compiler may fuse a
+multiply-add differently), so with the plans on the default radix split each
+plan's slice of the batched product equals its own product to rounding (1e-14 of the largest entry in
 FP64, 1e-6 with FP32 transforms), and the FP64 form matches the oracle to
 1e-12 relative to the largest entry.  Batched GMRES
 solves each system with vie_gmres's per-system semantics: every system's
@@ -58,7 +58,7 @@ def test_batched_product_equals_each_plan(near_tables, mixed):
     import torch
     plans, oracles = make(near_tables, mixed)
     for p in plans:
-        p.tune(0)          # heuristic schedule: the batched passes use the same tiles
+        p.tune(0)          # default radix split, as in the batched passes
     batch = nb.VolumeBatch(plans)
     assert batch.order == sum(p.n for p in plans)
     rng = np.random.default_rng(11)
