@@ -49,6 +49,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fft-schedule", default=None,
+                    help="JSON file of the c2 plans' FFT pass schedules: written by the first run "
+                         "that names it, pinned by later runs (a run under ncu would otherwise "
+                         "tune on serialised, slowed launches)")
     ap.add_argument("--only", choices=["matvec", "solve", "lu", "serving", "volume_batch"],
                     help="profiling driver: build the plans, run --steps FP32 and FP64 products "
                          "(matvec) or --steps mixed solves (solve), or factor the config-1 shaped "
@@ -298,6 +302,23 @@ def replica_rate(world, steps, total_ms):
 
 
 # ------------------------------------------------------------------ our arm
+def pin_schedules(path, nb, plan_m, plan_d):
+    """Saves the tuned pass schedules of the c2 plans to path, or pins the ones
+    saved there by an earlier run of the same command."""
+    if not path:
+        return
+    plans = {"mixed_fp32": (plan_m, False), "mixed_fp64": (plan_m, True), "plain_fp64": (plan_d, True)}
+    if os.path.exists(path):
+        with open(path) as f:
+            saved = json.load(f)
+        for key, (plan, fp64) in plans.items():
+            if not plan.set_schedule([tuple(e) for e in saved[key]], fp64=fp64):
+                raise RuntimeError("cannot pin the saved schedule: " + nb.last_error())
+        return
+    with open(path, "w") as f:
+        json.dump({key: plan.schedule(fp64=fp64)[1] for key, (plan, fp64) in plans.items()}, f)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import nec2c_b200 as nb
@@ -330,6 +351,7 @@ def run_ours(args, rank, world, local_rank):
 
     plan_m, build_s = make_plan(True)
     plan_d, _ = make_plan(False)
+    pin_schedules(args.fft_schedule, nb, plan_m, plan_d)
     n = plan_m.n
     if args.only:
         return profile_driver(args, lib, nb, torch, stream, plan_m, plan_d, w)
