@@ -177,9 +177,15 @@ typedef struct nec2c_cuda_vie_batch nec2c_cuda_vie_batch;
    batch and must not be used elsewhere while a batched call runs;
    permittivity changes made to them are picked up by the next call. */
 int nec2c_cuda_vie_batch_create(nec2c_cuda_vie_batch **out, nec2c_cuda_vie_plan *const *plans, size_t count);
+/* The same for hybrid conductor + volume systems (dielectric_fft.c: wire
+   segments beside a dielectric body, each with its volume plan and its blocks
+   uploaded): the conductor and cross rows of all systems are one launch each
+   as well.  A system's vector is its conductor unknowns, then its volume
+   unknowns, as nec2c_cuda_hybrid_apply orders them. */
+int nec2c_cuda_hybrid_batch_create(nec2c_cuda_vie_batch **out, nec2c_cuda_hybrid *const *systems, size_t count);
 void nec2c_cuda_vie_batch_destroy(nec2c_cuda_vie_batch *batch);
-/* Unknowns of the batch (sum of 3 x cells); plan q's entries start at
-   nec2c_cuda_vie_batch_offset(batch, q). */
+/* Unknowns of the batch (sum of the systems' orders); system q's entries
+   start at nec2c_cuda_vie_batch_offset(batch, q). */
 size_t nec2c_cuda_vie_batch_order(const nec2c_cuda_vie_batch *batch);
 size_t nec2c_cuda_vie_batch_offset(const nec2c_cuda_vie_batch *batch, size_t plan);
 /* y = A x of every plan (vie_fft.c:239-263 per plan) on device vectors of the
@@ -195,7 +201,7 @@ int nec2c_cuda_vie_batch_apply_device(nec2c_cuda_vie_batch *batch, const void *x
    every system converged. */
 int nec2c_cuda_gmres_batch_device(nec2c_cuda_vie_batch *batch, const void *b_dev, void *x_dev,
                                   const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *reports);
-/* The same with host vectors: b[q] and x[q] hold 3 x cells of plan q. */
+/* The same with host vectors: b[q] and x[q] hold the order of system q. */
 int nec2c_cuda_gmres_batch(nec2c_cuda_vie_batch *batch, const nec2c_cuda_complex *const *b,
                            nec2c_cuda_complex *const *x, const nec2c_cuda_gmres_options *options,
                            nec2c_cuda_gmres_report *reports);

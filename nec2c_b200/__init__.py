@@ -84,6 +84,7 @@ def load():
         "nec2c_cuda_vie_fft_set_schedule": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
         "nec2c_cuda_vie_batch_create": (i, [C.POINTER(vp), C.POINTER(vp), sz]),
         "nec2c_cuda_vie_batch_destroy": (None, [vp]),
+        "nec2c_cuda_hybrid_batch_create": (i, [C.POINTER(vp), C.POINTER(vp), sz]),
         "nec2c_cuda_vie_batch_order": (sz, [vp]),
         "nec2c_cuda_vie_batch_offset": (sz, [vp, sz]),
         "nec2c_cuda_vie_batch_apply_device": (i, [vp, vp, vp]),
@@ -254,14 +255,16 @@ def _gmres(fn, handle, b, x0, restart, maxit, rtol, atol):
 class VolumeBatch:
     """Ragged batch of VolumePlans solved together (nec2c_cuda_vie_batch_*)."""
 
-    def __init__(self, plans):
-        self.plans = list(plans)      # the plans must outlive the batch
+    def __init__(self, plans=None, hybrids=None):
+        """A batch of VolumePlans, or (hybrids=) of HybridSystems."""
+        self.plans = list(plans if hybrids is None else hybrids)   # must outlive the batch
         lib = load()
         arr = (C.c_void_p * len(self.plans))(*[p.h.value for p in self.plans])
         self.h = C.c_void_p()
-        if not lib.nec2c_cuda_vie_batch_create(C.byref(self.h), arr, len(self.plans)):
+        create = lib.nec2c_cuda_vie_batch_create if hybrids is None else lib.nec2c_cuda_hybrid_batch_create
+        if not create(C.byref(self.h), arr, len(self.plans)):
             self.h = None
-            raise RuntimeError("nec2c_cuda_vie_batch_create failed: " + last_error())
+            raise RuntimeError("batch create failed: " + last_error())
         self.order = lib.nec2c_cuda_vie_batch_order(self.h)
         self.offsets = [lib.nec2c_cuda_vie_batch_offset(self.h, q) for q in range(len(self.plans) + 1)]
 

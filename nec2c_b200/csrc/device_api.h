@@ -134,6 +134,9 @@ typedef struct n2d_vie_batch n2d_vie_batch;
 /* Plans with the same transform precision, padded axes <= 128, each at most
    once; their permittivities must have been uploaded (self terms set). */
 int n2d_vie_batch_create(n2d_vie_batch **out, n2d_vie *const *plans, long long count);
+/* Hybrid conductor + volume systems (each with a volume plan, blocks
+   uploaded) batched the same way. */
+int n2d_hybrid_batch_create(n2d_vie_batch **out, n2d_hybrid *const *systems, long long count);
 void n2d_vie_batch_destroy(n2d_vie_batch *b);
 /* Unknowns of the batch and the offset of plan q's vector in it. */
 long long n2d_vie_batch_order(const n2d_vie_batch *b);

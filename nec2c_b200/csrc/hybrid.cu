@@ -159,6 +159,8 @@ int n2c_hybrid_precondition_ok(const n2d_hybrid *h) { return h->precondition_ok;
 extern "C" int n2d_hybrid_precondition_ok(const n2d_hybrid *h) { return h->precondition_ok; }
 const double2 *n2c_hybrid_pdiag(const n2d_hybrid *h) { return h->pdiag; }
 n2d_vie *n2c_hybrid_volume(const n2d_hybrid *h) { return h->vol; }
+const double2 *n2c_hybrid_blocks(const n2d_hybrid *h) { return h->blocks; }
+long long n2c_hybrid_conductors(const n2d_hybrid *h) { return h->c; }
 
 extern "C" int n2d_hybrid_apply(n2d_hybrid *h, const double *x, double *y, int precondition_input,
                                 double *norm, int *flag, int full_precision) {

@@ -18,8 +18,11 @@
 // tenfold cancellation for plans with FP32 transforms and always for FP64
 // plans (CGS2, as stable as the two MGS passes of vie_iterative.c).
 //
-// The batch's vectors are the plans' cell vectors (3 x cells each)
-// concatenated in plan order.
+// A system is a volume plan or a hybrid conductor + volume system [C B; D V]
+// of dielectric_fft.c:41-83 (wire segments beside a dielectric body): its
+// conductor rows and cross rows are one launch each over all systems too.
+// The batch's vectors are the systems' vectors (conductor unknowns, then 3 x
+// cells) concatenated in system order.
 #include <float.h>
 #include <math.h>
 #include <string.h>
@@ -32,6 +35,12 @@
 #include "vie_internal.cuh"
 
 using namespace n2c;
+
+n2d_vie *n2c_hybrid_volume(const n2d_hybrid *h);
+const double2 *n2c_hybrid_pdiag(const n2d_hybrid *h);
+const double2 *n2c_hybrid_blocks(const n2d_hybrid *h);
+long long n2c_hybrid_conductors(const n2d_hybrid *h);
+int n2c_hybrid_precondition_ok(const n2d_hybrid *h);
 
 namespace {
 
@@ -52,6 +61,13 @@ template <typename C> struct BatchDesc {
   PassArgs<C> a;
   long long off;   // first element of the plan's cell vector in the batch vectors
   int L;           // line length of the pass
+};
+
+// Conductor blocks of a hybrid system: the c rows [C|B] (c x n) then the
+// v x c cross block D, row-major (n = c + v); c == 0 for a volume plan.
+struct BHyb {
+  const double2 *blocks;
+  long long c, n;
 };
 
 // Per-system GMRES state (device).
@@ -400,6 +416,81 @@ __global__ void __launch_bounds__(VEC_THREADS) seg_normalize_kernel(BView v, int
     vn[i] = make_double2(v.w[i].x / inv, v.w[i].y / inv);
 }
 
+// Gate of a kernel run for descriptor set `set` (0 Arnoldi, 1 residual, 2 plain).
+__device__ __forceinline__ bool sys_gated(const BSys *s, int set) {
+  return set == 0 ? !s->active : set == 1 ? !s->running : false;
+}
+
+// One CTA per conductor row of every hybrid system: y_i = sum_j [C|B]_ij z_j,
+// z = x or x ./ pdiag (dielectric_fft.c:54-66).
+__global__ void __launch_bounds__(256) seg_conductor_kernel(BView v, const BHyb *hyb, const long long *crow,
+                                                            const double2 *x, double2 *y, int set) {
+  const int q = find_seg(crow, v.K, blockIdx.x);
+  if (sys_gated(v.sys + q, set)) return;
+  const BHyb hb = hyb[q];
+  const long long i = (long long)blockIdx.x - crow[q];
+  const double2 *row = hb.blocks + i * hb.n, *xq = x + v.off[q], *pd = set == 0 ? v.diag[q] : nullptr;
+  double2 acc = make_double2(0, 0);
+  for (long long j = threadIdx.x; j < hb.n; j += blockDim.x) {
+    double2 z = xq[j];
+    if (pd) z = cdiv(z, pd[j]);
+    acc = cadd(acc, cmul(row[j], z));
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) y[v.off[q] + i] = acc;
+}
+
+// One warp per volume row of every hybrid system: y_{c+i} += sum_j D_ij z_j
+// over its conductor unknowns (dielectric_fft.c:67-74).
+__global__ void seg_cross_kernel(BView v, const BHyb *hyb, const long long *xrow, long long rows,
+                                 const double2 *x, double2 *y, int set) {
+  const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= rows) return;
+  const int q = find_seg(xrow, v.K, warp);
+  if (sys_gated(v.sys + q, set)) return;
+  const BHyb hb = hyb[q];
+  const long long i = warp - xrow[q];
+  const double2 *row = hb.blocks + hb.c * hb.n + i * hb.c, *xq = x + v.off[q];
+  const double2 *pd = set == 0 ? v.diag[q] : nullptr;
+  double2 acc = make_double2(0, 0);
+  for (long long j = lane; j < hb.c; j += 32) {
+    double2 z = xq[j];
+    if (pd) z = cdiv(z, pd[j]);
+    acc = cadd(acc, cmul(row[j], z));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+  }
+  if (lane == 0) y[v.off[q] + hb.c + i] = cadd(y[v.off[q] + hb.c + i], acc);
+}
+
+// ||w||^2 of every active system into before_sq (batches with hybrid
+// systems, whose conductor rows come after the volume epilogue); a
+// non-finite entry raises the system's flag.
+__global__ void __launch_bounds__(VEC_THREADS) seg_wnorm_kernel(BView v) {
+  const VecCta c = vec_cta(v);
+  BSys *s = v.sys + c.q;
+  if (!s->active) return;
+  double sq = 0;
+  bool bad = false;
+  for (long long i = c.lo + threadIdx.x; i < c.hi; i += VEC_THREADS) {
+    const double2 wi = v.w[i];
+    sq += wi.x * wi.x + wi.y * wi.y;
+    bad |= !finite2(wi);
+  }
+  if (bad) s->flag = 1;
+  const double2 bs = block_sum(make_double2(sq, 0));
+  if (threadIdx.x == 0) v.parts_v[blockIdx.x] = bs.x;
+  if (!last_of(&s->ticket, (unsigned)c.nctas)) return;
+  const double tot = sum_parts_v(v, c.q);
+  if (threadIdx.x == 0) {
+    s->before_sq = tot;
+    s->ticket = 0;
+  }
+}
+
 // *out = number of systems still in their cycle.
 __global__ void count_active_kernel(BView v, int *out) {
   int c = 0;
@@ -487,6 +578,11 @@ struct n2d_vie_batch {
   int K = 0, fp32 = 0;
   long long N = 0;
   std::vector<n2d_vie *> plans;
+  std::vector<n2d_hybrid *> hybrids;          // null for a volume plan
+  std::vector<long long> cond, crow, xrow;    // conductor unknowns; row prefixes
+  bool any_hybrid = false;
+  BHyb *hyb_dev = nullptr;
+  long long *crow_dev = nullptr, *xrow_dev = nullptr;
   std::vector<long long> off, first_d, first_v;
   long long *off_dev = nullptr, *first_d_dev = nullptr, *first_v_dev = nullptr;
   BSys *sys = nullptr;
@@ -518,6 +614,9 @@ extern "C" void n2d_vie_batch_destroy(n2d_vie_batch *b) {
   n2d_free(b->first_v_dev);
   n2d_free(b->sys);
   n2d_free((void *)b->diag_dev);
+  n2d_free(b->hyb_dev);
+  n2d_free(b->crow_dev);
+  n2d_free(b->xrow_dev);
   delete b;
 }
 
@@ -537,13 +636,13 @@ static int build_set(n2d_vie_batch *b, int set) {
     size_t smem[N2D_VIE_PASSES];
     long long tiles[N2D_VIE_PASSES];
     const int precondition = set == 0;
-    double *norm = set == 0 ? &s->before_sq : nullptr;
+    double *norm = set == 0 && !b->any_hybrid ? &s->before_sq : nullptr;
     int *flag = set == 0 ? &s->flag : set == 1 ? &s->rflag : nullptr;
     if (!n2c_vie_pass_plans<C>(b->plans[q], precondition, norm, flag, args, mode, L, smem, tiles)) return 0;
     for (int i = 0; i < N2D_VIE_PASSES; ++i) {
       args[i].gate = set == 0 ? &s->active : set == 1 ? &s->running : nullptr;
       desc[i][q].a = args[i];
-      desc[i][q].off = b->off[q];
+      desc[i][q].off = b->off[q] + b->cond[q];
       desc[i][q].L = L[i];
       first[i][q + 1] = first[i][q] + tiles[i];
       PassSet &ps = b->sets[set][i];
@@ -581,29 +680,50 @@ static int launch_set_t(const n2d_vie_batch *b, const PassSet &ps, const double2
   return n2c_check_launch("batched fft pass");
 }
 
-// y = A x over the whole batch with descriptor set `set`.
+static BView view_of(const n2d_vie_batch *b);
+
+// y = A x over the whole batch with descriptor set `set`: the volume passes,
+// then the conductor and cross rows of the hybrid systems (and, for the
+// Arnoldi set, the norm of w, which the volume epilogue cannot take there).
 static int batch_apply(const n2d_vie_batch *b, int set, const double2 *x, double2 *y) {
   for (int i = 0; i < N2D_VIE_PASSES; ++i) {
     const PassSet &ps = b->sets[set][i];
     const int ok = ps.fp32 ? launch_set_t<float2>(b, ps, x, y) : launch_set_t<double2>(b, ps, x, y);
     if (!ok) return 0;
   }
+  if (!b->any_hybrid) return 1;
+  const BView v = view_of(b);
+  const long long crows = b->crow[b->K], xrows = b->xrow[b->K];
+  if (crows) seg_conductor_kernel<<<(unsigned)crows, 256, 0, n2c_stream()>>>(v, b->hyb_dev, b->crow_dev, x, y, set);
+  if (xrows)
+    seg_cross_kernel<<<(unsigned)((xrows * 32 + 255) / 256), 256, 0, n2c_stream()>>>(v, b->hyb_dev, b->xrow_dev,
+                                                                                       xrows, x, y, set);
+  if (!n2c_check_launch("batched conductor rows")) return 0;
+  if (set == 0) {
+    seg_wnorm_kernel<<<(unsigned)b->first_v[b->K], VEC_THREADS, 0, n2c_stream()>>>(v);
+    if (!n2c_check_launch("batched norm of w")) return 0;
+  }
   return 1;
 }
 
-extern "C" int n2d_vie_batch_create(n2d_vie_batch **out, n2d_vie *const *plans, long long count) {
+static int batch_create(n2d_vie_batch **out, n2d_vie *const *plans, n2d_hybrid *const *hybrids,
+                        long long count) {
   *out = nullptr;
-  if (count < 1 || count > (1 << 20)) { n2c_set_error("batch of %lld plans", count); return 0; }
+  if (count < 1 || count > (1 << 20)) { n2c_set_error("batch of %lld systems", count); return 0; }
   n2d_vie_batch *b = new n2d_vie_batch();
   b->K = (int)count;
-  b->fp32 = n2d_vie_fp32(plans[0]);
   b->off.assign(count + 1, 0);
   b->first_d.assign(count + 1, 0);
   b->first_v.assign(count + 1, 0);
+  b->crow.assign(count + 1, 0);
+  b->xrow.assign(count + 1, 0);
   std::vector<const double2 *> diag(count);
+  std::vector<BHyb> hyb(count);
   for (long long q = 0; q < count; ++q) {
-    n2d_vie *p = plans[q];
-    if (!p || p->cells < 1) { n2c_set_error("batch plan %lld is empty", q); delete b; return 0; }
+    n2d_hybrid *h = hybrids ? hybrids[q] : nullptr;
+    n2d_vie *p = h ? n2c_hybrid_volume(h) : plans[q];
+    if (!p || p->cells < 1) { n2c_set_error("batch system %lld has no volume cells", q); delete b; return 0; }
+    if (q == 0) b->fp32 = n2d_vie_fp32(p);
     if (n2d_vie_fp32(p) != b->fp32) {
       n2c_set_error("batch plans mix FP32 and FP64 transforms");
       delete b;
@@ -611,30 +731,53 @@ extern "C" int n2d_vie_batch_create(n2d_vie_batch **out, n2d_vie *const *plans, 
     }
     for (int d = 0; d < 3; ++d)
       if (p->P[d] > MAX_L) {
-        n2c_set_error("batch plan %lld: padded axis %lld exceeds %d", q, p->P[d], MAX_L);
+        n2c_set_error("batch system %lld: padded axis %lld exceeds %d", q, p->P[d], MAX_L);
         delete b;
         return 0;
       }
     for (long long r = 0; r < q; ++r)
-      if (plans[r] == p) { n2c_set_error("plan %lld appears twice in the batch", q); delete b; return 0; }
-    const long long n = 3 * (p->mirror ? p->mirror : p->cells);
+      if (b->plans[r] == p) { n2c_set_error("plan of system %lld appears twice in the batch", q); delete b; return 0; }
+    const long long nv = 3 * (p->mirror ? p->mirror : p->cells);
+    const long long c = h ? n2c_hybrid_conductors(h) : 0;
+    if (h && n2d_hybrid_order(h) != c + nv) {
+      n2c_set_error("batch system %lld: hybrid order does not match its plan", q);
+      delete b;
+      return 0;
+    }
+    const long long n = c + nv;
     b->plans.push_back(p);
+    b->hybrids.push_back(h);
+    b->cond.push_back(c);
+    b->any_hybrid = b->any_hybrid || c > 0;
     b->off[q + 1] = b->off[q] + n;
     b->first_d[q + 1] = b->first_d[q] + (n + DOT_RANGE - 1) / DOT_RANGE;
     b->first_v[q + 1] = b->first_v[q] + (n + VEC_RANGE - 1) / VEC_RANGE;
-    diag[q] = (const double2 *)n2d_vie_diag(p);
+    b->crow[q + 1] = b->crow[q] + c;
+    b->xrow[q + 1] = b->xrow[q] + (c ? nv : 0);
+    diag[q] = h ? n2c_hybrid_pdiag(h) : (const double2 *)n2d_vie_diag(p);
+    hyb[q] = BHyb{h ? n2c_hybrid_blocks(h) : nullptr, c, n};
   }
   b->N = b->off[count];
-  if (b->first_v[count] > 0x7fffffffLL) { n2c_set_error("batch too large"); delete b; return 0; }
+  if (b->first_v[count] > 0x7fffffffLL || b->crow[count] > 0x7fffffffLL || b->xrow[count] * 32 > 0x7fffffffLL) {
+    n2c_set_error("batch too large");
+    delete b;
+    return 0;
+  }
   b->off_dev = (long long *)n2d_alloc((count + 1) * sizeof(long long));
   b->first_d_dev = (long long *)n2d_alloc((count + 1) * sizeof(long long));
   b->first_v_dev = (long long *)n2d_alloc((count + 1) * sizeof(long long));
+  b->crow_dev = (long long *)n2d_alloc((count + 1) * sizeof(long long));
+  b->xrow_dev = (long long *)n2d_alloc((count + 1) * sizeof(long long));
+  b->hyb_dev = (BHyb *)n2d_alloc(count * sizeof(BHyb));
   b->sys = (BSys *)n2d_alloc(count * sizeof(BSys));
   b->diag_dev = (const double2 **)n2d_alloc(count * sizeof(double2 *));
-  int ok = b->off_dev && b->first_d_dev && b->first_v_dev && b->sys && b->diag_dev &&
-           n2d_upload(b->off_dev, b->off.data(), (count + 1) * sizeof(long long)) &&
+  int ok = b->off_dev && b->first_d_dev && b->first_v_dev && b->crow_dev && b->xrow_dev && b->hyb_dev && b->sys &&
+           b->diag_dev && n2d_upload(b->off_dev, b->off.data(), (count + 1) * sizeof(long long)) &&
            n2d_upload(b->first_d_dev, b->first_d.data(), (count + 1) * sizeof(long long)) &&
            n2d_upload(b->first_v_dev, b->first_v.data(), (count + 1) * sizeof(long long)) &&
+           n2d_upload(b->crow_dev, b->crow.data(), (count + 1) * sizeof(long long)) &&
+           n2d_upload(b->xrow_dev, b->xrow.data(), (count + 1) * sizeof(long long)) &&
+           n2d_upload(b->hyb_dev, hyb.data(), count * sizeof(BHyb)) &&
            n2d_upload((void *)b->diag_dev, diag.data(), count * sizeof(double2 *)) &&
            n2d_memset(b->sys, 0, count * sizeof(BSys));
   if (ok) ok = b->fp32 ? build_set<float2>(b, 0) : build_set<double2>(b, 0);
@@ -645,6 +788,14 @@ extern "C" int n2d_vie_batch_create(n2d_vie_batch **out, n2d_vie *const *plans, 
   return 1;
 }
 
+extern "C" int n2d_vie_batch_create(n2d_vie_batch **out, n2d_vie *const *plans, long long count) {
+  return batch_create(out, plans, nullptr, count);
+}
+
+extern "C" int n2d_hybrid_batch_create(n2d_vie_batch **out, n2d_hybrid *const *systems, long long count) {
+  return batch_create(out, nullptr, systems, count);
+}
+
 extern "C" long long n2d_vie_batch_order(const n2d_vie_batch *b) { return b ? b->N : 0; }
 extern "C" long long n2d_vie_batch_offset(const n2d_vie_batch *b, long long q) {
   return b && q >= 0 && q <= b->K ? b->off[q] : -1;
@@ -652,6 +803,18 @@ extern "C" long long n2d_vie_batch_offset(const n2d_vie_batch *b, long long q) {
 
 extern "C" int n2d_vie_batch_apply(n2d_vie_batch *b, const double *x_dev, double *y_dev) {
   return batch_apply(b, 2, (const double2 *)x_dev, (double2 *)y_dev);
+}
+
+// The kernels' view of the batch: its systems and, once a solve has run, the
+// GMRES workspace (the products of batch_apply touch only sys, off, the
+// maps and the Jacobi divisors, plus parts_v for the norm of w).
+static BView view_of(const n2d_vie_batch *b) {
+  if (b->work) return b->work->v;
+  BView v;
+  memset(&v, 0, sizeof(v));
+  v.sys = b->sys; v.off = b->off_dev; v.first_d = b->first_d_dev; v.first_v = b->first_v_dev;
+  v.K = b->K; v.N = b->N; v.diag = b->diag_dev;
+  return v;
 }
 
 static BatchWork *work_get(n2d_vie_batch *b, int m) {
@@ -815,6 +978,14 @@ extern "C" int n2d_gmres_batch_dev(n2d_vie_batch *b, const double *b_dev, double
       const double beta = reps[q].residual_norm;
       if (beta <= target[q]) { reps[q].status = ST_CONVERGED; done[q] = 1; continue; }
       if ((long long)reps[q].iterations >= (long long)maxit) { reps[q].status = ST_LIMIT; done[q] = 1; continue; }
+      // A hybrid system with a zero or non-finite conductor diagonal cannot be
+      // preconditioned (dielectric_fft.c:77-81): it stops as the single
+      // system's solve does.
+      if (b->hybrids[q] && !n2c_hybrid_precondition_ok(b->hybrids[q])) {
+        reps[q].status = ST_CALLBACK;
+        done[q] = 1;
+        continue;
+      }
       hs[q].active = 1; hs[q].beta = beta; hs[q].used = 0; hs[q].breakdown = 0; hs[q].flag = 0;
       hs[q].normalize = 0; hs[q].reorth = 0; hs[q].status = ST_RUNNING;
       hs[q].iterations = (long long)reps[q].iterations;

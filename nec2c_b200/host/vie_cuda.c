@@ -473,15 +473,18 @@ int nec2c_cuda_gmres_hybrid_device(nec2c_cuda_hybrid *h, const void *b, void *x,
 struct nec2c_cuda_vie_batch {
   n2d_vie_batch *dev;
   size_t count, order;
-  nec2c_cuda_vie_plan **plans;
+  nec2c_cuda_vie_plan **plans;    /* volume plan of each system */
+  nec2c_cuda_hybrid **hybrids;    /* NULL for a batch of plans */
   size_t *offsets;
   void *b_dev, *x_dev;   /* staging of the host-vector solve */
 };
 
 static int batch_ready(nec2c_cuda_vie_batch *b)
 {
-  for(size_t q = 0; q < b->count; ++q)
+  for(size_t q = 0; q < b->count; ++q) {
+    if(b->hybrids && !hybrid_ready(b->hybrids[q])) return 0;
     if(!nec2c_cuda_plan_device(b->plans[q])) return 0;
+  }
   return 1;
 }
 
@@ -492,6 +495,7 @@ void nec2c_cuda_vie_batch_destroy(nec2c_cuda_vie_batch *b)
   n2d_free(b->b_dev);
   n2d_free(b->x_dev);
   free(b->plans);
+  free(b->hybrids);
   free(b->offsets);
   free(b);
 }
@@ -517,6 +521,40 @@ int nec2c_cuda_vie_batch_create(nec2c_cuda_vie_batch **out, nec2c_cuda_vie_plan 
     if(!devs[q]) { free(devs); nec2c_cuda_vie_batch_destroy(b); return 0; }
   }
   if(!n2d_vie_batch_create(&b->dev, devs, (long long)count)) { free(devs); nec2c_cuda_vie_batch_destroy(b); return 0; }
+  free(devs);
+  for(size_t q = 0; q <= count; ++q) b->offsets[q] = (size_t)n2d_vie_batch_offset(b->dev, (long long)q);
+  b->order = b->offsets[count];
+  *out = b;
+  return 1;
+}
+
+int nec2c_cuda_hybrid_batch_create(nec2c_cuda_vie_batch **out, nec2c_cuda_hybrid *const *systems, size_t count)
+{
+  nec2c_cuda_vie_batch *b;
+  n2d_hybrid **devs;
+  if(!out) return 0;
+  *out = NULL;
+  if(!systems || count == 0 || count > ((size_t)1 << 20)) { n2c_set_error("batch: bad system list"); return 0; }
+  b = calloc(1, sizeof(*b));
+  devs = calloc(count, sizeof(*devs));
+  if(!b || !devs) { free(b); free(devs); return 0; }
+  b->count = count;
+  b->plans = calloc(count, sizeof(*b->plans));
+  b->hybrids = calloc(count, sizeof(*b->hybrids));
+  b->offsets = calloc(count + 1, sizeof(*b->offsets));
+  if(!b->plans || !b->hybrids || !b->offsets) { free(devs); nec2c_cuda_vie_batch_destroy(b); return 0; }
+  for(size_t q = 0; q < count; ++q) {
+    nec2c_cuda_hybrid *h = systems[q];
+    if(!h || !h->volume) {
+      n2c_set_error("batch: system %zu has no volume plan", q);
+      free(devs); nec2c_cuda_vie_batch_destroy(b); return 0;
+    }
+    if(!hybrid_ready(h) || !nec2c_cuda_plan_device(h->volume)) { free(devs); nec2c_cuda_vie_batch_destroy(b); return 0; }
+    b->hybrids[q] = h;
+    b->plans[q] = h->volume;
+    devs[q] = h->dev;
+  }
+  if(!n2d_hybrid_batch_create(&b->dev, devs, (long long)count)) { free(devs); nec2c_cuda_vie_batch_destroy(b); return 0; }
   free(devs);
   for(size_t q = 0; q <= count; ++q) b->offsets[q] = (size_t)n2d_vie_batch_offset(b->dev, (long long)q);
   b->order = b->offsets[count];

@@ -19,7 +19,7 @@ import pytest
 
 import cases
 import nec2c_b200 as nb
-from oracle_lib import OraclePlan
+from oracle_lib import OracleHybrid, OraclePlan
 
 pytestmark = pytest.mark.gpu
 
@@ -150,3 +150,108 @@ def test_batch_refuses_bad_plan_lists(near_tables):
     ok, xs, reps = b.gmres([np.ones(plans[0].n)], restart=40, maxit=20)   # cycle capped by maxit
     assert reps[0]["status"] in (0, 1) and 0 < reps[0]["iterations"] <= 20
     b.close()
+
+
+# ------------------------------------------------------------ hybrid systems
+def hybrid_blocks(c, v, seed):
+    """[C|B] (c x n) then D (v x c), row-major: a diagonally dominant wire
+    block C with weak couplings B and D to the volume unknowns."""
+    rng = np.random.default_rng(seed)
+    n = c + v
+    cm = 0.1 * (rng.standard_normal((c, c)) + 1j * rng.standard_normal((c, c)))
+    cm += np.diag(np.full(c, 4.0 + 1.0j))
+    bm = 0.01 * (rng.standard_normal((c, v)) + 1j * rng.standard_normal((c, v)))
+    dm = 0.01 * (rng.standard_normal((v, c)) + 1j * rng.standard_normal((v, c)))
+    return np.concatenate([np.concatenate([cm, bm], axis=1).reshape(-1), dm.reshape(-1)]), n
+
+
+def make_hybrids(near_tables, mixed, specs):
+    """specs: (shape, fill, seed, conductors); plus one PEC-imaged system."""
+    from test_hybrid_gpu import material_case
+    h, k, table = near_tables["rand_k0.3"]
+    gh, oh, keep = [], [], []
+    for shape, fill, seed, c in specs:
+        xyz = cases.random_lattice(shape, fill, seed)
+        eps = cases.random_eps(xyz.size // 3, seed + 70, er=(2.0, 6.0))
+        gp = nb.VolumePlan(shape, xyz, h, k, 3.0, table, mixed=mixed)
+        op = OraclePlan(shape, xyz, h, k, 3.0, table)
+        for i, e in enumerate(eps):
+            assert gp.set_permittivity(i, e) and op.set_permittivity(i, e)
+        v = 3 * (xyz.size // 3)
+        blocks, n = hybrid_blocks(c, v, seed + 80)
+        g = nb.HybridSystem(gp, c, v)
+        g.set_blocks(blocks)
+        gh.append(g)
+        oh.append(OracleHybrid(op, c, v, blocks))
+        keep += [gp, op]
+    if not mixed:
+        op, gp, v = material_case(near_tables, 0.0, True)
+        blocks, n = hybrid_blocks(5, v, 99)
+        g = nb.HybridSystem(gp, 5, v, pec=True)
+        g.set_blocks(blocks)
+        gh.append(g)
+        oh.append(OracleHybrid(op, 5, v, blocks, True))
+        keep += [gp, op]
+    return gh, oh, keep
+
+
+HYB = [((6, 5, 4), 0.8, 1, 21), ((8, 8, 8), 1.0, 2, 11), ((5, 4, 3), 1.0, 3, 41), ((12, 9, 17), 0.4, 4, 2)]
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_hybrid_batch_product(near_tables, mixed):
+    import torch
+    gh, oh, keep = make_hybrids(near_tables, mixed, HYB)
+    batch = nb.VolumeBatch(hybrids=gh)
+    assert batch.order == sum(g.n for g in gh)
+    rng = np.random.default_rng(21)
+    x = rng.standard_normal(batch.order) + 1j * rng.standard_normal(batch.order)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.zeros_like(xd)
+    assert nb.load().nec2c_cuda_vie_batch_apply_device(batch.h, C.c_void_p(xd.data_ptr()),
+                                                       C.c_void_p(yd.data_ptr())), nb.last_error()
+    y = yd.cpu().numpy()
+    for q, (g, o) in enumerate(zip(gh, oh)):
+        xs, ys = x[batch.offsets[q]:batch.offsets[q + 1]], y[batch.offsets[q]:batch.offsets[q + 1]]
+        if mixed:
+            assert rel_l2(ys, o.apply(xs)) < 1e-5, q
+        else:
+            assert rel_max(ys, g.apply(xs)) < 1e-14, q
+            assert rel_max(ys, o.apply(xs)) < 1e-12, q
+    batch.close()
+
+
+@pytest.mark.parametrize("mixed,rtol,tol", [(False, 1e-11, 1e-8), (True, 1e-8, 1e-5)])
+def test_hybrid_batch_gmres(near_tables, mixed, rtol, tol):
+    gh, oh, keep = make_hybrids(near_tables, mixed, HYB)
+    batch = nb.VolumeBatch(hybrids=gh)
+    rng = np.random.default_rng(8)
+    bs = [rng.standard_normal(g.n) + 1j * rng.standard_normal(g.n) for g in gh]
+    ok, xs, reps = batch.gmres(bs, rtol=rtol, maxit=600)
+    assert ok, (reps, nb.last_error())
+    for q, (g, o) in enumerate(zip(gh, oh)):
+        assert reps[q]["status"] == 0 and reps[q]["relative_residual"] <= rtol
+        r = bs[q] - o.apply(xs[q])
+        assert np.linalg.norm(r) <= 1.01 * rtol * np.linalg.norm(bs[q])
+        ok_o, xo, _ = o.gmres(bs[q], rtol=1e-12, maxit=600)
+        assert ok_o and rel_l2(xs[q], xo) < tol
+        ok_s, _, rs = g.gmres(bs[q], rtol=rtol, maxit=600)
+        assert ok_s and abs(rs["iterations"] - reps[q]["iterations"]) <= max(3, rs["iterations"] // 10)
+    batch.close()
+
+
+def test_hybrid_batch_unpreconditionable_system(near_tables):
+    """A zero conductor diagonal stops that system with the callback status
+    (dielectric_fft.c:77-81), as the single solve does; the others converge."""
+    gh, oh, keep = make_hybrids(near_tables, False, HYB[:2])
+    blocks, n = hybrid_blocks(HYB[1][3], gh[1].n - HYB[1][3], 5)
+    blocks[0] = 0                       # C_00 = 0
+    gh[1].set_blocks(blocks)
+    batch = nb.VolumeBatch(hybrids=gh)
+    bs = [np.ones(g.n, dtype=np.complex128) for g in gh]
+    ok, xs, reps = batch.gmres(bs, rtol=1e-10, maxit=300)
+    _, _, single = gh[1].gmres(bs[1], rtol=1e-10, maxit=300)
+    assert not ok
+    assert reps[0]["status"] == 0
+    assert reps[1]["status"] == single["status"] == 3     # VIE_ITERATIVE_CALLBACK_FAILED
+    batch.close()
