@@ -681,45 +681,73 @@ def batched_bench(nb, torch):
 
 
 def volume_batch_bench(nb, torch, stream):
-    """Config-3 shaped volume sweep in one batch: the config-0 cube (16^3 cells,
-    0.2 lambda at 300 MHz, eps_r = 4 - 0.1j) at 128 frequencies uniform in
-    100-400 MHz, and 64 seeded random cubes of 8^3-32^3 cells (0.2 lambda at
-    300 MHz, eps_r ~ U[2,8], tan d = 0.05), x-polarised plane-wave excitation,
-    GMRES(30) to rtol 1e-6.  The far pairs of every plan are quadratured on the
-    GPU at its own frequency; the 13 near-pair tensors (the caller's certified
-    quadrature) come from the golden table of the nearest lattice, reused at
-    every frequency.  Timed: the whole batch in one nec2c_cuda_gmres_batch_device
-    call (FP32 transforms, and the plain FP64 form), against one device GMRES
-    call per plan (both forms), CUDA events on the launching stream."""
+    """Config-3 shaped sweep in one batch of dipole-plus-cube systems.
+
+    The batch holds 192 systems.  The first 128 are the config-0 model at 128
+    frequencies uniform in 100-400 MHz: a cube of 16^3 cells, 0.2 lambda at
+    300 MHz, eps_r = 4 - 0.1j, beside a 21-segment dipole.  The other 64 are
+    seeded cubes of 8^3-32^3 cells (0.2 lambda at 300 MHz, eps_r ~ U[2,8],
+    tan d = 0.05), each beside a dipole of 11-41 segments.  Each system is the
+    hybrid [C B; D V] operator, driven by a 1 V source at the dipole's centre
+    and an x-polarised plane wave on the cube, and solved with GMRES(30) to
+    rtol 1e-6.
+
+    - Every plan's far pairs are quadratured on the GPU at its own frequency.
+    - The 13 near-pair tensors come from the golden table of the nearest
+      lattice, reused at every frequency.  The wire blocks are seeded
+      diagonally dominant complex matrices with weak wire-cube couplings.  Both belong to the caller (the
+      reference's certified quadrature and its wire/coupling fill), which
+      bench.py may not run.
+    - Timed: the whole batch in one nec2c_cuda_gmres_batch_device call, in both
+      forms (FP32 transforms, and the plain FP64 form), against one device
+      GMRES call per system.  CUDA events on the launching stream."""
     tabs = near_tables_all()
     lam = C0 / 300e6
     rng = np.random.default_rng(7)
-    specs = [(16, 2 * math.pi * f / C0, "c0", 4 - 0.1j) for f in np.linspace(100e6, 400e6, 128)]
+    specs = [(16, 2 * math.pi * f / C0, "c0", 4 - 0.1j, 21) for f in np.linspace(100e6, 400e6, 128)]
     for n in rng.choice([8, 12, 16, 24, 32], 64):
-        specs.append((int(n), 2 * math.pi / lam, "c0" if n <= 16 else "c3_32", rng.uniform(2, 8) * (1 - 0.05j)))
+        specs.append((int(n), 2 * math.pi / lam, "c0" if n <= 16 else "c3_32", rng.uniform(2, 8) * (1 - 0.05j),
+                      int(rng.integers(11, 42))))
     lib = nb.load()
 
+    blocks = []
+    for q, (n, k, tab, eps, c) in enumerate(specs):
+        v = 3 * n ** 3
+        r = np.random.default_rng(5000 + q)
+        cm = r.standard_normal((c, c)) + 1j * r.standard_normal((c, c))
+        cm += np.diag(np.full(c, 2.0 * math.sqrt(c)))
+        bm = 0.01 * (r.standard_normal((c, v)) + 1j * r.standard_normal((c, v)))
+        dm = 0.01 * (r.standard_normal((v, c)) + 1j * r.standard_normal((v, c)))
+        blocks.append(np.concatenate([np.concatenate([cm, bm], axis=1).reshape(-1), dm.reshape(-1)]))
+
     def build(mixed):
-        plans, rhs = [], []
-        for n, k, tab, eps in specs:
+        systems, rhs, keep = [], [], []
+        for q, (n, k, tab, eps, c) in enumerate(specs):
             h = 0.2 * lam / n
             g = np.arange(n)
             xyz = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1).astype(np.uintp)
             p = nb.VolumePlan((n, n, n), xyz, h, k, eps, tabs[tab][2], mixed=mixed)
-            b = np.zeros(3 * n ** 3, dtype=np.complex128)
+            v = 3 * n ** 3
+            hs = nb.HybridSystem(p, c, v)
+            hs.set_blocks(blocks[q])
+            b = np.zeros(c + v, dtype=np.complex128)
+            b[c // 2] = 1.0
             z = xyz[2::3].astype(np.float64)
-            b[0::3] = 2 * np.exp(-1j * k * h * (z + 0.5)) * math.sin(k * h / 2) / (k * h / 2)
-            plans.append(p)
+            b[c::3] = 2 * np.exp(-1j * k * h * (z + 0.5)) * math.sin(k * h / 2) / (k * h / 2)
+            systems.append(hs)
             rhs.append(b)
-        return plans, rhs
+            keep.append(p)
+        return systems, rhs, keep
 
     t0 = time.perf_counter()
-    plans_m, rhs = build(True)
+    sys_m, rhs, keep_m = build(True)
     build_s = time.perf_counter() - t0
-    plans_d, _ = build(False)
+    sys_d, _, keep_d = build(False)
     opts = nb.GmresOptions(30, 3000, 1e-6, 0.0)
-    out = {"systems": len(specs), "lattices": "128 x 16^3 (100-400 MHz) + 64 random in {8,12,16,24,32}^3",
-           "unknowns": int(sum(p.n for p in plans_m)), "plan_build_s_fp32": build_s}
+    out = {"systems": len(specs),
+           "model": "dipole (11-41 segments) beside a cube: 128 x 16^3 (100-400 MHz) + 64 random in "
+                    "{8,12,16,24,32}^3",
+           "unknowns": int(sum(s.n for s in sys_m)), "plan_build_s_fp32": build_s}
 
     def timed(fn):
         torch.cuda.synchronize()
@@ -731,11 +759,11 @@ def volume_batch_bench(nb, torch, stream):
         return e0.elapsed_time(e1), r
 
     sols = {}
-    for form, plans in (("fp32_transforms", plans_m), ("fp64", plans_d)):
-        batch = nb.VolumeBatch(plans)
+    for form, systems, keep in (("fp32_transforms", sys_m, keep_m), ("fp64", sys_d, keep_d)):
+        batch = nb.VolumeBatch(hybrids=systems)
         b_dev = torch.from_numpy(np.concatenate(rhs)).cuda()
         x_dev = torch.zeros_like(b_dev)
-        reps = (nb.GmresReport * len(plans))()
+        reps = (nb.GmresReport * len(systems))()
 
         def solve_batch():
             x_dev.zero_()
@@ -751,35 +779,38 @@ def volume_batch_bench(nb, torch, stream):
             torch.cuda.nvtx.range_pop()
         ms, ok = min((timed(solve_batch) for _ in range(2)), key=lambda t: t[0])
         if not ok:
-            raise RuntimeError("batched volume solve failed: " + nb.last_error())
+            raise RuntimeError("batched solve failed: %s %s" % (
+                nb.last_error(), sorted(set((r.status, r.iterations) for r in reps))[:8]))
         sols[form] = x_dev.cpu().numpy()
         its = [r.iterations for r in reps]
         batch.close()
+        bs = [torch.from_numpy(b).cuda() for b in rhs]
+        x = torch.zeros(max(b.numel() for b in bs), dtype=torch.complex128, device="cuda")
 
         def one_by_one():
             ok = 1
-            for p, b in zip(plans, bs):
+            for s, b in zip(systems, bs):
                 x.zero_()
-                ok &= lib.nec2c_cuda_gmres_plan_device(p.h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()),
-                                                       C.byref(opts), C.byref(nb.GmresReport()))
+                ok &= lib.nec2c_cuda_gmres_hybrid_device(s.h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()),
+                                                         C.byref(opts), C.byref(nb.GmresReport()))
             return ok
-        bs = [torch.from_numpy(b).cuda() for b in rhs]
-        x = torch.zeros(max(b.numel() for b in bs), dtype=torch.complex128, device="cuda")
         timed(one_by_one)
         ms1, ok1 = timed(one_by_one)
         if not ok1:
-            raise RuntimeError("per-plan volume solve failed: " + nb.last_error())
-        out[form] = {"one_batch": {"ms": ms, "solves_per_s": 1e3 * len(plans) / ms},
-                     "one_call_per_plan": {"ms": ms1, "solves_per_s": 1e3 * len(plans) / ms1},
+            raise RuntimeError("per-system solve failed: " + nb.last_error())
+        out[form] = {"one_batch": {"ms": ms, "solves_per_s": 1e3 * len(systems) / ms},
+                     "one_call_per_system": {"ms": ms1, "solves_per_s": 1e3 * len(systems) / ms1},
                      "iterations": {"min": int(min(its)), "max": int(max(its)), "mean": float(np.mean(its))}}
-        for p in plans:
+        for s in systems:
+            s.close()
+        for p in keep:
             p.close()
     off = np.cumsum([0] + [b.size for b in rhs])
     out["max_rel_err_fp32_transforms_vs_fp64"] = max(
         float(np.linalg.norm(sols["fp32_transforms"][a:b] - sols["fp64"][a:b]) / np.linalg.norm(sols["fp64"][a:b]))
         for a, b in zip(off[:-1], off[1:]))
-    out["batch_fp32_vs_plain_fp64_one_call_per_plan"] = (
-        out["fp32_transforms"]["one_batch"]["solves_per_s"] / out["fp64"]["one_call_per_plan"]["solves_per_s"])
+    out["batch_fp32_vs_plain_fp64_one_call_per_system"] = (
+        out["fp32_transforms"]["one_batch"]["solves_per_s"] / out["fp64"]["one_call_per_system"]["solves_per_s"])
     return out
 
 

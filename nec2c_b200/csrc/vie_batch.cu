@@ -421,49 +421,95 @@ __device__ __forceinline__ bool sys_gated(const BSys *s, int set) {
   return set == 0 ? !s->active : set == 1 ? !s->running : false;
 }
 
-// One CTA per conductor row of every hybrid system: y_i = sum_j [C|B]_ij z_j,
-// z = x or x ./ pdiag (dielectric_fft.c:54-66).
+// Conductor rows per CTA of the conductor-row kernel, and the cross-row
+// layout: a system with at most CROSS_PACK conductor unknowns takes
+// CROSS_ELEMS / c volume rows per CTA (its D rows are contiguous, so the CTA
+// streams one contiguous block of D); a system with more takes 8 rows per
+// CTA, a warp per row.
+constexpr int COND_ROWS = 4;
+constexpr int CROSS_PACK = 64;
+constexpr int CROSS_ELEMS = 2048;
+__host__ __device__ __forceinline__ long long cross_rows_per_cta(long long c) {
+  return c <= CROSS_PACK ? CROSS_ELEMS / c : 8;
+}
+
+// z = x of every hybrid system, divided by its preconditioner divisor for
+// the Arnoldi set (the conductor and cross rows then read z, computed once).
+__global__ void __launch_bounds__(VEC_THREADS) seg_zc_kernel(BView v, const BHyb *hyb, const double2 *x, double2 *z,
+                                                             int set) {
+  const VecCta c = vec_cta(v);
+  if (hyb[c.q].c == 0 || sys_gated(v.sys + c.q, set)) return;
+  const double2 *pd = v.diag[c.q];
+  const long long base = v.off[c.q];
+  for (long long i = c.lo + threadIdx.x; i < c.hi; i += VEC_THREADS)
+    z[i] = set == 0 ? cdiv(x[i], pd[i - base]) : x[i];
+}
+
+// COND_ROWS conductor rows of one hybrid system per CTA: y_i = sum_j
+// [C|B]_ij z_j (dielectric_fft.c:54-66), z read once for all the CTA's rows.
 __global__ void __launch_bounds__(256) seg_conductor_kernel(BView v, const BHyb *hyb, const long long *crow,
-                                                            const double2 *x, double2 *y, int set) {
+                                                            const double2 *z, double2 *y, int set) {
   const int q = find_seg(crow, v.K, blockIdx.x);
   if (sys_gated(v.sys + q, set)) return;
   const BHyb hb = hyb[q];
-  const long long i = (long long)blockIdx.x - crow[q];
-  const double2 *row = hb.blocks + i * hb.n, *xq = x + v.off[q], *pd = set == 0 ? v.diag[q] : nullptr;
-  double2 acc = make_double2(0, 0);
+  const long long i0 = ((long long)blockIdx.x - crow[q]) * COND_ROWS;
+  const int rows = (int)min((long long)COND_ROWS, hb.c - i0);
+  const double2 *zq = z + v.off[q], *row = hb.blocks + i0 * hb.n;
+  double2 acc[COND_ROWS];
+#pragma unroll
+  for (int r = 0; r < COND_ROWS; ++r) acc[r] = make_double2(0, 0);
   for (long long j = threadIdx.x; j < hb.n; j += blockDim.x) {
-    double2 z = xq[j];
-    if (pd) z = cdiv(z, pd[j]);
-    acc = cadd(acc, cmul(row[j], z));
+    const double2 zj = zq[j];
+#pragma unroll
+    for (int r = 0; r < COND_ROWS; ++r)
+      if (r < rows) acc[r] = cadd(acc[r], cmul(row[r * hb.n + j], zj));
   }
-  acc = block_sum(acc);
-  if (threadIdx.x == 0) y[v.off[q] + i] = acc;
+  for (int r = 0; r < rows; ++r) {
+    const double2 t = block_sum(acc[r]);
+    if (threadIdx.x == 0) y[v.off[q] + i0 + r] = t;
+  }
 }
 
-// One warp per volume row of every hybrid system: y_{c+i} += sum_j D_ij z_j
-// over its conductor unknowns (dielectric_fft.c:67-74).
-__global__ void seg_cross_kernel(BView v, const BHyb *hyb, const long long *xrow, long long rows,
-                                 const double2 *x, double2 *y, int set) {
-  const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= rows) return;
-  const int q = find_seg(xrow, v.K, warp);
+// Volume rows of one hybrid system per CTA: y_{c+i} += sum_j D_ij z_j over
+// its conductor unknowns (dielectric_fft.c:67-74), summed in j order.  With
+// few conductor unknowns the CTA's D rows form one contiguous block: it is
+// read coalesced into shared memory as products D_ij z_j, then a thread per
+// row adds its row up.  With many, a warp per row.
+__global__ void __launch_bounds__(256) seg_cross_kernel(BView v, const BHyb *hyb, const long long *xrow,
+                                                        const double2 *z, double2 *y, int set) {
+  const int q = find_seg(xrow, v.K, blockIdx.x);
   if (sys_gated(v.sys + q, set)) return;
   const BHyb hb = hyb[q];
-  const long long i = warp - xrow[q];
-  const double2 *row = hb.blocks + hb.c * hb.n + i * hb.c, *xq = x + v.off[q];
-  const double2 *pd = set == 0 ? v.diag[q] : nullptr;
-  double2 acc = make_double2(0, 0);
-  for (long long j = lane; j < hb.c; j += 32) {
-    double2 z = xq[j];
-    if (pd) z = cdiv(z, pd[j]);
-    acc = cadd(acc, cmul(row[j], z));
+  const long long c = hb.c, nv = hb.n - c, per = cross_rows_per_cta(c);
+  const long long r0 = ((long long)blockIdx.x - xrow[q]) * per;
+  const int rows = (int)min(per, nv - r0);
+  const double2 *zq = z + v.off[q], *D = hb.blocks + c * hb.n + r0 * c;
+  double2 *yq = y + v.off[q] + c + r0;
+  __shared__ double2 prod[CROSS_ELEMS];
+  __shared__ double2 zc[CROSS_PACK];
+  if (c <= CROSS_PACK) {
+    for (int j = threadIdx.x; j < c; j += blockDim.x) zc[j] = zq[j];
+    __syncthreads();
+    const int cc = (int)c, total = rows * cc;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) prod[e] = cmul(D[e], zc[e % cc]);
+    __syncthreads();
+    for (int t = threadIdx.x; t < rows; t += blockDim.x) {
+      double2 acc = make_double2(0, 0);
+      for (int j = 0; j < cc; ++j) acc = cadd(acc, prod[t * cc + j]);
+      yq[t] = cadd(yq[t], acc);
+    }
+    return;
   }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp >= rows) return;
+  const double2 *row = D + (long long)warp * c;
+  double2 acc = make_double2(0, 0);
+  for (long long j = lane; j < c; j += 32) acc = cadd(acc, cmul(row[j], zq[j]));
   for (int o = 16; o > 0; o >>= 1) {
     acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
     acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
   }
-  if (lane == 0) y[v.off[q] + hb.c + i] = cadd(y[v.off[q] + hb.c + i], acc);
+  if (lane == 0) yq[warp] = cadd(yq[warp], acc);
 }
 
 // ||w||^2 of every active system into before_sq (batches with hybrid
@@ -582,7 +628,8 @@ struct n2d_vie_batch {
   std::vector<long long> cond, crow, xrow;    // conductor unknowns; row prefixes
   bool any_hybrid = false;
   BHyb *hyb_dev = nullptr;
-  long long *crow_dev = nullptr, *xrow_dev = nullptr;
+  long long *crow_dev = nullptr, *xrow_dev = nullptr;   // CTA prefixes of the conductor / cross kernels
+  double2 *zbuf = nullptr;                              // z of the hybrid systems (batch order)
   std::vector<long long> off, first_d, first_v;
   long long *off_dev = nullptr, *first_d_dev = nullptr, *first_v_dev = nullptr;
   BSys *sys = nullptr;
@@ -617,6 +664,7 @@ extern "C" void n2d_vie_batch_destroy(n2d_vie_batch *b) {
   n2d_free(b->hyb_dev);
   n2d_free(b->crow_dev);
   n2d_free(b->xrow_dev);
+  n2d_free(b->zbuf);
   delete b;
 }
 
@@ -693,11 +741,11 @@ static int batch_apply(const n2d_vie_batch *b, int set, const double2 *x, double
   }
   if (!b->any_hybrid) return 1;
   const BView v = view_of(b);
-  const long long crows = b->crow[b->K], xrows = b->xrow[b->K];
-  if (crows) seg_conductor_kernel<<<(unsigned)crows, 256, 0, n2c_stream()>>>(v, b->hyb_dev, b->crow_dev, x, y, set);
-  if (xrows)
-    seg_cross_kernel<<<(unsigned)((xrows * 32 + 255) / 256), 256, 0, n2c_stream()>>>(v, b->hyb_dev, b->xrow_dev,
-                                                                                       xrows, x, y, set);
+  const long long cctas = b->crow[b->K], xctas = b->xrow[b->K];
+  seg_zc_kernel<<<(unsigned)b->first_v[b->K], VEC_THREADS, 0, n2c_stream()>>>(v, b->hyb_dev, x, b->zbuf, set);
+  if (cctas)
+    seg_conductor_kernel<<<(unsigned)cctas, 256, 0, n2c_stream()>>>(v, b->hyb_dev, b->crow_dev, b->zbuf, y, set);
+  if (xctas) seg_cross_kernel<<<(unsigned)xctas, 256, 0, n2c_stream()>>>(v, b->hyb_dev, b->xrow_dev, b->zbuf, y, set);
   if (!n2c_check_launch("batched conductor rows")) return 0;
   if (set == 0) {
     seg_wnorm_kernel<<<(unsigned)b->first_v[b->K], VEC_THREADS, 0, n2c_stream()>>>(v);
@@ -752,13 +800,13 @@ static int batch_create(n2d_vie_batch **out, n2d_vie *const *plans, n2d_hybrid *
     b->off[q + 1] = b->off[q] + n;
     b->first_d[q + 1] = b->first_d[q] + (n + DOT_RANGE - 1) / DOT_RANGE;
     b->first_v[q + 1] = b->first_v[q] + (n + VEC_RANGE - 1) / VEC_RANGE;
-    b->crow[q + 1] = b->crow[q] + c;
-    b->xrow[q + 1] = b->xrow[q] + (c ? nv : 0);
+    b->crow[q + 1] = b->crow[q] + (c + COND_ROWS - 1) / COND_ROWS;
+    b->xrow[q + 1] = b->xrow[q] + (c ? (nv + cross_rows_per_cta(c) - 1) / cross_rows_per_cta(c) : 0);
     diag[q] = h ? n2c_hybrid_pdiag(h) : (const double2 *)n2d_vie_diag(p);
     hyb[q] = BHyb{h ? n2c_hybrid_blocks(h) : nullptr, c, n};
   }
   b->N = b->off[count];
-  if (b->first_v[count] > 0x7fffffffLL || b->crow[count] > 0x7fffffffLL || b->xrow[count] * 32 > 0x7fffffffLL) {
+  if (b->first_v[count] > 0x7fffffffLL || b->crow[count] > 0x7fffffffLL || b->xrow[count] > 0x7fffffffLL) {
     n2c_set_error("batch too large");
     delete b;
     return 0;
@@ -769,9 +817,11 @@ static int batch_create(n2d_vie_batch **out, n2d_vie *const *plans, n2d_hybrid *
   b->crow_dev = (long long *)n2d_alloc((count + 1) * sizeof(long long));
   b->xrow_dev = (long long *)n2d_alloc((count + 1) * sizeof(long long));
   b->hyb_dev = (BHyb *)n2d_alloc(count * sizeof(BHyb));
+  if (b->any_hybrid) b->zbuf = (double2 *)n2d_alloc(b->N * sizeof(double2));
   b->sys = (BSys *)n2d_alloc(count * sizeof(BSys));
   b->diag_dev = (const double2 **)n2d_alloc(count * sizeof(double2 *));
   int ok = b->off_dev && b->first_d_dev && b->first_v_dev && b->crow_dev && b->xrow_dev && b->hyb_dev && b->sys &&
+           (b->zbuf || !b->any_hybrid) &&
            b->diag_dev && n2d_upload(b->off_dev, b->off.data(), (count + 1) * sizeof(long long)) &&
            n2d_upload(b->first_d_dev, b->first_d.data(), (count + 1) * sizeof(long long)) &&
            n2d_upload(b->first_v_dev, b->first_v.data(), (count + 1) * sizeof(long long)) &&
