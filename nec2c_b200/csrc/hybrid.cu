@@ -19,6 +19,7 @@ struct n2d_hybrid {
   int pec;
   double2 *blocks;   // c*(c+v) then v*c
   double2 *pdiag;    // full preconditioner divisor [diag(C); volume Jacobi]
+  double2 *z;        // x or x ./ pdiag of the current product
   int precondition_ok;
   double *partials;
   unsigned int *ticket;
@@ -27,41 +28,39 @@ struct n2d_hybrid {
 void n2c_gmres_work_free(void *w);
 void **n2c_hybrid_gm_slot(n2d_hybrid *h) { return &h->gm_work; }
 
-// One block per conductor row: y_i = sum_j [C|B]_ij z_j, z = x (or x ./ pdiag).
+// z = x, or x ./ pdiag when the input is preconditioned: both row kernels
+// read z, so each division happens once per product.
+__global__ void zc_kernel(const double2 *__restrict__ x, const double2 *__restrict__ pdiag, double2 *__restrict__ z,
+                          long long n, const int *gate) {
+  if (gated_off(gate)) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    z[i] = pdiag ? cdiv(x[i], pdiag[i]) : x[i];
+}
+
+// One block per conductor row: y_i = sum_j [C|B]_ij z_j (dielectric_fft.c:54-66).
 __global__ void __launch_bounds__(256) conductor_rows_kernel(const double2 *__restrict__ blocks,
-                                                             const double2 *__restrict__ x,
-                                                             const double2 *__restrict__ pdiag,
-                                                             long long c, long long n,
-                                                             double2 *__restrict__ y,
-                                                             const int *gate) {
+                                                             const double2 *__restrict__ z, long long c, long long n,
+                                                             double2 *__restrict__ y, const int *gate) {
   if (gated_off(gate)) return;
   const long long i = blockIdx.x;
   const double2 *row = blocks + i * n;
   double2 acc = make_double2(0, 0);
-  for (long long j = threadIdx.x; j < n; j += blockDim.x) {
-    double2 z = x[j];
-    if (pdiag) z = cdiv(z, pdiag[j]);
-    acc = cadd(acc, cmul(row[j], z));
-  }
+  for (long long j = threadIdx.x; j < n; j += blockDim.x) acc = cadd(acc, cmul(row[j], z[j]));
   acc = block_sum(acc);
   if (threadIdx.x == 0) y[i] = acc;
 }
 
-// One warp per volume row: y_{c+i} += sum_j D_ij z_j over the c conductor unknowns.
-__global__ void cross_rows_kernel(const double2 *__restrict__ D, const double2 *__restrict__ x,
-                                  const double2 *__restrict__ pdiag, long long c, long long v,
-                                  double2 *__restrict__ y, const int *gate) {
+// One warp per volume row: y_{c+i} += sum_j D_ij z_j over the c conductor
+// unknowns (dielectric_fft.c:67-74).
+__global__ void cross_rows_kernel(const double2 *__restrict__ D, const double2 *__restrict__ z, long long c,
+                                  long long v, double2 *__restrict__ y, const int *gate) {
   if (gated_off(gate)) return;
   const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= v) return;
   const double2 *row = D + warp * c;
   double2 acc = make_double2(0, 0);
-  for (long long j = lane; j < c; j += 32) {
-    double2 z = x[j];
-    if (pdiag) z = cdiv(z, pdiag[j]);
-    acc = cadd(acc, cmul(row[j], z));
-  }
+  for (long long j = lane; j < c; j += 32) acc = cadd(acc, cmul(row[j], z[j]));
   for (int o = 16; o > 0; o >>= 1) {
     acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
     acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
@@ -118,8 +117,9 @@ extern "C" int n2d_hybrid_create(n2d_hybrid **out, n2d_vie *vol, long long c, lo
   h->blocks = (double2 *)n2d_alloc((nblk ? nblk : 1) * sizeof(double2));
   h->pdiag = (double2 *)n2d_alloc((h->n ? h->n : 1) * sizeof(double2));
   h->partials = (double *)n2d_alloc(4096 * sizeof(double));
+  h->z = (double2 *)n2d_alloc((h->n ? h->n : 1) * sizeof(double2));
   h->ticket = (unsigned int *)n2d_alloc(64);
-  if (!h->blocks || !h->pdiag || !h->partials || !h->ticket || !n2d_memset(h->ticket, 0, 64)) {
+  if (!h->blocks || !h->pdiag || !h->partials || !h->z || !h->ticket || !n2d_memset(h->ticket, 0, 64)) {
     n2d_hybrid_destroy(h);
     return 0;
   }
@@ -131,7 +131,7 @@ extern "C" int n2d_hybrid_create(n2d_hybrid **out, n2d_vie *vol, long long c, lo
 extern "C" void n2d_hybrid_destroy(n2d_hybrid *h) {
   if (!h) return;
   n2c_gmres_work_free(h->gm_work);
-  n2d_free(h->blocks); n2d_free(h->pdiag); n2d_free(h->partials); n2d_free(h->ticket);
+  n2d_free(h->blocks); n2d_free(h->pdiag); n2d_free(h->partials); n2d_free(h->ticket); n2d_free(h->z);
   delete h;
 }
 
@@ -170,13 +170,15 @@ extern "C" int n2d_hybrid_apply(n2d_hybrid *h, const double *x, double *y, int p
                           full_precision))
     return 0;
   if (c) {
-    conductor_rows_kernel<<<(unsigned)c, 256, 0, n2c_stream()>>>(h->blocks, (const double2 *)x, pd, c,
-                                                                 n, (double2 *)y, n2c_gate());
+    const long long zb = (n + 255) / 256;
+    zc_kernel<<<(unsigned)(zb < 4096 ? zb : 4096), 256, 0, n2c_stream()>>>((const double2 *)x, pd, h->z, n,
+                                                                            n2c_gate());
+    conductor_rows_kernel<<<(unsigned)c, 256, 0, n2c_stream()>>>(h->blocks, h->z, c, n, (double2 *)y, n2c_gate());
     if (!n2c_check_launch("conductor_rows")) return 0;
     if (v) {
       const long long threads = v * 32;
-      cross_rows_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, n2c_stream()>>>(
-          h->blocks + c * n, (const double2 *)x, pd, c, v, (double2 *)y, n2c_gate());
+      cross_rows_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, n2c_stream()>>>(h->blocks + c * n, h->z, c, v,
+                                                                                      (double2 *)y, n2c_gate());
       if (!n2c_check_launch("cross_rows")) return 0;
     }
   }
