@@ -783,6 +783,7 @@ def volume_batch_bench(nb, torch, stream):
                 nb.last_error(), sorted(set((r.status, r.iterations) for r in reps))[:8]))
         sols[form] = x_dev.cpu().numpy()
         its = [r.iterations for r in reps]
+        schedule = batch.schedule()
         batch.close()
         bs = [torch.from_numpy(b).cuda() for b in rhs]
         x = torch.zeros(max(b.numel() for b in bs), dtype=torch.complex128, device="cuda")
@@ -800,7 +801,9 @@ def volume_batch_bench(nb, torch, stream):
             raise RuntimeError("per-system solve failed: " + nb.last_error())
         out[form] = {"one_batch": {"ms": ms, "solves_per_s": 1e3 * len(systems) / ms},
                      "one_call_per_system": {"ms": ms1, "solves_per_s": 1e3 * len(systems) / ms1},
-                     "iterations": {"min": int(min(its)), "max": int(max(its)), "mean": float(np.mean(its))}}
+                     "iterations": {"min": int(min(its)), "max": int(max(its)), "mean": float(np.mean(its))},
+                     "batch_schedule": {"passes": ["z fwd", "y fwd", "x product", "y inv", "z inv"],
+                                        "tile_scale_and_radix_variant": schedule}}
         for s in systems:
             s.close()
         for p in keep:

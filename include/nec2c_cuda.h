@@ -188,6 +188,14 @@ void nec2c_cuda_vie_batch_destroy(nec2c_cuda_vie_batch *batch);
    start at nec2c_cuda_vie_batch_offset(batch, q). */
 size_t nec2c_cuda_vie_batch_order(const nec2c_cuda_vie_batch *batch);
 size_t nec2c_cuda_vie_batch_offset(const nec2c_cuda_vie_batch *batch, size_t plan);
+/* Schedule of the batched FFT passes.  Per pass: scale[i] in -1..1 halves,
+   keeps or doubles the batch's tile height, and variant[i] 0/1 picks the
+   default or the transposed radix split.  With autotuning on,
+   nec2c_cuda_vie_batch_create times the candidates on the batch and keeps the
+   fastest.  set_schedule pins a schedule and returns 0 (schedule unchanged)
+   when it cannot be built. */
+int nec2c_cuda_vie_batch_schedule(const nec2c_cuda_vie_batch *batch, int scale[5], int variant[5]);
+int nec2c_cuda_vie_batch_set_schedule(nec2c_cuda_vie_batch *batch, const int scale[5], const int variant[5]);
 /* y = A x of every plan (vie_fft.c:239-263 per plan) on device vectors of the
    batch's order. */
 int nec2c_cuda_vie_batch_apply_device(nec2c_cuda_vie_batch *batch, const void *x_dev, void *y_dev);

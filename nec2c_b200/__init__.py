@@ -88,6 +88,8 @@ def load():
         "nec2c_cuda_vie_batch_order": (sz, [vp]),
         "nec2c_cuda_vie_batch_offset": (sz, [vp, sz]),
         "nec2c_cuda_vie_batch_apply_device": (i, [vp, vp, vp]),
+        "nec2c_cuda_vie_batch_schedule": (i, [vp, C.POINTER(i), C.POINTER(i)]),
+        "nec2c_cuda_vie_batch_set_schedule": (i, [vp, C.POINTER(i), C.POINTER(i)]),
         "nec2c_cuda_gmres_batch_device": (i, [vp, vp, vp, vp, vp]),
         "nec2c_cuda_gmres_batch": (i, [vp, C.POINTER(vp), C.POINTER(vp), vp, vp]),
         "nec2c_cuda_hybrid_create": (i, [C.POINTER(vp), vp, sz, sz, i]),
@@ -274,6 +276,17 @@ class VolumeBatch:
             self.h = None
 
     __del__ = close
+
+    def schedule(self):
+        """[(tile height scale, radix variant)] x 5 of the batched passes."""
+        sc, va = (C.c_int * 5)(), (C.c_int * 5)()
+        load().nec2c_cuda_vie_batch_schedule(self.h, sc, va)
+        return list(zip(sc, va))
+
+    def set_schedule(self, passes):
+        sc = (C.c_int * 5)(*[int(a) for a, _ in passes])
+        va = (C.c_int * 5)(*[int(b) for _, b in passes])
+        return bool(load().nec2c_cuda_vie_batch_set_schedule(self.h, sc, va))
 
     def split(self, v):
         return [v[self.offsets[q]:self.offsets[q + 1]] for q in range(len(self.plans))]

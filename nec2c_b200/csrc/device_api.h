@@ -144,6 +144,10 @@ long long n2d_vie_batch_offset(const n2d_vie_batch *b, long long q);
 /* y = A x of every plan (transform precision, no preconditioning), five
    launches in all. */
 int n2d_vie_batch_apply(n2d_vie_batch *b, const double *x_dev, double *y_dev);
+/* Schedule of the batched passes (tile height scale -1..1 and radix split 0/1
+   per pass), chosen by the batch tuner at creation; pinning rebuilds it. */
+void n2d_vie_batch_schedule(const n2d_vie_batch *b, int *scale, int *variant);
+int n2d_vie_batch_set_schedule(n2d_vie_batch *b, const int *scale, const int *variant);
 /* GMRES(restart <= 30) on every plan in lockstep; reports[q] per system.
    Returns 1 when every system converged. */
 int n2d_gmres_batch_dev(n2d_vie_batch *b, const double *b_dev, double *x_dev, size_t restart,

@@ -985,32 +985,47 @@ extern "C" int n2d_vie_precondition(n2d_vie *p, const double *x, double *y) {
 // passes and 2048 in the x product pass (within 48 KB of shared memory), and
 // the default z tile of 56 KB (whole lattice columns).  Small plans then
 // give each thread several butterflies instead of leaving threads idle.
-static int batch_height(const n2d_vie *p, int pass, size_t elem) {
+// scale -1 / +1 halves / doubles that height (within the kernels' limits:
+// whole lattice columns up to 96 lines, powers of two up to 64 lines, 100 KB
+// of shared memory); the batch tuner picks the scale per pass.
+static int batch_height(const n2d_vie *p, int pass, size_t elem, int scale) {
   const int L = pass_length(p, pass);
-  if (pass == 0 || pass == 4) return zlines_per_tile(L, elem, 3);
+  if (pass == 0 || pass == 4) {
+    const int h = zlines_per_tile(L, elem, 3);
+    int nl = scale < 0 ? h / 2 : scale > 0 ? 2 * h : h;
+    nl = nl / 3 * 3;
+    if (nl < 3) nl = 3;
+    if (nl > 96) nl = 96;
+    while (nl > 3 && (size_t)2 * (nl + 1) * L * elem > 100 * 1024) nl -= 3;
+    return scale == 0 ? h : nl;
+  }
   const size_t ncomp = pass == 2 ? 3 : 1;
   const long long target = pass == 2 ? 2048 : 4096;
   int nl = 1;
   while ((long long)nl * 2 * L <= target && (size_t)nl * 2 * L * ncomp * elem <= 48 * 1024) nl *= 2;
+  if (scale < 0 && nl > 1) nl /= 2;
+  if (scale > 0 && nl < 64 && (size_t)2 * nl * L * ncomp * elem <= 100 * 1024) nl *= 2;
   return nl;
 }
 
 template <typename C>
-int n2c_vie_pass_plans(n2d_vie *p, int precondition, double *norm, int *flag, PassArgs<C> args[5], int mode[5],
-                       int L[5], size_t smem[5], long long tiles[5]) {
+int n2c_vie_pass_plans(n2d_vie *p, int precondition, double *norm, int *flag, const int *scale, const int *variant,
+                       PassArgs<C> args[5], int mode[5], int L[5], int var[5], size_t smem[5], long long tiles[5]) {
   for (int i = 0; i < N2D_VIE_PASSES; ++i) {
     PassPlan<C> pp;
-    const n2d_pass_choice ch = {batch_height(p, i, sizeof(C)), 0};
+    const int v = variant && variant[i] && fft_radix_variants(pass_length(p, i)) > 1 ? 1 : 0;
+    const n2d_pass_choice ch = {batch_height(p, i, sizeof(C), scale ? scale[i] : 0), v};
     if (!pass_plan<C>(p, i, ch, nullptr, nullptr, precondition, norm, flag, &pp)) return 0;
     args[i] = pp.a;
     mode[i] = pp.mode;
     L[i] = pp.L;
+    var[i] = v;
     smem[i] = pp.smem;
     tiles[i] = pp.tiles;
   }
   return 1;
 }
-template int n2c_vie_pass_plans<float2>(n2d_vie *, int, double *, int *, PassArgs<float2> *, int *, int *, size_t *,
-                                        long long *);
-template int n2c_vie_pass_plans<double2>(n2d_vie *, int, double *, int *, PassArgs<double2> *, int *, int *,
-                                         size_t *, long long *);
+template int n2c_vie_pass_plans<float2>(n2d_vie *, int, double *, int *, const int *, const int *,
+                                        PassArgs<float2> *, int *, int *, int *, size_t *, long long *);
+template int n2c_vie_pass_plans<double2>(n2d_vie *, int, double *, int *, const int *, const int *,
+                                         PassArgs<double2> *, int *, int *, int *, size_t *, long long *);

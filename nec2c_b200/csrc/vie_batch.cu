@@ -61,6 +61,7 @@ template <typename C> struct BatchDesc {
   PassArgs<C> a;
   long long off;   // first element of the plan's cell vector in the batch vectors
   int L;           // line length of the pass
+  int variant;     // radix split (fft_passes.cuh): 0 default, 1 transposed
 };
 
 // Conductor blocks of a hybrid system: the c rows [C|B] (c x n) then the
@@ -147,6 +148,15 @@ __global__ void __launch_bounds__(256, MODE <= 1 ? 1 : 3)
   }
   const long long tile = (long long)blockIdx.x - first[q];
   const unsigned ntiles = (unsigned)(first[q + 1] - first[q]);
+  if (desc[q].variant) {
+    switch (desc[q].L) {
+      case 16: tile_body<C, 4, 4, MODE>(a, tile, ntiles); break;
+      case 32: tile_body<C, 4, 8, MODE>(a, tile, ntiles); break;
+      case 64: tile_body<C, 16, 4, MODE>(a, tile, ntiles); break;
+      case 128: tile_body<C, 8, 16, MODE>(a, tile, ntiles); break;
+    }
+    return;
+  }
   switch (desc[q].L) {
     case 1: tile_body<C, 1, 1, MODE>(a, tile, ntiles); break;
     case 2: tile_body<C, 2, 1, MODE>(a, tile, ntiles); break;
@@ -635,6 +645,8 @@ struct n2d_vie_batch {
   BSys *sys = nullptr;
   const double2 **diag_dev = nullptr;
   PassSet sets[3][N2D_VIE_PASSES];
+  int scale[N2D_VIE_PASSES] = {0, 0, 0, 0, 0};     // tile height scale per pass (batch tuner)
+  int variant[N2D_VIE_PASSES] = {0, 0, 0, 0, 0};   // radix split per pass (batch tuner)
   BatchWork *work = nullptr;
 };
 
@@ -648,14 +660,18 @@ static void work_free(BatchWork *w) {
   delete w;
 }
 
+static void free_set(n2d_vie_batch *b, int set) {
+  for (PassSet &ps : b->sets[set]) {
+    n2d_free(ps.desc);
+    n2d_free(ps.first);
+    ps = PassSet();
+  }
+}
+
 extern "C" void n2d_vie_batch_destroy(n2d_vie_batch *b) {
   if (!b) return;
   work_free(b->work);
-  for (auto &set : b->sets)
-    for (PassSet &ps : set) {
-      n2d_free(ps.desc);
-      n2d_free(ps.first);
-    }
+  for (int set = 0; set < 3; ++set) free_set(b, set);
   n2d_free(b->off_dev);
   n2d_free(b->first_d_dev);
   n2d_free(b->first_v_dev);
@@ -680,18 +696,21 @@ static int build_set(n2d_vie_batch *b, int set) {
   for (int q = 0; q < K; ++q) {
     BSys *s = b->sys + q;
     PassArgs<C> args[N2D_VIE_PASSES];
-    int mode[N2D_VIE_PASSES], L[N2D_VIE_PASSES];
+    int mode[N2D_VIE_PASSES], L[N2D_VIE_PASSES], var[N2D_VIE_PASSES];
     size_t smem[N2D_VIE_PASSES];
     long long tiles[N2D_VIE_PASSES];
     const int precondition = set == 0;
     double *norm = set == 0 && !b->any_hybrid ? &s->before_sq : nullptr;
     int *flag = set == 0 ? &s->flag : set == 1 ? &s->rflag : nullptr;
-    if (!n2c_vie_pass_plans<C>(b->plans[q], precondition, norm, flag, args, mode, L, smem, tiles)) return 0;
+    if (!n2c_vie_pass_plans<C>(b->plans[q], precondition, norm, flag, b->scale, b->variant, args, mode, L, var, smem,
+                               tiles))
+      return 0;
     for (int i = 0; i < N2D_VIE_PASSES; ++i) {
       args[i].gate = set == 0 ? &s->active : set == 1 ? &s->running : nullptr;
       desc[i][q].a = args[i];
       desc[i][q].off = b->off[q] + b->cond[q];
       desc[i][q].L = L[i];
+      desc[i][q].variant = var[i];
       first[i][q + 1] = first[i][q] + tiles[i];
       PassSet &ps = b->sets[set][i];
       ps.mode = mode[i];
@@ -752,6 +771,63 @@ static int batch_apply(const n2d_vie_batch *b, int set, const double2 *x, double
     if (!n2c_check_launch("batched norm of w")) return 0;
   }
   return 1;
+}
+
+// Batch tuner: per pass, the tile height scale (-1, 0, +1 of the batch
+// height) and the radix split, timed on the plain products of this batch
+// (CUDA events, best of two runs of three launches after a warm-up); a
+// candidate replaces the incumbent only when it is at least 3% faster.
+// Scale -1 is not tried for the z epilogue, whose norm reduction must keep
+// within 65,536 tiles per plan.
+static int tune_batch(n2d_vie_batch *b) {
+  double2 *x = (double2 *)n2d_alloc(b->N * sizeof(double2)), *y = (double2 *)n2d_alloc(b->N * sizeof(double2));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int ok = x && y && n2d_memset(x, 0, b->N * sizeof(double2)) && cudaEventCreate(&e0) == cudaSuccess &&
+           cudaEventCreate(&e1) == cudaSuccess;
+  auto rebuild = [&]() {
+    free_set(b, 2);
+    return b->fp32 ? build_set<float2>(b, 2) : build_set<double2>(b, 2);
+  };
+  auto time_pass = [&](int i) -> float {
+    const PassSet &ps = b->sets[2][i];
+    auto launch = [&]() { return ps.fp32 ? launch_set_t<float2>(b, ps, x, y) : launch_set_t<double2>(b, ps, x, y); };
+    if (!launch()) return -1.0f;
+    float best = -1.0f;
+    for (int trial = 0; trial < 2; ++trial) {
+      if (cudaEventRecord(e0, n2c_stream()) != cudaSuccess) return -1.0f;
+      for (int r = 0; r < 3; ++r)
+        if (!launch()) return -1.0f;
+      float ms = 0;
+      if (cudaEventRecord(e1, n2c_stream()) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+        return -1.0f;
+      if (best < 0 || ms < best) best = ms;
+    }
+    return best;
+  };
+  for (int i = 0; i < N2D_VIE_PASSES && ok; ++i) {
+    float bt = time_pass(i);
+    if (bt < 0) { ok = 0; break; }
+    const int cand[5][2] = {{-1, 0}, {1, 0}, {0, 1}, {-1, 1}, {1, 1}};
+    int best_s = 0, best_v = 0;
+    for (const auto &c : cand) {
+      if (i == 4 && c[0] < 0) continue;
+      b->scale[i] = c[0];
+      b->variant[i] = c[1];
+      if (!rebuild()) { ok = 0; break; }
+      const float t = time_pass(i);
+      if (t >= 0 && t < 0.97f * bt) { bt = t; best_s = c[0]; best_v = c[1]; }
+    }
+    b->scale[i] = best_s;
+    b->variant[i] = best_v;
+    if (ok) ok = rebuild();
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaGetLastError();
+  n2d_free(x);
+  n2d_free(y);
+  return ok;
 }
 
 static int batch_create(n2d_vie_batch **out, n2d_vie *const *plans, n2d_hybrid *const *hybrids,
@@ -830,9 +906,10 @@ static int batch_create(n2d_vie_batch **out, n2d_vie *const *plans, n2d_hybrid *
            n2d_upload(b->hyb_dev, hyb.data(), count * sizeof(BHyb)) &&
            n2d_upload((void *)b->diag_dev, diag.data(), count * sizeof(double2 *)) &&
            n2d_memset(b->sys, 0, count * sizeof(BSys));
+  if (ok) ok = b->fp32 ? build_set<float2>(b, 2) : build_set<double2>(b, 2);
+  if (ok && n2d_vie_autotune_enabled()) ok = tune_batch(b);
   if (ok) ok = b->fp32 ? build_set<float2>(b, 0) : build_set<double2>(b, 0);
   if (ok) ok = build_set<double2>(b, 1);
-  if (ok) ok = b->fp32 ? build_set<float2>(b, 2) : build_set<double2>(b, 2);
   if (!ok || !n2d_sync()) { n2d_vie_batch_destroy(b); return 0; }
   *out = b;
   return 1;
@@ -844,6 +921,47 @@ extern "C" int n2d_vie_batch_create(n2d_vie_batch **out, n2d_vie *const *plans, 
 
 extern "C" int n2d_hybrid_batch_create(n2d_vie_batch **out, n2d_hybrid *const *systems, long long count) {
   return batch_create(out, nullptr, systems, count);
+}
+
+// Schedule of the batched passes: tile height scale and radix split per pass.
+extern "C" void n2d_vie_batch_schedule(const n2d_vie_batch *b, int *scale, int *variant) {
+  for (int i = 0; i < N2D_VIE_PASSES; ++i) {
+    scale[i] = b->scale[i];
+    variant[i] = b->variant[i];
+  }
+}
+
+// Pins the schedule (scale in -1..1, variant 0 or 1 per pass) and rebuilds the
+// descriptor sets; the batch is left as it was when a set cannot be built.
+extern "C" int n2d_vie_batch_set_schedule(n2d_vie_batch *b, const int *scale, const int *variant) {
+  int old_s[N2D_VIE_PASSES], old_v[N2D_VIE_PASSES];
+  for (int i = 0; i < N2D_VIE_PASSES; ++i) {
+    if (scale[i] < -1 || scale[i] > 1 || variant[i] < 0 || variant[i] > 1) {
+      n2c_set_error("batch schedule of pass %d out of range", i);
+      return 0;
+    }
+    old_s[i] = b->scale[i];
+    old_v[i] = b->variant[i];
+  }
+  auto build_all = [&]() {
+    for (int set = 0; set < 3; ++set) free_set(b, set);
+    return (b->fp32 ? build_set<float2>(b, 0) : build_set<double2>(b, 0)) && build_set<double2>(b, 1) &&
+           (b->fp32 ? build_set<float2>(b, 2) : build_set<double2>(b, 2));
+  };
+  for (int i = 0; i < N2D_VIE_PASSES; ++i) {
+    b->scale[i] = scale[i];
+    b->variant[i] = variant[i];
+  }
+  // Captured cycles bake the tile grids into their launches.
+  work_free(b->work);
+  b->work = nullptr;
+  if (build_all()) return 1;
+  for (int i = 0; i < N2D_VIE_PASSES; ++i) {
+    b->scale[i] = old_s[i];
+    b->variant[i] = old_v[i];
+  }
+  build_all();
+  return 0;
 }
 
 extern "C" long long n2d_vie_batch_order(const n2d_vie_batch *b) { return b ? b->N : 0; }

@@ -568,6 +568,19 @@ size_t nec2c_cuda_vie_batch_offset(const nec2c_cuda_vie_batch *b, size_t q)
   return b && q <= b->count ? b->offsets[q] : 0;
 }
 
+int nec2c_cuda_vie_batch_schedule(const nec2c_cuda_vie_batch *b, int scale[5], int variant[5])
+{
+  if(!b || !scale || !variant) return 0;
+  n2d_vie_batch_schedule(b->dev, scale, variant);
+  return 1;
+}
+
+int nec2c_cuda_vie_batch_set_schedule(nec2c_cuda_vie_batch *b, const int scale[5], const int variant[5])
+{
+  if(!b || !scale || !variant) { n2c_set_error("batch schedule: bad argument"); return 0; }
+  return n2d_vie_batch_set_schedule(b->dev, scale, variant);
+}
+
 int nec2c_cuda_vie_batch_apply_device(nec2c_cuda_vie_batch *b, const void *x_dev, void *y_dev)
 {
   if(!b || !x_dev || !y_dev || x_dev == y_dev) return 0;

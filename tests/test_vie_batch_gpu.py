@@ -2,8 +2,9 @@
 
 The batched product runs the same tile bodies as a single plan's product, on
 taller tiles and inlined into other kernels (the compiler may fuse a
-multiply-add differently), so with the plans on the default radix split each
-plan's slice of the batched product equals its own product to rounding (1e-14 of the largest entry in
+multiply-add differently), so each plan's slice of the batched product, under
+the tuned and under every pinned batch schedule, equals the plan's own
+product (default radix split) to rounding (1e-14 of the largest entry in
 FP64, 1e-6 with FP32 transforms), and the FP64 form matches the oracle to
 1e-12 relative to the largest entry.  Batched GMRES
 solves each system with vie_gmres's per-system semantics: every system's
@@ -67,16 +68,28 @@ def test_batched_product_equals_each_plan(near_tables, mixed):
     yd = torch.zeros_like(xd)
     assert nb.load().nec2c_cuda_vie_batch_apply_device(batch.h, C.c_void_p(xd.data_ptr()),
                                                        C.c_void_p(yd.data_ptr())), nb.last_error()
-    y = yd.cpu().numpy()
-    for q, (p, op) in enumerate(zip(plans, oracles)):
-        xs = x[batch.offsets[q]:batch.offsets[q + 1]]
-        ys = y[batch.offsets[q]:batch.offsets[q + 1]]
-        assert rel_max(ys, p.apply(xs)) < (1e-6 if mixed else 1e-14), q
-        ref = op.apply(xs)
-        if mixed:
-            assert rel_l2(ys, ref) < 1e-5
-        else:
-            assert rel_max(ys, ref) < 1e-12
+    own = [p.apply(x[batch.offsets[q]:batch.offsets[q + 1]]) for q, p in enumerate(plans)]
+    tuned = batch.schedule()
+    assert all(-1 <= a <= 1 and b in (0, 1) for a, b in tuned)
+    # The tuned schedule, then every height scale and radix split pinned.
+    for sched in (tuned, [(0, 1)] * 5, [(-1, 0)] * 4 + [(0, 0)], [(1, 1)] * 5, [(-1, 1)] * 4 + [(1, 0)]):
+        assert batch.set_schedule(sched), nb.last_error()
+        assert batch.schedule() == list(sched)
+        yd.zero_()
+        assert nb.load().nec2c_cuda_vie_batch_apply_device(batch.h, C.c_void_p(xd.data_ptr()),
+                                                           C.c_void_p(yd.data_ptr())), nb.last_error()
+        y = yd.cpu().numpy()
+        for q, (p, op) in enumerate(zip(plans, oracles)):
+            xs = x[batch.offsets[q]:batch.offsets[q + 1]]
+            ys = y[batch.offsets[q]:batch.offsets[q + 1]]
+            assert rel_max(ys, own[q]) < (1e-6 if mixed else 1e-14), (q, sched)
+            ref = op.apply(xs)
+            if mixed:
+                assert rel_l2(ys, ref) < 1e-5
+            else:
+                assert rel_max(ys, ref) < 1e-12
+    assert not batch.set_schedule([(2, 0)] * 5)       # out of range: refused, schedule kept
+    assert batch.schedule() == [(-1, 1)] * 4 + [(1, 0)]
     batch.close()
 
 
