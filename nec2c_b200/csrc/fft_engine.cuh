@@ -386,8 +386,10 @@ __device__ __forceinline__ void fft_product_tile(const PassArgs<C> &a, long long
     }
   }
 }
+// Three CTAs per SM in FP32; two in FP64, whose three components of R2
+// complex values per thread would otherwise spill.
 template <typename C, int R1, int R2>
-__global__ void __launch_bounds__(256, 3) fft_product_pass(PassArgs<C> a) {
+__global__ void __launch_bounds__(256, sizeof(C) == sizeof(float2) ? 3 : 2) fft_product_pass(PassArgs<C> a) {
   fft_product_tile<C, R1, R2>(a, blockIdx.x);
 }
 

@@ -422,21 +422,34 @@ __global__ void cycle_start_kernel(GmBuffers b, long long n, int m, double beta)
   for (long long i = tid; i <= m; i += stride) b.g[i] = make_double2(i == 0 ? beta : 0, 0);
 }
 
-// y = H^{-1} g (back substitution, vie_iterative.c:179-186).
+// y = H^{-1} g (back substitution, vie_iterative.c:179-186), one warp: the
+// lanes share each row's sum over the solved unknowns, added in a fixed
+// order (lane partials, then a butterfly).
 __global__ void backsolve_kernel(GmBuffers b, int m) {
   GmState *st = b.st;
   if (st->status != ST_RUNNING) return;
-  const int used = st->used;
+  const int used = st->used, lane = threadIdx.x;
+  __shared__ int broke;
+  if (lane == 0) broke = 0;
+  __syncwarp();
   for (int i = used - 1; i >= 0; --i) {
-    double2 val = b.g[i];
-    for (int k = i + 1; k < used; ++k) val = csub(val, cmul(b.H[(long long)i * m + k], b.y[k]));
-    const double2 d = b.H[(long long)i * m + i];
-    if (cabs_(d) == 0.0) { st->status = ST_BREAKDOWN; return; }
-    b.y[i] = cdiv(val, d);
+    double2 part = make_double2(0, 0);
+    for (int k = i + 1 + lane; k < used; k += 32) part = cadd(part, cmul(b.H[(long long)i * m + k], b.y[k]));
+    for (int o = 16; o > 0; o >>= 1) {
+      part.x += __shfl_xor_sync(0xffffffffu, part.x, o);
+      part.y += __shfl_xor_sync(0xffffffffu, part.y, o);
+    }
+    if (lane == 0) {
+      const double2 d = b.H[(long long)i * m + i];
+      if (cabs_(d) == 0.0) { st->status = ST_BREAKDOWN; broke = 1; }
+      else b.y[i] = cdiv(csub(b.g[i], part), d);
+    }
+    __syncwarp();
+    if (broke) return;
   }
 }
 
-// x += D^-1 (sum_j v_j y_j).
+// x += D^-1 (sum_j v_j y_j): the divisor is applied once to the sum.
 __global__ void update_kernel(GmBuffers b, const double2 *__restrict__ pdiag, double2 *__restrict__ x,
                               long long n) {
   if (b.st->status != ST_RUNNING) return;
@@ -444,11 +457,8 @@ __global__ void update_kernel(GmBuffers b, const double2 *__restrict__ pdiag, do
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     double2 acc = make_double2(0, 0);
-    for (int j = 0; j < used; ++j) {
-      double2 z = b.V[(long long)j * n + i];
-      if (pdiag) z = cdiv(z, pdiag[i]);
-      acc = cadd(acc, cmul(z, b.y[j]));
-    }
+    for (int j = 0; j < used; ++j) acc = cadd(acc, cmul(b.V[(long long)j * n + i], b.y[j]));
+    if (pdiag) acc = cdiv(acc, pdiag[i]);
     x[i] = cadd(x[i], acc);
   }
 }
@@ -721,7 +731,7 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
       launch_fail = !enqueue_inner(o, w);
     }
     if (launch_fail) { rep->status = ST_CALLBACK; break; }
-    backsolve_kernel<<<1, 1, 0, n2c_stream()>>>(b, (int)m);
+    backsolve_kernel<<<1, 32, 0, n2c_stream()>>>(b, (int)m);
     if (!n2c_check_launch("backsolve")) break;
     update_kernel<<<grid1(n), 256, 0, n2c_stream()>>>(b, o.pdiag, x_dev, n);
     if (!n2c_check_launch("update")) break;

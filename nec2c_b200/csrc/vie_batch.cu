@@ -135,7 +135,7 @@ __device__ __forceinline__ void tile_body(const PassArgs<C> &a, long long tile, 
 // One pass over the tiles of every plan; x / y are the batch vectors the z
 // passes scatter from and gather into.
 template <typename C, int MODE>
-__global__ void __launch_bounds__(256, MODE <= 1 ? 1 : 3)
+__global__ void __launch_bounds__(256, MODE <= 1 ? 1 : (MODE == 2 && sizeof(C) != sizeof(float2) ? 2 : 3))
     batch_pass_kernel(const BatchDesc<C> *desc, const long long *first, int count, const double2 *x, double2 *y) {
   const int q = find_seg(first, count, blockIdx.x);
   // A stopped system's tiles leave before its arguments are read.
@@ -562,10 +562,11 @@ __global__ void count_active_kernel(BView v, int *out) {
   }
 }
 
-// y = H^{-1} g of every running system (vie_iterative.c:179-186), one thread
-// per system.
+// y = H^{-1} g of every running system (vie_iterative.c:179-186), one warp
+// per system: the lanes share each row's sum over the solved unknowns, added
+// in a fixed order (lane partials, then a butterfly).
 __global__ void seg_backsolve_kernel(BView v) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (q >= v.K) return;
   BSys *s = v.sys + q;
   if (s->status != ST_RUNNING) return;
@@ -573,15 +574,24 @@ __global__ void seg_backsolve_kernel(BView v) {
   const double2 *H = v.H + (long long)q * (m + 1) * m, *g = v.g + (long long)q * (m + 1);
   double2 *y = v.y + (long long)q * m;
   for (int i = used - 1; i >= 0; --i) {
-    double2 val = g[i];
-    for (int k = i + 1; k < used; ++k) val = csub(val, cmul(H[(long long)i * m + k], y[k]));
+    double2 part = make_double2(0, 0);
+    for (int k = i + 1 + lane; k < used; k += 32) part = cadd(part, cmul(H[(long long)i * m + k], y[k]));
+    for (int o = 16; o > 0; o >>= 1) {
+      part.x += __shfl_xor_sync(0xffffffffu, part.x, o);
+      part.y += __shfl_xor_sync(0xffffffffu, part.y, o);
+    }
     const double2 d = H[(long long)i * m + i];
-    if (cabs_(d) == 0.0) { s->status = ST_BREAKDOWN; return; }
-    y[i] = cdiv(val, d);
+    if (cabs_(d) == 0.0) {
+      if (lane == 0) s->status = ST_BREAKDOWN;
+      return;
+    }
+    if (lane == 0) y[i] = cdiv(csub(g[i], part), d);
+    __syncwarp();
   }
 }
 
-// x += D^-1 (sum_j v_j y_j) of every running system.
+// x += D^-1 (sum_j v_j y_j) of every running system, the divisor applied
+// once to the sum.
 __global__ void __launch_bounds__(VEC_THREADS) seg_xupdate_kernel(BView v, double2 *x) {
   const VecCta c = vec_cta(v);
   const BSys *s = v.sys + c.q;
@@ -591,11 +601,8 @@ __global__ void __launch_bounds__(VEC_THREADS) seg_xupdate_kernel(BView v, doubl
   const long long base = v.off[c.q];
   for (long long i = c.lo + threadIdx.x; i < c.hi; i += VEC_THREADS) {
     double2 acc = make_double2(0, 0);
-    for (int jj = 0; jj < used; ++jj) {
-      const double2 z = cdiv(v.V[(long long)jj * v.N + i], diag[i - base]);
-      acc = cadd(acc, cmul(z, y[jj]));
-    }
-    x[i] = cadd(x[i], acc);
+    for (int jj = 0; jj < used; ++jj) acc = cadd(acc, cmul(v.V[(long long)jj * v.N + i], y[jj]));
+    x[i] = cadd(x[i], cdiv(acc, diag[i - base]));
   }
 }
 
@@ -1179,7 +1186,7 @@ extern "C" int n2d_gmres_batch_dev(n2d_vie_batch *b, const double *b_dev, double
       if (!n2d_download(&still, w->active_count, sizeof(int))) return 0;
       if (!still) break;
     }
-    seg_backsolve_kernel<<<(K + 127) / 128, 128, 0, n2c_stream()>>>(v);
+    seg_backsolve_kernel<<<(K + 3) / 4, 128, 0, n2c_stream()>>>(v);
     seg_xupdate_kernel<<<nv, VEC_THREADS, 0, n2c_stream()>>>(v, x);
     if (!n2c_check_launch("batched solution update") || !get()) return 0;
     std::vector<char> cycled(K, 0);
