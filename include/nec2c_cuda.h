@@ -81,6 +81,18 @@ int nec2c_cuda_vie_fft_apply_device(nec2c_cuda_vie_plan *plan, const void *x_dev
    order xx yy zz xy xz yz, each scaled by 1/grid (validation hook). */
 int nec2c_cuda_vie_fft_spectrum(nec2c_cuda_vie_plan *plan, nec2c_cuda_complex *out);
 
+/* Far-field radiation amplitude of a volume polarisation current in free
+   space, the volume term of dielectric_radiation_amplitude
+   (dielectric_solver.c:90-150): for each unit direction d (3 doubles each,
+   host), amplitude = i k c0 mu0 / (4 pi) ((I x d) x d) with
+   I = sum over cells of J_cell h^3 prod_a sinc(k d_a h / 2) exp(+i k d.r_cell),
+   r_cell = origin + h x the cell's lattice index (h, k: the plan's pitch and
+   wavenumber).  current_dev holds 3 x cells complex values on the device (a
+   solve's x); amplitude receives 3 complex values per direction (host).  Not
+   for plans with PEC images (the ground terms are not built). */
+int nec2c_cuda_vie_fft_radiation_device(nec2c_cuda_vie_plan *plan, const double origin[3], const void *current_dev,
+                                        size_t count, const double *directions, nec2c_cuda_complex *amplitude);
+
 /* FFT pass schedule.  A product runs five line-FFT passes: 0 z forward with
    the cell scatter, 1 y forward, 2 x forward + Green-tensor product + x
    inverse, 3 y inverse, 4 z inverse with the permittivity epilogue.  Each has

@@ -77,6 +77,7 @@ def load():
         "nec2c_cuda_vie_fft_precondition": (i, [vp, vp, vp]),
         "nec2c_cuda_vie_fft_apply_device": (i, [vp, vp, vp]),
         "nec2c_cuda_vie_fft_spectrum": (i, [vp, vp]),
+        "nec2c_cuda_vie_fft_radiation_device": (i, [vp, C.POINTER(dbl), vp, sz, vp, vp]),
         "nec2c_cuda_vie_fft_autotune": (None, [i]),
         "nec2c_cuda_vie_fft_autotune_enabled": (i, []),
         "nec2c_cuda_vie_fft_tune": (i, [vp, i]),
@@ -213,6 +214,19 @@ class VolumePlan:
         out = np.empty(6 * grid, dtype=np.complex128)
         if not load().nec2c_cuda_vie_fft_spectrum(self.h, _ptr(out)):
             raise RuntimeError("spectrum failed: " + last_error())
+        return out
+
+    def radiation(self, current, directions, origin=(0.0, 0.0, 0.0)):
+        """Far-field amplitudes (count x 3) of the cell current (3 x cells)
+        towards unit directions (count x 3)."""
+        import torch
+        cur = torch.from_numpy(_cvec(current)).cuda()
+        dirs = np.ascontiguousarray(directions, dtype=np.float64).reshape(-1, 3)
+        out = np.empty((dirs.shape[0], 3), dtype=np.complex128)
+        org = (C.c_double * 3)(*origin)
+        if not load().nec2c_cuda_vie_fft_radiation_device(self.h, org, C.c_void_p(cur.data_ptr()), dirs.shape[0],
+                                                          _ptr(dirs), _ptr(out)):
+            raise RuntimeError("radiation failed: " + last_error())
         return out
 
     def tune(self, measure=1):

@@ -94,6 +94,12 @@ void n2d_vie_set_mirror(n2d_vie *p, long long physical_cells);
 int n2d_vie_tune(n2d_vie *p, int measure);
 void n2d_vie_autotune(int enable);
 int n2d_vie_autotune_enabled(void);
+/* Far-field radiation amplitude (dielectric_solver.c:90-150, free space) of
+   the cell current current_dev (3 per cell) for count directions dirs_dev
+   (3 per direction) into out_dev (3 complex per direction); cell centres are
+   origin + h x lattice index. */
+int n2d_vie_radiation(n2d_vie *p, const double *current_dev, const double origin[3], double h, double k0,
+                      const double *dirs_dev, long long count, double *out_dev);
 /* Lines per tile and R1 (R2 = L / R1) of each pass for precision prec
    (0 FP32, 1 FP64); returns 1 when the schedule was measured. */
 int n2d_vie_schedule(n2d_vie *p, int prec, int *tiles, int *r1);

@@ -1008,6 +1008,103 @@ static int batch_height(const n2d_vie *p, int pass, size_t elem, int scale) {
   return nl;
 }
 
+// ------------------------------------------------------------ far field
+// Radiation amplitude of the volume polarisation current in free space
+// (dielectric_solver.c:90-150): for direction d,
+//   integral = V prod_a sinc(k d_a h / 2) sum_cells J_cell exp(+i k d.r_cell),
+//   amplitude = i k c0 mu0 / (4 pi) ((integral x d) x d),
+// with r_cell = origin + h (ix, iy, iz) from the cell's lattice index.  A CTA
+// takes RAD_DIRS directions and sums over all cells in a fixed order.
+constexpr int RAD_DIRS = 4;
+
+__device__ __forceinline__ double sinc_small(double x) {
+  if (fabs(x) < 1.0e-5) { const double x2 = x * x; return 1.0 - x2 / 6.0 + x2 * x2 / 120.0; }
+  return sin(x) / x;
+}
+
+__global__ void __launch_bounds__(256) radiation_kernel(const double2 *__restrict__ J, const int *__restrict__ cell_box,
+                                                        long long cells, long long ny, long long nz, double ox,
+                                                        double oy, double oz, double h, double k0,
+                                                        const double *__restrict__ dirs, int count,
+                                                        double2 *__restrict__ out) {
+  const int d0 = blockIdx.x * RAD_DIRS;
+  double dx[RAD_DIRS], dy[RAD_DIRS], dz[RAD_DIRS];
+#pragma unroll
+  for (int r = 0; r < RAD_DIRS; ++r) {
+    const int d = d0 + r < count ? d0 + r : count - 1;
+    dx[r] = dirs[3 * d]; dy[r] = dirs[3 * d + 1]; dz[r] = dirs[3 * d + 2];
+  }
+  double2 acc[RAD_DIRS][3];
+#pragma unroll
+  for (int r = 0; r < RAD_DIRS; ++r)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) acc[r][a] = make_double2(0, 0);
+  const long long nyz = ny * nz;
+  for (long long c = threadIdx.x; c < cells; c += blockDim.x) {
+    const long long box = cell_box[c], ix = box / nyz, rem = box - ix * nyz, iy = rem / nz, iz = rem - iy * nz;
+    const double x = ox + h * (double)ix, y = oy + h * (double)iy, z = oz + h * (double)iz;
+    const double2 j0 = J[3 * c], j1 = J[3 * c + 1], j2 = J[3 * c + 2];
+#pragma unroll
+    for (int r = 0; r < RAD_DIRS; ++r) {
+      double sn, cs;
+      sincos(k0 * (dx[r] * x + dy[r] * y + dz[r] * z), &sn, &cs);
+      const double2 e = make_double2(cs, sn);
+      acc[r][0] = cadd(acc[r][0], cmul(j0, e));
+      acc[r][1] = cadd(acc[r][1], cmul(j1, e));
+      acc[r][2] = cadd(acc[r][2], cmul(j2, e));
+    }
+  }
+  __shared__ double2 red[8][RAD_DIRS * 3];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int r = 0; r < RAD_DIRS; ++r)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      double2 v = acc[r][a];
+      for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+      }
+      if (lane == 0) red[warp][r * 3 + a] = v;
+    }
+  __syncthreads();
+  if (threadIdx.x >= RAD_DIRS || d0 + (int)threadIdx.x >= count) return;
+  const int r = threadIdx.x, d = d0 + r;
+  double2 in[3];
+  for (int a = 0; a < 3; ++a) {
+    double2 t = make_double2(0, 0);
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = cadd(t, red[w][r * 3 + a]);
+    in[a] = t;
+  }
+  const double dir[3] = {dx[r], dy[r], dz[r]};
+  double scale = h * h * h;
+  for (int a = 0; a < 3; ++a) scale *= sinc_small(0.5 * k0 * dir[a] * h);
+  for (int a = 0; a < 3; ++a) in[a] = cscale(in[a], scale);
+  const double2 cr0 = csub(cscale(in[1], dir[2]), cscale(in[2], dir[1]));
+  const double2 cr1 = csub(cscale(in[2], dir[0]), cscale(in[0], dir[2]));
+  const double2 cr2 = csub(cscale(in[0], dir[1]), cscale(in[1], dir[0]));
+  double2 t[3];
+  t[0] = csub(cscale(cr1, dir[2]), cscale(cr2, dir[1]));
+  t[1] = csub(cscale(cr2, dir[0]), cscale(cr0, dir[2]));
+  t[2] = csub(cscale(cr0, dir[1]), cscale(cr1, dir[0]));
+  const double f = k0 * 299792458.0 * 1.25663706212e-6 / (4.0 * 3.141592653589793238462643383279502884);
+  for (int a = 0; a < 3; ++a) out[3 * d + a] = make_double2(-f * t[a].y, f * t[a].x);   // i f t
+}
+
+// Amplitudes of count directions (dirs: 3 per direction, device) of the
+// current J_dev (3 per physical cell) into out_dev (3 per direction).
+extern "C" int n2d_vie_radiation(n2d_vie *p, const double *current_dev, const double origin[3], double h,
+                                 double k0, const double *dirs_dev, long long count, double *out_dev) {
+  if (p->mirror) { n2c_set_error("radiation amplitude: free space only (plan has PEC images)"); return 0; }
+  if (count <= 0) return 1;
+  const long long blocks = (count + RAD_DIRS - 1) / RAD_DIRS;
+  if (blocks > 0x7fffffffLL) { n2c_set_error("too many directions"); return 0; }
+  radiation_kernel<<<(unsigned)blocks, 256, 0, n2c_stream()>>>((const double2 *)current_dev, p->cell_box, p->cells,
+                                                               p->S[1], p->S[2], origin[0], origin[1], origin[2], h,
+                                                               k0, dirs_dev, (int)count, (double2 *)out_dev);
+  return n2c_check_launch("radiation");
+}
+
 template <typename C>
 int n2c_vie_pass_plans(n2d_vie *p, int precondition, double *norm, int *flag, const int *scale, const int *variant,
                        PassArgs<C> args[5], int mode[5], int L[5], int var[5], size_t smem[5], long long tiles[5]) {

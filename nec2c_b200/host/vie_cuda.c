@@ -38,6 +38,7 @@ const char *nec2c_cuda_vie_fft_backend_name(void) { return g_fft_fp32 ? "cuda-mi
 struct nec2c_cuda_vie_plan {
   n2d_vie *dev;
   size_t cells, shape[3], padded[3], grids, bytes;
+  double pitch, k0;
   double complex *eps;      /* host shadow of the per-cell permittivity */
   double complex self[3];
   int eps_dirty;
@@ -138,6 +139,7 @@ int nec2c_cuda_vie_fft_create(nec2c_cuda_vie_plan **out, const size_t shape[3], 
   if(!p) return 0;
   p->cells = cells; p->grids = g; p->bytes = bytes;
   memcpy(p->shape, shape, sizeof(p->shape)); memcpy(p->padded, padded, sizeof(p->padded));
+  p->pitch = h; p->k0 = k;
   p->eps = malloc(cells * sizeof(double complex));
   cell_box = malloc(cells * sizeof(int));
   size_t nbox = shape[0] * shape[1] * shape[2];
@@ -281,6 +283,24 @@ int nec2c_cuda_vie_fft_apply_device(nec2c_cuda_vie_plan *p, const void *x_dev, v
 int nec2c_cuda_vie_fft_spectrum(nec2c_cuda_vie_plan *p, nec2c_cuda_complex *out)
 {
   return p && out && n2d_vie_read_spectrum(p->dev, (double *)out);
+}
+
+int nec2c_cuda_vie_fft_radiation_device(nec2c_cuda_vie_plan *p, const double origin[3], const void *current_dev,
+                                        size_t count, const double *directions, nec2c_cuda_complex *amplitude)
+{
+  double *dirs, *out;
+  int ok;
+  if(!p || !origin || !current_dev || (count && (!directions || !amplitude))) return 0;
+  if(count == 0) return 1;
+  if(count > (size_t)1 << 28) { n2c_set_error("radiation: too many directions"); return 0; }
+  dirs = n2d_alloc(3 * count * sizeof(double));
+  out = n2d_alloc(3 * count * 2 * sizeof(double));
+  ok = dirs && out && n2d_upload(dirs, directions, 3 * count * sizeof(double)) &&
+       n2d_vie_radiation(p->dev, current_dev, origin, p->pitch, p->k0, dirs, (long long)count, out) &&
+       n2d_download(amplitude, out, 3 * count * 2 * sizeof(double));
+  n2d_free(dirs);
+  n2d_free(out);
+  return ok;
 }
 
 void nec2c_cuda_vie_fft_autotune(int enable) { n2d_vie_autotune(enable); }

@@ -594,3 +594,37 @@ int oracle_row_major_solve(ocplx *a, ocplx *b, size_t n)
   }
   return 1;
 }
+
+/* ------------------------------------------------ far-field amplitude */
+/* sin(x)/x with its series near 0 (dielectric_solver.c:47-55). */
+static double sinc_small(double x)
+{
+  if(fabs(x) < 1.0e-5) { const double x2 = x * x; return 1.0 - x2 / 6.0 + x2 * x2 / 120.0; }
+  return sin(x) / x;
+}
+
+/* dielectric_solver.c:90-150 in free space: integral = sum_cells J V
+   prod_a sinc(k d_a s_a / 2) exp(+i k d.r), then the transverse part
+   (integral x d) x d, times i k c0 mu0 / (4 pi) (c0 = 299792458,
+   mu0 = 1.25663706212e-6 as dielectric_solver.c:21-22). */
+void oracle_radiation_amplitude(size_t cells, const double *centers, double h, const ocplx *current,
+                                double k0, const double direction[3], ocplx out[3])
+{
+  const double c0 = 299792458.0, mu0 = 1.25663706212e-6, volume = h * h * h;
+  ocplx integral[3] = {0, 0, 0}, crossed[3];
+  double average = 1.0;
+  for(int a = 0; a < 3; ++a) average *= sinc_small(0.5 * k0 * direction[a] * h);
+  for(size_t i = 0; i < cells; ++i) {
+    const double dot = direction[0] * centers[3 * i] + direction[1] * centers[3 * i + 1] +
+                       direction[2] * centers[3 * i + 2];
+    const ocplx weight = volume * average * cexp(I * k0 * dot);
+    for(int a = 0; a < 3; ++a) integral[a] += current[3 * i + a] * weight;
+  }
+  crossed[0] = integral[1] * direction[2] - integral[2] * direction[1];
+  crossed[1] = integral[2] * direction[0] - integral[0] * direction[2];
+  crossed[2] = integral[0] * direction[1] - integral[1] * direction[0];
+  out[0] = crossed[1] * direction[2] - crossed[2] * direction[1];
+  out[1] = crossed[2] * direction[0] - crossed[0] * direction[2];
+  out[2] = crossed[0] * direction[1] - crossed[1] * direction[0];
+  for(int a = 0; a < 3; ++a) out[a] *= I * k0 * c0 * mu0 / (4.0 * kPi);
+}

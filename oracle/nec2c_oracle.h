@@ -78,4 +78,10 @@ void oracle_solve(int n, const ocplx *a, const int *ip, ocplx *b, int ndim);
 /* dense_backend.c:152-190 (builtin_row_major_solve). */
 int oracle_row_major_solve(ocplx *a, ocplx *b, size_t n);
 
+/* Far-field radiation amplitude of the volume polarisation current in free
+   space (dielectric_solver.c:90-150): cubic cells of side h centred at
+   centers[3 i], current[3 i + c] the c-th component of cell i. */
+void oracle_radiation_amplitude(size_t cells, const double *centers, double h, const ocplx *current,
+                                double k0, const double direction[3], ocplx out[3]);
+
 #endif

@@ -12,6 +12,7 @@
 #include "vie_ground.h"
 #include "vie_iterative.h"
 #include "dense_backend.h"
+#include "dielectric.h"
 
 #include <stdio.h>
 #include <stdlib.h>
@@ -118,4 +119,27 @@ int ref_row_major_solve(complex double *a, complex double *b, size_t n)
 {
   dense_backend_set("builtin");
   return dense_backend_solve_row_major(a, b, n);
+}
+
+/* dielectric_radiation_amplitude (dielectric_solver.c:124-150) of cubic cells
+   of side h centred at centers[3 i], in free space (gnd.ksymp = 1). */
+void dielectric_radiation_amplitude(const dielectric_mesh_result *mesh, const complex double *current,
+                                    double k0, const double direction[3], complex double amplitude[3]);
+int ref_radiation_amplitude(size_t cells, const double *centers, double h, const complex double *current,
+                            double k0, const double direction[3], complex double out[3])
+{
+  dielectric_mesh_result mesh;
+  dielectric_cell *c = calloc(cells ? cells : 1, sizeof(*c));
+  int saved = gnd.ksymp;
+  if(!c) return 0;
+  memset(&mesh, 0, sizeof(mesh));
+  for(size_t i = 0; i < cells; ++i)
+    for(int a = 0; a < 3; ++a) { c[i].center[a] = centers[3 * i + a]; c[i].size[a] = h; }
+  mesh.cells = c;
+  mesh.cell_count = cells;
+  gnd.ksymp = 1;
+  dielectric_radiation_amplitude(&mesh, current, k0, direction, out);
+  gnd.ksymp = saved;
+  free(c);
+  return 1;
 }

@@ -67,6 +67,7 @@ def oracle():
         o.oracle_solve.argtypes = [i, vp, vp, vp, i]
         o.oracle_row_major_solve.argtypes = [vp, vp, sz]
         o.oracle_row_major_solve.restype = i
+        o.oracle_radiation_amplitude.argtypes = [sz, vp, dbl, vp, dbl, vp, vp]
         _oracle = o
     return _oracle
 
@@ -105,6 +106,8 @@ def reference():
         r.ref_solve.argtypes = [i, vp, vp, vp, i]
         r.ref_row_major_solve.argtypes = [vp, vp, sz]
         r.ref_row_major_solve.restype = i
+        r.ref_radiation_amplitude.argtypes = [sz, vp, dbl, vp, dbl, vp, vp]
+        r.ref_radiation_amplitude.restype = i
         _ref = r
     return _ref
 
@@ -228,3 +231,16 @@ def far_failures(shape, h, k):
         if not o.oracle_far_kernel((C.c_size_t * 3)(*v), h, k, ptr(out)):
             fails.append(v)
     return fails
+
+
+def radiation_amplitude(centers, h, current, k0, direction, use_reference=False):
+    """3 complex amplitudes (oracle restatement, or the reference itself)."""
+    c = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1)
+    j = np.ascontiguousarray(current, dtype=np.complex128)
+    d = np.ascontiguousarray(direction, dtype=np.float64)
+    out = np.zeros(3, dtype=np.complex128)
+    if use_reference:
+        assert reference().ref_radiation_amplitude(c.size // 3, ptr(c), h, ptr(j), k0, ptr(d), ptr(out))
+    else:
+        oracle().oracle_radiation_amplitude(c.size // 3, ptr(c), h, ptr(j), k0, ptr(d), ptr(out))
+    return out

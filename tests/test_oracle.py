@@ -268,3 +268,27 @@ def test_hybrid_oracle_conductor_only():
     x = np.array([1 + 1j, 2 - 1j])
     y = h.apply(x)
     assert np.abs(y[0] - 2 * x[0]) + np.abs(y[1] - 3 * x[1]) < 1e-14
+
+
+def fibonacci_directions(count, seed=0):
+    """The reference's 974-point sphere quadrature rule (dielectric_solver.c:153-176)."""
+    golden = np.pi * (3 - np.sqrt(5))
+    i = np.arange(count)
+    z = 1 - 2 * (i + 0.5) / count
+    r = np.sqrt(np.maximum(0, 1 - z * z))
+    return np.stack([r * np.cos(golden * i), r * np.sin(golden * i), z], axis=1)
+
+
+@needs_ref
+def test_radiation_amplitude_matches_reference():
+    """dielectric_radiation_amplitude (free space) of random cells and currents,
+    oracle restatement against the reference compiled here, 1e-13 relative."""
+    rng = np.random.default_rng(31)
+    h, k0 = 0.01, 6.28
+    idx = rng.integers(0, 20, size=(300, 3))
+    centers = 0.3 + h * idx
+    current = rng.standard_normal(900) + 1j * rng.standard_normal(900)
+    for d in list(fibonacci_directions(24)) + [np.array([0.0, 0.0, 1.0]), np.array([1.0, 0.0, 0.0])]:
+        a = oracle_lib.radiation_amplitude(centers, h, current, k0, d)
+        r = oracle_lib.radiation_amplitude(centers, h, current, k0, d, use_reference=True)
+        assert np.max(np.abs(a - r)) <= 1e-13 * np.max(np.abs(r))

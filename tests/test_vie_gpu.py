@@ -195,3 +195,23 @@ def test_gmres_large_system_paths(near_tables):
     okm, xm, rm = gm.gmres(b, restart=30, maxit=400, rtol=1e-8)
     assert ok64 and okm and r64["relative_residual"] <= 1e-8 and rm["relative_residual"] <= 1e-8
     assert rel_l2(xm, x64) < 1e-6
+
+
+def test_radiation_amplitude(near_tables):
+    """Far-field amplitude of a cell current (dielectric_solver.c:90-150, free
+    space) on the device against the oracle restatement (pinned to the
+    reference in test_oracle.py): 1e-12 relative to the largest amplitude."""
+    import oracle_lib
+    from test_oracle import fibonacci_directions
+    h, k, table = near_tables["rand_k0.3"]
+    shape = (12, 9, 17)
+    xyz = cases.random_lattice(shape, 0.5, 41)
+    gp = nb.VolumePlan(shape, xyz, h, k, 3.0, table)
+    rng = np.random.default_rng(42)
+    cur = rng.standard_normal(gp.n) + 1j * rng.standard_normal(gp.n)
+    origin = (0.37, -1.25, 2.5)
+    dirs = np.concatenate([fibonacci_directions(97), np.eye(3), -np.eye(3)])
+    got = gp.radiation(cur, dirs, origin)
+    centers = np.asarray(origin) + h * xyz.reshape(-1, 3).astype(np.float64)
+    want = np.array([oracle_lib.radiation_amplitude(centers, h, cur, k, d) for d in dirs])
+    assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
