@@ -789,6 +789,296 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) lu_solve_kernel(const S *a, 
   }
 }
 
+// ------------------------------------------------ multi-CTA triangular solve
+// The same solve spread over SOLVE_CTAS co-resident CTAs (cooperative
+// launch), for orders where one CTA's row updates dominate.  Blocks of
+// SOLVE_NB = 64 rows.  In each block step CTA 0 solves the diagonal block by
+// warp shuffles (two 32-row halves), then every CTA subtracts the block's
+// contribution from its share of the rows below (above, backward), a warp
+// per row.  CTA 0 itself updates the next block's rows, so the next diagonal
+// solve needs no further barrier: one grid barrier per block.  While the
+// grid waits at that barrier CTA 0 already holds the next diagonal block and
+// the block of the next rows' update in shared memory (loaded before it
+// arrives).  The barrier spins are bounded; on time-out the kernel raises
+// *error and every CTA leaves at its next barrier.
+constexpr int SOLVE_NB = 64;
+constexpr int SOLVE_LDS = SOLVE_NB + 1;                  // padded shared row
+constexpr int SOLVE_CTAS = 32;
+constexpr int SOLVE_COOP_THREADS = 512;
+constexpr int SOLVE_COOP_MIN = 256;     // smaller orders keep the one-CTA kernel
+constexpr int SOLVE_COOP_RHS = 4;       // right-hand sides solved in turn by one launch
+// Shared memory: diagonal block, next rows' block, solved values.
+constexpr size_t SOLVE_COOP_SMEM = (size_t)(2 * SOLVE_NB * SOLVE_LDS + SOLVE_NB) * sizeof(double2);
+// Orders whose interchanges compose in that shared memory (two ints per row).
+constexpr int SOLVE_COOP_PERM_MAX = (int)(SOLVE_COOP_SMEM / 8);
+
+struct SolveSync {
+  unsigned count, gen;
+  int error;
+};
+
+__device__ __forceinline__ bool solve_barrier(SolveSync *sy) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    volatile unsigned *gen = &sy->gen;
+    volatile int *err = &sy->error;
+    if (*err) ok = 0;
+    else {
+      const unsigned g = *gen;
+      __threadfence();
+      if (atomicAdd(&sy->count, 1u) == gridDim.x - 1) {
+        sy->count = 0;
+        __threadfence();
+        atomicAdd(&sy->gen, 1u);
+      } else {
+        const long long t0 = clock64();
+        while (*gen == g) {
+          if (*err || clock64() - t0 > (1LL << 32)) { atomicExch(&sy->error, 1); ok = 0; break; }
+          __nanosleep(32);
+        }
+      }
+      __threadfence();
+    }
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// y[r] -= sum_c A[r][c0 + c] xs[c] for rows r of [r0, r1) taken warp by warp
+// from `first` with stride `step` (warp indices); four rows per round, their
+// loads issued together.
+template <typename S>
+__device__ __forceinline__ void solve_rows(const S *a, long long ld, double2 *y, long long r0, long long r1,
+                                           long long c0, int w, const double2 *xs, long long first, long long step) {
+  const int lane = threadIdx.x & 31;
+  const double2 x0 = lane < w ? xs[lane] : make_double2(0, 0);
+  const double2 x1 = lane + 32 < w ? xs[lane + 32] : make_double2(0, 0);
+  for (long long r = r0 + first; r < r1; r += 4 * step) {
+    double2 s[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const long long rr = r + u * step;
+      s[u] = make_double2(0, 0);
+      if (rr < r1) {
+        const S *row = a + rr * ld + c0;
+        if (lane < w) s[u] = cmul(to_d(row[lane]), x0);
+        if (lane + 32 < w) s[u] = cadd(s[u], cmul(to_d(row[lane + 32]), x1));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      for (int o = 16; o > 0; o >>= 1) {
+        s[u].x += __shfl_xor_sync(0xffffffffu, s[u].x, o);
+        s[u].y += __shfl_xor_sync(0xffffffffu, s[u].y, o);
+      }
+      const long long rr = r + u * step;
+      if (lane == 0 && rr < r1) y[rr] = csub(y[rr], s[u]);
+    }
+  }
+}
+
+// Loads the rows x cols block of A at (r0, c0) into shared memory (leading
+// dim SOLVE_LDS), zero elsewhere in the SOLVE_NB square; each thread issues
+// all its loads before it stores (blockDim.x must divide SOLVE_NB^2).
+constexpr int SOLVE_PER_THREAD = SOLVE_NB * SOLVE_NB / SOLVE_COOP_THREADS;
+template <typename S>
+__device__ __forceinline__ void solve_load_block(const S *a, long long ld, long long r0, long long c0, int rows,
+                                                 int cols, double2 *dst) {
+  double2 v[SOLVE_PER_THREAD];
+#pragma unroll
+  for (int u = 0; u < SOLVE_PER_THREAD; ++u) {
+    const int e = threadIdx.x + u * SOLVE_COOP_THREADS, r = e >> 6, c = e & (SOLVE_NB - 1);
+    v[u] = (r < rows && c < cols) ? to_d(a[(r0 + r) * ld + c0 + c]) : make_double2(0, 0);
+  }
+#pragma unroll
+  for (int u = 0; u < SOLVE_PER_THREAD; ++u) {
+    const int e = threadIdx.x + u * SOLVE_COOP_THREADS, r = e >> 6, c = e & (SOLVE_NB - 1);
+    dst[r * SOLVE_LDS + c] = v[u];
+  }
+}
+
+__device__ __forceinline__ double2 shfl2(double2 v, int src) {
+  return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+// Warp 0: forward solve of the unit-lower w x w diagonal block dg in place
+// on xs (two halves of 32: solve, update the second half, solve).
+__device__ __forceinline__ void solve_diag_lower(const double2 *dg, double2 *xs, int w) {
+  const int lane = threadIdx.x & 31;
+  double2 v0 = lane < w ? xs[lane] : make_double2(0, 0);
+  double2 v1 = lane + 32 < w ? xs[lane + 32] : make_double2(0, 0);
+  const int w0 = w < 32 ? w : 32;
+  for (int c = 0; c < w0 - 1; ++c) {
+    const double2 xc = shfl2(v0, c);
+    if (lane > c) v0 = csub(v0, cmul(dg[lane * SOLVE_LDS + c], xc));
+  }
+  if (w > 32) {
+    for (int c = 0; c < 32; ++c) v1 = csub(v1, cmul(dg[(lane + 32) * SOLVE_LDS + c], shfl2(v0, c)));
+    for (int c = 0; c < w - 33; ++c) {
+      const double2 xc = shfl2(v1, c);
+      if (lane > c) v1 = csub(v1, cmul(dg[(lane + 32) * SOLVE_LDS + 32 + c], xc));
+    }
+  }
+  if (lane < w) xs[lane] = v0;
+  if (lane + 32 < w) xs[lane + 32] = v1;
+}
+
+// Warp 0: backward solve of the upper w x w diagonal block dg in place on xs.
+__device__ __forceinline__ void solve_diag_upper(const double2 *dg, double2 *xs, int w) {
+  const int lane = threadIdx.x & 31;
+  double2 v0 = lane < w ? xs[lane] : make_double2(0, 0);
+  double2 v1 = lane + 32 < w ? xs[lane + 32] : make_double2(0, 0);
+  if (w > 32) {
+    for (int c = w - 33; c >= 0; --c) {
+      if (lane == c) v1 = cdiv(v1, dg[(c + 32) * SOLVE_LDS + c + 32]);
+      const double2 xc = shfl2(v1, c);
+      if (lane < c) v1 = csub(v1, cmul(dg[(lane + 32) * SOLVE_LDS + c + 32], xc));
+    }
+    for (int c = 0; c < w - 32; ++c) v0 = csub(v0, cmul(dg[lane * SOLVE_LDS + 32 + c], shfl2(v1, c)));
+  }
+  const int w0 = w < 32 ? w : 32;
+  for (int c = w0 - 1; c >= 0; --c) {
+    if (lane == c) v0 = cdiv(v0, dg[c * SOLVE_LDS + c]);
+    const double2 xc = shfl2(v0, c);
+    if (lane < c) v0 = csub(v0, cmul(dg[lane * SOLVE_LDS + c], xc));
+  }
+  if (lane < w) xs[lane] = v0;
+  if (lane + 32 < w) xs[lane + 32] = v1;
+}
+
+// CTA 0's update of the next block's rows from the shared block nb (rows x
+// w): y[r0 + r] -= sum_c nb[r][c] xs[c], a warp per row.
+__device__ __forceinline__ void solve_next_rows(const double2 *nb, const double2 *xs, double2 *y, long long r0,
+                                                int rows, int w) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int r = warp; r < rows; r += nw) {
+    double2 s = make_double2(0, 0);
+    for (int c = lane; c < w; c += 32) s = cadd(s, cmul(nb[r * SOLVE_LDS + c], xs[c]));
+    for (int o = 16; o > 0; o >>= 1) {
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+      s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+    }
+    if (lane == 0) y[r0 + r] = csub(y[r0 + r], s);
+  }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(SOLVE_COOP_THREADS) lu_solve_coop_kernel(const S *a, long long n, long long ld,
+                                                                         const int *ipiv, double2 *b, long long ldb,
+                                                                         int nrhs, double2 *scratch,
+                                                                         SolveSync *sy) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2 *dg = reinterpret_cast<double2 *>(smem_raw);   // diagonal block
+  double2 *nb = dg + SOLVE_NB * SOLVE_LDS;                // next rows' block
+  double2 *xs = nb + SOLVE_NB * SOLVE_LDS;                // solved block values
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  // Row updates of the other CTAs: warps of CTAs 1.. (CTA 0 takes the next block).
+  const long long ow = (long long)(blockIdx.x - 1) * nw + warp, onw = (long long)(gridDim.x - 1) * nw;
+  const long long nblk = (n + SOLVE_NB - 1) / SOLVE_NB;
+  for (int rhs = 0; rhs < nrhs; ++rhs) {
+    double2 *x = b + rhs * ldb;
+    // Interchanges, applied in pivot order by CTA 0 into the scratch vector:
+    // composed into an index permutation in shared memory (orders up to
+    // SOLVE_COOP_PERM_MAX), then gathered; beyond, swapped in place.
+    if (blockIdx.x == 0) {
+      if (n <= SOLVE_COOP_PERM_MAX) {
+        int *idx = reinterpret_cast<int *>(smem_raw), *pv = idx + n;
+        for (long long i = threadIdx.x; i < n; i += blockDim.x) { idx[i] = (int)i; pv[i] = ipiv[i] - 1; }
+        __syncthreads();
+        if (threadIdx.x == 0)
+          for (int i = 0; i < (int)n; ++i) {
+            const int q = pv[i];
+            if (q != i) { const int t = idx[q]; idx[q] = idx[i]; idx[i] = t; }
+          }
+        __syncthreads();
+        for (long long i = threadIdx.x; i < n; i += blockDim.x) scratch[i] = x[idx[i]];
+        __syncthreads();
+      } else {
+        for (long long i = threadIdx.x; i < n; i += blockDim.x) scratch[i] = x[i];
+        __syncthreads();
+        if (threadIdx.x == 0)
+          for (long long i = 0; i < n; ++i) {
+            const long long q = ipiv[i] - 1;
+            if (q != i) { const double2 t = scratch[q]; scratch[q] = scratch[i]; scratch[i] = t; }
+          }
+        __syncthreads();
+      }
+      solve_load_block(a, ld, 0, 0, (int)(n < SOLVE_NB ? n : SOLVE_NB), (int)(n < SOLVE_NB ? n : SOLVE_NB), dg);
+    }
+    if (!solve_barrier(sy)) return;
+    double2 *y = scratch;
+    // Forward: L unit lower.  dg holds block k's diagonal on entry.
+    for (long long k = 0; k < nblk; ++k) {
+      const long long j0 = k * SOLVE_NB;
+      const int w = (int)(n - j0 < SOLVE_NB ? n - j0 : SOLVE_NB);
+      const long long r1 = j0 + w + SOLVE_NB < n ? j0 + w + SOLVE_NB : n;   // end of the next block
+      if (blockIdx.x == 0) {
+        for (int r = threadIdx.x; r < w; r += blockDim.x) xs[r] = y[j0 + r];
+        __syncthreads();
+        if (warp == 0) solve_diag_lower(dg, xs, w);
+        __syncthreads();
+        for (int r = threadIdx.x; r < w; r += blockDim.x) y[j0 + r] = xs[r];
+        // The next rows' block of L and the next diagonal block while the
+        // grid gathers.
+        if (k + 1 < nblk) {
+          const int wn = (int)(r1 - j0 - w);
+          solve_load_block(a, ld, j0 + w, j0, wn, w, nb);
+          solve_load_block(a, ld, j0 + w, j0 + w, wn, wn, dg);
+        }
+      }
+      if (!solve_barrier(sy)) return;
+      if (k + 1 == nblk) break;
+      if (blockIdx.x != 0) {
+        for (int r = threadIdx.x; r < w; r += blockDim.x) xs[r] = y[j0 + r];
+        __syncthreads();
+        solve_rows(a, ld, y, r1, n, j0, w, xs, ow, onw);
+      } else {
+        solve_next_rows(nb, xs, y, j0 + w, (int)(r1 - j0 - w), w);
+        __syncthreads();
+      }
+    }
+    // Backward: U upper, non-unit diagonal.
+    if (blockIdx.x == 0) {
+      const long long j0 = (nblk - 1) * SOLVE_NB;
+      const int w = (int)(n - j0);
+      solve_load_block(a, ld, j0, j0, w, w, dg);
+    }
+    if (!solve_barrier(sy)) return;
+    for (long long k = nblk - 1; k >= 0; --k) {
+      const long long j0 = k * SOLVE_NB;
+      const int w = (int)(n - j0 < SOLVE_NB ? n - j0 : SOLVE_NB);
+      const long long p0 = j0 - SOLVE_NB > 0 ? j0 - SOLVE_NB : 0;   // rows of the next block up
+      if (blockIdx.x == 0) {
+        for (int r = threadIdx.x; r < w; r += blockDim.x) xs[r] = y[j0 + r];
+        __syncthreads();
+        if (warp == 0) solve_diag_upper(dg, xs, w);
+        __syncthreads();
+        for (int r = threadIdx.x; r < w; r += blockDim.x) y[j0 + r] = xs[r];
+        if (k > 0) {
+          solve_load_block(a, ld, p0, j0, (int)(j0 - p0), w, nb);
+          solve_load_block(a, ld, p0, p0, (int)(j0 - p0), (int)(j0 - p0), dg);
+        }
+      }
+      if (!solve_barrier(sy)) return;
+      if (k == 0) break;
+      if (blockIdx.x != 0) {
+        for (int r = threadIdx.x; r < w; r += blockDim.x) xs[r] = y[j0 + r];
+        __syncthreads();
+        solve_rows(a, ld, y, 0, p0, j0, w, xs, ow, onw);
+      } else {
+        solve_next_rows(nb, xs, y, p0, (int)(j0 - p0), w);
+        __syncthreads();
+      }
+    }
+    if (!solve_barrier(sy)) return;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      x[i] = y[i];
+    if (!solve_barrier(sy)) return;
+  }
+}
+
 __global__ void transpose_kernel(const double2 *src, long long lds, double2 *dst, long long ldd,
                                  long long rows, long long cols) {
   __shared__ double2 tile[32][33];
@@ -1081,9 +1371,62 @@ static int solve_configure() {
   return 1;
 }
 
+// Cooperative multi-CTA solve (orders >= SOLVE_COOP_MIN, up to
+// SOLVE_COOP_RHS right-hand sides); 0 with the error set on failure, -1 when
+// the one-CTA kernel should be used instead.
+template <typename S>
+static int solve_coop(const S *a, long long n, long long ld, const int *ipiv, double2 *b, long long ldb,
+                      long long nrhs) {
+  if (n < SOLVE_COOP_MIN || nrhs > SOLVE_COOP_RHS || n > 0x7fffffffLL) return -1;
+  static int configured = 0, blocks = 0;
+  const size_t smem = SOLVE_COOP_SMEM;
+  if (!configured) {
+    int per_sm = 0;
+    if (cudaFuncSetAttribute(lu_solve_coop_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lu_solve_coop_kernel<S>, SOLVE_COOP_THREADS, smem) !=
+            cudaSuccess ||
+        per_sm < 1) {
+      cudaGetLastError();
+      return -1;
+    }
+    blocks = n2c_sm_count() < SOLVE_CTAS ? n2c_sm_count() : SOLVE_CTAS;
+    configured = 1;
+  }
+  if (blocks < 2) return -1;   // the rows below the next block need a second CTA
+  double2 *scratch = (double2 *)n2d_alloc_async((size_t)n * sizeof(double2));
+  SolveSync *sy = (SolveSync *)n2d_alloc_async(sizeof(SolveSync) + 16);
+  int ok = scratch && sy && cudaMemsetAsync(sy, 0, sizeof(SolveSync), n2c_stream()) == cudaSuccess;
+  if (ok) {
+    int nr = (int)nrhs;
+    void *args[] = {(void *)&a, (void *)&n, (void *)&ld, (void *)&ipiv, (void *)&b, (void *)&ldb, (void *)&nr,
+                    (void *)&scratch, (void *)&sy};
+    const cudaError_t e = cudaLaunchCooperativeKernel((void *)lu_solve_coop_kernel<S>, blocks, SOLVE_COOP_THREADS,
+                                                      args, smem, n2c_stream());
+    if (e != cudaSuccess) {
+      // Not launchable as a cooperative grid here: the one-CTA kernel solves it.
+      cudaGetLastError();
+      n2d_free_async(scratch);
+      n2d_free_async(sy);
+      return -1;
+    }
+    n2c_count_launch(1);
+  }
+  int err = 0;
+  if (ok && (cudaMemcpyAsync(&err, &sy->error, sizeof(int), cudaMemcpyDeviceToHost, n2c_stream()) != cudaSuccess ||
+             cudaStreamSynchronize(n2c_stream()) != cudaSuccess))
+    ok = 0;
+  if (ok && err) { n2c_set_error("triangular solve: grid barrier time-out"); ok = 0; }
+  n2d_free_async(scratch);
+  n2d_free_async(sy);
+  return ok;
+}
+
 extern "C" int n2d_lu_solve(const double *a_dev, long long n, long long ld, const int *ipiv, double *b_dev,
                             long long ldb, long long nrhs) {
   if (n <= 0 || nrhs <= 0) return 1;
+  const int c = solve_coop((const double2 *)a_dev, n, ld, ipiv, (double2 *)b_dev, ldb, nrhs);
+  if (c >= 0) return c;
   if (!solve_configure<double2>()) return 0;
   lu_solve_kernel<double2><<<(unsigned)nrhs, SOLVE_THREADS, solve_smem(n), n2c_stream()>>>((const double2 *)a_dev, n, ld, ipiv,
                                                              (double2 *)b_dev, ldb);
@@ -1095,6 +1438,8 @@ extern "C" int n2d_lu_solve(const double *a_dev, long long n, long long ld, cons
 extern "C" int n2d_lu_solve32(const float *a_dev, long long n, long long ld, const int *ipiv, double *b_dev,
                               long long ldb, long long nrhs) {
   if (n <= 0 || nrhs <= 0) return 1;
+  const int c = solve_coop((const float2 *)a_dev, n, ld, ipiv, (double2 *)b_dev, ldb, nrhs);
+  if (c >= 0) return c;
   if (!solve_configure<float2>()) return 0;
   lu_solve_kernel<float2><<<(unsigned)nrhs, SOLVE_THREADS, solve_smem(n), n2c_stream()>>>((const float2 *)a_dev, n, ld, ipiv,
                                                                      (double2 *)b_dev, ldb);
