@@ -807,8 +807,9 @@ constexpr int SOLVE_CTAS = 32;
 constexpr int SOLVE_COOP_THREADS = 512;
 constexpr int SOLVE_COOP_MIN = 256;     // smaller orders keep the one-CTA kernel
 constexpr int SOLVE_COOP_RHS = 4;       // right-hand sides solved in turn by one launch
-// Shared memory: diagonal block, next rows' block, solved values.
-constexpr size_t SOLVE_COOP_SMEM = (size_t)(2 * SOLVE_NB * SOLVE_LDS + SOLVE_NB) * sizeof(double2);
+// Shared memory: diagonal block, next rows' block, solved values, inverse
+// diagonal (backward sweep).
+constexpr size_t SOLVE_COOP_SMEM = (size_t)(2 * SOLVE_NB * SOLVE_LDS + 2 * SOLVE_NB) * sizeof(double2);
 // Orders whose interchanges compose in that shared memory (two ints per row).
 constexpr int SOLVE_COOP_PERM_MAX = (int)(SOLVE_COOP_SMEM / 8);
 
@@ -925,14 +926,26 @@ __device__ __forceinline__ void solve_diag_lower(const double2 *dg, double2 *xs,
   if (lane + 32 < w) xs[lane + 32] = v1;
 }
 
-// Warp 0: backward solve of the upper w x w diagonal block dg in place on xs.
-__device__ __forceinline__ void solve_diag_upper(const double2 *dg, double2 *xs, int w) {
+// 1 / U_cc of the diagonal block's rows (threads 0..w-1), so that the
+// sequential back substitution multiplies instead of dividing.
+__device__ __forceinline__ void solve_diag_inverse(const double2 *dg, double2 *dinv, int w) {
+  const int c = threadIdx.x;
+  if (c < w) {
+    const double2 u = dg[c * SOLVE_LDS + c];
+    const double r = 1.0 / (u.x * u.x + u.y * u.y);
+    dinv[c] = make_double2(u.x * r, -u.y * r);
+  }
+}
+
+// Warp 0: backward solve of the upper w x w diagonal block dg in place on xs
+// (dinv: the inverse diagonal).
+__device__ __forceinline__ void solve_diag_upper(const double2 *dg, const double2 *dinv, double2 *xs, int w) {
   const int lane = threadIdx.x & 31;
   double2 v0 = lane < w ? xs[lane] : make_double2(0, 0);
   double2 v1 = lane + 32 < w ? xs[lane + 32] : make_double2(0, 0);
   if (w > 32) {
     for (int c = w - 33; c >= 0; --c) {
-      if (lane == c) v1 = cdiv(v1, dg[(c + 32) * SOLVE_LDS + c + 32]);
+      if (lane == c) v1 = cmul(v1, dinv[c + 32]);
       const double2 xc = shfl2(v1, c);
       if (lane < c) v1 = csub(v1, cmul(dg[(lane + 32) * SOLVE_LDS + c + 32], xc));
     }
@@ -940,7 +953,7 @@ __device__ __forceinline__ void solve_diag_upper(const double2 *dg, double2 *xs,
   }
   const int w0 = w < 32 ? w : 32;
   for (int c = w0 - 1; c >= 0; --c) {
-    if (lane == c) v0 = cdiv(v0, dg[c * SOLVE_LDS + c]);
+    if (lane == c) v0 = cmul(v0, dinv[c]);
     const double2 xc = shfl2(v0, c);
     if (lane < c) v0 = csub(v0, cmul(dg[lane * SOLVE_LDS + c], xc));
   }
@@ -973,6 +986,7 @@ __global__ void __launch_bounds__(SOLVE_COOP_THREADS) lu_solve_coop_kernel(const
   double2 *dg = reinterpret_cast<double2 *>(smem_raw);   // diagonal block
   double2 *nb = dg + SOLVE_NB * SOLVE_LDS;                // next rows' block
   double2 *xs = nb + SOLVE_NB * SOLVE_LDS;                // solved block values
+  double2 *dinv = xs + SOLVE_NB;                          // inverse diagonal (backward)
   const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   // Row updates of the other CTAs: warps of CTAs 1.. (CTA 0 takes the next block).
   const long long ow = (long long)(blockIdx.x - 1) * nw + warp, onw = (long long)(gridDim.x - 1) * nw;
@@ -1044,6 +1058,8 @@ __global__ void __launch_bounds__(SOLVE_COOP_THREADS) lu_solve_coop_kernel(const
       const long long j0 = (nblk - 1) * SOLVE_NB;
       const int w = (int)(n - j0);
       solve_load_block(a, ld, j0, j0, w, w, dg);
+      __syncthreads();
+      solve_diag_inverse(dg, dinv, w);
     }
     if (!solve_barrier(sy)) return;
     for (long long k = nblk - 1; k >= 0; --k) {
@@ -1053,12 +1069,14 @@ __global__ void __launch_bounds__(SOLVE_COOP_THREADS) lu_solve_coop_kernel(const
       if (blockIdx.x == 0) {
         for (int r = threadIdx.x; r < w; r += blockDim.x) xs[r] = y[j0 + r];
         __syncthreads();
-        if (warp == 0) solve_diag_upper(dg, xs, w);
+        if (warp == 0) solve_diag_upper(dg, dinv, xs, w);
         __syncthreads();
         for (int r = threadIdx.x; r < w; r += blockDim.x) y[j0 + r] = xs[r];
         if (k > 0) {
           solve_load_block(a, ld, p0, j0, (int)(j0 - p0), w, nb);
           solve_load_block(a, ld, p0, p0, (int)(j0 - p0), (int)(j0 - p0), dg);
+          __syncthreads();
+          solve_diag_inverse(dg, dinv, (int)(j0 - p0));
         }
       }
       if (!solve_barrier(sy)) return;
