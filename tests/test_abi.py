@@ -65,3 +65,37 @@ def test_product_never_loads_the_oracle():
     """The product library links no oracle code."""
     out = subprocess.run(["nm", "-D", LIB], capture_output=True, text=True).stdout
     assert "oracle_" not in out and "ref_" not in out
+
+
+def test_new_entry_points_refuse_bad_arguments_without_a_device():
+    """The batch, schedule and far-field entry points check their arguments
+    before any device call."""
+    import nec2c_b200 as nb
+    lib = nb.load()
+    vp = C.c_void_p
+    h = vp()
+    assert not lib.nec2c_cuda_vie_batch_create(None, None, 1)
+    assert not lib.nec2c_cuda_vie_batch_create(C.byref(h), None, 1)
+    assert not lib.nec2c_cuda_vie_batch_create(C.byref(h), (vp * 1)(None), 0)
+    assert not lib.nec2c_cuda_vie_batch_create(C.byref(h), (vp * 1)(None), 1) and not h.value
+    assert not lib.nec2c_cuda_hybrid_batch_create(C.byref(h), (vp * 1)(None), 1) and not h.value
+    reps = (nb.GmresReport * 1)()
+    assert not lib.nec2c_cuda_gmres_batch_device(None, vp(16), vp(32), None, reps)
+    assert not lib.nec2c_cuda_vie_fft_tune(None, 1)
+    tiles, r1 = (C.c_int * 5)(), (C.c_int * 5)()
+    assert lib.nec2c_cuda_vie_fft_schedule(None, 1, tiles, r1) == -1
+    assert not lib.nec2c_cuda_vie_fft_set_schedule(None, 1, tiles, r1)
+    assert not lib.nec2c_cuda_vie_batch_schedule(None, tiles, r1)
+    assert not lib.nec2c_cuda_vie_batch_set_schedule(None, tiles, r1)
+    origin = (C.c_double * 3)(0, 0, 0)
+    assert not lib.nec2c_cuda_vie_fft_radiation_device(None, origin, vp(16), 1, vp(16), vp(16))
+
+
+def test_autotune_switch():
+    import nec2c_b200 as nb
+    before = nb.fft_autotune_enabled()
+    nb.set_fft_autotune(False)
+    assert not nb.fft_autotune_enabled()
+    nb.set_fft_autotune(True)
+    assert nb.fft_autotune_enabled()
+    nb.set_fft_autotune(before)
