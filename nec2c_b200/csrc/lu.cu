@@ -966,14 +966,25 @@ __device__ __forceinline__ void solve_diag_upper(const double2 *dg, const double
 __device__ __forceinline__ void solve_next_rows(const double2 *nb, const double2 *xs, double2 *y, long long r0,
                                                 int rows, int w) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int r = warp; r < rows; r += nw) {
-    double2 s = make_double2(0, 0);
-    for (int c = lane; c < w; c += 32) s = cadd(s, cmul(nb[r * SOLVE_LDS + c], xs[c]));
-    for (int o = 16; o > 0; o >>= 1) {
-      s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
-      s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+  for (int r = warp; r < rows; r += 4 * nw) {
+    double2 s[4], yv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int rr = r + u * nw;
+      s[u] = make_double2(0, 0);
+      yv[u] = (lane == 0 && rr < rows) ? y[r0 + rr] : make_double2(0, 0);
+      if (rr < rows)
+        for (int c = lane; c < w; c += 32) s[u] = cadd(s[u], cmul(nb[rr * SOLVE_LDS + c], xs[c]));
     }
-    if (lane == 0) y[r0 + r] = csub(y[r0 + r], s);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      for (int o = 16; o > 0; o >>= 1) {
+        s[u].x += __shfl_xor_sync(0xffffffffu, s[u].x, o);
+        s[u].y += __shfl_xor_sync(0xffffffffu, s[u].y, o);
+      }
+      const int rr = r + u * nw;
+      if (lane == 0 && rr < rows) y[r0 + rr] = csub(yv[u], s[u]);
+    }
   }
 }
 
