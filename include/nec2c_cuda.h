@@ -199,6 +199,7 @@ void nec2c_cuda_vie_batch_destroy(nec2c_cuda_vie_batch *batch);
 /* Unknowns of the batch (sum of the systems' orders); system q's entries
    start at nec2c_cuda_vie_batch_offset(batch, q). */
 size_t nec2c_cuda_vie_batch_order(const nec2c_cuda_vie_batch *batch);
+size_t nec2c_cuda_vie_batch_systems(const nec2c_cuda_vie_batch *batch);
 size_t nec2c_cuda_vie_batch_offset(const nec2c_cuda_vie_batch *batch, size_t plan);
 /* Schedule of the batched FFT passes.  Per pass: scale[i] in -1..1 halves,
    keeps or doubles the batch's tile height, and variant[i] 0/1 picks the
@@ -300,8 +301,11 @@ int nec2c_cuda_dense_factor_device_static(size_t order, nec2c_cuda_complex *matr
    solve a private device copy of the matrix (the host matrix is not
    modified; rhs receives the solutions); volume requests run GMRES on a plan
    or hybrid system the caller created and keeps resident across requests
-   (never two at once on the same operator). */
-enum { NEC2C_CUDA_REQUEST_DENSE = 1, NEC2C_CUDA_REQUEST_VOLUME = 2 };
+   (never two at once on the same operator).  Batch requests solve every
+   system of a plan batch at once (a frequency sweep of one model), never
+   two at once on the same batch; a plan in a batch must not be submitted on
+   its own while a request on its batch is in flight. */
+enum { NEC2C_CUDA_REQUEST_DENSE = 1, NEC2C_CUDA_REQUEST_VOLUME = 2, NEC2C_CUDA_REQUEST_BATCH = 3 };
 typedef struct {
   int kind;
   /* dense: NEC's storage (order x order, leading dimension ld) and
@@ -324,6 +328,12 @@ typedef struct {
   size_t footprint;                /* device bytes admitted for it */
   double queued_s, started_s, finished_s;   /* CLOCK_MONOTONIC seconds */
   char error[128];
+  /* batch: b and x hold the batch's order of values in batch order (host);
+     reports receives one report per system; the request's report holds the
+     worst status, the largest iteration and restart counts, the sum of the
+     products and the largest relative residual */
+  nec2c_cuda_vie_batch *batch;
+  nec2c_cuda_gmres_report *reports;
 } nec2c_cuda_request;
 typedef struct nec2c_cuda_server nec2c_cuda_server;
 /* slots worker threads on device; device_budget 0 means the free device

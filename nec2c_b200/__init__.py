@@ -41,10 +41,11 @@ class Request(C.Structure):
                 ("system", C.c_void_p), ("b", C.c_void_p), ("x", C.c_void_p), ("options", GmresOptions),
                 ("status", C.c_int), ("done", C.c_int), ("skipped", C.c_uint), ("report", GmresReport),
                 ("footprint", C.c_size_t), ("queued_s", C.c_double), ("started_s", C.c_double),
-                ("finished_s", C.c_double), ("error", C.c_char * 128)]
+                ("finished_s", C.c_double), ("error", C.c_char * 128), ("batch", C.c_void_p),
+                ("reports", C.c_void_p)]
 
 
-REQUEST_DENSE, REQUEST_VOLUME = 1, 2
+REQUEST_DENSE, REQUEST_VOLUME, REQUEST_BATCH = 1, 2, 3
 
 _lib = None
 
@@ -87,6 +88,7 @@ def load():
         "nec2c_cuda_vie_batch_destroy": (None, [vp]),
         "nec2c_cuda_hybrid_batch_create": (i, [C.POINTER(vp), C.POINTER(vp), sz]),
         "nec2c_cuda_vie_batch_order": (sz, [vp]),
+        "nec2c_cuda_vie_batch_systems": (sz, [vp]),
         "nec2c_cuda_vie_batch_offset": (sz, [vp, sz]),
         "nec2c_cuda_vie_batch_apply_device": (i, [vp, vp, vp]),
         "nec2c_cuda_vie_batch_schedule": (i, [vp, C.POINTER(i), C.POINTER(i)]),
@@ -429,6 +431,21 @@ class Server:
         r.b, r.x = _ptr(b), _ptr(x)
         r.options = GmresOptions(restart, maxit, rtol, atol)
         self._submit(r, (op, b, x))
+        return r
+
+    def batch(self, batch, b, x, restart=30, maxit=300, rtol=1e-12, atol=0.0):
+        """Queues GMRES on every system of a VolumeBatch; b and x are the
+        concatenated vectors in batch order (x: initial guess and result).
+        The request's .reports array holds one report per system."""
+        r = Request()
+        r.kind = REQUEST_BATCH
+        r.batch = batch.h
+        r.b, r.x = _ptr(b), _ptr(x)
+        reps = (GmresReport * len(batch.plans))()
+        r.reports = C.cast(reps, C.c_void_p)
+        r.options = GmresOptions(restart, maxit, rtol, atol)
+        r.system_reports = reps
+        self._submit(r, (batch, b, x, reps))
         return r
 
     def _submit(self, r, keep):

@@ -12,6 +12,8 @@
  *
  * Dense requests factor and solve a private device copy (the split-precision
  * form with FP64 refinement when the server was created with split != 0).
+ * Batch requests solve every system of a plan batch at once (a frequency
+ * sweep of one model, nec2c_cuda_gmres_batch).
  * Volume requests run GMRES on a plan or hybrid system the caller created and
  * keeps on the device across requests (a frequency's spectrum is built once);
  * a plan is not reentrant (vie_fft.h:6), so two requests on the same plan
@@ -64,15 +66,49 @@ static size_t footprint(const nec2c_cuda_server *s, const nec2c_cuda_request *r)
     return bytes;
   }
   {
-    const size_t n = r->plan ? nec2c_cuda_vie_fft_order(r->plan) : nec2c_cuda_hybrid_order(r->system);
+    const size_t n = r->kind == NEC2C_CUDA_REQUEST_BATCH ? nec2c_cuda_vie_batch_order(r->batch)
+                     : r->plan ? nec2c_cuda_vie_fft_order(r->plan) : nec2c_cuda_hybrid_order(r->system);
     const size_t m = r->options.restart ? r->options.restart : 30;
-    return (m + 4) * n * CPX;
+    return (m + 4) * n * CPX + (r->kind == NEC2C_CUDA_REQUEST_BATCH ? 2 * n * CPX : 0);
   }
 }
 
 static const void *request_op(const nec2c_cuda_request *r)
 {
+  if(r->kind == NEC2C_CUDA_REQUEST_BATCH) return r->batch;
   return r->kind == NEC2C_CUDA_REQUEST_VOLUME ? (r->plan ? (const void *)r->plan : (const void *)r->system) : NULL;
+}
+
+/* Every system of the batch at once; the request's report summarises them. */
+static int run_batch(nec2c_cuda_request *r)
+{
+  const size_t k = nec2c_cuda_vie_batch_systems(r->batch);
+  size_t q;
+  const nec2c_cuda_complex **bv;
+  nec2c_cuda_complex **xv;
+  int ok;
+  bv = malloc((k ? k : 1) * sizeof(*bv));
+  xv = malloc((k ? k : 1) * sizeof(*xv));
+  if(!bv || !xv) { free(bv); free(xv); return 0; }
+  for(q = 0; q < k; ++q) {
+    bv[q] = r->b + nec2c_cuda_vie_batch_offset(r->batch, q);
+    xv[q] = r->x + nec2c_cuda_vie_batch_offset(r->batch, q);
+  }
+  ok = nec2c_cuda_gmres_batch(r->batch, bv, xv, &r->options, r->reports);
+  r->report.status = 0;
+  for(q = 0; q < k; ++q) {
+    const nec2c_cuda_gmres_report *p = &r->reports[q];
+    if(p->status != 0 && r->report.status == 0) r->report.status = p->status;
+    if(p->iterations > r->report.iterations) r->report.iterations = p->iterations;
+    if(p->restarts > r->report.restarts) r->report.restarts = p->restarts;
+    r->report.operator_applications += p->operator_applications;
+    if(q == 0 || p->relative_residual > r->report.relative_residual) {
+      r->report.relative_residual = p->relative_residual;
+      r->report.residual_norm = p->residual_norm;
+    }
+  }
+  free(bv); free(xv);
+  return ok;
 }
 
 static int op_busy(const nec2c_cuda_server *s, const void *op)
@@ -92,6 +128,8 @@ static void run_request(nec2c_cuda_server *s, nec2c_cuda_request *r)
                                         &steps);
     r->report.status = r->status;
     r->report.iterations = steps < 0 ? 0 : (size_t)steps;
+  } else if(r->kind == NEC2C_CUDA_REQUEST_BATCH) {
+    r->status = run_batch(r);
   } else if(r->plan) {
     r->status = nec2c_cuda_gmres_plan(r->plan, r->b, r->x, &r->options, &r->report);
   } else {
@@ -207,6 +245,8 @@ int nec2c_cuda_server_submit(nec2c_cuda_server *s, nec2c_cuda_request *r)
        r->rhs_stride < r->order) return 0;
   } else if(r->kind == NEC2C_CUDA_REQUEST_VOLUME) {
     if((!r->plan) == (!r->system) || !r->b || !r->x) return 0;
+  } else if(r->kind == NEC2C_CUDA_REQUEST_BATCH) {
+    if(!r->batch || !r->b || !r->x || !r->reports || r->b == (const nec2c_cuda_complex *)r->x) return 0;
   } else {
     return 0;
   }

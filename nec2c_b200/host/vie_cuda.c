@@ -583,6 +583,7 @@ int nec2c_cuda_hybrid_batch_create(nec2c_cuda_vie_batch **out, nec2c_cuda_hybrid
 }
 
 size_t nec2c_cuda_vie_batch_order(const nec2c_cuda_vie_batch *b) { return b ? b->order : 0; }
+size_t nec2c_cuda_vie_batch_systems(const nec2c_cuda_vie_batch *b) { return b ? b->count : 0; }
 size_t nec2c_cuda_vie_batch_offset(const nec2c_cuda_vie_batch *b, size_t q)
 {
   return b && q <= b->count ? b->offsets[q] : 0;

@@ -173,3 +173,45 @@ def test_rejects_malformed_requests():
     r.kind = nb.REQUEST_DENSE           # no matrix
     assert not nb.load().nec2c_cuda_server_submit(srv.h, C.byref(r))
     srv.close()
+
+
+def test_batch_requests_in_the_mix(near_tables):
+    """A batch request (every system of a plan batch solved at once) gives the
+    same result in a concurrent mix with dense requests as the batch solved
+    directly (bitwise: fixed-order reductions), and its summary report is
+    the worst of its systems'."""
+    h, k, table = near_tables["rand_k0.3"]
+    plans = []
+    for shape, fill, seed in (((7, 6, 5), 0.6, 1), ((8, 8, 8), 1.0, 2), ((12, 9, 17), 0.5, 3)):
+        xyz = cases.random_lattice(shape, fill, seed)
+        p = nb.VolumePlan(shape, xyz, h, k, 3.0, table, mixed=True)
+        for c, e in enumerate(cases.random_eps(xyz.size // 3, seed + 9, er=(2.0, 5.0))):
+            p.set_permittivity(c, e)
+        plans.append(p)
+    batch = nb.VolumeBatch(plans)
+    rng = np.random.default_rng(77)
+    b = rng.standard_normal(batch.order) + 1j * rng.standard_normal(batch.order)
+    ok, direct, reps = batch.gmres(batch.split(b), rtol=1e-9, maxit=400)
+    assert ok
+    dense = [dense_case(n, 900 + n) for n in (300, 700)]
+    srv = nb.Server(slots=3)
+    x = np.zeros_like(b)
+    rb = srv.batch(batch, b, x, rtol=1e-9, maxit=400)
+    outs = []
+    for a, st, rhs in dense:
+        out = rhs.copy(order="F")
+        outs.append((a, rhs, out, srv.dense(st, out)))
+    srv.drain()
+    assert rb.status, rb.error
+    for q, part in enumerate(batch.split(x)):
+        assert np.array_equal(part, direct[q])
+        assert rb.system_reports[q].iterations == reps[q]["iterations"]
+    assert rb.report.status == 0
+    assert rb.report.iterations == max(r["iterations"] for r in reps)
+    assert rb.report.relative_residual == max(r["relative_residual"] for r in reps)
+    for a, rhs, out, r in outs:
+        assert r.status
+        sol = np.linalg.solve(a, rhs[: a.shape[0]])
+        assert np.linalg.norm(out[: a.shape[0]] - sol) / np.linalg.norm(sol) < 1e-10
+    srv.close()
+    batch.close()
