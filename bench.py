@@ -577,7 +577,9 @@ def c1_matrix():
 
 def device_factor(nb, torch, stream, a, form, reps):
     """Factors a resident copy of a (reps + 1 times, the first untimed) with
-    the device LU of the given form; returns the fastest time in ms."""
+    the device LU of the given form, then solves one right-hand side with the
+    factors (reps + 1 times, the first untimed); returns the fastest factor
+    and solve times in ms."""
     lib = nb.load()
     n = a.shape[0]
     if form == "cuda":
@@ -611,13 +613,31 @@ def device_factor(nb, torch, stream, a, form, reps):
             raise RuntimeError("device factor failed: " + nb.last_error())
         if i:
             ts.append(e0.elapsed_time(e1))
-    return min(ts)
+    sf = lib.n2d_lu_solve if form == "cuda" else lib.n2d_lu_solve32
+    sf.restype, sf.argtypes = C.c_int, [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_void_p,
+                                        C.c_longlong, C.c_longlong]
+    rhs = torch.ones(n, dtype=torch.complex128, device="cuda")
+    ss = []
+    for i in range(reps + 1):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ok = sf(work.data_ptr(), n, ld, piv.data_ptr(), rhs.data_ptr(), n, 1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if not ok:
+            raise RuntimeError("device solve failed: " + nb.last_error())
+        if i:
+            ss.append(e0.elapsed_time(e1))
+    return min(ts), min(ss)
 
 
 def lu_driver(args, nb, torch, stream):
     a = c1_matrix()
     out = {form: device_factor(nb, torch, stream, a, form, max(1, args.steps)) for form in ("cuda", "cuda-mixed")}
-    print(json.dumps({"profile": "lu", "order": a.shape[0], "device_factor_ms": out}))
+    print(json.dumps({"profile": "lu", "order": a.shape[0],
+                      "device_factor_ms": {f: t[0] for f, t in out.items()},
+                      "device_solve_ms": {f: t[1] for f, t in out.items()}}))
     return 0
 
 
@@ -660,7 +680,7 @@ def dense_bench(nb, torch, stream):
         np.linalg.norm(sols["cuda-mixed"] - sols["cuda"]) / np.linalg.norm(sols["cuda"]))
     # Device factor alone (resident matrices, CUDA events).
     for form in ("cuda", "cuda-mixed"):
-        out[form]["device_factor_ms"] = device_factor(nb, torch, stream, a, form, 3)
+        out[form]["device_factor_ms"], out[form]["device_solve_ms"] = device_factor(nb, torch, stream, a, form, 3)
     return out
 
 
