@@ -16,8 +16,9 @@
  * sweep of one model, nec2c_cuda_gmres_batch).
  * Volume requests run GMRES on a plan or hybrid system the caller created and
  * keeps on the device across requests (a frequency's spectrum is built once);
- * a plan is not reentrant (vie_fft.h:6), so two requests on the same plan
- * never run at the same time.  Admission is FIFO, except that a request that
+ * a plan is not reentrant (vie_fft.h:6), so two requests that run on the same
+ * plan (directly, through a hybrid system or in a batch) never run at the
+ * same time.  Admission is FIFO, except that a request that
  * does not fit may be passed by later ones that do, at most `slots` times
  * each before the queue waits for it. */
 #include <errno.h>
@@ -33,6 +34,8 @@
 
 int n2c_dense_solve_private(size_t n, const nec2c_cuda_complex *matrix, size_t ld, nec2c_cuda_complex *rhs,
                             size_t stride, size_t count, int split, int *steps);
+const nec2c_cuda_vie_plan *n2c_hybrid_volume_plan(const nec2c_cuda_hybrid *h);
+const nec2c_cuda_vie_plan *n2c_batch_plan(const nec2c_cuda_vie_batch *b, size_t q);
 
 struct nec2c_cuda_server {
   int device, slots, split;
@@ -41,7 +44,7 @@ struct nec2c_cuda_server {
   pthread_cond_t work, done;
   nec2c_cuda_request **queue;   /* FIFO, [head, head + count) modulo cap */
   size_t head, count, cap;
-  const void **busy;            /* operators with a request in flight */
+  const nec2c_cuda_request **busy;   /* request in flight per worker */
   size_t pending;               /* submitted, not finished */
   int stop, started;
   pthread_t *threads;
@@ -73,10 +76,19 @@ static size_t footprint(const nec2c_cuda_server *s, const nec2c_cuda_request *r)
   }
 }
 
-static const void *request_op(const nec2c_cuda_request *r)
+/* The volume plans a request runs on.  A hybrid system runs its plan's
+ * passes on the plan's work grids, and a batch those of every system's plan
+ * (one plan appears at most once in a batch), so exclusivity is per plan. */
+static size_t request_plans(const nec2c_cuda_request *r)
 {
-  if(r->kind == NEC2C_CUDA_REQUEST_BATCH) return r->batch;
-  return r->kind == NEC2C_CUDA_REQUEST_VOLUME ? (r->plan ? (const void *)r->plan : (const void *)r->system) : NULL;
+  if(r->kind == NEC2C_CUDA_REQUEST_BATCH) return nec2c_cuda_vie_batch_systems(r->batch);
+  return r->kind == NEC2C_CUDA_REQUEST_VOLUME ? 1 : 0;
+}
+
+static const nec2c_cuda_vie_plan *request_plan(const nec2c_cuda_request *r, size_t q)
+{
+  if(r->kind == NEC2C_CUDA_REQUEST_BATCH) return n2c_batch_plan(r->batch, q);
+  return r->plan ? r->plan : n2c_hybrid_volume_plan(r->system);
 }
 
 /* Every system of the batch at once; the request's report summarises them. */
@@ -111,11 +123,20 @@ static int run_batch(nec2c_cuda_request *r)
   return ok;
 }
 
-static int op_busy(const nec2c_cuda_server *s, const void *op)
+/* True when c shares a volume plan with a request in flight. */
+static int plan_busy(const nec2c_cuda_server *s, const nec2c_cuda_request *c)
 {
+  const size_t n = request_plans(c);
+  size_t a, b;
   int i;
-  if(!op) return 0;
-  for(i = 0; i < s->slots; ++i) if(s->busy[i] == op) return 1;
+  if(n == 0) return 0;
+  for(i = 0; i < s->slots; ++i) {
+    const nec2c_cuda_request *r = s->busy[i];
+    const size_t m = r ? request_plans(r) : 0;
+    for(a = 0; a < n; ++a)
+      for(b = 0; b < m; ++b)
+        if(request_plan(c, a) == request_plan(r, b)) return 1;
+  }
   return 0;
 }
 
@@ -158,7 +179,7 @@ static void *worker(void *arg)
       nec2c_cuda_request *c = s->queue[(s->head + q) % s->cap];
       const size_t f = footprint(s, c);
       const int fits = s->in_use == 0 || (f <= s->budget && s->in_use + f <= s->budget);
-      if(fits && !op_busy(s, request_op(c))) { r = c; pick = q; fp = f; break; }
+      if(fits && !plan_busy(s, c)) { r = c; pick = q; fp = f; break; }
       /* A request that does not fit may be passed only `slots` times. */
       if(!fits && c->skipped >= (unsigned)s->slots) break;
     }
@@ -172,7 +193,7 @@ static void *worker(void *arg)
       s->queue[(s->head + q) % s->cap] = s->queue[(s->head + q + 1) % s->cap];
     s->count--;
     s->in_use += fp;
-    for(i = 0; i < s->slots; ++i) if(!s->busy[i]) { s->busy[i] = request_op(r) ? request_op(r) : (const void *)r; slot = i; break; }
+    for(i = 0; i < s->slots; ++i) if(!s->busy[i]) { s->busy[i] = r; slot = i; break; }
     r->footprint = fp;
     r->started_s = now_s();
     pthread_mutex_unlock(&s->lock);

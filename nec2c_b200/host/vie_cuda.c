@@ -379,6 +379,9 @@ int nec2c_cuda_hybrid_set_blocks(nec2c_cuda_hybrid *h, const nec2c_cuda_complex 
 
 size_t nec2c_cuda_hybrid_order(const nec2c_cuda_hybrid *h) { return h ? h->c + h->v : 0; }
 
+/* The volume plan a hybrid system runs on (request server exclusivity). */
+const nec2c_cuda_vie_plan *n2c_hybrid_volume_plan(const nec2c_cuda_hybrid *h) { return h ? h->volume : NULL; }
+
 static int hybrid_ready(struct nec2c_cuda_hybrid *h)
 {
   if(!h->blocks_set) { n2c_set_error("hybrid blocks were never uploaded"); return 0; }
@@ -584,6 +587,12 @@ int nec2c_cuda_hybrid_batch_create(nec2c_cuda_vie_batch **out, nec2c_cuda_hybrid
 
 size_t nec2c_cuda_vie_batch_order(const nec2c_cuda_vie_batch *b) { return b ? b->order : 0; }
 size_t nec2c_cuda_vie_batch_systems(const nec2c_cuda_vie_batch *b) { return b ? b->count : 0; }
+
+/* The volume plan of system q of a batch (request server exclusivity). */
+const nec2c_cuda_vie_plan *n2c_batch_plan(const nec2c_cuda_vie_batch *b, size_t q)
+{
+  return b && q < b->count ? b->plans[q] : NULL;
+}
 size_t nec2c_cuda_vie_batch_offset(const nec2c_cuda_vie_batch *b, size_t q)
 {
   return b && q <= b->count ? b->offsets[q] : 0;

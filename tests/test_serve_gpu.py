@@ -215,3 +215,66 @@ def test_batch_requests_in_the_mix(near_tables):
         assert np.linalg.norm(out[: a.shape[0]] - sol) / np.linalg.norm(sol) < 1e-10
     srv.close()
     batch.close()
+
+
+def test_requests_sharing_a_plan_never_overlap(near_tables):
+    """A plan is not reentrant, and a hybrid system or a batch runs on its
+    systems' plans: requests that reach one plan by any of these routes run
+    one after the other, and each result is the one it gives alone
+    (bitwise)."""
+    from test_vie_batch_gpu import hybrid_blocks
+    h, k, table = near_tables["rand_k0.3"]
+    plans = []
+    for shape, fill, seed in (((7, 6, 5), 0.6, 21), ((8, 8, 8), 1.0, 22), ((6, 9, 4), 0.7, 23)):
+        xyz = cases.random_lattice(shape, fill, seed)
+        p = nb.VolumePlan(shape, xyz, h, k, 3.0, table)
+        for c, e in enumerate(cases.random_eps(xyz.size // 3, seed + 9, er=(2.0, 5.0))):
+            p.set_permittivity(c, e)
+        plans.append(p)
+    p1, p2, p3 = plans
+    blocks, n = hybrid_blocks(9, p3.n, 31)
+    hyb = nb.HybridSystem(p3, 9, p3.n)
+    hyb.set_blocks(blocks)
+    b12, b13 = nb.VolumeBatch([p1, p2]), nb.VolumeBatch([p1, p3])
+    rng = np.random.default_rng(41)
+
+    def rhs(m):
+        return rng.standard_normal(m) + 1j * rng.standard_normal(m)
+    work = [("plan", p1, rhs(p1.n)), ("batch", b12, rhs(b12.order)), ("plan", p2, rhs(p2.n)),
+            ("system", hyb, rhs(hyb.n)), ("batch", b13, rhs(b13.order)), ("plan", p3, rhs(p3.n)),
+            ("plan", p1, rhs(p1.n))]
+    uses = {"plan": lambda op: {id(op)}, "system": lambda op: {id(op.plan)},
+            "batch": lambda op: {id(p) for p in op.plans}}
+
+    def submit(srv, kind, op, b):
+        x = np.zeros_like(b)
+        if kind == "batch":
+            return srv.batch(op, b, x, rtol=1e-9, maxit=400), x
+        return srv.volume(op, b, x, rtol=1e-9, maxit=400), x
+
+    alone = nb.Server(slots=1)
+    ref = []
+    for kind, op, b in work:
+        r, x = submit(alone, kind, op, b)
+        assert alone.wait(r), r.error
+        ref.append(x)
+    alone.close()
+    mix = nb.Server(slots=4)
+    got = [submit(mix, kind, op, b) for kind, op, b in work]
+    mix.drain()
+    for (r, x), expect in zip(got, ref):
+        assert r.status and r.report.status == 0, r.error
+        assert np.array_equal(x, expect)
+    shared = 0
+    for i, (ki, oi, _) in enumerate(work):
+        for j, (kj, oj, _) in enumerate(work):
+            if i < j and uses[ki](oi) & uses[kj](oj):
+                shared += 1
+                a, b = got[i][0], got[j][0]
+                assert a.finished_s <= b.started_s or b.finished_s <= a.started_s
+    assert shared >= 8
+    # p2 and the hybrid system (on p3) share nothing: free to overlap.
+    assert not uses["plan"](p2) & uses["system"](hyb)
+    mix.close()
+    for o in (b12, b13, hyb, *plans):
+        o.close()
