@@ -1,6 +1,8 @@
 // Definitions behind fft_passes.cuh, included by the two per-precision
 // translation units only.
 #pragma once
+#include <atomic>
+
 #include "fft_passes.cuh"
 #include "runtime.cuh"
 
@@ -19,15 +21,17 @@ static void (*pass_kernel(int mode))(PassArgs<C>) {
 
 template <typename C, int R1, int R2>
 static int launch_rr(int mode, const PassArgs<C> &a, size_t smem, long long tiles) {
-  static bool configured[9] = {false, false, false, false, false, false, false, false, false};
+  // Set by whichever worker thread launches a mode first (the attribute
+  // calls are idempotent).
+  static std::atomic<bool> configured[9];
   void (*k)(PassArgs<C>) = pass_kernel<C, R1, R2>(mode);
-  if (!configured[mode]) {
+  if (!configured[mode].load(std::memory_order_acquire)) {
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
         cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess) {
       n2c_set_error("cannot raise shared memory for FFT pass");
       return 0;
     }
-    configured[mode] = true;
+    configured[mode].store(true, std::memory_order_release);
   }
   if (tiles > 0x7fffffffLL) { n2c_set_error("FFT pass grid too large"); return 0; }
   k<<<(unsigned)tiles, 256, smem, n2c_stream()>>>(a);

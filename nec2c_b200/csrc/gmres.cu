@@ -659,12 +659,12 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
   if (m > n) m = n;
   if (m > (long long)maxit) m = (long long)maxit;
   if (o.mixed && m <= MAXM) {
-    static bool configured = false;
-    if (!configured) {
+    static const bool configured = [] {
       cudaFuncSetAttribute(cgs_dots_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
       cudaFuncSetAttribute(cgs_dots_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
-      configured = true;
-    }
+      return true;
+    }();
+    (void)configured;
   }
   GmWork *w = work_get(o, m);
   if (!w) { rep->status = ST_ALLOC; return 0; }

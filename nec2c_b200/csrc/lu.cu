@@ -1152,11 +1152,9 @@ static cudaError_t launch_cluster_panel(const PanelArgs &p, cudaStream_t s) {
   return cudaLaunchKernelEx(&cfg, kernel, p);
 }
 
-// 1 when 16-CTA clusters of the panel kernel can be resident (checked once).
-static int cluster16_ok() {
-  static int state = -1;
-  if (state >= 0) return state;
-  state = 0;
+// 1 when 16-CTA clusters of the panel kernel can be resident.
+static int cluster16_probe() {
+  int state = 0;
   void (*kernels[4])(PanelArgs) = {panel_cluster_kernel<CMAX, 0, double2>, panel_cluster_kernel<CMAX, 1, double2>,
                                    panel_cluster_kernel<CMAX, 0, float2>, panel_cluster_kernel<CMAX, 1, float2>};
   for (auto k : kernels) {
@@ -1179,6 +1177,13 @@ static int cluster16_ok() {
   if (cudaOccupancyMaxActiveClusters(&clusters, panel_cluster_kernel<CMAX, 0, double2>, &cfg) == cudaSuccess && clusters > 0)
     state = 1;
   cudaGetLastError();
+  return state;
+}
+
+// Probed once per process; the static's initialisation is thread-safe, so
+// server workers that factor concurrently all see the probe's result.
+static int cluster16_ok() {
+  static const int state = cluster16_probe();
   return state;
 }
 
@@ -1389,15 +1394,28 @@ extern "C" int n2d_lu_factor32(float *a_dev, long long n, long long ld, int *ipi
 static size_t solve_smem(long long n) { return n <= SOLVE_PERM_MAX ? (size_t)8 * n : 0; }
 template <typename S>
 static int solve_configure() {
-  static int done = 0;
-  if (done) return 1;
-  if (cudaFuncSetAttribute(lu_solve_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * SOLVE_PERM_MAX) !=
-      cudaSuccess) {
+  static const bool done = cudaFuncSetAttribute(lu_solve_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                8 * SOLVE_PERM_MAX) == cudaSuccess;
+  if (!done) {
     n2c_set_error("triangular solve: shared memory configuration failed");
     return 0;
   }
-  done = 1;
   return 1;
+}
+
+// CTAs of the cooperative solve on this device (0: it cannot run).
+template <typename S>
+static int solve_coop_blocks() {
+  int per_sm = 0;
+  if (cudaFuncSetAttribute(lu_solve_coop_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SOLVE_COOP_SMEM) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lu_solve_coop_kernel<S>, SOLVE_COOP_THREADS,
+                                                    SOLVE_COOP_SMEM) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n2c_sm_count() < SOLVE_CTAS ? n2c_sm_count() : SOLVE_CTAS;
 }
 
 // Cooperative multi-CTA solve (orders >= SOLVE_COOP_MIN, up to
@@ -1407,21 +1425,8 @@ template <typename S>
 static int solve_coop(const S *a, long long n, long long ld, const int *ipiv, double2 *b, long long ldb,
                       long long nrhs) {
   if (n < SOLVE_COOP_MIN || nrhs > SOLVE_COOP_RHS || n > 0x7fffffffLL) return -1;
-  static int configured = 0, blocks = 0;
+  static const int blocks = solve_coop_blocks<S>();
   const size_t smem = SOLVE_COOP_SMEM;
-  if (!configured) {
-    int per_sm = 0;
-    if (cudaFuncSetAttribute(lu_solve_coop_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lu_solve_coop_kernel<S>, SOLVE_COOP_THREADS, smem) !=
-            cudaSuccess ||
-        per_sm < 1) {
-      cudaGetLastError();
-      return -1;
-    }
-    blocks = n2c_sm_count() < SOLVE_CTAS ? n2c_sm_count() : SOLVE_CTAS;
-    configured = 1;
-  }
   if (blocks < 2) return -1;   // the rows below the next block need a second CTA
   double2 *scratch = (double2 *)n2d_alloc_async((size_t)n * sizeof(double2));
   SolveSync *sy = (SolveSync *)n2d_alloc_async(sizeof(SolveSync) + 16);

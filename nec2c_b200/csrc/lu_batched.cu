@@ -150,14 +150,12 @@ extern "C" int n2d_lu_batched(double *mats_dev, double *rhs_dev, int *piv_dev, c
   if (nmax > BATCH_MAX) nmax = BATCH_MAX;
   const int lda = nmax + 1;
   const size_t smem = (size_t)lda * lda * sizeof(double2);   // matrix rows, then x
-  static int configured = 0;
+  static const bool configured =
+      cudaFuncSetAttribute(batched_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (BATCH_MAX + 1) * (BATCH_MAX + 1) * (int)sizeof(double2)) == cudaSuccess;
   if (!configured) {
-    if (cudaFuncSetAttribute(batched_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (BATCH_MAX + 1) * (BATCH_MAX + 1) * (int)sizeof(double2)) != cudaSuccess) {
-      n2c_set_error("batched LU: shared memory configuration failed");
-      return 0;
-    }
-    configured = 1;
+    n2c_set_error("batched LU: shared memory configuration failed");
+    return 0;
   }
   batched_lu_kernel<<<(unsigned)count, BT, smem, n2c_stream()>>>((double2 *)mats_dev, (double2 *)rhs_dev, piv_dev,
                                                                  (const BatchSystem *)systems_dev, info_dev, lda);

@@ -254,14 +254,12 @@ int n2c_tc_update(float *C, long long ldc, const float *A, long long lda, const 
     n2c_set_error("tensor-core update: operand and result rows must start 16-byte aligned");
     return 0;
   }
-  static int configured = 0;
+  static const bool configured =
+      cudaFuncSetAttribute(gemm_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) ==
+      cudaSuccess;
   if (!configured) {
-    if (cudaFuncSetAttribute(gemm_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) !=
-        cudaSuccess) {
-      n2c_set_error("tensor-core update: shared memory configuration failed");
-      return 0;
-    }
-    configured = 1;
+    n2c_set_error("tensor-core update: shared memory configuration failed");
+    return 0;
   }
   dim3 grid((unsigned)((N + TNC - 1) / TNC), (unsigned)((M + TM - 1) / TM));
   gemm_tf32x3_kernel<<<grid, THREADS, SMEM_BYTES, s>>>((float2 *)C, ldc, (const float2 *)A, lda, bt_hi, bt_lo, M, N,

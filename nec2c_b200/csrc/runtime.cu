@@ -275,12 +275,11 @@ extern "C" int n2d_device_ok(void) {
 }
 
 int n2c_sm_count() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
+  static const int sms = [] {
+    int dev = 0, n = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+  }();
   return sms;
 }

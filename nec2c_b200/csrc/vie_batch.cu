@@ -27,6 +27,7 @@
 #include <math.h>
 #include <string.h>
 #include <algorithm>
+#include <atomic>
 #include <vector>
 #include "common.cuh"
 #include "device_api.h"
@@ -741,14 +742,14 @@ static int build_set(n2d_vie_batch *b, int set) {
 template <typename C>
 static int launch_set_t(const n2d_vie_batch *b, const PassSet &ps, const double2 *x, double2 *y) {
   auto k = batch_kernel<C>(ps.mode);
-  static bool configured[9] = {false, false, false, false, false, false, false, false, false};
-  if (!configured[ps.mode]) {
+  static std::atomic<bool> configured[9];   // per mode, set by the first launching thread
+  if (!configured[ps.mode].load(std::memory_order_acquire)) {
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
         cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess) {
       n2c_set_error("cannot raise shared memory for the batched FFT pass");
       return 0;
     }
-    configured[ps.mode] = true;
+    configured[ps.mode].store(true, std::memory_order_release);
   }
   k<<<(unsigned)ps.tiles, 256, ps.smem, n2c_stream()>>>((const BatchDesc<C> *)ps.desc, ps.first, b->K, x, y);
   return n2c_check_launch("batched fft pass");
@@ -1082,12 +1083,12 @@ extern "C" int n2d_gmres_batch_dev(n2d_vie_batch *b, const double *b_dev, double
     n2c_set_error("batched GMRES restarts after at most %d steps", BMAXM);
     return 0;
   }
-  static bool configured = false;
-  if (!configured) {
+  static const bool configured = [] {
     cudaFuncSetAttribute(seg_dots_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DOT_SMEM);
     cudaFuncSetAttribute(seg_dots_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DOT_SMEM);
-    configured = true;
-  }
+    return true;
+  }();
+  (void)configured;
   BatchWork *w = work_get(b, m);
   if (!w) {
     for (int q = 0; q < K; ++q) reps[q].status = ST_ALLOC;
