@@ -300,11 +300,12 @@ int nec2c_cuda_dense_factor_device_static(size_t order, nec2c_cuda_complex *matr
    of requests in flight overlaps on the device.  Dense requests factor and
    solve a private device copy of the matrix (the host matrix is not
    modified; rhs receives the solutions); volume requests run GMRES on a plan
-   or hybrid system the caller created and keeps resident across requests
-   (never two at once on the same operator).  Batch requests solve every
-   system of a plan batch at once (a frequency sweep of one model), never
-   two at once on the same batch; a plan in a batch must not be submitted on
-   its own while a request on its batch is in flight. */
+   or hybrid system the caller created and keeps resident across requests.
+   Batch requests solve every system of a plan batch at once (a frequency
+   sweep of one model).  A plan is not reentrant, and hybrid systems and
+   batches run on their plans' work grids, so two requests that reach the
+   same plan (directly, through a hybrid system or in a batch) never run at
+   the same time. */
 enum { NEC2C_CUDA_REQUEST_DENSE = 1, NEC2C_CUDA_REQUEST_VOLUME = 2, NEC2C_CUDA_REQUEST_BATCH = 3 };
 typedef struct {
   int kind;
