@@ -773,14 +773,16 @@ extern "C" int n2d_gmres(int kind, void *op, long long n, const double *b, doubl
   memset(rep, 0, sizeof(*rep));
   rep->status = ST_ALLOC;
   rep->residual_norm = rep->relative_residual = INFINITY;
-  double *bd = (double *)n2d_alloc(n * sizeof(double2)), *xd = (double *)n2d_alloc(n * sizeof(double2));
+  // Stream-ordered staging: a server worker's solve must not synchronise the
+  // device (cudaFree would wait for every other worker's work in flight).
+  double *bd = (double *)n2d_alloc_async(n * sizeof(double2)), *xd = (double *)n2d_alloc_async(n * sizeof(double2));
   int ok = 0;
   if (bd && xd && n2d_upload(bd, b, n * sizeof(double2)) && n2d_upload(xd, x, n * sizeof(double2))) {
     ok = n2d_gmres_dev(kind, op, n, bd, xd, restart, maxit, rtol, atol, rep);
     // x is updated even on failure (vie_iterative.h:51-53).
     if (!n2d_download(x, xd, n * sizeof(double2))) ok = 0;
   }
-  n2d_free(bd);
-  n2d_free(xd);
+  n2d_free_async(bd);
+  n2d_free_async(xd);
   return ok;
 }
