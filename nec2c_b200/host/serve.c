@@ -101,7 +101,7 @@ static int run_batch(nec2c_cuda_request *r)
   int ok;
   bv = malloc((k ? k : 1) * sizeof(*bv));
   xv = malloc((k ? k : 1) * sizeof(*xv));
-  if(!bv || !xv) { free(bv); free(xv); return 0; }
+  if(!bv || !xv) { free(bv); free(xv); n2c_set_error("batch request: out of host memory"); return 0; }
   for(q = 0; q < k; ++q) {
     bv[q] = r->b + nec2c_cuda_vie_batch_offset(r->batch, q);
     xv[q] = r->x + nec2c_cuda_vie_batch_offset(r->batch, q);
@@ -260,23 +260,34 @@ int nec2c_cuda_server_create(nec2c_cuda_server **out, int device, int slots, siz
 
 int nec2c_cuda_server_submit(nec2c_cuda_server *s, nec2c_cuda_request *r)
 {
-  if(!s || !r) return 0;
+  if(!s || !r) { n2c_set_error("submit: null server or request"); return 0; }
   if(r->kind == NEC2C_CUDA_REQUEST_DENSE) {
     if(!r->matrix || !r->rhs || r->order == 0 || r->ld < r->order || r->rhs_count == 0 ||
-       r->rhs_stride < r->order) return 0;
+       r->rhs_stride < r->order) {
+      n2c_set_error("submit: dense request needs matrix, rhs, order > 0, ld >= order, rhs_count > 0 and "
+                    "rhs_stride >= order");
+      return 0;
+    }
   } else if(r->kind == NEC2C_CUDA_REQUEST_VOLUME) {
-    if((!r->plan) == (!r->system) || !r->b || !r->x) return 0;
+    if((!r->plan) == (!r->system) || !r->b || !r->x) {
+      n2c_set_error("submit: volume request needs exactly one of plan / system, and b and x");
+      return 0;
+    }
   } else if(r->kind == NEC2C_CUDA_REQUEST_BATCH) {
-    if(!r->batch || !r->b || !r->x || !r->reports || r->b == (const nec2c_cuda_complex *)r->x) return 0;
+    if(!r->batch || !r->b || !r->x || !r->reports || r->b == (const nec2c_cuda_complex *)r->x) {
+      n2c_set_error("submit: batch request needs batch, reports and distinct b and x");
+      return 0;
+    }
   } else {
+    n2c_set_error("submit: unknown request kind %d", r->kind);
     return 0;
   }
   pthread_mutex_lock(&s->lock);
-  if(s->stop) { pthread_mutex_unlock(&s->lock); return 0; }
+  if(s->stop) { pthread_mutex_unlock(&s->lock); n2c_set_error("submit: server is stopping"); return 0; }
   if(s->count == s->cap) {
     nec2c_cuda_request **q = malloc(2 * s->cap * sizeof(*q));
     size_t i;
-    if(!q) { pthread_mutex_unlock(&s->lock); return 0; }
+    if(!q) { pthread_mutex_unlock(&s->lock); n2c_set_error("submit: out of host memory"); return 0; }
     for(i = 0; i < s->count; ++i) q[i] = s->queue[(s->head + i) % s->cap];
     free(s->queue);
     s->queue = q; s->head = 0; s->cap *= 2;

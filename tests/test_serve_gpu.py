@@ -278,3 +278,17 @@ def test_requests_sharing_a_plan_never_overlap(near_tables):
     mix.close()
     for o in (b12, b13, hyb, *plans):
         o.close()
+
+
+def test_submit_rejections_say_why():
+    """A request the server refuses at submission leaves the reason in
+    nec2c_cuda_last_error, and nothing is queued."""
+    srv = nb.Server(slots=1)
+    for kind, why in ((99, "unknown request kind 99"), (nb.REQUEST_VOLUME, "exactly one of plan"),
+                      (nb.REQUEST_BATCH, "batch request needs"), (nb.REQUEST_DENSE, "dense request needs")):
+        r = nb.Request()
+        r.kind = kind
+        with pytest.raises(RuntimeError, match=why):
+            srv._submit(r, ())
+    srv.drain()
+    srv.close()
