@@ -27,10 +27,10 @@ unsigned long long nec2c_cuda_launch_count(void) { return n2d_launch_count(); }
 
 int nec2c_cuda_vie_fft_backend_set(const char *name)
 {
-  if(!name) return 0;
+  if(!name) { n2c_set_error("FFT backend: null name"); return 0; }
   if(!strcmp(name, "cuda")) g_fft_fp32 = 0;
   else if(!strcmp(name, "cuda-mixed")) g_fft_fp32 = 1;
-  else return 0;
+  else { n2c_set_error("unknown FFT backend '%s' (cuda, cuda-mixed)", name); return 0; }
   return 1;
 }
 const char *nec2c_cuda_vie_fft_backend_name(void) { return g_fft_fp32 ? "cuda-mixed" : "cuda"; }
@@ -238,8 +238,13 @@ fail:
 int nec2c_cuda_vie_fft_set_permittivity(nec2c_cuda_vie_plan *p, size_t cell, double re, double im)
 {
   double complex er = re + I * im;
-  if(!p || cell >= p->cells || !isfinite(re) || !isfinite(im) || re < 1 || im > 0) return 0;
-  if(!diag_ok(p->self, er)) return 0;
+  if(!p || cell >= p->cells) { n2c_set_error("set_permittivity: no plan or cell out of range"); return 0; }
+  /* vie_fft.c's material check: finite, Re >= 1, Im <= 0. */
+  if(!isfinite(re) || !isfinite(im) || re < 1 || im > 0) {
+    n2c_set_error("set_permittivity: need a finite eps with Re >= 1 and Im <= 0");
+    return 0;
+  }
+  if(!diag_ok(p->self, er)) { n2c_set_error("set_permittivity: Jacobi divisor of cell %zu vanishes", cell); return 0; }
   p->eps[cell] = er;
   p->eps_dirty = 1;
   return 1;
@@ -252,6 +257,7 @@ size_t nec2c_cuda_vie_fft_order(const nec2c_cuda_vie_plan *p) { return p ? 3 * p
 /* Exposed to the hybrid and GMRES code in this layer. */
 __attribute__((visibility("hidden"))) n2d_vie *nec2c_cuda_plan_device(nec2c_cuda_vie_plan *p)
 {
+  if(!p) { n2c_set_error("null plan"); return NULL; }
   if(p->eps_dirty && !upload_eps(p)) return NULL;
   return p->dev;
 }
@@ -259,8 +265,10 @@ __attribute__((visibility("hidden"))) n2d_vie *nec2c_cuda_plan_device(nec2c_cuda
 int nec2c_cuda_vie_fft_apply(void *ctx, const nec2c_cuda_complex *x, nec2c_cuda_complex *y)
 {
   struct nec2c_cuda_vie_plan *p = ctx;
-  size_t bytes = 3 * p->cells * sizeof(double complex);
+  size_t bytes;
   if(!nec2c_cuda_plan_device(p)) return 0;
+  if(!x || !y) { n2c_set_error("null vector"); return 0; }
+  bytes = 3 * p->cells * sizeof(double complex);
   return n2d_upload(p->x_dev, x, bytes) && n2d_vie_apply(p->dev, p->x_dev, p->y_dev, 0, NULL, NULL, 0) &&
          n2d_download(y, p->y_dev, bytes);
 }
@@ -268,8 +276,10 @@ int nec2c_cuda_vie_fft_apply(void *ctx, const nec2c_cuda_complex *x, nec2c_cuda_
 int nec2c_cuda_vie_fft_precondition(void *ctx, const nec2c_cuda_complex *x, nec2c_cuda_complex *y)
 {
   struct nec2c_cuda_vie_plan *p = ctx;
-  size_t bytes = 3 * p->cells * sizeof(double complex);
+  size_t bytes;
   if(!nec2c_cuda_plan_device(p)) return 0;
+  if(!x || !y) { n2c_set_error("null vector"); return 0; }
+  bytes = 3 * p->cells * sizeof(double complex);
   return n2d_upload(p->x_dev, x, bytes) && n2d_vie_precondition(p->dev, p->x_dev, p->y_dev) &&
          n2d_download(y, p->y_dev, bytes);
 }
@@ -282,7 +292,8 @@ int nec2c_cuda_vie_fft_apply_device(nec2c_cuda_vie_plan *p, const void *x_dev, v
 
 int nec2c_cuda_vie_fft_spectrum(nec2c_cuda_vie_plan *p, nec2c_cuda_complex *out)
 {
-  return p && out && n2d_vie_read_spectrum(p->dev, (double *)out);
+  if(!p || !out) { n2c_set_error("spectrum: null plan or output"); return 0; }
+  return n2d_vie_read_spectrum(p->dev, (double *)out);
 }
 
 int nec2c_cuda_vie_fft_radiation_device(nec2c_cuda_vie_plan *p, const double origin[3], const void *current_dev,
@@ -290,7 +301,10 @@ int nec2c_cuda_vie_fft_radiation_device(nec2c_cuda_vie_plan *p, const double ori
 {
   double *dirs, *out;
   int ok;
-  if(!p || !origin || !current_dev || (count && (!directions || !amplitude))) return 0;
+  if(!p || !origin || !current_dev || (count && (!directions || !amplitude))) {
+    n2c_set_error("radiation: null plan, origin, current, directions or output");
+    return 0;
+  }
   if(count == 0) return 1;
   if(count > (size_t)1 << 28) { n2c_set_error("radiation: too many directions"); return 0; }
   dirs = n2d_alloc(3 * count * sizeof(double));
@@ -370,7 +384,7 @@ void nec2c_cuda_hybrid_destroy(nec2c_cuda_hybrid *h)
 
 int nec2c_cuda_hybrid_set_blocks(nec2c_cuda_hybrid *h, const nec2c_cuda_complex *blocks)
 {
-  if(!h || !blocks) return 0;
+  if(!h || !blocks) { n2c_set_error("set_blocks: null system or blocks"); return 0; }
   if(h->volume && !nec2c_cuda_plan_device(h->volume)) return 0;
   if(!n2d_hybrid_upload_blocks(h->dev, (const double *)blocks)) return 0;
   h->blocks_set = 1;
@@ -384,6 +398,7 @@ const nec2c_cuda_vie_plan *n2c_hybrid_volume_plan(const nec2c_cuda_hybrid *h) { 
 
 static int hybrid_ready(struct nec2c_cuda_hybrid *h)
 {
+  if(!h) { n2c_set_error("null hybrid system"); return 0; }
   if(!h->blocks_set) { n2c_set_error("hybrid blocks were never uploaded"); return 0; }
   return !h->volume || nec2c_cuda_plan_device(h->volume) != NULL;
 }
@@ -391,18 +406,27 @@ static int hybrid_ready(struct nec2c_cuda_hybrid *h)
 int nec2c_cuda_hybrid_apply(void *ctx, const nec2c_cuda_complex *x, nec2c_cuda_complex *y)
 {
   struct nec2c_cuda_hybrid *h = ctx;
-  size_t bytes = (h->c + h->v) * sizeof(double complex);
-  return hybrid_ready(h) && n2d_upload(h->x_dev, x, bytes) &&
+  size_t bytes;
+  if(!hybrid_ready(h)) return 0;
+  if(!x || !y) { n2c_set_error("null vector"); return 0; }
+  bytes = (h->c + h->v) * sizeof(double complex);
+  return n2d_upload(h->x_dev, x, bytes) &&
          n2d_hybrid_apply(h->dev, h->x_dev, h->y_dev, 0, NULL, NULL, 0) && n2d_download(y, h->y_dev, bytes);
 }
 
 int nec2c_cuda_hybrid_precondition(void *ctx, const nec2c_cuda_complex *x, nec2c_cuda_complex *y)
 {
   struct nec2c_cuda_hybrid *h = ctx;
-  size_t bytes = (h->c + h->v) * sizeof(double complex);
+  size_t bytes;
+  if(!hybrid_ready(h)) return 0;
+  if(!x || !y) { n2c_set_error("null vector"); return 0; }
+  bytes = (h->c + h->v) * sizeof(double complex);
   /* dielectric_fft.c:77-81: a zero or non-finite conductor diagonal fails. */
-  if(h->blocks_set && !n2d_hybrid_precondition_ok(h->dev)) return 0;
-  return hybrid_ready(h) && n2d_upload(h->x_dev, x, bytes) &&
+  if(!n2d_hybrid_precondition_ok(h->dev)) {
+    n2c_set_error("hybrid preconditioner: a diagonal entry is zero or not finite");
+    return 0;
+  }
+  return n2d_upload(h->x_dev, x, bytes) &&
          n2d_hybrid_precondition(h->dev, h->x_dev, h->y_dev) && n2d_download(y, h->y_dev, bytes);
 }
 
@@ -600,7 +624,7 @@ size_t nec2c_cuda_vie_batch_offset(const nec2c_cuda_vie_batch *b, size_t q)
 
 int nec2c_cuda_vie_batch_schedule(const nec2c_cuda_vie_batch *b, int scale[5], int variant[5])
 {
-  if(!b || !scale || !variant) return 0;
+  if(!b || !scale || !variant) { n2c_set_error("batch schedule: bad argument"); return 0; }
   n2d_vie_batch_schedule(b->dev, scale, variant);
   return 1;
 }
@@ -613,7 +637,7 @@ int nec2c_cuda_vie_batch_set_schedule(nec2c_cuda_vie_batch *b, const int scale[5
 
 int nec2c_cuda_vie_batch_apply_device(nec2c_cuda_vie_batch *b, const void *x_dev, void *y_dev)
 {
-  if(!b || !x_dev || !y_dev || x_dev == y_dev) return 0;
+  if(!b || !x_dev || !y_dev || x_dev == y_dev) { n2c_set_error("batch apply: bad argument"); return 0; }
   return batch_ready(b) && n2d_vie_batch_apply(b->dev, x_dev, y_dev);
 }
 
@@ -637,9 +661,12 @@ static int batch_solve(nec2c_cuda_vie_batch *b, const void *b_dev, void *x_dev,
     reports[q].residual_norm = reports[q].relative_residual = INFINITY;
   }
   if(!options) options = &defaults;
-  if(!batch_options_ok(options) || b_dev == x_dev) return 0;
+  if(!batch_options_ok(options) || b_dev == x_dev) {
+    n2c_set_error(b_dev == x_dev ? "batch solve: b and x must differ" : "batch solve: invalid GMRES options");
+    return 0;
+  }
   r = calloc(b->count, sizeof(*r));
-  if(!r) return 0;
+  if(!r) { n2c_set_error("batch solve: out of host memory"); return 0; }
   ok = batch_ready(b) &&
        n2d_gmres_batch_dev(b->dev, b_dev, x_dev, options->restart, options->maximum_iterations,
                            options->relative_tolerance, options->absolute_tolerance, r);
@@ -658,7 +685,7 @@ static int batch_solve(nec2c_cuda_vie_batch *b, const void *b_dev, void *x_dev,
 int nec2c_cuda_gmres_batch_device(nec2c_cuda_vie_batch *b, const void *b_dev, void *x_dev,
                                   const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *reports)
 {
-  if(!b || !b_dev || !x_dev || !reports) return 0;
+  if(!b || !b_dev || !x_dev || !reports) { n2c_set_error("batch solve: null batch, vector or reports"); return 0; }
   return batch_solve(b, b_dev, x_dev, options, reports);
 }
 
@@ -667,22 +694,35 @@ int nec2c_cuda_gmres_batch(nec2c_cuda_vie_batch *b, const nec2c_cuda_complex *co
                            nec2c_cuda_gmres_report *reports)
 {
   const size_t cpx = sizeof(nec2c_cuda_complex);
-  int ok = 1;
-  if(!b || !bv || !xv || !reports) return 0;
-  for(size_t q = 0; q < b->count; ++q) if(!bv[q] || !xv[q]) return 0;
+  int ok = 1, whole = 1;
+  if(!b || !bv || !xv || !reports) { n2c_set_error("batch solve: null batch, vector list or reports"); return 0; }
+  for(size_t q = 0; q < b->count; ++q)
+    if(!bv[q] || !xv[q]) { n2c_set_error("batch solve: vector of system %zu is NULL", q); return 0; }
+  /* Vectors that lie back to back in host memory (a server batch request's
+     concatenated b and x) move in one copy each way. */
+  for(size_t q = 1; q < b->count && whole; ++q)
+    whole = bv[q] == bv[0] + b->offsets[q] && xv[q] == xv[0] + b->offsets[q];
   if(!b->b_dev) b->b_dev = n2d_alloc(b->order * cpx);
   if(!b->x_dev) b->x_dev = n2d_alloc(b->order * cpx);
   if(!b->b_dev || !b->x_dev) return 0;
-  for(size_t q = 0; q < b->count && ok; ++q) {
-    const size_t off = b->offsets[q] * cpx, bytes = (b->offsets[q + 1] - b->offsets[q]) * cpx;
-    ok = n2d_upload((char *)b->b_dev + off, bv[q], bytes) && n2d_upload((char *)b->x_dev + off, xv[q], bytes);
+  if(whole) {
+    ok = n2d_upload(b->b_dev, bv[0], b->order * cpx) && n2d_upload(b->x_dev, xv[0], b->order * cpx);
+  } else {
+    for(size_t q = 0; q < b->count && ok; ++q) {
+      const size_t off = b->offsets[q] * cpx, bytes = (b->offsets[q + 1] - b->offsets[q]) * cpx;
+      ok = n2d_upload((char *)b->b_dev + off, bv[q], bytes) && n2d_upload((char *)b->x_dev + off, xv[q], bytes);
+    }
   }
   if(!ok) return 0;
   ok = batch_solve(b, b->b_dev, b->x_dev, options, reports);
   /* x is copied back even when a solve fails (vie_iterative.h:51-53). */
-  for(size_t q = 0; q < b->count; ++q) {
-    const size_t off = b->offsets[q] * cpx, bytes = (b->offsets[q + 1] - b->offsets[q]) * cpx;
-    if(!n2d_download(xv[q], (char *)b->x_dev + off, bytes)) ok = 0;
+  if(whole) {
+    if(!n2d_download(xv[0], b->x_dev, b->order * cpx)) ok = 0;
+  } else {
+    for(size_t q = 0; q < b->count; ++q) {
+      const size_t off = b->offsets[q] * cpx, bytes = (b->offsets[q + 1] - b->offsets[q]) * cpx;
+      if(!n2d_download(xv[q], (char *)b->x_dev + off, bytes)) ok = 0;
+    }
   }
   return ok;
 }

@@ -89,6 +89,35 @@ def test_new_entry_points_refuse_bad_arguments_without_a_device():
     assert not lib.nec2c_cuda_vie_batch_set_schedule(None, tiles, r1)
     origin = (C.c_double * 3)(0, 0, 0)
     assert not lib.nec2c_cuda_vie_fft_radiation_device(None, origin, vp(16), 1, vp(16), vp(16))
+    assert "radiation" in nb.last_error()
+
+
+def test_bad_arguments_say_why_without_a_device():
+    """Entry points refuse null handles and bad values before any device call,
+    with the reason in nec2c_cuda_last_error (no crash on a null handle)."""
+    import nec2c_b200 as nb
+    lib = nb.load()
+    vp = C.c_void_p
+    buf = (C.c_double * 8)()
+    cases = [
+        (lambda: lib.nec2c_cuda_vie_fft_backend_set(b"bogus"), "unknown FFT backend"),
+        (lambda: lib.nec2c_cuda_vie_fft_apply(None, buf, buf), "null plan"),
+        (lambda: lib.nec2c_cuda_vie_fft_precondition(None, buf, buf), "null plan"),
+        (lambda: lib.nec2c_cuda_vie_fft_apply_device(None, vp(16), vp(32)), "null plan"),
+        (lambda: lib.nec2c_cuda_hybrid_apply(None, buf, buf), "null hybrid"),
+        (lambda: lib.nec2c_cuda_hybrid_precondition(None, buf, buf), "null hybrid"),
+        (lambda: lib.nec2c_cuda_hybrid_set_blocks(None, buf), "set_blocks"),
+        (lambda: lib.nec2c_cuda_vie_fft_spectrum(None, buf), "spectrum"),
+        (lambda: lib.nec2c_cuda_gmres_batch_device(None, vp(16), vp(32), None, (nb.GmresReport * 1)()),
+         "batch solve"),
+        (lambda: lib.nec2c_cuda_gmres_batch(None, None, None, None, None), "batch solve"),
+        (lambda: lib.nec2c_cuda_vie_batch_apply_device(None, vp(16), vp(32)), "batch apply"),
+        (lambda: lib.nec2c_cuda_vie_batch_schedule(None, None, None), "batch schedule"),
+    ]
+    for call, why in cases:
+        assert not call()
+        assert why in nb.last_error(), (why, nb.last_error())
+    assert lib.nec2c_cuda_vie_fft_backend_set(b"cuda")
 
 
 def test_autotune_switch():
