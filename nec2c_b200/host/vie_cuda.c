@@ -239,7 +239,8 @@ int nec2c_cuda_vie_fft_set_permittivity(nec2c_cuda_vie_plan *p, size_t cell, dou
 {
   double complex er = re + I * im;
   if(!p || cell >= p->cells) { n2c_set_error("set_permittivity: no plan or cell out of range"); return 0; }
-  /* vie_fft.c's material check: finite, Re >= 1, Im <= 0. */
+  /* vie_fft.c:448-453: a finite eps with Re >= 1 and Im <= 0, and a Jacobi
+     divisor of at least 1e-30 on every axis. */
   if(!isfinite(re) || !isfinite(im) || re < 1 || im > 0) {
     n2c_set_error("set_permittivity: need a finite eps with Re >= 1 and Im <= 0");
     return 0;
