@@ -13,6 +13,7 @@
 #include "vie_iterative.h"
 #include "dense_backend.h"
 #include "dielectric.h"
+#include "dielectric_fft.h"
 
 #include <stdio.h>
 #include <stdlib.h>
@@ -142,4 +143,64 @@ int ref_radiation_amplitude(size_t cells, const double *centers, double h, const
   gnd.ksymp = saved;
   free(c);
   return 1;
+}
+
+/* The hybrid [C B; D V] system through the reference's own
+   dielectric_fft_prepare(_pec) (dielectric_fft.c:89-175): cubic cells of
+   side h centred at centers[3 i], cell i of permittivity eps[i] (one material
+   per cell, no conductivity), then the conductor rows [C|B] (row-major,
+   c x (c + 3 cells)) and the cross block D (row-major, 3 cells x c) written
+   through dielectric_fft_entry as the reference's wire assembly does. */
+void *ref_hybrid_create(size_t cells, const double *centers, double h, const complex double *eps,
+                        size_t conductors, const complex double *blocks, double k0, int pec)
+{
+  dielectric_model model;
+  dielectric_mesh_result mesh;
+  dielectric_diagnostic diagnostic;
+  dielectric_material *materials = calloc(cells ? cells : 1, sizeof(*materials));
+  dielectric_cell *cell = calloc(cells ? cells : 1, sizeof(*cell));
+  dielectric_fft_system *system = NULL;
+  const size_t c = conductors, n = conductors + 3 * cells;
+  int ok;
+  if(!materials || !cell) { free(materials); free(cell); return NULL; }
+  memset(&model, 0, sizeof(model));
+  memset(&mesh, 0, sizeof(mesh));
+  for(size_t i = 0; i < cells; ++i) {
+    materials[i].id = (int)i + 1;
+    materials[i].epsilon_r = creal(eps[i]);
+    materials[i].epsilon_loss = -cimag(eps[i]);
+    cell[i].material_id = (int)i + 1;
+    for(int a = 0; a < 3; ++a) { cell[i].center[a] = centers[3 * i + a]; cell[i].size[a] = h; }
+  }
+  model.materials = materials;
+  model.material_count = cells;
+  mesh.cells = cell;
+  mesh.cell_count = cells;
+  ok = pec ? dielectric_fft_prepare_pec(&system, &model, &mesh, c, k0, 0, &diagnostic)
+           : dielectric_fft_prepare(&system, &model, &mesh, c, k0, 0, &diagnostic);
+  free(materials);
+  free(cell);
+  if(!ok) return NULL;
+  for(size_t i = 0; i < n; ++i)
+    for(size_t j = 0; j < n; ++j)
+      if(i < c || j < c)
+        *dielectric_fft_entry(system, i, j) = i < c ? blocks[i * n + j] : blocks[c * n + (i - c) * c + j];
+  return system;
+}
+void ref_hybrid_destroy(void *system) { dielectric_fft_free(system); }
+int ref_hybrid_apply(void *system, const complex double *x, complex double *y)
+{ vie_linear_operator op; dielectric_fft_get_operator(system, &op); return op.apply(op.context, x, y); }
+int ref_hybrid_precondition(void *system, const complex double *x, complex double *y)
+{
+  vie_linear_operator op;
+  dielectric_fft_get_operator(system, &op);
+  return op.precondition(op.precondition_context, x, y);
+}
+int ref_hybrid_gmres(void *system, const complex double *b, complex double *x, size_t restart,
+                     size_t maxit, double rtol, double atol, vie_gmres_report *report)
+{
+  vie_linear_operator op;
+  vie_gmres_options o = {restart, maxit, rtol, atol};
+  dielectric_fft_get_operator(system, &op);
+  return vie_gmres(&op, b, x, &o, report);
 }

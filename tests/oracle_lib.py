@@ -108,6 +108,14 @@ def reference():
         r.ref_row_major_solve.restype = i
         r.ref_radiation_amplitude.argtypes = [sz, vp, dbl, vp, dbl, vp, vp]
         r.ref_radiation_amplitude.restype = i
+        r.ref_hybrid_create.argtypes = [sz, vp, dbl, vp, sz, vp, dbl, i]
+        r.ref_hybrid_create.restype = vp
+        r.ref_hybrid_destroy.argtypes = [vp]
+        for f in ("ref_hybrid_apply", "ref_hybrid_precondition"):
+            getattr(r, f).argtypes = [vp, vp, vp]
+            getattr(r, f).restype = i
+        r.ref_hybrid_gmres.argtypes = [vp, vp, vp, sz, sz, dbl, dbl, C.POINTER(Report)]
+        r.ref_hybrid_gmres.restype = i
         _ref = r
     return _ref
 

@@ -292,3 +292,51 @@ def test_radiation_amplitude_matches_reference():
         a = oracle_lib.radiation_amplitude(centers, h, current, k0, d)
         r = oracle_lib.radiation_amplitude(centers, h, current, k0, d, use_reference=True)
         assert np.max(np.abs(a - r)) <= 1e-13 * np.max(np.abs(r))
+
+
+@needs_ref
+@pytest.mark.parametrize("pec,gap", [(False, 0.0), (True, 0.0), (True, 0.125)])
+def test_hybrid_matches_reference(near_tables, pec, gap):
+    """The hybrid [C B; D V] operator, its preconditioner and GMRES on it, the
+    reference's through its own dielectric_fft_prepare(_pec) /
+    dielectric_fft_entry / dielectric_fft_get_operator, against the oracle
+    restatement on the same cells and blocks: bit-identical, in free space and
+    with PEC images (bottom gap 0 and half a cell)."""
+    from test_hybrid_gpu import lattice
+    from test_vie_batch_gpu import hybrid_blocks
+    h, k, table = near_tables["diel_k0.5"]
+    idx = cases.random_lattice((4, 3, 3), 0.7, seed=17).reshape(-1, 3).astype(float)
+    centers = np.ascontiguousarray(0.1 + h * idx)
+    centers[:, 2] = gap + h / 2 + h * idx[:, 2]
+    cells = len(centers)
+    eps = cases.random_eps(cells, seed=18, er=(2.0, 5.0))
+    c, v = 4, 3 * cells
+    blocks, n = hybrid_blocks(c, v, 19)
+    r = oracle_lib.reference()
+    r.ref_fft_backend_set(b"builtin")
+    rs = r.ref_hybrid_create(cells, ptr(centers), h, ptr(np.ascontiguousarray(eps)), c, ptr(blocks), k,
+                             1 if pec else 0)
+    assert rs
+    shape, xyz = lattice(centers, h, pec)
+    op = OraclePlan(shape, xyz, h, k, eps[0], table)
+    for i, e in enumerate(eps):
+        for q in ([i, cells + i] if pec else [i]):
+            assert op.set_permittivity(q, e)
+    oh = OracleHybrid(op, c, v, blocks, pec)
+    rng = np.random.default_rng(20)
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    y_ref, p_ref = np.empty(n, dtype=np.complex128), np.empty(n, dtype=np.complex128)
+    assert r.ref_hybrid_apply(rs, ptr(x), ptr(y_ref))
+    assert r.ref_hybrid_precondition(rs, ptr(x), ptr(p_ref))
+    assert np.array_equal(oh.apply(x), y_ref)
+    ok, p = oh.precondition(x)
+    assert ok and np.array_equal(p, p_ref)
+    b = y_ref.copy()
+    ok1, x1, rep1 = oh.gmres(b, rtol=1e-10)
+    x2 = np.zeros_like(b)
+    rep2 = Report()
+    ok2 = r.ref_hybrid_gmres(rs, ptr(b), ptr(x2), 30, 300, 1e-10, 0.0, C.byref(rep2))
+    assert ok1 and ok2
+    assert rep1["iterations"] == rep2.iterations and rep1["restarts"] == rep2.restarts
+    assert np.array_equal(x1, x2)
+    r.ref_hybrid_destroy(rs)
