@@ -340,3 +340,37 @@ def test_hybrid_matches_reference(near_tables, pec, gap):
     assert rep1["iterations"] == rep2.iterations and rep1["restarts"] == rep2.restarts
     assert np.array_equal(x1, x2)
     r.ref_hybrid_destroy(rs)
+
+
+@needs_ref
+@pytest.mark.parametrize("gap,pec", [(0.0, False), (0.0, True), (0.125, True)])
+def test_hybrid_against_dense_reference_kernel(near_tables, gap, pec):
+    """tests/dielectric_fft_test.c:8-46: two cells of two materials, the
+    product against the dense operator of the reference's pair tensors
+    (vie_cuboid_n, or vie_cuboid_pec_n over the ground plane) at 2e-7, and
+    GMRES recovering x to 1e-10."""
+    from test_hybrid_gpu import lattice
+    h, k, table = near_tables["diel_k0.5"]
+    centers = np.array([(0.0, 0.0, 0.125 + gap), (0.25, -0.25, 0.375 + gap)])
+    eps = [3 - 0.2j, 2 - 0.4j]
+    shape, xyz = lattice(centers, h, pec)
+    op = OraclePlan(shape, xyz, h, k, eps[0], table)
+    for i, e in enumerate(eps):
+        for q in ([i, 2 + i] if pec else [i]):
+            assert op.set_permittivity(q, e)
+    oh = OracleHybrid(op, 0, 6, np.zeros(1, dtype=np.complex128), pec)
+    j = np.arange(6)
+    x = np.sin(1 + j) + 1j * np.cos(0.3 * j)
+    expected = np.repeat(eps, 3) * x
+    r = oracle_lib.reference()
+    pair = r.ref_pair_tensor_pec if pec else r.ref_pair_tensor
+    block = np.empty(9, dtype=np.complex128)
+    for a in range(2):
+        for b in range(2):
+            assert pair(ptr(np.ascontiguousarray(centers[a])), ptr(np.ascontiguousarray(centers[b])), h, k,
+                        ptr(block))
+            expected[3 * a:3 * a + 3] -= (eps[a] - 1) * (block.reshape(3, 3) @ x[3 * b:3 * b + 3])
+    y = oh.apply(x)
+    assert np.max(np.abs(y - expected)) < 2e-7
+    ok, sol, rep = oh.gmres(y)
+    assert ok and np.max(np.abs(sol - x)) < 1e-10
