@@ -204,3 +204,14 @@ int ref_hybrid_gmres(void *system, const complex double *b, complex double *x, s
   dielectric_fft_get_operator(system, &op);
   return vie_gmres(&op, b, x, &o, report);
 }
+
+/* vie_gmres (vie_iterative.c:80-199) on caller callbacks: a NULL
+   preconditioner is the identity, as in vie_iterative.h. */
+int ref_callback_gmres(size_t n, vie_vector_map apply, void *apply_context, vie_vector_map precondition,
+                       void *precondition_context, const complex double *b, complex double *x, size_t restart,
+                       size_t maxit, double rtol, double atol, vie_gmres_report *report)
+{
+  vie_linear_operator op = {n, apply, apply_context, precondition, precondition_context};
+  vie_gmres_options o = {restart, maxit, rtol, atol};
+  return vie_gmres(&op, b, x, &o, report);
+}

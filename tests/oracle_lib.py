@@ -116,6 +116,7 @@ def reference():
             getattr(r, f).restype = i
         r.ref_hybrid_gmres.argtypes = [vp, vp, vp, sz, sz, dbl, dbl, C.POINTER(Report)]
         r.ref_hybrid_gmres.restype = i
+        r.ref_callback_gmres.restype = i
         _ref = r
     return _ref
 

@@ -374,3 +374,59 @@ def test_hybrid_against_dense_reference_kernel(near_tables, gap, pec):
     assert np.max(np.abs(y - expected)) < 2e-7
     ok, sol, rep = oh.gmres(y)
     assert ok and np.max(np.abs(sol - x)) < 1e-10
+
+
+def _ref_gmres(n, apply, prec, b, x, restart=30, maxit=300, rtol=1e-12, atol=0.0):
+    r = oracle_lib.reference()
+    r.ref_callback_gmres.argtypes = [C.c_size_t, MAP, C.c_void_p, MAP, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_size_t, C.c_size_t, C.c_double, C.c_double, C.POINTER(Report)]
+    rep = Report()
+    ok = r.ref_callback_gmres(n, apply, None, prec if prec else MAP(), None, ptr(b), ptr(x), restart, maxit,
+                              rtol, atol, C.byref(rep))
+    return ok, rep
+
+
+@needs_ref
+def test_gmres_statuses_match_reference():
+    """vie_iterative_test.c's operators (matrix-free stencil, identity, zero,
+    failing and non-finite callbacks) and invalid inputs, run by the oracle
+    and by the reference's vie_gmres on the same callbacks: same return
+    value, the same report field by field, and the same x, bit for bit."""
+    n = 40
+    i = np.arange(n)
+    b40 = np.zeros(n, dtype=np.complex128)
+    stencil(np.sin(i) + 1j * np.cos(0.4 * i), b40)
+    b3 = np.array([1 + 1j, 2 - 1j, -3 + 2j])
+
+    def nan_map(x, y):
+        y[:] = x
+        y[0] = np.nan
+        return 1
+    ident = _wrap(lambda x, y: (y.__setitem__(slice(None), x), 1)[1], 3)
+    runs = [
+        (40, _wrap(stencil, 40), None, b40, {"restart": 3}),
+        (40, _wrap(stencil, 40), None, b40, {"restart": 3, "maxit": 1}),
+        (40, _wrap(stencil, 40), None, b40, {"restart": 40, "rtol": 1e-6}),
+        (40, _wrap(stencil, 40), None, b40, {"restart": 5, "rtol": 0.0, "atol": 1e-9}),
+        (3, ident, None, b3, {}),
+        (3, _wrap(lambda x, y: (y.__setitem__(slice(None), 0), 1)[1], 3), None,
+         np.array([1, 0, 0], dtype=np.complex128), {}),
+        (3, _wrap(lambda x, y: 0, 3), None, b3, {}),
+        (3, ident, _wrap(lambda x, y: 0, 3), b3, {}),
+        (3, _wrap(nan_map, 3), None, b3, {}),
+        (3, ident, None, b3, {"restart": 0}),
+        (3, ident, None, b3, {"maxit": 0}),
+        (3, ident, None, b3, {"rtol": 0.0, "atol": 0.0}),
+        (3, ident, None, b3, {"rtol": -1.0}),
+        (3, ident, None, np.zeros(3, dtype=np.complex128), {}),
+    ]
+    for n, apply, prec, b, kw in runs:
+        x1 = np.zeros(n, dtype=np.complex128)
+        x2 = np.zeros(n, dtype=np.complex128)
+        ok1, rep1 = _gmres(n, apply, prec, b, x1, **kw)
+        ok2, rep2 = _ref_gmres(n, apply, prec, b, x2, **kw)
+        assert ok1 == ok2, kw
+        d1, d2 = rep1.as_dict(), rep2.as_dict()
+        for f in d1:
+            assert d1[f] == d2[f] or (np.isnan(d1[f]) and np.isnan(d2[f])), (kw, f, d1, d2)
+        assert np.array_equal(x1, x2, equal_nan=True), kw
