@@ -1,7 +1,8 @@
 /* Device layer of the nec2c CUDA backend: C-linkage entry points implemented
- * in CUDA C++ (csrc/*.cu) and called by the C host layer (host/*.c).  Not part
- * of the public ABI (that is include/nec2c_cuda.h).  All pointers named *_dev
- * are device pointers; everything else is host memory. */
+ * in CUDA C++ (the .cu files of csrc/) and called by the C host layer (the .c
+ * files of host/).  Not part of the public ABI (that is include/nec2c_cuda.h).
+ * All pointers named *_dev are device pointers; everything else is host
+ * memory. */
 #ifndef NEC2C_DEVICE_API_H
 #define NEC2C_DEVICE_API_H
 #include <stddef.h>

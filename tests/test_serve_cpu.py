@@ -1,0 +1,213 @@
+"""Host logic of the request server (nec2c_b200/host/serve.c) on the CPU.
+
+The server's own source is compiled with a fake device layer
+(tests/serve_fake.c): each fake solve holds the volume plans its request runs
+on for a few milliseconds and counts every overlap on one plan.  Checked here:
+exclusivity per plan (directly, through hybrid systems and in batches) while
+independent requests overlap, admission by device footprint, a request larger
+than the budget running alone after being passed at most `slots` times, the
+default budget (the reserve rule of concurrency.c:131-136) and the submission
+checks."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import nec2c_b200 as nb
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GIB = 1 << 30
+
+
+@pytest.fixture(scope="module")
+def fake():
+    build = os.path.join(ROOT, "tests", "_build")
+    os.makedirs(build, exist_ok=True)
+    out = os.path.join(build, "libserve_fake.so")
+    subprocess.run(["gcc", "-O1", "-std=gnu11", "-fPIC", "-shared", "-pthread", "-o", out,
+                    os.path.join(ROOT, "nec2c_b200", "host", "serve.c"),
+                    os.path.join(ROOT, "tests", "serve_fake.c")], check=True)
+    lib = C.CDLL(out)
+    vp, sz = C.c_void_p, C.c_size_t
+    lib.fake_reset.argtypes = [C.c_long, sz]
+    lib.fake_plan.argtypes = [sz]
+    lib.fake_plan.restype = vp
+    lib.fake_hybrid.argtypes = [vp, sz]
+    lib.fake_hybrid.restype = vp
+    lib.fake_batch.argtypes = [vp, sz]
+    lib.fake_batch.restype = vp
+    lib.fake_release.argtypes = [vp]
+    lib.nec2c_cuda_server_create.argtypes = [C.POINTER(vp), C.c_int, C.c_int, sz, C.c_int]
+    lib.nec2c_cuda_server_submit.argtypes = [vp, C.POINTER(nb.Request)]
+    lib.nec2c_cuda_server_wait.argtypes = [vp, C.POINTER(nb.Request)]
+    lib.nec2c_cuda_server_drain.argtypes = [vp]
+    lib.nec2c_cuda_server_budget.argtypes = [vp]
+    lib.nec2c_cuda_server_budget.restype = sz
+    lib.nec2c_cuda_server_destroy.argtypes = [vp]
+    lib.nec2c_cuda_last_error.restype = C.c_char_p
+    return lib
+
+
+class Server:
+    def __init__(self, lib, slots, budget=0):
+        self.lib, self.h, self.keep = lib, C.c_void_p(), []
+        assert lib.nec2c_cuda_server_create(C.byref(self.h), 0, slots, budget, 0)
+
+    def submit(self, r, *arrays):
+        self.keep.append((r, arrays))
+        ok = self.lib.nec2c_cuda_server_submit(self.h, C.byref(r))
+        if not ok:
+            self.keep.pop()
+        return ok
+
+    def dense(self, n):
+        r = nb.Request()
+        r.kind = nb.REQUEST_DENSE
+        r.order = r.ld = r.rhs_stride = n
+        r.rhs_count = 1
+        m = np.zeros(1, dtype=np.complex128)
+        rhs = np.zeros(n, dtype=np.complex128)
+        r.matrix, r.rhs = m.ctypes.data, rhs.ctypes.data
+        assert self.submit(r, m, rhs)
+        return r, rhs
+
+    def volume(self, plan=None, system=None, n=0):
+        r = nb.Request()
+        r.kind = nb.REQUEST_VOLUME
+        r.plan, r.system = plan, system
+        b = np.arange(1, n + 1) * (1 + 1j)
+        x = np.zeros(n, dtype=np.complex128)
+        r.b, r.x = b.ctypes.data, x.ctypes.data
+        r.options = nb.GmresOptions(30, 300, 1e-12, 0.0)
+        assert self.submit(r, b, x)
+        return r, (b, x)
+
+    def batch(self, batch, k, n):
+        r = nb.Request()
+        r.kind = nb.REQUEST_BATCH
+        r.batch = batch
+        b = np.arange(1, n + 1) * (2 - 1j)
+        x = np.zeros(n, dtype=np.complex128)
+        reps = (nb.GmresReport * k)()
+        r.b, r.x = b.ctypes.data, x.ctypes.data
+        r.reports = C.cast(reps, C.c_void_p)
+        r.options = nb.GmresOptions(30, 300, 1e-12, 0.0)
+        assert self.submit(r, b, x, reps)
+        return r, (b, x, reps)
+
+    def drain(self):
+        self.lib.nec2c_cuda_server_drain(self.h)
+
+    def close(self):
+        self.lib.nec2c_cuda_server_destroy(self.h)
+
+
+def overlap(a, b):
+    return a.started_s < b.finished_s and b.started_s < a.finished_s
+
+
+def test_exclusive_per_plan_through_systems_and_batches(fake):
+    fake.fake_reset(3000, 10 * GIB)
+    orders = (30, 60, 90)
+    p1, p2, p3 = plans = [fake.fake_plan(n) for n in orders]
+    hyb = fake.fake_hybrid(p3, 5)
+    b12 = fake.fake_batch((C.c_void_p * 2)(p1, p2), 2)
+    b13 = fake.fake_batch((C.c_void_p * 2)(p1, p3), 2)
+    srv = Server(fake, slots=4)
+    reqs = []
+    for _ in range(3):
+        reqs.append((srv.volume(plan=p1, n=30), {p1}))
+        reqs.append((srv.batch(b12, 2, 90), {p1, p2}))
+        reqs.append((srv.volume(plan=p2, n=60), {p2}))
+        reqs.append((srv.volume(system=hyb, n=95), {p3}))
+        reqs.append((srv.batch(b13, 2, 120), {p1, p3}))
+        reqs.append((srv.volume(plan=p3, n=90), {p3}))
+        reqs.append((srv.dense(64), set()))
+    srv.drain()
+    assert fake.fake_violations() == 0
+    assert fake.fake_peak() >= 2                       # independent requests overlapped
+    for (r, data), _ in reqs:
+        assert r.done and r.status, r.error
+        if r.kind == nb.REQUEST_DENSE:
+            assert data[0] == 64
+        else:
+            assert r.report.status == 0
+            assert np.array_equal(data[1], data[0])     # x received b
+        if r.kind == nb.REQUEST_BATCH:
+            assert [rep.iterations for rep in data[2]] == [1, 2]
+            assert r.report.iterations == 2 and r.report.operator_applications == 2 + 3
+    shared = 0
+    for i, ((a, _), ua) in enumerate(reqs):
+        for (b, _), ub in reqs[i + 1:]:
+            if ua & ub:
+                shared += 1
+                assert not overlap(a, b)
+    assert shared > 20
+    srv.close()
+    for o in (b12, b13, hyb, *plans):
+        fake.fake_release(o)
+
+
+def footprint(n):
+    return n * n * 16 + n * 16 + n * 4 + 4096
+
+
+def test_admission_by_footprint(fake):
+    fake.fake_reset(3000, 10 * GIB)
+    n = 256
+    budget = 2 * footprint(n) + footprint(n) // 2           # room for two at a time
+    srv = Server(fake, slots=4, budget=budget)
+    reqs = [srv.dense(n)[0] for _ in range(8)]
+    srv.drain()
+    assert all(r.status and r.footprint == footprint(n) for r in reqs)
+    assert fake.fake_peak() == 2
+    events = sorted([(r.started_s, r.footprint) for r in reqs] + [(r.finished_s, -r.footprint) for r in reqs],
+                    key=lambda e: (e[0], e[1]))
+    cur = peak = 0
+    for _, d in events:
+        cur += d
+        peak = max(peak, cur)
+    assert peak <= budget
+    srv.close()
+
+
+def test_oversized_request_runs_alone_after_at_most_slots_passes(fake):
+    fake.fake_reset(5000, 10 * GIB)
+    slots = 2
+    budget = 4 * footprint(100)
+    srv = Server(fake, slots=slots, budget=budget)
+    first = srv.dense(100)[0]
+    big = srv.dense(1000)[0]                                # 16 MB: above the budget
+    rest = [srv.dense(100)[0] for _ in range(10)]
+    srv.drain()
+    assert big.status and big.footprint > budget
+    assert big.skipped <= slots
+    for r in [first] + rest:
+        assert r.status and not overlap(r, big)
+    assert sum(1 for r in rest if r.started_s < big.started_s) <= slots
+    srv.close()
+
+
+def test_default_budget_keeps_the_reserve(fake):
+    for free, expect in ((10 * GIB, 8 * GIB), (2 * GIB, 1 * GIB)):
+        fake.fake_reset(0, free)
+        srv = Server(fake, slots=1)
+        assert fake.nec2c_cuda_server_budget(srv.h) == expect
+        srv.close()
+
+
+def test_submission_checks(fake):
+    fake.fake_reset(0, 10 * GIB)
+    srv = Server(fake, slots=1)
+    for kind, why in ((99, b"unknown request kind 99"), (nb.REQUEST_VOLUME, b"exactly one of plan"),
+                      (nb.REQUEST_BATCH, b"batch request needs"), (nb.REQUEST_DENSE, b"dense request needs")):
+        r = nb.Request()
+        r.kind = kind
+        assert not srv.submit(r)
+        assert why in fake.nec2c_cuda_last_error()
+    bad = C.c_void_p()
+    assert not fake.nec2c_cuda_server_create(C.byref(bad), 0, 0, 0, 0)
+    assert b"slots must be" in fake.nec2c_cuda_last_error()
+    srv.close()
