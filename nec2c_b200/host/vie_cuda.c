@@ -98,13 +98,19 @@ void nec2c_cuda_vie_fft_destroy(nec2c_cuda_vie_plan *p)
   free(p);
 }
 
+/* vie_fft_create starts its byte count at sizeof(struct vie_fft_plan)
+   (vie_fft.c:19-28, :381): seven size_t, an int, five pointers and three
+   complex doubles, 160 bytes on LP64 in a build without FFTW (whose three
+   plan handles and flag add 32). */
+enum { REF_PLAN_STRUCT_BYTES = 160 };
+
 int nec2c_cuda_vie_fft_create(nec2c_cuda_vie_plan **out, const size_t shape[3], size_t cells,
                               const size_t *xyz, double h, double k, double er_re, double er_im,
                               size_t limit, nec2c_cuda_near_tensor_fn near, void *near_ctx)
 {
   struct nec2c_cuda_vie_plan *p = NULL;
   double complex er = er_re + I * er_im;
-  size_t padded[3], g = 1, bytes = 256, tmp, root_bytes = 0;
+  size_t padded[3], g = 1, bytes = REF_PLAN_STRUCT_BYTES, tmp, root_bytes = 0;
   int *cell_box = NULL, *offsets = NULL, *far_ok = NULL;
   unsigned char *seen = NULL;
   double *tw[3] = {NULL, NULL, NULL}, *near_t = NULL;
