@@ -20,10 +20,10 @@ static int g_dense_mixed = 0;
 
 int nec2c_cuda_dense_backend_set(const char *name)
 {
-  if(!name) return 0;
+  if(!name) { n2c_set_error("dense backend: null name"); return 0; }
   if(!strcmp(name, "cuda")) g_dense_mixed = 0;
   else if(!strcmp(name, "cuda-mixed")) g_dense_mixed = 1;
-  else return 0;
+  else { n2c_set_error("unknown dense backend '%s' (cuda, cuda-mixed)", name); return 0; }
   return 1;
 }
 const char *nec2c_cuda_dense_backend_name(void) { return g_dense_mixed ? "cuda-mixed" : "cuda"; }
@@ -170,7 +170,11 @@ int nec2c_cuda_dense_factor_classic(size_t n, nec2c_cuda_complex *matrix, size_t
   int info = 0, ok;
   double *a;
   int *piv;
-  if(!matrix || !pivots || n == 0 || n > INT_MAX || ld < n || ld > INT_MAX) return 0;
+  /* dense_backend.c:71-81: the LAPACK branch's dimension checks. */
+  if(!matrix || !pivots || n == 0 || n > INT_MAX || ld < n || ld > INT_MAX) {
+    n2c_set_error("factor: null matrix or pivots, order 0, or leading dimension below the order");
+    return 0;
+  }
   if(!n2d_device_ok()) return 0;
   nec2c_cuda_dense_release();
   a = upload_matrix(matrix, n, ld);
@@ -209,7 +213,10 @@ int nec2c_cuda_dense_solve_classic_many(size_t n, const nec2c_cuda_complex *matr
   int *piv = NULL, own = 0, ok;
   if(count == 0) return 1;
   if(!matrix || !pivots || !rhs || n == 0 || n > INT_MAX || ld < n || ld > INT_MAX || stride < n ||
-     count > INT_MAX) return 0;
+     count > INT_MAX) {
+    n2c_set_error("solve: null matrix, pivots or rhs, order 0, or a leading dimension or stride below the order");
+    return 0;
+  }
   if(!n2d_device_ok()) return 0;
   const int cached = g_cache.piv_dev && g_cache.host == (const void *)matrix && g_cache.order == n && g_cache.ld == ld;
   b = n2d_alloc(n * count * CPX);
@@ -249,7 +256,7 @@ int nec2c_cuda_dense_solve_row_major(nec2c_cuda_complex *matrix, nec2c_cuda_comp
 {
   double *a, *b = NULL;
   int *piv = NULL, info = 0, ok;
-  if(!matrix || !rhs || n == 0 || n > INT_MAX) return 0;
+  if(!matrix || !rhs || n == 0 || n > INT_MAX) { n2c_set_error("row-major solve: null matrix or rhs, or order 0"); return 0; }
   if(!n2d_device_ok()) return 0;
   /* The row-major system is the classic storage with leading dimension n. */
   a = upload_matrix(matrix, n, n);

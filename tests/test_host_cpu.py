@@ -79,3 +79,25 @@ def test_invalid_arguments_refused_like_reference(case):
     assert reference_bytes(shape, xyz, h, k, eps) is None
     err = ours(shape, xyz, h, k, eps, 1 << 40)
     assert "invalid" in err, err
+
+
+def test_dense_entry_points_check_arguments_first():
+    """dense_backend.c's LAPACK-branch conventions, decided before any device
+    call: no right-hand sides is success, order 0 or a short leading
+    dimension is a failure with the reason set."""
+    lib = nb.load()
+    a = np.zeros((4, 4), dtype=np.complex128)
+    piv = np.zeros(4, dtype=np.int32)
+    rhs = np.zeros(4, dtype=np.complex128)
+    p = lambda arr: arr.ctypes.data
+    assert lib.nec2c_cuda_dense_solve_classic_many(4, p(a), 4, p(piv), p(rhs), 4, 0) == 1
+    assert not lib.nec2c_cuda_dense_factor_classic(0, p(a), 4, p(piv))
+    assert "order 0" in nb.last_error()
+    assert not lib.nec2c_cuda_dense_factor_classic(4, p(a), 3, p(piv))
+    assert "leading dimension" in nb.last_error()
+    assert not lib.nec2c_cuda_dense_solve_classic_many(4, p(a), 4, p(piv), p(rhs), 3, 1)
+    assert "stride" in nb.last_error()
+    assert not lib.nec2c_cuda_dense_solve_row_major(None, p(rhs), 4)
+    assert "row-major" in nb.last_error()
+    assert not lib.nec2c_cuda_dense_backend_set(b"lapack")
+    assert "unknown dense backend" in nb.last_error()
