@@ -7,10 +7,13 @@
  *
  * Parity is pinned two ways (see tests/test_oracle.py):
  *   - against the reference itself, compiled from its own sources into
- *     oracle/_ref/ by oracle/Makefile (identical operator, GMRES and LU
- *     results on the same inputs);
+ *     oracle/_ref/ by oracle/Makefile (identical volume and hybrid operator,
+ *     preconditioner, GMRES iterates and statuses, LU factors and far-field
+ *     amplitudes on the same inputs);
  *   - against the reference's own known-answer data (tests/dense_backend_test.c
- *     3x3 system, tests/m9-fft-skeleton-1e-8.txt integrated currents).
+ *     3x3 system, the dense-operator checks of tests/vie_fft_test.c and
+ *     tests/dielectric_fft_test.c, tests/m9-fft-skeleton-1e-8.txt integrated
+ *     currents).
  */
 #ifndef NEC2C_ORACLE_H
 #define NEC2C_ORACLE_H
