@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the nec2c CUDA backend on one B200 (replicas on N GPUs).
 
-Workload (BASELINE config 2): a 64x64x64-voxel block of side 1 lambda at
+Workload: a 64x64x64-voxel block of side 1 lambda at
 300 MHz (786,432 complex unknowns, 128^3 padded FFT grid), per-voxel
 eps_r ~ U[2,10] and loss tangent ~ U[0.01,0.1] (seeded), x-polarised plane
 wave excitation, GMRES(30) to rtol 1e-6 (iteration limit 10000, the CLI's
@@ -55,9 +55,9 @@ def parse():
                          "tune on serialised, slowed launches)")
     ap.add_argument("--only", choices=["matvec", "solve", "lu", "serving", "volume_batch"],
                     help="profiling driver: build the plans, run --steps FP32 and FP64 products "
-                         "(matvec) or --steps mixed solves (solve), or factor the config-1 shaped "
+                         "(matvec) or --steps mixed solves (solve), or factor the 1984-unknown dense "
                          "matrix --steps times in each LU form (lu), run the serving stream "
-                         "(serving) or the config-3 shaped volume batch (volume_batch); print "
+                         "(serving) or the 192-system dipole-plus-cube batch (volume_batch); print "
                          "timings and exit")
     return ap.parse_args()
 
@@ -488,13 +488,13 @@ def run_ours(args, rank, world, local_rank):
     peak, peak_kind = peaks()
     achieved = bytes32 / (mv32_ms * 1e-3) / 1e9
 
-    # Config-1 shaped dense LU (1984 unknowns), both forms.
+    # Dense LU of 1984 unknowns, both forms.
     dense = dense_bench(nb, torch, stream)
-    # Config-3 shaped wire blocks, ragged batch in one launch.
+    # 192 small wire blocks, ragged batch in one launch.
     batched = batched_bench(nb, torch)
-    # Config-3 shaped volume sweep, ragged batch of plans.
+    # 192-system dipole-plus-cube sweep, ragged batch of plans.
     volume_batch = volume_batch_bench(nb, torch, stream)
-    # Config-4 shaped serving stream (bounded), both forms.
+    # Mixed dense and volume serving stream (bounded), both forms.
     serving = serving_bench(nb, torch) if world == 1 else None
     lib.nec2c_cuda_set_stream(C.c_void_p(stream.cuda_stream))
 
@@ -642,7 +642,7 @@ def lu_driver(args, nb, torch, stream):
 
 
 def dense_bench(nb, torch, stream):
-    """Config-1 shaped dense solve (1984 unknowns, one right-hand side) in the
+    """Dense solve of 1984 unknowns (one right-hand side) in the
     FP64 form and the split-precision form (FP32 tensor-core factors + FP64
     refinement), through the classic C ABI with host buffers, plus the device
     factor alone on resident matrices."""
@@ -685,7 +685,7 @@ def dense_bench(nb, torch, stream):
 
 
 def batched_bench(nb, torch):
-    """Config-3 shaped wire blocks: 128 frequencies of the 21-segment dipole
+    """Small wire blocks: 128 frequencies of the 21-segment dipole
     plus 64 dipoles of 11-41 segments (seeded), each block factored and solved:
     the ragged batch in one call against one classic factor + solve per block."""
     rng = np.random.default_rng(6)
@@ -729,9 +729,9 @@ def batched_bench(nb, torch):
 
 
 def volume_batch_bench(nb, torch, stream):
-    """Config-3 shaped sweep in one batch of dipole-plus-cube systems.
+    """A frequency and geometry sweep in one batch of dipole-plus-cube systems.
 
-    The batch holds 192 systems.  The first 128 are the config-0 model at 128
+    The batch holds 192 systems.  The first 128 are one model at 128
     frequencies uniform in 100-400 MHz: a cube of 16^3 cells, 0.2 lambda at
     300 MHz, eps_r = 4 - 0.1j, beside a 21-segment dipole.  The other 64 are
     seeded cubes of 8^3-32^3 cells (0.2 lambda at 300 MHz, eps_r ~ U[2,8],
@@ -906,7 +906,7 @@ def volume_batch_bench(nb, torch, stream):
     return out
 
 
-# Config-4 shaped serving stream (bounded): 60% wire-only dense MoM solves of
+# Serving stream (bounded): 60% wire-only dense MoM solves of
 # 200-3000 unknowns (log-uniform), 40% volume solves on resident plans of two
 # lattices (0.2-lambda cubes voxelised 16^3 and 32^3 at 300 MHz, eps_r~U[2,10],
 # tand 0.05) with GMRES(30) to rtol 1e-6, two resident replicas per lattice.

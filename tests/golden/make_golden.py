@@ -44,11 +44,11 @@ def cases():
         "rand_k0.3": dict(h=0.25, k=0.3, shape=(24, 24, 24)),
         # M9 benchmark models (tools/m9_fft_benchmark.c: pitch 0.25 m, 28 MHz)
         "m9_tree": dict(h=0.25, k=k28, shape=(24, 24, 48)),
-        # BASELINE config 0: 16^3 cube of side 0.2 lambda at 300 MHz
+        # 16^3 cube of side 0.2 lambda at 300 MHz
         "c0": dict(h=0.2 * lam / 16, k=k300, shape=(16, 16, 16)),
-        # BASELINE config 2: 64^3 block of side 1 lambda at 300 MHz
+        # 64^3 block of side 1 lambda at 300 MHz
         "c2": dict(h=lam / 64, k=k300, shape=(64, 64, 64)),
-        # BASELINE config 3/4 cube sizes at their largest pitch in lambda
+        # 32^3 cube of side 0.2 lambda at 300 MHz (the finest pitch of the swept cubes)
         "c3_32": dict(h=0.2 * lam / 32, k=k300, shape=(32, 32, 32)),
     }
 

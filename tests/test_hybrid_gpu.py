@@ -110,7 +110,7 @@ def test_zero_conductor_diagonal_fails_preconditioner():
 
 
 def test_dipole_plus_cube_random_blocks(near_tables):
-    """A config-0-shaped system (16^3 cube plus 21 wire unknowns) with seeded
+    """A 16^3 cube beside 21 wire unknowns, with seeded
     synthetic conductor blocks, against the oracle at rtol 1e-12."""
     h, k, table = near_tables["c0"]
     shape = (16, 16, 16)
