@@ -279,14 +279,17 @@ int nec2c_cuda_dense_last_refinement(void);
    belongs to its own pool allocator, or a loop that cannot absorb cudaMalloc's
    device synchronisation).  matrix_dev and pivots_dev are device pointers the
    caller owns: NEC's storage (the algebraic matrix row-major, leading
-   dimension >= order) factored in place with the same pivots and factors as
-   nec2c_cuda_dense_factor_classic, and 1-based pivots written to pivots_dev.
-   The work runs on this thread's stream and the call returns when it is done.
-   Scratch is one 20 KiB array inside the library that each GPU using it holds
-   until exit; calls that overlap on the GPU share it and race.  The first
-   call on a device looks up that array's address, so make it before any
-   stream capture.  Orders above NEC2C_CUDA_STATIC_LU_MAX_ORDER are rejected.
-   Returns 1, or 0 when singular, too large or failed. */
+   dimension >= order) factored in place, and 1-based pivots written to
+   pivots_dev.  It is always the plain FP64 factor: the same pivots and
+   factors as nec2c_cuda_dense_factor_classic under the "cuda" backend,
+   whichever backend name is selected.  The work runs on this thread's stream
+   and the call returns when it is done.  Scratch is one 19 KiB array inside
+   the library that each GPU using it holds until exit; calls that overlap on
+   the GPU share it and race.  Each call looks up that array's address in the
+   current context; the first lookup loads the library's device code, so make
+   the first call on a device before any stream capture.  Orders above
+   NEC2C_CUDA_STATIC_LU_MAX_ORDER are rejected.  Returns 1, or 0 when
+   singular, too large or failed. */
 #define NEC2C_CUDA_STATIC_LU_MAX_ORDER 4096
 int nec2c_cuda_dense_factor_device_static(size_t order, nec2c_cuda_complex *matrix_dev,
                                           size_t leading_dimension, int *pivots_dev);

@@ -18,7 +18,6 @@ OBJ = os.path.join(HERE, "lib", "obj")
 LIB = os.path.join(HERE, "lib", "libnec2c_cuda.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUTLASS = "/opt/prime-rl/.venv/lib/python3.12/site-packages/flashinfer/data/cutlass/include"
 
 
 def _headers():
@@ -50,8 +49,6 @@ def build(verbose=False):
             src, obj = os.path.join(CSRC, f), os.path.join(OBJ, f[:-3] + ".o")
             cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                                    "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
-            if os.path.isdir(CUTLASS):
-                cmd += ["-I" + CUTLASS]
             cmd += ["-c", src, "-o", obj]
             jobs.append((src, obj, cmd))
     for f in sorted(os.listdir(HOST)):

@@ -24,6 +24,7 @@
 #include <float.h>
 #include <limits.h>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 #include "common.cuh"
 #include "device_api.h"
@@ -1153,8 +1154,12 @@ static cudaError_t launch_cluster_panel(const PanelArgs &p, cudaStream_t s) {
 }
 
 // 1 when 16-CTA clusters of the panel kernel can be resident.
+// NEC2C_CUDA_LU_CLUSTER8=1 in the environment (a test switch) limits the
+// panel to 8-CTA clusters, so orders above 2048 take the grid panel.
 static int cluster16_probe() {
   int state = 0;
+  const char *cap = getenv("NEC2C_CUDA_LU_CLUSTER8");
+  if (cap && cap[0] == '1') return 0;
   void (*kernels[4])(PanelArgs) = {panel_cluster_kernel<CMAX, 0, double2>, panel_cluster_kernel<CMAX, 1, double2>,
                                    panel_cluster_kernel<CMAX, 0, float2>, panel_cluster_kernel<CMAX, 1, float2>};
   for (auto k : kernels) {
@@ -1491,18 +1496,22 @@ extern "C" int n2d_lu_solve32(const float *a_dev, long long n, long long ld, con
 // one array defined in this file instead of being allocated per call.
 //
 // That array is a module global: every GPU on which the library is loaded
-// holds it (about 20 KiB) until the process exits, and every call on that
+// holds it (19 KiB) until the process exits, and every call on that
 // GPU shares it.  Calls whose work overlaps on the GPU (two streams, two host
 // threads) therefore race on it; callers serialise them.  The array keeps the
 // previous call's contents; only the panel status needs to start at zero and
 // is cleared at the start of every call.
 //
-// Set-up: the first call on a device, with that device current, looks up the
-// array's device address (cudaGetSymbolAddress; the array's name in host code
-// is only a stand-in) and keeps it.  Make that first call before any stream
-// capture on the device.
+// Set-up: every call looks up the array's device address on the current
+// device (cudaGetSymbolAddress; the array's name in host code is only a
+// stand-in).  The lookup allocates nothing, and repeating it keeps the address
+// right when the module is loaded again (after cudaDeviceReset, or in another
+// context on the same device).  The first lookup in a context loads the
+// module, so make the first call on a device before any stream capture.
+//
+// The factor is always the plain FP64 form (factr's pivot rule), whichever
+// dense backend name is selected.
 #include <climits>
-#include <mutex>
 #include "../../include/nec2c_cuda.h"
 
 namespace {
@@ -1517,31 +1526,23 @@ constexpr size_t STATIC_SCRATCH_BYTES = STATIC_GROW_OFF + (size_t)2 * STATIC_GRI
 static_assert(sizeof(LuStatus) <= STATIC_PAIRS_OFF - STATIC_STATUS_OFF, "status slot");
 static_assert(4 * KB * sizeof(int) <= STATIC_GVAL_OFF - STATIC_PAIRS_OFF, "pairs slot");
 static_assert(STATIC_GIDX_OFF + 2 * STATIC_GRID * sizeof(int) <= STATIC_GROWJ_OFF, "grid candidates slot");
-constexpr int STATIC_MAX_DEVICES = 64;
-std::mutex g_static_lock;
-unsigned char *g_static_addr[STATIC_MAX_DEVICES];
+// The documented size (header, integration notes): 19 KiB.
+static_assert(STATIC_SCRATCH_BYTES == 19 * 1024, "scratch array size changed: update its documentation");
 }  // namespace
 
 static __device__ __align__(256) unsigned char lu_static_scratch[STATIC_SCRATCH_BYTES];
 
-// Device address of the scratch array on the current device (looked up once
-// per device).
+// Device address of the scratch array in the current context.
 static unsigned char *static_scratch() {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) { n2c_set_error("cudaGetDevice: %s", cudaGetErrorString(e)); return nullptr; }
-  if (dev < 0 || dev >= STATIC_MAX_DEVICES) { n2c_set_error("device %d out of range", dev); return nullptr; }
-  std::lock_guard<std::mutex> hold(g_static_lock);
-  if (!g_static_addr[dev]) {
-    void *ptr = nullptr;
-    e = cudaGetSymbolAddress(&ptr, lu_static_scratch);
-    if (e != cudaSuccess || !ptr) {
-      n2c_set_error("scratch address on device %d: %s", dev, cudaGetErrorString(e));
-      return nullptr;
-    }
-    g_static_addr[dev] = (unsigned char *)ptr;
+  void *ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, lu_static_scratch);
+  if (e != cudaSuccess || !ptr) {
+    int dev = -1;
+    cudaGetDevice(&dev);
+    n2c_set_error("scratch address on device %d: %s", dev, cudaGetErrorString(e));
+    return nullptr;
   }
-  return g_static_addr[dev];
+  return (unsigned char *)ptr;
 }
 
 extern "C" int nec2c_cuda_dense_factor_device_static(size_t order, nec2c_cuda_complex *matrix_dev,

@@ -24,7 +24,8 @@ import numpy as np  # noqa: E402
 
 import oracle_lib  # noqa: E402
 
-REFERENCE = "/root/reference"
+# Reference tree whose published results are read; NEC2C_REFERENCE overrides it.
+REFERENCE = os.environ.get("NEC2C_REFERENCE", "/root/reference")
 C0 = 299792458.0
 
 

@@ -8,11 +8,15 @@ variant; it must give the same pivots and factors as the classic factor
 library's scratch array.  Named to run last, after every other test has used
 the library; it also passes alone in a fresh process."""
 import ctypes as C
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
 
-import nec2c_b200 as nb
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+import nec2c_b200 as nb  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -45,11 +49,13 @@ def _factor_static(st):
     return bool(ok), dev.cpu().numpy().T, piv.cpu().numpy()
 
 
-def test_static_factor_matches_classic():
+def _compare(cases):
+    """Static factor against the classic factor ("cuda" backend) on each
+    (order, leading dimension, seed), one call after another."""
     lib = nb.load()
     assert nb.dense_backend_set("cuda")
     lib.nec2c_cuda_set_stream(None)
-    for n, ld, seed in [(700, 703, 7), (2500, 2500, 25)]:
+    for n, ld, seed in cases:
         a = _system(n, seed)
         st = _nec_storage(a, ld)
         ok_s, lu_s, piv_s = _factor_static(st)
@@ -67,9 +73,29 @@ def test_static_factor_matches_classic():
         assert np.array_equal(lu_s[n:, :], st[n:, :])
 
 
+def test_static_factor_matches_classic():
+    _compare([(700, 703, 7), (2500, 2500, 25)])
+
+
+def test_static_factor_grid_panel():
+    """With the panel held to 8-CTA clusters (NEC2C_CUDA_LU_CLUSTER8=1, read
+    once per process, hence the child process), order 2500 takes the grid
+    panel, whose candidate slots also live in the static array."""
+    env = dict(os.environ, NEC2C_CUDA_LU_CLUSTER8="1")
+    r = subprocess.run([sys.executable, os.path.abspath(__file__)], env=env, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "grid panel ok" in r.stdout
+
+
 def test_static_factor_rejects_large_order():
     lib = nb.load()
     n = 4097
     # Rejected on the size alone, before any device pointer is used.
     assert not lib.nec2c_cuda_dense_factor_device_static(n, C.c_void_p(16), n, C.c_void_p(16))
     assert b"maximum" in lib.nec2c_cuda_last_error()
+
+
+if __name__ == "__main__":
+    _compare([(2500, 2500, 25), (2100, 2101, 21)])
+    print("grid panel ok")
