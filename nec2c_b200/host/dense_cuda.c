@@ -1,10 +1,9 @@
 /* Host side of the CUDA dense backend: dense_backend.c's classic factor/solve
- * and row-major solve entry points (C, like the reference).  The factor keeps
- * its device copy (and, for the mixed form, the original matrix) so the
- * solves that follow on the same thread do not re-upload it.  The cache is
- * per thread: the reference keeps one factorisation per process
- * (dense_backend.c:15), and threads that each own a stream (the request
- * server) keep one each. */
+ * and row-major solve entry points (C, like the reference).  Each factor
+ * keeps its device copy (and, for the mixed form, the original matrix) so the
+ * solves that follow on the same thread do not re-upload it.  The entries are
+ * per thread, since threads that each own a stream (the request server) work
+ * independently. */
 #include <complex.h>
 #include <float.h>
 #include <limits.h>
@@ -28,9 +27,18 @@ int nec2c_cuda_dense_backend_set(const char *name)
 }
 const char *nec2c_cuda_dense_backend_name(void) { return g_dense_mixed ? "cuda-mixed" : "cuda"; }
 
-/* The most recent classic factorisation of this thread, kept on the device. */
-static _Thread_local struct {
-  const void *host;      /* host matrix the factors were written to */
+/* Classic factorisations of this thread kept on the device: one entry per
+   host storage the factors were written to, so that the solves that follow
+   find them whatever the order of calls (netwk factors its network matrix
+   between the main matrix's factor and solves, network.c:505-560; factrs
+   factors every symmetry block before solves uses them, matrix.c:1424-1435
+   and 1683-1701).  An entry is recognised by the storage address, order and
+   leading dimension, and checked against the pivots and the diagonal of the
+   factors written back; a factorisation written over an entry's storage
+   replaces it. */
+typedef struct dense_entry {
+  struct dense_entry *next;
+  const void *host;      /* host storage the factors were written to */
   size_t order, ld;
   double *lu_dev;        /* FP64 form: row-major LU, leading dim order */
   int *piv_dev;
@@ -39,17 +47,141 @@ static _Thread_local struct {
   double *orig_dev;      /* split form: the FP64 matrix (refinement residuals) */
   double anorm;          /* split form: its infinity norm */
   int mixed;
-} g_cache;
+  int *piv_host;         /* pivots and diagonal written back (recognition) */
+  nec2c_cuda_complex *diag_host;
+  size_t bytes;          /* device bytes held */
+  unsigned long long stamp;
+} dense_entry;
 
+static _Thread_local dense_entry *g_entries = NULL;
+static _Thread_local size_t g_entry_bytes = 0;
+static _Thread_local unsigned long long g_entry_clock = 0;
 static _Thread_local int g_last_refinement = 0;
+
+static void entry_free(dense_entry *e)
+{
+  n2d_free(e->lu_dev); n2d_free(e->piv_dev); n2d_free_async(e->lu32_dev); n2d_free(e->orig_dev);
+  free(e->piv_host); free(e->diag_host);
+  g_entry_bytes -= e->bytes;
+  free(e);
+}
+
+/* Unlinks and frees every entry for which drop(e, ctx) holds. */
+static void entries_drop(int (*drop)(const dense_entry *, const void *), const void *ctx)
+{
+  dense_entry **pp = &g_entries;
+  while(*pp) {
+    dense_entry *e = *pp;
+    if(drop(e, ctx)) { *pp = e->next; entry_free(e); }
+    else pp = &e->next;
+  }
+}
+
+static int drop_all(const dense_entry *e, const void *ctx) { (void)e; (void)ctx; return 1; }
+
+/* Storage of a factorisation: n columns of n entries, ld apart (NEC's
+   transposed storage; factrs's symmetry blocks are row blocks of one matrix,
+   matrix.c:1424-1435, so their columns interleave without overlapping). */
+typedef struct { const char *base; size_t n, ld; } host_block;
+
+/* 1 when block b (offset d >= 0 elements after a, same leading dimension)
+   shares an entry with a. */
+static int blocks_overlap_after(size_t d, size_t na, size_t nb, size_t ld)
+{
+  const size_t q = d / ld, r = d % ld;
+  /* b's column j starts at row r of a's column q + j and, when r + nb > ld,
+     runs on into a's column q + j + 1 from row 0. */
+  if(r < na && q < na) return 1;
+  if(r + nb > ld && q + 1 < na) return 1;
+  return 0;
+}
+
+static int blocks_overlap(const host_block *a, const host_block *b)
+{
+  const size_t cpx = 2 * sizeof(double);
+  const char *alo = a->base, *ahi = alo + ((a->ld * (a->n - 1)) + a->n) * cpx;
+  const char *blo = b->base, *bhi = blo + ((b->ld * (b->n - 1)) + b->n) * cpx;
+  if(!(alo < bhi && blo < ahi)) return 0;
+  if(a->ld != b->ld || ((size_t)(blo > alo ? blo - alo : alo - blo)) % cpx) return 1;  /* conservative */
+  if(blo >= alo) return blocks_overlap_after((size_t)(blo - alo) / cpx, a->n, b->n, a->ld);
+  return blocks_overlap_after((size_t)(alo - blo) / cpx, b->n, a->n, a->ld);
+}
+
+static int drop_overlap(const dense_entry *e, const void *ctx)
+{
+  const host_block mine = {(const char *)e->host, e->order, e->ld};
+  return blocks_overlap(&mine, (const host_block *)ctx);
+}
+
+static _Thread_local const dense_entry *g_victim;
+static int drop_victim(const dense_entry *e, const void *ctx) { (void)ctx; return e == g_victim; }
 
 void nec2c_cuda_dense_release(void)
 {
-  n2d_free(g_cache.lu_dev); n2d_free(g_cache.piv_dev); n2d_free_async(g_cache.lu32_dev); n2d_free(g_cache.orig_dev);
-  memset(&g_cache, 0, sizeof(g_cache));
+  entries_drop(drop_all, NULL);
 }
 
 int nec2c_cuda_dense_last_refinement(void) { return g_last_refinement; }
+
+/* Keeps the entries of this thread within a quarter of the device's memory,
+   dropping the least recently used first (their FP64 factors are uploaded
+   again from the host storage when solved; split-precision ones must be
+   factored again). */
+static void entries_trim(size_t incoming)
+{
+  size_t free_b = 0, total_b = 0;
+  if(!n2d_mem_info(&free_b, &total_b) || total_b == 0) return;
+  while(g_entries && g_entry_bytes + incoming > total_b / 4) {
+    dense_entry *e, *lru = g_entries;
+    for(e = g_entries; e; e = e->next) if(e->stamp < lru->stamp) lru = e;
+    g_victim = lru;
+    entries_drop(drop_victim, NULL);
+  }
+}
+
+/* The entry whose factors the host storage holds, or NULL (a stale entry for
+   the same storage is dropped). */
+static dense_entry *entry_find(const void *matrix, size_t n, size_t ld, const int *pivots)
+{
+  dense_entry *e;
+  for(e = g_entries; e; e = e->next) {
+    if(e->host == matrix && e->order == n && e->ld == ld) {
+      const nec2c_cuda_complex *m = matrix;
+      size_t i;
+      int same = !memcmp(e->piv_host, pivots, n * sizeof(int));
+      for(i = 0; same && i < n; ++i) same = m[i * ld + i] == e->diag_host[i];
+      if(same) { e->stamp = ++g_entry_clock; return e; }
+      g_victim = e;
+      entries_drop(drop_victim, NULL);
+      return NULL;
+    }
+  }
+  return NULL;
+}
+
+/* Records a factorisation just written back to the host storage. */
+static int entry_add(dense_entry *proto, const nec2c_cuda_complex *matrix, const int *pivots)
+{
+  size_t i;
+  const size_t n = proto->order, ld = proto->ld;
+  dense_entry *e = malloc(sizeof(*e));
+  if(!e) { n2c_set_error("host allocation failed"); return 0; }
+  *e = *proto;
+  e->piv_host = malloc(n * sizeof(int));
+  e->diag_host = malloc(n * sizeof(nec2c_cuda_complex));
+  if(!e->piv_host || !e->diag_host) {
+    free(e->piv_host); free(e->diag_host); free(e);
+    n2c_set_error("host allocation failed");
+    return 0;
+  }
+  memcpy(e->piv_host, pivots, n * sizeof(int));
+  for(i = 0; i < n; ++i) e->diag_host[i] = matrix[i * ld + i];
+  e->stamp = ++g_entry_clock;
+  e->next = g_entries;
+  g_entries = e;
+  g_entry_bytes += e->bytes;
+  return 1;
+}
 
 static const size_t CPX = 2 * sizeof(double);
 
@@ -176,10 +308,18 @@ int nec2c_cuda_dense_factor_classic(size_t n, nec2c_cuda_complex *matrix, size_t
     return 0;
   }
   if(!n2d_device_ok()) return 0;
-  nec2c_cuda_dense_release();
+  {
+    /* Factors written over an entry's storage replace it. */
+    const host_block blk = {(const char *)matrix, n, ld};
+    entries_drop(drop_overlap, &blk);
+  }
+  entries_trim(n * n * CPX * (g_dense_mixed ? 2 : 1));
   a = upload_matrix(matrix, n, ld);
   piv = n2d_alloc(n * sizeof(int));
   if(!a || !piv) { n2d_free(a); n2d_free(piv); return 0; }
+  dense_entry proto;
+  memset(&proto, 0, sizeof(proto));
+  proto.host = matrix; proto.order = n; proto.ld = ld; proto.piv_dev = piv;
   if(g_dense_mixed) {
     /* Split form: FP32 factors on the device, widened into the host storage;
        the FP64 matrix stays for the refinement. */
@@ -192,16 +332,17 @@ int nec2c_cuda_dense_factor_classic(size_t n, nec2c_cuda_complex *matrix, size_t
          n2d_download2d(matrix, ld * CPX, wide, n * CPX, n * CPX, n) && n2d_download(pivots, piv, n * sizeof(int));
     n2d_free(wide);
     if(!ok) { n2d_free_async(f.lu32); n2d_free(a); n2d_free(piv); return 0; }
-    g_cache.host = matrix; g_cache.order = n; g_cache.ld = ld; g_cache.piv_dev = piv; g_cache.mixed = 1;
-    g_cache.lu32_dev = f.lu32; g_cache.ld32 = f.ld32; g_cache.orig_dev = a; g_cache.anorm = f.anorm;
+    proto.mixed = 1; proto.lu32_dev = f.lu32; proto.ld32 = f.ld32; proto.orig_dev = a; proto.anorm = f.anorm;
+    proto.bytes = n * n * CPX + n * f.ld32 * 2 * sizeof(float) + n * sizeof(int);
+    if(!entry_add(&proto, matrix, pivots)) { n2d_free_async(f.lu32); n2d_free(a); n2d_free(piv); return 0; }
     return 1;
   }
   ok = n2d_lu_factor(a, (long long)n, (long long)n, piv, 0, 0, &info);
   ok = ok && n2d_download2d(matrix, ld * CPX, a, n * CPX, n * CPX, n) &&
        n2d_download(pivots, piv, n * sizeof(int));
   if(!ok || info) { n2d_free(a); n2d_free(piv); if(ok && info) n2c_set_error("matrix is singular (pivot %d)", info); return 0; }
-  g_cache.host = matrix; g_cache.order = n; g_cache.ld = ld;
-  g_cache.lu_dev = a; g_cache.piv_dev = piv; g_cache.mixed = 0;
+  proto.lu_dev = a; proto.bytes = n * n * CPX + n * sizeof(int);
+  if(!entry_add(&proto, matrix, pivots)) { n2d_free(a); n2d_free(piv); return 0; }
   return 1;
 }
 
@@ -218,21 +359,30 @@ int nec2c_cuda_dense_solve_classic_many(size_t n, const nec2c_cuda_complex *matr
     return 0;
   }
   if(!n2d_device_ok()) return 0;
-  const int cached = g_cache.piv_dev && g_cache.host == (const void *)matrix && g_cache.order == n && g_cache.ld == ld;
+  const dense_entry *e = entry_find(matrix, n, ld, pivots);
+  if(!e && g_dense_mixed) {
+    /* Split-precision factors carry FP32 accuracy; only the refinement
+       against the FP64 matrix, which lives with the entry, gives the FP64
+       answer.  Without it the solve is refused rather than returned at FP32
+       accuracy. */
+    n2c_set_error("solve: the split-precision factors of this matrix are not on the device (factored in another "
+                  "thread or process, released, or overwritten); factor it again");
+    return 0;
+  }
   b = n2d_alloc(n * count * CPX);
   if(!b || !n2d_upload2d(b, n * CPX, rhs, stride * CPX, n * CPX, count)) { n2d_free(b); return 0; }
-  if(cached && g_cache.mixed) {
-    split_factors f = {g_cache.lu32_dev, g_cache.ld32, g_cache.piv_dev, g_cache.orig_dev, g_cache.anorm};
+  if(e && e->mixed) {
+    split_factors f = {e->lu32_dev, e->ld32, e->piv_dev, e->orig_dev, e->anorm};
     ok = solve_refined(n, &f, b, count, &g_last_refinement) &&
          n2d_download2d(rhs, stride * CPX, b, n * CPX, n * CPX, count);
     n2d_free(b);
     return ok;
   }
-  if(cached) {
-    lu = g_cache.lu_dev; piv = g_cache.piv_dev;
+  if(e) {
+    lu = e->lu_dev; piv = e->piv_dev;
   } else {
-    /* Factors produced earlier (or in another process): upload them as
-       stored.  Split-precision factors solved this way carry FP32 accuracy. */
+    /* FP64 factors produced earlier (in another thread or process, or
+       dropped from the device): upload them as stored. */
     own = 1;
     lu = n2d_alloc(n * n * CPX);
     piv = n2d_alloc(n * sizeof(int));

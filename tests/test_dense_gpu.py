@@ -175,3 +175,63 @@ def test_batched_ragged_matches_oracle():
         bo = b.copy()
         oracle().oracle_solve(n, ptr(st0), ptr(po), ptr(bo), ld)
         assert np.linalg.norm(xb - bo) / np.linalg.norm(bo) < 1e-12, k
+
+
+def test_split_precision_reference_call_order():
+    """"cuda-mixed" in the reference's call order: factrs factors every
+    symmetry block (row blocks of one storage, matrix.c:1424-1435), netwk then
+    factors its network matrix (network.c:505), and only afterwards solves
+    the blocks (solves, matrix.c:1683-1701) and the network matrix (solve,
+    network.c:550).  Every solution is within 1e-10 of the oracle's FP64
+    solve, each reached by refinement."""
+    nop, npb, nn = 4, 150, 40
+    nrow = nop * npb
+    blocks = [mom_like(npb, 60 + k) for k in range(nop)]
+    st = np.zeros((nrow, npb), dtype=np.complex128, order="F")
+    for k, a in enumerate(blocks):
+        st[k * npb:(k + 1) * npb, :] = a.T
+    cmn_a = mom_like(nn, 77)
+    cmn = nec_storage(cmn_a, nn + 2)
+    ip = np.zeros(nrow, dtype=np.int32)
+    lib = nb.load()
+    assert nb.dense_backend_set("cuda-mixed")
+    try:
+        # factrs: factr(np, &a[kk*np], &ip[kk*np], nrow) per block.
+        itemsize = st.itemsize
+        for k in range(nop):
+            assert lib.nec2c_cuda_dense_factor_classic(npb, st.ctypes.data + k * npb * itemsize, nrow,
+                                                       ip.ctypes.data + k * npb * 4), nb.last_error()
+        ok, ipn = nb.factor_classic(cmn)
+        assert ok
+        rng = np.random.default_rng(5)
+        for k, a in enumerate(blocks):
+            x = rng.standard_normal(npb) + 1j * rng.standard_normal(npb)
+            b = np.zeros(nrow, dtype=np.complex128)
+            b[k * npb:(k + 1) * npb] = a @ x
+            assert lib.nec2c_cuda_dense_solve_classic_many(npb, st.ctypes.data + k * npb * itemsize, nrow,
+                                                           ip.ctypes.data + k * npb * 4,
+                                                           b.ctypes.data + k * npb * itemsize, nrow, 1), \
+                nb.last_error()
+            assert lib.nec2c_cuda_dense_last_refinement() >= 1
+            ao = nec_storage(a, npb).copy(order="F")
+            po = np.zeros(npb, dtype=np.int32)
+            assert oracle().oracle_factr(npb, ptr(ao), ptr(po), npb)
+            bo = np.ascontiguousarray(a @ x)
+            oracle().oracle_solve(npb, ptr(ao), ptr(po), ptr(bo), npb)
+            got = b[k * npb:(k + 1) * npb]
+            assert np.linalg.norm(got - bo) / np.linalg.norm(bo) < 1e-10, k
+        xn = rng.standard_normal(nn) + 1j * rng.standard_normal(nn)
+        rhs = np.zeros((nn + 2, 1), dtype=np.complex128, order="F")
+        rhs[:nn, 0] = cmn_a @ xn
+        assert nb.solve_classic_many(cmn, ipn, rhs)
+        assert lib.nec2c_cuda_dense_last_refinement() >= 1
+        assert np.linalg.norm(rhs[:nn, 0] - xn) / np.linalg.norm(xn) < 1e-10
+        # Once the device copies are dropped, a split-precision solve is
+        # refused rather than returned at FP32 accuracy.
+        lib.nec2c_cuda_dense_release()
+        rhs[:nn, 0] = cmn_a @ xn
+        assert not nb.solve_classic_many(cmn, ipn, rhs)
+        assert "factor it again" in nb.last_error()
+    finally:
+        nb.dense_backend_set("cuda")
+        lib.nec2c_cuda_dense_release()
