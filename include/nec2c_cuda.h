@@ -120,6 +120,19 @@ int nec2c_cuda_vie_fft_schedule(nec2c_cuda_vie_plan *plan, int fp64, int tiles[5
    splits on offer for the pass's length.  Returns 0 (schedule unchanged) on
    anything else. */
 int nec2c_cuda_vie_fft_set_schedule(nec2c_cuda_vie_plan *plan, int fp64, const int tiles[5], const int r1[5]);
+/* Fused yz-plane passes.  Where the padded y and z axes have one length P of
+   32, 64 or 128, passes 0-1 and 3-4 can instead run as two kernels that
+   transform a whole lattice plane in shared memory (P = 2Q: each plane is four
+   Q x Q transforms of the parity classes of (ky, kz); the inverse sums them in
+   a four-CTA cluster), so a product is three launches.  The tuner times both
+   forms on a new plan and keeps the plane passes when they are at least 3%
+   faster; without autotuning they are used wherever they apply.  planes()
+   returns 1 (plane passes), 0 (five passes) or -1 (not applicable, or a bad
+   argument); set_planes pins the choice (with the schedule above, for
+   results that repeat bit for bit) and returns 0 when not applicable.  The
+   forms compute the same product; they round differently. */
+int nec2c_cuda_vie_fft_planes(nec2c_cuda_vie_plan *plan, int fp64);
+int nec2c_cuda_vie_fft_set_planes(nec2c_cuda_vie_plan *plan, int fp64, int planes);
 
 /* --------------------------------------- hybrid conductor + volume system */
 typedef struct nec2c_cuda_hybrid nec2c_cuda_hybrid;

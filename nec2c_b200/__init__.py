@@ -84,6 +84,8 @@ def load():
         "nec2c_cuda_vie_fft_tune": (i, [vp, i]),
         "nec2c_cuda_vie_fft_schedule": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
         "nec2c_cuda_vie_fft_set_schedule": (i, [vp, i, C.POINTER(i), C.POINTER(i)]),
+        "nec2c_cuda_vie_fft_planes": (i, [vp, i]),
+        "nec2c_cuda_vie_fft_set_planes": (i, [vp, i, i]),
         "nec2c_cuda_vie_batch_create": (i, [C.POINTER(vp), C.POINTER(vp), sz]),
         "nec2c_cuda_vie_batch_destroy": (None, [vp]),
         "nec2c_cuda_hybrid_batch_create": (i, [C.POINTER(vp), C.POINTER(vp), sz]),
@@ -250,6 +252,13 @@ class VolumePlan:
         tiles = (C.c_int * 5)(*[int(t) for t, _ in passes])
         r1 = (C.c_int * 5)(*[int(r) for _, r in passes])
         return bool(load().nec2c_cuda_vie_fft_set_schedule(self.h, int(bool(fp64)), tiles, r1))
+
+    def planes(self, fp64=False):
+        """1: fused yz-plane passes in use, 0: five passes, -1: not applicable."""
+        return load().nec2c_cuda_vie_fft_planes(self.h, int(bool(fp64)))
+
+    def set_planes(self, planes, fp64=False):
+        return bool(load().nec2c_cuda_vie_fft_set_planes(self.h, int(bool(fp64)), int(bool(planes))))
 
     def bytes(self):
         return load().nec2c_cuda_vie_fft_bytes(self.h)

@@ -106,6 +106,10 @@ int n2d_vie_radiation(n2d_vie *p, const double *current_dev, const double origin
 int n2d_vie_schedule(n2d_vie *p, int prec, int *tiles, int *r1);
 /* Pins a schedule (heights and splits the tuner would try; 0 otherwise). */
 int n2d_vie_set_schedule(n2d_vie *p, int prec, const int *tiles, const int *r1);
+/* Fused yz-plane passes for precision prec: 1 in use, 0 the five passes, -1
+   not applicable to the grid; set returns 0 (error set) when not applicable. */
+int n2d_vie_planes(n2d_vie *p, int prec);
+int n2d_vie_set_planes(n2d_vie *p, int prec, int planes);
 
 /* ---- hybrid [C B; D V] operator (dielectric_fft.c) ---- */
 typedef struct n2d_hybrid n2d_hybrid;

@@ -59,4 +59,36 @@ int fft_launch_pass(int mode, int L, int variant, const PassArgs<C> &a, size_t s
 template <typename C>
 int fft_zline_occupancy(int mode, int L, int variant, size_t smem);
 
+// ------------------------------------------------- fused yz-plane passes
+// (fft_plane.cuh): the y and z transforms of a lattice plane in one kernel,
+// for padded y and z axes of the same length P = 2Q.
+template <typename C> struct PlaneArgs {
+  C *grid;                       // [3][nx][P][P] (y, z padded to P)
+  const C *twy, *twz;            // exp(-2 pi i m / P), m < P, of the y and z axes
+  int nx, ny, nz;                // lattice
+  const int *gate;               // skip all work when *gate == 0 (NULL: always run)
+  const double2 *cx;             // cell vector x (3 per cell)
+  double2 *cy;                   // cell vector y (inverse pass)
+  const double2 *eps;            // per-cell permittivity
+  const int *box_cell;           // box index -> cell (-1: empty)
+  double2 self0, self1, self2;   // self terms of the Jacobi divisor
+  long long mirror;              // PEC physical cells (0: none)
+  int precondition;              // the operator acts on x ./ diag
+  int *flag;                     // non-finite input / output
+  double *partials, *norm;       // |y|^2 reduction (norm NULL: none)
+  unsigned int *ticket;
+};
+
+// Shared memory of one plane CTA: a Q x (Q+1) tile.
+template <typename C> constexpr size_t plane_smem(int Q) { return (size_t)Q * (Q + 1) * sizeof(C); }
+
+// Q (= P/2 of the y and z axes) values the plane kernels are built for.
+inline bool plane_supported(int Q) { return Q == 16 || Q == 32 || Q == 64; }
+
+// One plane pass (forward with the cell scatter, or inverse with the
+// epilogue) of 12 nx CTAs on stream.  Q as plane_supported; 0 with the error
+// set otherwise.
+template <typename C>
+int fft_plane_launch(bool inverse, int Q, const PlaneArgs<C> &a, cudaStream_t stream);
+
 }  // namespace n2c

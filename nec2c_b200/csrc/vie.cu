@@ -534,6 +534,7 @@ extern "C" int n2d_vie_create(n2d_vie **out, const long long shape[3], const lon
     free_plan(p);
     return 0;
   }
+  p->planes[0] = p->planes[1] = 1;
   *out = p;
   return 1;
 }
@@ -715,13 +716,48 @@ static int run_pass(n2d_vie *p, int pass, n2d_pass_choice ch, const double2 *x, 
   return fft_launch_pass<C>(pp.mode, pp.L, pp.variant, pp.a, pp.smem, pp.tiles);
 }
 
+// The fused yz-plane passes apply when the padded y and z axes have the same
+// length P = 2Q with Q one the plane kernels are built for, and the inverse
+// pass's norm reduction (one partial per CTA, 12 nx CTAs) fits the plan's
+// partials.
+static bool plane_ok(const n2d_vie *p) {
+  return p->P[1] == p->P[2] && plane_supported((int)(p->P[1] / 2)) && p->S[1] <= p->P[1] / 2 &&
+         p->S[2] <= p->P[2] / 2 && 12 * p->S[0] <= 65536;
+}
+
 template <typename C>
-static int apply_t(n2d_vie *p, const double2 *x, double2 *y, int precondition, double *norm,
-                   int *flag) {
+static int apply_planes(n2d_vie *p, const double2 *x, double2 *y, int precondition, double *norm, int *flag) {
+  constexpr bool single = sizeof(C) == sizeof(float2);
+  PlaneArgs<C> a;
+  memset(&a, 0, sizeof(a));
+  a.grid = (C *)p->t2;
+  a.twy = single ? (const C *)p->tw32[1] : (const C *)p->tw64[1];
+  a.twz = single ? (const C *)p->tw32[2] : (const C *)p->tw64[2];
+  a.nx = (int)p->S[0]; a.ny = (int)p->S[1]; a.nz = (int)p->S[2];
+  a.gate = n2c_gate();
+  a.cx = x; a.cy = y; a.eps = p->eps; a.box_cell = p->box_cell;
+  a.self0 = p->self[0]; a.self1 = p->self[1]; a.self2 = p->self[2];
+  a.mirror = p->mirror; a.precondition = precondition; a.flag = flag;
+  a.partials = p->partials; a.ticket = p->ticket; a.norm = norm;
+  const int Q = (int)(p->P[1] / 2);
+  return fft_plane_launch<C>(false, Q, a, n2c_stream()) &&
+         run_pass<C>(p, 2, p->sched[prec_of<C>()][2], x, y, precondition, norm, flag) &&
+         fft_plane_launch<C>(true, Q, a, n2c_stream());
+}
+
+template <typename C>
+static int apply_five(n2d_vie *p, const double2 *x, double2 *y, int precondition, double *norm, int *flag) {
   const n2d_pass_choice *s = p->sched[prec_of<C>()];
   for (int i = 0; i < N2D_VIE_PASSES; ++i)
     if (!run_pass<C>(p, i, s[i], x, y, precondition, norm, flag)) return 0;
   return 1;
+}
+
+template <typename C>
+static int apply_t(n2d_vie *p, const double2 *x, double2 *y, int precondition, double *norm,
+                   int *flag) {
+  if (p->planes[prec_of<C>()] && plane_ok(p)) return apply_planes<C>(p, x, y, precondition, norm, flag);
+  return apply_five<C>(p, x, y, precondition, norm, flag);
 }
 
 extern "C" int n2d_vie_apply(n2d_vie *p, const double *x, double *y, int precondition_input,
@@ -748,6 +784,7 @@ struct TuneEntry {
   long long S[3], P[3];
   int prec;
   n2d_pass_choice c[N2D_VIE_PASSES];
+  int planes;
 };
 std::mutex g_tune_lock;
 std::vector<TuneEntry> g_tune_cache;
@@ -826,6 +863,25 @@ float time_candidate(n2d_vie *p, int pass, n2d_pass_choice ch, const double2 *x,
   return best;
 }
 
+// Milliseconds of three whole products with the plan's current schedule
+// (best of two runs), or a negative value when a product fails.
+template <typename C>
+float time_product(n2d_vie *p, const double2 *x, double2 *y, double *norm, cudaEvent_t e0, cudaEvent_t e1) {
+  if (!apply_t<C>(p, x, y, 0, norm, nullptr)) return -1.0f;
+  float best = -1.0f;
+  for (int trial = 0; trial < 2; ++trial) {
+    if (cudaEventRecord(e0, n2c_stream()) != cudaSuccess) return -1.0f;
+    for (int r = 0; r < 3; ++r)
+      if (!apply_t<C>(p, x, y, 0, norm, nullptr)) return -1.0f;
+    float ms = 0;
+    if (cudaEventRecord(e1, n2c_stream()) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+      return -1.0f;
+    if (best < 0 || ms < best) best = ms;
+  }
+  return best;
+}
+
 template <typename C>
 int tune_precision(n2d_vie *p, const double2 *x, double2 *y, double *norm, bool use_cache) {
   const int prec = prec_of<C>();
@@ -834,6 +890,7 @@ int tune_precision(n2d_vie *p, const double2 *x, double2 *y, double *norm, bool 
     for (const TuneEntry &e : g_tune_cache)
       if (tune_key_is(e, p, prec)) {
         memcpy(p->sched[prec], e.c, sizeof(e.c));
+        p->planes[prec] = e.planes;
         p->tuned[prec] = 1;
         return 1;
       }
@@ -870,16 +927,28 @@ int tune_precision(n2d_vie *p, const double2 *x, double2 *y, double *norm, bool 
     }
     chosen[pass] = best;
   }
+  memcpy(p->sched[prec], chosen, sizeof(chosen));
+  // Whole products: the five tuned passes against the fused plane passes
+  // around the tuned x pass; the planes are kept when at least 3% faster.
+  int planes = 0;
+  if (plane_ok(p)) {
+    p->planes[prec] = 0;
+    const float t5 = time_product<C>(p, x, y, norm, e0, e1);
+    p->planes[prec] = 1;
+    const float t3 = time_product<C>(p, x, y, norm, e0, e1);
+    planes = t3 >= 0 && (t5 < 0 || t3 < 0.97f * t5);
+  }
+  p->planes[prec] = planes;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   // A candidate that could not run may have left a launch error behind.
   cudaGetLastError();
-  memcpy(p->sched[prec], chosen, sizeof(chosen));
   p->tuned[prec] = 1;
   std::lock_guard<std::mutex> hold(g_tune_lock);
   TuneEntry e;
   for (int d = 0; d < 3; ++d) { e.S[d] = p->S[d]; e.P[d] = p->P[d]; }
   e.prec = prec;
+  e.planes = planes;
   memcpy(e.c, chosen, sizeof(chosen));
   for (TuneEntry &old : g_tune_cache)
     if (tune_key_is(old, p, prec)) { old = e; return 1; }
@@ -900,6 +969,7 @@ extern "C" int n2d_vie_tune(n2d_vie *p, int measure) {
   p->gm_work = nullptr;
   memset(p->sched, 0, sizeof(p->sched));
   p->tuned[0] = p->tuned[1] = 0;
+  p->planes[0] = p->planes[1] = 1;
   if (measure == 0 || p->cells == 0) return 1;
   const size_t vec = 3 * (size_t)p->cells * sizeof(double2);
   double2 *x = (double2 *)n2d_alloc(vec), *y = (double2 *)n2d_alloc(vec);
@@ -914,6 +984,7 @@ extern "C" int n2d_vie_tune(n2d_vie *p, int measure) {
   if (!ok) {
     memset(p->sched, 0, sizeof(p->sched));
     p->tuned[0] = p->tuned[1] = 0;
+    p->planes[0] = p->planes[1] = 1;
   }
   return ok;
 }
@@ -947,6 +1018,27 @@ extern "C" int n2d_vie_set_schedule(n2d_vie *p, int prec, const int *tiles, cons
   p->gm_work = nullptr;
   memcpy(p->sched[prec], c, sizeof(c));
   p->tuned[prec] = 1;
+  return 1;
+}
+
+// Whether precision prec runs passes 0-1 and 3-4 as the fused plane passes:
+// 1 yes, 0 no (the five passes), -1 when the plane passes do not apply to the
+// plan's grid.
+extern "C" int n2d_vie_planes(n2d_vie *p, int prec) {
+  if (!plane_ok(p)) return -1;
+  return p->planes[prec ? 1 : 0] ? 1 : 0;
+}
+
+// Pins the choice above (the tuner makes it by timing both forms).  Returns 0
+// with the error set when the plane passes do not apply.
+extern "C" int n2d_vie_set_planes(n2d_vie *p, int prec, int planes) {
+  if (planes && !plane_ok(p)) {
+    n2c_set_error("the fused plane passes do not apply to this grid (padded y and z must be one length 32, 64 or 128)");
+    return 0;
+  }
+  n2c_gmres_work_free(p->gm_work);
+  p->gm_work = nullptr;
+  p->planes[prec ? 1 : 0] = planes ? 1 : 0;
   return 1;
 }
 

@@ -43,4 +43,7 @@ struct n2d_vie {
   // once the tuner has measured precision i for this plan.
   n2d_pass_choice sched[2][N2D_VIE_PASSES];
   int tuned[2];
+  // planes[i] != 0: passes 0-1 and 3-4 of precision i run as the fused
+  // yz-plane kernels (fft_plane.cuh) where the grid allows them.
+  int planes[2];
 };

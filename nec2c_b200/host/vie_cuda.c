@@ -350,6 +350,22 @@ int nec2c_cuda_vie_fft_set_schedule(nec2c_cuda_vie_plan *p, int fp64, const int 
   return n2d_vie_set_schedule(p->dev, fp64 ? 1 : 0, tiles, r1);
 }
 
+int nec2c_cuda_vie_fft_planes(nec2c_cuda_vie_plan *p, int fp64)
+{
+  if(!p) return -1;
+  if(!fp64 && !n2d_vie_fp32(p->dev)) return -1;
+  if(!nec2c_cuda_plan_device(p)) return -1;
+  return n2d_vie_planes(p->dev, fp64 ? 1 : 0);
+}
+
+int nec2c_cuda_vie_fft_set_planes(nec2c_cuda_vie_plan *p, int fp64, int planes)
+{
+  if(!p) { n2c_set_error("set_planes: bad argument"); return 0; }
+  if(!fp64 && !n2d_vie_fp32(p->dev)) { n2c_set_error("set_planes: the plan has no FP32 transforms"); return 0; }
+  if(!nec2c_cuda_plan_device(p)) return 0;
+  return n2d_vie_set_planes(p->dev, fp64 ? 1 : 0, planes);
+}
+
 /* ------------------------------------------------------------------ hybrid */
 struct nec2c_cuda_hybrid {
   n2d_hybrid *dev;
