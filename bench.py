@@ -53,6 +53,9 @@ def parse():
                     help="JSON file of the c2 plans' FFT pass schedules: written by the first run "
                          "that names it, pinned by later runs (a run under ncu would otherwise "
                          "tune on serialised, slowed launches)")
+    ap.add_argument("--planes", type=int, choices=[0, 1], default=None,
+                    help="profiling driver: pin the fused yz-plane passes on (1) or off (0) in both "
+                         "c2 plans instead of the tuner's choice")
     ap.add_argument("--only", choices=["matvec", "solve", "lu", "serving", "volume_batch"],
                     help="profiling driver: build the plans, run --steps FP32 and FP64 products "
                          "(matvec) or --steps mixed solves (solve), or factor the 1984-unknown dense "
@@ -483,6 +486,18 @@ def run_ours(args, rank, world, local_rank):
 
     mv32_ms = time_matvec(plan_m)
     mv64_ms = time_matvec(plan_d)
+    planes32, planes64 = plan_m.planes(fp64=False), plan_d.planes(fp64=True)
+    # Both product forms on the same plans: the fused plane passes (three
+    # launches) and the five passes.
+    forms = {}
+    for key, plan, fp64, chosen in (("fp32", plan_m, False, planes32), ("fp64", plan_d, True, planes64)):
+        if chosen < 0:
+            continue
+        forms[key] = {}
+        for planes in (1, 0):
+            plan.set_planes(planes, fp64=fp64)
+            forms[key]["planes_ms" if planes else "five_pass_ms"] = time_matvec(plan)
+        plan.set_planes(chosen, fp64=fp64)
     # The measured pass schedule against the heuristic one on the same plan.
     tuned32, tuned64 = plan_m.schedule(fp64=False)[1], plan_d.schedule(fp64=True)[1]
     plan_m.tune(0)
@@ -497,6 +512,8 @@ def run_ours(args, rank, world, local_rank):
         "fp32": {"tuned": tuned32, "heuristic": heur32, "tuned_ms": mv32_ms, "heuristic_ms": mv32_heur_ms},
         "fp64": {"tuned": tuned64, "heuristic": heur64, "tuned_ms": mv64_ms, "heuristic_ms": mv64_heur_ms},
         "entry": "[lines per tile, R1]",
+        "planes_in_use": {"fp32": planes32, "fp64": planes64},
+        "forms_ms": forms,
     }
     C_, G_ = w["cells"], w["grid"]
     bytes32 = 8 * (6 * C_ + 18 * G_)
@@ -534,7 +551,9 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": MATVEC_TRAFFIC_BYTES,
-                     "kernel": "FFT matvec (scatter + 5 transform passes + gather), FP32",
+                     "kernel": ("FFT matvec, FP32: fused yz-plane forward (scatter), x pass with the "
+                                "spectrum product, fused yz-plane inverse (epilogue)" if planes32 == 1 else
+                                "FFT matvec (scatter + 5 transform passes + gather), FP32"),
                      "algorithmic_bytes": bytes32, "ms": mv32_ms},
         "matvec_fp64": {"ms": mv64_ms, "achieved_gbs": bytes64 / (mv64_ms * 1e-3) / 1e9},
         "fft_schedule": schedule,
@@ -551,6 +570,11 @@ def run_ours(args, rank, world, local_rank):
 
 def profile_driver(args, lib, nb, torch, stream, plan_m, plan_d, w):
     n = plan_m.n
+    if args.planes is not None:
+        for plan, precs in ((plan_m, (False, True)), (plan_d, (True,))):
+            for fp64 in precs:
+                if not plan.set_planes(args.planes, fp64=fp64):
+                    raise RuntimeError(nb.last_error())
     x = torch.randn(n, dtype=torch.complex128, device="cuda")
     y = torch.empty_like(x)
     torch.cuda.synchronize()
@@ -579,7 +603,8 @@ def profile_driver(args, lib, nb, torch, stream, plan_m, plan_d, w):
     torch.cuda.nvtx.range_pop()
     print(json.dumps({"profile": args.only, "steps": args.steps, "s": time.perf_counter() - t0,
                       "fft_schedule": {"fp32": plan_m.schedule(fp64=False)[1],
-                                       "fp64": plan_d.schedule(fp64=True)[1]}}))
+                                       "fp64": plan_d.schedule(fp64=True)[1],
+                                       "planes": [plan_m.planes(fp64=False), plan_d.planes(fp64=True)]}}))
     return 0
 
 

@@ -492,25 +492,54 @@ __device__ __forceinline__ void fft_zline_tile(const PassArgs<C> &a, long long t
   const int NP = NL / 3;
   // ---- load
   if (CELLS && !INV) {
+    // CH elements per thread with their loads issued together (box index ->
+    // cell, then the cell's value and permittivity): two round trips per
+    // chunk instead of two per element.
+    constexpr int CH = 4;
     const long long p0 = tile * NP;
-    for (int idx = threadIdx.x; idx < NP * L * 3; idx += blockDim.x) {
-      const int c = idx % 3, rest = idx / 3, e = rest % L, p = rest / L;
-      C val = czero<C>();
-      const long long pos = p0 + p;
-      if (e < a.n_in && pos < a.nxy) {
-        long long cell = a.box_cell[pos * a.A_in + e];
-        if (cell >= 0) {
-          double sgn = 1;
-          if (a.mirror && cell >= a.mirror) { cell -= a.mirror; if (c < 2) sgn = -1; }
-          double2 v = a.cx[3 * cell + c];
-          if (a.precondition) v = jacobi_apply<C>(v, jacobi_divisor(a, a.eps[cell], c));
-          if (a.flag && !finite2(v)) *a.flag = 1;
-          val = from_d<C>(make_double2(sgn * v.x, sgn * v.y));
+    const int total = NP * L * 3;
+    for (int base = threadIdx.x; base < total; base += CH * blockDim.x) {
+      int cell[CH];
+#pragma unroll
+      for (int i = 0; i < CH; ++i) {
+        const int idx = base + i * blockDim.x;
+        cell[i] = -1;
+        if (idx < total) {
+          const int rest = idx / 3, e = rest % L, p = rest / L;
+          const long long pos = p0 + p;
+          if (e < a.n_in && pos < a.nxy) cell[i] = a.box_cell[pos * a.A_in + e];
         }
       }
-      S[e * NLP + c * NP + p] = val;
+      double2 v[CH], ep[CH];
+      bool neg[CH];
+#pragma unroll
+      for (int i = 0; i < CH; ++i) {
+        neg[i] = false;
+        if (cell[i] >= 0) {
+          const int c = (base + i * blockDim.x) % 3;
+          if (a.mirror && cell[i] >= a.mirror) { cell[i] -= (int)a.mirror; neg[i] = c < 2; }
+          v[i] = a.cx[3 * (long long)cell[i] + c];
+          if (a.precondition) ep[i] = a.eps[cell[i]];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < CH; ++i) {
+        const int idx = base + i * blockDim.x;
+        if (idx >= total) continue;
+        const int c = idx % 3, rest = idx / 3, e = rest % L, p = rest / L;
+        C val = czero<C>();
+        if (cell[i] >= 0) {
+          double2 w = v[i];
+          if (a.precondition) w = jacobi_apply<C>(w, jacobi_divisor(a, ep[i], c));
+          if (a.flag && !finite2(w)) *a.flag = 1;
+          if (neg[i]) w = make_double2(-w.x, -w.y);
+          val = from_d<C>(w);
+        }
+        S[e * NLP + c * NP + p] = val;
+      }
     }
   } else {
+#pragma unroll 4
     for (int idx = threadIdx.x; idx < NL * L; idx += blockDim.x) {
       const int t = idx / L, e = idx - t * L;
       const long long l = zline_global(a, CELLS, NP, t, tile);
@@ -525,19 +554,44 @@ __device__ __forceinline__ void fft_zline_tile(const PassArgs<C> &a, long long t
   if (CELLS && INV) {
     double sq = 0;
     const long long p0 = tile * NP;
-    for (int idx = threadIdx.x; idx < NP * a.n_out * 3; idx += blockDim.x) {
-      const int c = idx % 3, rest = idx / 3, p = fdiv(rest, a.nout_div), e = rest - p * a.n_out;
-      const long long pos = p0 + p;
-      if (pos >= a.nxy) continue;
-      const long long cell = a.box_cell[pos * a.A_out + e];
-      if (cell < 0 || (a.mirror && cell >= a.mirror)) continue;
-      const double2 ep = a.eps[cell], em1 = make_double2(ep.x - 1.0, ep.y);
-      double2 z = a.cx[3 * cell + c];
-      if (a.precondition) z = jacobi_apply<C>(z, jacobi_divisor(a, ep, c));
-      const double2 v = csub(cmul(ep, z), cmul(em1, to_d(R[e * NLP + c * NP + p])));
-      a.cy[3 * cell + c] = v;
-      if (a.flag && !finite2(v)) *a.flag = 1;
-      sq += v.x * v.x + v.y * v.y;
+    constexpr int CH = 4;   // outputs per thread whose loads are issued together
+    const int total = NP * a.n_out * 3;
+    for (int base = threadIdx.x; base < total; base += CH * blockDim.x) {
+      int cell[CH];
+#pragma unroll
+      for (int i = 0; i < CH; ++i) {
+        const int idx = base + i * blockDim.x;
+        cell[i] = -1;
+        if (idx < total) {
+          const int rest = idx / 3, p = fdiv(rest, a.nout_div), e = rest - p * a.n_out;
+          const long long pos = p0 + p;
+          if (pos < a.nxy) {
+            const int cl = a.box_cell[pos * a.A_out + e];
+            if (cl >= 0 && !(a.mirror && cl >= a.mirror)) cell[i] = cl;
+          }
+        }
+      }
+      double2 ep[CH], z[CH];
+#pragma unroll
+      for (int i = 0; i < CH; ++i) {
+        if (cell[i] < 0) continue;
+        const int c = (base + i * blockDim.x) % 3;
+        ep[i] = a.eps[cell[i]];
+        z[i] = a.cx[3 * (long long)cell[i] + c];
+      }
+#pragma unroll
+      for (int i = 0; i < CH; ++i) {
+        if (cell[i] < 0) continue;
+        const int idx = base + i * blockDim.x;
+        const int c = idx % 3, rest = idx / 3, p = fdiv(rest, a.nout_div), e = rest - p * a.n_out;
+        const double2 em1 = make_double2(ep[i].x - 1.0, ep[i].y);
+        double2 zz = z[i];
+        if (a.precondition) zz = jacobi_apply<C>(zz, jacobi_divisor(a, ep[i], c));
+        const double2 v = csub(cmul(ep[i], zz), cmul(em1, to_d(R[e * NLP + c * NP + p])));
+        a.cy[3 * (long long)cell[i] + c] = v;
+        if (a.flag && !finite2(v)) *a.flag = 1;
+        sq += v.x * v.x + v.y * v.y;
+      }
     }
     if (a.norm) {
       const double2 bs = block_sum(make_double2(sq, 0));

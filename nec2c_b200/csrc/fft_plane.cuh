@@ -168,31 +168,54 @@ constexpr int PLANE_THREADS = 256;
 
 // Forward: CTA b = ((c * nx + x) * 4 + ry * 2 + rz).
 template <typename C, int R1, int R2>
-__global__ void __launch_bounds__(PLANE_THREADS) fft_plane_forward(PlaneArgs<C> a) {
+__global__ void __launch_bounds__(PLANE_THREADS, 3) fft_plane_forward(PlaneArgs<C> a) {
   if (a.gate && *(volatile const int *)a.gate == 0) return;
   constexpr int Q = R1 * R2, QP = Q + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *S = reinterpret_cast<C *>(smem_raw);
   const int par = blockIdx.x & 3, ry = par >> 1, rz = par & 1;
   const int plane = blockIdx.x >> 2, c = plane / a.nx, x = plane - c * a.nx;
-  // Load: S[jz][jy] = twiddled cell value (zero outside the lattice).
-  for (int idx = threadIdx.x; idx < Q * Q; idx += PLANE_THREADS) {
-    const int jy = idx / Q, jz = idx - jy * Q;
-    C val = czero<C>();
-    if (jy < a.ny && jz < a.nz) {
-      long long cell = a.box_cell[((long long)x * a.ny + jy) * a.nz + jz];
-      if (cell >= 0) {
-        double sgn = 1;
-        if (a.mirror && cell >= a.mirror) { cell -= a.mirror; if (c < 2) sgn = -1; }
-        double2 v = a.cx[3 * cell + c];
-        if (a.precondition) v = jacobi_apply<C>(v, plane_divisor(a, a.eps[cell], c));
-        if (a.flag && !finite2(v)) *a.flag = 1;
-        val = from_d<C>(make_double2(sgn * v.x, sgn * v.y));
+  // Load: S[jz][jy] = twiddled cell value (zero outside the lattice).  Each
+  // thread takes PER elements, CH at a time with their loads issued together
+  // (box index -> cell, then the cell's value and permittivity), so the
+  // dependent global loads cost two round trips per chunk, not two per
+  // element.
+  constexpr int PER = Q * Q / PLANE_THREADS, CH = PER < 4 ? PER : 4;
+  static_assert(PER * PLANE_THREADS == Q * Q && PER % CH == 0, "plane tile per thread");
+#pragma unroll
+  for (int base = 0; base < PER; base += CH) {
+    int cell[CH];
+#pragma unroll
+    for (int i = 0; i < CH; ++i) {
+      const int idx = threadIdx.x + (base + i) * PLANE_THREADS, jy = idx / Q, jz = idx - jy * Q;
+      cell[i] = (jy < a.ny && jz < a.nz) ? a.box_cell[((long long)x * a.ny + jy) * a.nz + jz] : -1;
+    }
+    double2 v[CH], e[CH];
+    bool neg[CH];
+#pragma unroll
+    for (int i = 0; i < CH; ++i) {
+      neg[i] = false;
+      if (cell[i] >= 0) {
+        if (a.mirror && cell[i] >= a.mirror) { cell[i] -= (int)a.mirror; neg[i] = c < 2; }
+        v[i] = a.cx[3 * (long long)cell[i] + c];
+        if (a.precondition) e[i] = a.eps[cell[i]];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < CH; ++i) {
+      const int idx = threadIdx.x + (base + i) * PLANE_THREADS, jy = idx / Q, jz = idx - jy * Q;
+      C val = czero<C>();
+      if (cell[i] >= 0) {
+        double2 w = v[i];
+        if (a.precondition) w = jacobi_apply<C>(w, plane_divisor(a, e[i], c));
+        if (a.flag && !finite2(w)) *a.flag = 1;
+        if (neg[i]) w = make_double2(-w.x, -w.y);
+        val = from_d<C>(w);
         if (ry && jy) val = cmul(val, __ldg(&a.twy[jy]));
         if (rz && jz) val = cmul(val, __ldg(&a.twz[jz]));
       }
+      S[jz * QP + jy] = val;
     }
-    S[jz * QP + jy] = val;
   }
   __syncthreads();
   plane_step1<C, R1, R2, false>(S, a.twz);                          // z, lines jy
@@ -207,7 +230,7 @@ __global__ void __launch_bounds__(PLANE_THREADS) fft_plane_forward(PlaneArgs<C> 
 
 // Inverse with the epilogue: cluster of the four parity CTAs of a plane.
 template <typename C, int R1, int R2>
-__global__ void __launch_bounds__(PLANE_THREADS) fft_plane_inverse(PlaneArgs<C> a) {
+__global__ void __launch_bounds__(PLANE_THREADS, 3) fft_plane_inverse(PlaneArgs<C> a) {
   if (a.gate && *(volatile const int *)a.gate == 0) return;
   namespace cg = cooperative_groups;
   constexpr int Q = R1 * R2, QP = Q + 1;
@@ -218,10 +241,22 @@ __global__ void __launch_bounds__(PLANE_THREADS) fft_plane_inverse(PlaneArgs<C> 
   const int plane = blockIdx.x >> 2, c = plane / a.nx, x = plane - c * a.nx;
   const int P = 2 * Q;
   const C *in = a.grid + ((long long)c * a.nx + x) * P * P;
-  // Load: S[mz][my] = grid[2my+ry][2mz+rz].
-  for (int idx = threadIdx.x; idx < Q * Q; idx += PLANE_THREADS) {
-    const int my = idx / Q, mz = idx - my * Q;
-    S[mz * QP + my] = in[(2 * my + ry) * P + 2 * mz + rz];
+  // Load: S[mz][my] = grid[2my+ry][2mz+rz], CH loads in flight per thread.
+  constexpr int PER = Q * Q / PLANE_THREADS, CH = PER < 8 ? PER : 8;
+  static_assert(PER * PLANE_THREADS == Q * Q && PER % CH == 0, "plane tile per thread");
+#pragma unroll
+  for (int base = 0; base < PER; base += CH) {
+    C g[CH];
+#pragma unroll
+    for (int i = 0; i < CH; ++i) {
+      const int idx = threadIdx.x + (base + i) * PLANE_THREADS, my = idx / Q, mz = idx - my * Q;
+      g[i] = in[(2 * my + ry) * P + 2 * mz + rz];
+    }
+#pragma unroll
+    for (int i = 0; i < CH; ++i) {
+      const int idx = threadIdx.x + (base + i) * PLANE_THREADS, my = idx / Q, mz = idx - my * Q;
+      S[mz * QP + my] = g[i];
+    }
   }
   __syncthreads();
   plane_inv_stepA<C, R1, R2>(S, a.twz);                              // z, lines my
@@ -244,23 +279,45 @@ __global__ void __launch_bounds__(PLANE_THREADS) fft_plane_inverse(PlaneArgs<C> 
 #pragma unroll
   for (int r = 0; r < 4; ++r) peer[r] = cluster.map_shared_rank(S, r);
   double sq = 0;
-  const int rows = (a.ny - par + 3) / 4;
-  for (int idx = threadIdx.x; idx < rows * a.nz; idx += PLANE_THREADS) {
-    const int i = idx / a.nz, jz = idx - i * a.nz, jy = par + 4 * i;
-    const long long cell = a.box_cell[((long long)x * a.ny + jy) * a.nz + jz];
-    if (cell < 0 || (a.mirror && cell >= a.mirror)) continue;
-    const int s = jz * QP + jy;
-    C f = peer[0][s];
-    f = cadd(f, peer[1][s]);
-    f = cadd(f, peer[2][s]);
-    f = cadd(f, peer[3][s]);
-    const double2 ep = a.eps[cell], em1 = make_double2(ep.x - 1.0, ep.y);
-    double2 z = a.cx[3 * cell + c];
-    if (a.precondition) z = jacobi_apply<C>(z, plane_divisor(a, ep, c));
-    const double2 v = csub(cmul(ep, z), cmul(em1, to_d(f)));
-    a.cy[3 * cell + c] = v;
-    if (a.flag && !finite2(v)) *a.flag = 1;
-    sq += v.x * v.x + v.y * v.y;
+  const int rows = (a.ny - par + 3) / 4, total = rows * a.nz;
+  constexpr int EC = 4;   // outputs per thread whose loads are issued together
+  for (int base = threadIdx.x; base < total; base += EC * PLANE_THREADS) {
+    int cell[EC], s[EC];
+#pragma unroll
+    for (int i = 0; i < EC; ++i) {
+      const int idx = base + i * PLANE_THREADS;
+      cell[i] = -1;
+      s[i] = 0;
+      if (idx < total) {
+        const int r = idx / a.nz, jz = idx - r * a.nz, jy = par + 4 * r;
+        const int cl = a.box_cell[((long long)x * a.ny + jy) * a.nz + jz];
+        if (cl >= 0 && !(a.mirror && cl >= a.mirror)) cell[i] = cl;
+        s[i] = jz * QP + jy;
+      }
+    }
+    double2 ep[EC], z[EC];
+    C f[EC];
+#pragma unroll
+    for (int i = 0; i < EC; ++i) {
+      if (cell[i] < 0) continue;
+      ep[i] = a.eps[cell[i]];
+      z[i] = a.cx[3 * (long long)cell[i] + c];
+      f[i] = peer[0][s[i]];
+      f[i] = cadd(f[i], peer[1][s[i]]);
+      f[i] = cadd(f[i], peer[2][s[i]]);
+      f[i] = cadd(f[i], peer[3][s[i]]);
+    }
+#pragma unroll
+    for (int i = 0; i < EC; ++i) {
+      if (cell[i] < 0) continue;
+      const double2 em1 = make_double2(ep[i].x - 1.0, ep[i].y);
+      double2 zz = z[i];
+      if (a.precondition) zz = jacobi_apply<C>(zz, plane_divisor(a, ep[i], c));
+      const double2 v = csub(cmul(ep[i], zz), cmul(em1, to_d(f[i])));
+      a.cy[3 * (long long)cell[i] + c] = v;
+      if (a.flag && !finite2(v)) *a.flag = 1;
+      sq += v.x * v.x + v.y * v.y;
+    }
   }
   cluster.sync();   // peers' shared memory stays alive until every CTA has read it
   if (a.norm) {

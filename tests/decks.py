@@ -68,6 +68,44 @@ def dipole_cube(directory, freq_mhz=300.0, side_cells=16, eps=(4.0, 0.1), patter
     return path
 
 
+def dipole_cube_sweep(directory, freqs_mhz=(280.0, 300.0, 320.0)):
+    """The dipole beside a 0.2 lambda (at 300 MHz) cube whose permittivity is
+    a frequency table (resource version 3: ER 4 -> 3 -> 2 and conductivity
+    0.01 -> 0.03 S/m between 260 and 340 MHz, interpolated linearly by the
+    reference's material law, dielectric.h:36-56), swept over freqs_mhz in one
+    run (FR card; one execution per frequency).  The mesher sizes the cells for
+    the highest frequency and the table's largest permittivity."""
+    lam = C0 / 300e6
+    deck = "\n".join([
+        "CM dipole beside a dispersive dielectric cube, frequency sweep",
+        "CE",
+        "GW 1 21 0 0 %r 0 0 %r 0.001" % (-lam / 4, lam / 4),
+        "GE 0",
+        "FR 0 %d 0 0 %r %r" % (len(freqs_mhz), freqs_mhz[0],
+                              (freqs_mhz[1] - freqs_mhz[0]) if len(freqs_mhz) > 1 else 0.0),
+        "EX 0 1 11 0 1 0",
+        'DF "cube_table.diel"',
+        "XQ",
+        "EN", ""])
+    diel = "\n".join([
+        "NEC2C-DIELECTRIC 3",
+        "MATERIAL 1 TABLE",
+        "SAMPLE 1 FREQ_MHZ 260 ER 4 SIGMA .01",
+        "SAMPLE 1 FREQ_MHZ 300 ER 3 SIGMA .02",
+        "SAMPLE 1 FREQ_MHZ 340 ER 2 SIGMA .03",
+        "REGION 1 MATERIAL 1",
+        "BOX 1 %r %r %r %r %r %r" % (0.1 * lam, -0.1 * lam, -0.1 * lam, 0.3 * lam, 0.1 * lam, 0.1 * lam),
+        "MESH MAX_KH 0.3 MAX_CELLS 4096",
+        "END", ""])
+    os.makedirs(directory, exist_ok=True)
+    with open(os.path.join(directory, "cube_table.diel"), "w") as f:
+        f.write(diel)
+    path = os.path.join(directory, "dipole_cube_sweep.nec")
+    with open(path, "w") as f:
+        f.write(deck)
+    return path
+
+
 def dipole_array(directory, rows=8, cols=8, segments=31, seed=1, freq_mhz=300.0, pattern=True):
     """rows x cols parallel z-directed half-wave dipoles at 0.5 lambda pitch in
     the xy plane, radius lambda/1000, free space.  Element (3, 3) (the last
@@ -121,22 +159,27 @@ def run(binary, deck, args, timeout=900):
         return json.load(f), wall, p.stderr
 
 
-def execution(doc):
-    return doc["jobs"][0]["executions"][0]
+def executions(doc):
+    return doc["jobs"][0]["executions"]
 
 
-def feed_impedance(doc):
-    z = execution(doc)["feeds"][0]["impedance_ohm"]
+def execution(doc, index=0):
+    return executions(doc)[index]
+
+
+def feed_impedance(doc, index=0):
+    z = execution(doc, index)["feeds"][0]["impedance_ohm"]
     return complex(z["re"], z["im"])
 
 
-def wire_currents(doc):
-    return np.array([complex(w["current_a"]["re"], w["current_a"]["im"]) for w in execution(doc)["wire_currents"]])
+def wire_currents(doc, index=0):
+    return np.array([complex(w["current_a"]["re"], w["current_a"]["im"])
+                     for w in execution(doc, index)["wire_currents"]])
 
 
-def volume_currents(doc):
-    vc = execution(doc)["volume_currents"]
-    if not vc["rows"]:
+def volume_currents(doc, index=0):
+    vc = execution(doc, index)["volume_currents"]
+    if not vc or not vc["rows"]:
         return np.zeros(0, dtype=np.complex128)
     cols = vc["columns"]
     idx = [cols.index(n) for n in ("jx_re_a_per_m2", "jx_im_a_per_m2", "jy_re_a_per_m2", "jy_im_a_per_m2",
