@@ -36,23 +36,65 @@ __device__ __forceinline__ void bitrev_perm(C (&a)[R]) {
   }
 }
 
+// v * W_SPAN^k (W_SPAN = exp(-2 pi i / SPAN); conjugated when INV) for the
+// butterflies of spans up to 16, whose roots are the constants below (cos and
+// sin of multiples of pi/8), so a register DFT of up to 16 points reads no
+// twiddle table: the quarter-turn factors become swaps, the others one
+// complex multiply by a literal.  Larger spans read the table (root
+// tw[k * (R / SPAN) * STRIDE]).
+template <int SPAN, int K, bool INV, typename C>
+__device__ __forceinline__ C root_mul(C v) {
+  using R = decltype(v.x);
+  constexpr double c8 = 0.92387953251128674, s8 = 0.38268343236508977, h = 0.70710678118654752;
+  // Angle index on the 16-point circle: W_SPAN^K = W_16^(K * 16 / SPAN).
+  constexpr int m = K * (16 / SPAN);
+  C r;
+  if constexpr (m == 4) {                        // -i (forward) / +i (inverse)
+    if (INV) { r.x = -v.y; r.y = v.x; } else { r.x = v.y; r.y = -v.x; }
+    return r;
+  } else {
+    constexpr double wr = m == 1 ? c8 : m == 2 ? h : m == 3 ? s8 : m == 5 ? -s8 : m == 6 ? -h : -c8;
+    constexpr double wi = m == 1 ? -s8 : m == 2 ? -h : m == 3 ? -c8 : m == 5 ? -c8 : m == 6 ? -h : -s8;
+    C w;
+    w.x = (R)wr;
+    w.y = INV ? (R)-wi : (R)wi;
+    return cmul(v, w);
+  }
+}
+
+template <int SPAN, int K, bool INV, typename C>
+__device__ __forceinline__ void span_butterflies(C *a, int base) {
+  if constexpr (K < SPAN / 2) {
+    C u = a[base + K], v = a[base + K + SPAN / 2];
+    if constexpr (K != 0) v = root_mul<SPAN, K, INV>(v);
+    a[base + K] = cadd(u, v);
+    a[base + K + SPAN / 2] = csub(u, v);
+    span_butterflies<SPAN, K + 1, INV>(a, base);
+  }
+}
+
 // Butterflies of one radix-2 stage (span SPAN) and, recursively, the rest.
 template <int R, bool INV, int STRIDE, int SPAN, typename C>
 __device__ __forceinline__ void dit_stages(C (&a)[R], const C *__restrict__ tw) {
   if constexpr (SPAN <= R) {
     constexpr int HALF = SPAN / 2;
+    if constexpr (SPAN <= 16) {
 #pragma unroll
-    for (int base = 0; base < R; base += SPAN) {
+      for (int base = 0; base < R; base += SPAN) span_butterflies<SPAN, 0, INV>(a, base);
+    } else {
 #pragma unroll
-      for (int k = 0; k < HALF; ++k) {
-        C u = a[base + k], v = a[base + k + HALF];
-        if (k != 0) {
-          C w = __ldg(&tw[k * (R / SPAN) * STRIDE]);
-          if (INV) w.y = -w.y;
-          v = cmul(v, w);
+      for (int base = 0; base < R; base += SPAN) {
+#pragma unroll
+        for (int k = 0; k < HALF; ++k) {
+          C u = a[base + k], v = a[base + k + HALF];
+          if (k != 0) {
+            C w = __ldg(&tw[k * (R / SPAN) * STRIDE]);
+            if (INV) w.y = -w.y;
+            v = cmul(v, w);
+          }
+          a[base + k] = cadd(u, v);
+          a[base + k + HALF] = csub(u, v);
         }
-        a[base + k] = cadd(u, v);
-        a[base + k + HALF] = csub(u, v);
       }
     }
     dit_stages<R, INV, STRIDE, SPAN * 2>(a, tw);
@@ -389,7 +431,7 @@ __device__ __forceinline__ void fft_product_tile(const PassArgs<C> &a, long long
 // Three CTAs per SM in FP32; two in FP64, whose three components of R2
 // complex values per thread would otherwise spill.
 template <typename C, int R1, int R2>
-__global__ void __launch_bounds__(256, sizeof(C) == sizeof(float2) ? 3 : 2) fft_product_pass(PassArgs<C> a) {
+__global__ void __launch_bounds__(256, 2) fft_product_pass(PassArgs<C> a) {
   fft_product_tile<C, R1, R2>(a, blockIdx.x);
 }
 
