@@ -228,8 +228,26 @@ def cpu_baseline(w, full_iterations):
     return {"value": 1.0 / (per_iter * full_iterations), "unit": "solves/s", "cores": cpu_threads(),
             "kind": "reference",
             "sample": "reference vie_gmres (builtin FFT, OpenMP) for %d iterations (%.2f s incl. the "
-                      "initial true residual), scaled to the %d iterations of a full solve"
-                      % (rep.iterations, t, full_iterations)}
+                      "initial true residual), scaled to the %d iterations of a full solve (the reference's "
+                      "own full solve takes the same count: tests/golden/c2_reference_solve.json)"
+                      % (rep.iterations, t, full_iterations),
+            "c0_deck": reference_c0_deck()}
+
+
+def reference_c0_deck():
+    """The stock reference program (oracle/_ref/nec2c) on BASELINE config 0
+    end to end, -s fft -r 1e-6, all host threads: the time the drop-in
+    program's deck_c0_dropin line compares with."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import tempfile
+    import decks
+    if not os.path.exists(decks.REF_BIN):
+        return None
+    deck = decks.dipole_cube(tempfile.mkdtemp())
+    doc, wall, _ = decks.run(decks.REF_BIN, deck, ["-s", "fft", "-r", "1e-6", "--jobs", "1"])
+    z = decks.feed_impedance(doc)
+    return {"wall_s": wall, "threads": os.cpu_count(), "zin_ohm": [z.real, z.imag],
+            "iterations": decks.execution(doc)["solver"]["iterations"]}
 
 
 def run_reference(args, rank, world):
@@ -529,6 +547,8 @@ def run_ours(args, rank, world, local_rank):
     volume_batch = volume_batch_bench(nb, torch, stream)
     # Mixed dense and volume serving stream (bounded), both forms.
     serving = serving_bench(nb, torch) if world == 1 else None
+    # Config 0 end to end through the drop-in program (rank 0 only).
+    deck_c0 = deck_bench() if rank == 0 else None
     lib.nec2c_cuda_set_stream(C.c_void_p(stream.cuda_stream))
 
     if rank != 0:
@@ -561,6 +581,7 @@ def run_ours(args, rank, world, local_rank):
         "batched_wire_blocks_c3": batched,
         "batched_volume_c3": volume_batch,
         "serving_c4": serving,
+        "deck_c0_dropin": deck_c0,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }
@@ -680,6 +701,48 @@ def lu_driver(args, nb, torch, stream):
                       "device_factor_ms": {f: t[0] for f, t in out.items()},
                       "device_solve_ms": {f: t[1] for f, t in out.items()}}))
     return 0
+
+
+def deck_bench():
+    """BASELINE config 0 end to end through the drop-in program (nec2c with
+    the CUDA backend bound in, nec2c_b200/binding/_build/nec2c_cuda): the
+    21-segment dipole beside the 16^3 dielectric cube at 300 MHz, FFT-GMRES to
+    -r 1e-6, once with --fft-backend cuda (plain FP64) and once with
+    cuda-mixed (FP32 transforms).  Reports the wall time and the program's own
+    phase timings, and the mixed form's errors against the FP64 form: feed
+    impedance, segment and voxel currents (relative L2) and far-field gain
+    (dB, directions within 30 dB of the peak).  Host work: the matrix fill
+    and the wire-volume coupling stay on the CPU as in the reference."""
+    import tempfile
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import decks
+    if not os.path.exists(decks.CUDA_BIN):
+        return {"unavailable": "drop-in program not built (make -C oracle binding)"}
+    out = {"workload": "c0: 21-segment half-wave dipole 0.1 lambda from a 0.2 lambda cube (16^3 cells, "
+                       "eps_r 4 - 0.1j), 300 MHz, -s fft -r 1e-6", "threads": os.cpu_count()}
+    d = tempfile.mkdtemp()
+    deck = decks.dipole_cube(d)
+    docs = {}
+    for name in ("cuda", "cuda-mixed"):
+        timing = os.path.join(d, name + ".timing.json")
+        doc, wall, _ = decks.run(decks.CUDA_BIN, deck, ["-s", "fft", "-r", "1e-6", "--jobs", "1",
+                                                        "--fft-backend", name, "--timing-json", timing])
+        with open(timing) as f:
+            phases = {p["name"]: p["seconds"] for p in json.load(f)["phases"]}
+        e = decks.execution(doc)
+        z = decks.feed_impedance(doc)
+        docs[name] = doc
+        out[name] = {"wall_s": wall, "phases_s": phases, "zin_ohm": [z.real, z.imag],
+                     "iterations": e["solver"]["iterations"], "true_residual": e["solver"]["true_residual"]}
+    a, b = docs["cuda-mixed"], docs["cuda"]
+    za, zb = decks.feed_impedance(a), decks.feed_impedance(b)
+    wa, wb = decks.wire_currents(a), decks.wire_currents(b)
+    va, vb = decks.volume_currents(a), decks.volume_currents(b)
+    out["mixed_vs_fp64"] = {"zin_rel_err": abs(za - zb) / abs(zb),
+                            "wire_current_rel_l2": float(np.linalg.norm(wa - wb) / np.linalg.norm(wb)),
+                            "voxel_current_rel_l2": float(np.linalg.norm(va - vb) / np.linalg.norm(vb)),
+                            "gain_db_max_abs": decks.gain_difference_db(a, b)}
+    return out
 
 
 def dense_bench(nb, torch, stream):

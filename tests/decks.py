@@ -1,7 +1,8 @@
 """Seeded NEC decks of the dipole-plus-cube and dipole-array workloads, for
 the deck-level parity tests: the stock reference program (oracle/_ref/nec2c)
-and the same program with the CUDA backend bound in (oracle/_ref/nec2c_cuda)
-run the same deck, and their result JSON documents are compared.
+and the same program with the CUDA backend bound in
+(nec2c_b200/binding/_build/nec2c_cuda) run the same deck, and their result
+JSON documents are compared.
 
 Coordinates are written with full double precision (repr): the reference's
 FFT lattice inference accepts cubes equal to 1e-10 only
@@ -16,7 +17,7 @@ C0 = 299792458.0
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "nec2c")
-CUDA_BIN = os.path.join(ROOT, "oracle", "_ref", "nec2c_cuda")
+CUDA_BIN = os.path.join(ROOT, "nec2c_b200", "binding", "_build", "nec2c_cuda")
 
 # Far-field request of both decks: theta 0..180 and phi 0..350 in 10-degree
 # steps, power gain (RP card, XNDA = 1000).
@@ -104,6 +105,53 @@ def dipole_cube_sweep(directory, freqs_mhz=(280.0, 300.0, 320.0)):
     with open(path, "w") as f:
         f.write(deck)
     return path
+
+
+def plane_wave_cube(directory, side_cells, freq_mhz=300.0, eps=(4.0, 0.1)):
+    """A dielectric cube of side 0.2 lambda (ER 4, EI 0.1) meshed side_cells per
+    side, alone in free space, lit by an x-polarised plane wave travelling
+    along z (EX 1; the volume-only solver, dielectric_solver.c:315).  Returns
+    the deck path."""
+    lam = C0 / (freq_mhz * 1e6)
+    q = 4.0 * np.pi * 0.2 * np.sqrt(abs(complex(eps[0], -eps[1]))) / (2 * side_cells)
+    deck = "\n".join([
+        "CM dielectric cube in a plane wave",
+        "CE",
+        "GE",
+        "FR 0 1 0 0 %r 0" % freq_mhz,
+        "EX 1 1 1 0 0 0 0 0 0 0",
+        'DF "pw.diel"',
+        "XQ",
+        "EN", ""])
+    diel = "\n".join([
+        "NEC2C-DIELECTRIC 2",
+        "MATERIAL 1 ER %r EI %r" % eps,
+        "REGION 1 MATERIAL 1",
+        "BOX 1 %r %r %r %r %r %r" % (-0.1 * lam, -0.1 * lam, -0.1 * lam, 0.1 * lam, 0.1 * lam, 0.1 * lam),
+        "MESH MAX_KH %r MAX_ASPECT 1 MAX_CELLS %d" % (float(q * (1.0 + 1e-6)), side_cells ** 3),
+        "END", ""])
+    os.makedirs(directory, exist_ok=True)
+    with open(os.path.join(directory, "pw.diel"), "w") as f:
+        f.write(diel)
+    path = os.path.join(directory, "plane_wave_cube.nec")
+    with open(path, "w") as f:
+        f.write(deck)
+    return path
+
+
+def run_status(binary, deck, args, timeout=900):
+    """Runs a nec2c program on a deck; returns (exit code, result JSON or None,
+    printed output)."""
+    base = os.path.splitext(deck)[0] + "_" + os.path.basename(binary)
+    out, res = base + ".out", base + ".json"
+    p = subprocess.run([binary, "-i", deck, "-o", out, "--result-json", res] + list(args),
+                       capture_output=True, text=True, timeout=timeout, cwd=os.path.dirname(deck))
+    doc = None
+    if os.path.exists(res):
+        with open(res) as f:
+            doc = json.load(f)
+    text = open(out).read() if os.path.exists(out) else ""
+    return p.returncode, doc, text + p.stderr
 
 
 def dipole_array(directory, rows=8, cols=8, segments=31, seed=1, freq_mhz=300.0, pattern=True):

@@ -1,5 +1,5 @@
 """The reference-side binding on the CPU (no GPU needed): the program with the
-CUDA backend bound in (oracle/_ref/nec2c_cuda) behaves exactly like the stock
+CUDA backend bound in (nec2c_b200/binding/_build/nec2c_cuda) behaves exactly like the stock
 reference program when the builtin backends are selected, since every
 wrapped entry point forwards to the reference's own; and selecting a CUDA
 backend where no usable device exists fails loudly at the command line
