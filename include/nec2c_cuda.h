@@ -307,6 +307,47 @@ int nec2c_cuda_dense_last_refinement(void);
 int nec2c_cuda_dense_factor_device_static(size_t order, nec2c_cuda_complex *matrix_dev,
                                           size_t leading_dimension, int *pivots_dev);
 
+/* ------------------------------------------- wire <-> volume coupling */
+/* The wires of a NEC model as NEC holds them while a hybrid system is
+   assembled (dielectric_wire.c: geometry scaled to wavelengths): segment
+   centres, lengths and radii in wavelengths, direction cosines, the
+   wavelength in metres, NEC's lumped-element distance rkh (wavelengths, the
+   RK card, 1 by default) and whether a perfectly conducting ground plane
+   (GN 1) mirrors every segment. */
+typedef struct {
+  size_t segments;
+  const double *x, *y, *z;
+  const double *length, *radius;
+  const double *cab, *sab, *salp;
+  double wavelength;
+  double rkh;
+  int pec_ground;
+} nec2c_cuda_wire_model;
+/* Replaces dw_assemble_wire_to_volume (dielectric_wire.c:396-510) for the
+   NEC-2 wire engine with the classic thin-wire kernel, in free space or over
+   a perfect ground: for each of columns conductor unknowns, whose basis
+   currents sources holds (per segment the constant, sine and cosine
+   coefficients cabc gives for a unit vector, dw_prepare_conductor_sources),
+   the NEC field (nefld/efld, fields.c:38-253, 1123-1380) averaged over each
+   cell by a 6-point Gauss rule per axis, times -i omega eps0 chi[cell].
+   centers and sizes hold 3 doubles per cell (m); out receives columns rows
+   of 3 x cells values (row column, entry 3 cell + component).  Returns 1, or
+   0 with the reason in nec2c_cuda_last_error(). */
+int nec2c_cuda_coupling_wire_to_volume(const nec2c_cuda_wire_model *wires, size_t columns,
+                                       const nec2c_cuda_complex *sources, size_t cells,
+                                       const double *centers, const double *sizes,
+                                       const nec2c_cuda_complex *chi, double omega, nec2c_cuda_complex *out);
+/* Replaces the wire-row loop of dielectric_solve_conductor_coupled
+   (dielectric_wire.c:1164-1213) in free space or over a perfect ground: the
+   point-tested N dyad of each cell (dw_point_cuboid_n, dielectric_wire.c:
+   101-138, 193-201; 10-point Gauss rule per axis) at each segment centre
+   (centers_m, metres), projected on the segment direction (tangents) and
+   divided by i omega eps0.  out receives segments rows of 3 x cells values.
+   Returns 1, or 0 with the reason set. */
+int nec2c_cuda_coupling_volume_to_wire(size_t segments, const double *centers_m, const double *tangents,
+                                       size_t cells, const double *cell_centers, const double *cell_sizes,
+                                       double k0, double omega, int pec_ground, nec2c_cuda_complex *out);
+
 /* ------------------------------------------------------- request server */
 /* No single counterpart in the reference: replaces the fork()ed frequency
    workers (main.c:586-760) and their memory-capped job count

@@ -21,6 +21,11 @@
  *                                              -> nec2c_cuda_gmres_plan / _hybrid
  *   concurrency.c concurrency_plan_for         -> one frequency job at a time
  *
+ * The two wire <-> volume coupling blocks of dielectric_wire.c are computed
+ * by static code the wrapping cannot reach; the drop-in program compiles a
+ * copy of that file with three insertions (patch_dielectric_wire.py) that
+ * call nec2c_binding_wire_to_volume and nec2c_binding_volume_to_wire below.
+ *
  * The certified near-pair Green tensor stays on the CPU: the CUDA plan calls
  * back into the reference's vie_cuboid_n with the options vie_fft.c:344 uses.
  * A GPU solve runs in the nec2c process itself; the reference's forked
@@ -36,9 +41,11 @@
 #include "concurrency.h"
 #include "dense_backend.h"
 #include "dielectric_fft.h"
+#include "shared.h"
 #include "vie_fft.h"
 #include "vie_iterative.h"
 #include "vie_kernel.h"
+#include "wire_operator.h"
 
 #include "nec2c_cuda.h"
 
@@ -404,7 +411,11 @@ void __wrap_dielectric_fft_get_operator(dielectric_fft_system *s, vie_linear_ope
     report_failure("hybrid system");
     b->hybrid = NULL;
   }
-  if(b->hybrid && b->conductors && !nec2c_cuda_hybrid_set_blocks(b->hybrid, dielectric_fft_entry(s, 0, 0))) {
+  /* Uploaded with no conductors too: the upload also sets the
+     preconditioner's volume divisor. */
+  static const complex double no_blocks = 0;
+  if(b->hybrid && !nec2c_cuda_hybrid_set_blocks(b->hybrid, b->conductors ? dielectric_fft_entry(s, 0, 0)
+                                                                         : &no_blocks)) {
     report_failure("hybrid block upload");
     nec2c_cuda_hybrid_destroy(b->hybrid);
     b->hybrid = NULL;
@@ -432,15 +443,26 @@ int __real_vie_gmres(const vie_linear_operator *op, const complex double *rhs, c
 
 /* vie_iterative.c:80-199: device-resident when the operator is one of the
    CUDA callbacks (options and report have the same layout as the library's). */
+static int device_gmres_done(int converged, const vie_gmres_report *report)
+{
+  /* A failure on the device side (not the iteration itself) says why. */
+  if(!converged && report &&
+     (report->status == VIE_ITERATIVE_CALLBACK_FAILED || report->status == VIE_ITERATIVE_INVALID_INPUT ||
+      report->status == VIE_ITERATIVE_ALLOCATION_FAILED))
+    report_failure("GMRES");
+  return converged;
+}
+
 int __wrap_vie_gmres(const vie_linear_operator *op, const complex double *rhs, complex double *x,
                      const vie_gmres_options *options, vie_gmres_report *report)
 {
   if(op && op->apply == nec2c_cuda_hybrid_apply)
-    return nec2c_cuda_gmres_hybrid(op->context, rhs, x, (const nec2c_cuda_gmres_options *)options,
-                                   (nec2c_cuda_gmres_report *)report);
+    return device_gmres_done(nec2c_cuda_gmres_hybrid(op->context, rhs, x,
+                                                     (const nec2c_cuda_gmres_options *)options,
+                                                     (nec2c_cuda_gmres_report *)report), report);
   if(op && op->apply == nec2c_cuda_vie_fft_apply)
-    return nec2c_cuda_gmres_plan(op->context, rhs, x, (const nec2c_cuda_gmres_options *)options,
-                                 (nec2c_cuda_gmres_report *)report);
+    return device_gmres_done(nec2c_cuda_gmres_plan(op->context, rhs, x, (const nec2c_cuda_gmres_options *)options,
+                                                   (nec2c_cuda_gmres_report *)report), report);
   return __real_vie_gmres(op, rhs, x, options, report);
 }
 
@@ -460,3 +482,92 @@ concurrency_plan __wrap_concurrency_plan_for(size_t frequency_count, size_t esti
 /* Layout agreement the casts in __wrap_vie_gmres rely on. */
 _Static_assert(sizeof(vie_gmres_options) == sizeof(nec2c_cuda_gmres_options), "options layout");
 _Static_assert(sizeof(vie_gmres_report) == sizeof(nec2c_cuda_gmres_report), "report layout");
+
+/* ------------------------------------------- wire <-> volume coupling */
+static int coupling_ground_ok(void)
+{
+  return !wire_operator_ground_direct_only() && (gnd.ksymp == 1 || (gnd.ksymp == 2 && gnd.iperf == 1));
+}
+
+static int cell_arrays(const dielectric_mesh_result *mesh, double **centers, double **sizes)
+{
+  size_t c;
+  int d;
+  *centers = malloc(3 * mesh->cell_count * sizeof(double));
+  *sizes = malloc(3 * mesh->cell_count * sizeof(double));
+  if(!*centers || !*sizes) { free(*centers); free(*sizes); return 0; }
+  for(c = 0; c < mesh->cell_count; ++c)
+    for(d = 0; d < 3; ++d) {
+      (*centers)[3 * c + d] = mesh->cells[c].center[d];
+      (*sizes)[3 * c + d] = mesh->cells[c].size[d];
+    }
+  return 1;
+}
+
+/* dielectric_wire.c:422-510 on the GPU: 1 handled (result allocated with
+   calloc, as the reference's serial path allocates it), 0 not a model the
+   kernels cover (the reference's own assembly runs), -1 failed.  Covered:
+   a CUDA backend selected, wires only, the NEC-2 wire engine with the
+   classic thin-wire kernel, free space or a perfect ground. */
+int nec2c_binding_wire_to_volume(const dielectric_mesh_result *mesh, size_t nw, size_t np,
+    size_t conductor_unknowns, const complex double *sources,
+    const complex double *wire_background_basis, const complex double *volume_chi,
+    double k0, double omega, complex double **result, int *result_mapped,
+    size_t *workers_used, int *fell_back)
+{
+  nec2c_cuda_wire_model w;
+  double *centers = NULL, *sizes = NULL;
+  complex double *out;
+  (void)k0;
+  if(!(g_dense_cuda || g_fft_cuda) || np || wire_background_basis || wire_operator_nec4_basis() ||
+     dataj.iexk != 0 || !coupling_ground_ok() || conductor_unknowns != nw || nw != (size_t)data.n)
+    return 0;
+  if(!mesh->cell_count || !conductor_unknowns) return 0;
+  out = calloc(conductor_unknowns * 3 * mesh->cell_count, sizeof(*out));
+  if(!out || !cell_arrays(mesh, &centers, &sizes)) { free(out); return -1; }
+  w.segments = nw;
+  w.x = data.x; w.y = data.y; w.z = data.z; w.length = data.si; w.radius = data.bi;
+  w.cab = data.cab; w.sab = data.sab; w.salp = data.salp;
+  w.wavelength = data.wlam; w.rkh = dataj.rkh; w.pec_ground = gnd.ksymp == 2;
+  if(!nec2c_cuda_coupling_wire_to_volume(&w, conductor_unknowns, sources, mesh->cell_count, centers, sizes,
+                                         volume_chi, omega, out)) {
+    report_failure("wire-to-volume coupling");
+    free(out); free(centers); free(sizes);
+    return -1;
+  }
+  free(centers); free(sizes);
+  *result = out;
+  *result_mapped = 0;
+  *workers_used = 1;
+  *fell_back = 0;
+  return 1;
+}
+
+/* The wire rows of dielectric_wire.c:1164-1213 on the GPU: nw rows of 3 x
+   cells values (malloc), or NULL when the model is not covered (a ground
+   other than free space or a perfect ground) or the computation failed (the
+   reference's loop then runs). */
+complex double *nec2c_binding_volume_to_wire(const dielectric_mesh_result *mesh, size_t nw,
+    const double *x, const double *y, const double *z, double k0, double omega)
+{
+  double *centers = NULL, *sizes = NULL, *obs, *tangent;
+  complex double *out;
+  size_t i;
+  if(!(g_dense_cuda || g_fft_cuda) || !coupling_ground_ok() || !nw || !mesh->cell_count) return NULL;
+  obs = malloc(6 * nw * sizeof(double));
+  out = malloc(nw * 3 * mesh->cell_count * sizeof(*out));
+  if(!obs || !out || !cell_arrays(mesh, &centers, &sizes)) { free(obs); free(out); return NULL; }
+  tangent = obs + 3 * nw;
+  for(i = 0; i < nw; ++i) {
+    obs[3 * i] = x[i]; obs[3 * i + 1] = y[i]; obs[3 * i + 2] = z[i];
+    tangent[3 * i] = data.cab[i]; tangent[3 * i + 1] = data.sab[i]; tangent[3 * i + 2] = data.salp[i];
+  }
+  if(!nec2c_cuda_coupling_volume_to_wire(nw, obs, tangent, mesh->cell_count, centers, sizes, k0, omega,
+                                         gnd.ksymp == 2, out)) {
+    report_failure("volume-to-wire coupling");
+    free(out);
+    out = NULL;
+  }
+  free(obs); free(centers); free(sizes);
+  return out;
+}

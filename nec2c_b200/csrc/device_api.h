@@ -214,6 +214,24 @@ size_t n2d_lu_batched_descriptor_bytes(long long count);
 int n2d_transpose(const double *src_dev, long long lds, double *dst_dev, long long ldd,
                   long long rows, long long cols);
 
+/* ---- wire <-> volume coupling blocks (dielectric_wire.c) ---- */
+/* seg_dev: 8 doubles per segment (x y z length radius cab sab salp, lengths
+   in wavelengths); sources_dev: per column, per segment the constant, sine
+   and cosine current coefficients (complex); centers/sizes: 3 doubles per
+   cell (m); chi_dev: eps_r - 1 per cell (complex); node/weight: the 6-point
+   Gauss rule on [-1, 1].  out_dev: columns x 3 cells complex. */
+int n2d_coupling_wire_to_volume(const double *seg_dev, int nseg, double rkh, int image, double wlam,
+                                const double *sources_dev, int columns, const double *center_dev,
+                                const double *size_dev, const double *chi_dev, long long cells,
+                                double omega_eps0, const double *node_dev, const double *weight_dev,
+                                double *out_dev);
+/* obs/tangent: 3 doubles per segment (m); node/weight: the 10-point Gauss
+   rule.  out_dev: segments x 3 cells complex. */
+int n2d_coupling_volume_to_wire(const double *obs_dev, const double *tangent_dev, int nseg,
+                                const double *center_dev, const double *size_dev, long long cells,
+                                double k0, double omega_eps0, int image, const double *node_dev,
+                                const double *weight_dev, double *out_dev);
+
 #ifdef __cplusplus
 }
 #endif
