@@ -56,11 +56,12 @@ def parse():
     ap.add_argument("--planes", type=int, choices=[0, 1], default=None,
                     help="profiling driver: pin the fused yz-plane passes on (1) or off (0) in both "
                          "c2 plans instead of the tuner's choice")
-    ap.add_argument("--only", choices=["matvec", "solve", "lu", "serving", "volume_batch"],
+    ap.add_argument("--only", choices=["matvec", "solve", "lu", "serving", "volume_batch", "coupling"],
                     help="profiling driver: build the plans, run --steps FP32 and FP64 products "
                          "(matvec) or --steps mixed solves (solve), or factor the 1984-unknown dense "
                          "matrix --steps times in each LU form (lu), run the serving stream "
-                         "(serving) or the 192-system dipole-plus-cube batch (volume_batch); print "
+                         "(serving), the 192-system dipole-plus-cube batch (volume_batch) or the wire-volume "
+                         "coupling blocks of the dipole-plus-cube model --steps times (coupling); print "
                          "timings and exit")
     return ap.parse_args()
 
@@ -398,6 +399,9 @@ def run_ours(args, rank, world, local_rank):
     if args.only == "serving":
         print(json.dumps({"profile": "serving", "serving_c4": serving_bench(nb, torch)}))
         return 0
+    if args.only == "coupling":
+        print(json.dumps({"profile": "coupling", "coupling_c0": coupling_bench(nb, args.steps)}))
+        return 0
     if args.only == "volume_batch":
         print(json.dumps({"profile": "volume_batch", "batched_volume_c3": volume_batch_bench(nb, torch, stream)}))
         return 0
@@ -547,8 +551,10 @@ def run_ours(args, rank, world, local_rank):
     volume_batch = volume_batch_bench(nb, torch, stream)
     # Mixed dense and volume serving stream (bounded), both forms.
     serving = serving_bench(nb, torch) if world == 1 else None
-    # Config 0 end to end through the drop-in program (rank 0 only).
+    # Config 0 end to end through the drop-in program, and its two coupling
+    # blocks through the C ABI (rank 0 only).
     deck_c0 = deck_bench() if rank == 0 else None
+    coupling = coupling_bench(nb, 10) if rank == 0 else None
     lib.nec2c_cuda_set_stream(C.c_void_p(stream.cuda_stream))
 
     if rank != 0:
@@ -582,6 +588,7 @@ def run_ours(args, rank, world, local_rank):
         "batched_volume_c3": volume_batch,
         "serving_c4": serving,
         "deck_c0_dropin": deck_c0,
+        "coupling_c0": coupling,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }
@@ -743,6 +750,67 @@ def deck_bench():
                             "voxel_current_rel_l2": float(np.linalg.norm(va - vb) / np.linalg.norm(vb)),
                             "gain_db_max_abs": decks.gain_difference_db(a, b)}
     return out
+
+
+class WireModel(C.Structure):
+    """nec2c_cuda_wire_model (include/nec2c_cuda.h)."""
+    _fields_ = [("segments", C.c_size_t), ("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p),
+                ("length", C.c_void_p), ("radius", C.c_void_p), ("cab", C.c_void_p), ("sab", C.c_void_p),
+                ("salp", C.c_void_p), ("wavelength", C.c_double), ("rkh", C.c_double), ("pec_ground", C.c_int)]
+
+
+def coupling_bench(nb, reps):
+    """The two wire-volume coupling blocks of the dipole-plus-cube model
+    (21 segments, 16^3 cells, 21 conductor unknowns whose
+    basis spreads over three segments each, seeded coefficients) through the
+    C ABI, reps times after one untimed call; host wall time per call
+    (uploads, kernels, download)."""
+    lam = C0 / 300e6
+    n = 21
+    seg = np.zeros((n, 8))
+    for i in range(n):
+        seg[i] = [0.0, 0.0, -0.25 + (i + 0.5) * 0.5 / n, 0.5 / n, 0.001 / lam, 0.0, 0.0, 1.0]
+    h = 0.2 * lam / 16
+    g = (np.arange(16) + 0.5) * h
+    X, Y, Z = np.meshgrid(0.1 * lam + g, -0.1 * lam + g, -0.1 * lam + g, indexing="ij")
+    centers = np.ascontiguousarray(np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1))
+    sizes = np.full_like(centers, h)
+    cells = len(centers)
+    rng = np.random.default_rng(1)
+    src = np.zeros((n, n, 3), dtype=np.complex128)
+    for j in range(n):
+        for s in range(max(0, j - 1), min(n, j + 2)):
+            src[j, s] = rng.standard_normal(3) + 1j * rng.standard_normal(3)
+    chi = np.full(cells, 3.0 - 0.1j)
+    lib = nb.load()
+    vp = C.c_void_p
+    lib.nec2c_cuda_coupling_wire_to_volume.argtypes = [vp, C.c_size_t, vp, C.c_size_t, vp, vp, vp, C.c_double, vp]
+    lib.nec2c_cuda_coupling_volume_to_wire.argtypes = [C.c_size_t, vp, vp, C.c_size_t, vp, vp, C.c_double,
+                                                       C.c_double, C.c_int, vp]
+    cols = [np.ascontiguousarray(seg[:, k]) for k in range(8)]
+    w = WireModel(n, *[c.ctypes.data for c in cols], lam, 1.0, 0)
+    w2v = np.zeros((n, 3 * cells), dtype=np.complex128)
+    v2w = np.zeros((n, 3 * cells), dtype=np.complex128)
+    obs = np.ascontiguousarray(seg[:, :3] * lam)
+    tan = np.ascontiguousarray(seg[:, 5:8])
+    k0, om = 2 * math.pi / lam, 2 * math.pi * 300e6
+    t_w2v, t_v2w = [], []
+    for rep in range(reps + 1):
+        t0 = time.perf_counter()
+        if not lib.nec2c_cuda_coupling_wire_to_volume(C.byref(w), n, src.ctypes.data, cells, centers.ctypes.data,
+                                                      sizes.ctypes.data, chi.ctypes.data, om, w2v.ctypes.data):
+            raise RuntimeError(nb.last_error())
+        t1 = time.perf_counter()
+        if not lib.nec2c_cuda_coupling_volume_to_wire(n, obs.ctypes.data, tan.ctypes.data, cells,
+                                                      centers.ctypes.data, sizes.ctypes.data, k0, om, 0,
+                                                      v2w.ctypes.data):
+            raise RuntimeError(nb.last_error())
+        t2 = time.perf_counter()
+        if rep:
+            t_w2v.append(t1 - t0)
+            t_v2w.append(t2 - t1)
+    return {"segments": n, "cells": cells, "unknowns": n, "wire_to_volume_ms": 1e3 * statistics.median(t_w2v),
+            "volume_to_wire_ms": 1e3 * statistics.median(t_v2w)}
 
 
 def dense_bench(nb, torch, stream):
