@@ -53,10 +53,13 @@ def parse():
                     help="JSON file of the c2 plans' FFT pass schedules: written by the first run "
                          "that names it, pinned by later runs (a run under ncu would otherwise "
                          "tune on serialised, slowed launches)")
+    ap.add_argument("--requests", type=int, default=240,
+                    help="serving_c4 profiling mode: requests in the stream (config 4 names 10,000)")
     ap.add_argument("--planes", type=int, choices=[0, 1], default=None,
                     help="profiling driver: pin the fused yz-plane passes on (1) or off (0) in both "
                          "c2 plans instead of the tuner's choice")
-    ap.add_argument("--only", choices=["matvec", "solve", "lu", "serving", "volume_batch", "coupling"],
+    ap.add_argument("--only", choices=["matvec", "solve", "lu", "serving", "serving_c4", "volume_batch",
+                                       "coupling"],
                     help="profiling driver: build the plans, run --steps FP32 and FP64 products "
                          "(matvec) or --steps mixed solves (solve), or factor the 1984-unknown dense "
                          "matrix --steps times in each LU form (lu), run the serving stream "
@@ -399,6 +402,9 @@ def run_ours(args, rank, world, local_rank):
     if args.only == "serving":
         print(json.dumps({"profile": "serving", "serving_c4": serving_bench(nb, torch)}))
         return 0
+    if args.only == "serving_c4":
+        print(json.dumps({"profile": "serving_c4", "serving_c4_stream": serving_stream_c4(nb, torch, args.requests)}))
+        return 0
     if args.only == "coupling":
         print(json.dumps({"profile": "coupling", "coupling_c0": coupling_bench(nb, args.steps)}))
         return 0
@@ -629,7 +635,24 @@ def profile_driver(args, lib, nb, torch, stream, plan_m, plan_d, w):
                 raise RuntimeError(nb.last_error())
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
-    print(json.dumps({"profile": args.only, "steps": args.steps, "s": time.perf_counter() - t0,
+    elapsed = time.perf_counter() - t0
+    timed = {}
+    if args.only == "matvec":
+        # Event-timed products outside the NVTX range, L2 flushed before each.
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        for key, plan in (("fp32_us", plan_m), ("fp64_us", plan_d)):
+            out = []
+            for i in range(23):
+                flush.zero_()
+                a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a0.record(stream)
+                lib.nec2c_cuda_vie_fft_apply_device(plan.h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()))
+                a1.record(stream)
+                torch.cuda.synchronize()
+                if i >= 3:
+                    out.append(1e3 * a0.elapsed_time(a1))
+            timed[key] = statistics.median(out)
+    print(json.dumps({"profile": args.only, "steps": args.steps, "s": elapsed, "products": timed,
                       "fft_schedule": {"fp32": plan_m.schedule(fp64=False)[1],
                                        "fp64": plan_d.schedule(fp64=True)[1],
                                        "planes": [plan_m.planes(fp64=False), plan_d.planes(fp64=True)]}}))
@@ -1226,6 +1249,208 @@ def serving_bench(nb, torch):
     out["mixed_vs_fp64_solves_per_s"] = sat[True]["solves_per_s"] / sat[False]["solves_per_s"]
     out["max_rel_err_mixed_vs_fp64"] = err
     out["gpu_launches"] = int(lib.nec2c_cuda_launch_count() - l0)
+    return out
+
+
+def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0.5, 0.7, 0.9, 1.1),
+                      lattices=(8, 16, 24, 32, 48), seed=11):
+    """BASELINE config 4 shaped stream through the request server.
+
+    Requests: 60% dense MoM models (orders log-uniform in 200-3000, ten orders
+    with three seeded matrices each standing for their frequencies), 40%
+    dipole-plus-dielectric VIE models over a perfectly conducting ground plane
+    (PEC image embedding): cubes of 8^3-48^3 cells (0.2 lambda at 300 MHz,
+    eps_r ~ U[2,10], tan d 0.05) raised one cell above the plane, each beside a
+    dipole of 11-41 segments, every model resident on the device at 16
+    frequencies (280-355 MHz).  Each request asks for F in {1, 2, 4, 8, 16}
+    distinct frequencies of its model and is submitted as F solve requests
+    (one per frequency); its latency runs from the first being queued to the
+    last being done.
+
+    Forms (16 workers): `mixed` = FP32 transforms with the FP64 LU (the split
+    LU's refinement only adds latency at these orders), the server merging
+    queued volume requests on one model's frequencies into one batched solve
+    (each model's 16 frequency systems are one registered batch);
+    `mixed_unmerged` = the same without merging; `mixed_split_lu` = merged,
+    with the split-precision LU; `fp64` = FP64 transforms, merged;
+    `plain_fp64_one_at_a_time` = FP64, one worker, no merging.  Saturation:
+    everything queued at once.  Poisson: request arrivals at the given
+    fractions of the mixed form's saturated request rate (the sweep shows
+    where p99 latency diverges).  Seeded synthetic matrices, lattices and
+    wire blocks stand in for the reference's decks; the near-pair tensors
+    come from the golden table whose cell size is nearest."""
+    rng = np.random.default_rng(seed)
+    tabs = near_tables_all()
+    lam = C0 / 300e6
+    slots = 16
+
+    def pinned(arr):
+        t = torch.empty(arr.size, dtype=torch.complex128, pin_memory=True)
+        out = np.lib.stride_tricks.as_strided(t.numpy(), shape=arr.shape, strides=arr.strides)
+        out[...] = arr
+        return out, t
+
+    keep = []
+    orders = sorted(set(int(round(math.exp(v))) for v in rng.uniform(math.log(200), math.log(3000), 10)))
+    dense_pool = []
+    for i, n in enumerate(orders):
+        mats = []
+        for f in range(3):
+            r = np.random.default_rng(300 + 7 * i + f)
+            a = r.standard_normal((n, n)) + 1j * r.standard_normal((n, n))
+            a += np.diag(np.full(n, 0.5 * math.sqrt(n)))
+            st, t1 = pinned(np.asfortranarray(a.T))
+            x = r.standard_normal(n) + 1j * r.standard_normal(n)
+            rhs, t2 = pinned(np.asfortranarray((a @ x).reshape(n, 1)))
+            keep += [t1, t2]
+            mats.append((st, rhs))
+        dense_pool.append(mats)
+
+    freqs = np.linspace(280e6, 355e6, sizes_per_model)
+    specs = []
+    for m, n in enumerate(lattices):
+        r = np.random.default_rng(400 + m)
+        h = 0.2 * lam / n
+        tab = min(("c0", "c2", "c3_32"), key=lambda t: abs(tabs[t][0] - h))
+        specs.append(dict(n=int(n), c=int(r.integers(11, 42)), eps=r.uniform(2, 10) * (1 - 0.05j),
+                          tab=tab, seed=500 + m))
+
+    def build_models(mixed):
+        models = []
+        for sp in specs:
+            n, c = sp["n"], sp["c"]
+            h = 0.2 * lam / n
+            g = np.arange(n)
+            xyz = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3)
+            # PEC image embedding: physical cells one cell (two half cells)
+            # above the plane, their images below; lattice index as
+            # dielectric_fft.c:137-154 lays it out (gap of 2 half cells).
+            phys = xyz.copy()
+            phys[:, 2] += n + 2
+            img = xyz.copy()
+            img[:, 2] = n - 1 - xyz[:, 2]
+            lat = np.concatenate([phys, img]).astype(np.uintp).reshape(-1)
+            shape = (n, n, 2 * n + 2)
+            v = 3 * n ** 3
+            r = np.random.default_rng(sp["seed"])
+            cm = r.standard_normal((c, c)) + 1j * r.standard_normal((c, c))
+            cm += np.diag(np.full(c, 2.0 * math.sqrt(c)))
+            bm = 0.01 * (r.standard_normal((c, v)) + 1j * r.standard_normal((c, v)))
+            dm = 0.01 * (r.standard_normal((v, c)) + 1j * r.standard_normal((v, c)))
+            blocks = np.concatenate([np.concatenate([cm, bm], axis=1).reshape(-1), dm.reshape(-1)])
+            systems, plans, rhs = [], [], []
+            for f in freqs:
+                k = 2 * math.pi * f / C0
+                p = nb.VolumePlan(shape, lat, h, k, sp["eps"], tabs[sp["tab"]][2], mixed=mixed)
+                hs = nb.HybridSystem(p, c, v, pec=True)
+                hs.set_blocks(blocks)
+                b = np.zeros(c + v, dtype=np.complex128)
+                b[c // 2] = 1.0
+                z = xyz[:, 2].astype(np.float64)
+                b[c::3] = 2 * np.exp(-1j * k * h * (z + 0.5)) * math.sin(k * h / 2) / (k * h / 2)
+                plans.append(p)
+                systems.append(hs)
+                rhs.append(b)
+            # Every frequency of the model in one batch, registered with the
+            # server: queued requests on its systems merge into one solve.
+            models.append(dict(plans=plans, systems=systems, rhs=rhs,
+                               batch=nb.VolumeBatch(hybrids=systems)))
+        return models
+
+    nreq = requests
+    kinds = rng.random(nreq) < 0.6
+    fsel = rng.choice([1, 2, 4, 8, 16], nreq)
+    picks = rng.integers(0, 1 << 30, nreq)
+    # The frequencies each request asks for: F distinct ones of its model's 16.
+    fsets = [np.sort(rng.choice(len(freqs), int(F), replace=False)) for F in fsel]
+
+    def run(models, split, slots_, gaps, merge):
+        srv = nb.Server(slots=slots_, split=split)
+        if merge:
+            for mdl in models:
+                srv.merge(mdl["batch"])
+        # Warm every worker (stream state, kernel attributes) and every system.
+        for mdl in models:
+            for hs, b in zip(mdl["systems"], mdl["rhs"]):
+                srv.volume(hs, b, np.zeros_like(b), rtol=1e-6, maxit=3000)
+        for _ in range(2 * slots_):
+            st, rhs = dense_pool[len(dense_pool) // 2][0]
+            srv.dense(st, rhs.copy(order="F"))
+        srv.drain()
+        groups = []
+        t0 = time.perf_counter()
+        for i in range(nreq):
+            if gaps is not None:
+                target = t0 + gaps[i]
+                while time.perf_counter() < target:
+                    time.sleep(min(1e-3, max(0.0, target - time.perf_counter())))
+            subs = []
+            if kinds[i]:
+                mats = dense_pool[picks[i] % len(dense_pool)]
+                for f in fsets[i]:
+                    st, rhs = mats[f % len(mats)]
+                    subs.append(srv.dense(st, rhs.copy(order="F")))
+            else:
+                mdl = models[picks[i] % len(models)]
+                for f in fsets[i]:
+                    b = mdl["rhs"][f]
+                    subs.append(srv.volume(mdl["systems"][f], b, np.zeros_like(b), rtol=1e-6, maxit=3000))
+            groups.append((kinds[i], subs))
+        srv.drain()
+        lat, merged = [], []
+        for dense_req, subs in groups:
+            for r in subs:
+                if not r.status or (r.kind != nb.REQUEST_DENSE and r.report.status != 0):
+                    raise RuntimeError("c4 stream request failed: %s (status %d)" % (r.error.decode(),
+                                                                                    r.report.status))
+                if not dense_req:
+                    merged.append(r.merged)
+            lat.append(1e3 * (max(r.finished_s for r in subs) - min(r.queued_s for r in subs)))
+        first = min(r.queued_s for _, subs in groups for r in subs)
+        last = max(r.finished_s for _, subs in groups for r in subs)
+        solves = int(sum(len(subs) for _, subs in groups))
+        srv.close()
+        lat.sort()
+        return {"requests": nreq, "solves": solves, "solves_per_s": solves / (last - first),
+                "requests_per_s": nreq / (last - first), "makespan_s": last - first,
+                "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                "volume_solves_merged_mean": float(np.mean(merged)) if merged else None}
+
+    t0 = time.perf_counter()
+    m32 = build_models(True)
+    m64 = build_models(False)
+    out = {"requests": nreq, "dense_fraction": float(kinds.mean()), "frequencies_per_request": [1, 2, 4, 8, 16],
+           "mean_frequencies": float(fsel.mean()), "dense_orders": orders,
+           "vie_lattices_over_pec_ground": ["%d^3" % n for n in lattices], "frequencies_per_model": len(freqs),
+           "slots": slots, "setup_s": time.perf_counter() - t0,
+           "device_gb_in_use_after_setup": (lambda f: (f[1] - f[0]) / 1e9)(torch.cuda.mem_get_info())}
+    sat = {}
+    sat["mixed"] = max((run(m32, False, slots, None, True) for _ in range(2)), key=lambda r: r["solves_per_s"])
+    sat["mixed_unmerged"] = run(m32, False, slots, None, False)
+    sat["mixed_split_lu"] = run(m32, True, slots, None, True)
+    sat["fp64"] = max((run(m64, False, slots, None, True) for _ in range(2)), key=lambda r: r["solves_per_s"])
+    plain = run(m64, False, 1, None, False)
+    out["saturation"] = sat
+    out["plain_fp64_one_at_a_time"] = plain
+    out["mixed_vs_plain_fp64"] = sat["mixed"]["solves_per_s"] / plain["solves_per_s"]
+    out["mixed_split_lu_vs_plain_fp64"] = sat["mixed_split_lu"]["solves_per_s"] / plain["solves_per_s"]
+    out["fp64_batched_vs_plain_fp64"] = sat["fp64"]["solves_per_s"] / plain["solves_per_s"]
+    sweep = []
+    for frac in rates:
+        rate = frac * sat["mixed"]["requests_per_s"]
+        gaps = np.cumsum(np.random.default_rng(13).exponential(1.0 / rate, nreq))
+        res = run(m32, False, slots, gaps, True)
+        res["offered_requests_per_s"] = rate
+        res["fraction_of_saturation"] = frac
+        sweep.append(res)
+    out["poisson_mixed"] = sweep
+    for ms in (m32, m64):
+        for mdl in ms:
+            mdl["batch"].close()
+            for hs in mdl["systems"]:
+                hs.close()
+            for p in mdl["plans"]:
+                p.close()
     return out
 
 

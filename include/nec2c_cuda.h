@@ -192,7 +192,7 @@ int nec2c_cuda_gmres_hybrid_device(nec2c_cuda_hybrid *system, const void *b_dev,
 /* ------------------------------------------------- ragged batch of plans */
 typedef struct nec2c_cuda_vie_batch nec2c_cuda_vie_batch;
 /* Many volume plans (frequencies or geometries with ragged lattices, padded
-   axes up to 128, all with the same transform precision, each at most once)
+   axes up to 256, all with the same transform precision, each at most once)
    solved together: every FFT pass of a GMRES step is one launch over all the
    plans, every Gram-Schmidt sweep one launch over all the systems, and the
    steps of a restart cycle run as CUDA graphs of five steps, the cycle ending
@@ -392,6 +392,9 @@ typedef struct {
      products and the largest relative residual */
   nec2c_cuda_vie_batch *batch;
   nec2c_cuda_gmres_report *reports;
+  /* filled by the server: how many volume requests ran together in the
+     batched solve this one was merged into (1: it ran alone) */
+  size_t merged;
 } nec2c_cuda_request;
 typedef struct nec2c_cuda_server nec2c_cuda_server;
 /* slots worker threads on device; device_budget 0 means the free device
@@ -405,6 +408,15 @@ int nec2c_cuda_server_wait(nec2c_cuda_server *server, nec2c_cuda_request *reques
 /* Blocks until every submitted request is done. */
 int nec2c_cuda_server_drain(nec2c_cuda_server *server);
 size_t nec2c_cuda_server_budget(const nec2c_cuda_server *server);
+/* Lets the server merge queued volume requests: a worker that takes a volume
+   request whose plan (or hybrid system) is one of batch's systems also takes
+   every other queued volume request on a system of the same batch with the
+   same GMRES options (restart <= 30), and solves them as one batched solve
+   in which the batch's other systems stay idle (the batched GMRES, to the
+   same tolerances as the single-system solve).  Each request gets its
+   own report, x and status; `merged` tells how many ran together.  The
+   batch must outlive the server; registering it twice is refused. */
+int nec2c_cuda_server_merge_batch(nec2c_cuda_server *server, nec2c_cuda_vie_batch *batch);
 /* Drains, stops the workers and frees the server. */
 void nec2c_cuda_server_destroy(nec2c_cuda_server *server);
 

@@ -42,7 +42,7 @@ class Request(C.Structure):
                 ("status", C.c_int), ("done", C.c_int), ("skipped", C.c_uint), ("report", GmresReport),
                 ("footprint", C.c_size_t), ("queued_s", C.c_double), ("started_s", C.c_double),
                 ("finished_s", C.c_double), ("error", C.c_char * 128), ("batch", C.c_void_p),
-                ("reports", C.c_void_p)]
+                ("reports", C.c_void_p), ("merged", C.c_size_t)]
 
 
 REQUEST_DENSE, REQUEST_VOLUME, REQUEST_BATCH = 1, 2, 3
@@ -456,6 +456,12 @@ class Server:
         r.system_reports = reps
         self._submit(r, (batch, b, x, reps))
         return r
+
+    def merge(self, batch):
+        """Registers a VolumeBatch whose systems' queued volume requests the
+        server may merge into one batched solve."""
+        if not load().nec2c_cuda_server_merge_batch(self.h, batch.h):
+            raise RuntimeError("merge registration failed: " + last_error())
 
     def _submit(self, r, keep):
         self._keep[C.addressof(r)] = (r, keep)

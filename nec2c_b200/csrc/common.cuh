@@ -63,6 +63,17 @@ __device__ __forceinline__ double2 block_sum(double2 v) {
   return t;
 }
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream
+// serialisation may be scheduled while its predecessor in the stream is still
+// finishing: it first waits here for that grid to complete and its writes to
+// be visible, then lets its own successor begin launching (whose CTAs take the
+// SMs this grid's last wave leaves idle, and wait in turn).  Both are no-ops
+// for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 }  // namespace n2c
 
 #define N2C_CHECK(call)                                                        \

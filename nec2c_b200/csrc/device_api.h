@@ -142,7 +142,7 @@ int n2d_gmres_dev(int kind, void *op, long long n, const double *b_dev, double *
 
 /* ---- ragged batch of volume plans (vie_batch.cu) ---- */
 typedef struct n2d_vie_batch n2d_vie_batch;
-/* Plans with the same transform precision, padded axes <= 128, each at most
+/* Plans with the same transform precision, padded axes <= 256, each at most
    once; their permittivities must have been uploaded (self terms set). */
 int n2d_vie_batch_create(n2d_vie_batch **out, n2d_vie *const *plans, long long count);
 /* Hybrid conductor + volume systems (each with a volume plan, blocks
@@ -160,9 +160,12 @@ int n2d_vie_batch_apply(n2d_vie_batch *b, const double *x_dev, double *y_dev);
 void n2d_vie_batch_schedule(const n2d_vie_batch *b, int *scale, int *variant);
 int n2d_vie_batch_set_schedule(n2d_vie_batch *b, const int *scale, const int *variant);
 /* GMRES(restart <= 30) on every plan in lockstep; reports[q] per system.
-   Returns 1 when every system converged. */
+   idle (NULL, or one flag per system): systems flagged non-zero take no part
+   and their reports stay "invalid".  Returns 1 when every other system
+   converged. */
 int n2d_gmres_batch_dev(n2d_vie_batch *b, const double *b_dev, double *x_dev, size_t restart,
-                        size_t maximum_iterations, double rtol, double atol, n2d_gmres_report *reports);
+                        size_t maximum_iterations, double rtol, double atol, const unsigned char *idle,
+                        n2d_gmres_report *reports);
 
 /* ---- dense LU (matrix.c factr/solve, dense_backend.c) ---- */
 /* Factor order x order in place on the device: the algebraic matrix

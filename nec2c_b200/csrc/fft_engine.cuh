@@ -261,6 +261,7 @@ __device__ __forceinline__ void fft_forward_tile(const PassArgs<C> &a, long long
 }
 template <typename C, int R1, int R2, bool CELLS = false>
 __global__ void __launch_bounds__(256) fft_forward_pass(PassArgs<C> a) {
+  pdl_begin();
   fft_forward_tile<C, R1, R2, CELLS>(a, blockIdx.x);
 }
 
@@ -332,6 +333,7 @@ __device__ __forceinline__ void fft_inverse_tile(const PassArgs<C> &a, long long
 }
 template <typename C, int R1, int R2, bool CELLS = false>
 __global__ void __launch_bounds__(256) fft_inverse_pass(PassArgs<C> a) {
+  pdl_begin();
   fft_inverse_tile<C, R1, R2, CELLS>(a, blockIdx.x, gridDim.x);
 }
 
@@ -432,6 +434,7 @@ __device__ __forceinline__ void fft_product_tile(const PassArgs<C> &a, long long
 // complex values per thread would otherwise spill.
 template <typename C, int R1, int R2>
 __global__ void __launch_bounds__(256, 2) fft_product_pass(PassArgs<C> a) {
+  pdl_begin();
   fft_product_tile<C, R1, R2>(a, blockIdx.x);
 }
 
@@ -660,6 +663,7 @@ __device__ __forceinline__ void fft_zline_tile(const PassArgs<C> &a, long long t
 }
 template <typename C, int R1, int R2, bool INV, bool CELLS>
 __global__ void __launch_bounds__(256, 3) fft_zline_pass(PassArgs<C> a) {
+  pdl_begin();
   fft_zline_tile<C, R1, R2, INV, CELLS>(a, blockIdx.x, gridDim.x);
 }
 

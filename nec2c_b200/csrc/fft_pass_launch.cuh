@@ -1,6 +1,8 @@
 // Definitions behind fft_passes.cuh, included by the two per-precision
 // translation units only.
 #pragma once
+#include <stdlib.h>
+
 #include <atomic>
 
 #include "fft_passes.cuh"
@@ -34,7 +36,28 @@ static int launch_rr(int mode, const PassArgs<C> &a, size_t smem, long long tile
     configured[mode].store(true, std::memory_order_release);
   }
   if (tiles > 0x7fffffffLL) { n2c_set_error("FFT pass grid too large"); return 0; }
-  k<<<(unsigned)tiles, 256, smem, n2c_stream()>>>(a);
+  // Programmatic dependent launch (the kernels wait for their predecessor
+  // first thing, pdl_begin), so a pass's launch and first CTAs overlap the
+  // previous pass's last wave.  NEC2C_CUDA_PDL=0 (read once) turns it off.
+  static const bool pdl = [] {
+    const char *v = getenv("NEC2C_CUDA_PDL");
+    return !(v && v[0] == '0');
+  }();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)tiles);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = n2c_stream();
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k, a);
+  if (e != cudaSuccess) {
+    n2c_set_error("fft pass launch: %s", cudaGetErrorString(e));
+    return 0;
+  }
   return n2c_check_launch("fft pass");
 }
 

@@ -21,6 +21,7 @@
 // eight warps read the accumulator back (tcgen05.ld: warp w its 32 lanes of
 // quarter w%4, half the columns per warpgroup) and update C.
 // No cluster, no multicast.
+#include <stdlib.h>
 #include <stdint.h>
 #include <string.h>
 #include "common.cuh"
@@ -81,7 +82,7 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
 
 __global__ void __launch_bounds__(THREADS, 2)
 gemm_tf32x3_kernel(float2 *C, long long ldc, const float2 *A, long long lda, const float *bt_hi, const float *bt_lo,
-                   long long M, long long N, int *error) {
+                   long long M, long long N, int *error, long long wait_cycles) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ uint32_t tmem_base;
   __shared__ __align__(8) unsigned long long done_bar;
@@ -171,13 +172,14 @@ gemm_tf32x3_kernel(float2 *C, long long ldc, const float2 *A, long long lda, con
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                  :: "r"(smem_u32(&done_bar)) : "memory");
   }
-  // Bounded wait for the products (about a second at boost clock).
-  bool ok = true;
-  {
+  // Bounded wait for the products (wait_cycles, about a second at boost
+  // clock by default; zero gives up at once and takes the time-out path).
+  bool ok = wait_cycles > 0;
+  if (ok) {
     const uint32_t bar = smem_u32(&done_bar);
     const long long t0 = clock64();
     while (!mbar_try(bar, 0)) {
-      if (clock64() - t0 > (1LL << 31)) { ok = false; break; }
+      if (clock64() - t0 > wait_cycles) { ok = false; break; }
     }
   }
   // Every thread takes the same path (tcgen05.ld is warp-aligned).
@@ -245,7 +247,18 @@ gemm_tf32x3_kernel(float2 *C, long long ldc, const float2 *A, long long lda, con
 // -= A (M x 32, lda) times the complex 32 x N block whose packed expansion is
 // bt_hi + bt_lo (2N rows of 64 floats).  The rows of A and C must start
 // 16-byte aligned (lda, ldc even; A, C 16-byte aligned).  error: device int
-// set to 1 on a time-out.
+// set to 1 on a time-out; C is then left as it was.  The wait for the
+// products is 2^31 clocks unless NEC2C_CUDA_TC_WAIT_CYCLES (read once) sets
+// another limit; 0 makes every launch take the time-out path, which is how the
+// tests exercise it.
+static long long tc_wait_cycles() {
+  const char *v = getenv("NEC2C_CUDA_TC_WAIT_CYCLES");
+  if (!v || !*v) return 1LL << 31;
+  char *end = nullptr;
+  const long long c = strtoll(v, &end, 10);
+  return (end && *end == 0 && c >= 0) ? c : 1LL << 31;
+}
+
 int n2c_tc_update(float *C, long long ldc, const float *A, long long lda, const float *bt_hi, const float *bt_lo,
                   long long M, long long N, int *error, cudaStream_t s) {
   if (M <= 0 || N <= 0) return 1;
@@ -261,9 +274,10 @@ int n2c_tc_update(float *C, long long ldc, const float *A, long long lda, const 
     n2c_set_error("tensor-core update: shared memory configuration failed");
     return 0;
   }
+  static const long long wait_cycles = tc_wait_cycles();
   dim3 grid((unsigned)((N + TNC - 1) / TNC), (unsigned)((M + TM - 1) / TM));
   gemm_tf32x3_kernel<<<grid, THREADS, SMEM_BYTES, s>>>((float2 *)C, ldc, (const float2 *)A, lda, bt_hi, bt_lo, M, N,
-                                                       error);
+                                                       error, wait_cycles);
   return n2c_check_launch("tensor-core update");
 }
 

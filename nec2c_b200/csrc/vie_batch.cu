@@ -1,7 +1,7 @@
 // Ragged batch of volume FFT plans solved together on one GPU.
 //
 // Many frequencies or geometries, each a plan with its own lattice, padded
-// grid (axes up to 128) and spectrum, advance through GMRES(m) in lockstep:
+// grid (axes up to 256) and spectrum, advance through GMRES(m) in lockstep:
 //   - every FFT pass of a product is ONE launch over the tiles of all plans:
 //     a CTA finds its plan by binary search over the plans' first tiles and
 //     runs the tile body of that plan's line length (fft_engine.cuh);
@@ -23,6 +23,7 @@
 // conductor rows and cross rows are one launch each over all systems too.
 // The batch's vectors are the systems' vectors (conductor unknowns, then 3 x
 // cells) concatenated in system order.
+#include <stdlib.h>
 #include <float.h>
 #include <math.h>
 #include <string.h>
@@ -49,7 +50,7 @@ enum { ST_CONVERGED, ST_LIMIT, ST_BREAKDOWN, ST_CALLBACK, ST_INVALID, ST_ALLOC, 
 enum { ST_RUNNING = -1 };
 
 constexpr int BMAXM = 30;                         // longest restart cycle of a batch
-constexpr int MAX_L = 128;                        // longest padded axis of a batched plan
+constexpr int MAX_L = 256;                        // longest padded axis of a batched plan
 constexpr double REORTH = 10.0;                   // cancellation factor of the FP32-transform form
 constexpr int DOT_E = 4;                          // elements per lane per dots load
 constexpr int DOT_GROUP = 32 * DOT_E;             // elements per warp group
@@ -138,6 +139,7 @@ __device__ __forceinline__ void tile_body(const PassArgs<C> &a, long long tile, 
 template <typename C, int MODE>
 __global__ void __launch_bounds__(256, MODE <= 1 ? 1 : (MODE == 2 && sizeof(C) != sizeof(float2) ? 2 : 3))
     batch_pass_kernel(const BatchDesc<C> *desc, const long long *first, int count, const double2 *x, double2 *y) {
+  pdl_begin();
   const int q = find_seg(first, count, blockIdx.x);
   // A stopped system's tiles leave before its arguments are read.
   const int *gate = desc[q].a.gate;
@@ -167,6 +169,7 @@ __global__ void __launch_bounds__(256, MODE <= 1 ? 1 : (MODE == 2 && sizeof(C) !
     case 32: tile_body<C, 8, 4, MODE>(a, tile, ntiles); break;
     case 64: tile_body<C, 8, 8, MODE>(a, tile, ntiles); break;
     case 128: tile_body<C, 16, 8, MODE>(a, tile, ntiles); break;
+    case 256: tile_body<C, 16, 16, MODE>(a, tile, ntiles); break;
   }
 }
 
@@ -751,7 +754,28 @@ static int launch_set_t(const n2d_vie_batch *b, const PassSet &ps, const double2
     }
     configured[ps.mode].store(true, std::memory_order_release);
   }
-  k<<<(unsigned)ps.tiles, 256, ps.smem, n2c_stream()>>>((const BatchDesc<C> *)ps.desc, ps.first, b->K, x, y);
+  // Programmatic dependent launch, as for the single-plan passes
+  // (NEC2C_CUDA_PDL=0 turns it off).
+  static const bool pdl = [] {
+    const char *v = getenv("NEC2C_CUDA_PDL");
+    return !(v && v[0] == '0');
+  }();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)ps.tiles);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = ps.smem;
+  cfg.stream = n2c_stream();
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k, (const BatchDesc<C> *)ps.desc, (const long long *)ps.first,
+                                           b->K, x, y);
+  if (e != cudaSuccess) {
+    n2c_set_error("batched fft pass launch: %s", cudaGetErrorString(e));
+    return 0;
+  }
   return n2c_check_launch("batched fft pass");
 }
 
@@ -1070,7 +1094,8 @@ static void try_capture(n2d_vie_batch *b, BatchWork *w) {
 }
 
 extern "C" int n2d_gmres_batch_dev(n2d_vie_batch *b, const double *b_dev, double *x_dev, size_t restart,
-                                   size_t maxit, double rtol, double atol, n2d_gmres_report *reps) {
+                                   size_t maxit, double rtol, double atol, const unsigned char *idle,
+                                   n2d_gmres_report *reps) {
   const int K = b->K;
   for (int q = 0; q < K; ++q) {
     memset(&reps[q], 0, sizeof(reps[q]));
@@ -1113,10 +1138,14 @@ extern "C" int n2d_gmres_batch_dev(n2d_vie_batch *b, const double *b_dev, double
     hs[q].status = ST_RUNNING;
     hs[q].max_iterations = (long long)maxit;
     hs[q].m = (int)std::min<long long>(m, n);
+    // An idle system takes no part: it is done from the start, never
+    // active or running, so its tiles leave at their gates.
+    if (idle && idle[q]) { done[q] = 1; hs[q].status = ST_INVALID; }
   }
   // ||b|| and ||x|| (finite check) of every system (vie_iterative.c:116-119).
   if (!put() || !norms_of(rhs, norms.data()) || !norms_of(x, norms.data() + K) || !get()) return 0;
   for (int q = 0; q < K; ++q) {
+    if (done[q]) continue;
     bnorm[q] = sqrt(norms[q]);
     target[q] = fmax(atol, rtol * bnorm[q]);
     hs[q].target = target[q];
@@ -1207,6 +1236,6 @@ extern "C" int n2d_gmres_batch_dev(n2d_vie_batch *b, const double *b_dev, double
     }
   }
   int all = 1;
-  for (int q = 0; q < K; ++q) all = all && reps[q].status == ST_CONVERGED;
+  for (int q = 0; q < K; ++q) all = all && ((idle && idle[q]) || reps[q].status == ST_CONVERGED);
   return all;
 }

@@ -20,7 +20,14 @@
  * plan (directly, through a hybrid system or in a batch) never run at the
  * same time.  Admission is FIFO, except that a request that
  * does not fit may be passed by later ones that do, at most `slots` times
- * each before the queue waits for it. */
+ * each before the queue waits for it.
+ *
+ * Continuous batching: for a batch registered with
+ * nec2c_cuda_server_merge_batch, a worker that takes a volume request on one
+ * of the batch's systems also takes the queued volume requests on its other
+ * systems (same GMRES options) and runs them as one batched solve with the
+ * remaining systems idle, so the requests that pile up while the device is
+ * busy (frequencies of one model from many callers) share each launch. */
 #include <errno.h>
 #include <limits.h>
 #include <pthread.h>
@@ -36,6 +43,22 @@ int n2c_dense_solve_private(size_t n, const nec2c_cuda_complex *matrix, size_t l
                             size_t stride, size_t count, int split, int *steps);
 const nec2c_cuda_vie_plan *n2c_hybrid_volume_plan(const nec2c_cuda_hybrid *h);
 const nec2c_cuda_vie_plan *n2c_batch_plan(const nec2c_cuda_vie_batch *b, size_t q);
+size_t n2c_batch_index(const nec2c_cuda_vie_batch *b, const nec2c_cuda_vie_plan *plan,
+                       const nec2c_cuda_hybrid *system);
+int n2c_gmres_batch_subset(nec2c_cuda_vie_batch *b, const nec2c_cuda_complex *const *bv,
+                           nec2c_cuda_complex *const *xv, const nec2c_cuda_gmres_options *options,
+                           nec2c_cuda_gmres_report *reports);
+
+/* The batched GMRES restarts after at most this many steps. */
+#define MERGE_MAX_RESTART 30
+
+/* What one worker runs: a request, or (batch != NULL, n >= 2) the volume
+   requests merged into one solve of that batch, member j on system index[j]. */
+typedef struct {
+  nec2c_cuda_request **member;
+  size_t *index, n;
+  nec2c_cuda_vie_batch *batch;
+} run_t;
 
 struct nec2c_cuda_server {
   int device, slots, split;
@@ -44,7 +67,9 @@ struct nec2c_cuda_server {
   pthread_cond_t work, done;
   nec2c_cuda_request **queue;   /* FIFO, [head, head + count) modulo cap */
   size_t head, count, cap;
-  const nec2c_cuda_request **busy;   /* request in flight per worker */
+  run_t *busy;                  /* in flight per worker (n == 0: idle) */
+  nec2c_cuda_vie_batch **merge; /* batches whose systems' requests merge */
+  size_t merges;
   size_t pending;               /* submitted, not finished */
   int stop, started;
   pthread_t *threads;
@@ -127,23 +152,90 @@ static int run_batch(nec2c_cuda_request *r)
 static int plan_busy(const nec2c_cuda_server *s, const nec2c_cuda_request *c)
 {
   const size_t n = request_plans(c);
-  size_t a, b;
+  size_t a, b, j;
   int i;
   if(n == 0) return 0;
+  for(i = 0; i < s->slots; ++i)
+    for(j = 0; j < s->busy[i].n; ++j) {
+      const nec2c_cuda_request *r = s->busy[i].member[j];
+      const size_t m = request_plans(r);
+      for(a = 0; a < n; ++a)
+        for(b = 0; b < m; ++b)
+          if(request_plan(c, a) == request_plan(r, b)) return 1;
+    }
+  return 0;
+}
+
+/* True when a run in flight uses batch b's own vectors: a batch request on
+   it, or volume requests merged into it. */
+static int batch_busy(const nec2c_cuda_server *s, const nec2c_cuda_vie_batch *b)
+{
+  int i;
   for(i = 0; i < s->slots; ++i) {
-    const nec2c_cuda_request *r = s->busy[i];
-    const size_t m = r ? request_plans(r) : 0;
-    for(a = 0; a < n; ++a)
-      for(b = 0; b < m; ++b)
-        if(request_plan(c, a) == request_plan(r, b)) return 1;
+    const run_t *u = &s->busy[i];
+    if(u->n == 0) continue;
+    if(u->batch == b || (u->member[0]->kind == NEC2C_CUDA_REQUEST_BATCH && u->member[0]->batch == b)) return 1;
   }
   return 0;
+}
+
+static int same_options(const nec2c_cuda_gmres_options *a, const nec2c_cuda_gmres_options *b)
+{
+  return a->restart == b->restart && a->maximum_iterations == b->maximum_iterations &&
+         a->relative_tolerance == b->relative_tolerance && a->absolute_tolerance == b->absolute_tolerance;
+}
+
+/* The registered batch holding volume request r's operator (its index in
+   *q), or NULL. */
+static nec2c_cuda_vie_batch *merge_batch_of(const nec2c_cuda_server *s, const nec2c_cuda_request *r, size_t *q)
+{
+  size_t i;
+  if(r->kind != NEC2C_CUDA_REQUEST_VOLUME || r->options.restart == 0 || r->options.restart > MERGE_MAX_RESTART)
+    return NULL;
+  for(i = 0; i < s->merges; ++i) {
+    const size_t k = n2c_batch_index(s->merge[i], r->plan, r->system);
+    if(k != (size_t)-1) { *q = k; return s->merge[i]; }
+  }
+  return NULL;
+}
+
+/* Merged volume requests: one batched solve over their systems. */
+static void run_merged(run_t *u)
+{
+  const size_t k = nec2c_cuda_vie_batch_systems(u->batch);
+  const nec2c_cuda_complex **bv = calloc(k, sizeof(*bv));
+  nec2c_cuda_complex **xv = calloc(k, sizeof(*xv));
+  nec2c_cuda_gmres_report *reps = calloc(k, sizeof(*reps));
+  size_t j;
+  int ok = bv && xv && reps;
+  if(!ok) n2c_set_error("merged requests: out of host memory");
+  for(j = 0; ok && j < u->n; ++j) {
+    bv[u->index[j]] = u->member[j]->b;
+    xv[u->index[j]] = u->member[j]->x;
+  }
+  if(ok) ok = n2c_gmres_batch_subset(u->batch, bv, xv, &u->member[0]->options, reps);
+  for(j = 0; j < u->n; ++j) {
+    nec2c_cuda_request *r = u->member[j];
+    if(reps) r->report = reps[u->index[j]];
+    /* 1 when the system converged and its x came back, as a single solve
+       returns 1 only on convergence. */
+    r->status = ok && reps && reps[u->index[j]].status == 0;
+    r->merged = u->n;
+    if(!r->status) {
+      const int st = ok ? (int)r->report.status : -1;
+      strncpy(r->error, st == 1 ? "GMRES iteration limit" : st == 2 ? "GMRES breakdown" : nec2c_cuda_last_error(),
+              sizeof(r->error) - 1);
+      r->error[sizeof(r->error) - 1] = 0;
+    }
+  }
+  free(bv); free(xv); free(reps);
 }
 
 static void run_request(nec2c_cuda_server *s, nec2c_cuda_request *r)
 {
   int steps = 0;
   memset(&r->report, 0, sizeof(r->report));
+  r->merged = 1;
   if(r->kind == NEC2C_CUDA_REQUEST_DENSE) {
     r->status = n2c_dense_solve_private(r->order, r->matrix, r->ld, r->rhs, r->rhs_stride, r->rhs_count, s->split,
                                         &steps);
@@ -162,6 +254,45 @@ static void run_request(nec2c_cuda_server *s, nec2c_cuda_request *r)
   }
 }
 
+static int fits(const nec2c_cuda_server *s, size_t f)
+{
+  return s->in_use == 0 || (f <= s->budget && s->in_use + f <= s->budget);
+}
+
+/* With the lock held: the queued volume requests that can join r (at queue
+   position pick, on system q0 of registered batch b) in one batched solve,
+   r first.  Fills u (member / index arrays of b's system count) and marks
+   the chosen queue positions in taken; returns the run's footprint, or 0
+   when fewer than two requests can merge or the merged run does not fit. */
+static size_t gather_merge(const nec2c_cuda_server *s, nec2c_cuda_request *r, size_t pick, size_t q0,
+                           nec2c_cuda_vie_batch *b, run_t *u, unsigned char *taken)
+{
+  const size_t k = nec2c_cuda_vie_batch_systems(b), order = nec2c_cuda_vie_batch_order(b);
+  unsigned char *used = calloc(k, 1);
+  size_t q, f;
+  if(!used) return 0;
+  u->n = 0;
+  u->member[u->n] = r; u->index[u->n++] = q0; used[q0] = 1; taken[pick] = 1;
+  for(q = 0; q < s->count && u->n < k; ++q) {
+    nec2c_cuda_request *c = s->queue[(s->head + q) % s->cap];
+    size_t qc;
+    if(q == pick || c->kind != NEC2C_CUDA_REQUEST_VOLUME || !same_options(&c->options, &r->options)) continue;
+    qc = n2c_batch_index(b, c->plan, c->system);
+    if(qc == (size_t)-1 || used[qc] || plan_busy(s, c)) continue;
+    used[qc] = 1; taken[q] = 1;
+    u->member[u->n] = c; u->index[u->n++] = qc;
+  }
+  free(used);
+  /* The batch request's footprint for the whole batch's vectors. */
+  f = (r->options.restart + 4) * order * CPX + 2 * order * CPX;
+  if(u->n < 2 || !fits(s, f)) {
+    for(q = 0; q < s->count; ++q) taken[q] = 0;
+    u->n = 0;
+    return 0;
+  }
+  return f;
+}
+
 static void *worker(void *arg)
 {
   nec2c_cuda_server *s = arg;
@@ -173,38 +304,86 @@ static void *worker(void *arg)
   pthread_mutex_lock(&s->lock);
   for(;;) {
     nec2c_cuda_request *r = NULL;
-    size_t pick = 0, q, fp = 0;
+    nec2c_cuda_vie_batch *mb = NULL;
+    run_t *u;
+    size_t pick = 0, q, fp = 0, q0 = 0, kept, j;
+    unsigned char *taken = NULL;
     if(s->stop && s->count == 0) break;
     for(q = 0; q < s->count; ++q) {
       nec2c_cuda_request *c = s->queue[(s->head + q) % s->cap];
       const size_t f = footprint(s, c);
-      const int fits = s->in_use == 0 || (f <= s->budget && s->in_use + f <= s->budget);
-      if(fits && !plan_busy(s, c)) { r = c; pick = q; fp = f; break; }
+      const int ok = fits(s, f);
+      if(ok && !plan_busy(s, c)) { r = c; pick = q; fp = f; break; }
       /* A request that does not fit may be passed only `slots` times. */
-      if(!fits && c->skipped >= (unsigned)s->slots) break;
+      if(!ok && c->skipped >= (unsigned)s->slots) break;
     }
     if(!r) { pthread_cond_wait(&s->work, &s->lock); continue; }
     for(q = 0; q < pick; ++q) {
       nec2c_cuda_request *c = s->queue[(s->head + q) % s->cap];
-      const size_t f = footprint(s, c);
-      if(!(s->in_use == 0 || (f <= s->budget && s->in_use + f <= s->budget))) c->skipped++;
+      if(!fits(s, footprint(s, c))) c->skipped++;
     }
-    for(q = pick; q + 1 < s->count; ++q)
-      s->queue[(s->head + q) % s->cap] = s->queue[(s->head + q + 1) % s->cap];
-    s->count--;
+    for(i = 0; i < s->slots; ++i) if(s->busy[i].n == 0) { slot = i; break; }
+    if(slot < 0) { pthread_cond_wait(&s->work, &s->lock); continue; }   /* one run per worker: not reached */
+    u = &s->busy[slot];
+    u->batch = NULL;
+    /* Continuous batching: the queued requests on the other systems of r's
+       registered batch join it. */
+    mb = merge_batch_of(s, r, &q0);
+    if(mb && !batch_busy(s, mb) && s->count > 1 && (taken = calloc(s->count, 1)) != NULL &&
+       (u->member = malloc(nec2c_cuda_vie_batch_systems(mb) * sizeof(*u->member))) != NULL &&
+       (u->index = malloc(nec2c_cuda_vie_batch_systems(mb) * sizeof(*u->index))) != NULL) {
+      const size_t f = gather_merge(s, r, pick, q0, mb, u, taken);
+      if(f) { fp = f; u->batch = mb; }
+    }
+    if(!u->batch) {
+      free(u->member); free(u->index);
+      u->member = NULL; u->index = NULL;
+      free(taken);
+      taken = calloc(s->count, 1);
+      u->member = malloc(sizeof(*u->member));
+      if(!taken || !u->member) {
+        /* Out of host memory: fail the request rather than the server. */
+        free(taken); free(u->member); u->member = NULL;
+        for(q = pick; q + 1 < s->count; ++q)
+          s->queue[(s->head + q) % s->cap] = s->queue[(s->head + q + 1) % s->cap];
+        s->count--;
+        r->status = 0;
+        strncpy(r->error, "server: out of host memory", sizeof(r->error) - 1);
+        r->finished_s = now_s();
+        r->done = 1;
+        s->pending--;
+        pthread_cond_broadcast(&s->done);
+        continue;
+      }
+      taken[pick] = 1;
+      u->member[0] = r;
+      u->n = 1;
+    }
+    /* Take the chosen requests out of the queue, keeping the order of the rest. */
+    for(q = 0, kept = 0; q < s->count; ++q)
+      if(!taken[q]) s->queue[(s->head + kept++) % s->cap] = s->queue[(s->head + q) % s->cap];
+    s->count = kept;
+    free(taken);
     s->in_use += fp;
-    for(i = 0; i < s->slots; ++i) if(!s->busy[i]) { s->busy[i] = r; slot = i; break; }
-    r->footprint = fp;
-    r->started_s = now_s();
+    for(j = 0; j < u->n; ++j) {
+      u->member[j]->footprint = j == 0 ? fp : 0;
+      u->member[j]->started_s = now_s();
+    }
     pthread_mutex_unlock(&s->lock);
-    run_request(s, r);
+    if(u->batch) run_merged(u);
+    else run_request(s, r);
     pthread_mutex_lock(&s->lock);
-    r->finished_s = now_s();
     s->in_use -= fp;
-    if(slot >= 0) s->busy[slot] = NULL;
+    for(j = 0; j < u->n; ++j) {
+      u->member[j]->finished_s = now_s();
+      u->member[j]->done = 1;
+      s->pending--;
+    }
+    u->n = 0;
+    u->batch = NULL;
+    free(u->member); free(u->index);
+    u->member = NULL; u->index = NULL;
     slot = -1;
-    r->done = 1;
-    s->pending--;
     pthread_cond_broadcast(&s->done);
     pthread_cond_broadcast(&s->work);
   }
@@ -322,6 +501,27 @@ int nec2c_cuda_server_drain(nec2c_cuda_server *s)
 
 size_t nec2c_cuda_server_budget(const nec2c_cuda_server *s) { return s ? s->budget : 0; }
 
+int nec2c_cuda_server_merge_batch(nec2c_cuda_server *s, nec2c_cuda_vie_batch *b)
+{
+  nec2c_cuda_vie_batch **m;
+  size_t i;
+  if(!s || !b) { n2c_set_error("merge batch: null server or batch"); return 0; }
+  pthread_mutex_lock(&s->lock);
+  for(i = 0; i < s->merges; ++i)
+    if(s->merge[i] == b) {
+      pthread_mutex_unlock(&s->lock);
+      n2c_set_error("merge batch: batch already registered");
+      return 0;
+    }
+  m = realloc(s->merge, (s->merges + 1) * sizeof(*m));
+  if(!m) { pthread_mutex_unlock(&s->lock); n2c_set_error("merge batch: out of host memory"); return 0; }
+  s->merge = m;
+  s->merge[s->merges++] = b;
+  pthread_cond_broadcast(&s->work);
+  pthread_mutex_unlock(&s->lock);
+  return 1;
+}
+
 void nec2c_cuda_server_destroy(nec2c_cuda_server *s)
 {
   int i;
@@ -335,6 +535,6 @@ void nec2c_cuda_server_destroy(nec2c_cuda_server *s)
   pthread_mutex_destroy(&s->lock);
   pthread_cond_destroy(&s->work);
   pthread_cond_destroy(&s->done);
-  free(s->queue); free(s->busy); free(s->threads);
+  free(s->queue); free(s->busy); free(s->threads); free(s->merge);
   free(s);
 }

@@ -672,7 +672,7 @@ static int batch_options_ok(const nec2c_cuda_gmres_options *o)
          !(o->relative_tolerance == 0 && o->absolute_tolerance == 0);
 }
 
-static int batch_solve(nec2c_cuda_vie_batch *b, const void *b_dev, void *x_dev,
+static int batch_solve(nec2c_cuda_vie_batch *b, const void *b_dev, void *x_dev, const unsigned char *idle,
                        const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *reports)
 {
   nec2c_cuda_gmres_options defaults = {30, 300, 1e-12, 0.0};
@@ -692,7 +692,7 @@ static int batch_solve(nec2c_cuda_vie_batch *b, const void *b_dev, void *x_dev,
   if(!r) { n2c_set_error("batch solve: out of host memory"); return 0; }
   ok = batch_ready(b) &&
        n2d_gmres_batch_dev(b->dev, b_dev, x_dev, options->restart, options->maximum_iterations,
-                           options->relative_tolerance, options->absolute_tolerance, r);
+                           options->relative_tolerance, options->absolute_tolerance, idle, r);
   for(size_t q = 0; q < b->count; ++q) {
     reports[q].status = r[q].status;
     reports[q].iterations = r[q].iterations;
@@ -709,43 +709,93 @@ int nec2c_cuda_gmres_batch_device(nec2c_cuda_vie_batch *b, const void *b_dev, vo
                                   const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *reports)
 {
   if(!b || !b_dev || !x_dev || !reports) { n2c_set_error("batch solve: null batch, vector or reports"); return 0; }
-  return batch_solve(b, b_dev, x_dev, options, reports);
+  return batch_solve(b, b_dev, x_dev, NULL, options, reports);
 }
 
-int nec2c_cuda_gmres_batch(nec2c_cuda_vie_batch *b, const nec2c_cuda_complex *const *bv,
-                           nec2c_cuda_complex *const *xv, const nec2c_cuda_gmres_options *options,
-                           nec2c_cuda_gmres_report *reports)
+/* Host vectors through the batch's staging buffers.  With subset != 0 a
+   system whose bv[q] is NULL is idle: its segments are zeroed, it takes no
+   part in the solve and its xv[q] is not written. */
+static int batch_host(nec2c_cuda_vie_batch *b, const nec2c_cuda_complex *const *bv, nec2c_cuda_complex *const *xv,
+                      int subset, const nec2c_cuda_gmres_options *options, nec2c_cuda_gmres_report *reports)
 {
   const size_t cpx = sizeof(nec2c_cuda_complex);
+  unsigned char *idle = NULL;
+  size_t active = 0;
   int ok = 1, whole = 1;
   if(!b || !bv || !xv || !reports) { n2c_set_error("batch solve: null batch, vector list or reports"); return 0; }
-  for(size_t q = 0; q < b->count; ++q)
+  for(size_t q = 0; q < b->count; ++q) {
+    if(subset && !bv[q]) continue;
     if(!bv[q] || !xv[q]) { n2c_set_error("batch solve: vector of system %zu is NULL", q); return 0; }
+    ++active;
+  }
+  if(active < b->count) {
+    if(active == 0) { n2c_set_error("batch solve: no system to solve"); return 0; }
+    idle = calloc(b->count, 1);
+    if(!idle) { n2c_set_error("batch solve: out of host memory"); return 0; }
+    for(size_t q = 0; q < b->count; ++q) idle[q] = !bv[q];
+    whole = 0;
+  }
   /* Vectors that lie back to back in host memory (a server batch request's
      concatenated b and x) move in one copy each way. */
   for(size_t q = 1; q < b->count && whole; ++q)
     whole = bv[q] == bv[0] + b->offsets[q] && xv[q] == xv[0] + b->offsets[q];
   if(!b->b_dev) b->b_dev = n2d_alloc(b->order * cpx);
   if(!b->x_dev) b->x_dev = n2d_alloc(b->order * cpx);
-  if(!b->b_dev || !b->x_dev) return 0;
+  if(!b->b_dev || !b->x_dev) { free(idle); return 0; }
   if(whole) {
     ok = n2d_upload(b->b_dev, bv[0], b->order * cpx) && n2d_upload(b->x_dev, xv[0], b->order * cpx);
   } else {
+    if(idle) ok = n2d_memset(b->b_dev, 0, b->order * cpx) && n2d_memset(b->x_dev, 0, b->order * cpx);
     for(size_t q = 0; q < b->count && ok; ++q) {
       const size_t off = b->offsets[q] * cpx, bytes = (b->offsets[q + 1] - b->offsets[q]) * cpx;
+      if(idle && idle[q]) continue;
       ok = n2d_upload((char *)b->b_dev + off, bv[q], bytes) && n2d_upload((char *)b->x_dev + off, xv[q], bytes);
     }
   }
-  if(!ok) return 0;
-  ok = batch_solve(b, b->b_dev, b->x_dev, options, reports);
+  if(!ok) { free(idle); return 0; }
+  const int solved = batch_solve(b, b->b_dev, b->x_dev, idle, options, reports);
   /* x is copied back even when a solve fails (vie_iterative.h:51-53). */
   if(whole) {
     if(!n2d_download(xv[0], b->x_dev, b->order * cpx)) ok = 0;
   } else {
     for(size_t q = 0; q < b->count; ++q) {
       const size_t off = b->offsets[q] * cpx, bytes = (b->offsets[q + 1] - b->offsets[q]) * cpx;
+      if(idle && idle[q]) continue;
       if(!n2d_download(xv[q], (char *)b->x_dev + off, bytes)) ok = 0;
     }
   }
-  return ok;
+  free(idle);
+  /* A subset solve reports convergence per system only. */
+  return subset ? ok : ok && solved;
+}
+
+int nec2c_cuda_gmres_batch(nec2c_cuda_vie_batch *b, const nec2c_cuda_complex *const *bv,
+                           nec2c_cuda_complex *const *xv, const nec2c_cuda_gmres_options *options,
+                           nec2c_cuda_gmres_report *reports)
+{
+  return batch_host(b, bv, xv, 0, options, reports);
+}
+
+/* The request server's merged volume requests: the systems whose bv[q] is
+   non-NULL, solved together; the others idle.  Returns 1 when the solve ran
+   and every x came back (each system's convergence is in its report), 0
+   with the error set otherwise. */
+int n2c_gmres_batch_subset(nec2c_cuda_vie_batch *b, const nec2c_cuda_complex *const *bv,
+                           nec2c_cuda_complex *const *xv, const nec2c_cuda_gmres_options *options,
+                           nec2c_cuda_gmres_report *reports)
+{
+  return batch_host(b, bv, xv, 1, options, reports);
+}
+
+/* Index of a volume request's operator (a plan, or a hybrid system) among a
+   batch's systems; (size_t)-1 when it is not one of them. */
+size_t n2c_batch_index(const nec2c_cuda_vie_batch *b, const nec2c_cuda_vie_plan *plan,
+                       const nec2c_cuda_hybrid *system)
+{
+  if(!b || (!plan) == (!system)) return (size_t)-1;
+  for(size_t q = 0; q < b->count; ++q) {
+    if(system && b->hybrids && b->hybrids[q] == system) return q;
+    if(plan && !b->hybrids && b->plans[q] == plan) return q;
+  }
+  return (size_t)-1;
 }

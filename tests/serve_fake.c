@@ -29,11 +29,13 @@ struct nec2c_cuda_hybrid {
 struct nec2c_cuda_vie_batch {
   size_t count, order;
   nec2c_cuda_vie_plan **plans;
+  nec2c_cuda_hybrid **hybrids;   /* NULL for a batch of plans */
   size_t *offsets;
 };
 
 static pthread_mutex_t g_lock = PTHREAD_MUTEX_INITIALIZER;
 static int g_violations, g_running, g_peak;
+static int g_merged_runs, g_merged_peak;   /* merged solves seen; most systems in one */
 static long g_delay_us = 2000;
 static size_t g_free_bytes = (size_t)10 << 30;
 static __thread char g_error[256];
@@ -43,6 +45,7 @@ void fake_reset(long delay_us, size_t free_bytes)
 {
   pthread_mutex_lock(&g_lock);
   g_violations = g_running = g_peak = 0;
+  g_merged_runs = g_merged_peak = 0;
   g_delay_us = delay_us;
   g_free_bytes = free_bytes;
   pthread_mutex_unlock(&g_lock);
@@ -76,7 +79,26 @@ nec2c_cuda_vie_batch *fake_batch(nec2c_cuda_vie_plan *const *plans, size_t count
   b->order = b->offsets[count];
   return b;
 }
+nec2c_cuda_vie_batch *fake_hybrid_batch(nec2c_cuda_hybrid *const *systems, size_t count)
+{
+  nec2c_cuda_vie_batch *b = calloc(1, sizeof(*b));
+  if(!b) return NULL;
+  b->count = count;
+  b->plans = calloc(count, sizeof(*b->plans));
+  b->hybrids = calloc(count, sizeof(*b->hybrids));
+  b->offsets = calloc(count + 1, sizeof(*b->offsets));
+  for(size_t q = 0; q < count; ++q) {
+    b->hybrids[q] = systems[q];
+    b->plans[q] = systems[q]->volume;
+    b->offsets[q + 1] = b->offsets[q] + systems[q]->conductors + systems[q]->volume->order;
+  }
+  b->order = b->offsets[count];
+  return b;
+}
 void fake_release(void *p) { free(p); }
+
+int fake_merged_runs(void) { return g_merged_runs; }
+int fake_merged_peak(void) { return g_merged_peak; }
 
 /* Holds the plans for the solve's duration; a plan already held is an
    exclusivity violation. */
@@ -168,6 +190,41 @@ int nec2c_cuda_gmres_batch(nec2c_cuda_vie_batch *b, const nec2c_cuda_complex *co
     converged(&reports[q], q + 1);
   }
   return 1;
+}
+
+/* A merged solve: holds only the plans of the systems it solves, copies b
+   into x for those (reports: q + 1 iterations), leaves the rest alone. */
+int n2c_gmres_batch_subset(nec2c_cuda_vie_batch *b, const nec2c_cuda_complex *const *bv,
+                           nec2c_cuda_complex *const *xv, const nec2c_cuda_gmres_options *options,
+                           nec2c_cuda_gmres_report *reports)
+{
+  nec2c_cuda_vie_plan *held[64];
+  size_t n = 0;
+  (void)options;
+  for(size_t q = 0; q < b->count; ++q)
+    if(bv[q] && n < 64) held[n++] = b->plans[q];
+  pthread_mutex_lock(&g_lock);
+  ++g_merged_runs;
+  if((int)n > g_merged_peak) g_merged_peak = (int)n;
+  pthread_mutex_unlock(&g_lock);
+  hold(held, n);
+  for(size_t q = 0; q < b->count; ++q) {
+    if(!bv[q]) { memset(&reports[q], 0, sizeof(reports[q])); reports[q].status = 4; continue; }
+    memcpy(xv[q], bv[q], (b->offsets[q + 1] - b->offsets[q]) * sizeof(*xv[q]));
+    converged(&reports[q], q + 1);
+  }
+  return 1;
+}
+
+size_t n2c_batch_index(const nec2c_cuda_vie_batch *b, const nec2c_cuda_vie_plan *plan,
+                       const nec2c_cuda_hybrid *system)
+{
+  if(!b || (!plan) == (!system)) return (size_t)-1;
+  for(size_t q = 0; q < b->count; ++q) {
+    if(system && b->hybrids && b->hybrids[q] == system) return q;
+    if(plan && !b->hybrids && b->plans[q] == plan) return q;
+  }
+  return (size_t)-1;
 }
 
 size_t nec2c_cuda_vie_batch_systems(const nec2c_cuda_vie_batch *b) { return b ? b->count : 0; }

@@ -38,6 +38,9 @@ def fake():
     lib.fake_hybrid.restype = vp
     lib.fake_batch.argtypes = [vp, sz]
     lib.fake_batch.restype = vp
+    lib.fake_hybrid_batch.argtypes = [vp, sz]
+    lib.fake_hybrid_batch.restype = vp
+    lib.nec2c_cuda_server_merge_batch.argtypes = [vp, vp]
     lib.fake_release.argtypes = [vp]
     lib.nec2c_cuda_server_create.argtypes = [C.POINTER(vp), C.c_int, C.c_int, sz, C.c_int]
     lib.nec2c_cuda_server_submit.argtypes = [vp, C.POINTER(nb.Request)]
@@ -73,14 +76,14 @@ class Server:
         assert self.submit(r, m, rhs)
         return r, rhs
 
-    def volume(self, plan=None, system=None, n=0):
+    def volume(self, plan=None, system=None, n=0, restart=30):
         r = nb.Request()
         r.kind = nb.REQUEST_VOLUME
         r.plan, r.system = plan, system
-        b = np.arange(1, n + 1) * (1 + 1j)
+        b = np.arange(1, n + 1) * (1 + 1j) + len(self.keep)
         x = np.zeros(n, dtype=np.complex128)
         r.b, r.x = b.ctypes.data, x.ctypes.data
-        r.options = nb.GmresOptions(30, 300, 1e-12, 0.0)
+        r.options = nb.GmresOptions(restart, 300, 1e-12, 0.0)
         assert self.submit(r, b, x)
         return r, (b, x)
 
@@ -211,3 +214,44 @@ def test_submission_checks(fake):
     assert not fake.nec2c_cuda_server_create(C.byref(bad), 0, 0, 0, 0)
     assert b"slots must be" in fake.nec2c_cuda_last_error()
     srv.close()
+
+
+def test_queued_volume_requests_merge(fake):
+    """Continuous batching: volume requests that queue up behind busy workers
+    on systems of a registered batch run as one batched solve; the same
+    system twice, other GMRES options, or a system outside the batch run
+    alone; merged runs keep plan and batch exclusivity."""
+    fake.fake_reset(20000, 10 * GIB)
+    plans = [fake.fake_plan(40 + q) for q in range(8)]
+    hyb = [fake.fake_hybrid(p, 3) for p in plans]
+    batch = fake.fake_hybrid_batch((C.c_void_p * 8)(*hyb), 8)
+    lone = fake.fake_hybrid(fake.fake_plan(50), 2)
+    srv = Server(fake, slots=2)
+    assert fake.nec2c_cuda_server_merge_batch(srv.h, batch)
+    assert not fake.nec2c_cuda_server_merge_batch(srv.h, batch)
+    assert b"already registered" in fake.nec2c_cuda_last_error()
+    blockers = [srv.dense(64)[0] for _ in range(2)]          # both workers busy
+    reqs = [(q, srv.volume(system=hyb[q], n=43 + q)) for q in range(8)]
+    again = srv.volume(system=hyb[0], n=43)                   # system 0 a second time
+    other = srv.volume(system=hyb[5], n=48, restart=40)       # other GMRES options
+    alone = srv.volume(system=lone, n=52)                     # not in a registered batch
+    whole = srv.batch(batch, 8, sum(43 + q for q in range(8)))
+    srv.drain()
+    assert fake.fake_violations() == 0
+    assert fake.fake_merged_runs() >= 1 and fake.fake_merged_peak() >= 7
+    for q, (r, (b, x)) in reqs:
+        assert r.done and r.status, r.error
+        assert np.array_equal(x, b)
+        if r.merged > 1:
+            assert r.report.iterations == q + 1               # its own system's report
+    assert sum(1 for _, (r, _) in reqs if r.merged > 1) >= 7
+    for r, (b, x) in (again, other, alone):
+        assert r.status and np.array_equal(x, b)
+    assert not overlap(again[0], reqs[0][1][0])
+    assert other[0].merged == 1 and alone[0].merged == 1
+    members = [r for _, (r, _) in reqs] + [again[0], other[0]]
+    assert whole[0].status and all(not overlap(whole[0], r) for r in members)
+    assert all(r.status for r in blockers)
+    srv.close()
+    for o in (batch, lone, *hyb, *plans):
+        fake.fake_release(o)

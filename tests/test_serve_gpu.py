@@ -292,3 +292,45 @@ def test_submit_rejections_say_why():
             srv._submit(r, ())
     srv.drain()
     srv.close()
+
+
+def test_queued_volume_requests_merge(near_tables):
+    """Continuous batching: volume requests on the systems of a registered
+    batch that queue behind busy workers run as one batched solve.  Each
+    merged request gets its own system's result: the one the whole batch
+    gives that system solved directly (to 1e-12: per-system reductions in a
+    fixed order), converged to the request's tolerance."""
+    h, k, table = near_tables["rand_k0.3"]
+    plans = []
+    for shape, fill, seed in (((7, 6, 5), 0.6, 51), ((8, 8, 8), 1.0, 52), ((12, 9, 17), 0.5, 53),
+                              ((6, 9, 4), 0.7, 54)):
+        xyz = cases.random_lattice(shape, fill, seed)
+        p = nb.VolumePlan(shape, xyz, h, k, 3.0, table)
+        for c, e in enumerate(cases.random_eps(xyz.size // 3, seed + 9, er=(2.0, 5.0))):
+            p.set_permittivity(c, e)
+        plans.append(p)
+    batch = nb.VolumeBatch(plans)
+    rng = np.random.default_rng(61)
+    bs = [rng.standard_normal(p.n) + 1j * rng.standard_normal(p.n) for p in plans]
+    ok, direct, reps = batch.gmres(bs, rtol=1e-10, maxit=400)
+    assert ok
+    srv = nb.Server(slots=2)
+    srv.merge(batch)
+    dense = [dense_case(2048, 990 + i, k=1) for i in range(2)]
+    blockers = [srv.dense(st, rhs.copy(order="F")) for _, st, rhs in dense]   # both workers busy
+    xs = [np.zeros_like(b) for b in bs]
+    reqs = [srv.volume(p, b, x, rtol=1e-10, maxit=400) for p, b, x in zip(plans, bs, xs)]
+    srv.drain()
+    assert all(r.status for r in blockers)
+    assert max(r.merged for r in reqs) >= 2, [r.merged for r in reqs]
+    for q, (r, x) in enumerate(zip(reqs, xs)):
+        assert r.status, r.error
+        assert r.report.status == 0 and r.report.relative_residual <= 1e-10
+        if r.merged > 1:
+            assert r.report.iterations == reps[q]["iterations"]
+            assert np.max(np.abs(x - direct[q])) <= 1e-12 * np.max(np.abs(direct[q]))
+        else:
+            ok_s, xs_, rs = plans[q].gmres(bs[q], rtol=1e-10, maxit=400)
+            assert np.linalg.norm(x - xs_) <= 1e-8 * np.linalg.norm(xs_)
+    srv.close()
+    batch.close()

@@ -62,3 +62,63 @@ def test_tf32x3_update(m, n, ld):
     # Columns outside C untouched.
     assert np.array_equal(out[:, :32], a)
     assert np.array_equal(out[:, 32 + n:], w[:, 32 + n:])
+
+
+# Run in a child process with NEC2C_CUDA_TC_WAIT_CYCLES=0: every update gives
+# up its wait for the products at once, sets the error word, leaves C as it
+# was, still waits (bounded) for the products before freeing its tensor
+# memory, and returns; the context stays usable.
+TIMEOUT_CHILD = r"""
+import ctypes as C, os, sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+sys.path.insert(0, os.path.join(sys.argv[1], "tests"))
+import nec2c_b200 as nb
+from test_tc_update_gpu import pack_bt
+rng = np.random.default_rng(5)
+m, n, ld = 300, 517, 600
+w = np.zeros((m, ld), dtype=np.complex64)
+w[:, :32 + n] = (rng.standard_normal((m, 32 + n)) + 1j * rng.standard_normal((m, 32 + n))).astype(np.complex64)
+u = (rng.standard_normal((32, n)) + 1j * rng.standard_normal((32, n))).astype(np.complex64)
+hi, lo = pack_bt(u)
+dw = torch.from_numpy(w.view(np.float32)).cuda()
+dhi, dlo = torch.from_numpy(hi).cuda(), torch.from_numpy(lo).cuda()
+err = torch.zeros(1, dtype=torch.int32, device="cuda")
+torch.cuda.synchronize()
+lib = nb.load()
+f = lib.n2d_gemm_tf32x3
+f.restype = C.c_int
+f.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_longlong,
+              C.c_longlong, C.c_void_p]
+base = dw.data_ptr()
+assert f(base + 32 * 8, ld, base, ld, dhi.data_ptr(), dlo.data_ptr(), m, n, err.data_ptr())
+torch.cuda.synchronize()
+assert int(err.item()) == 1, "time-out not reported"
+assert np.array_equal(dw.cpu().numpy().view(np.complex64), w), "C changed on the time-out path"
+# The split-precision factor reads the same word and fails with the reason.
+k = 300
+a = rng.standard_normal((k, k)) + 1j * rng.standard_normal((k, k)) + np.diag(np.full(k, 10.0))
+st = np.asfortranarray(a.T.copy())
+assert nb.dense_backend_set("cuda-mixed")
+ok, _ = nb.factor_classic(st)
+assert not ok and "time-out" in nb.last_error(), nb.last_error()
+# The context is still usable: the FP64 factor runs and is right.
+assert nb.dense_backend_set("cuda")
+st = np.asfortranarray(a.T.copy())
+ok, piv = nb.factor_classic(st)
+assert ok, nb.last_error()
+print("time-out path ok")
+"""
+
+
+def test_update_timeout_reported():
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, NEC2C_CUDA_TC_WAIT_CYCLES="0")
+    r = subprocess.run([sys.executable, "-c", TIMEOUT_CHILD, root], env=env, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "time-out path ok" in r.stdout

@@ -24,9 +24,10 @@ from oracle_lib import OracleHybrid, OraclePlan
 
 pytestmark = pytest.mark.gpu
 
-# Ragged lattices: padded axes from 1 to 128 (every line length of the batch).
+# Ragged lattices: padded axes from 1 to 256 (every line length of the batch).
 LATTICES = [((7, 6, 5), 0.6, 1), ((12, 9, 17), 0.5, 2), ((1, 1, 1), 1.0, 3), ((16, 16, 16), 1.0, 4),
-            ((40, 3, 2), 0.8, 5), ((2, 31, 3), 1.0, 6), ((5, 4, 33), 0.7, 7)]
+            ((40, 3, 2), 0.8, 5), ((2, 31, 3), 1.0, 6), ((5, 4, 33), 0.7, 7), ((3, 2, 70), 0.9, 8),
+            ((66, 2, 2), 0.8, 9)]
 
 
 def rel_max(a, b):
@@ -153,9 +154,9 @@ def test_batch_refuses_bad_plan_lists(near_tables):
     assert "mix" in nb.last_error()
     with pytest.raises(RuntimeError):
         nb.VolumeBatch(plans + plans)                 # the same plan twice
-    big = nb.VolumePlan((70, 1, 1), cases.random_lattice((70, 1, 1), 1.0, 3), h, k, 3.0, table)
+    big = nb.VolumePlan((140, 1, 1), cases.random_lattice((140, 1, 1), 1.0, 3), h, k, 3.0, table)
     with pytest.raises(RuntimeError):
-        nb.VolumeBatch([big])                         # padded axis 256 > 128
+        nb.VolumeBatch([big])                         # padded axis 512 > 256
     assert "exceeds" in nb.last_error()
     b = nb.VolumeBatch(plans)
     ok, _, reps = b.gmres([np.ones(plans[0].n)], restart=31)    # restart above 30
