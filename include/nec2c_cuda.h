@@ -348,6 +348,25 @@ int nec2c_cuda_coupling_volume_to_wire(size_t segments, const double *centers_m,
                                        size_t cells, const double *cell_centers, const double *cell_sizes,
                                        double k0, double omega, int pec_ground, nec2c_cuda_complex *out);
 
+/* ------------------------------------------------------- wire MoM fill */
+/* Replaces cmset (matrix.c:48-195) for wires alone (no patches, no symmetry,
+   one block in core), the NEC-2 wire engine with the classic thin-wire
+   kernel, free space or a perfect ground: the wire-wire interaction matrix
+   of cmww (matrix.c:742-966) with the transposed fill cmset uses, plus the
+   segment loads (matrix.c:107-121).  wires->wavelength is not used.
+   Basis functions per source segment j (the reference's trio):
+   basis_first[j] .. basis_first[j+1]-1 index basis_column (0-based, < the
+   segment count) and basis_coef (3 per entry: the constant, sine and cosine
+   coefficients of that basis function on segment j).  loads: the load
+   impedance of every segment as cmset takes it (zload.zarray), or NULL.
+   cm receives rows 0 .. segments-1 of nrow values each (nrow >= segments):
+   entry (i, b) at cm[i * nrow + b], the field of basis b tested on segment i,
+   zeros beyond column segments-1.  Returns 1, or 0 with the reason in
+   nec2c_cuda_last_error(). */
+int nec2c_cuda_mom_fill(const nec2c_cuda_wire_model *wires, const size_t *basis_first, const int *basis_column,
+                        const nec2c_cuda_complex *basis_coef, const nec2c_cuda_complex *loads,
+                        nec2c_cuda_complex *cm, size_t nrow);
+
 /* ------------------------------------------------------- request server */
 /* No single counterpart in the reference: replaces the fork()ed frequency
    workers (main.c:586-760) and their memory-capped job count

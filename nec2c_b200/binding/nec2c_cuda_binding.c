@@ -20,6 +20,8 @@
  *   vie_iterative.c vie_gmres (vie_iterative.h:55-57), for the CUDA operators
  *                                              -> nec2c_cuda_gmres_plan / _hybrid
  *   concurrency.c concurrency_plan_for         -> one frequency job at a time
+ *   matrix.c cmset (wires, classic kernel, free space or perfect ground, with
+ *   the CUDA dense backend selected)           -> nec2c_cuda_mom_fill
  *
  * The two wire <-> volume coupling blocks of dielectric_wire.c are computed
  * by static code the wrapping cannot reach; the drop-in program compiles a
@@ -31,13 +33,14 @@
  * A GPU solve runs in the nec2c process itself; the reference's forked
  * frequency workers could not use the parent's CUDA context, so with a CUDA
  * backend selected the planner is held to one job (its threads still serve
- * the CPU work around the solve, e.g. the matrix fill).
+ * the CPU work around the solve).
  */
 #include <complex.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
+#include "coated_wire.h"
 #include "concurrency.h"
 #include "dense_backend.h"
 #include "dielectric_fft.h"
@@ -570,4 +573,101 @@ complex double *nec2c_binding_volume_to_wire(const dielectric_mesh_result *mesh,
   }
   free(obs); free(centers); free(sizes);
   return out;
+}
+
+/* ------------------------------------------------------- wire MoM fill */
+void __real_cmset(int nrow, complex double *cm, double rkhx, int iexkx);
+
+/* A model the GPU fill covers: wires alone, no symmetry, the matrix in core
+   (fblock's icase 1), the NEC-2 wire engine with the classic thin-wire
+   kernel, no coated segments, free space or a perfect ground. */
+static int mom_fill_covered(int nrow, int iexkx)
+{
+  int j;
+  if(!g_dense_cuda || data.n <= 0 || data.m != 0 || data.np != data.n || nrow != data.n ||
+     matpar.icase != 1 || matpar.nlast != data.n || iexkx != 0 || wire_operator_nec4_basis() ||
+     !coupling_ground_ok())
+    return 0;
+  for(j = 1; j <= data.n; ++j)
+    if(coated_wire_segment_active(j)) return 0;
+  return 1;
+}
+
+/* cmset (matrix.c:48-195) on the GPU for the models mom_fill_covered
+   accepts: the reference's own trio supplies each segment's basis
+   functions, nec2c_cuda_mom_fill the matrix with the segment loads.  Other
+   models take the reference's cmset.  A GPU failure stops the program, as
+   the reference stops on a fill error. */
+void __wrap_cmset(int nrow, complex double *cm, double rkhx, int iexkx)
+{
+  nec2c_cuda_wire_model w;
+  size_t *first = NULL, cap = 0, used = 0;
+  int *column = NULL;
+  complex double *coef = NULL, *loads = NULL;
+  int j, i, ok = 1;
+  if(!mom_fill_covered(nrow, iexkx)) {
+    __real_cmset(nrow, cm, rkhx, iexkx);
+    return;
+  }
+  /* The state cmset leaves behind (matrix.c:54-60). */
+  smat.nop = 1;
+  dataj.rkh = rkhx;
+  dataj.iexk = iexkx;
+  first = malloc(((size_t)data.n + 1) * sizeof(*first));
+  if(!first) ok = 0;
+  for(j = 1; ok && j <= data.n; ++j) {
+    first[j - 1] = used;
+    wire_operator_trio(j);
+    if(used + (size_t)segj.jsno > cap) {
+      size_t ncap = 2 * cap + (size_t)segj.jsno + 64;
+      int *nc = realloc(column, ncap * sizeof(*column));
+      complex double *nf = nc ? realloc(coef, 3 * ncap * sizeof(*coef)) : NULL;
+      if(nc) column = nc;
+      if(nf) coef = nf;
+      if(!nc || !nf) { ok = 0; break; }
+      cap = ncap;
+    }
+    for(i = 0; i < segj.jsno; ++i) {
+      column[used] = segj.jco[i] - 1;
+      coef[3 * used] = segj.ax[i];
+      coef[3 * used + 1] = segj.bx[i];
+      coef[3 * used + 2] = segj.cx[i];
+      ++used;
+    }
+  }
+  if(ok) first[data.n] = used;
+  if(ok && zload.nload != 0) {
+    loads = malloc((size_t)data.n * sizeof(*loads));
+    if(!loads) ok = 0;
+    for(j = 0; ok && j < data.n; ++j) loads[j] = zload.zarray[j];
+  }
+  if(ok) {
+    w.segments = (size_t)data.n;
+    w.x = data.x; w.y = data.y; w.z = data.z; w.length = data.si; w.radius = data.bi;
+    w.cab = data.cab; w.sab = data.sab; w.salp = data.salp;
+    w.wavelength = data.wlam; w.rkh = rkhx; w.pec_ground = gnd.ksymp == 2;
+    ok = nec2c_cuda_mom_fill(&w, first, column, coef, loads, cm, (size_t)nrow);
+    if(!ok) report_failure("MoM fill");
+  } else {
+    fprintf(stderr, "nec2c: CUDA MoM fill: out of host memory\n");
+  }
+  free(first); free(column); free(coef); free(loads);
+  if(!ok) stop(-1);
+  if(getenv("NEC2C_CUDA_FILL_CHECK")) {
+    /* Test hook: the reference's own fill of the same matrix beside the
+       GPU's, largest difference relative to the largest entry on stderr. */
+    complex double *ref = malloc((size_t)nrow * (size_t)nrow * sizeof(*ref));
+    if(ref) {
+      double diff = 0.0, big = 0.0;
+      size_t e;
+      __real_cmset(nrow, ref, rkhx, iexkx);
+      for(e = 0; e < (size_t)nrow * (size_t)nrow; ++e) {
+        if(cabs(ref[e]) > big) big = cabs(ref[e]);
+        if(cabs(ref[e] - cm[e]) > diff) diff = cabs(ref[e] - cm[e]);
+      }
+      fprintf(stderr, "nec2c: MoM fill check: order %d, largest difference %.3e of largest entry %.6e\n",
+              nrow, big > 0 ? diff / big : diff, big);
+      free(ref);
+    }
+  }
 }

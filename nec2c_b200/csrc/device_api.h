@@ -235,6 +235,16 @@ int n2d_coupling_volume_to_wire(const double *obs_dev, const double *tangent_dev
                                 double k0, double omega_eps0, int image, const double *node_dev,
                                 const double *weight_dev, double *out_dev);
 
+/* ---- wire MoM fill (matrix.c cmset / cmww) ---- */
+/* seg_dev: 8 doubles per segment as for the coupling; sup_first_dev: n + 1
+   entry offsets per basis column; sup_src_dev: the source segment of each
+   entry (increasing within a column); sup_coef_dev: 3 complex coefficients
+   per entry; loads_dev: n complex load impedances or NULL.  out_dev: n rows
+   of nrow complex values. */
+int n2d_mom_fill(const double *seg_dev, int n, double rkh, int image, const int *sup_first_dev,
+                 const int *sup_src_dev, const double *sup_coef_dev, const double *loads_dev, double *out_dev,
+                 long long nrow);
+
 #ifdef __cplusplus
 }
 #endif

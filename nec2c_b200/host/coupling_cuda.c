@@ -1,8 +1,9 @@
 /* Host side of the wire <-> volume coupling blocks (dielectric_wire.c's
  * dw_assemble_wire_to_volume and the wire-row loop of
- * dielectric_solve_conductor_coupled): argument checks, the Gauss rules, the
- * uploads and downloads around the device kernels of coupling.cu.  C, like
- * the reference. */
+ * dielectric_solve_conductor_coupled) and of the wire MoM fill (matrix.c
+ * cmset): argument checks, the Gauss rules, the basis lists, the uploads and
+ * downloads around the device kernels of coupling.cu and mom_fill.cu.  C,
+ * like the reference. */
 #include <complex.h>
 #include <float.h>
 #include <math.h>
@@ -144,5 +145,88 @@ int nec2c_cuda_coupling_volume_to_wire(size_t segments, const double *centers_m,
        n2d_download(out, out_d, segments * 3 * cells * sizeof(nec2c_cuda_complex));
   n2d_free_async(obs_d); n2d_free_async(tan_d); n2d_free_async(ctr_d); n2d_free_async(sz_d);
   n2d_free_async(node_d); n2d_free_async(wt_d); n2d_free_async(out_d);
+  return ok;
+}
+
+int nec2c_cuda_mom_fill(const nec2c_cuda_wire_model *w, const size_t *basis_first, const int *basis_column,
+                        const nec2c_cuda_complex *basis_coef, const nec2c_cuda_complex *loads,
+                        nec2c_cuda_complex *cm, size_t nrow)
+{
+  size_t n, total, i, j, k;
+  double *seg = NULL;
+  int *sup_first = NULL, *sup_src = NULL, *fill = NULL;
+  nec2c_cuda_complex *sup_coef = NULL;
+  void *seg_d = NULL, *first_d = NULL, *src_d = NULL, *coef_d = NULL, *load_d = NULL, *out_d = NULL;
+  int ok;
+  if(!w || !cm || !basis_first || w->segments == 0 || w->segments > 65536 || nrow < w->segments ||
+     !w->x || !w->y || !w->z || !w->length || !w->radius || !w->cab || !w->sab || !w->salp ||
+     !(w->rkh > 0) || (w->pec_ground != 0 && w->pec_ground != 1)) {
+    n2c_set_error("MoM fill: invalid arguments");
+    return 0;
+  }
+  n = w->segments;
+  total = basis_first[n];
+  if(basis_first[0] != 0 || total > 64 * n || (total && (!basis_column || !basis_coef))) {
+    n2c_set_error("MoM fill: invalid basis lists");
+    return 0;
+  }
+  for(j = 0; j < n; ++j)
+    if(basis_first[j + 1] < basis_first[j]) { n2c_set_error("MoM fill: invalid basis lists"); return 0; }
+  for(k = 0; k < total; ++k)
+    if(basis_column[k] < 0 || (size_t)basis_column[k] >= n || !isfinite(creal(basis_coef[3 * k])) ||
+       !isfinite(cimag(basis_coef[3 * k])) || !isfinite(creal(basis_coef[3 * k + 1])) ||
+       !isfinite(cimag(basis_coef[3 * k + 1])) || !isfinite(creal(basis_coef[3 * k + 2])) ||
+       !isfinite(cimag(basis_coef[3 * k + 2]))) {
+      n2c_set_error("MoM fill: invalid basis entry %zu", k);
+      return 0;
+    }
+  for(i = 0; i < n; ++i)
+    if(!isfinite(w->x[i]) || !isfinite(w->y[i]) || !isfinite(w->z[i]) || !(w->length[i] > 0) ||
+       !(w->radius[i] > 0) || !isfinite(w->cab[i]) || !isfinite(w->sab[i]) || !isfinite(w->salp[i]) ||
+       (loads && (!isfinite(creal(loads[i])) || !isfinite(cimag(loads[i]))))) {
+      n2c_set_error("MoM fill: invalid segment %zu", i);
+      return 0;
+    }
+  if(!n2d_device_ok()) return 0;
+  /* The per-source lists transposed to per-column lists, sources increasing
+     (the order cmset's source loop adds them in). */
+  seg = malloc(8 * n * sizeof(double));
+  sup_first = calloc(n + 1, sizeof(int));
+  fill = calloc(n, sizeof(int));
+  sup_src = malloc((total ? total : 1) * sizeof(int));
+  sup_coef = malloc((total ? total : 1) * 3 * sizeof(nec2c_cuda_complex));
+  if(!seg || !sup_first || !fill || !sup_src || !sup_coef) {
+    free(seg); free(sup_first); free(fill); free(sup_src); free(sup_coef);
+    n2c_set_error("host allocation failed");
+    return 0;
+  }
+  for(k = 0; k < total; ++k) sup_first[basis_column[k] + 1]++;
+  for(i = 0; i < n; ++i) sup_first[i + 1] += sup_first[i];
+  for(j = 0; j < n; ++j)
+    for(k = basis_first[j]; k < basis_first[j + 1]; ++k) {
+      const size_t b = (size_t)basis_column[k], at = (size_t)sup_first[b] + (size_t)fill[b]++;
+      sup_src[at] = (int)j;
+      sup_coef[3 * at] = basis_coef[3 * k];
+      sup_coef[3 * at + 1] = basis_coef[3 * k + 1];
+      sup_coef[3 * at + 2] = basis_coef[3 * k + 2];
+    }
+  for(i = 0; i < n; ++i) {
+    double *g = seg + 8 * i;
+    g[0] = w->x[i]; g[1] = w->y[i]; g[2] = w->z[i]; g[3] = w->length[i]; g[4] = w->radius[i];
+    g[5] = w->cab[i]; g[6] = w->sab[i]; g[7] = w->salp[i];
+  }
+  seg_d = upload_new(seg, 8 * n * sizeof(double));
+  first_d = upload_new(sup_first, (n + 1) * sizeof(int));
+  src_d = upload_new(sup_src, total * sizeof(int));
+  coef_d = upload_new(sup_coef, 3 * total * sizeof(nec2c_cuda_complex));
+  load_d = loads ? upload_new(loads, n * sizeof(nec2c_cuda_complex)) : NULL;
+  out_d = n2d_alloc_async(n * nrow * sizeof(nec2c_cuda_complex));
+  ok = seg_d && first_d && src_d && coef_d && (!loads || load_d) && out_d &&
+       n2d_mom_fill(seg_d, (int)n, w->rkh, w->pec_ground, first_d, src_d, coef_d, load_d, out_d,
+                    (long long)nrow) &&
+       n2d_download(cm, out_d, n * nrow * sizeof(nec2c_cuda_complex));
+  n2d_free_async(seg_d); n2d_free_async(first_d); n2d_free_async(src_d); n2d_free_async(coef_d);
+  n2d_free_async(load_d); n2d_free_async(out_d);
+  free(seg); free(sup_first); free(fill); free(sup_src); free(sup_coef);
   return ok;
 }

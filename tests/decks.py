@@ -139,13 +139,14 @@ def plane_wave_cube(directory, side_cells, freq_mhz=300.0, eps=(4.0, 0.1)):
     return path
 
 
-def run_status(binary, deck, args, timeout=900):
+def run_status(binary, deck, args, timeout=900, env=None):
     """Runs a nec2c program on a deck; returns (exit code, result JSON or None,
-    printed output)."""
+    printed output).  env: extra environment variables."""
     base = os.path.splitext(deck)[0] + "_" + os.path.basename(binary)
     out, res = base + ".out", base + ".json"
     p = subprocess.run([binary, "-i", deck, "-o", out, "--result-json", res] + list(args),
-                       capture_output=True, text=True, timeout=timeout, cwd=os.path.dirname(deck))
+                       capture_output=True, text=True, timeout=timeout, cwd=os.path.dirname(deck),
+                       env=dict(os.environ, **env) if env else None)
     doc = None
     if os.path.exists(res):
         with open(res) as f:
@@ -154,9 +155,10 @@ def run_status(binary, deck, args, timeout=900):
     return p.returncode, doc, text + p.stderr
 
 
-def dipole_array(directory, rows=8, cols=8, segments=31, seed=1, freq_mhz=300.0, pattern=True):
+def dipole_array(directory, rows=8, cols=8, segments=31, seed=1, freq_mhz=300.0, pattern=True, pec=False):
     """rows x cols parallel z-directed half-wave dipoles at 0.5 lambda pitch in
-    the xy plane, radius lambda/1000, free space.  Element (3, 3) (the last
+    the xy plane, radius lambda/1000, free space (pec: raised 0.3 lambda
+    above a perfectly conducting ground, GN 1).  Element (3, 3) (the last
     row or column of a smaller array) is driven
     with 1 V at its centre segment; every other element carries a seeded
     resistive load of 50 +- 10 ohm at its centre segment.  Returns the deck
@@ -164,6 +166,7 @@ def dipole_array(directory, rows=8, cols=8, segments=31, seed=1, freq_mhz=300.0,
     lam = C0 / (freq_mhz * 1e6)
     rng = np.random.default_rng(seed)
     mid = segments // 2 + 1
+    z0 = 0.55 * lam if pec else 0.0
     lines = ["CM %dx%d dipole array, seed %d" % (rows, cols, seed), "CE"]
     tag = 0
     driven = None
@@ -173,18 +176,18 @@ def dipole_array(directory, rows=8, cols=8, segments=31, seed=1, freq_mhz=300.0,
             x, y = c * 0.5 * lam, r * 0.5 * lam
             # %.12g keeps a card within NEC's 132-character line limit.
             lines.append("GW %d %d %.12g %.12g %.12g %.12g %.12g %.12g %.12g"
-                         % (tag, segments, x, y, -lam / 4, x, y, lam / 4, lam / 1000))
+                         % (tag, segments, x, y, z0 - lam / 4, x, y, z0 + lam / 4, lam / 1000))
             if (r, c) == (min(3, rows - 1), min(3, cols - 1)):
                 driven = tag
-    lines += ["GE 0"]
+    lines += ["GE 1" if pec else "GE 0"]
     tag = 0
     for r in range(rows):
         for c in range(cols):
             tag += 1
             if tag != driven:
                 lines.append("LD 0 %d %d %d %r 0 0" % (tag, mid, mid, float(rng.uniform(40.0, 60.0))))
-    lines += ["FR 0 1 0 0 %r" % freq_mhz, "EX 0 %d %d 0 1 0" % (driven, mid),
-              PATTERN if pattern else "XQ", "EN", ""]
+    lines += ["FR 0 1 0 0 %r" % freq_mhz] + (["GN 1"] if pec else []) + ["EX 0 %d %d 0 1 0" % (driven, mid),
+              (PATTERN_UPPER if pec else PATTERN) if pattern else "XQ", "EN", ""]
     os.makedirs(directory, exist_ok=True)
     path = os.path.join(directory, "dipole_array.nec")
     with open(path, "w") as f:
@@ -192,14 +195,43 @@ def dipole_array(directory, rows=8, cols=8, segments=31, seed=1, freq_mhz=300.0,
     return path
 
 
-def run(binary, deck, args, timeout=900):
-    """Runs a nec2c program on a deck; returns (result JSON, wall seconds, stderr)."""
+def junctions(directory, freq_mhz=300.0, pec=False):
+    """Wires meeting at junctions, for the basis functions a junction gives
+    (NEC's trio over several connected segments): a vertical half-wave
+    dipole in two wires, two horizontal quarter-wave arms from its centre
+    (a four-wire junction), a bent wire continuing the first arm, a short
+    stub off the second, radius lambda/500; 1 V at the lower wire's middle
+    segment, a 75 ohm load on the bent wire.  pec: raised 0.4 lambda above a
+    perfectly conducting ground (GN 1).  Returns the deck path."""
+    lam = C0 / (freq_mhz * 1e6)
+    z0 = 0.4 * lam if pec else 0.0
+    a = lam / 500
+    q = lam / 4
+    wires = [(1, 9, 0, 0, z0 - q, 0, 0, z0), (2, 9, 0, 0, z0, 0, 0, z0 + q),
+             (3, 7, 0, 0, z0, q, 0, z0), (4, 7, 0, 0, z0, 0, q, z0),
+             (5, 5, q, 0, z0, q, 0.6 * q, z0 + 0.3 * q), (6, 3, 0, q, z0, -0.2 * q, q, z0 - 0.25 * q)]
+    lines = ["CM junctions", "CE"]
+    for tag, nseg, x1, y1, z1, x2, y2, z2 in wires:
+        lines.append("GW %d %d %.12g %.12g %.12g %.12g %.12g %.12g %.12g" % (tag, nseg, x1, y1, z1, x2, y2, z2, a))
+    lines += ["GE 1" if pec else "GE 0", "LD 0 5 3 3 75 0 0", "FR 0 1 0 0 %r" % freq_mhz]
+    lines += (["GN 1"] if pec else []) + ["EX 0 1 5 0 1 0", PATTERN_UPPER if pec else PATTERN, "EN", ""]
+    os.makedirs(directory, exist_ok=True)
+    path = os.path.join(directory, "junctions.nec")
+    with open(path, "w") as f:
+        f.write("\n".join(lines))
+    return path
+
+
+def run(binary, deck, args, timeout=900, env=None):
+    """Runs a nec2c program on a deck; returns (result JSON, wall seconds,
+    stderr).  env: extra environment variables."""
     import time
     base = os.path.splitext(deck)[0] + "_" + os.path.basename(binary)
     out, res = base + ".out", base + ".json"
     t0 = time.perf_counter()
     p = subprocess.run([binary, "-i", deck, "-o", out, "--result-json", res] + list(args),
-                       capture_output=True, text=True, timeout=timeout, cwd=os.path.dirname(deck))
+                       capture_output=True, text=True, timeout=timeout, cwd=os.path.dirname(deck),
+                       env=dict(os.environ, **env) if env else None)
     wall = time.perf_counter() - t0
     if p.returncode != 0:
         raise RuntimeError("%s failed (%d): %s" % (os.path.basename(binary), p.returncode, p.stderr[-2000:]))
