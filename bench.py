@@ -1398,6 +1398,7 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
             groups.append((kinds[i], subs))
         srv.drain()
         lat, merged = [], []
+        service = {"dense_s": 0.0, "volume_s": 0.0}
         for dense_req, subs in groups:
             for r in subs:
                 if not r.status or (r.kind != nb.REQUEST_DENSE and r.report.status != 0):
@@ -1405,6 +1406,11 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
                                                                                     r.report.status))
                 if not dense_req:
                     merged.append(r.merged)
+                # Worker time per kind (merged requests share one run: counted once).
+                if dense_req:
+                    service["dense_s"] += r.finished_s - r.started_s
+                elif r.merged <= 1 or r.footprint:
+                    service["volume_s"] += r.finished_s - r.started_s
             lat.append(1e3 * (max(r.finished_s for r in subs) - min(r.queued_s for r in subs)))
         first = min(r.queued_s for _, subs in groups for r in subs)
         last = max(r.finished_s for _, subs in groups for r in subs)
@@ -1414,7 +1420,8 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
         return {"requests": nreq, "solves": solves, "solves_per_s": solves / (last - first),
                 "requests_per_s": nreq / (last - first), "makespan_s": last - first,
                 "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
-                "volume_solves_merged_mean": float(np.mean(merged)) if merged else None}
+                "volume_solves_merged_mean": float(np.mean(merged)) if merged else None,
+                "worker_time": service}
 
     t0 = time.perf_counter()
     m32 = build_models(True)
