@@ -53,6 +53,8 @@ def parse():
                     help="JSON file of the c2 plans' FFT pass schedules: written by the first run "
                          "that names it, pinned by later runs (a run under ncu would otherwise "
                          "tune on serialised, slowed launches)")
+    ap.add_argument("--lu-order", type=int, default=1984,
+                    help="lu profiling mode: order of the seeded MoM-like matrix (config 1: 1984)")
     ap.add_argument("--requests", type=int, default=240,
                     help="serving_c4 profiling mode: requests in the stream (config 4 names 10,000)")
     ap.add_argument("--planes", type=int, choices=[0, 1], default=None,
@@ -556,7 +558,7 @@ def run_ours(args, rank, world, local_rank):
     # 192-system dipole-plus-cube sweep, ragged batch of plans.
     volume_batch = volume_batch_bench(nb, torch, stream)
     # Mixed dense and volume serving stream (bounded), both forms.
-    serving = serving_bench(nb, torch) if world == 1 else None
+    serving = serving_stream_c4(nb, torch) if world == 1 else None
     # Config 0 end to end through the drop-in program, and its two coupling
     # blocks through the C ABI (rank 0 only).
     deck_c0 = deck_bench() if rank == 0 else None
@@ -659,8 +661,7 @@ def profile_driver(args, lib, nb, torch, stream, plan_m, plan_d, w):
     return 0
 
 
-def c1_matrix():
-    n = 1984
+def c1_matrix(n=1984):
     rng = np.random.default_rng(1)
     a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
     a += np.diag(np.full(n, 0.5 * math.sqrt(n)))
@@ -725,7 +726,7 @@ def device_factor(nb, torch, stream, a, form, reps):
 
 
 def lu_driver(args, nb, torch, stream):
-    a = c1_matrix()
+    a = c1_matrix(args.lu_order)
     out = {form: device_factor(nb, torch, stream, a, form, max(1, args.steps)) for form in ("cuda", "cuda-mixed")}
     print(json.dumps({"profile": "lu", "order": a.shape[0],
                       "device_factor_ms": {f: t[0] for f, t in out.items()},
@@ -1378,6 +1379,7 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
             srv.dense(st, rhs.copy(order="F"))
         srv.drain()
         groups = []
+        sols = {}   # a solution per (kind, model, frequency), for the error between forms
         t0 = time.perf_counter()
         for i in range(nreq):
             if gaps is not None:
@@ -1386,15 +1388,21 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
                     time.sleep(min(1e-3, max(0.0, target - time.perf_counter())))
             subs = []
             if kinds[i]:
-                mats = dense_pool[picks[i] % len(dense_pool)]
+                pi = picks[i] % len(dense_pool)
+                mats = dense_pool[pi]
                 for f in fsets[i]:
                     st, rhs = mats[f % len(mats)]
-                    subs.append(srv.dense(st, rhs.copy(order="F")))
+                    out = rhs.copy(order="F")
+                    subs.append(srv.dense(st, out))
+                    sols[("dense", pi, int(f) % len(mats))] = out
             else:
-                mdl = models[picks[i] % len(models)]
+                mi = picks[i] % len(models)
+                mdl = models[mi]
                 for f in fsets[i]:
                     b = mdl["rhs"][f]
-                    subs.append(srv.volume(mdl["systems"][f], b, np.zeros_like(b), rtol=1e-6, maxit=3000))
+                    x = np.zeros_like(b)
+                    subs.append(srv.volume(mdl["systems"][f], b, x, rtol=1e-6, maxit=3000))
+                    sols[("volume", mi, int(f))] = x
             groups.append((kinds[i], subs))
         srv.drain()
         lat, merged = [], []
@@ -1421,7 +1429,7 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
                 "requests_per_s": nreq / (last - first), "makespan_s": last - first,
                 "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                 "volume_solves_merged_mean": float(np.mean(merged)) if merged else None,
-                "worker_time": service}
+                "worker_time": service}, sols
 
     t0 = time.perf_counter()
     m32 = build_models(True)
@@ -1432,11 +1440,30 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
            "slots": slots, "setup_s": time.perf_counter() - t0,
            "device_gb_in_use_after_setup": (lambda f: (f[1] - f[0]) / 1e9)(torch.cuda.mem_get_info())}
     sat = {}
-    sat["mixed"] = max((run(m32, False, slots, None, True) for _ in range(2)), key=lambda r: r["solves_per_s"])
-    sat["mixed_unmerged"] = run(m32, False, slots, None, False)
-    sat["mixed_split_lu"] = run(m32, True, slots, None, True)
-    sat["fp64"] = max((run(m64, False, slots, None, True) for _ in range(2)), key=lambda r: r["solves_per_s"])
-    plain = run(m64, False, 1, None, False)
+    runs = [run(m32, False, slots, None, True) for _ in range(2)]
+    sat["mixed"], sols_mixed = max(runs, key=lambda r: r[0]["solves_per_s"])
+    sat["mixed_unmerged"], _ = run(m32, False, slots, None, False)
+    sat["mixed_split_lu"], sols_split = run(m32, True, slots, None, True)
+    runs = [run(m64, False, slots, None, True) for _ in range(2)]
+    sat["fp64"], sols_fp64 = max(runs, key=lambda r: r[0]["solves_per_s"])
+    plain, sols_plain = run(m64, False, 1, None, False)
+
+    def rel_err(a, b):
+        return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+    def worst(sols, ref, kind):
+        errs = [rel_err(v, ref[k]) for k, v in sols.items() if k[0] == kind and k in ref]
+        return max(errs) if errs else None
+    # Current error of each form against the plain FP64 form on the same
+    # systems (volume: GMRES to rtol 1e-6 in both, so the difference is the
+    # solver's tolerance as much as the precision).
+    out["error_vs_plain_fp64"] = {
+        "mixed": {"volume_current": worst(sols_mixed, sols_plain, "volume"),
+                  "dense_current": worst(sols_mixed, sols_plain, "dense")},
+        "mixed_split_lu": {"volume_current": worst(sols_split, sols_plain, "volume"),
+                           "dense_current": worst(sols_split, sols_plain, "dense")},
+        "fp64_merged": {"volume_current": worst(sols_fp64, sols_plain, "volume"),
+                        "dense_current": worst(sols_fp64, sols_plain, "dense")}}
     out["saturation"] = sat
     out["plain_fp64_one_at_a_time"] = plain
     out["mixed_vs_plain_fp64"] = sat["mixed"]["solves_per_s"] / plain["solves_per_s"]
@@ -1446,7 +1473,7 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
     for frac in rates:
         rate = frac * sat["mixed"]["requests_per_s"]
         gaps = np.cumsum(np.random.default_rng(13).exponential(1.0 / rate, nreq))
-        res = run(m32, False, slots, gaps, True)
+        res, _ = run(m32, False, slots, gaps, True)
         res["offered_requests_per_s"] = rate
         res["fraction_of_saturation"] = frac
         sweep.append(res)

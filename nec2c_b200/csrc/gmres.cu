@@ -10,6 +10,7 @@
 // so iterations after convergence cost only a launch.  x += D^-1 (V y) and
 // the true residual close the cycle.  Reductions are deterministic (fixed-order
 // block partials), so results are bitwise reproducible run to run.
+#include <stdlib.h>
 #include <float.h>
 #include <math.h>
 #include <string.h>
@@ -282,6 +283,7 @@ __device__ void finish_step(GmBuffers &b, GmState *st, int m, int j, double afte
 // element group q / kk; the w chunk sits in shared memory.
 template <int P>
 __global__ void __launch_bounds__(1024) cgs_dots_kernel(GmBuffers b, long long n, int m, int j) {
+  pdl_begin();
   GmState *st = b.st;
   if (!st->active || (P == 1 && !st->reorth)) return;
   if (P == 0 && st->flag) {
@@ -369,6 +371,7 @@ __global__ void __launch_bounds__(1024) cgs_dots_kernel(GmBuffers b, long long n
 // either requests the reorthogonalisation pass or finishes the column.
 template <int P>
 __global__ void __launch_bounds__(256) cgs_update_kernel(GmBuffers b, long long n, int m, int j) {
+  pdl_begin();
   GmState *st = b.st;
   if (!st->active || (P == 1 && !st->reorth)) return;
   const int kk = j + 1;
@@ -404,6 +407,7 @@ __global__ void __launch_bounds__(256) cgs_update_kernel(GmBuffers b, long long 
 // v_{j+1} = w / ||w|| after a CGS2 step (skipped on breakdown and once the
 // cycle has ended: only v_0..v_{used-1} enter the update).
 __global__ void normalize_kernel(GmBuffers b, long long n, int j) {
+  pdl_begin();
   GmState *st = b.st;
   if (!st->active || !st->normalize) return;
   const double inv = st->after;
@@ -614,13 +618,18 @@ static int enqueue_inner(const OpView &o, GmWork *w) {
     if (use_cgs) {
       const unsigned gb = (unsigned)n2c_sm_count();
       const unsigned ub = grid1(n) < 4096 ? grid1(n) : 4096;
-      cgs_dots_kernel<0><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
-      cgs_update_kernel<0><<<ub, 256, 0, n2c_stream()>>>(b, n, (int)m, j);
-      cgs_dots_kernel<1><<<gb, 1024, CGS_SMEM, n2c_stream()>>>(b, n, (int)m, j);
-      cgs_update_kernel<1><<<ub, 256, 0, n2c_stream()>>>(b, n, (int)m, j);
-      normalize_kernel<<<grid1(n), 256, 0, n2c_stream()>>>(b, n, j);
-      ok = n2c_check_launch("cgs sweeps");
-      n2c_count_launch(4);
+      // Programmatic dependent launches when NEC2C_CUDA_PDL_GMRES=1: each
+      // sweep's launch overlaps the previous kernel's last wave (the kernels
+      // wait for it first).
+      static const bool pdl = [] {
+        const char *v = getenv("NEC2C_CUDA_PDL_GMRES");
+        return v && v[0] == '1';
+      }();
+      ok = n2c_launch_pdl(pdl, cgs_dots_kernel<0>, dim3(gb), dim3(1024), CGS_SMEM, "cgs dots", b, n, (int)m, j) &&
+           n2c_launch_pdl(pdl, cgs_update_kernel<0>, dim3(ub), dim3(256), 0, "cgs update", b, n, (int)m, j) &&
+           n2c_launch_pdl(pdl, cgs_dots_kernel<1>, dim3(gb), dim3(1024), CGS_SMEM, "cgs dots", b, n, (int)m, j) &&
+           n2c_launch_pdl(pdl, cgs_update_kernel<1>, dim3(ub), dim3(256), 0, "cgs update", b, n, (int)m, j) &&
+           n2c_launch_pdl(pdl, normalize_kernel, dim3(grid1(n)), dim3(256), 0, "cgs normalize", b, n, j);
     } else {
       ok = w->arnoldi(b, n, (int)m, j, w->blocks, w->threads);
     }

@@ -1288,7 +1288,8 @@ static int launch_gemm(float2 *a, long long ld, long long k0, int kb, long long 
   if (cols <= 0 || rows <= 0) return 1;
   const long long r2 = 2 * (c_first - k0 - kb);
   return n2c_tc_update((float *)(a + (k0 + kb) * ld + c_first), ld, (const float *)(a + (k0 + kb) * ld + k0), ld,
-                       w.bt_hi + r2 * (2 * KB), w.bt_lo + r2 * (2 * KB), rows, cols, &w.st->error, s);
+                       w.bt_hi + r2 * (2 * KB), w.bt_lo + r2 * (2 * KB), rows, cols, &w.st->error, s,
+                       n2c_tc_form(rows, cols));
 }
 
 // The blocked factorisation; the status must be zero on entry.  Reads the

@@ -1,5 +1,6 @@
 // Runtime plumbing of the nec2c CUDA backend: per-thread error text, the
 // stream work is enqueued on, device buffers and a launch counter.
+#include <stdlib.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
@@ -28,6 +29,14 @@ extern "C" void n2d_set_gate(const int *gate_dev) { g_gate = gate_dev; }
 const int *n2c_gate() { return g_gate; }
 void n2c_count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 extern "C" unsigned long long n2d_launch_count(void) { return g_launches.load(); }
+
+bool n2c_pdl_enabled() {
+  static const bool on = [] {
+    const char *v = getenv("NEC2C_CUDA_PDL");
+    return !(v && v[0] == '0');
+  }();
+  return on;
+}
 
 int n2c_check_launch(const char *what) {
   cudaError_t e = cudaGetLastError();

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+extern "C" void n2c_set_error(const char *fmt, ...);
 cudaStream_t n2c_stream();
 // Device int that operator kernels check first: when it reads 0 they return
 // at once (set by the GMRES driver around its inner iterations; NULL = off).
@@ -10,10 +11,43 @@ void n2c_count_launch(unsigned n);
 // Checks cudaGetLastError after a launch; counts the launch on success.
 int n2c_check_launch(const char *what);
 int n2c_sm_count();
+// Programmatic dependent launch in use (NEC2C_CUDA_PDL=0 turns it off; read
+// once).  Kernels launched with it must call pdl_begin() (common.cuh) first.
+bool n2c_pdl_enabled();
+
+// Launches k on the current stream, with programmatic stream serialisation
+// when enable and n2c_pdl_enabled(); checks and counts the launch like
+// n2c_check_launch.
+template <typename... KArgs, typename... Args>
+int n2c_launch_pdl(bool enable, void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, const char *what,
+                   Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = n2c_stream();
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = enable && n2c_pdl_enabled() ? 1 : 0;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    n2c_set_error("%s launch failed: %s", what, cudaGetErrorString(e));
+    return 0;
+  }
+  return n2c_check_launch(what);
+}
 // Split-precision (3xTF32) tensor-core trailing update of the FP32 LU on
 // stream s; see lu_tc.cu.
+// form: N2C_TC_STAGED (thread-staged operands, one tile per CTA) or
+// N2C_TC_PERSISTENT (TMA-fed, one CTA per SM over a band's tiles).
+enum { N2C_TC_STAGED = 0, N2C_TC_PERSISTENT = 1 };
 int n2c_tc_update(float *C, long long ldc, const float *A, long long lda, const float *bt_hi, const float *bt_lo,
-                  long long M, long long N, int *error, cudaStream_t s);
+                  long long M, long long N, int *error, cudaStream_t s, int form);
+// The form the LU's trailing update of an M x N block takes.
+int n2c_tc_form(long long M, long long N);
 
 // Deterministic block-partial reduction: each block stores its partial in
 // partials[blockIdx.x]; the block that arrives last (ticket counter) sums the

@@ -1,4 +1,6 @@
-"""Tensor-core trailing update of the split-precision LU (n2d_gemm_tf32x3):
+"""Tensor-core trailing update of the split-precision LU, both forms
+(n2d_gemm_tf32x3: operands staged by the threads, one tile per CTA;
+n2d_gemm_tf32x3_persistent: TMA-fed, one CTA per SM over a band's tiles):
 C -= A B for complex FP32 blocks through tcgen05 3xTF32, against a float64
 numpy product.  The 3xTF32 split keeps the result at FP32 accuracy: the
 tolerance is 2e-6 relative to the largest |A||B| term."""
@@ -28,8 +30,10 @@ def pack_bt(u):
     return np.ascontiguousarray(hi), np.ascontiguousarray(lo)
 
 
-@pytest.mark.parametrize("m,n,ld", [(128, 128, 256), (300, 517, 600), (1, 3, 64), (1000, 1000, 1040)])
-def test_tf32x3_update(m, n, ld):
+@pytest.mark.parametrize("form", ["n2d_gemm_tf32x3", "n2d_gemm_tf32x3_persistent"])
+@pytest.mark.parametrize("m,n,ld", [(128, 128, 256), (300, 517, 600), (1, 3, 64), (1000, 1000, 1040),
+                                    (1100, 1300, 1340), (2047, 1024, 1090)])
+def test_tf32x3_update(m, n, ld, form):
     import torch
     rng = np.random.default_rng(m + n)
     a = (rng.standard_normal((m, 32)) + 1j * rng.standard_normal((m, 32))).astype(np.complex64)
@@ -46,7 +50,7 @@ def test_tf32x3_update(m, n, ld):
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     torch.cuda.synchronize()
     lib = nb.load()
-    f = lib.n2d_gemm_tf32x3
+    f = getattr(lib, form)
     f.restype = C.c_int
     f.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_longlong,
                   C.c_longlong, C.c_void_p]
@@ -77,25 +81,27 @@ sys.path.insert(0, os.path.join(sys.argv[1], "tests"))
 import nec2c_b200 as nb
 from test_tc_update_gpu import pack_bt
 rng = np.random.default_rng(5)
-m, n, ld = 300, 517, 600
-w = np.zeros((m, ld), dtype=np.complex64)
-w[:, :32 + n] = (rng.standard_normal((m, 32 + n)) + 1j * rng.standard_normal((m, 32 + n))).astype(np.complex64)
-u = (rng.standard_normal((32, n)) + 1j * rng.standard_normal((32, n))).astype(np.complex64)
-hi, lo = pack_bt(u)
-dw = torch.from_numpy(w.view(np.float32)).cuda()
-dhi, dlo = torch.from_numpy(hi).cuda(), torch.from_numpy(lo).cuda()
-err = torch.zeros(1, dtype=torch.int32, device="cuda")
-torch.cuda.synchronize()
 lib = nb.load()
-f = lib.n2d_gemm_tf32x3
-f.restype = C.c_int
-f.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_longlong,
-              C.c_longlong, C.c_void_p]
-base = dw.data_ptr()
-assert f(base + 32 * 8, ld, base, ld, dhi.data_ptr(), dlo.data_ptr(), m, n, err.data_ptr())
-torch.cuda.synchronize()
-assert int(err.item()) == 1, "time-out not reported"
-assert np.array_equal(dw.cpu().numpy().view(np.complex64), w), "C changed on the time-out path"
+for name in ("n2d_gemm_tf32x3", "n2d_gemm_tf32x3_persistent"):
+    f = getattr(lib, name)
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_longlong,
+                  C.c_longlong, C.c_void_p]
+for name, (m, n, ld) in (("n2d_gemm_tf32x3", (300, 517, 600)), ("n2d_gemm_tf32x3_persistent", (1100, 1300, 1340))):
+    f = getattr(lib, name)
+    w = np.zeros((m, ld), dtype=np.complex64)
+    w[:, :32 + n] = (rng.standard_normal((m, 32 + n)) + 1j * rng.standard_normal((m, 32 + n))).astype(np.complex64)
+    u = (rng.standard_normal((32, n)) + 1j * rng.standard_normal((32, n))).astype(np.complex64)
+    hi, lo = pack_bt(u)
+    dw = torch.from_numpy(w.view(np.float32)).cuda()
+    dhi, dlo = torch.from_numpy(hi).cuda(), torch.from_numpy(lo).cuda()
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    base = dw.data_ptr()
+    assert f(base + 32 * 8, ld, base, ld, dhi.data_ptr(), dlo.data_ptr(), m, n, err.data_ptr())
+    torch.cuda.synchronize()
+    assert int(err.item()) == 1, "time-out not reported"
+    assert np.array_equal(dw.cpu().numpy().view(np.complex64), w), "C changed on the time-out path"
 # The split-precision factor reads the same word and fails with the reason.
 k = 300
 a = rng.standard_normal((k, k)) + 1j * rng.standard_normal((k, k)) + np.diag(np.full(k, 10.0))
