@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--planes", type=int, choices=[0, 1], default=None,
                     help="profiling driver: pin the fused yz-plane passes on (1) or off (0) in both "
                          "c2 plans instead of the tuner's choice")
-    ap.add_argument("--only", choices=["matvec", "solve", "lu", "serving", "serving_c4", "volume_batch",
+    ap.add_argument("--only", choices=["matvec", "solve", "lu", "lu_batch", "serving", "serving_c4", "volume_batch",
                                        "coupling"],
                     help="profiling driver: build the plans, run --steps FP32 and FP64 products "
                          "(matvec) or --steps mixed solves (solve), or factor the 1984-unknown dense "
@@ -401,6 +401,9 @@ def run_ours(args, rank, world, local_rank):
     lib.nec2c_cuda_set_stream(C.c_void_p(stream.cuda_stream))
     if args.only == "lu":
         return lu_driver(args, nb, torch, stream)
+    if args.only == "lu_batch":
+        print(json.dumps({"profile": "lu_batch", "lockstep_factor": lockstep_factor_bench(nb, torch, stream)}))
+        return 0
     if args.only == "serving":
         print(json.dumps({"profile": "serving", "serving_c4": serving_bench(nb, torch)}))
         return 0
@@ -732,6 +735,56 @@ def lu_driver(args, nb, torch, stream):
                       "device_factor_ms": {f: t[0] for f, t in out.items()},
                       "device_solve_ms": {f: t[1] for f, t in out.items()}}))
     return 0
+
+
+def lockstep_factor_bench(nb, torch, stream, orders=(250, 1000, 2608), counts=(1, 4, 16), reps=3):
+    """Lockstep batch of FP64 factorisations against one factorisation at a
+    time, on device-resident copies of seeded MoM-like matrices: device ms per
+    batch (CUDA events, fastest of reps after a warm-up) and the achieved
+    factorisation rate (8n^3/3 flops each)."""
+    lib = nb.load()
+    single = lib.n2d_lu_factor
+    single.restype, single.argtypes = C.c_int, [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_int,
+                                                C.c_int, C.POINTER(C.c_int)]
+    batch = lib.n2d_lu_factor_batch
+    batch.restype, batch.argtypes = C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                              C.c_void_p]
+    out = []
+    for n in orders:
+        src = torch.from_numpy(c1_matrix(n)).cuda()
+        for k in counts:
+            work = [src.clone() for _ in range(k)]
+            piv = [torch.zeros(n, dtype=torch.int32, device="cuda") for _ in range(k)]
+            ptrs = (C.c_void_p * k)(*[w.data_ptr() for w in work])
+            pps = (C.c_void_p * k)(*[p.data_ptr() for p in piv])
+            ns = (C.c_longlong * k)(*([n] * k))
+            info = (C.c_int * k)()
+
+            def timed(fn):
+                best = None
+                for i in range(reps + 1):
+                    for w in work:
+                        w.copy_(src)
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    if not fn():
+                        raise RuntimeError("factor failed: " + nb.last_error())
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                    if i:
+                        t = e0.elapsed_time(e1)
+                        best = t if best is None else min(best, t)
+                return best
+            one = C.c_int(0)
+            t_single = timed(lambda: all(single(w.data_ptr(), n, n, p.data_ptr(), 0, 0, C.byref(one))
+                                         for w, p in zip(work, piv)))
+            t_batch = timed(lambda: batch(ptrs, ns, ns, pps, k, 0, info))
+            flops = k * 8.0 * n ** 3 / 3
+            out.append({"order": n, "systems": k, "one_at_a_time_ms": t_single, "lockstep_ms": t_batch,
+                        "speedup": t_single / t_batch, "lockstep_tflops": flops / (t_batch * 1e-3) / 1e12})
+            del work, piv
+    return out
 
 
 def deck_bench():
@@ -1253,6 +1306,10 @@ def serving_bench(nb, torch):
     return out
 
 
+# Most dense requests of one size class in one lockstep batch.
+DENSE_MERGE = 16
+
+
 def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0.5, 0.7, 0.9, 1.1),
                       lattices=(8, 16, 24, 32, 48), seed=11):
     """BASELINE config 4 shaped stream through the request server.
@@ -1271,9 +1328,11 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
     Forms (16 workers): `mixed` = FP32 transforms with the FP64 LU (the split
     LU's refinement only adds latency at these orders), the server merging
     queued volume requests on one model's frequencies into one batched solve
-    (each model's 16 frequency systems are one registered batch);
-    `mixed_unmerged` = the same without merging; `mixed_split_lu` = merged,
-    with the split-precision LU; `fp64` = FP64 transforms, merged;
+    (each model's 16 frequency systems are one registered batch) and queued
+    dense requests of one size class into one lockstep factorisation (at most
+    DENSE_MERGE); `mixed_unmerged` = the same without merging;
+    `mixed_split_lu` = volume requests merged, with the split-precision LU
+    (its dense requests run one at a time); `fp64` = FP64 transforms, merged;
     `plain_fp64_one_at_a_time` = FP64, one worker, no merging.  Saturation:
     everything queued at once.  Poisson: request arrivals at the given
     fractions of the mixed form's saturated request rate (the sweep shows
@@ -1365,11 +1424,15 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
     # The frequencies each request asks for: F distinct ones of its model's 16.
     fsets = [np.sort(rng.choice(len(freqs), int(F), replace=False)) for F in fsel]
 
-    def run(models, split, slots_, gaps, merge):
+    def run(models, split, slots_, gaps, merge, only=None):
         srv = nb.Server(slots=slots_, split=split)
         if merge:
             for mdl in models:
                 srv.merge(mdl["batch"])
+            # Queued dense requests of one size class factor in lockstep (the
+            # FP64 form; a split-precision server keeps them one at a time).
+            if not split:
+                srv.merge_dense(DENSE_MERGE)
         # Warm every worker (stream state, kernel attributes) and every system.
         for mdl in models:
             for hs, b in zip(mdl["systems"], mdl["rhs"]):
@@ -1387,6 +1450,8 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
                 while time.perf_counter() < target:
                     time.sleep(min(1e-3, max(0.0, target - time.perf_counter())))
             subs = []
+            if only is not None and bool(kinds[i]) != only:
+                continue
             if kinds[i]:
                 pi = picks[i] % len(dense_pool)
                 mats = dense_pool[pi]
@@ -1403,32 +1468,35 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
                     x = np.zeros_like(b)
                     subs.append(srv.volume(mdl["systems"][f], b, x, rtol=1e-6, maxit=3000))
                     sols[("volume", mi, int(f))] = x
-            groups.append((kinds[i], subs))
+            groups.append((kinds[i], subs, i))
         srv.drain()
-        lat, merged = [], []
+        lat, merged, dmerged = [], [], []
         service = {"dense_s": 0.0, "volume_s": 0.0}
-        for dense_req, subs in groups:
+        per_size = {}
+        for dense_req, subs, i in groups:
+            size = ("order %d" % orders[picks[i] % len(dense_pool)] if dense_req
+                    else "%d^3" % specs[picks[i] % len(models)]["n"])
             for r in subs:
                 if not r.status or (r.kind != nb.REQUEST_DENSE and r.report.status != 0):
                     raise RuntimeError("c4 stream request failed: %s (status %d)" % (r.error.decode(),
                                                                                     r.report.status))
-                if not dense_req:
-                    merged.append(r.merged)
+                (dmerged if dense_req else merged).append(r.merged)
                 # Worker time per kind (merged requests share one run: counted once).
-                if dense_req:
-                    service["dense_s"] += r.finished_s - r.started_s
-                elif r.merged <= 1 or r.footprint:
-                    service["volume_s"] += r.finished_s - r.started_s
+                if r.merged <= 1 or r.footprint:
+                    service["dense_s" if dense_req else "volume_s"] += r.finished_s - r.started_s
+                    per_size[size] = per_size.get(size, 0.0) + r.finished_s - r.started_s
             lat.append(1e3 * (max(r.finished_s for r in subs) - min(r.queued_s for r in subs)))
-        first = min(r.queued_s for _, subs in groups for r in subs)
-        last = max(r.finished_s for _, subs in groups for r in subs)
-        solves = int(sum(len(subs) for _, subs in groups))
+        first = min(r.queued_s for _, subs, _ in groups for r in subs)
+        last = max(r.finished_s for _, subs, _ in groups for r in subs)
+        solves = int(sum(len(subs) for _, subs, _ in groups))
         srv.close()
         lat.sort()
-        return {"requests": nreq, "solves": solves, "solves_per_s": solves / (last - first),
-                "requests_per_s": nreq / (last - first), "makespan_s": last - first,
+        service["per_size_s"] = per_size
+        return {"requests": len(groups), "solves": solves, "solves_per_s": solves / (last - first),
+                "requests_per_s": len(groups) / (last - first), "makespan_s": last - first,
                 "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                 "volume_solves_merged_mean": float(np.mean(merged)) if merged else None,
+                "dense_solves_merged_mean": float(np.mean(dmerged)) if dmerged else None,
                 "worker_time": service}, sols
 
     t0 = time.perf_counter()
@@ -1466,6 +1534,14 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
                         "dense_current": worst(sols_fp64, sols_plain, "dense")}}
     out["saturation"] = sat
     out["plain_fp64_one_at_a_time"] = plain
+    # Each kind of request alone (the same requests), both forms: where the
+    # mixed stream's time goes.
+    out["by_kind"] = {}
+    for name, only in (("dense", True), ("volume", False)):
+        mx, _ = run(m32, False, slots, None, True, only)
+        pl, _ = run(m64, False, 1, None, False, only)
+        out["by_kind"][name] = {"mixed": mx, "plain_fp64_one_at_a_time": pl,
+                                "mixed_vs_plain_fp64": mx["solves_per_s"] / pl["solves_per_s"]}
     out["mixed_vs_plain_fp64"] = sat["mixed"]["solves_per_s"] / plain["solves_per_s"]
     out["mixed_split_lu_vs_plain_fp64"] = sat["mixed_split_lu"]["solves_per_s"] / plain["solves_per_s"]
     out["fp64_batched_vs_plain_fp64"] = sat["fp64"]["solves_per_s"] / plain["solves_per_s"]

@@ -272,8 +272,13 @@ int nec2c_cuda_dense_solve_row_major(nec2c_cuda_complex *matrix, nec2c_cuda_comp
 /* No single counterpart in the reference: factr + solve (matrix.c:1313-1416,
    1523-1555) of count independent systems (the wire blocks of many
    frequencies or geometries) at once.  Systems of order <= 64 are factored
-   and solved together in one launch (one CTA per system); larger ones run
-   through the classic factor and solve.  Each matrix is NEC's storage
+   and solved together in one launch (one CTA per system).  Under the "cuda"
+   backend the larger ones up to nec2c_cuda_dense_batch_max_order() are
+   factored in lockstep: each panel step is one launch per kernel for all of
+   them (a thread-block cluster per system for the panel), then they are
+   solved together; they get the pivots and factors each would get alone.
+   The others (larger, or under "cuda-mixed") run through the classic factor
+   and solve.  Each matrix is NEC's storage
    (leading dimension lds[i]) and receives its factors as
    nec2c_cuda_dense_factor_classic writes them; pivots[i] (optional) the
    1-based pivots; rhs[i] the solution.  status[i] is 1 when system i was
@@ -281,6 +286,9 @@ int nec2c_cuda_dense_solve_row_major(nec2c_cuda_complex *matrix, nec2c_cuda_comp
 int nec2c_cuda_dense_solve_batched(size_t count, const size_t *orders, nec2c_cuda_complex *const *matrices,
                                    const size_t *lds, int *const *pivots, nec2c_cuda_complex *const *rhs,
                                    int *status);
+/* Largest order the lockstep batch takes on the current device (4096 where
+   16-CTA clusters can run, else 2048). */
+size_t nec2c_cuda_dense_batch_max_order(void);
 /* Drops the device copies kept between a factor and its solves. */
 void nec2c_cuda_dense_release(void);
 /* No counterpart in the reference (diagnostic of the "cuda-mixed" form):
@@ -436,6 +444,17 @@ size_t nec2c_cuda_server_budget(const nec2c_cuda_server *server);
    own report, x and status; `merged` tells how many ran together.  The
    batch must outlive the server; registering it twice is refused. */
 int nec2c_cuda_server_merge_batch(nec2c_cuda_server *server, nec2c_cuda_vie_batch *batch);
+/* Lets the server merge queued dense requests: a worker that takes a dense
+   request of order up to nec2c_cuda_dense_batch_max_order() also takes the
+   queued dense requests of the same size class (orders up to 256, 512, 1024,
+   2048 or 4096: the cluster size of the first panel), as many as fit the
+   device budget and at most max_systems in all, and factors and solves their
+   private matrix copies as one lockstep batch (the FP64 form, one launch per
+   kernel and panel step for all of them, each system's pivots and factors as
+   its own factorisation gives them).  Each request gets its own status;
+   `merged` tells how many ran together.  max_systems < 2 turns merging off.
+   Refused on a split-precision server. */
+int nec2c_cuda_server_merge_dense(nec2c_cuda_server *server, size_t max_systems);
 /* Drains, stops the workers and frees the server. */
 void nec2c_cuda_server_destroy(nec2c_cuda_server *server);
 

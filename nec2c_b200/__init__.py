@@ -119,6 +119,8 @@ def load():
         "nec2c_cuda_server_drain": (i, [vp]),
         "nec2c_cuda_server_budget": (sz, [vp]),
         "nec2c_cuda_server_destroy": (None, [vp]),
+        "nec2c_cuda_server_merge_dense": (i, [vp, sz]),
+        "nec2c_cuda_dense_batch_max_order": (sz, []),
         "nec2c_cuda_dense_solve_classic": (i, [sz, vp, sz, vp, vp]),
         "nec2c_cuda_dense_solve_classic_many": (i, [sz, vp, sz, vp, vp, sz, sz]),
         "nec2c_cuda_dense_solve_row_major": (i, [vp, vp, sz]),
@@ -462,6 +464,12 @@ class Server:
         server may merge into one batched solve."""
         if not load().nec2c_cuda_server_merge_batch(self.h, batch.h):
             raise RuntimeError("merge registration failed: " + last_error())
+
+    def merge_dense(self, max_systems):
+        """Lets the server merge queued dense requests of one size class into
+        lockstep batches of at most max_systems (FP64 server only)."""
+        if not load().nec2c_cuda_server_merge_dense(self.h, max_systems):
+            raise RuntimeError("dense merging refused: " + last_error())
 
     def _submit(self, r, keep):
         self._keep[C.addressof(r)] = (r, keep)

@@ -213,6 +213,19 @@ int n2d_read_norms(const void *norm_dev, long long count, double *host);
 int n2d_lu_batched(double *mats_dev, double *rhs_dev, int *piv_dev, const int *orders, long long count,
                    int *info_dev, void *systems_dev);
 size_t n2d_lu_batched_descriptor_bytes(long long count);
+/* Ragged batch of count FP64 factorisations advanced in lockstep (one launch
+   per kernel and panel step for all of them): system i is order[i] x order[i]
+   at a_dev[i] (leading dim ld[i]), factored exactly as n2d_lu_factor would
+   (pivots into ipiv_dev[i]); info_host[i] gets its first zero / rejected
+   pivot (1-based) or 0.  Orders up to n2d_lu_batch_max_order(). */
+int n2d_lu_factor_batch(double *const *a_dev, const long long *order, const long long *ld, int *const *ipiv_dev,
+                        int count, int rule, int *info_host);
+long long n2d_lu_batch_max_order(void);
+/* Solves of count factored systems as n2d_lu_solve would, all at once:
+   nrhs[i] columns of b_dev[i] (leading dim ldb[i]). */
+int n2d_lu_solve_batch(const double *const *a_dev, const long long *order, const long long *ld,
+                       const int *const *ipiv_dev, double *const *b_dev, const long long *ldb,
+                       const long long *nrhs, int count);
 /* In-place device transpose of an order x order block (leading dims lda/ldb). */
 int n2d_transpose(const double *src_dev, long long lds, double *dst_dev, long long ldd,
                   long long rows, long long cols);

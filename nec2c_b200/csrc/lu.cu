@@ -26,6 +26,7 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <vector>
 #include "common.cuh"
 #include "device_api.h"
 #include "runtime.cuh"
@@ -387,7 +388,7 @@ __device__ __forceinline__ bool panel_column(const PanelArgs &p, PanelShared<CSZ
 }
 
 template <int CSZ, int RULE, typename S>
-__global__ void __launch_bounds__(CPT, 1) panel_cluster_kernel(PanelArgs p) {
+__device__ __forceinline__ void panel_cluster_body(const PanelArgs &p) {
   static_assert(sizeof(CandEntry) % 16 == 0 && CSZ <= 32 && CCW == 4 && KB == 32, "panel layout");
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
@@ -468,6 +469,11 @@ __global__ void __launch_bounds__(CPT, 1) panel_cluster_kernel(PanelArgs p) {
       base += __popc(moved[k]);
     }
   }
+}
+
+template <int CSZ, int RULE, typename S>
+__global__ void __launch_bounds__(CPT, 1) panel_cluster_kernel(PanelArgs p) {
+  panel_cluster_body<CSZ, RULE, S>(p);
 }
 
 // Cooperative-grid panel for orders beyond the cluster's capacity: one row per
@@ -579,14 +585,14 @@ constexpr int SWT = 256;   // threads per block (8 columns)
 // rows 2c', 2c'+1 (c' = c - k0 - kb) of 64 floats, (Re, -Im) and (Im, Re) per
 // k, each split into a TF32-representable hi part and the FP32 remainder.
 template <typename S>
-__global__ void __launch_bounds__(SWT) swap_trsm_kernel(S *a, long long n, long long ld, long long k0, int kb,
-                                                        const int *pairs, const LuStatus *st, float *bt_hi,
-                                                        float *bt_lo) {
+__device__ __forceinline__ void swap_trsm_body(S *a, long long n, long long ld, long long k0, int kb,
+                                               const int *pairs, const LuStatus *st, float *bt_hi, float *bt_lo,
+                                               long long blk) {
   __shared__ int dst[2 * KB], src[2 * KB];
   __shared__ double2 L[KB][KB + 1];
   const int np = st->npairs;
   for (int t = threadIdx.x; t < np; t += blockDim.x) { dst[t] = pairs[t]; src[t] = pairs[2 * KB + t]; }
-  const long long first = (long long)blockIdx.x * (SWT / 32);
+  const long long first = blk * (SWT / 32);
   const long long cols = n - kb;
   const bool any_right = first + SWT / 32 - 1 >= k0;   // some column of this block is right of the panel
   if (any_right) {
@@ -633,14 +639,20 @@ __global__ void __launch_bounds__(SWT) swap_trsm_kernel(S *a, long long n, long 
   }
 }
 
+template <typename S>
+__global__ void __launch_bounds__(SWT) swap_trsm_kernel(S *a, long long n, long long ld, long long k0, int kb,
+                                                        const int *pairs, const LuStatus *st, float *bt_hi,
+                                                        float *bt_lo) {
+  swap_trsm_body<S>(a, n, ld, k0, kb, pairs, st, bt_hi, bt_lo, blockIdx.x);
+}
+
 // C[M x N] -= A[M x K] B[K x N], row-major complex FP64 blocks (leading dim ld).
 constexpr int GT = 64;   // tile edge
 constexpr int GK = 16;   // K chunk
-__global__ void __launch_bounds__(256) gemm_update_kernel(double2 *C, const double2 *A, const double2 *B,
-                                                          long long M, long long N, int K, long long ld) {
+__device__ __forceinline__ void gemm_update_body(double2 *C, const double2 *A, const double2 *B, long long M,
+                                                 long long N, int K, long long ld, long long row0, long long col0) {
   __shared__ double2 As[GK][GT + 1];
   __shared__ double2 Bs[GK][GT + 1];
-  const long long row0 = blockIdx.y * (long long)GT, col0 = blockIdx.x * (long long)GT;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // 16 x 16 threads, 4 x 4 each
   double2 acc[4][4];
 #pragma unroll
@@ -687,6 +699,10 @@ __global__ void __launch_bounds__(256) gemm_update_kernel(double2 *C, const doub
       }
     }
 }
+__global__ void __launch_bounds__(256) gemm_update_kernel(double2 *C, const double2 *A, const double2 *B,
+                                                          long long M, long long N, int K, long long ld) {
+  gemm_update_body(C, A, B, M, N, K, ld, blockIdx.y * (long long)GT, blockIdx.x * (long long)GT);
+}
 
 // Solve with the row-major getrf-convention factors: all interchanges, unit
 // lower forward substitution, upper back substitution (the system
@@ -705,10 +721,8 @@ constexpr int SOLVE_THREADS = 512;    // fits beside other work on a busy SM
 constexpr int SOLVE_PERM_MAX = 4 * 1024;    // 8 bytes of shared memory per row, 8 values per thread
 constexpr int SOLVE_REG = SOLVE_PERM_MAX / SOLVE_THREADS;
 template <typename S>
-__global__ void __launch_bounds__(SOLVE_THREADS, 2) lu_solve_kernel(const S *a, long long n, long long ld,
-                                                                 const int *ipiv, double2 *b, long long ldb) {
+__device__ __forceinline__ void lu_solve_body(const S *a, long long n, long long ld, const int *ipiv, double2 *x) {
   extern __shared__ int perm_smem[];
-  double2 *x = b + blockIdx.x * ldb;
   __shared__ double2 xs[32];
   if (n <= SOLVE_PERM_MAX) {
     int *idx = perm_smem, *pv = perm_smem + n;
@@ -788,6 +802,12 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) lu_solve_kernel(const S *a, 
     }
     __syncthreads();
   }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(SOLVE_THREADS, 2) lu_solve_kernel(const S *a, long long n, long long ld,
+                                                                 const int *ipiv, double2 *b, long long ldb) {
+  lu_solve_body<S>(a, n, ld, ipiv, b + blockIdx.x * ldb);
 }
 
 // ------------------------------------------------ multi-CTA triangular solve
@@ -990,10 +1010,8 @@ __device__ __forceinline__ void solve_next_rows(const double2 *nb, const double2
 }
 
 template <typename S>
-__global__ void __launch_bounds__(SOLVE_COOP_THREADS) lu_solve_coop_kernel(const S *a, long long n, long long ld,
-                                                                         const int *ipiv, double2 *b, long long ldb,
-                                                                         int nrhs, double2 *scratch,
-                                                                         SolveSync *sy) {
+__device__ __forceinline__ void lu_solve_coop_body(const S *a, long long n, long long ld, const int *ipiv, double2 *b,
+                                                   long long ldb, int nrhs, double2 *scratch, SolveSync *sy) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2 *dg = reinterpret_cast<double2 *>(smem_raw);   // diagonal block
   double2 *nb = dg + SOLVE_NB * SOLVE_LDS;                // next rows' block
@@ -1107,6 +1125,13 @@ __global__ void __launch_bounds__(SOLVE_COOP_THREADS) lu_solve_coop_kernel(const
       x[i] = y[i];
     if (!solve_barrier(sy)) return;
   }
+}
+template <typename S>
+__global__ void __launch_bounds__(SOLVE_COOP_THREADS) lu_solve_coop_kernel(const S *a, long long n, long long ld,
+                                                                         const int *ipiv, double2 *b, long long ldb,
+                                                                         int nrhs, double2 *scratch,
+                                                                         SolveSync *sy) {
+  lu_solve_coop_body<S>(a, n, ld, ipiv, b, ldb, nrhs, scratch, sy);
 }
 
 __global__ void transpose_kernel(const double2 *src, long long lds, double2 *dst, long long ldd,
@@ -1484,6 +1509,313 @@ extern "C" int n2d_lu_solve32(const float *a_dev, long long n, long long ld, con
   lu_solve_kernel<float2><<<(unsigned)nrhs, SOLVE_THREADS, solve_smem(n), n2c_stream()>>>((const float2 *)a_dev, n, ld, ipiv,
                                                                      (double2 *)b_dev, ldb);
   return n2c_check_launch("lu_solve");
+}
+
+// ------------------------------------------------ ragged batch of factors
+// Many independent FP64 factorisations (orders up to the cluster panel's
+// rows) advanced in lockstep: each panel step is one launch of each kernel
+// for the whole batch (one cluster per matrix for the panel; the matrix index
+// in grid.y or grid.z for the interchanges, the triangular solve and the
+// update), so the latency of the pivot chain is paid once per step for every
+// matrix and the updates of all of them fill the device together.  A matrix
+// whose order has been passed takes no further part (its blocks return at
+// once).  The kernel bodies are the single factorisation's, so each matrix
+// gets exactly the pivots and factors n2d_lu_factor gives it alone.
+namespace {
+
+struct LuBatchEntry {
+  double2 *a;
+  long long n, ld;
+  int *ipiv;
+  int *pairs;      // 4 KB ints of this matrix's interchange pairs
+  LuStatus *st;
+};
+
+__device__ __forceinline__ int batch_kb(long long n, long long k0) { return (int)(n - k0 < KB ? n - k0 : KB); }
+
+template <int CSZ, int RULE>
+__global__ void __launch_bounds__(CPT, 1) panel_cluster_batch_kernel(const LuBatchEntry *e, long long k0) {
+  const LuBatchEntry m = e[blockIdx.y];   // clusters run along x: one matrix per cluster
+  if (m.n <= k0) return;
+  PanelArgs p{};
+  p.a = m.a; p.n = m.n; p.ld = m.ld; p.k0 = k0; p.kb = batch_kb(m.n, k0); p.rule = RULE;
+  p.ipiv = m.ipiv; p.pairs = m.pairs; p.st = m.st;
+  panel_cluster_body<CSZ, RULE, double2>(p);
+}
+
+__global__ void __launch_bounds__(SWT) swap_trsm_batch_kernel(const LuBatchEntry *e, long long k0) {
+  const LuBatchEntry m = e[blockIdx.y];
+  if (m.n <= k0) return;
+  const int kb = batch_kb(m.n, k0);
+  if ((long long)blockIdx.x * (SWT / 32) >= m.n - kb) return;   // no column of this matrix in the block
+  swap_trsm_body<double2>(m.a, m.n, m.ld, k0, kb, m.pairs, m.st, nullptr, nullptr, blockIdx.x);
+}
+
+// part 0: the next panel's columns (look-ahead); part 1: the columns after it.
+__global__ void __launch_bounds__(256) gemm_update_batch_kernel(const LuBatchEntry *e, long long k0, int part) {
+  const LuBatchEntry m = e[blockIdx.z];
+  if (m.n <= k0) return;
+  const int kb = batch_kb(m.n, k0);
+  const long long right = m.n - k0 - kb;
+  const long long nb = right < KB ? right : KB;
+  const long long cf = k0 + kb + (part ? nb : 0);
+  const long long cols = part ? right - nb : nb;
+  const long long row0 = blockIdx.y * (long long)GT, col0 = blockIdx.x * (long long)GT;
+  if (right <= 0 || cols <= 0 || row0 >= right || col0 >= cols) return;
+  double2 *below = m.a + (k0 + kb) * m.ld;
+  gemm_update_body(below + cf, below + k0, m.a + k0 * m.ld + cf, right, cols, kb, m.ld, row0, col0);
+}
+
+struct SolveBatchEntry {
+  const double2 *a;
+  long long n, ld;
+  const int *ipiv;
+  double2 *b;
+  long long ldb;
+  int nrhs;
+  double2 *scratch;   // cooperative form: n values
+  SolveSync *sy;      // cooperative form: this system's barrier
+};
+
+// One CTA per (right-hand side, system).
+__global__ void __launch_bounds__(SOLVE_THREADS, 2) lu_solve_batch_kernel(const SolveBatchEntry *e) {
+  const SolveBatchEntry m = e[blockIdx.y];
+  if ((int)blockIdx.x >= m.nrhs) return;
+  lu_solve_body<double2>(m.a, m.n, m.ld, m.ipiv, m.b + blockIdx.x * m.ldb);
+}
+
+// gridDim.x co-resident CTAs per system (grid.y = system), each group on its
+// own barrier.
+__global__ void __launch_bounds__(SOLVE_COOP_THREADS) lu_solve_coop_batch_kernel(const SolveBatchEntry *e) {
+  const SolveBatchEntry m = e[blockIdx.y];
+  lu_solve_coop_body<double2>(m.a, m.n, m.ld, m.ipiv, m.b, m.ldb, m.nrhs, m.scratch, m.sy);
+}
+
+template <int CSZ>
+static cudaError_t launch_cluster_panel_batch(const LuBatchEntry *e, int count, long long k0, int rule,
+                                              cudaStream_t s) {
+  void (*kernel)(const LuBatchEntry *, long long) =
+      rule == 0 ? panel_cluster_batch_kernel<CSZ, 0> : panel_cluster_batch_kernel<CSZ, 1>;
+  if (CSZ > 8) {
+    static const bool opted = cudaFuncSetAttribute(panel_cluster_batch_kernel<CSZ, 0>,
+                                                   cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess &&
+                              cudaFuncSetAttribute(panel_cluster_batch_kernel<CSZ, 1>,
+                                                   cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
+    if (!opted) return cudaErrorInvalidConfiguration;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(CSZ, (unsigned)count);
+  cfg.blockDim = dim3(CPT);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CSZ;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, e, k0);
+}
+
+// The batch's panels at step k0 (rows: the largest panel's row count).
+static int launch_panel_batch(const LuBatchEntry *e, int count, long long k0, long long rows, int rule,
+                              cudaStream_t s) {
+  cudaError_t err;
+  if (rows <= CROWS) err = launch_cluster_panel_batch<1>(e, count, k0, rule, s);
+  else if (rows <= 2 * CROWS) err = launch_cluster_panel_batch<2>(e, count, k0, rule, s);
+  else if (rows <= 4 * CROWS) err = launch_cluster_panel_batch<4>(e, count, k0, rule, s);
+  else if (rows <= 8 * CROWS) err = launch_cluster_panel_batch<8>(e, count, k0, rule, s);
+  else err = launch_cluster_panel_batch<CMAX>(e, count, k0, rule, s);
+  if (err != cudaSuccess) {
+    cudaGetLastError();
+    n2c_set_error("batched panel launch: %s", cudaGetErrorString(err));
+    return 0;
+  }
+  n2c_count_launch(1);
+  return 1;
+}
+
+}  // namespace
+
+extern "C" long long n2d_lu_batch_max_order(void) { return cluster_rows(); }
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+extern "C" int n2d_lu_factor_batch(double *const *a_dev, const long long *n, const long long *ld, int *const *ipiv,
+                                   int count, int rule, int *info) {
+  if (count <= 0) return 1;
+  const long long cap = cluster_rows();
+  if (count > 65535) {
+    n2c_set_error("batched factor: %d systems (at most 65535)", count);
+    return 0;
+  }
+  long long nmax = 0;
+  for (int i = 0; i < count; ++i) {
+    info[i] = 0;
+    if (!a_dev[i] || !ipiv[i] || n[i] <= 0 || n[i] > cap || ld[i] < n[i]) {
+      n2c_set_error("batched factor: system %d has a null matrix or pivots, an order outside 1..%lld, or a "
+                    "leading dimension below its order", i, cap);
+      return 0;
+    }
+    if (n[i] > nmax) nmax = n[i];
+  }
+  cudaStream_t s = n2c_stream();
+  LookAhead *la = nmax > KB ? look_ahead() : nullptr;
+  if (nmax > KB && !la) return 0;
+  const size_t eb = align256(count * sizeof(LuBatchEntry)), sb = align256(count * sizeof(LuStatus));
+  char *dev = (char *)n2d_alloc_async(eb + sb + (size_t)count * 4 * KB * sizeof(int));
+  if (!dev) return 0;
+  LuBatchEntry *de = (LuBatchEntry *)dev;
+  LuStatus *dst = (LuStatus *)(dev + eb);
+  int *dpairs = (int *)(dev + eb + sb);
+  std::vector<LuBatchEntry> h((size_t)count);
+  for (int i = 0; i < count; ++i)
+    h[i] = LuBatchEntry{(double2 *)a_dev[i], n[i], ld[i], ipiv[i], dpairs + (size_t)i * 4 * KB, dst + i};
+  int ok = cudaMemsetAsync(dst, 0, count * sizeof(LuStatus), s) == cudaSuccess &&
+           cudaMemcpyAsync(de, h.data(), count * sizeof(LuBatchEntry), cudaMemcpyHostToDevice, s) == cudaSuccess;
+  if (!ok) n2c_set_error("batched factor: descriptor upload failed");
+  ok = ok && launch_panel_batch(de, count, 0, nmax, rule, s);
+  const unsigned gb = (unsigned)((nmax + SWT / 32 - 1) / (SWT / 32));
+  for (long long k0 = 0; ok && k0 < nmax; k0 += KB) {
+    swap_trsm_batch_kernel<<<dim3(gb, (unsigned)count), SWT, 0, s>>>(de, k0);
+    if (!n2c_check_launch("batched interchanges and triangular solve")) { ok = 0; break; }
+    const long long right = nmax - k0 - (nmax - k0 < KB ? nmax - k0 : KB);
+    if (right <= 0) break;
+    const unsigned rt = (unsigned)((right + GT - 1) / GT);
+    const long long rest = right - (right < KB ? right : KB);
+    gemm_update_batch_kernel<<<dim3(1, rt, (unsigned)count), 256, 0, s>>>(de, k0, 0);
+    ok = n2c_check_launch("batched update (next panel)");
+    if (ok && (cudaEventRecord(la->next, s) != cudaSuccess || cudaStreamWaitEvent(la->aux, la->next, 0) != cudaSuccess)) {
+      n2c_set_error("look-ahead event");
+      ok = 0;
+    }
+    ok = ok && launch_panel_batch(de, count, k0 + KB, right, rule, la->aux);
+    if (ok && cudaEventRecord(la->panel, la->aux) != cudaSuccess) { n2c_set_error("look-ahead event"); ok = 0; }
+    if (ok && rest > 0) {
+      gemm_update_batch_kernel<<<dim3((unsigned)((rest + GT - 1) / GT), rt, (unsigned)count), 256, 0, s>>>(de, k0, 1);
+      ok = n2c_check_launch("batched update");
+    }
+    if (ok && cudaStreamWaitEvent(s, la->panel, 0) != cudaSuccess) { n2c_set_error("look-ahead event"); ok = 0; }
+  }
+  if (la && !ok) cudaStreamSynchronize(la->aux);
+  std::vector<LuStatus> hs((size_t)count);
+  cudaError_t e = cudaMemcpyAsync(hs.data(), dst, count * sizeof(LuStatus), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (ok && e != cudaSuccess) { n2c_set_error("reading the batch status: %s", cudaGetErrorString(e)); ok = 0; }
+  for (int i = 0; ok && i < count; ++i) {
+    if (hs[i].error) { n2c_set_error("LU kernel wait time-out (batched system %d)", i); ok = 0; }
+    info[i] = hs[i].info;
+  }
+  n2d_free_async(dev);
+  return ok;
+}
+
+// Cooperative CTAs per system when `systems` solves share the device.
+static int solve_batch_group(int systems) {
+  const int sms = n2c_sm_count();
+  int g = systems > 0 ? sms / systems : SOLVE_CTAS;
+  if (g > SOLVE_CTAS) g = SOLVE_CTAS;
+  if (g < 2) g = 2;
+  return g;
+}
+
+extern "C" int n2d_lu_solve_batch(const double *const *a_dev, const long long *n, const long long *ld,
+                                  const int *const *ipiv, double *const *b_dev, const long long *ldb,
+                                  const long long *nrhs, int count) {
+  if (count <= 0) return 1;
+  if (count > 65535) {
+    n2c_set_error("batched solve: %d systems (at most 65535)", count);
+    return 0;
+  }
+  cudaStream_t s = n2c_stream();
+  std::vector<SolveBatchEntry> one, coop;
+  long long one_n = 0, one_rhs = 0, coop_n = 0;
+  for (int i = 0; i < count; ++i) {
+    if (!a_dev[i] || !ipiv[i] || !b_dev[i] || n[i] <= 0 || n[i] > 0x7fffffffLL || ld[i] < n[i] || ldb[i] < n[i] ||
+        nrhs[i] < 0 || nrhs[i] > 65535) {
+      n2c_set_error("batched solve: system %d has a null pointer, an order of 0, a leading dimension below its "
+                    "order or a right-hand side count outside 0..65535", i);
+      return 0;
+    }
+    if (nrhs[i] == 0) continue;
+    SolveBatchEntry m{(const double2 *)a_dev[i], n[i], ld[i], ipiv[i], (double2 *)b_dev[i], ldb[i], (int)nrhs[i],
+                      nullptr, nullptr};
+    if (n[i] >= SOLVE_COOP_MIN && nrhs[i] <= SOLVE_COOP_RHS) {
+      coop.push_back(m);
+      if (n[i] > coop_n) coop_n = n[i];
+    } else {
+      one.push_back(m);
+      if (n[i] > one_n) one_n = n[i];
+      if (nrhs[i] > one_rhs) one_rhs = nrhs[i];
+    }
+  }
+  static const bool attrs =
+      cudaFuncSetAttribute(lu_solve_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * SOLVE_PERM_MAX) ==
+          cudaSuccess &&
+      cudaFuncSetAttribute(lu_solve_coop_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SOLVE_COOP_SMEM) == cudaSuccess;
+  if (!attrs) {
+    cudaGetLastError();
+    n2c_set_error("batched solve: shared memory configuration failed");
+    return 0;
+  }
+  // Cooperative groups: scratch vectors and barriers of every such system.
+  const size_t nc = coop.size();
+  size_t scratch_bytes = 0;
+  for (const SolveBatchEntry &m : coop) scratch_bytes += align256((size_t)m.n * sizeof(double2));
+  const size_t eb = align256((one.size() + nc) * sizeof(SolveBatchEntry)), syb = align256(nc * sizeof(SolveSync));
+  char *dev = (char *)n2d_alloc_async(eb + syb + scratch_bytes + 256);
+  if (!dev) return 0;
+  SolveBatchEntry *de = (SolveBatchEntry *)dev;
+  SolveSync *dsy = (SolveSync *)(dev + eb);
+  char *sp = dev + eb + syb;
+  for (size_t i = 0; i < nc; ++i) {
+    coop[i].sy = dsy + i;
+    coop[i].scratch = (double2 *)sp;
+    sp += align256((size_t)coop[i].n * sizeof(double2));
+  }
+  std::vector<SolveBatchEntry> all(one);
+  all.insert(all.end(), coop.begin(), coop.end());
+  int ok = (nc == 0 || cudaMemsetAsync(dsy, 0, nc * sizeof(SolveSync), s) == cudaSuccess) &&
+           cudaMemcpyAsync(de, all.data(), all.size() * sizeof(SolveBatchEntry), cudaMemcpyHostToDevice, s) ==
+               cudaSuccess;
+  if (!ok) n2c_set_error("batched solve: descriptor upload failed");
+  if (ok && !one.empty()) {
+    const size_t smem = (size_t)8 * (one_n < SOLVE_PERM_MAX ? one_n : SOLVE_PERM_MAX);
+    lu_solve_batch_kernel<<<dim3((unsigned)one_rhs, (unsigned)one.size()), SOLVE_THREADS, smem, s>>>(de);
+    ok = n2c_check_launch("batched solve");
+  }
+  // Cooperative systems in rounds that fit the device at one CTA per SM.
+  const int g = solve_batch_group((int)nc);
+  const int per_round = n2c_sm_count() / g > 0 ? n2c_sm_count() / g : 1;
+  for (size_t i0 = 0; ok && i0 < nc; i0 += (size_t)per_round) {
+    const unsigned k = (unsigned)(nc - i0 < (size_t)per_round ? nc - i0 : (size_t)per_round);
+    const SolveBatchEntry *first = de + one.size() + i0;
+    void *args[] = {(void *)&first};
+    const cudaError_t e = cudaLaunchCooperativeKernel((void *)lu_solve_coop_batch_kernel, dim3((unsigned)g, k),
+                                                      SOLVE_COOP_THREADS, args, SOLVE_COOP_SMEM, s);
+    if (e != cudaSuccess) {
+      // Not launchable as one cooperative grid here: one CTA per system.
+      cudaGetLastError();
+      const size_t smem = (size_t)8 * (coop_n < SOLVE_PERM_MAX ? coop_n : SOLVE_PERM_MAX);
+      lu_solve_batch_kernel<<<dim3(SOLVE_COOP_RHS, k), SOLVE_THREADS, smem, s>>>(first);
+      ok = n2c_check_launch("batched solve");
+    } else {
+      n2c_count_launch(1);
+    }
+  }
+  if (ok && nc) {
+    std::vector<SolveSync> hs(nc);
+    if (cudaMemcpyAsync(hs.data(), dsy, nc * sizeof(SolveSync), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      n2c_set_error("batched solve: reading the barrier status failed");
+      ok = 0;
+    }
+    for (size_t i = 0; ok && i < nc; ++i)
+      if (hs[i].error) { n2c_set_error("triangular solve: grid barrier time-out (batched)"); ok = 0; }
+  }
+  n2d_free_async(dev);
+  return ok;
 }
 
 // ------------------------------------------------------ allocation-free factor

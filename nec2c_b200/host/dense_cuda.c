@@ -426,6 +426,76 @@ int nec2c_cuda_dense_solve_row_major(nec2c_cuda_complex *matrix, nec2c_cuda_comp
    place (factr's pivots and factors, as nec2c_cuda_dense_factor_classic
    writes them) and solved for one right-hand side each.  Larger orders go
    through the classic factor and solve one after another. */
+size_t nec2c_cuda_dense_batch_max_order(void)
+{
+  const long long m = n2d_device_ok() ? n2d_lu_batch_max_order() : 0;
+  return m > 0 ? (size_t)m : 0;
+}
+
+/* Lockstep batch (FP64 form): count systems in NEC storage on the host are
+   uploaded, factored together by n2d_lu_factor_batch and solved together by
+   n2d_lu_solve_batch on this thread's stream.  rhs_count[i] right-hand sides
+   of rhs[i] (stride[i]) receive the solutions; factors / pivots (either may
+   be NULL, or hold NULL entries) receive the factors in NEC storage as
+   nec2c_cuda_dense_factor_classic writes them, and the 1-based pivots.
+   status[i] is 1 when system i was solved, 0 when it is singular.  Returns 0
+   (error set) when the device work itself failed. */
+static int lockstep_batch(size_t count, const size_t *order, const nec2c_cuda_complex *const *matrix,
+                          const size_t *ld, nec2c_cuda_complex *const *factors, int *const *pivots,
+                          nec2c_cuda_complex *const *rhs, const size_t *stride, const size_t *rhs_count, int *status)
+{
+  double **a = calloc(count, sizeof(*a)), **b = calloc(count, sizeof(*b));
+  int **piv = calloc(count, sizeof(*piv)), *info = calloc(count, sizeof(int));
+  long long *n = calloc(count, sizeof(long long)), *nr = calloc(count, sizeof(long long));
+  size_t i;
+  int ok = a && b && piv && info && n && nr;
+  if(!ok) n2c_set_error("batched solve: out of host memory");
+  for(i = 0; ok && i < count; ++i) {
+    const size_t k = order[i];
+    status[i] = 0;
+    n[i] = (long long)k;
+    a[i] = n2d_alloc_async(k * k * CPX);
+    b[i] = n2d_alloc_async(k * (rhs_count[i] ? rhs_count[i] : 1) * CPX);
+    piv[i] = n2d_alloc_async(k * sizeof(int));
+    ok = a[i] && b[i] && piv[i] && n2d_upload2d(a[i], k * CPX, matrix[i], ld[i] * CPX, k * CPX, k) &&
+         n2d_upload2d(b[i], k * CPX, rhs[i], stride[i] * CPX, k * CPX, rhs_count[i]);
+  }
+  ok = ok && n2d_lu_factor_batch(a, n, n, piv, (int)count, 0, info);
+  /* Singular systems take no part in the solve. */
+  for(i = 0; ok && i < count; ++i) nr[i] = info[i] ? 0 : (long long)rhs_count[i];
+  ok = ok && n2d_lu_solve_batch((const double *const *)a, n, n, (const int *const *)piv, b, n, nr, (int)count);
+  for(i = 0; ok && i < count; ++i) {
+    const size_t k = order[i];
+    if(factors && factors[i])
+      ok = n2d_download2d(factors[i], ld[i] * CPX, a[i], k * CPX, k * CPX, k);
+    if(ok && pivots && pivots[i]) ok = n2d_download(pivots[i], piv[i], k * sizeof(int));
+    if(ok && !info[i]) ok = n2d_download2d(rhs[i], stride[i] * CPX, b[i], k * CPX, k * CPX, rhs_count[i]);
+    if(ok) status[i] = info[i] == 0;
+  }
+  if(ok) n2d_sync();
+  for(i = 0; a && b && piv && i < count; ++i) { n2d_free_async(a[i]); n2d_free_async(b[i]); n2d_free_async(piv[i]); }
+  free(a); free(b); free(piv); free(info); free(n); free(nr);
+  return ok;
+}
+
+/* The request server's merged dense run (FP64 form): the private copies of
+   count requests' matrices factored and solved as one lockstep batch. */
+int n2c_dense_solve_private_batch(size_t count, const size_t *order, const nec2c_cuda_complex *const *matrix,
+                                  const size_t *ld, nec2c_cuda_complex *const *rhs, const size_t *stride,
+                                  const size_t *rhs_count, int *status)
+{
+  size_t i;
+  for(i = 0; i < count; ++i) {
+    status[i] = 0;
+    if(!matrix[i] || !rhs[i] || order[i] == 0 || (long long)order[i] > n2d_lu_batch_max_order() || ld[i] < order[i] ||
+       stride[i] < order[i] || rhs_count[i] == 0 || rhs_count[i] > 65535) {
+      n2c_set_error("merged dense run: invalid request %zu", i);
+      return 0;
+    }
+  }
+  return lockstep_batch(count, order, matrix, ld, NULL, NULL, rhs, stride, rhs_count, status);
+}
+
 int nec2c_cuda_dense_solve_batched(size_t count, const size_t *orders, nec2c_cuda_complex *const *matrices,
                                    const size_t *lds, int *const *pivots, nec2c_cuda_complex *const *rhs,
                                    int *status)
@@ -493,9 +563,39 @@ int nec2c_cuda_dense_solve_batched(size_t count, const size_t *orders, nec2c_cud
     free(order32); free(info); free(piv_host); free(a_host); free(b_host);
     if(!ok) return 0;
   }
+  /* FP64 form: the larger systems up to the batch limit in one lockstep
+     batch (one launch per kernel and panel step for all of them). */
+  if(!g_dense_mixed) {
+    size_t k = 0, j;
+    const long long cap = n2d_lu_batch_max_order();
+    size_t *ord = malloc(count * sizeof(size_t)), *ldv = malloc(count * sizeof(size_t)), *one = malloc(count * sizeof(size_t));
+    size_t *idx = malloc(count * sizeof(size_t));
+    const nec2c_cuda_complex **mat = malloc(count * sizeof(*mat));
+    nec2c_cuda_complex **fac = malloc(count * sizeof(*fac)), **rv = malloc(count * sizeof(*rv));
+    int **pv = malloc(count * sizeof(*pv)), *st = malloc(count * sizeof(int));
+    ok = ord && ldv && one && idx && mat && fac && rv && pv && st;
+    for(i = 0; ok && i < count; ++i) {
+      if(orders[i] <= 64 || (long long)orders[i] > cap) continue;
+      {
+        /* Factors written over an entry's storage replace it. */
+        const host_block blk = {(const char *)matrices[i], orders[i], lds[i]};
+        entries_drop(drop_overlap, &blk);
+      }
+      idx[k] = i; ord[k] = orders[i]; ldv[k] = lds[i]; one[k] = 1;
+      mat[k] = matrices[i]; fac[k] = matrices[i]; rv[k] = rhs[i]; pv[k] = pivots ? pivots[i] : NULL;
+      k++;
+    }
+    ok = ok && (k == 0 || lockstep_batch(k, ord, mat, ldv, fac, pv, rv, ord, one, st));
+    for(j = 0; ok && j < k; ++j) {
+      status[idx[j]] = st[j];
+      if(!st[j]) all = 0;
+    }
+    free(ord); free(ldv); free(one); free(idx); free(mat); free(fac); free(rv); free(pv); free(st);
+    if(!ok) return 0;
+  }
   for(i = 0; i < count; ++i) {
     int *p;
-    if(orders[i] <= 64) continue;
+    if(orders[i] <= 64 || (!g_dense_mixed && (long long)orders[i] <= n2d_lu_batch_max_order())) continue;
     p = (pivots && pivots[i]) ? pivots[i] : malloc(orders[i] * sizeof(int));
     status[i] = p && nec2c_cuda_dense_factor_classic(orders[i], matrices[i], lds[i], p) &&
                 nec2c_cuda_dense_solve_classic(orders[i], matrices[i], lds[i], p, rhs[i]);

@@ -41,6 +41,9 @@
 
 int n2c_dense_solve_private(size_t n, const nec2c_cuda_complex *matrix, size_t ld, nec2c_cuda_complex *rhs,
                             size_t stride, size_t count, int split, int *steps);
+int n2c_dense_solve_private_batch(size_t count, const size_t *order, const nec2c_cuda_complex *const *matrix,
+                                  const size_t *ld, nec2c_cuda_complex *const *rhs, const size_t *stride,
+                                  const size_t *rhs_count, int *status);
 const nec2c_cuda_vie_plan *n2c_hybrid_volume_plan(const nec2c_cuda_hybrid *h);
 const nec2c_cuda_vie_plan *n2c_batch_plan(const nec2c_cuda_vie_batch *b, size_t q);
 size_t n2c_batch_index(const nec2c_cuda_vie_batch *b, const nec2c_cuda_vie_plan *plan,
@@ -53,11 +56,14 @@ int n2c_gmres_batch_subset(nec2c_cuda_vie_batch *b, const nec2c_cuda_complex *co
 #define MERGE_MAX_RESTART 30
 
 /* What one worker runs: a request, or (batch != NULL, n >= 2) the volume
-   requests merged into one solve of that batch, member j on system index[j]. */
+   requests merged into one solve of that batch, member j on system index[j],
+   or (dense, n >= 2) dense requests factored and solved as one lockstep
+   batch. */
 typedef struct {
   nec2c_cuda_request **member;
   size_t *index, n;
   nec2c_cuda_vie_batch *batch;
+  int dense;
 } run_t;
 
 struct nec2c_cuda_server {
@@ -70,6 +76,7 @@ struct nec2c_cuda_server {
   run_t *busy;                  /* in flight per worker (n == 0: idle) */
   nec2c_cuda_vie_batch **merge; /* batches whose systems' requests merge */
   size_t merges;
+  size_t dense_merge;           /* most dense requests in one lockstep batch (< 2: none) */
   size_t pending;               /* submitted, not finished */
   int stop, started;
   pthread_t *threads;
@@ -293,6 +300,87 @@ static size_t gather_merge(const nec2c_cuda_server *s, nec2c_cuda_request *r, si
   return f;
 }
 
+/* Size class of a dense request: the cluster size of its first panel (one
+   CTA per 256 rows, rounded up to a power of two), so that the members of a
+   lockstep batch, which advances at its largest member's pace, are within a
+   factor of two of each other in order. */
+static size_t dense_class(size_t n)
+{
+  size_t c = 1;
+  while(c * 256 < n) c <<= 1;
+  return c;
+}
+
+static int dense_mergeable(const nec2c_cuda_server *s, const nec2c_cuda_request *r)
+{
+  return r->kind == NEC2C_CUDA_REQUEST_DENSE && s->dense_merge >= 2 && !s->split && r->order > 0 &&
+         (long long)r->order <= n2d_lu_batch_max_order() && r->rhs_count > 0 && r->rhs_count <= 65535 &&
+         r->ld >= r->order && r->rhs_stride >= r->order;
+}
+
+/* With the lock held: the queued dense requests of r's size class that join
+   r (at queue position pick) in one lockstep batch, r first, while their
+   summed footprint fits (at most dense_merge).  Fills u and taken; returns
+   the run's footprint, or 0 when no other request joins. */
+static size_t gather_dense(const nec2c_cuda_server *s, nec2c_cuda_request *r, size_t pick, size_t fp, run_t *u,
+                           unsigned char *taken)
+{
+  const size_t cls = dense_class(r->order);
+  size_t q, f = fp;
+  u->n = 0;
+  u->member[u->n++] = r;
+  taken[pick] = 1;
+  for(q = 0; q < s->count && u->n < s->dense_merge; ++q) {
+    nec2c_cuda_request *c = s->queue[(s->head + q) % s->cap];
+    size_t fc;
+    if(q == pick || !dense_mergeable(s, c) || dense_class(c->order) != cls) continue;
+    fc = footprint(s, c);
+    /* Members after the first always fit within the budget (a lone request
+       larger than the budget may still run alone). */
+    if(s->in_use + f + fc > s->budget) continue;
+    f += fc;
+    taken[q] = 1;
+    u->member[u->n++] = c;
+  }
+  if(u->n < 2) {
+    for(q = 0; q < s->count; ++q) taken[q] = 0;
+    u->n = 0;
+    return 0;
+  }
+  return f;
+}
+
+/* Merged dense requests: one lockstep factorisation and solve of their
+   private matrix copies. */
+static void run_dense_merged(run_t *u)
+{
+  const size_t k = u->n;
+  size_t *order = calloc(k, sizeof(size_t)), *ld = calloc(k, sizeof(size_t)), *stride = calloc(k, sizeof(size_t));
+  size_t *count = calloc(k, sizeof(size_t)), j;
+  const nec2c_cuda_complex **mat = calloc(k, sizeof(*mat));
+  nec2c_cuda_complex **rhs = calloc(k, sizeof(*rhs));
+  int *st = calloc(k, sizeof(int)), ok = order && ld && stride && count && mat && rhs && st;
+  if(!ok) n2c_set_error("merged dense run: out of host memory");
+  for(j = 0; ok && j < k; ++j) {
+    const nec2c_cuda_request *r = u->member[j];
+    order[j] = r->order; ld[j] = r->ld; stride[j] = r->rhs_stride; count[j] = r->rhs_count;
+    mat[j] = r->matrix; rhs[j] = r->rhs;
+  }
+  if(ok) ok = n2c_dense_solve_private_batch(k, order, mat, ld, rhs, stride, count, st);
+  for(j = 0; j < k; ++j) {
+    nec2c_cuda_request *r = u->member[j];
+    memset(&r->report, 0, sizeof(r->report));
+    r->status = ok && st && st[j];
+    r->report.status = r->status;
+    r->merged = k;
+    if(!r->status) {
+      strncpy(r->error, ok ? "matrix is singular" : nec2c_cuda_last_error(), sizeof(r->error) - 1);
+      r->error[sizeof(r->error) - 1] = 0;
+    }
+  }
+  free(order); free(ld); free(stride); free(count); free(mat); free(rhs); free(st);
+}
+
 static void *worker(void *arg)
 {
   nec2c_cuda_server *s = arg;
@@ -326,6 +414,7 @@ static void *worker(void *arg)
     if(slot < 0) { pthread_cond_wait(&s->work, &s->lock); continue; }   /* one run per worker: not reached */
     u = &s->busy[slot];
     u->batch = NULL;
+    u->dense = 0;
     /* Continuous batching: the queued requests on the other systems of r's
        registered batch join it. */
     mb = merge_batch_of(s, r, &q0);
@@ -335,7 +424,19 @@ static void *worker(void *arg)
       const size_t f = gather_merge(s, r, pick, q0, mb, u, taken);
       if(f) { fp = f; u->batch = mb; }
     }
-    if(!u->batch) {
+    /* Dense requests of r's size class queued behind it join it in one
+       lockstep factorisation. */
+    if(!u->batch && dense_mergeable(s, r) && s->count > 1) {
+      free(u->member); free(u->index); free(taken);
+      u->index = NULL;
+      taken = calloc(s->count, 1);
+      u->member = malloc(s->dense_merge * sizeof(*u->member));
+      if(taken && u->member) {
+        const size_t f = gather_dense(s, r, pick, fp, u, taken);
+        if(f) { fp = f; u->dense = 1; }
+      }
+    }
+    if(!u->batch && !u->dense) {
       free(u->member); free(u->index);
       u->member = NULL; u->index = NULL;
       free(taken);
@@ -371,6 +472,7 @@ static void *worker(void *arg)
     }
     pthread_mutex_unlock(&s->lock);
     if(u->batch) run_merged(u);
+    else if(u->dense) run_dense_merged(u);
     else run_request(s, r);
     pthread_mutex_lock(&s->lock);
     s->in_use -= fp;
@@ -381,6 +483,7 @@ static void *worker(void *arg)
     }
     u->n = 0;
     u->batch = NULL;
+    u->dense = 0;
     free(u->member); free(u->index);
     u->member = NULL; u->index = NULL;
     slot = -1;
@@ -518,6 +621,20 @@ int nec2c_cuda_server_merge_batch(nec2c_cuda_server *s, nec2c_cuda_vie_batch *b)
   s->merge = m;
   s->merge[s->merges++] = b;
   pthread_cond_broadcast(&s->work);
+  pthread_mutex_unlock(&s->lock);
+  return 1;
+}
+
+int nec2c_cuda_server_merge_dense(nec2c_cuda_server *s, size_t max_systems)
+{
+  if(!s) { n2c_set_error("dense merging: null server"); return 0; }
+  if(s->split && max_systems >= 2) {
+    n2c_set_error("dense merging: the lockstep batch is the FP64 form; this server runs the split-precision form");
+    return 0;
+  }
+  if(max_systems > 65535) { n2c_set_error("dense merging: at most 65535 systems per batch"); return 0; }
+  pthread_mutex_lock(&s->lock);
+  s->dense_merge = max_systems;
   pthread_mutex_unlock(&s->lock);
   return 1;
 }

@@ -36,6 +36,7 @@ struct nec2c_cuda_vie_batch {
 static pthread_mutex_t g_lock = PTHREAD_MUTEX_INITIALIZER;
 static int g_violations, g_running, g_peak;
 static int g_merged_runs, g_merged_peak;   /* merged solves seen; most systems in one */
+static int g_dense_runs, g_dense_peak, g_dense_mixed_classes;   /* lockstep dense batches */
 static long g_delay_us = 2000;
 static size_t g_free_bytes = (size_t)10 << 30;
 static __thread char g_error[256];
@@ -46,6 +47,7 @@ void fake_reset(long delay_us, size_t free_bytes)
   pthread_mutex_lock(&g_lock);
   g_violations = g_running = g_peak = 0;
   g_merged_runs = g_merged_peak = 0;
+  g_dense_runs = g_dense_peak = g_dense_mixed_classes = 0;
   g_delay_us = delay_us;
   g_free_bytes = free_bytes;
   pthread_mutex_unlock(&g_lock);
@@ -156,6 +158,38 @@ int n2c_dense_solve_private(size_t n, const nec2c_cuda_complex *matrix, size_t l
   hold(NULL, 0);
   rhs[0] = (double)n;
   *steps = split ? 3 : 0;
+  return 1;
+}
+
+/* Lockstep dense batches: each member's rhs[0] receives its order, and the
+   batch records the size classes it mixed (a class is the power of two
+   ceil(order / 256) rounded up) and its device footprint sum. */
+static long long g_batch_max_order = 4096;
+int fake_dense_runs(void) { return g_dense_runs; }
+int fake_dense_peak(void) { return g_dense_peak; }
+int fake_dense_mixed_classes(void) { return g_dense_mixed_classes; }
+long long n2d_lu_batch_max_order(void) { return g_batch_max_order; }
+
+static size_t fake_class(size_t n)
+{
+  size_t c = 1;
+  while(c * 256 < n) c <<= 1;
+  return c;
+}
+
+int n2c_dense_solve_private_batch(size_t count, const size_t *order, const nec2c_cuda_complex *const *matrix,
+                                  const size_t *ld, nec2c_cuda_complex *const *rhs, const size_t *stride,
+                                  const size_t *rhs_count, int *status)
+{
+  (void)matrix; (void)ld; (void)stride; (void)rhs_count;
+  pthread_mutex_lock(&g_lock);
+  ++g_dense_runs;
+  if((int)count > g_dense_peak) g_dense_peak = (int)count;
+  for(size_t i = 1; i < count; ++i)
+    if(fake_class(order[i]) != fake_class(order[0])) ++g_dense_mixed_classes;
+  pthread_mutex_unlock(&g_lock);
+  hold(NULL, 0);
+  for(size_t i = 0; i < count; ++i) { rhs[i][0] = (double)order[i]; status[i] = 1; }
   return 1;
 }
 

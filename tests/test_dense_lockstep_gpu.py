@@ -1,0 +1,98 @@
+"""Lockstep batch of FP64 factorisations (one launch per kernel and panel
+step for every system of a ragged batch), through the C ABI: each system's
+pivots and factors bit for bit those of its own classic factorisation (the
+kernels are the same), its solution within 1e-12 of its own classic solve
+and of the oracle; a singular system is reported without disturbing the
+others; orders above the batch limit take the classic path.  Then the
+request server's dense merging: queued requests of one size class run as
+lockstep batches with each result equal to the same request served alone."""
+import numpy as np
+import pytest
+
+import nec2c_b200 as nb
+from oracle_lib import oracle, ptr
+from test_dense_gpu import mom_like, nec_storage
+
+pytestmark = pytest.mark.gpu
+
+
+def test_lockstep_batch_matches_single():
+    assert nb.dense_backend_set("cuda")
+    cap = nb.load().nec2c_cuda_dense_batch_max_order()
+    assert cap in (2048, 4096)
+    sizes = [65, 100, 257, 300, 511, 700, 1100, 300, 2100, 2500, 40, 5000]
+    sizes = [n for n in sizes if n <= cap or n == 5000]
+    systems, ref = [], []
+    for k, n in enumerate(sizes):
+        a = mom_like(n, 1200 + k)
+        if k == 7:
+            a[:, 5] = 0.0            # singular
+        ld = n + (k % 4)
+        st = nec_storage(a, ld)
+        rng = np.random.default_rng(50 + k)
+        x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        b = np.ascontiguousarray(a @ x)
+        systems.append((st, b.copy()))
+        ref.append((a, st.copy(order="F"), b, ld, x))
+    ok, status, pivs = nb.solve_batched(systems)
+    assert not ok                    # the singular one
+    for k, (n, (st, xb), piv, (a, st0, b, ld, x)) in enumerate(zip(sizes, systems, pivs, ref)):
+        if k == 7:
+            assert status[k] == 0
+            continue
+        assert status[k] == 1, (k, nb.last_error())
+        single = st0.copy(order="F")
+        ok1, p1 = nb.factor_classic(single)
+        assert ok1, nb.last_error()
+        assert np.array_equal(piv, p1), (k, n)
+        if 64 < n <= cap:            # lockstep batch: the classic kernels, bit for bit
+            assert np.array_equal(st[:n, :n], single[:n, :n]), (k, n)
+        else:                        # the one-launch small-system kernel / the classic path
+            assert np.max(np.abs(st[:n, :n] - single[:n, :n])) / np.max(np.abs(single[:n, :n])) < 1e-12, (k, n)
+        xs = np.zeros((ld, 1), dtype=np.complex128, order="F")
+        xs[:n, 0] = b
+        assert nb.solve_classic_many(single, p1, xs)
+        assert np.linalg.norm(xb - xs[:n, 0]) / np.linalg.norm(xs[:n, 0]) < 1e-12, (k, n)
+        assert np.linalg.norm(xb - x) / np.linalg.norm(x) < 1e-9, (k, n)
+        if n <= 700:
+            po = np.zeros(n, dtype=np.int32)
+            assert oracle().oracle_factr(n, ptr(st0), ptr(po), ld)
+            assert np.array_equal(piv, po), (k, n)
+            bo = b.copy()
+            oracle().oracle_solve(n, ptr(st0), ptr(po), ptr(bo), ld)
+            assert np.linalg.norm(xb - bo) / np.linalg.norm(bo) < 1e-12, (k, n)
+    nb.load().nec2c_cuda_dense_release()
+
+
+def test_server_merges_dense_requests():
+    assert nb.dense_backend_set("cuda")
+    orders = [300, 320, 400, 480, 350, 300, 700, 900, 1000, 600, 290, 310, 1800, 1200, 64, 200]
+    mats, rhss = [], []
+    for k, n in enumerate(orders):
+        a = mom_like(n, 1400 + k)
+        mats.append(np.asfortranarray(a.T))
+        rng = np.random.default_rng(80 + k)
+        rhss.append(np.asfortranarray((a @ (rng.standard_normal(n) + 1j * rng.standard_normal(n))).reshape(n, 1)))
+
+    def serve(merge, slots):
+        srv = nb.Server(slots=slots)
+        if merge:
+            srv.merge_dense(merge)
+        outs, reqs = [], []
+        for m, b in zip(mats, rhss):
+            o = b.copy(order="F")
+            reqs.append(srv.dense(m, o))
+            outs.append(o)
+        srv.drain()
+        res = [(bool(r.status), int(r.merged)) for r in reqs]
+        srv.close()
+        return outs, res
+
+    alone, res1 = serve(0, 1)
+    assert all(ok and m == 1 for ok, m in res1)
+    for _ in range(2):               # twice: the batch state starts clean every run
+        merged, res2 = serve(6, 2)
+        assert all(ok for ok, _ in res2)
+        assert max(m for _, m in res2) >= 2
+        for k, (x, y) in enumerate(zip(merged, alone)):
+            assert np.linalg.norm(x - y) / np.linalg.norm(y) < 1e-12, (k, orders[k])

@@ -41,6 +41,7 @@ def fake():
     lib.fake_hybrid_batch.argtypes = [vp, sz]
     lib.fake_hybrid_batch.restype = vp
     lib.nec2c_cuda_server_merge_batch.argtypes = [vp, vp]
+    lib.nec2c_cuda_server_merge_dense.argtypes = [vp, sz]
     lib.fake_release.argtypes = [vp]
     lib.nec2c_cuda_server_create.argtypes = [C.POINTER(vp), C.c_int, C.c_int, sz, C.c_int]
     lib.nec2c_cuda_server_submit.argtypes = [vp, C.POINTER(nb.Request)]
@@ -255,3 +256,47 @@ def test_queued_volume_requests_merge(fake):
     srv.close()
     for o in (batch, lone, *hyb, *plans):
         fake.fake_release(o)
+
+
+def test_queued_dense_requests_merge(fake):
+    """Dense requests that queue behind busy workers run as lockstep batches
+    of one size class (orders up to 256, 512, 1024, 2048, 4096), at most the
+    registered count per batch and within the device budget; each request
+    gets its own result; orders above the batch limit and a split-precision
+    server do not merge."""
+    fake.fake_reset(20000, 10 * GIB)
+    srv = Server(fake, slots=2)
+    assert fake.nec2c_cuda_server_merge_dense(srv.h, 4)
+    blockers = [srv.dense(64)[0] for _ in range(2)]           # both workers busy
+    orders = [300, 400, 500, 310, 320, 1000, 700, 900, 5000, 2000, 1500, 330]
+    reqs = [(n, srv.dense(n)) for n in orders]
+    srv.drain()
+    assert fake.fake_dense_runs() >= 2 and fake.fake_dense_peak() == 4
+    assert fake.fake_dense_mixed_classes() == 0
+    for n, (r, rhs) in reqs:
+        assert r.done and r.status, r.error
+        assert rhs[0] == n                                    # its own result
+    big = dict((n, r) for n, (r, _) in reqs)[5000]
+    assert big.merged == 1                                    # above the batch limit
+    assert sum(1 for _, (r, _) in reqs if r.merged > 1) >= 6
+    assert all(r.status for r in blockers)
+    srv.close()
+
+    # The budget bounds a merged run: room for two of order 300 at a time.
+    fake.fake_reset(20000, 10 * GIB)
+    budget = 2 * footprint(300) + footprint(300) // 2
+    srv = Server(fake, slots=1, budget=budget)
+    assert fake.nec2c_cuda_server_merge_dense(srv.h, 8)
+    first = srv.dense(64)[0]
+    rest = [srv.dense(300)[0] for _ in range(6)]
+    srv.drain()
+    assert fake.fake_dense_peak() == 2
+    assert all(r.status and r.merged <= 2 for r in rest)
+    srv.close()
+
+    split = C.c_void_p()
+    assert fake.nec2c_cuda_server_create(C.byref(split), 0, 1, 0, 1)
+    assert not fake.nec2c_cuda_server_merge_dense(split, 4)
+    assert b"split-precision" in fake.nec2c_cuda_last_error()
+    assert fake.nec2c_cuda_server_merge_dense(split, 1)       # off is always accepted
+    fake.nec2c_cuda_server_destroy(split)
