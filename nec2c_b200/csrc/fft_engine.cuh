@@ -119,6 +119,10 @@ template <typename C> struct PassArgs {
   long long A_in, A_out;        // axis extent stored in the input / output array
   int n_in, n_out;    // nonzero inputs (rest is zero padding) / outputs kept
   int NL;             // lines per tile
+  // Strided passes: pow2 = 1 when NL and I (and, for the product pass, Pz)
+  // are powers of two, whose logarithms follow; the index arithmetic then
+  // shifts instead of dividing by runtime values.
+  int pow2, nl_log2, i_log2, pz_log2;
   const int *gate;    // skip all work when *gate == 0 (NULL: always run)
   long long comp_in, comp_out;  // product pass: distance between the 3 components
   long long spec_comp;          // product pass: distance between spectrum slots
@@ -129,6 +133,7 @@ template <typename C> struct PassArgs {
   double2 *cy;                  // cell vector y (3 per cell)
   const double2 *eps;           // per-cell permittivity
   const int *box_cell;          // box index -> cell (-1: empty)
+  int box_identity;             // z passes: box_cell is the identity (not read)
   double2 self0, self1, self2;  // self terms of the Jacobi divisor
   long long nxy, mirror;        // lines per component; PEC physical cells (0: none)
   int precondition;             // input is v, the operator acts on v ./ diag
@@ -205,9 +210,14 @@ __device__ __forceinline__ Fold fold(int k, int P) {
   return f;
 }
 
+// x / NL for the strided passes' work items.
+template <typename C> __device__ __forceinline__ int div_nl(const PassArgs<C> &a, int x) {
+  return a.pow2 ? x >> a.nl_log2 : x / a.NL;
+}
+
 template <typename C>
 __device__ __forceinline__ void line_base(const PassArgs<C> &a, long long l, long long &bin, long long &bout) {
-  const long long b = l / a.I, i = l - b * a.I;
+  const long long b = a.pow2 ? l >> a.i_log2 : l / a.I, i = l - b * a.I;
   bin = b * a.A_in * a.I + i;
   bout = b * a.A_out * a.I + i;
 }
@@ -222,7 +232,7 @@ __device__ __forceinline__ void fft_forward_tile(const PassArgs<C> &a, long long
   const int NL = a.NL;
   const long long l0 = tile * NL;
   for (int item = threadIdx.x; item < NL * R2; item += blockDim.x) {
-    const int t = item & (NL - 1), j2 = item / NL;
+    const int t = item & (NL - 1), j2 = div_nl(a, item);
     const long long l = l0 + t;
     if (l >= a.lines) continue;
     long long bin, bout;
@@ -243,7 +253,7 @@ __device__ __forceinline__ void fft_forward_tile(const PassArgs<C> &a, long long
   }
   __syncthreads();
   for (int item = threadIdx.x; item < NL * R1; item += blockDim.x) {
-    const int t = item & (NL - 1), k1 = item / NL;
+    const int t = item & (NL - 1), k1 = div_nl(a, item);
     const long long l = l0 + t;
     if (l >= a.lines) continue;
     long long bin, bout;
@@ -276,7 +286,7 @@ __device__ __forceinline__ void fft_inverse_tile(const PassArgs<C> &a, long long
   const long long l0 = tile * NL;
   double sq = 0;
   for (int item = threadIdx.x; item < NL * R1; item += blockDim.x) {
-    const int t = item & (NL - 1), k1 = item / NL;
+    const int t = item & (NL - 1), k1 = div_nl(a, item);
     const long long l = l0 + t;
     if (l >= a.lines) continue;
     long long bin, bout;
@@ -296,7 +306,7 @@ __device__ __forceinline__ void fft_inverse_tile(const PassArgs<C> &a, long long
   }
   __syncthreads();
   for (int item = threadIdx.x; item < NL * R2; item += blockDim.x) {
-    const int t = item & (NL - 1), n1 = item / NL;
+    const int t = item & (NL - 1), n1 = div_nl(a, item);
     const long long l = l0 + t;
     if (l >= a.lines) continue;
     long long bin, bout;
@@ -349,8 +359,8 @@ __device__ __forceinline__ void fft_product_tile(const PassArgs<C> &a, long long
   const int NL = a.NL, L = R1 * R2;
   const long long l0 = tile * NL;
   for (int item = threadIdx.x; item < 3 * NL * R2; item += blockDim.x) {
-    const int c = item / (NL * R2), rem = item - c * NL * R2;
-    const int t = rem & (NL - 1), j2 = rem / NL;
+    const int c = div_nl(a, item) / R2, rem = item - c * NL * R2;
+    const int t = rem & (NL - 1), j2 = div_nl(a, rem);
     const long long l = l0 + t;
     if (l >= a.lines) continue;
     const C *in = a.in + c * a.comp_in + l;
@@ -370,7 +380,7 @@ __device__ __forceinline__ void fft_product_tile(const PassArgs<C> &a, long long
   }
   __syncthreads();
   for (int item = threadIdx.x; item < NL * R1; item += blockDim.x) {
-    const int t = item & (NL - 1), k1 = item / NL;
+    const int t = item & (NL - 1), k1 = div_nl(a, item);
     const long long l = l0 + t;
     if (l >= a.lines) continue;
     C s0[R2], s1[R2], s2[R2];
@@ -382,7 +392,7 @@ __device__ __forceinline__ void fft_product_tile(const PassArgs<C> &a, long long
     dft_reg<R2, false, R1>(s0, a.tw);
     dft_reg<R2, false, R1>(s1, a.tw);
     dft_reg<R2, false, R1>(s2, a.tw);
-    const int ky = (int)(l / a.Pz), kz = (int)(l - (long long)ky * a.Pz);
+    const int ky = (int)(a.pow2 ? l >> a.pz_log2 : l / a.Pz), kz = (int)(l - (long long)ky * a.Pz);
     const Fold fy = fold(ky, a.Py), fz = fold(kz, a.Pz);
     const long long yz = (long long)fy.idx * a.Hz + fz.idx;
 #pragma unroll
@@ -413,8 +423,8 @@ __device__ __forceinline__ void fft_product_tile(const PassArgs<C> &a, long long
   }
   __syncthreads();
   for (int item = threadIdx.x; item < 3 * NL * R2; item += blockDim.x) {
-    const int c = item / (NL * R2), rem = item - c * NL * R2;
-    const int t = rem & (NL - 1), n1 = rem / NL;
+    const int c = div_nl(a, item) / R2, rem = item - c * NL * R2;
+    const int t = rem & (NL - 1), n1 = div_nl(a, rem);
     const long long l = l0 + t;
     if (l >= a.lines) continue;
     const C *Sc = S + c * L * NL;
@@ -552,7 +562,8 @@ __device__ __forceinline__ void fft_zline_tile(const PassArgs<C> &a, long long t
         if (idx < total) {
           const int rest = idx / 3, e = rest % L, p = rest / L;
           const long long pos = p0 + p;
-          if (e < a.n_in && pos < a.nxy) cell[i] = a.box_cell[pos * a.A_in + e];
+          if (e < a.n_in && pos < a.nxy)
+            cell[i] = a.box_identity ? (int)(pos * a.A_in + e) : a.box_cell[pos * a.A_in + e];
         }
       }
       double2 v[CH], ep[CH];
@@ -611,7 +622,7 @@ __device__ __forceinline__ void fft_zline_tile(const PassArgs<C> &a, long long t
           const int rest = idx / 3, p = fdiv(rest, a.nout_div), e = rest - p * a.n_out;
           const long long pos = p0 + p;
           if (pos < a.nxy) {
-            const int cl = a.box_cell[pos * a.A_out + e];
+            const int cl = a.box_identity ? (int)(pos * a.A_out + e) : a.box_cell[pos * a.A_out + e];
             if (cl >= 0 && !(a.mirror && cl >= a.mirror)) cell[i] = cl;
           }
         }

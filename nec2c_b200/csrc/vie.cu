@@ -97,6 +97,22 @@ static int zline_tile(int mode, int L, int unit, long long groups) {
   return best;
 }
 
+// log2(v) for a power of two v > 0, else -1.
+static int ilog2_exact(long long v) {
+  if (v <= 0 || (v & (v - 1))) return -1;
+  int k = 0;
+  while ((1LL << k) < v) ++k;
+  return k;
+}
+
+// Shift forms of the strided passes' index arithmetic (PassArgs::pow2), set
+// once NL, I and Pz are final.
+template <typename C> static void set_shifts(PassArgs<C> &a) {
+  const int nl = ilog2_exact(a.NL), ii = ilog2_exact(a.I), pz = a.Pz ? ilog2_exact(a.Pz) : 0;
+  a.pow2 = nl >= 0 && ii >= 0 && pz >= 0;
+  a.nl_log2 = nl; a.i_log2 = ii; a.pz_log2 = pz;
+}
+
 // One axis transform over a batch of lines.  Element e of line (b, i) lives at
 // (b*A + e)*I + i; lines = B*I.  Strided lines (I > 1) take the tile height
 // and radix split of `ch` (heuristic height when ch.nl == 0); contiguous lines
@@ -117,6 +133,7 @@ static int axis_pass(int mode, int L, const C *in, C *out, const C *tw, long lon
     return fft_launch_pass<C>(mode + 5, L, 0, a, (size_t)2 * (a.NL + 1) * L * sizeof(C), tiles);
   }
   a.NL = ch.nl ? ch.nl : lines_per_tile(L, 1, sizeof(C));
+  set_shifts(a);
   const long long tiles = (a.lines + a.NL - 1) / a.NL;
   return fft_launch_pass<C>(mode, L, ch.radix, a, (size_t)L * a.NL * sizeof(C), tiles);
 }
@@ -143,6 +160,7 @@ static void product_plan(const n2d_vie *p, const C *in, C *out, const C *tw, con
   a.Py = (int)p->P[1]; a.Pz = (int)p->P[2]; a.Hy = (int)p->H[1]; a.Hz = (int)p->H[2];
   a.NL = ch.nl ? ch.nl : lines_per_tile(L, 3, sizeof(C));
   a.gate = n2c_gate();
+  set_shifts(a);
   pp->mode = 2; pp->L = L; pp->variant = ch.radix;
   pp->smem = (size_t)3 * L * a.NL * sizeof(C);
   pp->tiles = (a.lines + a.NL - 1) / a.NL;
@@ -158,6 +176,7 @@ static void strided_plan(int mode, int L, const C *in, C *out, const C *tw, long
   a.lines = B * I; a.I = I; a.A_in = A_in; a.A_out = A_out; a.n_in = n_in; a.n_out = n_out;
   a.gate = n2c_gate();
   a.NL = ch.nl ? ch.nl : lines_per_tile(L, 1, sizeof(C));
+  set_shifts(a);
   pp->mode = mode; pp->L = L; pp->variant = ch.radix;
   pp->smem = (size_t)L * a.NL * sizeof(C);
   pp->tiles = (a.lines + a.NL - 1) / a.NL;
@@ -520,6 +539,10 @@ extern "C" int n2d_vie_create(n2d_vie **out, const long long shape[3], const lon
   }
   std::vector<int> inv(p->nbox, -1);
   for (long long c = 0; c < cells; ++c) inv[cell_box[c]] = (int)c;
+  // A lattice filled in box order (every box a cell, cell c in box c) lets
+  // the z passes index cells directly.
+  p->box_identity = cells == p->nbox;
+  for (long long c = 0; p->box_identity && c < cells; ++c) p->box_identity = cell_box[c] == c;
   for (int d = 0; d < 3; ++d) {
     std::vector<float2> t32(padded[d]);
     for (long long j = 0; j < padded[d]; ++j)
@@ -670,6 +693,7 @@ static int z_cell_plan(int mode, n2d_vie *p, const C *in, C *out, const C *tw, c
   a.nout_div = div_magic(a.n_out);
   a.gate = n2c_gate();
   a.cx = x; a.cy = y; a.eps = p->eps; a.box_cell = p->box_cell;
+  a.box_identity = p->box_identity && !p->mirror;
   a.self0 = p->self[0]; a.self1 = p->self[1]; a.self2 = p->self[2];
   a.nxy = nx * ny; a.mirror = p->mirror; a.precondition = precondition;
   a.flag = flag; a.partials = p->partials; a.ticket = p->ticket; a.norm = norm;

@@ -22,6 +22,7 @@ struct n2d_vie {
   long long mirror;         // >0: PEC image embedding, cells = 2*mirror (images last)
   int *cell_box;            // [cells] box index of each cell
   int *box_cell;            // [nbox] cell index or -1
+  int box_identity;         // 1: every box holds a cell and cell index == box index
   double2 *eps;             // [cells]
   double2 *diag;            // [3 cells] eps - (eps-1) self[i]
   double2 self[3];
