@@ -19,7 +19,6 @@
 #include "device_api.h"
 #include <atomic>
 #include <mutex>
-#include <stdlib.h>
 #include "fft_passes.cuh"
 #include "runtime.cuh"
 #include "vie_internal.cuh"
@@ -163,6 +162,7 @@ static void product_plan(const n2d_vie *p, const C *in, C *out, const C *tw, con
   set_shifts(a);
   pp->mode = 2; pp->L = L; pp->variant = ch.radix;
   pp->smem = (size_t)3 * L * a.NL * sizeof(C);
+
   pp->tiles = (a.lines + a.NL - 1) / a.NL;
 }
 
@@ -888,12 +888,12 @@ float time_candidate(n2d_vie *p, int pass, n2d_pass_choice ch, const double2 *x,
 }
 
 // Milliseconds of three whole products with the plan's current schedule
-// (best of two runs), or a negative value when a product fails.
+// (best of three runs), or a negative value when a product fails.
 template <typename C>
 float time_product(n2d_vie *p, const double2 *x, double2 *y, double *norm, cudaEvent_t e0, cudaEvent_t e1) {
   if (!apply_t<C>(p, x, y, 0, norm, nullptr)) return -1.0f;
   float best = -1.0f;
-  for (int trial = 0; trial < 2; ++trial) {
+  for (int trial = 0; trial < 3; ++trial) {
     if (cudaEventRecord(e0, n2c_stream()) != cudaSuccess) return -1.0f;
     for (int r = 0; r < 3; ++r)
       if (!apply_t<C>(p, x, y, 0, norm, nullptr)) return -1.0f;
@@ -952,6 +952,31 @@ int tune_precision(n2d_vie *p, const double2 *x, double2 *y, double *norm, bool 
     chosen[pass] = best;
   }
   memcpy(p->sched[prec], chosen, sizeof(chosen));
+  // Whole-product refinement: a pass timed alone (its input warm in L2, no
+  // neighbours) can favour a height that loses inside a product, so each
+  // pass's neighbouring heights are tried in whole products as well and
+  // replace the choice when at least 2% faster.
+  {
+    p->planes[prec] = 0;   // the five passes (the plane forms are weighed below)
+    float tb = time_product<C>(p, x, y, norm, e0, e1);
+    for (int pass = 0; tb >= 0 && pass < N2D_VIE_PASSES; ++pass) {
+      const std::vector<int> hs = candidate_heights<C>(p, pass);
+      int at = -1;
+      for (int i = 0; i < (int)hs.size(); ++i)
+        if (hs[i] == chosen[pass].nl) at = i;
+      if (at < 0) continue;
+      const int reach = pass == 0 || pass == 4 ? 2 : 1;
+      for (int i = at - reach; i <= at + reach; ++i) {
+        if (i < 0 || i >= (int)hs.size() || i == at) continue;
+        const n2d_pass_choice keep = p->sched[prec][pass];
+        p->sched[prec][pass] = n2d_pass_choice{hs[i], chosen[pass].radix};
+        const float t = time_product<C>(p, x, y, norm, e0, e1);
+        if (t >= 0 && t < 0.98f * tb) tb = t;
+        else p->sched[prec][pass] = keep;
+      }
+      chosen[pass] = p->sched[prec][pass];
+    }
+  }
   // Whole products: the five tuned passes against the fused plane passes
   // around the tuned x pass; the planes are kept when at least 3% faster.
   int planes = 0;
