@@ -55,6 +55,15 @@ def parse():
                          "tune on serialised, slowed launches)")
     ap.add_argument("--lu-order", type=int, default=1984,
                     help="lu profiling mode: order of the seeded MoM-like matrix (config 1: 1984)")
+    ap.add_argument("--c4-arms", default=None,
+                    help="serving_c4 profiling mode: a long-stream run of only these arms (mixed[,plain]): "
+                         "the mixed form saturated and under Poisson arrivals, the plain FP64 form on the "
+                         "first --c4-plain-requests requests")
+    ap.add_argument("--c4-rates", default=None,
+                    help="serving_c4 profiling mode: comma-separated Poisson rates as fractions of the "
+                         "mixed form's saturated request rate")
+    ap.add_argument("--c4-plain-requests", type=int, default=None,
+                    help="serving_c4 long-stream run: requests of the plain FP64 arm (a prefix of the stream)")
     ap.add_argument("--requests", type=int, default=240,
                     help="serving_c4 profiling mode: requests in the stream (config 4 names 10,000)")
     ap.add_argument("--planes", type=int, choices=[0, 1], default=None,
@@ -408,7 +417,10 @@ def run_ours(args, rank, world, local_rank):
         print(json.dumps({"profile": "serving", "serving_c4": serving_bench(nb, torch)}))
         return 0
     if args.only == "serving_c4":
-        print(json.dumps({"profile": "serving_c4", "serving_c4_stream": serving_stream_c4(nb, torch, args.requests)}))
+        rates = tuple(float(r) for r in args.c4_rates.split(",")) if args.c4_rates else (0.3, 0.5, 0.7, 0.9, 1.1)
+        arms = set(args.c4_arms.split(",")) if args.c4_arms else None
+        print(json.dumps({"profile": "serving_c4", "serving_c4_stream": serving_stream_c4(
+            nb, torch, args.requests, rates=rates, arms=arms, plain_requests=args.c4_plain_requests)}))
         return 0
     if args.only == "coupling":
         print(json.dumps({"profile": "coupling", "coupling_c0": coupling_bench(nb, args.steps)}))
@@ -1311,7 +1323,7 @@ DENSE_MERGE = 16
 
 
 def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0.5, 0.7, 0.9, 1.1),
-                      lattices=(8, 16, 24, 32, 48), seed=11):
+                      lattices=(8, 16, 24, 32, 48), seed=11, arms=None, plain_requests=None):
     """BASELINE config 4 shaped stream through the request server.
 
     Requests: 60% dense MoM models (orders log-uniform in 200-3000, ten orders
@@ -1424,7 +1436,7 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
     # The frequencies each request asks for: F distinct ones of its model's 16.
     fsets = [np.sort(rng.choice(len(freqs), int(F), replace=False)) for F in fsel]
 
-    def run(models, split, slots_, gaps, merge, only=None):
+    def run(models, split, slots_, gaps, merge, only=None, limit=None):
         srv = nb.Server(slots=slots_, split=split)
         if merge:
             for mdl in models:
@@ -1450,7 +1462,7 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
                 while time.perf_counter() < target:
                     time.sleep(min(1e-3, max(0.0, target - time.perf_counter())))
             subs = []
-            if only is not None and bool(kinds[i]) != only:
+            if (only is not None and bool(kinds[i]) != only) or (limit is not None and i >= limit):
                 continue
             if kinds[i]:
                 pi = picks[i] % len(dense_pool)
@@ -1508,43 +1520,58 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
            "slots": slots, "setup_s": time.perf_counter() - t0,
            "device_gb_in_use_after_setup": (lambda f: (f[1] - f[0]) / 1e9)(torch.cuda.mem_get_info())}
     sat = {}
-    runs = [run(m32, False, slots, None, True) for _ in range(2)]
-    sat["mixed"], sols_mixed = max(runs, key=lambda r: r[0]["solves_per_s"])
-    sat["mixed_unmerged"], _ = run(m32, False, slots, None, False)
-    sat["mixed_split_lu"], sols_split = run(m32, True, slots, None, True)
-    runs = [run(m64, False, slots, None, True) for _ in range(2)]
-    sat["fp64"], sols_fp64 = max(runs, key=lambda r: r[0]["solves_per_s"])
-    plain, sols_plain = run(m64, False, 1, None, False)
+    if arms is not None:
+        # A long stream: the mixed form at saturation and under Poisson
+        # arrivals, and (arms holding "plain") the plain FP64 form on the
+        # first plain_requests requests; its throughput per solve does not
+        # depend on the stream's length.
+        sat["mixed"], _ = run(m32, False, slots, None, True)
+        out["saturation"] = sat
+        if "plain" in arms:
+            pl, _ = run(m64, False, 1, None, False, None, plain_requests)
+            pl["first_requests"] = plain_requests
+            out["plain_fp64_one_at_a_time"] = pl
+            out["mixed_vs_plain_fp64"] = sat["mixed"]["solves_per_s"] / pl["solves_per_s"]
+    else:
+        runs = [run(m32, False, slots, None, True) for _ in range(2)]
+        sat["mixed"], sols_mixed = max(runs, key=lambda r: r[0]["solves_per_s"])
+        sat["mixed_unmerged"], _ = run(m32, False, slots, None, False)
+        sat["mixed_split_lu"], sols_split = run(m32, True, slots, None, True)
+        runs = [run(m64, False, slots, None, True) for _ in range(2)]
+        sat["fp64"], sols_fp64 = max(runs, key=lambda r: r[0]["solves_per_s"])
+        plain, sols_plain = run(m64, False, 1, None, False)
 
-    def rel_err(a, b):
-        return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+        def rel_err(a, b):
+            return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
 
-    def worst(sols, ref, kind):
-        errs = [rel_err(v, ref[k]) for k, v in sols.items() if k[0] == kind and k in ref]
-        return max(errs) if errs else None
-    # Current error of each form against the plain FP64 form on the same
-    # systems (volume: GMRES to rtol 1e-6 in both, so the difference is the
-    # solver's tolerance as much as the precision).
-    out["error_vs_plain_fp64"] = {
-        "mixed": {"volume_current": worst(sols_mixed, sols_plain, "volume"),
-                  "dense_current": worst(sols_mixed, sols_plain, "dense")},
-        "mixed_split_lu": {"volume_current": worst(sols_split, sols_plain, "volume"),
-                           "dense_current": worst(sols_split, sols_plain, "dense")},
-        "fp64_merged": {"volume_current": worst(sols_fp64, sols_plain, "volume"),
-                        "dense_current": worst(sols_fp64, sols_plain, "dense")}}
-    out["saturation"] = sat
-    out["plain_fp64_one_at_a_time"] = plain
-    # Each kind of request alone (the same requests), both forms: where the
-    # mixed stream's time goes.
-    out["by_kind"] = {}
-    for name, only in (("dense", True), ("volume", False)):
-        mx, _ = run(m32, False, slots, None, True, only)
-        pl, _ = run(m64, False, 1, None, False, only)
-        out["by_kind"][name] = {"mixed": mx, "plain_fp64_one_at_a_time": pl,
-                                "mixed_vs_plain_fp64": mx["solves_per_s"] / pl["solves_per_s"]}
-    out["mixed_vs_plain_fp64"] = sat["mixed"]["solves_per_s"] / plain["solves_per_s"]
-    out["mixed_split_lu_vs_plain_fp64"] = sat["mixed_split_lu"]["solves_per_s"] / plain["solves_per_s"]
-    out["fp64_batched_vs_plain_fp64"] = sat["fp64"]["solves_per_s"] / plain["solves_per_s"]
+        def worst(sols, ref, kind):
+            errs = [rel_err(v, ref[k]) for k, v in sols.items() if k[0] == kind and k in ref]
+            return max(errs) if errs else None
+        # Current error of each form against the plain FP64 form on the same
+        # systems (volume: GMRES to rtol 1e-6 in both, so the difference is
+        # the solver's tolerance as much as the precision).
+        out["error_vs_plain_fp64"] = {
+            "mixed": {"volume_current": worst(sols_mixed, sols_plain, "volume"),
+                      "dense_current": worst(sols_mixed, sols_plain, "dense")},
+            "mixed_split_lu": {"volume_current": worst(sols_split, sols_plain, "volume"),
+                               "dense_current": worst(sols_split, sols_plain, "dense")},
+            "fp64_merged": {"volume_current": worst(sols_fp64, sols_plain, "volume"),
+                            "dense_current": worst(sols_fp64, sols_plain, "dense")}}
+        out["saturation"] = sat
+        out["plain_fp64_one_at_a_time"] = plain
+        # Each kind of request alone (the same requests), both forms: where
+        # the mixed stream's time goes; volume requests also unmerged.
+        out["by_kind"] = {}
+        for name, only in (("dense", True), ("volume", False)):
+            mx, _ = run(m32, False, slots, None, True, only)
+            pl, _ = run(m64, False, 1, None, False, only)
+            out["by_kind"][name] = {"mixed": mx, "plain_fp64_one_at_a_time": pl,
+                                    "mixed_vs_plain_fp64": mx["solves_per_s"] / pl["solves_per_s"]}
+            if not only:
+                out["by_kind"][name]["mixed_unmerged"], _ = run(m32, False, slots, None, False, only)
+        out["mixed_vs_plain_fp64"] = sat["mixed"]["solves_per_s"] / plain["solves_per_s"]
+        out["mixed_split_lu_vs_plain_fp64"] = sat["mixed_split_lu"]["solves_per_s"] / plain["solves_per_s"]
+        out["fp64_batched_vs_plain_fp64"] = sat["fp64"]["solves_per_s"] / plain["solves_per_s"]
     sweep = []
     for frac in rates:
         rate = frac * sat["mixed"]["requests_per_s"]
