@@ -53,6 +53,9 @@ def parse():
                     help="JSON file of the c2 plans' FFT pass schedules: written by the first run "
                          "that names it, pinned by later runs (a run under ncu would otherwise "
                          "tune on serialised, slowed launches)")
+    ap.add_argument("--lu-systems", type=int, default=0,
+                    help="lu_batch profiling mode: one batch of this many systems of order --lu-order "
+                         "(0: the default table of orders and batch sizes)")
     ap.add_argument("--lu-order", type=int, default=1984,
                     help="lu profiling mode: order of the seeded MoM-like matrix (config 1: 1984)")
     ap.add_argument("--c4-arms", default=None,
@@ -411,7 +414,10 @@ def run_ours(args, rank, world, local_rank):
     if args.only == "lu":
         return lu_driver(args, nb, torch, stream)
     if args.only == "lu_batch":
-        print(json.dumps({"profile": "lu_batch", "lockstep_factor": lockstep_factor_bench(nb, torch, stream)}))
+        kw = {}
+        if args.lu_systems:
+            kw = {"orders": (args.lu_order,), "counts": (args.lu_systems,), "reps": max(1, args.steps)}
+        print(json.dumps({"profile": "lu_batch", "lockstep_factor": lockstep_factor_bench(nb, torch, stream, **kw)}))
         return 0
     if args.only == "serving":
         print(json.dumps({"profile": "serving", "serving_c4": serving_bench(nb, torch)}))
