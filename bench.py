@@ -767,6 +767,8 @@ def lockstep_factor_bench(nb, torch, stream, orders=(250, 1000, 2608), counts=(1
     batch = lib.n2d_lu_factor_batch
     batch.restype, batch.argtypes = C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                               C.c_void_p]
+    batch32 = lib.n2d_lu_factor32_batch
+    batch32.restype, batch32.argtypes = batch.restype, batch.argtypes
     out = []
     for n in orders:
         src = torch.from_numpy(c1_matrix(n)).cuda()
@@ -778,7 +780,7 @@ def lockstep_factor_bench(nb, torch, stream, orders=(250, 1000, 2608), counts=(1
             ns = (C.c_longlong * k)(*([n] * k))
             info = (C.c_int * k)()
 
-            def timed(fn):
+            def timed(fn, work, src):
                 best = None
                 for i in range(reps + 1):
                     for w in work:
@@ -796,11 +798,23 @@ def lockstep_factor_bench(nb, torch, stream, orders=(250, 1000, 2608), counts=(1
                 return best
             one = C.c_int(0)
             t_single = timed(lambda: all(single(w.data_ptr(), n, n, p.data_ptr(), 0, 0, C.byref(one))
-                                         for w, p in zip(work, piv)))
-            t_batch = timed(lambda: batch(ptrs, ns, ns, pps, k, 0, info))
+                                         for w, p in zip(work, piv)), work, src)
+            t_batch = timed(lambda: batch(ptrs, ns, ns, pps, k, 0, info), work, src)
+            # Split-precision lockstep on FP32 copies (even leading dimension):
+            # the factorisation alone, its refinement not included.
+            ld32 = n + (n & 1)
+            a32 = torch.zeros((n, 2 * ld32), dtype=torch.float32, device="cuda")
+            a32.view(torch.complex64)[:, :n] = src.to(torch.complex64)
+            work32 = [a32.clone() for _ in range(k)]
+            ptrs32 = (C.c_void_p * k)(*[w.data_ptr() for w in work32])
+            lds32 = (C.c_longlong * k)(*([ld32] * k))
+            t_split = timed(lambda: batch32(ptrs32, ns, lds32, pps, k, 0, info), work32, a32)
+            del work32, a32
             flops = k * 8.0 * n ** 3 / 3
             out.append({"order": n, "systems": k, "one_at_a_time_ms": t_single, "lockstep_ms": t_batch,
-                        "speedup": t_single / t_batch, "lockstep_tflops": flops / (t_batch * 1e-3) / 1e12})
+                        "speedup": t_single / t_batch, "lockstep_tflops": flops / (t_batch * 1e-3) / 1e12,
+                        "split_lockstep_factor_ms": t_split,
+                        "split_lockstep_tflops": flops / (t_split * 1e-3) / 1e12})
             del work, piv
     return out
 
@@ -1343,15 +1357,14 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
     (one per frequency); its latency runs from the first being queued to the
     last being done.
 
-    Forms (16 workers): `mixed` = FP32 transforms with the FP64 LU (the split
-    LU's refinement only adds latency at these orders), the server merging
-    queued volume requests on one model's frequencies into one batched solve
-    (each model's 16 frequency systems are one registered batch) and queued
-    dense requests of one size class into one lockstep factorisation (at most
-    DENSE_MERGE); `mixed_unmerged` = the same without merging;
-    `mixed_split_lu` = volume requests merged, with the split-precision LU
-    (its dense requests run one at a time); `fp64` = FP64 transforms, merged;
-    `plain_fp64_one_at_a_time` = FP64, one worker, no merging.  Saturation:
+    Forms (16 workers): `mixed` = FP32 transforms and the split-precision LU,
+    the server merging queued volume requests on one model's frequencies into
+    one batched solve (each model's 16 frequency systems are one registered
+    batch) and queued dense requests of one size class into one lockstep
+    factorisation (at most DENSE_MERGE) of FP32 copies on the tensor cores,
+    refined in FP64; `mixed_unmerged` = the same without merging;
+    `mixed_fp64_lu` = merged, FP32 transforms with the FP64 LU; `fp64` = FP64
+    transforms and LU, merged; `plain_fp64_one_at_a_time` = FP64, one worker, no merging.  Saturation:
     everything queued at once.  Poisson: request arrivals at the given
     fractions of the mixed form's saturated request rate (the sweep shows
     where p99 latency diverges).  Seeded synthetic matrices, lattices and
@@ -1447,10 +1460,9 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
         if merge:
             for mdl in models:
                 srv.merge(mdl["batch"])
-            # Queued dense requests of one size class factor in lockstep (the
-            # FP64 form; a split-precision server keeps them one at a time).
-            if not split:
-                srv.merge_dense(DENSE_MERGE)
+            # Queued dense requests of one size class factor in lockstep (on a
+            # split-precision server: FP32 tensor-core factors, FP64 refinement).
+            srv.merge_dense(DENSE_MERGE)
         # Warm every worker (stream state, kernel attributes) and every system.
         for mdl in models:
             for hs, b in zip(mdl["systems"], mdl["rhs"]):
@@ -1531,7 +1543,7 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
         # arrivals, and (arms holding "plain") the plain FP64 form on the
         # first plain_requests requests; its throughput per solve does not
         # depend on the stream's length.
-        sat["mixed"], _ = run(m32, False, slots, None, True)
+        sat["mixed"], _ = run(m32, True, slots, None, True)
         out["saturation"] = sat
         if "plain" in arms:
             pl, _ = run(m64, False, 1, None, False, None, plain_requests)
@@ -1539,10 +1551,10 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
             out["plain_fp64_one_at_a_time"] = pl
             out["mixed_vs_plain_fp64"] = sat["mixed"]["solves_per_s"] / pl["solves_per_s"]
     else:
-        runs = [run(m32, False, slots, None, True) for _ in range(2)]
+        runs = [run(m32, True, slots, None, True) for _ in range(2)]
         sat["mixed"], sols_mixed = max(runs, key=lambda r: r[0]["solves_per_s"])
-        sat["mixed_unmerged"], _ = run(m32, False, slots, None, False)
-        sat["mixed_split_lu"], sols_split = run(m32, True, slots, None, True)
+        sat["mixed_unmerged"], _ = run(m32, True, slots, None, False)
+        sat["mixed_fp64_lu"], sols_fp64lu = run(m32, False, slots, None, True)
         runs = [run(m64, False, slots, None, True) for _ in range(2)]
         sat["fp64"], sols_fp64 = max(runs, key=lambda r: r[0]["solves_per_s"])
         plain, sols_plain = run(m64, False, 1, None, False)
@@ -1559,8 +1571,8 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
         out["error_vs_plain_fp64"] = {
             "mixed": {"volume_current": worst(sols_mixed, sols_plain, "volume"),
                       "dense_current": worst(sols_mixed, sols_plain, "dense")},
-            "mixed_split_lu": {"volume_current": worst(sols_split, sols_plain, "volume"),
-                               "dense_current": worst(sols_split, sols_plain, "dense")},
+            "mixed_fp64_lu": {"volume_current": worst(sols_fp64lu, sols_plain, "volume"),
+                              "dense_current": worst(sols_fp64lu, sols_plain, "dense")},
             "fp64_merged": {"volume_current": worst(sols_fp64, sols_plain, "volume"),
                             "dense_current": worst(sols_fp64, sols_plain, "dense")}}
         out["saturation"] = sat
@@ -1569,20 +1581,20 @@ def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0
         # the mixed stream's time goes; volume requests also unmerged.
         out["by_kind"] = {}
         for name, only in (("dense", True), ("volume", False)):
-            mx, _ = run(m32, False, slots, None, True, only)
+            mx, _ = run(m32, True, slots, None, True, only)
             pl, _ = run(m64, False, 1, None, False, only)
             out["by_kind"][name] = {"mixed": mx, "plain_fp64_one_at_a_time": pl,
                                     "mixed_vs_plain_fp64": mx["solves_per_s"] / pl["solves_per_s"]}
             if not only:
-                out["by_kind"][name]["mixed_unmerged"], _ = run(m32, False, slots, None, False, only)
+                out["by_kind"][name]["mixed_unmerged"], _ = run(m32, True, slots, None, False, only)
         out["mixed_vs_plain_fp64"] = sat["mixed"]["solves_per_s"] / plain["solves_per_s"]
-        out["mixed_split_lu_vs_plain_fp64"] = sat["mixed_split_lu"]["solves_per_s"] / plain["solves_per_s"]
+        out["mixed_fp64_lu_vs_plain_fp64"] = sat["mixed_fp64_lu"]["solves_per_s"] / plain["solves_per_s"]
         out["fp64_batched_vs_plain_fp64"] = sat["fp64"]["solves_per_s"] / plain["solves_per_s"]
     sweep = []
     for frac in rates:
         rate = frac * sat["mixed"]["requests_per_s"]
         gaps = np.cumsum(np.random.default_rng(13).exponential(1.0 / rate, nreq))
-        res, _ = run(m32, False, slots, gaps, True)
+        res, _ = run(m32, True, slots, gaps, True)
         res["offered_requests_per_s"] = rate
         res["fraction_of_saturation"] = frac
         sweep.append(res)

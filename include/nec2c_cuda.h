@@ -449,11 +449,13 @@ int nec2c_cuda_server_merge_batch(nec2c_cuda_server *server, nec2c_cuda_vie_batc
    queued dense requests of the same size class (orders up to 256, 512, 1024,
    2048 or 4096: the cluster size of the first panel), as many as fit the
    device budget and at most max_systems in all, and factors and solves their
-   private matrix copies as one lockstep batch (the FP64 form, one launch per
-   kernel and panel step for all of them, each system's pivots and factors as
-   its own factorisation gives them).  Each request gets its own status;
-   `merged` tells how many ran together.  max_systems < 2 turns merging off.
-   Refused on a split-precision server. */
+   private matrix copies as one lockstep batch: one launch per kernel and
+   panel step for all of them, each system's pivots and factors as its own
+   factorisation gives them.  On an FP64 server the batch is the FP64 form; on
+   a split-precision server it factors FP32 copies with tensor-core (3xTF32)
+   updates and refines every system's solution in FP64 (report.iterations:
+   its refinement steps).  Each request gets its own status; `merged` tells
+   how many ran together.  max_systems < 2 turns merging off. */
 int nec2c_cuda_server_merge_dense(nec2c_cuda_server *server, size_t max_systems);
 /* Drains, stops the workers and frees the server. */
 void nec2c_cuda_server_destroy(nec2c_cuda_server *server);

@@ -221,11 +221,20 @@ size_t n2d_lu_batched_descriptor_bytes(long long count);
 int n2d_lu_factor_batch(double *const *a_dev, const long long *order, const long long *ld, int *const *ipiv_dev,
                         int count, int rule, int *info_host);
 long long n2d_lu_batch_max_order(void);
+/* The split-precision form of the same (FP32 matrices, even leading dims,
+   16-byte aligned; tensor-core 3xTF32 updates), factored as n2d_lu_factor32
+   would factor each. */
+int n2d_lu_factor32_batch(float *const *a_dev, const long long *order, const long long *ld, int *const *ipiv_dev,
+                          int count, int rule, int *info_host);
 /* Solves of count factored systems as n2d_lu_solve would, all at once:
    nrhs[i] columns of b_dev[i] (leading dim ldb[i]). */
 int n2d_lu_solve_batch(const double *const *a_dev, const long long *order, const long long *ld,
                        const int *const *ipiv_dev, double *const *b_dev, const long long *ldb,
                        const long long *nrhs, int count);
+/* The same with FP32 factors (FP64 arithmetic and right-hand sides). */
+int n2d_lu_solve32_batch(const float *const *a_dev, const long long *order, const long long *ld,
+                         const int *const *ipiv_dev, double *const *b_dev, const long long *ldb,
+                         const long long *nrhs, int count);
 /* In-place device transpose of an order x order block (leading dims lda/ldb). */
 int n2d_transpose(const double *src_dev, long long lds, double *dst_dev, long long ldd,
                   long long rows, long long cols);

@@ -1524,31 +1524,33 @@ extern "C" int n2d_lu_solve32(const float *a_dev, long long n, long long ld, con
 namespace {
 
 struct LuBatchEntry {
-  double2 *a;
+  void *a;         // double2 (FP64 form) or float2 (split-precision form)
   long long n, ld;
   int *ipiv;
   int *pairs;      // 4 KB ints of this matrix's interchange pairs
   LuStatus *st;
+  float *bt_hi, *bt_lo;   // split-precision form: packed U12 expansion (2n x 64 floats each)
 };
 
 __device__ __forceinline__ int batch_kb(long long n, long long k0) { return (int)(n - k0 < KB ? n - k0 : KB); }
 
-template <int CSZ, int RULE>
+template <int CSZ, int RULE, typename S>
 __global__ void __launch_bounds__(CPT, 1) panel_cluster_batch_kernel(const LuBatchEntry *e, long long k0) {
   const LuBatchEntry m = e[blockIdx.y];   // clusters run along x: one matrix per cluster
   if (m.n <= k0) return;
   PanelArgs p{};
   p.a = m.a; p.n = m.n; p.ld = m.ld; p.k0 = k0; p.kb = batch_kb(m.n, k0); p.rule = RULE;
   p.ipiv = m.ipiv; p.pairs = m.pairs; p.st = m.st;
-  panel_cluster_body<CSZ, RULE, double2>(p);
+  panel_cluster_body<CSZ, RULE, S>(p);
 }
 
+template <typename S>
 __global__ void __launch_bounds__(SWT) swap_trsm_batch_kernel(const LuBatchEntry *e, long long k0) {
   const LuBatchEntry m = e[blockIdx.y];
   if (m.n <= k0) return;
   const int kb = batch_kb(m.n, k0);
   if ((long long)blockIdx.x * (SWT / 32) >= m.n - kb) return;   // no column of this matrix in the block
-  swap_trsm_body<double2>(m.a, m.n, m.ld, k0, kb, m.pairs, m.st, nullptr, nullptr, blockIdx.x);
+  swap_trsm_body<S>((S *)m.a, m.n, m.ld, k0, kb, m.pairs, m.st, m.bt_hi, m.bt_lo, blockIdx.x);
 }
 
 // part 0: the next panel's columns (look-ahead); part 1: the columns after it.
@@ -1562,12 +1564,12 @@ __global__ void __launch_bounds__(256) gemm_update_batch_kernel(const LuBatchEnt
   const long long cols = part ? right - nb : nb;
   const long long row0 = blockIdx.y * (long long)GT, col0 = blockIdx.x * (long long)GT;
   if (right <= 0 || cols <= 0 || row0 >= right || col0 >= cols) return;
-  double2 *below = m.a + (k0 + kb) * m.ld;
-  gemm_update_body(below + cf, below + k0, m.a + k0 * m.ld + cf, right, cols, kb, m.ld, row0, col0);
+  double2 *a = (double2 *)m.a, *below = a + (k0 + kb) * m.ld;
+  gemm_update_body(below + cf, below + k0, a + k0 * m.ld + cf, right, cols, kb, m.ld, row0, col0);
 }
 
 struct SolveBatchEntry {
-  const double2 *a;
+  const void *a;      // double2 or float2 factors
   long long n, ld;
   const int *ipiv;
   double2 *b;
@@ -1578,28 +1580,30 @@ struct SolveBatchEntry {
 };
 
 // One CTA per (right-hand side, system).
+template <typename S>
 __global__ void __launch_bounds__(SOLVE_THREADS, 2) lu_solve_batch_kernel(const SolveBatchEntry *e) {
   const SolveBatchEntry m = e[blockIdx.y];
   if ((int)blockIdx.x >= m.nrhs) return;
-  lu_solve_body<double2>(m.a, m.n, m.ld, m.ipiv, m.b + blockIdx.x * m.ldb);
+  lu_solve_body<S>((const S *)m.a, m.n, m.ld, m.ipiv, m.b + blockIdx.x * m.ldb);
 }
 
 // gridDim.x co-resident CTAs per system (grid.y = system), each group on its
 // own barrier.
+template <typename S>
 __global__ void __launch_bounds__(SOLVE_COOP_THREADS) lu_solve_coop_batch_kernel(const SolveBatchEntry *e) {
   const SolveBatchEntry m = e[blockIdx.y];
-  lu_solve_coop_body<double2>(m.a, m.n, m.ld, m.ipiv, m.b, m.ldb, m.nrhs, m.scratch, m.sy);
+  lu_solve_coop_body<S>((const S *)m.a, m.n, m.ld, m.ipiv, m.b, m.ldb, m.nrhs, m.scratch, m.sy);
 }
 
-template <int CSZ>
+template <int CSZ, typename S>
 static cudaError_t launch_cluster_panel_batch(const LuBatchEntry *e, int count, long long k0, int rule,
                                               cudaStream_t s) {
   void (*kernel)(const LuBatchEntry *, long long) =
-      rule == 0 ? panel_cluster_batch_kernel<CSZ, 0> : panel_cluster_batch_kernel<CSZ, 1>;
+      rule == 0 ? panel_cluster_batch_kernel<CSZ, 0, S> : panel_cluster_batch_kernel<CSZ, 1, S>;
   if (CSZ > 8) {
-    static const bool opted = cudaFuncSetAttribute(panel_cluster_batch_kernel<CSZ, 0>,
+    static const bool opted = cudaFuncSetAttribute(panel_cluster_batch_kernel<CSZ, 0, S>,
                                                    cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess &&
-                              cudaFuncSetAttribute(panel_cluster_batch_kernel<CSZ, 1>,
+                              cudaFuncSetAttribute(panel_cluster_batch_kernel<CSZ, 1, S>,
                                                    cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
     if (!opted) return cudaErrorInvalidConfiguration;
   }
@@ -1618,14 +1622,15 @@ static cudaError_t launch_cluster_panel_batch(const LuBatchEntry *e, int count, 
 }
 
 // The batch's panels at step k0 (rows: the largest panel's row count).
+template <typename S>
 static int launch_panel_batch(const LuBatchEntry *e, int count, long long k0, long long rows, int rule,
                               cudaStream_t s) {
   cudaError_t err;
-  if (rows <= CROWS) err = launch_cluster_panel_batch<1>(e, count, k0, rule, s);
-  else if (rows <= 2 * CROWS) err = launch_cluster_panel_batch<2>(e, count, k0, rule, s);
-  else if (rows <= 4 * CROWS) err = launch_cluster_panel_batch<4>(e, count, k0, rule, s);
-  else if (rows <= 8 * CROWS) err = launch_cluster_panel_batch<8>(e, count, k0, rule, s);
-  else err = launch_cluster_panel_batch<CMAX>(e, count, k0, rule, s);
+  if (rows <= CROWS) err = launch_cluster_panel_batch<1, S>(e, count, k0, rule, s);
+  else if (rows <= 2 * CROWS) err = launch_cluster_panel_batch<2, S>(e, count, k0, rule, s);
+  else if (rows <= 4 * CROWS) err = launch_cluster_panel_batch<4, S>(e, count, k0, rule, s);
+  else if (rows <= 8 * CROWS) err = launch_cluster_panel_batch<8, S>(e, count, k0, rule, s);
+  else err = launch_cluster_panel_batch<CMAX, S>(e, count, k0, rule, s);
   if (err != cudaSuccess) {
     cudaGetLastError();
     n2c_set_error("batched panel launch: %s", cudaGetErrorString(err));
@@ -1641,9 +1646,13 @@ extern "C" long long n2d_lu_batch_max_order(void) { return cluster_rows(); }
 
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-extern "C" int n2d_lu_factor_batch(double *const *a_dev, const long long *n, const long long *ld, int *const *ipiv,
-                                   int count, int rule, int *info) {
+// Lockstep factorisation of count matrices of storage S (FP64, or FP32 with
+// the tensor-core update); see n2d_lu_factor_batch.
+template <typename S>
+static int factor_batch(void *const *a_dev, const long long *n, const long long *ld, int *const *ipiv, int count,
+                        int rule, int *info) {
   if (count <= 0) return 1;
+  constexpr bool split = sizeof(S) == sizeof(float2);
   const long long cap = cluster_rows();
   if (count > 65535) {
     n2c_set_error("batched factor: %d systems (at most 65535)", count);
@@ -1652,9 +1661,11 @@ extern "C" int n2d_lu_factor_batch(double *const *a_dev, const long long *n, con
   long long nmax = 0;
   for (int i = 0; i < count; ++i) {
     info[i] = 0;
-    if (!a_dev[i] || !ipiv[i] || n[i] <= 0 || n[i] > cap || ld[i] < n[i]) {
+    if (!a_dev[i] || !ipiv[i] || n[i] <= 0 || n[i] > cap || ld[i] < n[i] ||
+        (split && ((ld[i] & 1) || ((uintptr_t)a_dev[i] & 15)))) {
       n2c_set_error("batched factor: system %d has a null matrix or pivots, an order outside 1..%lld, or a "
-                    "leading dimension below its order", i, cap);
+                    "leading dimension below its order%s", i, cap,
+                    split ? " (split form: even leading dimension, 16-byte aligned matrix)" : "");
       return 0;
     }
     if (n[i] > nmax) nmax = n[i];
@@ -1663,38 +1674,58 @@ extern "C" int n2d_lu_factor_batch(double *const *a_dev, const long long *n, con
   LookAhead *la = nmax > KB ? look_ahead() : nullptr;
   if (nmax > KB && !la) return 0;
   const size_t eb = align256(count * sizeof(LuBatchEntry)), sb = align256(count * sizeof(LuStatus));
-  char *dev = (char *)n2d_alloc_async(eb + sb + (size_t)count * 4 * KB * sizeof(int));
+  const size_t pb = align256((size_t)count * 4 * KB * sizeof(int)), tb = split ? align256(count * sizeof(N2cTcBatch)) : 0;
+  size_t btb = 0;   // split form: packed U12 expansions, 2n x 64 floats, hi and lo, per matrix
+  if (split)
+    for (int i = 0; i < count; ++i) btb += 2 * align256((size_t)2 * n[i] * 2 * KB * sizeof(float));
+  char *dev = (char *)n2d_alloc_async(eb + sb + pb + tb + btb);
   if (!dev) return 0;
   LuBatchEntry *de = (LuBatchEntry *)dev;
   LuStatus *dst = (LuStatus *)(dev + eb);
   int *dpairs = (int *)(dev + eb + sb);
+  N2cTcBatch *dtc = split ? (N2cTcBatch *)(dev + eb + sb + pb) : nullptr;
+  char *bt = dev + eb + sb + pb + tb;
   std::vector<LuBatchEntry> h((size_t)count);
-  for (int i = 0; i < count; ++i)
-    h[i] = LuBatchEntry{(double2 *)a_dev[i], n[i], ld[i], ipiv[i], dpairs + (size_t)i * 4 * KB, dst + i};
+  std::vector<N2cTcBatch> htc(split ? (size_t)count : 0);
+  for (int i = 0; i < count; ++i) {
+    h[i] = LuBatchEntry{a_dev[i], n[i], ld[i], ipiv[i], dpairs + (size_t)i * 4 * KB, dst + i, nullptr, nullptr};
+    if (split) {
+      const size_t one = align256((size_t)2 * n[i] * 2 * KB * sizeof(float));
+      h[i].bt_hi = (float *)bt;
+      h[i].bt_lo = (float *)(bt + one);
+      bt += 2 * one;
+      htc[i] = N2cTcBatch{(float2 *)a_dev[i], n[i], ld[i], h[i].bt_hi, h[i].bt_lo};
+    }
+  }
   int ok = cudaMemsetAsync(dst, 0, count * sizeof(LuStatus), s) == cudaSuccess &&
-           cudaMemcpyAsync(de, h.data(), count * sizeof(LuBatchEntry), cudaMemcpyHostToDevice, s) == cudaSuccess;
+           cudaMemcpyAsync(de, h.data(), count * sizeof(LuBatchEntry), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+           (!split ||
+            cudaMemcpyAsync(dtc, htc.data(), count * sizeof(N2cTcBatch), cudaMemcpyHostToDevice, s) == cudaSuccess);
   if (!ok) n2c_set_error("batched factor: descriptor upload failed");
-  ok = ok && launch_panel_batch(de, count, 0, nmax, rule, s);
+  // The update of panel step k0, part 0 (next panel's columns) or 1 (the rest).
+  auto update = [&](long long k0, int part, long long rows, long long cols, cudaStream_t st) -> int {
+    if (rows <= 0 || cols <= 0) return 1;
+    if (split) return n2c_tc_update_batch(dtc, count, k0, part, rows, cols, &dst[0].error, st);
+    gemm_update_batch_kernel<<<dim3((unsigned)((cols + GT - 1) / GT), (unsigned)((rows + GT - 1) / GT), (unsigned)count),
+                               256, 0, st>>>(de, k0, part);
+    return n2c_check_launch("batched update");
+  };
+  ok = ok && launch_panel_batch<S>(de, count, 0, nmax, rule, s);
   const unsigned gb = (unsigned)((nmax + SWT / 32 - 1) / (SWT / 32));
   for (long long k0 = 0; ok && k0 < nmax; k0 += KB) {
-    swap_trsm_batch_kernel<<<dim3(gb, (unsigned)count), SWT, 0, s>>>(de, k0);
+    swap_trsm_batch_kernel<S><<<dim3(gb, (unsigned)count), SWT, 0, s>>>(de, k0);
     if (!n2c_check_launch("batched interchanges and triangular solve")) { ok = 0; break; }
     const long long right = nmax - k0 - (nmax - k0 < KB ? nmax - k0 : KB);
     if (right <= 0) break;
-    const unsigned rt = (unsigned)((right + GT - 1) / GT);
-    const long long rest = right - (right < KB ? right : KB);
-    gemm_update_batch_kernel<<<dim3(1, rt, (unsigned)count), 256, 0, s>>>(de, k0, 0);
-    ok = n2c_check_launch("batched update (next panel)");
+    const long long nb = right < KB ? right : KB, rest = right - nb;
+    ok = update(k0, 0, right, nb, s);
     if (ok && (cudaEventRecord(la->next, s) != cudaSuccess || cudaStreamWaitEvent(la->aux, la->next, 0) != cudaSuccess)) {
       n2c_set_error("look-ahead event");
       ok = 0;
     }
-    ok = ok && launch_panel_batch(de, count, k0 + KB, right, rule, la->aux);
+    ok = ok && launch_panel_batch<S>(de, count, k0 + KB, right, rule, la->aux);
     if (ok && cudaEventRecord(la->panel, la->aux) != cudaSuccess) { n2c_set_error("look-ahead event"); ok = 0; }
-    if (ok && rest > 0) {
-      gemm_update_batch_kernel<<<dim3((unsigned)((rest + GT - 1) / GT), rt, (unsigned)count), 256, 0, s>>>(de, k0, 1);
-      ok = n2c_check_launch("batched update");
-    }
+    ok = ok && update(k0, 1, right, rest, s);
     if (ok && cudaStreamWaitEvent(s, la->panel, 0) != cudaSuccess) { n2c_set_error("look-ahead event"); ok = 0; }
   }
   if (la && !ok) cudaStreamSynchronize(la->aux);
@@ -1710,6 +1741,16 @@ extern "C" int n2d_lu_factor_batch(double *const *a_dev, const long long *n, con
   return ok;
 }
 
+extern "C" int n2d_lu_factor_batch(double *const *a_dev, const long long *n, const long long *ld, int *const *ipiv,
+                                   int count, int rule, int *info) {
+  return factor_batch<double2>((void *const *)a_dev, n, ld, ipiv, count, rule, info);
+}
+
+extern "C" int n2d_lu_factor32_batch(float *const *a_dev, const long long *n, const long long *ld, int *const *ipiv,
+                                     int count, int rule, int *info) {
+  return factor_batch<float2>((void *const *)a_dev, n, ld, ipiv, count, rule, info);
+}
+
 // Cooperative CTAs per system when `systems` solves share the device.
 static int solve_batch_group(int systems) {
   const int sms = n2c_sm_count();
@@ -1719,9 +1760,9 @@ static int solve_batch_group(int systems) {
   return g;
 }
 
-extern "C" int n2d_lu_solve_batch(const double *const *a_dev, const long long *n, const long long *ld,
-                                  const int *const *ipiv, double *const *b_dev, const long long *ldb,
-                                  const long long *nrhs, int count) {
+template <typename S>
+static int solve_batch(const void *const *a_dev, const long long *n, const long long *ld, const int *const *ipiv,
+                       double *const *b_dev, const long long *ldb, const long long *nrhs, int count) {
   if (count <= 0) return 1;
   if (count > 65535) {
     n2c_set_error("batched solve: %d systems (at most 65535)", count);
@@ -1738,8 +1779,7 @@ extern "C" int n2d_lu_solve_batch(const double *const *a_dev, const long long *n
       return 0;
     }
     if (nrhs[i] == 0) continue;
-    SolveBatchEntry m{(const double2 *)a_dev[i], n[i], ld[i], ipiv[i], (double2 *)b_dev[i], ldb[i], (int)nrhs[i],
-                      nullptr, nullptr};
+    SolveBatchEntry m{a_dev[i], n[i], ld[i], ipiv[i], (double2 *)b_dev[i], ldb[i], (int)nrhs[i], nullptr, nullptr};
     if (n[i] >= SOLVE_COOP_MIN && nrhs[i] <= SOLVE_COOP_RHS) {
       coop.push_back(m);
       if (n[i] > coop_n) coop_n = n[i];
@@ -1750,9 +1790,9 @@ extern "C" int n2d_lu_solve_batch(const double *const *a_dev, const long long *n
     }
   }
   static const bool attrs =
-      cudaFuncSetAttribute(lu_solve_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * SOLVE_PERM_MAX) ==
-          cudaSuccess &&
-      cudaFuncSetAttribute(lu_solve_coop_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(lu_solve_batch_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           8 * SOLVE_PERM_MAX) == cudaSuccess &&
+      cudaFuncSetAttribute(lu_solve_coop_batch_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)SOLVE_COOP_SMEM) == cudaSuccess;
   if (!attrs) {
     cudaGetLastError();
@@ -1782,7 +1822,7 @@ extern "C" int n2d_lu_solve_batch(const double *const *a_dev, const long long *n
   if (!ok) n2c_set_error("batched solve: descriptor upload failed");
   if (ok && !one.empty()) {
     const size_t smem = (size_t)8 * (one_n < SOLVE_PERM_MAX ? one_n : SOLVE_PERM_MAX);
-    lu_solve_batch_kernel<<<dim3((unsigned)one_rhs, (unsigned)one.size()), SOLVE_THREADS, smem, s>>>(de);
+    lu_solve_batch_kernel<S><<<dim3((unsigned)one_rhs, (unsigned)one.size()), SOLVE_THREADS, smem, s>>>(de);
     ok = n2c_check_launch("batched solve");
   }
   // Cooperative systems in rounds that fit the device at one CTA per SM.
@@ -1792,13 +1832,13 @@ extern "C" int n2d_lu_solve_batch(const double *const *a_dev, const long long *n
     const unsigned k = (unsigned)(nc - i0 < (size_t)per_round ? nc - i0 : (size_t)per_round);
     const SolveBatchEntry *first = de + one.size() + i0;
     void *args[] = {(void *)&first};
-    const cudaError_t e = cudaLaunchCooperativeKernel((void *)lu_solve_coop_batch_kernel, dim3((unsigned)g, k),
+    const cudaError_t e = cudaLaunchCooperativeKernel((void *)lu_solve_coop_batch_kernel<S>, dim3((unsigned)g, k),
                                                       SOLVE_COOP_THREADS, args, SOLVE_COOP_SMEM, s);
     if (e != cudaSuccess) {
       // Not launchable as one cooperative grid here: one CTA per system.
       cudaGetLastError();
       const size_t smem = (size_t)8 * (coop_n < SOLVE_PERM_MAX ? coop_n : SOLVE_PERM_MAX);
-      lu_solve_batch_kernel<<<dim3(SOLVE_COOP_RHS, k), SOLVE_THREADS, smem, s>>>(first);
+      lu_solve_batch_kernel<S><<<dim3(SOLVE_COOP_RHS, k), SOLVE_THREADS, smem, s>>>(first);
       ok = n2c_check_launch("batched solve");
     } else {
       n2c_count_launch(1);
@@ -1816,6 +1856,18 @@ extern "C" int n2d_lu_solve_batch(const double *const *a_dev, const long long *n
   }
   n2d_free_async(dev);
   return ok;
+}
+
+extern "C" int n2d_lu_solve_batch(const double *const *a_dev, const long long *n, const long long *ld,
+                                  const int *const *ipiv, double *const *b_dev, const long long *ldb,
+                                  const long long *nrhs, int count) {
+  return solve_batch<double2>((const void *const *)a_dev, n, ld, ipiv, b_dev, ldb, nrhs, count);
+}
+
+extern "C" int n2d_lu_solve32_batch(const float *const *a_dev, const long long *n, const long long *ld,
+                                    const int *const *ipiv, double *const *b_dev, const long long *ldb,
+                                    const long long *nrhs, int count) {
+  return solve_batch<float2>((const void *const *)a_dev, n, ld, ipiv, b_dev, ldb, nrhs, count);
 }
 
 // ------------------------------------------------------ allocation-free factor

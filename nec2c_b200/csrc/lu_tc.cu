@@ -86,16 +86,16 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
-__global__ void __launch_bounds__(THREADS, 2)
-gemm_tf32x3_kernel(float2 *C, long long ldc, const float2 *A, long long lda, const float *bt_hi, const float *bt_lo,
-                   long long M, long long N, int *error, long long wait_cycles) {
+// One 128 x 32-complex tile at (r0, c0) of C (the body of the staged form).
+__device__ __forceinline__ void tf32x3_tile(float2 *C, long long ldc, const float2 *A, long long lda,
+                                            const float *bt_hi, const float *bt_lo, long long M, long long N,
+                                            int *error, long long wait_cycles, long long r0, long long c0) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ uint32_t tmem_base;
   __shared__ __align__(8) unsigned long long done_bar;
   unsigned char *sm = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char *a_hi = sm, *a_lo = sm + A_BYTES, *b_hi = sm + 2 * A_BYTES, *b_lo = sm + 2 * A_BYTES + B_BYTES;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const long long r0 = (long long)blockIdx.y * TM, c0 = (long long)blockIdx.x * TNC;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -245,6 +245,33 @@ gemm_tf32x3_kernel(float2 *C, long long ldc, const float2 *A, long long lda, con
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TMEM_COLS) : "memory");
   }
+}
+
+__global__ void __launch_bounds__(THREADS, 2)
+gemm_tf32x3_kernel(float2 *C, long long ldc, const float2 *A, long long lda, const float *bt_hi, const float *bt_lo,
+                   long long M, long long N, int *error, long long wait_cycles) {
+  tf32x3_tile(C, ldc, A, lda, bt_hi, bt_lo, M, N, error, wait_cycles, (long long)blockIdx.y * TM,
+              (long long)blockIdx.x * TNC);
+}
+
+// Lockstep batch (grid.z = matrix): the trailing update of panel step k0 of
+// every matrix of a batch of split-precision factorisations, part 0 the next
+// panel's 32 columns, part 1 the columns after them.  A matrix whose order is
+// passed, or whose update has no tile at this block, leaves before touching
+// tensor memory.
+__global__ void __launch_bounds__(THREADS, 2)
+gemm_tf32x3_batch_kernel(const N2cTcBatch *e, long long k0, int part, int *error, long long wait_cycles) {
+  const N2cTcBatch m = e[blockIdx.z];
+  if (m.n <= k0) return;
+  const long long kb = m.n - k0 < TNC ? m.n - k0 : TNC;
+  const long long right = m.n - k0 - kb, nb = right < TNC ? right : TNC;
+  const long long cf = k0 + kb + (part ? nb : 0), cols = part ? right - nb : nb;
+  const long long r0 = (long long)blockIdx.y * TM, c0 = (long long)blockIdx.x * TNC;
+  if (right <= 0 || cols <= 0 || r0 >= right || c0 >= cols) return;
+  float2 *below = m.a + (k0 + kb) * m.ld;
+  const long long r2 = 2 * (cf - k0 - kb);
+  tf32x3_tile(below + cf, m.ld, below + k0, m.ld, m.bt_hi + r2 * KR, m.bt_lo + r2 * KR, right, cols, error,
+              wait_cycles, r0, c0);
 }
 
 
@@ -619,6 +646,22 @@ static int launch_persistent(float *C, long long ldc, const float *A, long long 
   gemm_tf32x3_tma_kernel<<<(unsigned)(bands * cpb), P_THREADS, P_SMEM_BYTES, s>>>(
       ta, tbh, tbl, (float2 *)C, ldc, M, N, (int)cpb, error, wait_cycles);
   return n2c_check_launch("tensor-core update");
+}
+
+int n2c_tc_update_batch(const N2cTcBatch *e, int count, long long k0, int part, long long rows_max,
+                        long long cols_max, int *error, cudaStream_t s) {
+  if (rows_max <= 0 || cols_max <= 0 || count <= 0) return 1;
+  static const bool configured =
+      cudaFuncSetAttribute(gemm_tf32x3_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) ==
+      cudaSuccess;
+  if (!configured) {
+    n2c_set_error("batched tensor-core update: shared memory configuration failed");
+    return 0;
+  }
+  static const long long wait_cycles = tc_wait_cycles();
+  dim3 grid((unsigned)((cols_max + TNC - 1) / TNC), (unsigned)((rows_max + TM - 1) / TM), (unsigned)count);
+  gemm_tf32x3_batch_kernel<<<grid, THREADS, SMEM_BYTES, s>>>(e, k0, part, error, wait_cycles);
+  return n2c_check_launch("batched tensor-core update");
 }
 
 int n2c_tc_update(float *C, long long ldc, const float *A, long long lda, const float *bt_hi, const float *bt_lo,

@@ -48,6 +48,19 @@ int n2c_tc_update(float *C, long long ldc, const float *A, long long lda, const 
                   long long M, long long N, int *error, cudaStream_t s, int form);
 // The form the LU's trailing update of an M x N block takes.
 int n2c_tc_form(long long M, long long N);
+// One matrix of a lockstep batch of split-precision factorisations, as the
+// batched tensor-core update reads it: the FP32 working matrix (leading dim
+// ld complex, even; rows 16-byte aligned) and its packed U12 expansion.
+struct N2cTcBatch {
+  float2 *a;
+  long long n, ld;
+  const float *bt_hi, *bt_lo;
+};
+// The trailing updates of panel step k0 (panel width 32) of count matrices
+// (entries e on the device): part 0 the next panel's columns, part 1 the
+// rest; rows_max / cols_max bound every matrix's update block.
+int n2c_tc_update_batch(const N2cTcBatch *e, int count, long long k0, int part, long long rows_max,
+                        long long cols_max, int *error, cudaStream_t s);
 
 // Deterministic block-partial reduction: each block stores its partial in
 // partials[blockIdx.x]; the block that arrives last (ticket counter) sums the

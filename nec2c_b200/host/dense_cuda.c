@@ -478,11 +478,108 @@ static int lockstep_batch(size_t count, const size_t *order, const nec2c_cuda_co
   return ok;
 }
 
-/* The request server's merged dense run (FP64 form): the private copies of
-   count requests' matrices factored and solved as one lockstep batch. */
+/* The split-precision lockstep batch (the server's merged dense run on a
+   split-precision server): each system's FP64 matrix uploaded and kept for the
+   refinement residuals, narrowed to FP32 (even leading dimension), the FP32
+   copies factored together by n2d_lu_factor32_batch (tensor-core updates),
+   then solve_refined's iteration for every system at once: one batched FP32
+   solve per step, each system's correction and FP64 residual, one read of all
+   the norms, and the systems that meet solve_refined's test leave the loop.
+   A system not converged in 30 steps is solved by an FP64 factorisation of
+   its original, as solve_refined does.  steps[i] receives its step count
+   (-1: the FP64 fallback). */
+static int lockstep_batch_split(size_t count, const size_t *order, const nec2c_cuda_complex *const *matrix,
+                                const size_t *ld, nec2c_cuda_complex *const *rhs, const size_t *stride,
+                                const size_t *rhs_count, int *status, int *steps)
+{
+  double **a = calloc(count, sizeof(*a)), **b = calloc(count, sizeof(*b)), **x = calloc(count, sizeof(*x));
+  double **r = calloc(count, sizeof(*r)), **d = calloc(count, sizeof(*d)), *anorm = calloc(count, sizeof(double));
+  float **lu = calloc(count, sizeof(*lu));
+  int **piv = calloc(count, sizeof(*piv)), *info = calloc(count, sizeof(int)), *live = calloc(count, sizeof(int));
+  long long *n = calloc(count, sizeof(long long)), *ld32 = calloc(count, sizeof(long long));
+  long long *nr = calloc(count, sizeof(long long));
+  size_t *noff = calloc(count, sizeof(size_t)), ntot = 0, i;
+  double *norms = NULL;
+  unsigned long long *norm_dev = NULL;
+  int ok = a && b && x && r && d && anorm && lu && piv && info && live && n && ld32 && nr && noff, it, left;
+  if(!ok) n2c_set_error("batched solve: out of host memory");
+  for(i = 0; ok && i < count; ++i) {
+    const size_t k = order[i], c = rhs_count[i];
+    status[i] = 0; steps[i] = 0;
+    n[i] = (long long)k; ld32[i] = (long long)(k + (k & 1));
+    noff[i] = ntot; ntot += 2 * c;
+    a[i] = n2d_alloc_async(k * k * CPX);
+    lu[i] = n2d_alloc_async(k * (size_t)ld32[i] * 2 * sizeof(float));
+    piv[i] = n2d_alloc_async(k * sizeof(int));
+    b[i] = n2d_alloc_async(k * c * CPX); x[i] = n2d_alloc_async(k * c * CPX);
+    r[i] = n2d_alloc_async(k * c * CPX); d[i] = n2d_alloc_async(k * c * CPX);
+    ok = a[i] && lu[i] && piv[i] && b[i] && x[i] && r[i] && d[i] &&
+         n2d_upload2d(a[i], k * CPX, matrix[i], ld[i] * CPX, k * CPX, k) &&
+         n2d_upload2d(b[i], k * CPX, rhs[i], stride[i] * CPX, k * CPX, c) &&
+         n2d_narrow(a[i], n[i], lu[i], ld32[i], n[i], n[i]);
+  }
+  norm_dev = ok ? n2d_alloc_async((ntot > count ? ntot : count) * sizeof(unsigned long long)) : NULL;
+  norms = ok ? malloc(ntot * sizeof(double)) : NULL;
+  ok = ok && norm_dev && norms;
+  for(i = 0; ok && i < count; ++i) ok = n2d_norm_inf(a[i], n[i], n[i], norm_dev, &anorm[i]);
+  ok = ok && n2d_lu_factor32_batch(lu, n, ld32, piv, (int)count, 0, info);
+  for(i = 0, left = 0; ok && i < count; ++i) {
+    live[i] = !info[i];   /* singular systems take no part */
+    left += live[i];
+    ok = n2d_memset(x[i], 0, order[i] * rhs_count[i] * CPX) && n2d_copy_d2d(r[i], b[i], order[i] * rhs_count[i] * CPX);
+  }
+  for(it = 1; ok && it <= 30 && left; ++it) {
+    for(i = 0; ok && i < count; ++i) {
+      nr[i] = live[i] ? (long long)rhs_count[i] : 0;
+      if(live[i]) ok = n2d_copy_d2d(d[i], r[i], order[i] * rhs_count[i] * CPX);
+    }
+    ok = ok && n2d_lu_solve32_batch((const float *const *)lu, n, ld32, (const int *const *)piv, d, n, nr, (int)count);
+    for(i = 0; ok && i < count; ++i) {
+      const long long K = (long long)rhs_count[i];
+      if(!live[i]) continue;
+      ok = n2d_add_correction(x[i], d[i], n[i], K, n[i], norm_dev + noff[i] + rhs_count[i], NULL) &&
+           n2d_residual(a[i], n[i], n[i], x[i], b[i], r[i], K, n[i], norm_dev + noff[i], NULL);
+    }
+    ok = ok && n2d_read_norms(norm_dev, (long long)ntot, norms);
+    for(i = 0; ok && i < count; ++i) {
+      const double cte = anorm[i] * DBL_EPSILON * sqrt((double)order[i]);
+      size_t j;
+      int done = live[i];
+      if(!live[i]) continue;
+      for(j = 0; j < rhs_count[i]; ++j)
+        if(!(norms[noff[i] + j] <= norms[noff[i] + rhs_count[i] + j] * cte)) done = 0;
+      if(done) { live[i] = 0; left--; steps[i] = it; status[i] = 1; }
+    }
+  }
+  /* Not converged in 30 steps: an FP64 factorisation of the original. */
+  for(i = 0; ok && i < count; ++i) {
+    const size_t k = order[i], c = rhs_count[i];
+    int inf = 0;
+    if(!live[i]) continue;
+    ok = n2d_lu_factor(a[i], n[i], n[i], piv[i], 0, 0, &inf) && n2d_copy_d2d(x[i], b[i], k * c * CPX) &&
+         (inf || n2d_lu_solve(a[i], n[i], n[i], piv[i], x[i], n[i], (long long)c));
+    status[i] = ok && !inf;
+    steps[i] = -1;
+  }
+  for(i = 0; ok && i < count; ++i)
+    if(status[i]) ok = n2d_download2d(rhs[i], stride[i] * CPX, x[i], order[i] * CPX, order[i] * CPX, rhs_count[i]);
+  if(ok) n2d_sync();
+  for(i = 0; a && b && x && r && d && lu && piv && i < count; ++i) {
+    n2d_free_async(a[i]); n2d_free_async(lu[i]); n2d_free_async(piv[i]);
+    n2d_free_async(b[i]); n2d_free_async(x[i]); n2d_free_async(r[i]); n2d_free_async(d[i]);
+  }
+  n2d_free_async(norm_dev);
+  free(a); free(b); free(x); free(r); free(d); free(anorm); free(lu); free(piv); free(info); free(live);
+  free(n); free(ld32); free(nr); free(noff); free(norms);
+  return ok;
+}
+
+/* The request server's merged dense run: the private copies of count
+   requests' matrices factored and solved as one lockstep batch, in the FP64
+   form or (split) the split-precision form with FP64 refinement. */
 int n2c_dense_solve_private_batch(size_t count, const size_t *order, const nec2c_cuda_complex *const *matrix,
                                   const size_t *ld, nec2c_cuda_complex *const *rhs, const size_t *stride,
-                                  const size_t *rhs_count, int *status)
+                                  const size_t *rhs_count, int split, int *status, int *steps)
 {
   size_t i;
   for(i = 0; i < count; ++i) {
@@ -493,6 +590,8 @@ int n2c_dense_solve_private_batch(size_t count, const size_t *order, const nec2c
       return 0;
     }
   }
+  if(split) return lockstep_batch_split(count, order, matrix, ld, rhs, stride, rhs_count, status, steps);
+  for(i = 0; i < count; ++i) steps[i] = 0;
   return lockstep_batch(count, order, matrix, ld, NULL, NULL, rhs, stride, rhs_count, status);
 }
 

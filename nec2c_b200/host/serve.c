@@ -43,7 +43,7 @@ int n2c_dense_solve_private(size_t n, const nec2c_cuda_complex *matrix, size_t l
                             size_t stride, size_t count, int split, int *steps);
 int n2c_dense_solve_private_batch(size_t count, const size_t *order, const nec2c_cuda_complex *const *matrix,
                                   const size_t *ld, nec2c_cuda_complex *const *rhs, const size_t *stride,
-                                  const size_t *rhs_count, int *status);
+                                  const size_t *rhs_count, int split, int *status, int *steps);
 const nec2c_cuda_vie_plan *n2c_hybrid_volume_plan(const nec2c_cuda_hybrid *h);
 const nec2c_cuda_vie_plan *n2c_batch_plan(const nec2c_cuda_vie_batch *b, size_t q);
 size_t n2c_batch_index(const nec2c_cuda_vie_batch *b, const nec2c_cuda_vie_plan *plan,
@@ -313,7 +313,7 @@ static size_t dense_class(size_t n)
 
 static int dense_mergeable(const nec2c_cuda_server *s, const nec2c_cuda_request *r)
 {
-  return r->kind == NEC2C_CUDA_REQUEST_DENSE && s->dense_merge >= 2 && !s->split && r->order > 0 &&
+  return r->kind == NEC2C_CUDA_REQUEST_DENSE && s->dense_merge >= 2 && r->order > 0 &&
          (long long)r->order <= n2d_lu_batch_max_order() && r->rhs_count > 0 && r->rhs_count <= 65535 &&
          r->ld >= r->order && r->rhs_stride >= r->order;
 }
@@ -351,34 +351,37 @@ static size_t gather_dense(const nec2c_cuda_server *s, nec2c_cuda_request *r, si
 }
 
 /* Merged dense requests: one lockstep factorisation and solve of their
-   private matrix copies. */
-static void run_dense_merged(run_t *u)
+   private matrix copies (the split-precision form with FP64 refinement on a
+   split server). */
+static void run_dense_merged(const nec2c_cuda_server *s, run_t *u)
 {
   const size_t k = u->n;
   size_t *order = calloc(k, sizeof(size_t)), *ld = calloc(k, sizeof(size_t)), *stride = calloc(k, sizeof(size_t));
   size_t *count = calloc(k, sizeof(size_t)), j;
   const nec2c_cuda_complex **mat = calloc(k, sizeof(*mat));
   nec2c_cuda_complex **rhs = calloc(k, sizeof(*rhs));
-  int *st = calloc(k, sizeof(int)), ok = order && ld && stride && count && mat && rhs && st;
+  int *st = calloc(k, sizeof(int)), *steps = calloc(k, sizeof(int));
+  int ok = order && ld && stride && count && mat && rhs && st && steps;
   if(!ok) n2c_set_error("merged dense run: out of host memory");
   for(j = 0; ok && j < k; ++j) {
     const nec2c_cuda_request *r = u->member[j];
     order[j] = r->order; ld[j] = r->ld; stride[j] = r->rhs_stride; count[j] = r->rhs_count;
     mat[j] = r->matrix; rhs[j] = r->rhs;
   }
-  if(ok) ok = n2c_dense_solve_private_batch(k, order, mat, ld, rhs, stride, count, st);
+  if(ok) ok = n2c_dense_solve_private_batch(k, order, mat, ld, rhs, stride, count, s->split, st, steps);
   for(j = 0; j < k; ++j) {
     nec2c_cuda_request *r = u->member[j];
     memset(&r->report, 0, sizeof(r->report));
     r->status = ok && st && st[j];
     r->report.status = r->status;
+    r->report.iterations = ok && steps && steps[j] > 0 ? (size_t)steps[j] : 0;
     r->merged = k;
     if(!r->status) {
       strncpy(r->error, ok ? "matrix is singular" : nec2c_cuda_last_error(), sizeof(r->error) - 1);
       r->error[sizeof(r->error) - 1] = 0;
     }
   }
-  free(order); free(ld); free(stride); free(count); free(mat); free(rhs); free(st);
+  free(order); free(ld); free(stride); free(count); free(mat); free(rhs); free(st); free(steps);
 }
 
 static void *worker(void *arg)
@@ -472,7 +475,7 @@ static void *worker(void *arg)
     }
     pthread_mutex_unlock(&s->lock);
     if(u->batch) run_merged(u);
-    else if(u->dense) run_dense_merged(u);
+    else if(u->dense) run_dense_merged(s, u);
     else run_request(s, r);
     pthread_mutex_lock(&s->lock);
     s->in_use -= fp;
@@ -628,10 +631,6 @@ int nec2c_cuda_server_merge_batch(nec2c_cuda_server *s, nec2c_cuda_vie_batch *b)
 int nec2c_cuda_server_merge_dense(nec2c_cuda_server *s, size_t max_systems)
 {
   if(!s) { n2c_set_error("dense merging: null server"); return 0; }
-  if(s->split && max_systems >= 2) {
-    n2c_set_error("dense merging: the lockstep batch is the FP64 form; this server runs the split-precision form");
-    return 0;
-  }
   if(max_systems > 65535) { n2c_set_error("dense merging: at most 65535 systems per batch"); return 0; }
   pthread_mutex_lock(&s->lock);
   s->dense_merge = max_systems;

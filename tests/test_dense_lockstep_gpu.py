@@ -96,3 +96,75 @@ def test_server_merges_dense_requests():
         assert max(m for _, m in res2) >= 2
         for k, (x, y) in enumerate(zip(merged, alone)):
             assert np.linalg.norm(x - y) / np.linalg.norm(y) < 1e-12, (k, orders[k])
+
+
+def test_split_lockstep_matches_single():
+    """Split-precision lockstep batch (FP32 storage, tensor-core 3xTF32
+    updates) against n2d_lu_factor32 on each matrix alone: pivots and FP32
+    factors bit for bit (the same kernel bodies), ragged orders in one batch."""
+    import ctypes as C
+    import torch
+    lib = nb.load()
+    cap = lib.nec2c_cuda_dense_batch_max_order()
+    single = lib.n2d_lu_factor32
+    single.restype = C.c_int
+    single.argtypes = [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    batch = lib.n2d_lu_factor32_batch
+    batch.restype = C.c_int
+    batch.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    sizes = [n for n in (70, 257, 300, 1100, 2100, 33) if n <= cap]
+    mats, pivs, works, lds = [], [], [], []
+    for k, n in enumerate(sizes):
+        ld = n + (n & 1) + 2 * (k % 2)
+        a = np.zeros((n, ld), dtype=np.complex64)
+        a[:, :n] = mom_like(n, 1600 + k)
+        mats.append(a)
+        lds.append(ld)
+        works.append(torch.from_numpy(a.view(np.float32)).cuda())
+        pivs.append(torch.zeros(n, dtype=torch.int32, device="cuda"))
+    count = len(sizes)
+    info = (C.c_int * count)()
+    ok = batch((C.c_void_p * count)(*[w.data_ptr() for w in works]), (C.c_longlong * count)(*sizes),
+               (C.c_longlong * count)(*lds), (C.c_void_p * count)(*[p.data_ptr() for p in pivs]), count, 0, info)
+    torch.cuda.synchronize()
+    assert ok, nb.last_error()
+    for k, n in enumerate(sizes):
+        assert info[k] == 0
+        w1 = torch.from_numpy(mats[k].view(np.float32)).cuda()
+        p1 = torch.zeros(n, dtype=torch.int32, device="cuda")
+        i1 = C.c_int(0)
+        assert single(w1.data_ptr(), n, lds[k], p1.data_ptr(), 0, C.byref(i1)), nb.last_error()
+        torch.cuda.synchronize()
+        assert i1.value == 0
+        assert torch.equal(pivs[k], p1), (k, n)
+        assert torch.equal(works[k], w1), (k, n)
+
+
+def test_split_server_merges_with_refinement():
+    """A split-precision server merging dense requests: every solution within
+    1e-10 of the exact one (FP64 refinement of the tensor-core factors), the
+    merged requests reporting their refinement steps."""
+    orders = [300, 320, 400, 480, 350, 700, 900, 1000, 600, 1800, 1300, 200]
+    mats, rhss, xs = [], [], []
+    for k, n in enumerate(orders):
+        a = mom_like(n, 1700 + k)
+        mats.append(np.asfortranarray(a.T))
+        rng = np.random.default_rng(90 + k)
+        x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        xs.append(x)
+        rhss.append(np.asfortranarray((a @ x).reshape(n, 1)))
+    srv = nb.Server(slots=2, split=True)
+    srv.merge_dense(6)
+    outs, reqs = [], []
+    for m, b in zip(mats, rhss):
+        o = b.copy(order="F")
+        reqs.append(srv.dense(m, o))
+        outs.append(o)
+    srv.drain()
+    assert all(r.status for r in reqs), [r.error for r in reqs]
+    assert max(r.merged for r in reqs) >= 2
+    for k, (o, x, r) in enumerate(zip(outs, xs, reqs)):
+        assert np.linalg.norm(o[:, 0] - x) / np.linalg.norm(x) < 1e-10, (k, orders[k])
+        if r.merged > 1:
+            assert r.report.iterations >= 1, k
+    srv.close()

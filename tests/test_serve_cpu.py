@@ -262,8 +262,8 @@ def test_queued_dense_requests_merge(fake):
     """Dense requests that queue behind busy workers run as lockstep batches
     of one size class (orders up to 256, 512, 1024, 2048, 4096), at most the
     registered count per batch and within the device budget; each request
-    gets its own result; orders above the batch limit and a split-precision
-    server do not merge."""
+    gets its own result; orders above the batch limit do not merge, and a
+    split-precision server's merged requests report their refinement steps."""
     fake.fake_reset(20000, 10 * GIB)
     srv = Server(fake, slots=2)
     assert fake.nec2c_cuda_server_merge_dense(srv.h, 4)
@@ -294,9 +294,17 @@ def test_queued_dense_requests_merge(fake):
     assert all(r.status and r.merged <= 2 for r in rest)
     srv.close()
 
-    split = C.c_void_p()
-    assert fake.nec2c_cuda_server_create(C.byref(split), 0, 1, 0, 1)
-    assert not fake.nec2c_cuda_server_merge_dense(split, 4)
-    assert b"split-precision" in fake.nec2c_cuda_last_error()
-    assert fake.nec2c_cuda_server_merge_dense(split, 1)       # off is always accepted
-    fake.nec2c_cuda_server_destroy(split)
+    # A split-precision server merges too; its requests report the
+    # refinement steps of their lockstep run.
+    fake.fake_reset(20000, 10 * GIB)
+    split = Server(fake, slots=1)
+    fake.nec2c_cuda_server_destroy(split.h)
+    assert fake.nec2c_cuda_server_create(C.byref(split.h), 0, 1, 0, 1)
+    assert fake.nec2c_cuda_server_merge_dense(split.h, 4)
+    first = split.dense(64)[0]
+    rest = [split.dense(300) for _ in range(3)]
+    split.drain()
+    assert all(r.status for r, _ in rest) and max(r.merged for r, _ in rest) >= 2
+    assert all(r.report.iterations == 3 for r, _ in rest if r.merged > 1)
+    assert first.status
+    split.close()
