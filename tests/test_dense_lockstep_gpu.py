@@ -168,3 +168,51 @@ def test_split_server_merges_with_refinement():
         if r.merged > 1:
             assert r.report.iterations >= 1, k
     srv.close()
+
+
+@pytest.mark.parametrize("split", [False, True])
+def test_lockstep_small_orders(split):
+    """Orders at and around one panel (1, 2, 5, 31, 32, 33, 64, 65) in one
+    lockstep batch, as the server's smallest size class can hold them: each
+    bit for bit its own factorisation (FP64 or split precision)."""
+    import ctypes as C
+    import torch
+    lib = nb.load()
+    if split:
+        one, many, dt = lib.n2d_lu_factor32, lib.n2d_lu_factor32_batch, np.complex64
+    else:
+        one, many, dt = lib.n2d_lu_factor, lib.n2d_lu_factor_batch, np.complex128
+    many.restype = C.c_int
+    many.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    one.restype = C.c_int
+    if split:
+        one.argtypes = [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    else:
+        one.argtypes = [C.c_void_p, C.c_longlong, C.c_longlong, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]
+    sizes = [1, 2, 5, 31, 32, 33, 64, 65]
+    host, dev, piv, lds = [], [], [], []
+    for k, n in enumerate(sizes):
+        ld = n + (n & 1)
+        a = np.zeros((n, ld), dtype=dt)
+        a[:, :n] = mom_like(n, 1800 + k)
+        host.append(a)
+        lds.append(ld)
+        dev.append(torch.from_numpy(a.view(np.float32 if split else np.float64)).cuda())
+        piv.append(torch.zeros(n, dtype=torch.int32, device="cuda"))
+    count = len(sizes)
+    info = (C.c_int * count)()
+    assert many((C.c_void_p * count)(*[d.data_ptr() for d in dev]), (C.c_longlong * count)(*sizes),
+                (C.c_longlong * count)(*lds), (C.c_void_p * count)(*[p.data_ptr() for p in piv]), count, 0, info), \
+        nb.last_error()
+    torch.cuda.synchronize()
+    for k, n in enumerate(sizes):
+        assert info[k] == 0
+        d1 = torch.from_numpy(host[k].view(np.float32 if split else np.float64)).cuda()
+        p1 = torch.zeros(n, dtype=torch.int32, device="cuda")
+        i1 = C.c_int(0)
+        ok = (one(d1.data_ptr(), n, lds[k], p1.data_ptr(), 0, C.byref(i1)) if split else
+              one(d1.data_ptr(), n, lds[k], p1.data_ptr(), 0, 0, C.byref(i1)))
+        torch.cuda.synchronize()
+        assert ok and i1.value == 0, nb.last_error()
+        assert torch.equal(piv[k], p1), (k, n)
+        assert torch.equal(dev[k], d1), (k, n)
