@@ -647,35 +647,60 @@ __global__ void __launch_bounds__(SWT) swap_trsm_kernel(S *a, long long n, long 
 }
 
 // C[M x N] -= A[M x K] B[K x N], row-major complex FP64 blocks (leading dim ld).
+// The K chunks are copied into two shared-memory stages by cp.async, the next
+// chunk's copy in flight while the current one is multiplied (a panel's
+// K = 32 is two chunks, so both loads go out at once); each C element's
+// products are summed in increasing k as before.
 constexpr int GT = 64;   // tile edge
 constexpr int GK = 16;   // K chunk
+constexpr size_t GEMM_STAGE = (size_t)GK * (GT + 1) * sizeof(double2);
+constexpr size_t GEMM_SMEM = 4 * GEMM_STAGE;   // A and B, two stages each (66,560 bytes)
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
 __device__ __forceinline__ void gemm_update_body(double2 *C, const double2 *A, const double2 *B, long long M,
                                                  long long N, int K, long long ld, long long row0, long long col0) {
-  __shared__ double2 As[GK][GT + 1];
-  __shared__ double2 Bs[GK][GT + 1];
+  extern __shared__ __align__(16) unsigned char gemm_smem[];
+  typedef double2 Stage[GK][GT + 1];
+  Stage *As = reinterpret_cast<Stage *>(gemm_smem), *Bs = reinterpret_cast<Stage *>(gemm_smem + 2 * GEMM_STAGE);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // 16 x 16 threads, 4 x 4 each
   double2 acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0, 0);
-  for (int k0 = 0; k0 < K; k0 += GK) {
+  auto stage = [&](int st, int k0) {
     for (int t = threadIdx.x; t < GT * GK; t += 256) {
       const int k = t % GK, r = t / GK;
       const long long gr = row0 + r;
-      As[k][r] = (gr < M && k0 + k < K) ? A[gr * ld + k0 + k] : make_double2(0, 0);
+      if (gr < M && k0 + k < K) cp_async16(&As[st][k][r], A + gr * ld + k0 + k);
+      else As[st][k][r] = make_double2(0, 0);
       const int cc = t % GT, kk = t / GT;
       const long long gc = col0 + cc;
-      Bs[kk][cc] = (gc < N && k0 + kk < K) ? B[(long long)(k0 + kk) * ld + gc] : make_double2(0, 0);
+      if (gc < N && k0 + kk < K) cp_async16(&Bs[st][kk][cc], B + (long long)(k0 + kk) * ld + gc);
+      else Bs[st][kk][cc] = make_double2(0, 0);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  const int chunks = (K + GK - 1) / GK;
+  if (chunks > 0) stage(0, 0);
+  for (int ch = 0; ch < chunks; ++ch) {
+    const int st = ch & 1;
+    if (ch + 1 < chunks) {
+      stage(st ^ 1, (ch + 1) * GK);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < GK; ++k) {
       double2 av[4], bv[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = As[k][ty + 16 * i];
+      for (int i = 0; i < 4; ++i) av[i] = As[st][k][ty + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bv[j] = Bs[k][tx + 16 * j];
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[st][k][tx + 16 * j];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -699,7 +724,7 @@ __device__ __forceinline__ void gemm_update_body(double2 *C, const double2 *A, c
       }
     }
 }
-__global__ void __launch_bounds__(256) gemm_update_kernel(double2 *C, const double2 *A, const double2 *B,
+__global__ void __launch_bounds__(256, 2) gemm_update_kernel(double2 *C, const double2 *A, const double2 *B,
                                                           long long M, long long N, int K, long long ld) {
   gemm_update_body(C, A, B, M, N, K, ld, blockIdx.y * (long long)GT, blockIdx.x * (long long)GT);
 }
@@ -1304,7 +1329,14 @@ static int launch_gemm(double2 *a, long long ld, long long k0, int kb, long long
                        long long rows, const FactorScratch &, cudaStream_t s) {
   if (cols <= 0 || rows <= 0) return 1;
   dim3 grid((unsigned)((cols + GT - 1) / GT), (unsigned)((rows + GT - 1) / GT));
-  gemm_update_kernel<<<grid, 256, 0, s>>>(a + (k0 + kb) * ld + c_first, a + (k0 + kb) * ld + k0,
+  static const bool configured = cudaFuncSetAttribute(gemm_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)GEMM_SMEM) == cudaSuccess;
+  if (!configured) {
+    cudaGetLastError();
+    n2c_set_error("gemm_update: shared memory configuration failed");
+    return 0;
+  }
+  gemm_update_kernel<<<grid, 256, GEMM_SMEM, s>>>(a + (k0 + kb) * ld + c_first, a + (k0 + kb) * ld + k0,
                                           a + k0 * ld + c_first, rows, cols, kb, ld);
   return n2c_check_launch("gemm_update");
 }
@@ -1554,7 +1586,7 @@ __global__ void __launch_bounds__(SWT) swap_trsm_batch_kernel(const LuBatchEntry
 }
 
 // part 0: the next panel's columns (look-ahead); part 1: the columns after it.
-__global__ void __launch_bounds__(256) gemm_update_batch_kernel(const LuBatchEntry *e, long long k0, int part) {
+__global__ void __launch_bounds__(256, 2) gemm_update_batch_kernel(const LuBatchEntry *e, long long k0, int part) {
   const LuBatchEntry m = e[blockIdx.z];
   if (m.n <= k0) return;
   const int kb = batch_kb(m.n, k0);
@@ -1706,8 +1738,16 @@ static int factor_batch(void *const *a_dev, const long long *n, const long long 
   auto update = [&](long long k0, int part, long long rows, long long cols, cudaStream_t st) -> int {
     if (rows <= 0 || cols <= 0) return 1;
     if (split) return n2c_tc_update_batch(dtc, count, k0, part, rows, cols, &dst[0].error, st);
+    static const bool configured = cudaFuncSetAttribute(gemm_update_batch_kernel,
+                                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                        (int)GEMM_SMEM) == cudaSuccess;
+    if (!configured) {
+      cudaGetLastError();
+      n2c_set_error("batched update: shared memory configuration failed");
+      return 0;
+    }
     gemm_update_batch_kernel<<<dim3((unsigned)((cols + GT - 1) / GT), (unsigned)((rows + GT - 1) / GT), (unsigned)count),
-                               256, 0, st>>>(de, k0, part);
+                               256, GEMM_SMEM, st>>>(de, k0, part);
     return n2c_check_launch("batched update");
   };
   ok = ok && launch_panel_batch<S>(de, count, 0, nmax, rule, s);
