@@ -574,6 +574,9 @@ def run_ours(args, rank, world, local_rank):
 
     # Dense LU of 1984 unknowns, both forms.
     dense = dense_bench(nb, torch, stream)
+    # Lockstep batches of 16 dense factorisations (FP64 and split precision)
+    # against one factorisation at a time, resident matrices.
+    lockstep = lockstep_factor_bench(nb, torch, stream, orders=(1000, 2608), counts=(16,), reps=2)
     # 192 small wire blocks, ragged batch in one launch.
     batched = batched_bench(nb, torch)
     # 192-system dipole-plus-cube sweep, ragged batch of plans.
@@ -613,6 +616,7 @@ def run_ours(args, rank, world, local_rank):
         "matvec_fp64": {"ms": mv64_ms, "achieved_gbs": bytes64 / (mv64_ms * 1e-3) / 1e9},
         "fft_schedule": schedule,
         "dense_lu_c1": dense,
+        "lockstep_lu": lockstep,
         "batched_wire_blocks_c3": batched,
         "batched_volume_c3": volume_batch,
         "serving_c4": serving,
