@@ -129,7 +129,7 @@ extern "C" int n2d_norm_inf(const double *a, long long n, long long ld, void *no
   unsigned long long *m = (unsigned long long *)norm_dev;
   if (!n2d_memset(m, 0, sizeof(unsigned long long))) return 0;
   norm_inf_kernel<<<grid_for(n * 32, 256), 256, 0, n2c_stream()>>>((const double2 *)a, n, ld, m);
-  return n2c_check_launch("norm") && read_maxima(m, 1, norm_host);
+  return n2c_check_launch("norm") && (!norm_host || read_maxima(m, 1, norm_host));
 }
 
 extern "C" int n2d_residual(const double *a, long long n, long long ld, const double *x, const double *b, double *r,

@@ -194,6 +194,7 @@ int n2d_widen(const float *src_dev, long long lds, double *dst_dev, long long ld
 /* Infinity norm of the row-major complex matrix (max row sum of |Re|+|Im|).
    norm_dev: caller-owned device scratch of 8 bytes per column. */
 int n2d_norm_inf(const double *a_dev, long long order, long long ld, void *norm_dev, double *norm_host);
+/* (With norm_host NULL the norm stays in norm_dev for n2d_read_norms.) */
 /* Refinement step pieces for nrhs columns (leading dim ldb): r = b - A x with
    A row-major (ld), and x += d; each reports per-column infinity norms
    (|Re|+|Im|) of r and of the updated x into rnorm_host / xnorm_host. */

@@ -521,7 +521,11 @@ static int lockstep_batch_split(size_t count, const size_t *order, const nec2c_c
   norm_dev = ok ? n2d_alloc_async((ntot > count ? ntot : count) * sizeof(unsigned long long)) : NULL;
   norms = ok ? malloc(ntot * sizeof(double)) : NULL;
   ok = ok && norm_dev && norms;
-  for(i = 0; ok && i < count; ++i) ok = n2d_norm_inf(a[i], n[i], n[i], norm_dev, &anorm[i]);
+  /* Every system's ||A||_inf into its own slot, one read for all. */
+  for(i = 0; ok && i < count; ++i)
+    ok = n2d_norm_inf(a[i], n[i], n[i], (unsigned long long *)norm_dev + noff[i], NULL);
+  ok = ok && n2d_read_norms(norm_dev, (long long)ntot, norms);
+  for(i = 0; ok && i < count; ++i) anorm[i] = norms[noff[i]];
   ok = ok && n2d_lu_factor32_batch(lu, n, ld32, piv, (int)count, 0, info);
   for(i = 0, left = 0; ok && i < count; ++i) {
     live[i] = !info[i];   /* singular systems take no part */
