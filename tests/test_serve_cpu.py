@@ -265,7 +265,11 @@ def test_queued_dense_requests_merge(fake):
     gets its own result; orders above the batch limit do not merge, and a
     split-precision server's merged requests report their refinement steps."""
     fake.fake_reset(20000, 10 * GIB)
+    assert not fake.nec2c_cuda_server_merge_dense(None, 4)
+    assert b"null server" in fake.nec2c_cuda_last_error()
     srv = Server(fake, slots=2)
+    assert not fake.nec2c_cuda_server_merge_dense(srv.h, 70000)
+    assert b"at most 65535" in fake.nec2c_cuda_last_error()
     assert fake.nec2c_cuda_server_merge_dense(srv.h, 4)
     blockers = [srv.dense(64)[0] for _ in range(2)]           # both workers busy
     orders = [300, 400, 500, 310, 320, 1000, 700, 900, 5000, 2000, 1500, 330]
