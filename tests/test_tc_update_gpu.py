@@ -68,6 +68,36 @@ def test_tf32x3_update(m, n, ld, form):
     assert np.array_equal(out[:, 32 + n:], w[:, 32 + n:])
 
 
+@pytest.mark.parametrize("m,n,ld", [(1100, 1300, 1340), (2047, 1024, 1090)])
+def test_tf32x3_forms_agree_bitwise(m, n, ld):
+    """The staged and the persistent form issue the same products in the same
+    order per accumulator element, so C comes out the same bit for bit (the
+    lockstep batch may take either form for a step's updates)."""
+    import torch
+    rng = np.random.default_rng(7 * m + n)
+    w = np.zeros((m, ld), dtype=np.complex64)
+    w[:, :32 + n] = (rng.standard_normal((m, 32 + n)) + 1j * rng.standard_normal((m, 32 + n))).astype(np.complex64)
+    u = (rng.standard_normal((32, n)) + 1j * rng.standard_normal((32, n))).astype(np.complex64)
+    hi, lo = pack_bt(u)
+    lib = nb.load()
+    outs = []
+    for name in ("n2d_gemm_tf32x3", "n2d_gemm_tf32x3_persistent"):
+        f = getattr(lib, name)
+        f.restype = C.c_int
+        f.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_longlong,
+                      C.c_longlong, C.c_void_p]
+        dw = torch.from_numpy(w.view(np.float32).copy()).cuda()
+        dhi, dlo = torch.from_numpy(hi).cuda(), torch.from_numpy(lo).cuda()
+        err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        base = dw.data_ptr()
+        assert f(base + 32 * 8, ld, base, ld, dhi.data_ptr(), dlo.data_ptr(), m, n, err.data_ptr())
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0
+        outs.append(dw.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
+
+
 # Run in a child process with NEC2C_CUDA_TC_WAIT_CYCLES=0: every update gives
 # up its wait for the products at once, sets the error word, leaves C as it
 # was, still waits (bounded) for the products before freeing its tensor
