@@ -139,6 +139,24 @@ st = np.asfortranarray(a.T.copy())
 assert nb.dense_backend_set("cuda-mixed")
 ok, _ = nb.factor_classic(st)
 assert not ok and "time-out" in nb.last_error(), nb.last_error()
+# So does the split-precision lockstep batch, through its batched kernel
+# (small updates) and the per-matrix persistent kernel (four large systems).
+f32b = lib.n2d_lu_factor32_batch
+f32b.restype = C.c_int
+f32b.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+for sizes in ((300, 200), (1200, 1200, 1200, 1200)):
+    cnt = len(sizes)
+    mats = []
+    for q, nq in enumerate(sizes):
+        aq = np.zeros((nq, nq), dtype=np.complex64)
+        aq[:, :] = rng.standard_normal((nq, nq)) + 1j * rng.standard_normal((nq, nq)) + np.diag(np.full(nq, 10.0))
+        mats.append(torch.from_numpy(aq.view(np.float32)).cuda())
+    pivs = [torch.zeros(nq, dtype=torch.int32, device="cuda") for nq in sizes]
+    info = (C.c_int * cnt)()
+    ok = f32b((C.c_void_p * cnt)(*[t.data_ptr() for t in mats]), (C.c_longlong * cnt)(*sizes),
+              (C.c_longlong * cnt)(*sizes), (C.c_void_p * cnt)(*[t.data_ptr() for t in pivs]), cnt, 0, info)
+    torch.cuda.synchronize()
+    assert not ok and "time-out" in nb.last_error(), nb.last_error()
 # The context is still usable: the FP64 factor runs and is right.
 assert nb.dense_backend_set("cuda")
 st = np.asfortranarray(a.T.copy())
