@@ -242,7 +242,6 @@ constexpr int MAXM = 30;   // restarts up to MAXM use this path
 constexpr int CGS_E = 4;   // elements per lane in the dots kernel
 constexpr double REORTH = 10.0;   // cancellation factor that triggers the second pass
 constexpr int CGS_GROUP = 32 * CGS_E;   // elements per warp group
-constexpr size_t CGS_SMEM = (size_t)(32 * CGS_GROUP) * sizeof(double2);
 
 // Hessenberg column j finished with h_{j+1,j} = after: previous rotations,
 // the new rotation, the residual estimate and the cycle's stop conditions
@@ -280,7 +279,8 @@ __device__ void finish_step(GmBuffers &b, GmState *st, int m, int j, double afte
 
 // h = V^H w for pass P (0: first, 1: reorthogonalisation, run only when
 // requested).  Warp q of a 1024-thread block handles basis vector q % kk over
-// element group q / kk; the w chunk sits in shared memory.
+// element group q / kk, reading w directly (each vector's warp reads the same
+// w values, so they come from L2 and L1).
 template <int P>
 __global__ void __launch_bounds__(1024) cgs_dots_kernel(GmBuffers b, long long n, int m, int j) {
   pdl_begin();
@@ -296,46 +296,32 @@ __global__ void __launch_bounds__(1024) cgs_dots_kernel(GmBuffers b, long long n
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int k = warp % kk, grp = warp / kk;
   const bool active = grp < groups;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2 *sw = reinterpret_cast<double2 *>(smem_raw);   // [chunk]
   double2 acc = make_double2(0, 0);
   const long long stride = (long long)gridDim.x * chunk;
-  const int wper = (chunk + blockDim.x - 1) / blockDim.x;
-  double2 v[CGS_E], vn[CGS_E], wv[4], wn[4];
-  auto load = [&](long long base, double2 (&vv)[CGS_E], double2 (&ww)[4]) {
-    if (active) {
-      const double2 *vk = b.V + (long long)k * n;
+  // Each active warp streams its vector's elements of the group with the
+  // matching w values, read straight from global memory (w is read by every
+  // vector's warp, so it is served from L2 and L1); the next chunk's loads are
+  // issued before the current one is used.  No barrier inside the loop.
+  double2 v[CGS_E], vn[CGS_E], wv[CGS_E], wn[CGS_E];
+  auto load = [&](long long base, double2 (&vv)[CGS_E], double2 (&ww)[CGS_E]) {
+    const double2 *vk = b.V + (long long)k * n;
 #pragma unroll
-      for (int e = 0; e < CGS_E; ++e) {
-        const long long i = base + grp * CGS_GROUP + lane + 32 * e;
-        vv[e] = i < n ? vk[i] : make_double2(0, 0);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int t = threadIdx.x + q * blockDim.x;
-      ww[q] = (q < wper && t < chunk && base + t < n) ? b.w[base + t] : make_double2(0, 0);
+    for (int e = 0; e < CGS_E; ++e) {
+      const long long i = base + grp * CGS_GROUP + lane + 32 * e;
+      vv[e] = i < n ? vk[i] : make_double2(0, 0);
+      ww[e] = i < n ? b.w[i] : make_double2(0, 0);
     }
   };
   long long base = (long long)blockIdx.x * chunk;
-  if (base < n) load(base, v, wv);
-  for (; base < n; base += stride) {
+  if (active && base < n) {
+    load(base, v, wv);
+    for (; base < n; base += stride) {
+      if (base + stride < n) load(base + stride, vn, wn);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int t = threadIdx.x + q * blockDim.x;
-      if (q < wper && t < chunk) sw[t] = wv[q];
+      for (int e = 0; e < CGS_E; ++e) acc = cadd(acc, cconjmul(v[e], wv[e]));
+#pragma unroll
+      for (int e = 0; e < CGS_E; ++e) { v[e] = vn[e]; wv[e] = wn[e]; }
     }
-    if (base + stride < n) load(base + stride, vn, wn);
-    __syncthreads();
-    if (active) {
-#pragma unroll
-      for (int e = 0; e < CGS_E; ++e) acc = cadd(acc, cconjmul(v[e], sw[grp * CGS_GROUP + lane + 32 * e]));
-    }
-    __syncthreads();
-#pragma unroll
-    for (int e = 0; e < CGS_E; ++e) v[e] = vn[e];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) wv[q] = wn[q];
   }
   double2 *parts = (double2 *)(b.partials + PART_BLOCKS);
   __shared__ double2 red[32];
@@ -625,9 +611,9 @@ static int enqueue_inner(const OpView &o, GmWork *w) {
         const char *v = getenv("NEC2C_CUDA_PDL_GMRES");
         return v && v[0] == '1';
       }();
-      ok = n2c_launch_pdl(pdl, cgs_dots_kernel<0>, dim3(gb), dim3(1024), CGS_SMEM, "cgs dots", b, n, (int)m, j) &&
+      ok = n2c_launch_pdl(pdl, cgs_dots_kernel<0>, dim3(gb), dim3(1024), 0, "cgs dots", b, n, (int)m, j) &&
            n2c_launch_pdl(pdl, cgs_update_kernel<0>, dim3(ub), dim3(256), 0, "cgs update", b, n, (int)m, j) &&
-           n2c_launch_pdl(pdl, cgs_dots_kernel<1>, dim3(gb), dim3(1024), CGS_SMEM, "cgs dots", b, n, (int)m, j) &&
+           n2c_launch_pdl(pdl, cgs_dots_kernel<1>, dim3(gb), dim3(1024), 0, "cgs dots", b, n, (int)m, j) &&
            n2c_launch_pdl(pdl, cgs_update_kernel<1>, dim3(ub), dim3(256), 0, "cgs update", b, n, (int)m, j) &&
            n2c_launch_pdl(pdl, normalize_kernel, dim3(grid1(n)), dim3(256), 0, "cgs normalize", b, n, j);
     } else {
@@ -667,14 +653,6 @@ static int gmres_core(const OpView &o, const double2 *b_dev, double2 *x_dev, siz
   long long m = (long long)restart;
   if (m > n) m = n;
   if (m > (long long)maxit) m = (long long)maxit;
-  if (o.mixed && m <= MAXM) {
-    static const bool configured = [] {
-      cudaFuncSetAttribute(cgs_dots_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
-      cudaFuncSetAttribute(cgs_dots_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CGS_SMEM);
-      return true;
-    }();
-    (void)configured;
-  }
   GmWork *w = work_get(o, m);
   if (!w) { rep->status = ST_ALLOC; return 0; }
   GmBuffers &b = w->b;
