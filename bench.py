@@ -67,7 +67,7 @@ def parse():
                          "mixed form's saturated request rate")
     ap.add_argument("--c4-plain-requests", type=int, default=None,
                     help="serving_c4 long-stream run: requests of the plain FP64 arm (a prefix of the stream)")
-    ap.add_argument("--requests", type=int, default=240,
+    ap.add_argument("--requests", type=int, default=400,
                     help="serving_c4 profiling mode: requests in the stream (config 4 names 10,000)")
     ap.add_argument("--planes", type=int, choices=[0, 1], default=None,
                     help="profiling driver: pin the fused yz-plane passes on (1) or off (0) in both "
@@ -1346,7 +1346,7 @@ def serving_bench(nb, torch):
 DENSE_MERGE = 16
 
 
-def serving_stream_c4(nb, torch, requests=240, sizes_per_model=16, rates=(0.3, 0.5, 0.7, 0.9, 1.1),
+def serving_stream_c4(nb, torch, requests=400, sizes_per_model=16, rates=(0.3, 0.5, 0.7, 0.9, 1.1),
                       lattices=(8, 16, 24, 32, 48), seed=11, arms=None, plain_requests=None):
     """BASELINE config 4 shaped stream through the request server.
 
