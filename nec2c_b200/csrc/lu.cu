@@ -1805,8 +1805,14 @@ static int factor_batch(void *const *a_dev, const long long *n, const long long 
   cudaError_t e = cudaMemcpyAsync(hs.data(), dst, count * sizeof(LuStatus), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (ok && e != cudaSuccess) { n2c_set_error("reading the batch status: %s", cudaGetErrorString(e)); ok = 0; }
+  // A panel's time-out lands in its own system's word; the batched staged
+  // update's in the first system's (its launch covers them all).
   for (int i = 0; ok && i < count; ++i) {
-    if (hs[i].error) { n2c_set_error("LU kernel wait time-out (batched system %d)", i); ok = 0; }
+    if (hs[i].error) {
+      n2c_set_error("LU kernel wait time-out in a batch of %d (a panel of system %d, or a batched update when "
+                    "%d is 0)", count, i, i);
+      ok = 0;
+    }
     info[i] = hs[i].info;
   }
   n2d_free_async(dev);
