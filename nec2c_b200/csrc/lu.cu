@@ -1805,12 +1805,12 @@ static int factor_batch(void *const *a_dev, const long long *n, const long long 
   cudaError_t e = cudaMemcpyAsync(hs.data(), dst, count * sizeof(LuStatus), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (ok && e != cudaSuccess) { n2c_set_error("reading the batch status: %s", cudaGetErrorString(e)); ok = 0; }
-  // A panel's time-out lands in its own system's word; the batched staged
-  // update's in the first system's (its launch covers them all).
+  // A panel's or a per-matrix update's time-out lands in its own system's
+  // status word; the batched staged update's in the first system's (its
+  // launch covers them all).
   for (int i = 0; ok && i < count; ++i) {
     if (hs[i].error) {
-      n2c_set_error("LU kernel wait time-out in a batch of %d (a panel of system %d, or a batched update when "
-                    "%d is 0)", count, i, i);
+      n2c_set_error("LU kernel wait time-out in a batch of %d (status word of system %d)", count, i);
       ok = 0;
     }
     info[i] = hs[i].info;
